@@ -1,0 +1,224 @@
+/*
+ * pvof.h -- C ABI of the B200 implementation of PARTIES' two-phase
+ * (diffuse-interface Cahn-Hilliard) RK3 substep.
+ *
+ * Every entry point takes plain pointers and sizes; no CUDA or torch type
+ * appears here.  A context owns the device copy of the solver state.  Host
+ * arrays exchanged with pvof_upload_field / pvof_download_field use the
+ * reference's field layout: one contiguous block per field, element (i,j,k)
+ * at ((k-Ks)*nJ + (j-Js))*nI + (i-Is), i fastest, where
+ *   ghosted ("flow") fields span i in [-G, NX+G), j in [-G, NY+G),
+ *     k in [-G, NZ+G)            (PARTIES/src/Memory.c:36-89), and
+ *   no-ghost ("ng_") fields span i in [0, NX), j in [0, NY), k in [0, NZ)
+ *                                (PARTIES/src/Memory.c:270-323),
+ * with NX = NXM+1, NY = NYM+1, NZ = NZM+1 (a half cell is added at the far end
+ * of every direction, PARTIES/src/Grid.c:60-64) and G = ghost_nodes = 3.
+ * In the 2D modes NZM = 1 and the device keeps the k = 0 plane only; upload
+ * reads the k = 0 plane of the block and download writes it to every plane
+ * of the G range (the reference keeps those planes identical).
+ *
+ * Routine entry points keep the reference's names with a pvof_ prefix.  The
+ * reference passes the RK stage and dt through Parameters (which_stage, dt);
+ * here they are set once per substep with pvof_set_stage().
+ *
+ * Errors: functions return 0 (or a non-negative count) on success and a
+ * negative PVOF_E* code on failure; pvof_last_error() gives a message.  The
+ * reference aborts through Display_throw_error (PARTIES/src/IO/Display.c:910);
+ * the caller decides what to do with the code.  Iterative solvers always stop
+ * at their iteration limits and report non-convergence in the statistics.
+ */
+#ifndef PVOF_H
+#define PVOF_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PVOF_ABI_VERSION 1
+
+/* error codes */
+#define PVOF_OK 0
+#define PVOF_EINVAL (-1)     /* bad argument or unsupported configuration */
+#define PVOF_ECUDA (-2)      /* CUDA runtime error */
+#define PVOF_ENOMEM (-3)     /* device allocation failed */
+#define PVOF_ENODEV (-4)     /* no CUDA device */
+#define PVOF_EDIVERGED (-5)  /* the outer Poisson loop did not reach div < 1e-6 in 10 passes */
+
+/* geometry (runtime form of the reference's TWOD_CARTESIAN / AXISYM_RZ flags,
+ * PARTIES/src/Include/Boundary.h:36-38) */
+#define PVOF_GEOM_3D 0
+#define PVOF_GEOM_PLANAR 1
+#define PVOF_GEOM_AXISYM 2
+
+/* wall type per face (Boundary.h x/y/z boundary macros) */
+#define PVOF_WALL_NOSLIP 0
+#define PVOF_WALL_FREESLIP 1
+
+/* faces */
+#define PVOF_LEFT 0
+#define PVOF_RIGHT 1
+#define PVOF_BOTTOM 2
+#define PVOF_TOP 3
+#define PVOF_BACK 4
+#define PVOF_FRONT 5
+
+/* Grid and case description: the [geometry], [grid], [twod] sections of the
+ * reference's parties.inp (PARTIES/src/IO/default.inp) plus the compile-time
+ * boundary flags of Boundary.h. */
+typedef struct pvof_grid_desc {
+    int NXM, NYM, NZM;          /* physical cells per direction */
+    int ghost_nodes;            /* must be 3 */
+    int geometry;               /* PVOF_GEOM_* */
+    int periodic[3];            /* XPERIODIC, YPERIODIC, ZPERIODIC */
+    int wall[6];                /* PVOF_WALL_* per face (ignored on periodic axes) */
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+    double slab_thickness;      /* twod_slab_thickness after Input.c defaults */
+    double theta_span;          /* axisym_theta_span */
+} pvof_grid_desc;
+
+/* Physical and solver parameters: [flow], [vof], [particle] grav, [conc]
+ * richardson and [lsolve] of parties.inp, plus the SURFACE_TENSION and
+ * VOF_GRAVITY compile flags. */
+typedef struct pvof_params {
+    double Re, We;
+    double rho1, rho2, mu1, mu2;
+    double Cn, Pe_CH;
+    double grav[3];
+    double richardson;
+    double dp_dx;
+    int weno_order;
+    int ch_iter_max;
+    double ch_tol;
+    int CG_MAXIT;
+    double CG_ETOL;
+    int P_CG_MAXIT;
+    double P_CG_ETOL;
+    int surface_tension;        /* SURFACE_TENSION */
+    int gravity;                /* VOF_GRAVITY */
+} pvof_params;
+
+/* Field identifiers for upload/download. */
+enum pvof_field {
+    PVOF_F_C_L = 0, PVOF_F_C_G, PVOF_F_C_S, PVOF_F_F,
+    PVOF_F_RHO, PVOF_F_MU, PVOF_F_PSI_LG, PVOF_F_LAP_C,
+    PVOF_F_CH_RHS_N, PVOF_F_CH_RHS_CUR,
+    PVOF_F_U, PVOF_F_V, PVOF_F_W, PVOF_F_U_BC, PVOF_F_V_BC,
+    PVOF_F_P, PVOF_F_DELTAP, PVOF_F_P_RHS,
+    /* no-ghost momentum arrays (Velocity ng_*) */
+    PVOF_F_U_EXPLICIT, PVOF_F_U_EXPLICIT_OLD, PVOF_F_U_IMPLICIT,
+    PVOF_F_U_VISC_EXPLICIT, PVOF_F_U_VISC_EXPLICIT_OLD, PVOF_F_U_RHS,
+    PVOF_F_V_EXPLICIT, PVOF_F_V_EXPLICIT_OLD, PVOF_F_V_IMPLICIT,
+    PVOF_F_V_VISC_EXPLICIT, PVOF_F_V_VISC_EXPLICIT_OLD, PVOF_F_V_RHS,
+    /* no-ghost surface-tension face forces */
+    PVOF_F_FSIG_OLD_X, PVOF_F_FSIG_OLD_Y, PVOF_F_FSIG_NEW_X, PVOF_F_FSIG_NEW_Y,
+    PVOF_F_COUNT
+};
+
+/* Per-substep statistics (iteration counts and residuals the reference
+ * prints through Display_progress). */
+typedef struct pvof_stats {
+    int ch_iters;          /* biharmonic CG iterations (VOF_DIFFUSE.c:1048) */
+    double ch_rel_res;
+    int u_iters, v_iters;  /* velocity PCG iterations (msolve_cg.c:716) */
+    double u_rms, v_rms;
+    int p_iters;           /* pressure PCG iterations of the last Poisson pass */
+    int p_iters_total;     /* over all passes of the outer Poisson loop */
+    double p_res;
+    int poisson_passes;    /* outer loop count (Temporal_int.c:1052-1107) */
+    double div_max;        /* Pressure_compute_velocity_divergence */
+    double clamp_mass;     /* liquid mass changed by the C_L clamp (VOF_DIFFUSE.c:1093) */
+} pvof_stats;
+
+typedef struct pvof_ctx pvof_ctx;
+
+/* Library */
+int pvof_abi_version(void);
+const char *pvof_last_error(void);
+int pvof_device_count(void);
+
+/* Context: allocates the device state for one case on `device`.
+ * Replaces the allocation done by Velocity_create / Pressure_create /
+ * VoF_create (PARTIES/src/Cart3d.c:339-390) for the fields listed above. */
+int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int device, pvof_ctx **out);
+int pvof_destroy(pvof_ctx *ctx);
+
+/* Host <-> device copies of one field in the reference block layout (see the
+ * header comment); count = number of doubles in the host block, checked. */
+int pvof_upload_field(pvof_ctx *ctx, int field, const double *host_block, size_t count);
+int pvof_download_field(pvof_ctx *ctx, int field, double *host_block, size_t count);
+/* number of doubles in the host block of `field` */
+size_t pvof_field_block_count(const pvof_ctx *ctx, int field);
+int pvof_synchronize(pvof_ctx *ctx);
+
+/* Stage and time step of the following routine calls: the reference's
+ * params->which_stage (0..2) and params->dt. */
+int pvof_set_stage(pvof_ctx *ctx, int which_stage, double dt);
+
+/* Start-up after the initial fields (F, u, v, p) are uploaded:
+ * Velocity_update_boundaries of u and v, Pressure_apply_BCs and ghost update
+ * of p, the VOF part of Cart3d_initialize_primitive_data
+ * (PARTIES/src/Cart3d.c:1096-1130: boundary values of F, VOF_DIFFUSE_init,
+ * density and viscosity, surface-tension bootstrap with f_old = f_new) and the
+ * cell-centred velocity of the first substep.  Resets the time to 0. */
+int pvof_initialize(pvof_ctx *ctx);
+
+/* --- routines, reference name and file:line each replaces --------------- */
+/* VOF_DIFFUSE.c:524-568 VOF_DIFFUSE_init (C_L from F, clamp, phase cache) */
+int pvof_VOF_DIFFUSE_init(pvof_ctx *ctx);
+/* VOF_DIFFUSE.c:1262-1359 VOF_DIFFUSE_step: WENO5 advection, explicit
+ * diffusion, RK assembly, implicit biharmonic CG, clamp, history shift */
+int pvof_VOF_DIFFUSE_step(pvof_ctx *ctx, pvof_stats *stats);
+/* VOF_DIFFUSE.c:931-996 VOF_DIFFUSE_advect_WENO5, result in CH_RHS_CUR */
+int pvof_VOF_DIFFUSE_advect_WENO5(pvof_ctx *ctx);
+/* VOF_Advection.c:743-749 -> VOF_DIFFUSE.c:1453-1488 rho, mu from C */
+int pvof_VOF_update_density_viscosity(pvof_ctx *ctx);
+/* VOF_DIFFUSE.c:907-929 psi_LG */
+int pvof_VOF_DIFFUSE_compute_psi_LG(pvof_ctx *ctx);
+/* VOF_DIFFUSE.c:1364-1445 face surface-tension force into f_sigma_new */
+int pvof_VOF_DIFFUSE_compute_f_sigma(pvof_ctx *ctx);
+/* VOF_SurfaceTension.c:1983-2041 rhs += f_sigma_old */
+int pvof_VOF_apply_f_sigma_old(pvof_ctx *ctx);
+/* VOF_SurfaceTension.c:2055-2071 swap new/old force arrays */
+int pvof_VOF_swap_f_sigma(pvof_ctx *ctx);
+/* VOF_SurfaceTension.c:2075-2154 gravity term */
+int pvof_Velocity_add_gravity_2_RHS(pvof_ctx *ctx);
+/* Velocity.c:278-357 cell-centred velocity (with ghost update) */
+int pvof_Velocity_cell_center(pvof_ctx *ctx);
+/* Velocity.c:366-762 (component 'u'), :771-1148 ('v') */
+int pvof_Velocity_set_implicit_explicit(pvof_ctx *ctx, char component);
+/* Velocity.c:1494-1728 ('u'), :1739-1940 ('v') */
+int pvof_Velocity_set_RHS(pvof_ctx *ctx, char component);
+/* msolve_cg.c:525-722 Velocity_solve_cg; returns iterations */
+int pvof_Velocity_solve_cg(pvof_ctx *ctx, char component, pvof_stats *stats);
+/* Velocity.c:2427-2806 Velocity_update_boundaries (VEL_TYPE_NORMAL) */
+int pvof_Velocity_update_boundaries(pvof_ctx *ctx, char component);
+/* Pressure.c:100-196 (after the deltap reset of Temporal_int.c:1056) */
+int pvof_Pressure_set_RHS(pvof_ctx *ctx);
+/* psolve_cg.c:63-101 */
+int pvof_Pressure_compute_preconditioner(pvof_ctx *ctx);
+/* psolve_cg.c:130-293; returns iterations */
+int pvof_Pressure_solve_cg(pvof_ctx *ctx, pvof_stats *stats);
+/* Pressure.c:218-464 */
+int pvof_Pressure_project_velocity(pvof_ctx *ctx);
+/* Pressure.c:475-597; writes the max |div| to *div_max */
+int pvof_Pressure_compute_velocity_divergence(pvof_ctx *ctx, double *div_max);
+
+/* Temporal_int.c:563-1279 Temporal_int_all_the_equations for a case without
+ * solids: one complete RK substep at the stage/dt set by pvof_set_stage. */
+int pvof_substep(pvof_ctx *ctx, pvof_stats *stats);
+/* Temporal_int.c:399-448: nsteps time steps of three substeps each at a
+ * constant dt (cell-centred velocity refreshed at stage 0 after t = 0).
+ * stats (optional) receives the last substep's statistics. */
+int pvof_run_steps(pvof_ctx *ctx, int nsteps, double dt, pvof_stats *stats);
+
+/* Sum of C_L * cell measure over the physical cells (mass diagnostic,
+ * VOF_DIFFUSE.c:1071-1091), computed on the device in FP64. */
+int pvof_liquid_mass(pvof_ctx *ctx, double *mass);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,3 @@
+"""Host side of the B200 two-phase substep: ctypes mirror of include/pvof.h,
+case builders and the ``Solver`` wrapper around the CUDA library."""
+from . import abi, cases  # noqa: F401

@@ -1,0 +1,155 @@
+"""Synthetic two-phase cases and the reference field layout on the host.
+
+Each case returns a grid description, the solver parameters and the initial
+fields on the G range of one k plane ([j][i], i fastest, NX = NXM+1 by
+NY = NYM+1 values, the half cell included).  ``plane_to_block`` expands such a
+plane into the reference's ghosted block layout (PARTIES/src/Memory.c:36-89)
+the same way the reference's arrays hold it: values on the G range of every k
+plane, zeros in the ghost frame.
+
+The initial conditions are injected directly because the reference's own
+initialisers (PARTIES/src/IO/VoF_Init.c) use other amplitudes and profiles.
+"""
+import math
+
+import numpy as np
+
+from . import abi
+
+G = 3  # ghost_nodes
+
+
+def dims(grid):
+    return grid.NXM + 1, grid.NYM + 1, grid.NZM + 1
+
+
+def block_shape(grid, ng=False):
+    NX, NY, NZ = dims(grid)
+    if ng:
+        return (NZ, NY, NX)
+    return (NZ + 2 * G, NY + 2 * G, NX + 2 * G)
+
+
+def plane_to_block(grid, plane, ng=False):
+    """Expand a G-range plane (NY, NX) into a host block of the field layout."""
+    NX, NY, NZ = dims(grid)
+    plane = np.asarray(plane, dtype=np.float64)
+    assert plane.shape == (NY, NX), (plane.shape, (NY, NX))
+    blk = np.zeros(block_shape(grid, ng), dtype=np.float64)
+    if ng:
+        blk[:, :, :] = plane[None]
+    else:
+        blk[G:G + NZ, G:G + NY, G:G + NX] = plane[None]
+    return blk
+
+
+def block_plane(grid, block, ng=False):
+    """The k = 0 plane of a host block, ghosts included for flow fields:
+    shape (NY+2G, NX+2G) for flow fields, (NY, NX) for no-ghost fields."""
+    blk = np.asarray(block).reshape(block_shape(grid, ng))
+    return blk[0] if ng else blk[G]
+
+
+def interior(grid, plane2d, ghosted=True):
+    """Physical cells (i < NX-1, j < NY-1) of a k = 0 plane."""
+    NX, NY, _ = dims(grid)
+    if ghosted:
+        return plane2d[G:G + NY - 1, G:G + NX - 1]
+    return plane2d[:NY - 1, :NX - 1]
+
+
+def default_params(**kw):
+    p = abi.Params()
+    p.Re = 100.0
+    p.We = 1.0
+    p.rho1 = 1.0
+    p.rho2 = 1.0
+    p.mu1 = 1.0
+    p.mu2 = 1.0
+    p.Cn = 0.01
+    p.Pe_CH = 100.0
+    p.grav[0], p.grav[1], p.grav[2] = 0.0, -1.0, 0.0
+    p.richardson = 1.0
+    p.dp_dx = 0.0
+    p.weno_order = 5
+    p.ch_iter_max = 300
+    p.ch_tol = 1e-9
+    p.CG_MAXIT = 120
+    p.CG_ETOL = 1e-9
+    p.P_CG_MAXIT = 300
+    p.P_CG_ETOL = 1e-7
+    p.surface_tension = 0
+    p.gravity = 1
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def planar_grid(NXM, NYM, xmax, ymax, periodic_x=True, wall_y=abi.WALL_NOSLIP):
+    g = abi.GridDesc()
+    g.NXM, g.NYM, g.NZM = NXM, NYM, 1
+    g.ghost_nodes = G
+    g.geometry = abi.GEOM_PLANAR
+    g.periodic[0], g.periodic[1], g.periodic[2] = (1 if periodic_x else 0), 0, 1
+    for f in range(6):
+        g.wall[f] = abi.WALL_NOSLIP
+    g.wall[abi.BOTTOM] = wall_y
+    g.wall[abi.TOP] = wall_y
+    g.xmin, g.xmax = 0.0, float(xmax)
+    g.ymin, g.ymax = 0.0, float(ymax)
+    # 2D slab: thickness = min(hx, hy) (PARTIES/src/IO/Input.c:51-67)
+    hx = (g.xmax - g.xmin) / float(NXM)
+    hy = (g.ymax - g.ymin) / float(NYM)
+    g.slab_thickness = min(hx, hy)
+    g.zmin, g.zmax = 0.0, g.slab_thickness
+    g.theta_span = 2.0 * math.pi
+    return g
+
+
+def cell_centres(grid):
+    NX, NY, _ = dims(grid)
+    dx = (grid.xmax - grid.xmin) / float(NX - 1)
+    dy = (grid.ymax - grid.ymin) / float(NY - 1)
+    xc = grid.xmin + (0.5 + np.arange(NX)) * dx
+    yc = grid.ymin + (0.5 + np.arange(NY)) * dy
+    xu = grid.xmin + np.arange(NX) * dx
+    yv = grid.ymin + np.arange(NY) * dy
+    return xc, yc, xu, yv
+
+
+def rayleigh_taylor(NXM=128, NYM=512, Lx=1.0, Ly=4.0, Cn=0.01, amp=0.05,
+                    atwood=0.5, Re=3000.0, surface_tension=False, We=100.0,
+                    velocity_seed=None, velocity_amp=0.0, **param_kw):
+    """Planar two-phase instability: x periodic, no-slip walls in y, heavy
+    fluid (C = 1) on top of an interface at mid-height perturbed by
+    amp*cos(2 pi x / Lx); C = 0.5 (1 + tanh(d / (sqrt(2) Cn))).
+
+    ``velocity_seed`` adds a seeded random divergence-carrying velocity of
+    size ``velocity_amp`` (for parity cases that exercise the advection and
+    projection from the first substep)."""
+    grid = planar_grid(NXM, NYM, Lx, Ly)
+    rho2 = (1.0 - atwood) / (1.0 + atwood)
+    params = default_params(Re=Re, rho1=1.0, rho2=rho2, mu1=1.0, mu2=1.0,
+                            Cn=Cn, Pe_CH=1.0 / Cn,
+                            surface_tension=1 if surface_tension else 0,
+                            We=We, **param_kw)
+    xc, yc, xu, yv = cell_centres(grid)
+    X, Y = np.meshgrid(xc, yc)
+    d = Y - (0.5 * Ly + amp * np.cos(2.0 * np.pi * X / Lx))
+    C = 0.5 * (1.0 + np.tanh(d / (math.sqrt(2.0) * Cn)))
+    NX, NY, _ = dims(grid)
+    u = np.zeros((NY, NX))
+    v = np.zeros((NY, NX))
+    p = np.zeros((NY, NX))
+    if velocity_seed is not None:
+        rng = np.random.default_rng(velocity_seed)
+        Xu, Yc = np.meshgrid(xu, yc)
+        Xc, Yv = np.meshgrid(xc, yv)
+        k1, k2 = rng.integers(1, 4, size=2)
+        ph = rng.uniform(0, 2 * np.pi, size=4)
+        u = velocity_amp * (np.sin(2 * np.pi * k1 * Xu / Lx + ph[0]) * np.sin(np.pi * Yc / Ly)
+                            + 0.3 * rng.standard_normal((NY, NX)))
+        v = velocity_amp * (np.cos(2 * np.pi * k2 * Xc / Lx + ph[1]) * np.sin(np.pi * Yv / Ly)
+                            + 0.3 * rng.standard_normal((NY, NX)))
+        p = velocity_amp * rng.standard_normal((NY, NX))
+    return grid, params, {"F": C, "U": u, "V": v, "P": p}
