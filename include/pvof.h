@@ -217,6 +217,10 @@ int pvof_run_steps(pvof_ctx *ctx, int nsteps, double dt, pvof_stats *stats);
  * VOF_DIFFUSE.c:1071-1091), computed on the device in FP64. */
 int pvof_liquid_mass(pvof_ctx *ctx, double *mass);
 
+/* Number of CUDA kernels this context has launched so far (bookkeeping for
+ * benchmarks). */
+long long pvof_launch_count(const pvof_ctx *ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,1000 @@
+// C ABI (include/pvof.h) and host orchestration of the two-phase substep.
+//
+// Each pvof_* routine issues, on the context's stream, the kernels that
+// restate one reference routine, in the reference's order, including every
+// ghost update the reference performs at that point (file:line citations are
+// relative to PARTIES/src).  Nothing here computes on the host; there is no
+// CPU fallback: without a CUDA device pvof_create fails with PVOF_ENODEV.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pvof_kernels.cuh"
+
+using namespace pvof;
+
+struct pvof_ctx : public Ctx {};
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return set_err(PVOF_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+
+#define CKL(ctx)                                                                              \
+    do {                                                                                      \
+        (ctx)->launches++;                                                                    \
+        cudaError_t e_ = cudaGetLastError();                                                  \
+        if (e_ != cudaSuccess) return set_err(PVOF_ECUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define TRY(x)                      \
+    do {                            \
+        int rc_ = (x);              \
+        if (rc_ < 0) return rc_;    \
+    } while (0)
+
+constexpr int TBX = 32, TBY = 8;
+constexpr int COOP_THREADS = 256;
+
+bool is_ng(int field) { return field >= PVOF_F_U_EXPLICIT && field <= PVOF_F_FSIG_NEW_Y; }
+
+// ---------------------------------------------------------------------------
+// metrics and ghost maps, built on the host exactly as the reference does
+// ---------------------------------------------------------------------------
+
+// Grid.c:797-862 (uniform coordinates), :372-420 (widths), :871-918 (radii)
+struct HostMetrics {
+    std::vector<double> xu, xc, dx_u, dx_c, idx_u, idx_c, yv, yc, dy_v, dy_c, idy_v, idy_c;
+    std::vector<double> r_u, r_c, inv_r_u, inv_r_c, ring_wt_c;
+};
+
+void build_metrics(const pvof_grid_desc &g, int NX, int NY, HostMetrics &h)
+{
+    int nx = NX + 2 * NG, ny = NY + 2 * NG;
+    auto z = [](std::vector<double> &v, int n) { v.assign((size_t)n, 0.0); };
+    z(h.xu, nx); z(h.xc, nx); z(h.dx_u, nx); z(h.dx_c, nx); z(h.idx_u, nx); z(h.idx_c, nx);
+    z(h.yv, ny); z(h.yc, ny); z(h.dy_v, ny); z(h.dy_c, ny); z(h.idy_v, ny); z(h.idy_c, ny);
+    z(h.r_u, nx); z(h.r_c, nx); z(h.inv_r_u, nx); z(h.inv_r_c, nx); z(h.ring_wt_c, nx);
+    double Lx = g.xmax - g.xmin, Ly = g.ymax - g.ymin;
+    double dx = Lx / (double)(NX - 1), dy = Ly / (double)(NY - 1);
+    for (int i = -NG; i < NX + NG; i++) {
+        h.xu[i + NG] = g.xmin + i * dx;
+        h.xc[i + NG] = g.xmin + (0.5 + i) * dx;
+    }
+    for (int j = -NG; j < NY + NG; j++) {
+        h.yv[j + NG] = g.ymin + j * dy;
+        h.yc[j + NG] = g.ymin + (0.5 + j) * dy;
+    }
+    for (int i = -NG; i < NX + NG - 1; i++) {
+        h.dx_u[i + NG] = h.xu[i + 1 + NG] - h.xu[i + NG];
+        h.dx_c[i + NG] = h.xc[i + 1 + NG] - h.xc[i + NG];
+        h.idx_u[i + NG] = 1.0 / h.dx_u[i + NG];
+        h.idx_c[i + NG] = 1.0 / h.dx_c[i + NG];
+    }
+    for (int j = -NG; j < NY + NG - 1; j++) {
+        h.dy_v[j + NG] = h.yv[j + 1 + NG] - h.yv[j + NG];
+        h.dy_c[j + NG] = h.yc[j + 1 + NG] - h.yc[j + NG];
+        h.idy_v[j + NG] = 1.0 / h.dy_v[j + NG];
+        h.idy_c[j + NG] = 1.0 / h.dy_c[j + NG];
+    }
+    if (g.geometry == PVOF_GEOM_AXISYM) {
+        for (int i = -NG; i < NX + NG; i++) {
+            double ru = std::fabs(h.xu[i + NG]), rc = std::fabs(h.xc[i + NG]);
+            h.r_u[i + NG] = ru;
+            h.r_c[i + NG] = rc;
+            h.inv_r_u[i + NG] = (ru > 1.0e-14) ? 1.0 / ru : 0.0;
+            h.inv_r_c[i + NG] = (rc > 1.0e-14) ? 1.0 / rc : 0.0;
+            h.ring_wt_c[i + NG] = g.theta_span * rc;
+        }
+    }
+}
+
+struct Map1 {
+    std::vector<int> src;
+    std::vector<double> mul;
+    int N;
+    void init(int n)
+    {
+        N = n;
+        src.resize((size_t)n + 2 * NG);
+        mul.assign((size_t)n + 2 * NG, 1.0);
+        for (int i = -NG; i < n + NG; i++) src[i + NG] = i;
+    }
+    void set(int i, int s, double m) { src[i + NG] = s; mul[i + NG] = m; }
+    // scalar-component periodic exchange (Communication.c:168-229)
+    void wrap_scalar()
+    {
+        for (int i = -NG; i <= -1; i++) set(i, i + (N - 1), 1.0);
+        for (int i = N - 1; i <= N + 1; i++) set(i, i - (N - 1), 1.0);
+    }
+    // face-component periodic exchange: first face aliased to the last
+    void wrap_face()
+    {
+        for (int i = -NG; i <= 0; i++) set(i, i + (N - 1), 1.0);
+        for (int i = N; i <= N + 2; i++) set(i, i - (N - 1), 1.0);
+    }
+};
+
+// One axis of one ghost-update kind.  `normal` is true for the velocity
+// component normal to this axis' walls (u on x, v on y).
+void axis_map(Map1 &m, int kind, int N, bool periodic, int wall_lo, int wall_hi, bool axisym_lo, bool normal_u_x,
+              bool is_x)
+{
+    m.init(N);
+    bool is_u = (kind == BK_U || kind == BK_U_CG);
+    bool is_v = (kind == BK_V || kind == BK_V_CG);
+    bool cg = (kind == BK_U_CG || kind == BK_V_CG);
+    bool normal = (is_x && is_u) || (!is_x && is_v);
+    (void)normal_u_x;
+    if (periodic) {
+        bool face = (kind == BK_WRAP_U && is_x) || (kind == BK_WRAP_V && !is_x) || (normal && (is_u || is_v));
+        if (face) m.wrap_face();
+        else m.wrap_scalar();
+        return;
+    }
+    switch (kind) {
+    case BK_SCALAR:  // VOF_DIFFUSE.c:591-663
+        for (int g = 1; g <= NG; g++) {
+            if (axisym_lo) m.set(-g, 0, 1.0);
+            else if (wall_lo == PVOF_WALL_FREESLIP) m.set(-g, g - 1, 1.0);
+            else m.set(-g, 0, 1.0);
+        }
+        for (int g = 0; g < NG; g++) {
+            if (wall_hi == PVOF_WALL_FREESLIP) m.set(N - 1 + g, N - 2 - g, 1.0);
+            else m.set(N - 1 + g, N - 2, 1.0);
+        }
+        break;
+    case BK_PRESSURE:  // psolve_cg.c:374-460
+        m.set(-1, 0, 1.0);
+        m.set(N - 1, N - 2, 1.0);
+        break;
+    case BK_U:
+    case BK_V:
+    case BK_U_CG:
+    case BK_V_CG:  // Velocity.c:2480-2700
+        if (normal) {
+            if (!cg || axisym_lo) m.set(0, 0, 0.0);
+            if (!cg) m.set(N - 1, N - 1, 0.0);
+        } else {
+            if (axisym_lo) m.set(-1, 0, 1.0);
+            else m.set(-1, 0, wall_lo == PVOF_WALL_NOSLIP ? -1.0 : 1.0);
+            m.set(N - 1, N - 2, wall_hi == PVOF_WALL_NOSLIP ? -1.0 : 1.0);
+        }
+        break;
+    default:  // exchange-only kinds on a walled axis: nothing
+        break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+template <class K, class... Args>
+int launch2d(pvof_ctx *c, K kernel, int i0, int i1, int j0, int j1, Args... args)
+{
+    if (i1 <= i0 || j1 <= j0) return PVOF_OK;
+    dim3 blk(TBX, TBY);
+    dim3 grd((unsigned)((i1 - i0 + TBX - 1) / TBX), (unsigned)((j1 - j0 + TBY - 1) / TBY));
+    kernel<<<grd, blk, 0, c->stream>>>(c->dom, i0, i1, j0, j1, args...);
+    CKL(c);
+    return PVOF_OK;
+}
+
+int fill(pvof_ctx *c, int kind, double *f)
+{
+    int n = 8 * (c->dom.NY + 2 * NG) + 8 * (c->dom.NX + 2 * NG);
+    k_fill<<<(n + 255) / 256, 256, 0, c->stream>>>(c->dom, c->maps[kind], f);
+    CKL(c);
+    return PVOF_OK;
+}
+
+int coop_blocks(pvof_ctx *c, int n)
+{
+    int b = (n + COOP_THREADS - 1) / COOP_THREADS;
+    if (b > c->coop_blocks) b = c->coop_blocks;
+    if (b < 1) b = 1;
+    return b;
+}
+
+template <class A>
+int coop_launch(pvof_ctx *c, const void *fn, A &args, int n)
+{
+    void *params[] = {&args};
+    int nb = coop_blocks(c, n);
+    CK(cudaLaunchCooperativeKernel(fn, dim3((unsigned)nb), dim3(COOP_THREADS), params, 0, c->stream));
+    c->launches++;
+    return PVOF_OK;
+}
+
+double *F(pvof_ctx *c, int id) { return c->f[id]; }
+double *S(pvof_ctx *c, int id) { return c->s[id]; }
+
+// loop ranges of the face-centred arrays (e.g. Velocity.c:395-410)
+void u_range(const pvof_ctx *c, int &i0, int &i1, int &j0, int &j1)
+{
+    i0 = 1; i1 = c->dom.NX - 1; j0 = 0; j1 = c->dom.NY - 1;
+    if (c->dom.perx) i1 = c->dom.NX;
+}
+void v_range(const pvof_ctx *c, int &i0, int &i1, int &j0, int &j1)
+{
+    i0 = 0; i1 = c->dom.NX - 1; j0 = 1; j1 = c->dom.NY - 1;
+    if (c->dom.pery) j1 = c->dom.NY;
+}
+
+// ---------------------------------------------------------------------------
+// routines
+// ---------------------------------------------------------------------------
+
+// VOF_DIFFUSE_compute_laplacian (VOF_DIFFUSE.c:834-861)
+int compute_laplacian(pvof_ctx *c, double *in, double *out)
+{
+    TRY(fill(c, BK_SCALAR, in));
+    TRY(launch2d(c, k_laplacian, 0, c->dom.NX, 0, c->dom.NY, (const double *)in, out));
+    return fill(c, BK_SCALAR, out);
+}
+
+int advect(pvof_ctx *c, double *out)
+{
+    const int NX = c->dom.NX, NY = c->dom.NY;
+    double *CL = F(c, PVOF_F_C_L);
+    TRY(fill(c, BK_SCALAR, CL));
+    TRY(launch2d(c, k_weno_flux, 0, NX, 0, NY, (const double *)CL, (const double *)F(c, PVOF_F_U),
+                 (const double *)F(c, PVOF_F_V), S(c, SC_FLUX_X), S(c, SC_FLUX_Y), c->p.weno_order == 5 ? 1 : 0));
+    TRY(fill(c, BK_WRAP_U, S(c, SC_FLUX_X)));
+    TRY(fill(c, BK_WRAP_V, S(c, SC_FLUX_Y)));
+    TRY(launch2d(c, k_flux_div, 0, NX, 0, NY, (const double *)S(c, SC_FLUX_X), (const double *)S(c, SC_FLUX_Y), out));
+    return fill(c, BK_SCALAR, out);
+}
+
+int phase_cache(pvof_ctx *c)
+{
+    size_t n = c->plane_elems;
+    k_phase_cache<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, c->base[PVOF_F_C_L], c->base[PVOF_F_C_S],
+                                                                      c->base[PVOF_F_C_G], c->base[PVOF_F_F]);
+    CKL(c);
+    return PVOF_OK;
+}
+
+int bound(pvof_ctx *c)
+{
+    const int NX = c->dom.NX, NY = c->dom.NY;
+    dim3 blk(TBX, TBY);
+    dim3 grd((unsigned)((NX + TBX - 1) / TBX), (unsigned)((NY + TBY - 1) / TBY));
+    k_bound<<<grd, blk, 0, c->stream>>>(c->dom, 0, NX, 0, NY, F(c, PVOF_F_C_L), F(c, PVOF_F_C_S), F(c, PVOF_F_C_G),
+                                        c->partials);
+    CKL(c);
+    k_finalize_sum<<<1, 256, 0, c->stream>>>(c->partials, (int)(grd.x * grd.y), &c->scal->clamp_delta);
+    CKL(c);
+    return PVOF_OK;
+}
+
+int vof_diffuse_init(pvof_ctx *c)
+{
+    size_t n = c->plane_elems;
+    k_clamp_from<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, c->base[PVOF_F_F], c->base[PVOF_F_C_L]);
+    CKL(c);
+    TRY(fill(c, BK_SCALAR, F(c, PVOF_F_C_L)));
+    TRY(phase_cache(c));
+    TRY(bound(c));
+    TRY(fill(c, BK_SCALAR, F(c, PVOF_F_C_L)));
+    TRY(phase_cache(c));
+    TRY(fill(c, BK_SCALAR, F(c, PVOF_F_C_L)));
+    TRY(phase_cache(c));
+    return fill(c, BK_SCALAR, F(c, PVOF_F_C_G));
+}
+
+int vof_diffuse_step(pvof_ctx *c)
+{
+    const int NX = c->dom.NX, NY = c->dom.NY, s = c->stage;
+    const double a_dt = 1.0 / (c->dt * bet(s));
+    const double bih = c->p.Cn * c->p.Cn / c->p.Pe_CH;
+    double *CL = F(c, PVOF_F_C_L), *cur = F(c, PVOF_F_CH_RHS_CUR), *aux = S(c, SC_CH_AUX1);
+    double *vec = S(c, SC_CH_RHS_NM1), *rn = F(c, PVOF_F_CH_RHS_N), *bS = S(c, SC_BULK_S);
+    double *psiLG = F(c, PVOF_F_PSI_LG);
+    // R(C) = -div(u C) + Pe^-1 L S(C)  (VOF_DIFFUSE.c:1287-1297)
+    TRY(advect(c, cur));
+    TRY(launch2d(c, k_bulk_S, 0, NX, 0, NY, (const double *)CL, (const double *)F(c, PVOF_F_C_S), bS));
+    TRY(fill(c, BK_SCALAR, bS));
+    TRY(compute_laplacian(c, bS, aux));
+    TRY(launch2d(c, k_div_by, 0, NX, 0, NY, aux, c->p.Pe_CH));
+    TRY(fill(c, BK_SCALAR, aux));
+    TRY(launch2d(c, k_add, 0, NX, 0, NY, cur, (const double *)aux));
+    TRY(fill(c, BK_SCALAR, cur));
+    TRY(launch2d(c, k_rhs_vec, 0, NX, 0, NY, vec, (const double *)CL, (const double *)cur, (const double *)rn, a_dt, s));
+    TRY(fill(c, BK_SCALAR, vec));
+    // implicit biharmonic (VOF_DIFFUSE.c:1018-1069)
+    TRY(compute_laplacian(c, CL, aux));
+    TRY(compute_laplacian(c, aux, psiLG));
+    TRY(launch2d(c, k_sub_scaled, 0, NX, 0, NY, vec, (const double *)psiLG, bih));
+    BihArgs A;
+    A.d = c->dom;
+    A.msc = c->maps[BK_SCALAR];
+    A.x = CL;
+    A.b = vec;
+    A.r = S(c, SC_CH_RES);
+    A.p1 = S(c, SC_CH_DIR);
+    A.p2 = S(c, SC_CH_DIR2);
+    A.Ap = F(c, PVOF_F_LAP_C);
+    A.aux = aux;
+    A.a_dt = a_dt;
+    A.bih = bih;
+    A.tol = (c->p.ch_tol > 0.0) ? c->p.ch_tol : c->p.CG_ETOL;
+    A.maxit = (c->p.ch_iter_max > 0) ? c->p.ch_iter_max : c->p.CG_MAXIT;
+    A.partials = c->partials;
+    A.scal = c->scal;
+    TRY(coop_launch(c, (const void *)k_cg_biharmonic, A, NX * NY));
+    TRY(fill(c, BK_SCALAR, CL));
+    // clamp, phase cache, history shift (VOF_DIFFUSE.c:1324-1358)
+    TRY(bound(c));
+    TRY(fill(c, BK_SCALAR, CL));
+    TRY(phase_cache(c));
+    size_t bytes = c->plane_elems * sizeof(double);
+    CK(cudaMemcpyAsync(c->sbase[SC_CH_RHS_NM1], c->base[PVOF_F_CH_RHS_N], bytes,
+                       cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->base[PVOF_F_CH_RHS_N], c->base[PVOF_F_CH_RHS_CUR], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    return PVOF_OK;
+}
+
+int update_density_viscosity(pvof_ctx *c)
+{
+    const double rho_g = c->p.rho2 / c->p.rho1, mu_g = c->p.mu2 / c->p.mu1;
+    TRY(launch2d(c, k_density, 0, c->dom.NX, 0, c->dom.NY, (const double *)F(c, PVOF_F_C_L),
+                 (const double *)F(c, PVOF_F_C_S), (const double *)F(c, PVOF_F_C_G), F(c, PVOF_F_RHO), F(c, PVOF_F_MU),
+                 rho_g, mu_g));
+    TRY(fill(c, BK_SCALAR, F(c, PVOF_F_RHO)));
+    return fill(c, BK_SCALAR, F(c, PVOF_F_MU));
+}
+
+int compute_psi_LG(pvof_ctx *c)
+{
+    double *CL = F(c, PVOF_F_C_L), *lap = F(c, PVOF_F_LAP_C), *psi = F(c, PVOF_F_PSI_LG);
+    TRY(compute_laplacian(c, CL, lap));
+    TRY(launch2d(c, k_psi_LG, 0, c->dom.NX, 0, c->dom.NY, (const double *)CL, (const double *)lap, psi,
+                 c->p.Cn * c->p.Cn));
+    return fill(c, BK_SCALAR, psi);
+}
+
+int compute_f_sigma(pvof_ctx *c)
+{
+    int ui0, ui1, uj0, uj1, vi0, vi1, vj0, vj1;
+    u_range(c, ui0, ui1, uj0, uj1);
+    v_range(c, vi0, vi1, vj0, vj1);
+    const double scale = 2.0 * 6.0 * std::sqrt(2.0) / (c->p.Cn * c->p.We + 1e-30);
+    return launch2d(c, k_f_sigma, 0, c->dom.NX, 0, c->dom.NY, (const double *)F(c, PVOF_F_C_L),
+                    (const double *)F(c, PVOF_F_C_G), (const double *)F(c, PVOF_F_C_S),
+                    (const double *)F(c, PVOF_F_PSI_LG), F(c, PVOF_F_FSIG_NEW_X), F(c, PVOF_F_FSIG_NEW_Y), scale, ui0,
+                    ui1, uj1, vj0, vi1, vj1);
+}
+
+int apply_f_sigma_old(pvof_ctx *c)
+{
+    int i0, i1, j0, j1;
+    u_range(c, i0, i1, j0, j1);
+    TRY(launch2d(c, k_add_to, i0, i1, j0, j1, F(c, PVOF_F_U_RHS), (const double *)F(c, PVOF_F_FSIG_OLD_X)));
+    v_range(c, i0, i1, j0, j1);
+    return launch2d(c, k_add_to, i0, i1, j0, j1, F(c, PVOF_F_V_RHS), (const double *)F(c, PVOF_F_FSIG_OLD_Y));
+}
+
+void swap_f_sigma(pvof_ctx *c)
+{
+    std::swap(c->f[PVOF_F_FSIG_OLD_X], c->f[PVOF_F_FSIG_NEW_X]);
+    std::swap(c->base[PVOF_F_FSIG_OLD_X], c->base[PVOF_F_FSIG_NEW_X]);
+    std::swap(c->f[PVOF_F_FSIG_OLD_Y], c->f[PVOF_F_FSIG_NEW_Y]);
+    std::swap(c->base[PVOF_F_FSIG_OLD_Y], c->base[PVOF_F_FSIG_NEW_Y]);
+}
+
+int add_gravity(pvof_ctx *c)
+{
+    const double *gr = c->p.grav;
+    double gm = std::sqrt(gr[0] * gr[0] + gr[1] * gr[1]);
+    double gx = 0.0, gy = 0.0;
+    if (gm > 0.0) { gx = gr[0] / gm; gy = gr[1] / gm; }
+    int i0, i1, j0, j1;
+    u_range(c, i0, i1, j0, j1);
+    TRY(launch2d(c, k_gravity, i0, i1, j0, j1, (const double *)F(c, PVOF_F_RHO), F(c, PVOF_F_U_RHS), 1, 0,
+                 c->p.richardson, gx));
+    v_range(c, i0, i1, j0, j1);
+    return launch2d(c, k_gravity, i0, i1, j0, j1, (const double *)F(c, PVOF_F_RHO), F(c, PVOF_F_V_RHS), 0, 1,
+                    c->p.richardson, gy);
+}
+
+int cell_center(pvof_ctx *c)
+{
+    TRY(fill(c, BK_WRAP_U, F(c, PVOF_F_U)));
+    TRY(fill(c, BK_WRAP_V, F(c, PVOF_F_V)));
+    return launch2d(c, k_cell_center, -NG, c->dom.NX + NG - 1, -NG, c->dom.NY + NG - 1, (const double *)F(c, PVOF_F_U),
+                    (const double *)F(c, PVOF_F_V), F(c, PVOF_F_U_BC), F(c, PVOF_F_V_BC));
+}
+
+int implicit_explicit(pvof_ctx *c, int comp)
+{
+    int i0, i1, j0, j1;
+    double iRe = 1.0 / c->p.Re;
+    if (comp == 0) {
+        u_range(c, i0, i1, j0, j1);
+        return launch2d(c, k_u_impexp, i0, i1, j0, j1, (const double *)F(c, PVOF_F_U), (const double *)F(c, PVOF_F_V),
+                        (const double *)F(c, PVOF_F_U_BC), (const double *)F(c, PVOF_F_MU), F(c, PVOF_F_U_EXPLICIT),
+                        F(c, PVOF_F_U_IMPLICIT), F(c, PVOF_F_U_VISC_EXPLICIT), iRe);
+    }
+    v_range(c, i0, i1, j0, j1);
+    return launch2d(c, k_v_impexp, i0, i1, j0, j1, (const double *)F(c, PVOF_F_U), (const double *)F(c, PVOF_F_V),
+                    (const double *)F(c, PVOF_F_V_BC), (const double *)F(c, PVOF_F_MU), F(c, PVOF_F_V_EXPLICIT),
+                    F(c, PVOF_F_V_IMPLICIT), F(c, PVOF_F_V_VISC_EXPLICIT), iRe);
+}
+
+int set_rhs(pvof_ctx *c, int comp)
+{
+    int s = c->stage;
+    double a_dt = 1.0 / (c->dt * bet(s));
+    int i0, i1, j0, j1;
+    if (comp == 0) {
+        u_range(c, i0, i1, j0, j1);
+        return launch2d(c, k_set_rhs, i0, i1, j0, j1, 0, (const double *)F(c, PVOF_F_U), (const double *)F(c, PVOF_F_P),
+                        (const double *)F(c, PVOF_F_RHO), F(c, PVOF_F_U_RHS), (const double *)F(c, PVOF_F_U_EXPLICIT),
+                        F(c, PVOF_F_U_EXPLICIT_OLD), (const double *)F(c, PVOF_F_U_VISC_EXPLICIT),
+                        F(c, PVOF_F_U_VISC_EXPLICIT_OLD), (const double *)F(c, PVOF_F_U_IMPLICIT), a_dt, s,
+                        -c->p.dp_dx);
+    }
+    v_range(c, i0, i1, j0, j1);
+    return launch2d(c, k_set_rhs, i0, i1, j0, j1, 1, (const double *)F(c, PVOF_F_V), (const double *)F(c, PVOF_F_P),
+                    (const double *)F(c, PVOF_F_RHO), F(c, PVOF_F_V_RHS), (const double *)F(c, PVOF_F_V_EXPLICIT),
+                    F(c, PVOF_F_V_EXPLICIT_OLD), (const double *)F(c, PVOF_F_V_VISC_EXPLICIT),
+                    F(c, PVOF_F_V_VISC_EXPLICIT_OLD), (const double *)F(c, PVOF_F_V_IMPLICIT), a_dt, s, -c->p.dp_dx);
+}
+
+int velocity_solve(pvof_ctx *c, int comp)
+{
+    VelArgs A;
+    A.d = c->dom;
+    A.comp = comp;
+    A.mcg = c->maps[comp == 0 ? BK_U_CG : BK_V_CG];
+    if (comp == 0) u_range(c, A.i0, A.i1, A.j0, A.j1);
+    else v_range(c, A.i0, A.i1, A.j0, A.j1);
+    A.x = F(c, comp == 0 ? PVOF_F_U : PVOF_F_V);
+    A.rhs = F(c, comp == 0 ? PVOF_F_U_RHS : PVOF_F_V_RHS);
+    A.rho = F(c, PVOF_F_RHO);
+    A.mu = F(c, PVOF_F_MU);
+    A.r = S(c, comp == 0 ? SC_U_R : SC_V_R);
+    A.dir = S(c, comp == 0 ? SC_U_D : SC_V_D);
+    A.Ad = S(c, comp == 0 ? SC_U_AD : SC_V_AD);
+    A.diag = S(c, comp == 0 ? SC_U_DIAG : SC_V_DIAG);
+    A.iRe = 1.0 / c->p.Re;
+    A.alpha_dt = bet(c->stage) * c->dt;
+    const int NX = c->dom.NX, NY = c->dom.NY, NZ = 2;
+    if (comp == 0) A.in_tot = c->dom.perx ? 1.0 / (double)((NX - 1) * (NY - 1) * (NZ - 1)) : 1.0 / (double)((NX - 2) * (NY - 1) * (NZ - 1));
+    else A.in_tot = c->dom.pery ? 1.0 / (double)((NX - 1) * (NY - 1) * (NZ - 1)) : 1.0 / (double)((NX - 1) * (NY - 2) * (NZ - 1));
+    A.tol = c->p.CG_ETOL;
+    A.maxit = c->p.CG_MAXIT;
+    A.partials = c->partials;
+    A.scal = c->scal;
+    return coop_launch(c, (const void *)k_cg_velocity, A, (A.i1 - A.i0) * (A.j1 - A.j0));
+}
+
+}  // namespace
+
+// the host copy of idx_u[1] is needed for the pressure RHS scale
+static double host_idx_u1(const pvof_ctx *c)
+{
+    double Lx = c->g.xmax - c->g.xmin;
+    int NX = c->g.NXM + 1;
+    double dx = Lx / (double)(NX - 1);
+    double xu1 = c->g.xmin + 1 * dx, xu2 = c->g.xmin + 2 * dx;
+    return 1.0 / (xu2 - xu1);
+}
+
+namespace {
+
+int p_set_rhs(pvof_ctx *c)
+{
+    CK(cudaMemsetAsync(c->base[PVOF_F_DELTAP], 0, c->plane_elems * sizeof(double), c->stream));
+    double a_dt = 1.0 / (c->dt * 2.0 * bet(c->stage));
+    double ihdt = host_idx_u1(c) * a_dt;
+    return launch2d(c, k_p_rhs, 0, c->dom.NX - 1, 0, c->dom.NY - 1, (const double *)F(c, PVOF_F_U),
+                    (const double *)F(c, PVOF_F_V), F(c, PVOF_F_P_RHS), ihdt);
+}
+
+int p_precond(pvof_ctx *c)
+{
+    return launch2d(c, k_p_precond, 0, c->dom.NX - 1, 0, c->dom.NY - 1, (const double *)F(c, PVOF_F_RHO), S(c, SC_P_MINV));
+}
+
+int p_solve(pvof_ctx *c)
+{
+    PresArgs A;
+    A.d = c->dom;
+    A.mp = c->maps[BK_PRESSURE];
+    A.phi = F(c, PVOF_F_DELTAP);
+    A.rhs = F(c, PVOF_F_P_RHS);
+    A.rho = F(c, PVOF_F_RHO);
+    A.M = S(c, SC_P_MINV);
+    A.res = S(c, SC_P_RES);
+    A.dir = S(c, SC_P_D);
+    A.Ad = S(c, SC_P_AD);
+    A.tol = c->p.P_CG_ETOL;
+    A.maxit = c->p.P_CG_MAXIT;
+    A.partials = c->partials;
+    A.scal = c->scal;
+    TRY(coop_launch(c, (const void *)k_cg_pressure, A, (c->dom.NX - 1) * (c->dom.NY - 1)));
+    return fill(c, BK_WRAP_C, F(c, PVOF_F_DELTAP));
+}
+
+int p_project(pvof_ctx *c)
+{
+    double *dp = F(c, PVOF_F_DELTAP), *pd = F(c, PVOF_F_P);
+    TRY(fill(c, BK_PRESSURE, dp));
+    TRY(launch2d(c, k_p_update, 0, c->dom.NX - 1, 0, c->dom.NY - 1, pd, (const double *)dp));
+    TRY(fill(c, BK_PRESSURE, pd));
+    double mdt = 2.0 * bet(c->stage) * c->dt;
+    int i0, i1, j0, j1;
+    u_range(c, i0, i1, j0, j1);
+    TRY(launch2d(c, k_project, i0, i1, j0, j1, 0, F(c, PVOF_F_U), (const double *)dp, (const double *)F(c, PVOF_F_RHO), mdt));
+    v_range(c, i0, i1, j0, j1);
+    return launch2d(c, k_project, i0, i1, j0, j1, 1, F(c, PVOF_F_V), (const double *)dp, (const double *)F(c, PVOF_F_RHO), mdt);
+}
+
+int p_divergence_async(pvof_ctx *c)
+{
+    CK(cudaMemsetAsync(&c->scal->div_max, 0, sizeof(double), c->stream));
+    return launch2d(c, k_div_max, 0, c->dom.NX - 1, 0, c->dom.NY - 1, (const double *)F(c, PVOF_F_U),
+                    (const double *)F(c, PVOF_F_V), (unsigned long long *)&c->scal->div_max);
+}
+
+int read_scalars(pvof_ctx *c)
+{
+    CK(cudaMemcpyAsync(c->scal_host, c->scal, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->scal_host->error) {
+        CK(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return set_err(PVOF_ECUDA, "solver grid barrier timed out");
+    }
+    return PVOF_OK;
+}
+
+void fill_stats(pvof_ctx *c, pvof_stats *st)
+{
+    if (!st) return;
+    const DevScalars &h = *c->scal_host;
+    st->ch_iters = h.ch_iters;
+    st->ch_rel_res = h.ch_rel;
+    st->u_iters = h.vel_iters[0];
+    st->v_iters = h.vel_iters[1];
+    st->u_rms = h.vel_rms[0];
+    st->v_rms = h.vel_rms[1];
+    st->p_iters = h.p_iters;
+    st->p_res = h.p_res;
+    st->div_max = h.div_max;
+    st->clamp_mass = h.clamp_delta;
+}
+
+int initialize(pvof_ctx *c)
+{
+    TRY(fill(c, BK_U, F(c, PVOF_F_U)));
+    TRY(fill(c, BK_V, F(c, PVOF_F_V)));
+    TRY(fill(c, BK_PRESSURE, F(c, PVOF_F_P)));
+    TRY(fill(c, BK_SCALAR, F(c, PVOF_F_F)));
+    TRY(vof_diffuse_init(c));
+    TRY(update_density_viscosity(c));
+    if (c->p.surface_tension) {
+        TRY(compute_psi_LG(c));
+        TRY(compute_f_sigma(c));
+        size_t bytes = c->plane_elems * sizeof(double);
+        CK(cudaMemcpyAsync(c->base[PVOF_F_FSIG_OLD_X], c->base[PVOF_F_FSIG_NEW_X], bytes, cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->base[PVOF_F_FSIG_OLD_Y], c->base[PVOF_F_FSIG_NEW_Y], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    TRY(cell_center(c));
+    c->time = 0.0;
+    return PVOF_OK;
+}
+
+// Temporal_int_all_the_equations (Temporal_int.c:563-1279), no solids
+int substep(pvof_ctx *c, pvof_stats *st)
+{
+    if (c->stage > 0) TRY(cell_center(c));
+    TRY(fill(c, BK_WRAP_C, F(c, PVOF_F_U_BC)));
+    TRY(fill(c, BK_WRAP_C, F(c, PVOF_F_V_BC)));
+    TRY(vof_diffuse_step(c));
+    TRY(update_density_viscosity(c));
+    TRY(implicit_explicit(c, 0));
+    TRY(implicit_explicit(c, 1));
+    TRY(set_rhs(c, 0));
+    TRY(set_rhs(c, 1));
+    if (c->p.surface_tension) {
+        TRY(compute_psi_LG(c));
+        TRY(compute_f_sigma(c));
+        TRY(apply_f_sigma_old(c));
+    }
+    if (c->p.gravity) TRY(add_gravity(c));
+    TRY(velocity_solve(c, 0));
+    TRY(velocity_solve(c, 1));
+    TRY(fill(c, BK_U, F(c, PVOF_F_U)));
+    TRY(fill(c, BK_V, F(c, PVOF_F_V)));
+    int passes = 0, p_total = 0;
+    int rc = PVOF_OK;
+    for (;;) {
+        TRY(p_set_rhs(c));
+        TRY(p_precond(c));
+        TRY(p_solve(c));
+        TRY(p_project(c));
+        TRY(fill(c, BK_U, F(c, PVOF_F_U)));
+        TRY(fill(c, BK_V, F(c, PVOF_F_V)));
+        TRY(p_divergence_async(c));
+        TRY(read_scalars(c));
+        passes++;
+        p_total += c->scal_host->p_iters;
+        if (passes > 10) { rc = set_err(PVOF_EDIVERGED, "Poisson solver did not converge"); break; }
+        if (!(c->scal_host->div_max > 1e-6)) break;
+    }
+    if (c->p.surface_tension) swap_f_sigma(c);
+    if (st) {
+        fill_stats(c, st);
+        st->p_iters_total = p_total;
+        st->poisson_passes = passes;
+    }
+    return rc;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int pvof_abi_version(void) { return PVOF_ABI_VERSION; }
+
+const char *pvof_last_error(void) { return g_err.c_str(); }
+
+int pvof_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int device, pvof_ctx **out)
+{
+    if (!grid || !params || !out) return set_err(PVOF_EINVAL, "null argument");
+    *out = nullptr;
+    if (grid->ghost_nodes != NG) return set_err(PVOF_EINVAL, "ghost_nodes must be 3");
+    if (grid->geometry != PVOF_GEOM_PLANAR && grid->geometry != PVOF_GEOM_AXISYM)
+        return set_err(PVOF_EINVAL, "only the 2D modes (planar, axisymmetric) are supported");
+    if (grid->NZM != 1) return set_err(PVOF_EINVAL, "2D modes need NZM == 1");
+    if (grid->NXM < 8 || grid->NYM < 8) return set_err(PVOF_EINVAL, "at least 8 cells per direction");
+    if (grid->geometry == PVOF_GEOM_AXISYM && grid->periodic[0]) return set_err(PVOF_EINVAL, "the axis cannot be periodic");
+    if (params->Re <= 0 || params->Pe_CH <= 0 || params->Cn <= 0) return set_err(PVOF_EINVAL, "Re, Pe_CH and Cn must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(PVOF_ENODEV, "no CUDA device");
+    if (device < 0 || device >= ndev) return set_err(PVOF_EINVAL, "bad device index");
+    CK(cudaSetDevice(device));
+
+    pvof_ctx *c = new pvof_ctx();
+    std::memset(static_cast<Ctx *>(c), 0, sizeof(Ctx));
+    c->g = *grid;
+    c->p = *params;
+    c->device = device;
+    Dom &d = c->dom;
+    d.NX = grid->NXM + 1;
+    d.NY = grid->NYM + 1;
+    d.P = ((d.NX + OX + NG + 1) + 31) / 32 * 32;
+    d.planar = grid->geometry == PVOF_GEOM_PLANAR;
+    d.axisym = grid->geometry == PVOF_GEOM_AXISYM;
+    d.perx = grid->periodic[0] != 0;
+    d.pery = grid->periodic[1] != 0;
+    d.nk = grid->NZM + 1;
+    d.slab = grid->slab_thickness;
+    c->plane_elems = (size_t)d.P * (size_t)(d.NY + 2 * NG);
+    const size_t origin = (size_t)OY * d.P + OX;
+    auto fail = [&](int code, const std::string &m) {
+        pvof_destroy(c);
+        return set_err(code, m);
+    };
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (int q = 0; q < PVOF_F_COUNT; q++) {
+        if (cudaMalloc(&c->base[q], c->plane_elems * sizeof(double)) != cudaSuccess) return fail(PVOF_ENOMEM, "cudaMalloc field");
+        cudaMemset(c->base[q], 0, c->plane_elems * sizeof(double));
+        c->f[q] = c->base[q] + origin;
+    }
+    for (int q = 0; q < SC_COUNT; q++) {
+        if (cudaMalloc(&c->sbase[q], c->plane_elems * sizeof(double)) != cudaSuccess) return fail(PVOF_ENOMEM, "cudaMalloc scratch");
+        cudaMemset(c->sbase[q], 0, c->plane_elems * sizeof(double));
+        c->s[q] = c->sbase[q] + origin;
+    }
+    // metrics
+    HostMetrics hm;
+    build_metrics(*grid, d.NX, d.NY, hm);
+    std::vector<const std::vector<double> *> mv = {&hm.idx_u, &hm.idx_c, &hm.dx_c, &hm.dx_u, &hm.r_u, &hm.r_c,
+                                                   &hm.inv_r_u, &hm.inv_r_c, &hm.ring_wt_c,
+                                                   &hm.idy_v, &hm.idy_c, &hm.dy_c, &hm.dy_v};
+    size_t mtot = 0;
+    for (auto *v : mv) mtot += v->size();
+    if (cudaMalloc(&c->metric_mem, mtot * sizeof(double)) != cudaSuccess) return fail(PVOF_ENOMEM, "cudaMalloc metrics");
+    std::vector<double> mh;
+    mh.reserve(mtot);
+    std::vector<const double *> mptr;
+    for (auto *v : mv) {
+        mptr.push_back(c->metric_mem + mh.size() + NG);
+        mh.insert(mh.end(), v->begin(), v->end());
+    }
+    if (cudaMemcpy(c->metric_mem, mh.data(), mtot * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(PVOF_ECUDA, "metric copy");
+    d.m.idx_u = mptr[0]; d.m.idx_c = mptr[1]; d.m.dx_c = mptr[2]; d.m.dx_u = mptr[3];
+    d.m.r_u = mptr[4]; d.m.r_c = mptr[5]; d.m.inv_r_u = mptr[6]; d.m.inv_r_c = mptr[7]; d.m.ring_wt_c = mptr[8];
+    d.m.idy_v = mptr[9]; d.m.idy_c = mptr[10]; d.m.dy_c = mptr[11]; d.m.dy_v = mptr[12];
+    // ghost maps
+    std::vector<int> srcs;
+    std::vector<double> muls;
+    std::vector<size_t> offx(BK_COUNT), offy(BK_COUNT);
+    bool axis_lo = d.axisym;
+    for (int k = 0; k < BK_COUNT; k++) {
+        Map1 mx, my;
+        axis_map(mx, k, d.NX, d.perx, grid->wall[PVOF_LEFT], grid->wall[PVOF_RIGHT], axis_lo, true, true);
+        axis_map(my, k, d.NY, d.pery, grid->wall[PVOF_BOTTOM], grid->wall[PVOF_TOP], false, false, false);
+        offx[k] = srcs.size();
+        srcs.insert(srcs.end(), mx.src.begin(), mx.src.end());
+        muls.insert(muls.end(), mx.mul.begin(), mx.mul.end());
+        offy[k] = srcs.size();
+        srcs.insert(srcs.end(), my.src.begin(), my.src.end());
+        muls.insert(muls.end(), my.mul.begin(), my.mul.end());
+    }
+    if (cudaMalloc(&c->map_src_mem, srcs.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c->map_mul_mem, muls.size() * sizeof(double)) != cudaSuccess)
+        return fail(PVOF_ENOMEM, "cudaMalloc maps");
+    cudaMemcpy(c->map_src_mem, srcs.data(), srcs.size() * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->map_mul_mem, muls.data(), muls.size() * sizeof(double), cudaMemcpyHostToDevice);
+    for (int k = 0; k < BK_COUNT; k++) {
+        c->maps[k].x.src = c->map_src_mem + offx[k];
+        c->maps[k].x.mul = c->map_mul_mem + offx[k];
+        c->maps[k].y.src = c->map_src_mem + offy[k];
+        c->maps[k].y.mul = c->map_mul_mem + offy[k];
+    }
+    // persistent-solver occupancy
+    int nsm = 0, ob = 0, o1 = 0, o2 = 0, o3 = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    if (!coop) return fail(PVOF_ENODEV, "device without cooperative launch");
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_cg_biharmonic, COOP_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_cg_velocity, COOP_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, k_cg_pressure, COOP_THREADS, 0);
+    ob = std::min(o1, std::min(o2, o3));
+    if (ob < 1) return fail(PVOF_ECUDA, "persistent solver kernels do not fit on an SM");
+    c->coop_blocks = ob * nsm;
+    c->coop_threads = COOP_THREADS;
+    size_t npart = 4 * (size_t)std::max(c->coop_blocks, (int)(((d.NX + TBX - 1) / TBX) * ((d.NY + TBY - 1) / TBY)));
+    if (cudaMalloc(&c->partials, npart * sizeof(double)) != cudaSuccess) return fail(PVOF_ENOMEM, "cudaMalloc partials");
+    if (cudaMalloc(&c->scal, sizeof(DevScalars)) != cudaSuccess) return fail(PVOF_ENOMEM, "cudaMalloc scalars");
+    cudaMemset(c->scal, 0, sizeof(DevScalars));
+    if (cudaMallocHost(&c->scal_host, sizeof(DevScalars)) != cudaSuccess) return fail(PVOF_ENOMEM, "pinned scalars");
+    std::memset(c->scal_host, 0, sizeof(DevScalars));
+    if (cudaDeviceSynchronize() != cudaSuccess) return fail(PVOF_ECUDA, "create sync");
+    c->stage = 0;
+    c->dt = 0.0;
+    *out = c;
+    return PVOF_OK;
+}
+
+int pvof_destroy(pvof_ctx *c)
+{
+    if (!c) return PVOF_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (int q = 0; q < PVOF_F_COUNT; q++) if (c->base[q]) cudaFree(c->base[q]);
+    for (int q = 0; q < SC_COUNT; q++) if (c->sbase[q]) cudaFree(c->sbase[q]);
+    if (c->metric_mem) cudaFree(c->metric_mem);
+    if (c->map_src_mem) cudaFree(c->map_src_mem);
+    if (c->map_mul_mem) cudaFree(c->map_mul_mem);
+    if (c->partials) cudaFree(c->partials);
+    if (c->scal) cudaFree(c->scal);
+    if (c->scal_host) cudaFreeHost(c->scal_host);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return PVOF_OK;
+}
+
+size_t pvof_field_block_count(const pvof_ctx *c, int field)
+{
+    if (!c || field < 0 || field >= PVOF_F_COUNT) return 0;
+    size_t NX = (size_t)c->dom.NX, NY = (size_t)c->dom.NY, NZ = (size_t)c->g.NZM + 1;
+    if (is_ng(field)) return NX * NY * NZ;
+    return (NX + 2 * NG) * (NY + 2 * NG) * (NZ + 2 * NG);
+}
+
+int pvof_upload_field(pvof_ctx *c, int field, const double *host, size_t count)
+{
+    if (!c || !host) return set_err(PVOF_EINVAL, "null argument");
+    if (count != pvof_field_block_count(c, field)) return set_err(PVOF_EINVAL, "block size does not match the field");
+    CK(cudaSetDevice(c->device));
+    const size_t NX = (size_t)c->dom.NX, NY = (size_t)c->dom.NY;
+    if (is_ng(field)) {
+        // k = 0 plane of the G range -> device rows 0..NY-1, columns 0..NX-1
+        CK(cudaMemcpy2DAsync(c->f[field], (size_t)c->dom.P * sizeof(double), host, NX * sizeof(double),
+                             NX * sizeof(double), NY, cudaMemcpyHostToDevice, c->stream));
+    } else {
+        const size_t SX = NX + 2 * NG, SY = NY + 2 * NG;
+        const double *plane = host + (size_t)NG * SX * SY;  // k = 0
+        CK(cudaMemcpy2DAsync(c->f[field] - (ptrdiff_t)NG * c->dom.P - NG, (size_t)c->dom.P * sizeof(double), plane,
+                             SX * sizeof(double), SX * sizeof(double), SY, cudaMemcpyHostToDevice, c->stream));
+    }
+    return PVOF_OK;
+}
+
+int pvof_download_field(pvof_ctx *c, int field, double *host, size_t count)
+{
+    if (!c || !host) return set_err(PVOF_EINVAL, "null argument");
+    if (count != pvof_field_block_count(c, field)) return set_err(PVOF_EINVAL, "block size does not match the field");
+    CK(cudaSetDevice(c->device));
+    const size_t NX = (size_t)c->dom.NX, NY = (size_t)c->dom.NY, NZ = (size_t)c->g.NZM + 1;
+    if (is_ng(field)) {
+        for (size_t k = 0; k < NZ; k++)
+            CK(cudaMemcpy2DAsync(host + k * NX * NY, NX * sizeof(double), c->f[field], (size_t)c->dom.P * sizeof(double),
+                                 NX * sizeof(double), NY, cudaMemcpyDeviceToHost, c->stream));
+    } else {
+        const size_t SX = NX + 2 * NG, SY = NY + 2 * NG;
+        for (size_t k = 0; k < NZ; k++)
+            CK(cudaMemcpy2DAsync(host + (NG + k) * SX * SY, SX * sizeof(double), c->f[field] - (ptrdiff_t)NG * c->dom.P - NG,
+                                 (size_t)c->dom.P * sizeof(double), SX * sizeof(double), SY, cudaMemcpyDeviceToHost,
+                                 c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return PVOF_OK;
+}
+
+int pvof_synchronize(pvof_ctx *c)
+{
+    if (!c) return set_err(PVOF_EINVAL, "null context");
+    CK(cudaStreamSynchronize(c->stream));
+    return PVOF_OK;
+}
+
+int pvof_set_stage(pvof_ctx *c, int which_stage, double dt)
+{
+    if (!c) return set_err(PVOF_EINVAL, "null context");
+    if (which_stage < 0 || which_stage > 2 || !(dt > 0.0)) return set_err(PVOF_EINVAL, "stage must be 0..2 and dt > 0");
+    c->stage = which_stage;
+    c->dt = dt;
+    return PVOF_OK;
+}
+
+#define ENTER(c)                                                        \
+    do {                                                                \
+        if (!(c)) return set_err(PVOF_EINVAL, "null context");          \
+        CK(cudaSetDevice((c)->device));                                 \
+    } while (0)
+#define NEED_DT(c)                                                      \
+    do {                                                                \
+        if (!((c)->dt > 0.0)) return set_err(PVOF_EINVAL, "pvof_set_stage() first"); \
+    } while (0)
+
+int pvof_initialize(pvof_ctx *c) { ENTER(c); return initialize(c); }
+int pvof_VOF_DIFFUSE_init(pvof_ctx *c) { ENTER(c); return vof_diffuse_init(c); }
+int pvof_VOF_DIFFUSE_step(pvof_ctx *c, pvof_stats *st)
+{
+    ENTER(c);
+    NEED_DT(c);
+    TRY(vof_diffuse_step(c));
+    TRY(read_scalars(c));
+    fill_stats(c, st);
+    return PVOF_OK;
+}
+int pvof_VOF_DIFFUSE_advect_WENO5(pvof_ctx *c) { ENTER(c); return advect(c, F(c, PVOF_F_CH_RHS_CUR)); }
+int pvof_VOF_update_density_viscosity(pvof_ctx *c) { ENTER(c); return update_density_viscosity(c); }
+int pvof_VOF_DIFFUSE_compute_psi_LG(pvof_ctx *c) { ENTER(c); return compute_psi_LG(c); }
+int pvof_VOF_DIFFUSE_compute_f_sigma(pvof_ctx *c) { ENTER(c); return compute_f_sigma(c); }
+int pvof_VOF_apply_f_sigma_old(pvof_ctx *c) { ENTER(c); return apply_f_sigma_old(c); }
+int pvof_VOF_swap_f_sigma(pvof_ctx *c) { ENTER(c); swap_f_sigma(c); return PVOF_OK; }
+int pvof_Velocity_add_gravity_2_RHS(pvof_ctx *c) { ENTER(c); return add_gravity(c); }
+int pvof_Velocity_cell_center(pvof_ctx *c) { ENTER(c); return cell_center(c); }
+
+static int comp_of(char c) { return c == 'u' ? 0 : (c == 'v' ? 1 : -1); }
+
+int pvof_Velocity_set_implicit_explicit(pvof_ctx *c, char component)
+{
+    ENTER(c);
+    int k = comp_of(component);
+    if (k < 0) return set_err(PVOF_EINVAL, "component must be 'u' or 'v' in the 2D modes");
+    return implicit_explicit(c, k);
+}
+int pvof_Velocity_set_RHS(pvof_ctx *c, char component)
+{
+    ENTER(c);
+    NEED_DT(c);
+    int k = comp_of(component);
+    if (k < 0) return set_err(PVOF_EINVAL, "component must be 'u' or 'v' in the 2D modes");
+    return set_rhs(c, k);
+}
+int pvof_Velocity_solve_cg(pvof_ctx *c, char component, pvof_stats *st)
+{
+    ENTER(c);
+    NEED_DT(c);
+    int k = comp_of(component);
+    if (k < 0) return set_err(PVOF_EINVAL, "component must be 'u' or 'v' in the 2D modes");
+    TRY(velocity_solve(c, k));
+    TRY(read_scalars(c));
+    fill_stats(c, st);
+    return c->scal_host->vel_iters[k];
+}
+int pvof_Velocity_update_boundaries(pvof_ctx *c, char component)
+{
+    ENTER(c);
+    int k = comp_of(component);
+    if (k < 0) return set_err(PVOF_EINVAL, "component must be 'u' or 'v' in the 2D modes");
+    return fill(c, k == 0 ? BK_U : BK_V, F(c, k == 0 ? PVOF_F_U : PVOF_F_V));
+}
+int pvof_Pressure_set_RHS(pvof_ctx *c) { ENTER(c); NEED_DT(c); return p_set_rhs(c); }
+int pvof_Pressure_compute_preconditioner(pvof_ctx *c) { ENTER(c); return p_precond(c); }
+int pvof_Pressure_solve_cg(pvof_ctx *c, pvof_stats *st)
+{
+    ENTER(c);
+    TRY(p_solve(c));
+    TRY(read_scalars(c));
+    fill_stats(c, st);
+    return c->scal_host->p_iters;
+}
+int pvof_Pressure_project_velocity(pvof_ctx *c) { ENTER(c); NEED_DT(c); return p_project(c); }
+int pvof_Pressure_compute_velocity_divergence(pvof_ctx *c, double *div_max)
+{
+    ENTER(c);
+    TRY(p_divergence_async(c));
+    TRY(read_scalars(c));
+    if (div_max) *div_max = c->scal_host->div_max;
+    return PVOF_OK;
+}
+
+int pvof_substep(pvof_ctx *c, pvof_stats *st)
+{
+    ENTER(c);
+    NEED_DT(c);
+    return substep(c, st);
+}
+
+int pvof_run_steps(pvof_ctx *c, int nsteps, double dt, pvof_stats *st)
+{
+    ENTER(c);
+    if (nsteps < 0 || !(dt > 0.0)) return set_err(PVOF_EINVAL, "nsteps >= 0 and dt > 0");
+    for (int n = 0; n < nsteps; n++) {
+        for (int rk = 0; rk < 3; rk++) {
+            if (c->time != 0 && rk == 0) TRY(cell_center(c));
+            c->stage = rk;
+            c->dt = dt;
+            TRY(substep(c, st));
+            c->time += dt * bet2(rk);
+        }
+    }
+    return PVOF_OK;
+}
+
+int pvof_liquid_mass(pvof_ctx *c, double *mass)
+{
+    ENTER(c);
+    const int NX = c->dom.NX, NY = c->dom.NY;
+    dim3 blk(TBX, TBY);
+    dim3 grd((unsigned)((NX - 1 + TBX - 1) / TBX), (unsigned)((NY - 1 + TBY - 1) / TBY));
+    k_mass<<<grd, blk, 0, c->stream>>>(c->dom, 0, NX - 1, 0, NY - 1, F(c, PVOF_F_C_L), c->partials);
+    CKL(c);
+    k_finalize_sum<<<1, 256, 0, c->stream>>>(c->partials, (int)(grd.x * grd.y), &c->scal->mass);
+    CKL(c);
+    TRY(read_scalars(c));
+    if (mass) *mass = c->scal_host->mass;
+    return PVOF_OK;
+}
+
+// number of kernels this context has launched (benchmark bookkeeping)
+long long pvof_launch_count(const pvof_ctx *c) { return c ? c->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,387 @@
+// Persistent iterative solvers of the two-phase substep.
+//
+// Each solve is ONE cooperative launch that runs the reference's whole CG
+// loop on the device: the blocks step through the iterations together,
+// separated by a grid barrier, and every block reduces the per-block partial
+// sums of each inner product in the same fixed order, so all blocks take the
+// same convergence decisions.  Cells are assigned to threads by the same
+// grid-stride mapping in every phase, so a thread reads back its own cells'
+// private vectors (diagonal, Ad, the new direction) without a barrier.
+//
+// The grid barrier is this file's own (not cooperative_groups::grid_group::
+// sync) so that its wait is bounded: if the other blocks never arrive it
+// records an error in DevScalars::error and every block leaves the solver.
+#include <cuda/atomic>
+
+#include "pvof_device.cuh"
+#include "pvof_kernels.cuh"
+
+namespace pvof {
+
+constexpr unsigned long long BARRIER_SPIN_LIMIT = 1ull << 25;
+
+struct GridSync {
+    DevScalars *s;
+    unsigned nblocks;
+};
+
+// Returns false (in every thread of the block) when the barrier gave up.
+__device__ bool grid_barrier(const GridSync &gs)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(gs.s->bar_count);
+        cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(gs.s->bar_gen);
+        cuda::atomic_ref<int, cuda::thread_scope_device> err(gs.s->error);
+        int good = err.load(cuda::memory_order_relaxed) == 0;
+        unsigned g = gen.load(cuda::memory_order_acquire);
+        unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+        if (arrived == gs.nblocks - 1) {
+            cnt.store(0u, cuda::memory_order_relaxed);
+            gen.fetch_add(1u, cuda::memory_order_release);
+        } else {
+            unsigned long long spins = 0;
+            while (gen.load(cuda::memory_order_acquire) == g) {
+                if (err.load(cuda::memory_order_relaxed) != 0 || ++spins > BARRIER_SPIN_LIMIT) {
+                    err.store(1, cuda::memory_order_relaxed);
+                    good = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// sum of v over the block (1D blocks, multiple of 32 threads)
+__device__ double block_sum(double v)
+{
+    __shared__ double sh[32];
+    __shared__ double res;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        double w = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+        if (lane == 0) res = w;
+    }
+    __syncthreads();
+    return res;
+}
+
+// Sum of the per-block partials, identical in every block.  Each reduction
+// uses its own slot of the partials buffer; a slot is rewritten only after at
+// least one more barrier has passed since every block read it.
+__device__ double grid_total(const double *part)
+{
+    __shared__ double res;
+    if (threadIdx.x < 32) {
+        double v = 0.0;
+        for (unsigned q = threadIdx.x; q < gridDim.x; q += 32) v += part[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) res = v;
+    }
+    __syncthreads();
+    double r = res;
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ void put_partial(double *part, double v)
+{
+    double s = block_sum(v);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+struct Range {
+    int i0, j0, w, n;
+    __device__ __forceinline__ void ij(int q, int &i, int &j) const { i = i0 + q % w; j = j0 + q / w; }
+};
+
+// ---------------------------------------------------------------------------
+// diffuse_solve_biharmonic_pcg (Eulerian/VOF_DIFFUSE.c:339-429): CG on
+// [a_dt I + bih L.L] x = b over the G range, inner products weighted by the
+// cell measure and summed over the reference's nk identical planes.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_cg_biharmonic(BihArgs A)
+{
+    const Dom &d = A.d;
+    const int P = d.P, NX = d.NX, NY = d.NY;
+    const GridSync gs{A.scal, gridDim.x};
+    const Range R{0, 0, NX, NX * NY};
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    const double nk = (double)d.nk;
+    double *part0 = A.partials, *part1 = A.partials + gridDim.x;
+    double *part2 = A.partials + 2 * gridDim.x, *part3 = A.partials + 3 * gridDim.x;
+    auto X = [&](int a, int b) { return remap(A.msc, A.x, P, NX, NY, a, b); };
+
+    // Ap = A x (two Laplacians with the scalar ghost update in between)
+    for (int q = tid; q < R.n; q += nth) {
+        int i, j;
+        R.ij(q, i, j);
+        AT_(A.aux, i, j) = lap_at(d, i, j, X);
+    }
+    if (!grid_barrier(gs)) return;
+    double sbb = 0.0, srr = 0.0;
+    for (int q = tid; q < R.n; q += nth) {
+        int i, j;
+        R.ij(q, i, j);
+        double l2 = lap_at(d, i, j, [&](int a, int b) { return remap(A.msc, A.aux, P, NX, NY, a, b); });
+        double ap = A.a_dt * AT_(A.x, i, j) + A.bih * l2;
+        double bv = AT_(A.b, i, j);
+        double rv = bv - ap;
+        AT_(A.r, i, j) = rv;
+        AT_(A.p1, i, j) = rv;
+        double m = cell_measure(d, i, j);
+        sbb += m * bv * bv;
+        srr += m * rv * rv;
+    }
+    put_partial(part0, sbb);
+    put_partial(part1, srr);
+    if (!grid_barrier(gs)) return;
+    double rhs_norm = sqrt(nk * grid_total(part0));
+    if (rhs_norm < 1e-30) rhs_norm = 1.0;
+    double rz = nk * grid_total(part1);
+    double rel = sqrt(rz) / rhs_norm;
+    int iter = 0;
+    if (rel < A.tol) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->ch_iters = 0; A.scal->ch_rel = rel; }
+        return;
+    }
+    double *pcur = A.p1, *pold = A.p2;
+    double beta = 0.0;
+    bool first = true;
+    while (iter < A.maxit) {
+        // direction p = r + beta p_old (the first direction is r itself) and
+        // aux = L(p) with the scalar ghost update of p applied on the fly
+        if (!first) {
+            double *t = pold; pold = pcur; pcur = t;
+            for (int q = tid; q < R.n; q += nth) {
+                int i, j;
+                R.ij(q, i, j);
+                AT_(pcur, i, j) = AT_(A.r, i, j) + beta * AT_(pold, i, j);
+            }
+            for (int q = tid; q < R.n; q += nth) {
+                int i, j;
+                R.ij(q, i, j);
+                AT_(A.aux, i, j) = lap_at(d, i, j, [&](int a, int b) {
+                    return remap(A.msc, A.r, P, NX, NY, a, b) + beta * remap(A.msc, pold, P, NX, NY, a, b);
+                });
+            }
+        } else {
+            for (int q = tid; q < R.n; q += nth) {
+                int i, j;
+                R.ij(q, i, j);
+                AT_(A.aux, i, j) = lap_at(d, i, j, [&](int a, int b) { return remap(A.msc, pcur, P, NX, NY, a, b); });
+            }
+        }
+        first = false;
+        if (!grid_barrier(gs)) return;
+        double spap = 0.0;
+        for (int q = tid; q < R.n; q += nth) {
+            int i, j;
+            R.ij(q, i, j);
+            double l2 = lap_at(d, i, j, [&](int a, int b) { return remap(A.msc, A.aux, P, NX, NY, a, b); });
+            double pv = AT_(pcur, i, j);
+            double ap = A.a_dt * pv + A.bih * l2;
+            AT_(A.Ap, i, j) = ap;
+            spap += cell_measure(d, i, j) * pv * ap;
+        }
+        put_partial(part2, spap);
+        if (!grid_barrier(gs)) return;
+        double pAp = nk * grid_total(part2);
+        if (fabs(pAp) < 1e-30) break;
+        double alpha = rz / pAp;
+        double srr2 = 0.0;
+        for (int q = tid; q < R.n; q += nth) {
+            int i, j;
+            R.ij(q, i, j);
+            AT_(A.x, i, j) += alpha * AT_(pcur, i, j);
+            double rv = AT_(A.r, i, j) - alpha * AT_(A.Ap, i, j);
+            AT_(A.r, i, j) = rv;
+            srr2 += cell_measure(d, i, j) * rv * rv;
+        }
+        put_partial(part3, srr2);
+        if (!grid_barrier(gs)) return;
+        ++iter;
+        double rr = nk * grid_total(part3);
+        rel = sqrt(rr) / rhs_norm;
+        if (rel < A.tol) break;
+        double rz_new = rr;  // z == r: the same weighted sum
+        beta = rz_new / (rz + 1e-30);
+        rz = rz_new;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->ch_iters = iter; A.scal->ch_rel = rel; }
+}
+
+// ---------------------------------------------------------------------------
+// Velocity_solve_cg (Eulerian/lsolver/msolve_cg.c:525-722): Jacobi PCG with
+// the RMS residual stop, one velocity component.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_cg_velocity(VelArgs A)
+{
+    const Dom &d = A.d;
+    const int P = d.P, NX = d.NX, NY = d.NY;
+    const GridSync gs{A.scal, gridDim.x};
+    const Range R{A.i0, A.j0, A.i1 - A.i0, (A.i1 - A.i0) * (A.j1 - A.j0)};
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    const double EPS = 1e-14;
+    double *part0 = A.partials, *part1 = A.partials + gridDim.x;
+    double *part2 = A.partials + 2 * gridDim.x, *part3 = A.partials + 3 * gridDim.x;
+
+    double srz = 0.0;
+    for (int q = tid; q < R.n; q += nth) {
+        int i, j;
+        R.ij(q, i, j);
+        double dg = vel_diag(d, A.comp, A.rho, A.mu, i, j, A.iRe, A.alpha_dt) + EPS;
+        AT_(A.diag, i, j) = dg;
+        double ad = vel_op(d, A.comp, A.rho, A.mu, i, j, A.iRe, A.alpha_dt, [&](int a, int b) { return AT_(A.x, a, b); });
+        double rv = AT_(A.rhs, i, j) - ad;
+        AT_(A.r, i, j) = rv;
+        double dv = rv / dg;
+        AT_(A.dir, i, j) = dv;
+        srz += rv * dv;
+    }
+    put_partial(part0, srz);
+    if (!grid_barrier(gs)) return;
+    double rz = grid_total(part0);
+    double RMS = 0.0;
+    int iters = 0;
+    while (iters < A.maxit) {
+        iters++;
+        double sdad = 0.0;
+        for (int q = tid; q < R.n; q += nth) {
+            int i, j;
+            R.ij(q, i, j);
+            double ad = vel_op(d, A.comp, A.rho, A.mu, i, j, A.iRe, A.alpha_dt,
+                               [&](int a, int b) { return remap(A.mcg, A.dir, P, NX, NY, a, b); });
+            AT_(A.Ad, i, j) = ad;
+            sdad += AT_(A.dir, i, j) * ad;
+        }
+        put_partial(part1, sdad);
+        if (!grid_barrier(gs)) return;
+        double dAd = grid_total(part1);
+        double alpha = rz / (dAd + EPS);
+        double s0 = 0.0, s1 = 0.0;
+        for (int q = tid; q < R.n; q += nth) {
+            int i, j;
+            R.ij(q, i, j);
+            AT_(A.x, i, j) += alpha * AT_(A.dir, i, j);
+            double ri = AT_(A.r, i, j) - alpha * AT_(A.Ad, i, j);
+            AT_(A.r, i, j) = ri;
+            s0 += ri * ri / AT_(A.diag, i, j);
+            s1 += ri * ri;
+        }
+        put_partial(part2, s0);
+        put_partial(part3, s1);
+        if (!grid_barrier(gs)) return;
+        double rz_new = grid_total(part2), rr = grid_total(part3);
+        RMS = sqrt(A.in_tot * rr);
+        if (RMS < A.tol) break;
+        double beta = rz_new / (rz + EPS);
+        rz = rz_new;
+        for (int q = tid; q < R.n; q += nth) {
+            int i, j;
+            R.ij(q, i, j);
+            AT_(A.dir, i, j) = AT_(A.r, i, j) / AT_(A.diag, i, j) + beta * AT_(A.dir, i, j);
+        }
+        if (!grid_barrier(gs)) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->vel_iters[A.comp] = iters; A.scal->vel_rms[A.comp] = RMS; }
+}
+
+// ---------------------------------------------------------------------------
+// Pressure_solve_cg (Eulerian/lsolver/psolve_cg.c:130-293): Jacobi PCG on the
+// variable-density Poisson operator, absolute stop on sqrt(r.M^-1 r), mean
+// removed at the end.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_cg_pressure(PresArgs A)
+{
+    const Dom &d = A.d;
+    const int P = d.P, NX = d.NX, NY = d.NY;
+    const GridSync gs{A.scal, gridDim.x};
+    const Range R{0, 0, NX - 1, (NX - 1) * (NY - 1)};
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    double *part0 = A.partials, *part1 = A.partials + gridDim.x, *part2 = A.partials + 2 * gridDim.x;
+
+    double sg = 0.0;
+    for (int q = tid; q < R.n; q += nth) {
+        int i, j;
+        R.ij(q, i, j);
+        double ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, A.phi, P, NX, NY, a, b); });
+        double rv = AT_(A.rhs, i, j) - ad;
+        AT_(A.res, i, j) = rv;
+        double z = rv * AT_(A.M, i, j);
+        AT_(A.dir, i, j) = z;
+        sg += rv * z;
+    }
+    put_partial(part0, sg);
+    if (!grid_barrier(gs)) return;
+    double gamma = grid_total(part0), gamma_new = 0.0;
+    if (sqrt(gamma) < A.tol) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->p_iters = 0; A.scal->p_res = sqrt(gamma); }
+        return;
+    }
+    int iters;
+    for (iters = 1; iters <= A.maxit; iters++) {
+        double sdad = 0.0;
+        for (int q = tid; q < R.n; q += nth) {
+            int i, j;
+            R.ij(q, i, j);
+            double ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, A.dir, P, NX, NY, a, b); });
+            AT_(A.Ad, i, j) = ad;
+            sdad += AT_(A.dir, i, j) * ad;
+        }
+        put_partial(part1, sdad);
+        if (!grid_barrier(gs)) return;
+        double alpha = gamma / (grid_total(part1) + 1e-30);
+        double sgn = 0.0;
+        for (int q = tid; q < R.n; q += nth) {
+            int i, j;
+            R.ij(q, i, j);
+            AT_(A.phi, i, j) += alpha * AT_(A.dir, i, j);
+            double rv = AT_(A.res, i, j) - alpha * AT_(A.Ad, i, j);
+            AT_(A.res, i, j) = rv;
+            sgn += rv * (rv * AT_(A.M, i, j));
+        }
+        put_partial(part2, sgn);
+        if (!grid_barrier(gs)) return;
+        gamma_new = grid_total(part2);
+        if (sqrt(gamma_new) < A.tol) break;
+        double beta = gamma_new / (gamma + 1e-30);
+        for (int q = tid; q < R.n; q += nth) {
+            int i, j;
+            R.ij(q, i, j);
+            AT_(A.dir, i, j) = AT_(A.res, i, j) * AT_(A.M, i, j) + beta * AT_(A.dir, i, j);
+        }
+        if (!grid_barrier(gs)) return;
+        gamma = gamma_new;
+    }
+    // remove the mean (every face Neumann or periodic), psolve_cg.c:255-279
+    double ssum = 0.0;
+    for (int q = tid; q < R.n; q += nth) {
+        int i, j;
+        R.ij(q, i, j);
+        ssum += AT_(A.phi, i, j);
+    }
+    put_partial(part0, ssum);
+    if (!grid_barrier(gs)) return;
+    double avg = grid_total(part0) / (double)R.n;
+    for (int q = tid; q < R.n; q += nth) {
+        int i, j;
+        R.ij(q, i, j);
+        AT_(A.phi, i, j) -= avg;
+    }
+    if (iters > A.maxit) iters = A.maxit;
+    if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->p_iters = iters; A.scal->p_res = sqrt(gamma_new); }
+}
+
+}  // namespace pvof

@@ -1,0 +1,127 @@
+// Internal definitions of the B200 two-phase substep library.
+//
+// Device layout: one k plane per field (the 2D modes of PARTIES keep all
+// planes identical), stored row-major with a pitch of P doubles.  The pointer
+// handed to kernels addresses element (i=0, j=0); element (i,j) is at
+// f[j*P + i] for i in [-3, NX+3), j in [-3, NY+3) -- the reference's own
+// ghosted index space (PARTIES/src/Memory.c:36-89), so every kernel runs on
+// the reference's index ranges.  NX = NXM+1 and NY = NYM+1 include the half
+// cell the reference adds at the far end of each direction.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/pvof.h"
+
+namespace pvof {
+
+constexpr int NG = 3;        // ghost layers
+constexpr int OX = 4;        // column of i = 0 inside a row (i = -3 at column 1)
+constexpr int OY = NG;       // row of j = 0
+
+// RK3 coefficients (PARTIES/src/Include/definitions.h:197-204)
+__host__ __device__ inline double bet(int s) { return s == 0 ? 4.0 / 15.0 : (s == 1 ? 1.0 / 15.0 : 1.0 / 6.0); }
+__host__ __device__ inline double bet2(int s) { return s == 0 ? 8.0 / 15.0 : (s == 1 ? 2.0 / 15.0 : 1.0 / 3.0); }
+__host__ __device__ inline double gamb(int s) { return s == 0 ? 2.0 : (s == 1 ? 25.0 / 4.0 : 9.0 / 2.0); }
+__host__ __device__ inline double zetb(int s) { return s == 0 ? 0.0 : (s == 1 ? -17.0 / 4.0 : -2.5); }
+
+// Ghost-update kinds.  Each is the composition of the reference's boundary
+// routine and its periodic exchange for one kind of field.
+enum BcKind {
+    BK_SCALAR = 0,   // VOF_DIFFUSE_set_boundary_values (VOF_DIFFUSE.c:571-683)
+    BK_PRESSURE,     // Pressure_apply_BCs + exchange (psolve_cg.c:358-529)
+    BK_U,            // Velocity_update_boundaries('u', VEL_TYPE_NORMAL)
+    BK_V,            // Velocity_update_boundaries('v', VEL_TYPE_NORMAL)
+    BK_U_CG,         // Velocity_update_boundaries('u', VEL_TYPE_CG)
+    BK_V_CG,         // Velocity_update_boundaries('v', VEL_TYPE_CG)
+    BK_WRAP_C,       // exchange only, scalar component (Communication.c:146-291)
+    BK_WRAP_U,       // exchange only, x-face component (U_VELOCITY, FLUX_X)
+    BK_WRAP_V,       // exchange only, y-face component (V_VELOCITY, FLUX_Y)
+    BK_COUNT
+};
+
+// Per-axis source maps of one kind: entry [i + NG] for i in [-NG, N + NG).
+// src == i and mul == 1 means "not written"; mul == 0 means "set to zero".
+struct AxisMap {
+    const int *src;
+    const double *mul;
+};
+
+struct BcMap {
+    AxisMap x, y;
+};
+
+// Grid metrics, each offset so that m[i] is valid for i in [-NG, N + NG - 1).
+struct Metrics {
+    const double *idx_u, *idx_c, *dx_c, *dx_u;
+    const double *idy_v, *idy_c, *dy_c, *dy_v;
+    const double *r_u, *r_c, *inv_r_u, *inv_r_c, *ring_wt_c;
+};
+
+struct Dom {
+    int NX, NY;       // G-range extents (NXM+1, NYM+1)
+    int P;            // pitch in doubles
+    int planar;       // TWOD_CARTESIAN
+    int axisym;       // AXISYM_RZ
+    int perx, pery;   // XPERIODIC, YPERIODIC
+    int nk;           // planes of the reference's G range in k (2 in 2D)
+    double slab;      // dummy_z_slab_thickness
+    Metrics m;
+};
+
+__host__ __device__ inline size_t at(const Dom &d, int i, int j) { return (size_t)((ptrdiff_t)j * d.P + i); }
+
+// scratch arrays beyond the public fields
+enum Scratch {
+    SC_PSI = 0, SC_BULK_S, SC_CH_AUX1, SC_CH_RHS_NM1, SC_CH_RES, SC_CH_DIR, SC_CH_DIR2,
+    SC_FLUX_X, SC_FLUX_Y, SC_P_RES, SC_P_D, SC_P_AD, SC_P_MINV,
+    SC_U_R, SC_U_D, SC_U_AD, SC_U_DIAG, SC_V_R, SC_V_D, SC_V_AD, SC_V_DIAG,
+    SC_OLD, SC_COUNT
+};
+
+// device-side scalars written by solver kernels and read once per substep
+struct DevScalars {
+    int ch_iters;
+    double ch_rel;
+    int vel_iters[2];
+    double vel_rms[2];
+    int p_iters;
+    double p_res;
+    double div_max;
+    double clamp_delta;
+    double mass;
+    int error;          // non-zero: a grid barrier gave up (see pvof_cg.cu)
+    unsigned bar_count; // grid barrier state
+    unsigned bar_gen;
+};
+
+struct Ctx {
+    pvof_grid_desc g;
+    pvof_params p;
+    int device;
+    Dom dom;
+    size_t plane_elems;      // P * (NY + 2*NG)
+    double *base[PVOF_F_COUNT];   // allocation bases
+    double *f[PVOF_F_COUNT];      // element (0,0) of each field
+    double *sbase[SC_COUNT];
+    double *s[SC_COUNT];
+    double *metric_mem;
+    int *map_src_mem;
+    double *map_mul_mem;
+    BcMap maps[BK_COUNT];
+    double *partials;        // per-block partial sums (3 per block)
+    DevScalars *scal;        // device scalars
+    DevScalars *scal_host;   // pinned host mirror
+    double *host_plane;      // pinned staging plane for uploads/downloads
+    cudaStream_t stream;
+    int stage;
+    double dt;
+    double time;
+    int coop_blocks;         // co-resident blocks for the persistent solvers
+    int coop_threads;
+    long long launches;      // kernels launched by this context
+};
+
+}  // namespace pvof

@@ -1,0 +1,91 @@
+// Kernel declarations shared by the routine kernels, the solvers and the
+// host orchestration.
+#pragma once
+
+#include "pvof_internal.cuh"
+
+namespace pvof {
+
+struct BihArgs {
+    Dom d;
+    BcMap msc;             // scalar ghost update of x, p and the Laplacian
+    double *x;             // C_L (solution, updated in place)
+    const double *b;       // rhs_vec
+    double *r, *p1, *p2, *Ap, *aux;
+    double a_dt, bih, tol;
+    int maxit;
+    double *partials;
+    DevScalars *scal;
+};
+
+struct VelArgs {
+    Dom d;
+    BcMap mcg;             // VEL_TYPE_CG ghost update of the direction
+    int comp;              // 0 = u, 1 = v
+    int i0, i1, j0, j1;    // solve range
+    double *x;             // velocity component (updated in place)
+    const double *rhs, *rho, *mu;
+    double *r, *dir, *Ad, *diag;
+    double iRe, alpha_dt, in_tot, tol;
+    int maxit;
+    double *partials;
+    DevScalars *scal;
+};
+
+struct PresArgs {
+    Dom d;
+    BcMap mp;              // Pressure_apply_BCs + exchange
+    double *phi;           // deltap
+    const double *rhs, *rho, *M;
+    double *res, *dir, *Ad;
+    double tol;
+    int maxit;
+    double *partials;
+    DevScalars *scal;
+};
+
+__global__ void k_fill(Dom d, BcMap m, double *f);
+__global__ void k_weno_flux(Dom d, int i0, int i1, int j0, int j1, const double *C, const double *u, const double *v,
+                            double *fx, double *fy, int weno5);
+__global__ void k_flux_div(Dom d, int i0, int i1, int j0, int j1, const double *fx, const double *fy, double *out);
+__global__ void k_bulk_S(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *CS, double *bS);
+__global__ void k_laplacian(Dom d, int i0, int i1, int j0, int j1, const double *in, double *out);
+__global__ void k_div_by(Dom d, int i0, int i1, int j0, int j1, double *a, double s);
+__global__ void k_add(Dom d, int i0, int i1, int j0, int j1, double *a, const double *b);
+__global__ void k_sub_scaled(Dom d, int i0, int i1, int j0, int j1, double *a, const double *b, double s);
+__global__ void k_rhs_vec(Dom d, int i0, int i1, int j0, int j1, double *vec, const double *CL, const double *cur,
+                          const double *rn, double a_dt, int s);
+__global__ void k_bound(Dom d, int i0, int i1, int j0, int j1, double *CL, const double *CS, double *CG, double *partials);
+__global__ void k_finalize_sum(const double *partials, int n, double *out);
+__global__ void k_phase_cache(size_t n, const double *CL, const double *CS, double *CG, double *F);
+__global__ void k_clamp_from(size_t n, const double *F, double *CL);
+__global__ void k_density(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *CS, const double *CG,
+                          double *rho, double *mu, double rho_g, double mu_g);
+__global__ void k_psi_LG(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *lap, double *psi, double cn2);
+__global__ void k_f_sigma(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *CG, const double *CS,
+                          const double *psi, double *fx, double *fy, double scale, int ui0, int ui1, int uj1, int vj0,
+                          int vi1, int vj1);
+__global__ void k_add_to(Dom d, int i0, int i1, int j0, int j1, double *rhs, const double *f);
+__global__ void k_gravity(Dom d, int i0, int i1, int j0, int j1, const double *rho, double *rhs, int di, int dj,
+                          double Ri, double g);
+__global__ void k_cell_center(Dom d, int i0, int i1, int j0, int j1, const double *u, const double *v, double *ub, double *vb);
+__global__ void k_u_impexp(Dom d, int i0, int i1, int j0, int j1, const double *u, const double *v, const double *ub,
+                           const double *mu, double *ex, double *im, double *vx, double iRe);
+__global__ void k_v_impexp(Dom d, int i0, int i1, int j0, int j1, const double *u, const double *v, const double *vb,
+                           const double *mu, double *ex, double *im, double *vx, double iRe);
+__global__ void k_set_rhs(Dom d, int i0, int i1, int j0, int j1, int comp, const double *data, const double *pd,
+                          const double *rho, double *rhs, const double *ex, double *exo, const double *vx, double *vxo,
+                          const double *im, double a_dt, int s, double dp_src);
+__global__ void k_p_rhs(Dom d, int i0, int i1, int j0, int j1, const double *u, const double *v, double *rhs, double ihdt);
+__global__ void k_p_precond(Dom d, int i0, int i1, int j0, int j1, const double *rho, double *M);
+__global__ void k_p_update(Dom d, int i0, int i1, int j0, int j1, double *pd, const double *dp);
+__global__ void k_project(Dom d, int i0, int i1, int j0, int j1, int comp, double *vel, const double *dp,
+                          const double *rho, double mdt);
+__global__ void k_div_max(Dom d, int i0, int i1, int j0, int j1, const double *u, const double *v, unsigned long long *out);
+__global__ void k_mass(Dom d, int i0, int i1, int j0, int j1, const double *CL, double *partials);
+
+__global__ void k_cg_biharmonic(BihArgs A);
+__global__ void k_cg_velocity(VelArgs A);
+__global__ void k_cg_pressure(PresArgs A);
+
+}  // namespace pvof

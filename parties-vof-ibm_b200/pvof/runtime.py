@@ -1,0 +1,150 @@
+"""ctypes binding of the CUDA library (pvof/libpvof.so, include/pvof.h).
+
+``Solver`` owns one pvof context: upload the initial planes, initialise,
+advance, download.  The library must be present and a CUDA device visible;
+otherwise construction raises -- there is no CPU path.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi, cases
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libpvof.so")
+_lib = None
+
+
+class PvofError(RuntimeError):
+    pass
+
+
+def load():
+    """Load libpvof.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise PvofError("libpvof.so is not built (python parties-vof-ibm_b200/build.py)")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    V = C.c_void_p
+    L.pvof_abi_version.restype = C.c_int
+    L.pvof_last_error.restype = C.c_char_p
+    L.pvof_device_count.restype = C.c_int
+    L.pvof_create.argtypes = [P(abi.GridDesc), P(abi.Params), C.c_int, P(V)]
+    L.pvof_destroy.argtypes = [V]
+    L.pvof_field_block_count.argtypes = [V, C.c_int]
+    L.pvof_field_block_count.restype = C.c_size_t
+    L.pvof_upload_field.argtypes = [V, C.c_int, P(C.c_double), C.c_size_t]
+    L.pvof_download_field.argtypes = [V, C.c_int, P(C.c_double), C.c_size_t]
+    L.pvof_synchronize.argtypes = [V]
+    L.pvof_set_stage.argtypes = [V, C.c_int, C.c_double]
+    L.pvof_initialize.argtypes = [V]
+    for name in ["pvof_VOF_DIFFUSE_init", "pvof_VOF_DIFFUSE_advect_WENO5",
+                 "pvof_VOF_update_density_viscosity", "pvof_VOF_DIFFUSE_compute_psi_LG",
+                 "pvof_VOF_DIFFUSE_compute_f_sigma", "pvof_VOF_apply_f_sigma_old",
+                 "pvof_VOF_swap_f_sigma", "pvof_Velocity_add_gravity_2_RHS",
+                 "pvof_Velocity_cell_center", "pvof_Pressure_set_RHS",
+                 "pvof_Pressure_compute_preconditioner", "pvof_Pressure_project_velocity"]:
+        getattr(L, name).argtypes = [V]
+    L.pvof_VOF_DIFFUSE_step.argtypes = [V, P(abi.Stats)]
+    for name in ["pvof_Velocity_set_implicit_explicit", "pvof_Velocity_set_RHS",
+                 "pvof_Velocity_update_boundaries"]:
+        getattr(L, name).argtypes = [V, C.c_char]
+    L.pvof_Velocity_solve_cg.argtypes = [V, C.c_char, P(abi.Stats)]
+    L.pvof_Pressure_solve_cg.argtypes = [V, P(abi.Stats)]
+    L.pvof_Pressure_compute_velocity_divergence.argtypes = [V, P(C.c_double)]
+    L.pvof_substep.argtypes = [V, P(abi.Stats)]
+    L.pvof_run_steps.argtypes = [V, C.c_int, C.c_double, P(abi.Stats)]
+    L.pvof_liquid_mass.argtypes = [V, P(C.c_double)]
+    L.pvof_launch_count.argtypes = [V]
+    L.pvof_launch_count.restype = C.c_longlong
+    _lib = L
+    return L
+
+
+def check(rc, what=""):
+    if rc < 0:
+        msg = load().pvof_last_error().decode(errors="replace")
+        raise PvofError("%s failed (%d): %s" % (what, rc, msg))
+    return rc
+
+
+class Solver:
+    """One case on one GPU, driven through the C ABI."""
+
+    def __init__(self, grid, params, device=0):
+        L = load()
+        self.grid, self.params = grid, params
+        self.h = C.c_void_p()
+        check(L.pvof_create(C.byref(grid), C.byref(params), device, C.byref(self.h)), "pvof_create")
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().pvof_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- fields ------------------------------------------------------------
+    def block_count(self, name):
+        return load().pvof_field_block_count(self.h, abi.FIELD[name])
+
+    def upload(self, name, block):
+        a = np.ascontiguousarray(block, dtype=np.float64).ravel()
+        check(load().pvof_upload_field(self.h, abi.FIELD[name], a.ctypes.data_as(C.POINTER(C.c_double)), a.size),
+              "upload " + name)
+
+    def download(self, name, out=None):
+        n = self.block_count(name)
+        a = out if out is not None else np.empty(n, dtype=np.float64)
+        check(load().pvof_download_field(self.h, abi.FIELD[name], a.ctypes.data_as(C.POINTER(C.c_double)), n),
+              "download " + name)
+        return a
+
+    def get(self, name):
+        """k = 0 plane of a field (ghost frame included for flow fields)."""
+        f = abi.FIELD[name]
+        return cases.block_plane(self.grid, self.download(name), ng=f in abi.NG_FIELDS)
+
+    def set_planes(self, planes):
+        for name, plane in planes.items():
+            ng = abi.FIELD[name] in abi.NG_FIELDS
+            self.upload(name, cases.plane_to_block(self.grid, plane, ng=ng))
+
+    # -- routines ----------------------------------------------------------
+    def set_stage(self, stage, dt):
+        check(load().pvof_set_stage(self.h, stage, dt), "pvof_set_stage")
+
+    def initialize(self):
+        check(load().pvof_initialize(self.h), "pvof_initialize")
+
+    def call(self, name, *args):
+        fn = getattr(load(), "pvof_" + name)
+        return check(fn(self.h, *args), name)
+
+    def substep(self):
+        st = abi.Stats()
+        check(load().pvof_substep(self.h, C.byref(st)), "pvof_substep")
+        return st
+
+    def run_steps(self, n, dt):
+        st = abi.Stats()
+        check(load().pvof_run_steps(self.h, n, dt, C.byref(st)), "pvof_run_steps")
+        return st
+
+    def liquid_mass(self):
+        m = C.c_double()
+        check(load().pvof_liquid_mass(self.h, C.byref(m)), "pvof_liquid_mass")
+        return m.value
+
+    def synchronize(self):
+        check(load().pvof_synchronize(self.h), "pvof_synchronize")
+
+    def launch_count(self):
+        return load().pvof_launch_count(self.h)
