@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark: cell-updates/s per RK3 time step of the planar two-phase case.
+
+Workload: the planar two-phase (Rayleigh-Taylor type) instability on its
+128x512 grid -- x periodic, no-slip walls in y, Atwood 0.5, Re 3000,
+Cn 0.01, Pe 1/Cn, gravity -y -- advanced with the full diffuse-interface
+substep (WENO5 + explicit diffusion + implicit biharmonic CG, density and
+viscosity, momentum with velocity PCG, gravity, variable-density pressure
+PCG and projection) at a constant dt of 1e-4.  Synthetic initial condition
+(tanh interface at mid-height perturbed by 0.05 cos 2 pi x).  Solver
+tolerances are the reference defaults except the pressure iteration cap
+(2000 instead of 300: with 300 the reference's own outer Poisson loop does
+not reach div < 1e-6 on this grid and aborts).
+
+One "step" = one time step (three RK substeps).  metric = N_cells x steps /
+seconds.  value: device time of the timed steps with the state resident in
+HBM, the L2 flushed before every step (outside the timed intervals).  e2e:
+the same steps driven through the C ABI with the state uploaded from pinned
+host buffers before every step and downloaded after it.
+
+--impl reference runs the reference's own time step (compiled from its
+sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host.
+With N > 1 (torchrun) every rank advances its own replica of the case
+(replicas only; the case is not split across GPUs).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "parties-vof-ibm_b200"))
+
+METRIC = "cell-updates/s per RK step"
+UNIT = "cell-updates/s"
+NXM, NYM = 128, 512
+DT = 1e-4
+WORKLOAD = ("planar two-phase instability 128x512 (x periodic, no-slip y), Atwood 0.5, Re 3000, Cn 0.01, "
+            "dt 1e-4, full RK3 substep")
+# algorithmic bytes per cell and solver iteration (x, r, direction read+write,
+# plus the phase field that the coefficients are derived from)
+ALG_BYTES = {0: 48.0, 1: 56.0, 2: 56.0}
+SOLVER_NAMES = {0: "k_cg_biharmonic", 1: "k_cg_velocity", 2: "k_cg_pressure"}
+STATE_FIELDS = ["C_L", "U", "V", "P", "CH_RHS_N", "U_EXPLICIT_OLD", "V_EXPLICIT_OLD",
+                "U_VISC_EXPLICIT_OLD", "V_VISC_EXPLICIT_OLD"]
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def case():
+    from pvof import cases
+    return cases.rayleigh_taylor(NXM, NYM, Lx=1.0, Ly=4.0, Cn=0.01, P_CG_MAXIT=2000)
+
+
+def dist_env():
+    from pvof import dist as pdist
+    return pdist.env()
+
+
+def init_dist(ws, local):
+    from pvof import dist as pdist
+    return pdist.init("nccl")
+
+
+def max_over_ranks(dist, x):
+    from pvof import dist as pdist
+    return pdist.max_over_ranks(dist, x, device="cuda")
+
+
+def barrier(dist):
+    if dist is not None:
+        import torch
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        for line in self.f.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"],
+                                 parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per cell-iteration of a solver kernel from the committed ncu
+    summary (profiles/ncu_traffic.json), or None."""
+    try:
+        with open(os.path.join(REPO, "profiles", "ncu_traffic.json")) as f:
+            d = json.load(f)
+        return float(d[kernel]["dram_bytes_per_cell_iter"])
+    except (OSError, KeyError, ValueError, TypeError):
+        return None
+
+
+def reference_timing(steps, timeout=1800):
+    """Run the reference build on the bench case; (cell-updates/s, seconds, steps)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle as po  # checker / CPU baseline only
+    binary = po.ref_binary("rt2d")
+    if not os.path.exists(binary):
+        return None
+    grid, params, planes = case()
+    with tempfile.TemporaryDirectory() as wd:
+        cp = po.run_reference("rt2d", wd, grid, params, planes, steps, DT, 0, timeout=timeout)
+    for line in cp.stdout.splitlines():
+        if line.startswith("REF_TIMING"):
+            kv = dict(x.split("=") for x in line.split()[1:])
+            secs = float(kv["seconds"])
+            cells = int(kv["cells"])
+            return cells * steps / secs, secs, steps
+    return None
+
+
+def run_reference_arm(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    steps = max(1, min(args.steps, args.ref_steps))
+    r = reference_timing(steps)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/ref_rt2d is missing"}))
+        return 0
+    value, secs, n = r
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": n, "warmup": 0, "ms_per_step": 1e3 * secs / n, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": "%dx%d" % (NXM, NYM), "cells": NXM * NYM, "dt": DT},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": "%d time steps of the same case, single-rank reference build (no MPI on this "
+                                   "host), %.1f s" % (n, secs)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def pinned_like(n):
+    import torch
+    return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+
+
+def run_ours(args):
+    ws, rank, local = dist_env()
+    dist = init_dist(ws, local)
+    from pvof import abi, cases, runtime
+    grid, params, planes = case()
+    cells = NXM * NYM
+    g = runtime.Solver(grid, params, device=local)
+    g.set_planes(planes)
+    g.initialize()
+    log("rank %d: warmup %d steps" % (rank, args.warmup))
+    for _ in range(args.warmup):
+        g.run_steps(1, DT)
+    g.synchronize()
+
+    # ---- device-resident timing ------------------------------------------
+    clocks = Clocks(local)
+    g.set_solver_timing(True)
+    barrier(dist)
+    l0 = g.launch_count()
+    clocks.start()
+    wall0 = time.time()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        g.flush_l2()
+        g.timer_start()
+        g.run_steps(1, DT)
+        total_ms += g.timer_stop()
+    wall = time.time() - wall0
+    clk = clocks.stop()
+    barrier(dist)
+    launches = g.launch_count() - l0
+    timing = {k: g.solver_timing(k) for k in (0, 1, 2)}
+    g.set_solver_timing(False)
+    t_max = max_over_ranks(dist, total_ms)
+    value = ws * cells * args.steps / (t_max * 1e-3)
+
+    # ---- end to end through the C ABI with host buffers ---------------------
+    blocks = {f: pinned_like(g.block_count(f)) for f in STATE_FIELDS}
+    for f in STATE_FIELDS:
+        g.download(f, out=blocks[f])
+    h2d = d2h = 0
+    NX, NY, NZ = cases.dims(grid)
+    plane_flow = (NX + 6) * (NY + 6) * 8
+    plane_ng = NX * NY * 8
+    for f in STATE_FIELDS:
+        ng = abi.FIELD[f] in abi.NG_FIELDS
+        h2d += plane_ng if ng else plane_flow
+        d2h += (plane_ng if ng else plane_flow) * NZ
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    barrier(dist)
+    e2e_ms = 0.0
+    for _ in range(e2e_steps):
+        g.timer_start()
+        for f in STATE_FIELDS:
+            g.upload(f, blocks[f])
+        g.run_steps(1, DT)
+        for f in STATE_FIELDS:
+            g.download(f, out=blocks[f])
+        e2e_ms += g.timer_stop()
+    barrier(dist)
+    e2e_max = max_over_ranks(dist, e2e_ms)
+    e2e_value = ws * cells * e2e_steps / (e2e_max * 1e-3)
+
+    # ---- roofline of the dominant kernel ----------------------------------
+    dom = max(timing, key=lambda k: timing[k]["ms"])
+    t = timing[dom]
+    peak, peak_kind = measured_peak()
+    achieved = ALG_BYTES[dom] * t["cell_iters"] / (t["ms"] * 1e-3) / 1e9 if t["ms"] > 0 else 0.0
+    tr = profile_traffic(SOLVER_NAMES[dom])
+    traffic = tr * t["cell_iters"] / max(t["launches"], 1) if tr is not None else None
+    shares = {SOLVER_NAMES[k]: round(timing[k]["ms"] / total_ms, 4) for k in timing}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        r = reference_timing(args.cpu_steps)
+        if r is not None:
+            v, secs, n = r
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": "%d time steps of the same 128x512 case by the single-rank reference build, %.1f s"
+                             % (n, secs)}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": "%dx%d" % (NXM, NYM), "cells": cells, "dt": DT,
+                       "parallelism": "replicas" if ws > 1 else "single",
+                       "l2": "flushed before every timed step (memset of 2x L2, outside the timed intervals)",
+                       "solver_iterations": {SOLVER_NAMES[k]: timing[k]["iterations"] for k in timing},
+                       "solver_time_share": shares},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps},
+            "gpu_launches": launches,
+            "roofline": {"kernel": SOLVER_NAMES[dom], "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "alg_bytes_per_cell_iter": ALG_BYTES[dom],
+                         "avg_launch_ms": t["ms"] / max(t["launches"], 1)},
+            "clocks": clk,
+            "wall_s": wall,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    g.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-steps", type=int, default=5)
+    ap.add_argument("--ref-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        log("note: fewer than 3 warm-up steps")
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -217,9 +217,28 @@ int pvof_run_steps(pvof_ctx *ctx, int nsteps, double dt, pvof_stats *stats);
  * VOF_DIFFUSE.c:1071-1091), computed on the device in FP64. */
 int pvof_liquid_mass(pvof_ctx *ctx, double *mass);
 
-/* Number of CUDA kernels this context has launched so far (bookkeeping for
- * benchmarks). */
+/* --- measurement (no counterpart in the reference) ---------------------- */
+/* Number of CUDA kernels this context has launched so far. */
 long long pvof_launch_count(const pvof_ctx *ctx);
+/* Device time of everything issued on the context's stream between
+ * pvof_timer_start and pvof_timer_stop (CUDA events on that stream);
+ * pvof_timer_stop waits for the work and returns milliseconds. */
+int pvof_timer_start(pvof_ctx *ctx);
+int pvof_timer_stop(pvof_ctx *ctx, double *ms);
+/* Write a device buffer larger than the L2 cache on the context's stream so
+ * the next timed region starts with a cold L2. */
+int pvof_flush_l2(pvof_ctx *ctx);
+/* Per-solver launch timing, collected while enabled: PVOF_SOLVER_* selects
+ * the biharmonic CG, the velocity PCG or the pressure PCG.  ms is the summed
+ * device duration of its launches (CUDA events around each launch),
+ * cell_iters the sum over launches of (cells in the solve range) x
+ * (iterations). */
+#define PVOF_SOLVER_BIHARMONIC 0
+#define PVOF_SOLVER_VELOCITY 1
+#define PVOF_SOLVER_PRESSURE 2
+int pvof_set_solver_timing(pvof_ctx *ctx, int enabled);
+int pvof_solver_timing(const pvof_ctx *ctx, int solver, double *ms, long long *launches, long long *iterations,
+                       long long *cell_iters);
 
 #ifdef __cplusplus
 }

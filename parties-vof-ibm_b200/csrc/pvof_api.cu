@@ -5,6 +5,7 @@
 // ghost update the reference performs at that point (file:line citations are
 // relative to PARTIES/src).  Nothing here computes on the host; there is no
 // CPU fallback: without a CUDA device pvof_create fails with PVOF_ENODEV.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -211,14 +212,43 @@ int coop_blocks(pvof_ctx *c, int n)
     return b;
 }
 
+// kind: PVOF_SOLVER_*; comp: velocity component (0/1)
 template <class A>
-int coop_launch(pvof_ctx *c, const void *fn, A &args, int n)
+int coop_launch(pvof_ctx *c, const void *fn, A &args, int n, int kind, int comp)
 {
     void *params[] = {&args};
     int nb = coop_blocks(c, n);
+    int slot = -1;
+    if (c->solver_timing && c->npend < Ctx::NPEND) {
+        slot = c->npend++;
+        c->pend_kind[slot] = kind;
+        c->pend_comp[slot] = comp;
+        c->pend_cells[slot] = n;
+        CK(cudaEventRecord(c->pend_ev[slot][0], c->stream));
+    }
     CK(cudaLaunchCooperativeKernel(fn, dim3((unsigned)nb), dim3(COOP_THREADS), params, 0, c->stream));
     c->launches++;
+    if (slot >= 0) CK(cudaEventRecord(c->pend_ev[slot][1], c->stream));
     return PVOF_OK;
+}
+
+// after a stream synchronisation: fold the finished solver launches into the
+// per-solver totals (iteration counts come from the device scalars)
+void collect_solver_timing(pvof_ctx *c)
+{
+    const DevScalars &h = *c->scal_host;
+    for (int q = 0; q < c->npend; q++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, c->pend_ev[q][0], c->pend_ev[q][1]) != cudaSuccess) continue;
+        int k = c->pend_kind[q];
+        long long it = k == PVOF_SOLVER_BIHARMONIC ? h.ch_iters
+                     : (k == PVOF_SOLVER_VELOCITY ? h.vel_iters[c->pend_comp[q]] : h.p_iters);
+        c->sol_ms[k] += ms;
+        c->sol_launches[k] += 1;
+        c->sol_iters[k] += it;
+        c->sol_cell_iters[k] += it * c->pend_cells[q];
+    }
+    c->npend = 0;
 }
 
 double *F(pvof_ctx *c, int id) { return c->f[id]; }
@@ -337,7 +367,7 @@ int vof_diffuse_step(pvof_ctx *c)
     A.maxit = (c->p.ch_iter_max > 0) ? c->p.ch_iter_max : c->p.CG_MAXIT;
     A.partials = c->partials;
     A.scal = c->scal;
-    TRY(coop_launch(c, (const void *)k_cg_biharmonic, A, NX * NY));
+    TRY(coop_launch(c, (const void *)k_cg_biharmonic, A, NX * NY, PVOF_SOLVER_BIHARMONIC, 0));
     TRY(fill(c, BK_SCALAR, CL));
     // clamp, phase cache, history shift (VOF_DIFFUSE.c:1324-1358)
     TRY(bound(c));
@@ -482,7 +512,7 @@ int velocity_solve(pvof_ctx *c, int comp)
     A.maxit = c->p.CG_MAXIT;
     A.partials = c->partials;
     A.scal = c->scal;
-    return coop_launch(c, (const void *)k_cg_velocity, A, (A.i1 - A.i0) * (A.j1 - A.j0));
+    return coop_launch(c, (const void *)k_cg_velocity, A, (A.i1 - A.i0) * (A.j1 - A.j0), PVOF_SOLVER_VELOCITY, comp);
 }
 
 }  // namespace
@@ -529,7 +559,7 @@ int p_solve(pvof_ctx *c)
     A.maxit = c->p.P_CG_MAXIT;
     A.partials = c->partials;
     A.scal = c->scal;
-    TRY(coop_launch(c, (const void *)k_cg_pressure, A, (c->dom.NX - 1) * (c->dom.NY - 1)));
+    TRY(coop_launch(c, (const void *)k_cg_pressure, A, (c->dom.NX - 1) * (c->dom.NY - 1), PVOF_SOLVER_PRESSURE, 0));
     return fill(c, BK_WRAP_C, F(c, PVOF_F_DELTAP));
 }
 
@@ -558,6 +588,7 @@ int read_scalars(pvof_ctx *c)
 {
     CK(cudaMemcpyAsync(c->scal_host, c->scal, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (c->npend) collect_solver_timing(c);
     if (c->scal_host->error) {
         CK(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
         CK(cudaStreamSynchronize(c->stream));
@@ -782,6 +813,11 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     cudaMemset(c->scal, 0, sizeof(DevScalars));
     if (cudaMallocHost(&c->scal_host, sizeof(DevScalars)) != cudaSuccess) return fail(PVOF_ENOMEM, "pinned scalars");
     std::memset(c->scal_host, 0, sizeof(DevScalars));
+    for (int q = 0; q < 2; q++)
+        if (cudaEventCreate(&c->timer_ev[q]) != cudaSuccess) return fail(PVOF_ECUDA, "event create");
+    for (int q = 0; q < Ctx::NPEND; q++)
+        for (int e = 0; e < 2; e++)
+            if (cudaEventCreate(&c->pend_ev[q][e]) != cudaSuccess) return fail(PVOF_ECUDA, "event create");
     if (cudaDeviceSynchronize() != cudaSuccess) return fail(PVOF_ECUDA, "create sync");
     c->stage = 0;
     c->dt = 0.0;
@@ -802,6 +838,10 @@ int pvof_destroy(pvof_ctx *c)
     if (c->partials) cudaFree(c->partials);
     if (c->scal) cudaFree(c->scal);
     if (c->scal_host) cudaFreeHost(c->scal_host);
+    if (c->flush_buf) cudaFree(c->flush_buf);
+    for (int q = 0; q < 2; q++) if (c->timer_ev[q]) cudaEventDestroy(c->timer_ev[q]);
+    for (int q = 0; q < Ctx::NPEND; q++)
+        for (int e = 0; e < 2; e++) if (c->pend_ev[q][e]) cudaEventDestroy(c->pend_ev[q][e]);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PVOF_OK;
@@ -994,7 +1034,63 @@ int pvof_liquid_mass(pvof_ctx *c, double *mass)
     return PVOF_OK;
 }
 
-// number of kernels this context has launched (benchmark bookkeeping)
 long long pvof_launch_count(const pvof_ctx *c) { return c ? c->launches : 0; }
+
+int pvof_timer_start(pvof_ctx *c)
+{
+    ENTER(c);
+    CK(cudaEventRecord(c->timer_ev[0], c->stream));
+    return PVOF_OK;
+}
+
+int pvof_timer_stop(pvof_ctx *c, double *ms)
+{
+    ENTER(c);
+    CK(cudaEventRecord(c->timer_ev[1], c->stream));
+    CK(cudaEventSynchronize(c->timer_ev[1]));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, c->timer_ev[0], c->timer_ev[1]));
+    if (ms) *ms = t;
+    return PVOF_OK;
+}
+
+int pvof_flush_l2(pvof_ctx *c)
+{
+    ENTER(c);
+    if (!c->flush_buf) {
+        int l2 = 0;
+        cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, c->device);
+        c->flush_bytes = (size_t)std::max(l2, 1 << 20) * 2;
+        if (cudaMalloc(&c->flush_buf, c->flush_bytes) != cudaSuccess) {
+            c->flush_buf = nullptr;
+            return set_err(PVOF_ENOMEM, "cudaMalloc flush buffer");
+        }
+    }
+    CK(cudaMemsetAsync(c->flush_buf, (int)(c->launches & 0xff), c->flush_bytes, c->stream));
+    return PVOF_OK;
+}
+
+int pvof_set_solver_timing(pvof_ctx *c, int enabled)
+{
+    ENTER(c);
+    c->solver_timing = enabled ? 1 : 0;
+    for (int k = 0; k < 3; k++) {
+        c->sol_ms[k] = 0.0;
+        c->sol_launches[k] = c->sol_iters[k] = c->sol_cell_iters[k] = 0;
+    }
+    c->npend = 0;
+    return PVOF_OK;
+}
+
+int pvof_solver_timing(const pvof_ctx *c, int solver, double *ms, long long *launches, long long *iterations,
+                       long long *cell_iters)
+{
+    if (!c || solver < 0 || solver > 2) return set_err(PVOF_EINVAL, "bad solver index");
+    if (ms) *ms = c->sol_ms[solver];
+    if (launches) *launches = c->sol_launches[solver];
+    if (iterations) *iterations = c->sol_iters[solver];
+    if (cell_iters) *cell_iters = c->sol_cell_iters[solver];
+    return PVOF_OK;
+}
 
 }  // extern "C"

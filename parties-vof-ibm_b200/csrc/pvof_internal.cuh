@@ -122,6 +122,18 @@ struct Ctx {
     int coop_blocks;         // co-resident blocks for the persistent solvers
     int coop_threads;
     long long launches;      // kernels launched by this context
+    // measurement
+    cudaEvent_t timer_ev[2];
+    double *flush_buf;
+    size_t flush_bytes;
+    int solver_timing;
+    static constexpr int NPEND = 16;
+    cudaEvent_t pend_ev[NPEND][2];
+    int pend_kind[NPEND], pend_comp[NPEND];
+    long long pend_cells[NPEND];
+    int npend;
+    double sol_ms[3];
+    long long sol_launches[3], sol_iters[3], sol_cell_iters[3];
 };
 
 }  // namespace pvof

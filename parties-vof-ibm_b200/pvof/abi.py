@@ -110,4 +110,10 @@ EXPORTS = [
     "pvof_Pressure_compute_velocity_divergence",
     "pvof_substep", "pvof_run_steps", "pvof_liquid_mass",
     "pvof_initialize",
+    "pvof_launch_count", "pvof_timer_start", "pvof_timer_stop", "pvof_flush_l2",
+    "pvof_set_solver_timing", "pvof_solver_timing",
 ]
+
+SOLVER_BIHARMONIC = 0
+SOLVER_VELOCITY = 1
+SOLVER_PRESSURE = 2

@@ -60,6 +60,11 @@ def load():
     L.pvof_liquid_mass.argtypes = [V, P(C.c_double)]
     L.pvof_launch_count.argtypes = [V]
     L.pvof_launch_count.restype = C.c_longlong
+    L.pvof_timer_start.argtypes = [V]
+    L.pvof_timer_stop.argtypes = [V, P(C.c_double)]
+    L.pvof_flush_l2.argtypes = [V]
+    L.pvof_set_solver_timing.argtypes = [V, C.c_int]
+    L.pvof_solver_timing.argtypes = [V, C.c_int, P(C.c_double), P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]
     _lib = L
     return L
 
@@ -148,3 +153,24 @@ class Solver:
 
     def launch_count(self):
         return load().pvof_launch_count(self.h)
+
+    # -- measurement ---------------------------------------------------------
+    def timer_start(self):
+        check(load().pvof_timer_start(self.h), "pvof_timer_start")
+
+    def timer_stop(self):
+        ms = C.c_double()
+        check(load().pvof_timer_stop(self.h, C.byref(ms)), "pvof_timer_stop")
+        return ms.value
+
+    def flush_l2(self):
+        check(load().pvof_flush_l2(self.h), "pvof_flush_l2")
+
+    def set_solver_timing(self, on):
+        check(load().pvof_set_solver_timing(self.h, 1 if on else 0), "pvof_set_solver_timing")
+
+    def solver_timing(self, solver):
+        ms, nl, it, ci = C.c_double(), C.c_longlong(), C.c_longlong(), C.c_longlong()
+        check(load().pvof_solver_timing(self.h, solver, C.byref(ms), C.byref(nl), C.byref(it), C.byref(ci)),
+              "pvof_solver_timing")
+        return {"ms": ms.value, "launches": nl.value, "iterations": it.value, "cell_iters": ci.value}
