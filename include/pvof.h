@@ -128,7 +128,8 @@ typedef struct pvof_stats {
     double p_res;
     int poisson_passes;    /* outer loop count (Temporal_int.c:1052-1107) */
     double div_max;        /* Pressure_compute_velocity_divergence */
-    double clamp_mass;     /* liquid mass changed by the C_L clamp (VOF_DIFFUSE.c:1093) */
+    double clamp_mass;     /* liquid mass changed by the C_L clamp over the physical cells
+                              (VOF_DIFFUSE.c:1093-1127) */
 } pvof_stats;
 
 typedef struct pvof_ctx pvof_ctx;

@@ -50,7 +50,7 @@ int set_err(int code, const std::string &msg)
     } while (0)
 
 constexpr int TBX = 32, TBY = 8;
-constexpr int COOP_THREADS = 256;
+constexpr int COOP_THREADS = 512;
 
 bool is_ng(int field) { return field >= PVOF_F_U_EXPLICIT && field <= PVOF_F_FSIG_NEW_Y; }
 
@@ -62,10 +62,12 @@ bool is_ng(int field) { return field >= PVOF_F_U_EXPLICIT && field <= PVOF_F_FSI
 struct HostMetrics {
     std::vector<double> xu, xc, dx_u, dx_c, idx_u, idx_c, yv, yc, dy_v, dy_c, idy_v, idy_c;
     std::vector<double> r_u, r_c, inv_r_u, inv_r_c, ring_wt_c;
+    std::vector<double> wx, wy;
 };
 
 void build_metrics(const pvof_grid_desc &g, int NX, int NY, HostMetrics &h)
 {
+    const bool perx = g.periodic[0] != 0, pery = g.periodic[1] != 0;
     int nx = NX + 2 * NG, ny = NY + 2 * NG;
     auto z = [](std::vector<double> &v, int n) { v.assign((size_t)n, 0.0); };
     z(h.xu, nx); z(h.xc, nx); z(h.dx_u, nx); z(h.dx_c, nx); z(h.idx_u, nx); z(h.idx_c, nx);
@@ -102,6 +104,21 @@ void build_metrics(const pvof_grid_desc &g, int NX, int NY, HostMetrics &h)
             h.inv_r_c[i + NG] = (rc > 1.0e-14) ? 1.0 / rc : 0.0;
             h.ring_wt_c[i + NG] = g.theta_span * rc;
         }
+    }
+    // inner-product weights: each G-range position adds its measure to the
+    // physical cell the scalar ghost update copies into it (the half cell
+    // i = NX-1 copies cell 0 when periodic, NX-2 at a wall; likewise in y)
+    h.wx.assign((size_t)nx, 0.0);
+    h.wy.assign((size_t)ny, 0.0);
+    for (int i = 0; i < NX; i++) {
+        int s = (i == NX - 1) ? (perx ? 0 : NX - 2) : i;
+        double w = h.dx_u[i + NG];
+        if (g.geometry == PVOF_GEOM_AXISYM) w = w * h.ring_wt_c[i + NG];
+        h.wx[s + NG] += w;
+    }
+    for (int j = 0; j < NY; j++) {
+        int s = (j == NY - 1) ? (pery ? 0 : NY - 2) : j;
+        h.wy[s + NG] += h.dy_v[j + NG];
     }
 }
 
@@ -212,12 +229,11 @@ int coop_blocks(pvof_ctx *c, int n)
     return b;
 }
 
-// kind: PVOF_SOLVER_*; comp: velocity component (0/1)
-template <class A>
-int coop_launch(pvof_ctx *c, const void *fn, A &args, int n, int kind, int comp)
+// Issue one solver launch, bracketed by timing events when enabled.
+// kind: PVOF_SOLVER_*; comp: velocity component (0/1); n: cells solved.
+template <class L>
+int timed_launch(pvof_ctx *c, int kind, int comp, int n, L launch)
 {
-    void *params[] = {&args};
-    int nb = coop_blocks(c, n);
     int slot = -1;
     if (c->solver_timing && c->npend < Ctx::NPEND) {
         slot = c->npend++;
@@ -226,10 +242,20 @@ int coop_launch(pvof_ctx *c, const void *fn, A &args, int n, int kind, int comp)
         c->pend_cells[slot] = n;
         CK(cudaEventRecord(c->pend_ev[slot][0], c->stream));
     }
-    CK(cudaLaunchCooperativeKernel(fn, dim3((unsigned)nb), dim3(COOP_THREADS), params, 0, c->stream));
+    CK(launch());
     c->launches++;
     if (slot >= 0) CK(cudaEventRecord(c->pend_ev[slot][1], c->stream));
     return PVOF_OK;
+}
+
+template <class A>
+int coop_launch(pvof_ctx *c, const void *fn, A &args, int n, int kind, int comp)
+{
+    int nb = coop_blocks(c, n);
+    return timed_launch(c, kind, comp, n, [&]() {
+        void *params[] = {&args};
+        return cudaLaunchCooperativeKernel(fn, dim3((unsigned)nb), dim3(COOP_THREADS), params, 0, c->stream);
+    });
 }
 
 // after a stream synchronisation: fold the finished solver launches into the
@@ -501,6 +527,8 @@ int velocity_solve(pvof_ctx *c, int comp)
     A.mu = F(c, PVOF_F_MU);
     A.r = S(c, comp == 0 ? SC_U_R : SC_V_R);
     A.dir = S(c, comp == 0 ? SC_U_D : SC_V_D);
+    A.dir2 = S(c, comp == 0 ? SC_U_D2 : SC_V_D2);
+    A.z = S(c, comp == 0 ? SC_U_Z : SC_V_Z);
     A.Ad = S(c, comp == 0 ? SC_U_AD : SC_V_AD);
     A.diag = S(c, comp == 0 ? SC_U_DIAG : SC_V_DIAG);
     A.iRe = 1.0 / c->p.Re;
@@ -554,12 +582,18 @@ int p_solve(pvof_ctx *c)
     A.M = S(c, SC_P_MINV);
     A.res = S(c, SC_P_RES);
     A.dir = S(c, SC_P_D);
+    A.dir2 = S(c, SC_P_D2);
+    A.z = S(c, SC_P_Z);
     A.Ad = S(c, SC_P_AD);
     A.tol = c->p.P_CG_ETOL;
     A.maxit = c->p.P_CG_MAXIT;
     A.partials = c->partials;
     A.scal = c->scal;
-    TRY(coop_launch(c, (const void *)k_cg_pressure, A, (c->dom.NX - 1) * (c->dom.NY - 1), PVOF_SOLVER_PRESSURE, 0));
+    const int n = (c->dom.NX - 1) * (c->dom.NY - 1);
+    if (c->cgc_smem)
+        TRY(timed_launch(c, PVOF_SOLVER_PRESSURE, 0, n, [&]() { return cgc_pressure_launch(A, c->cgc_smem, c->stream); }));
+    else
+        TRY(coop_launch(c, (const void *)k_cg_pressure, A, n, PVOF_SOLVER_PRESSURE, 0));
     return fill(c, BK_WRAP_C, F(c, PVOF_F_DELTAP));
 }
 
@@ -729,6 +763,7 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     d.pery = grid->periodic[1] != 0;
     d.nk = grid->NZM + 1;
     d.slab = grid->slab_thickness;
+    d.wz = d.planar ? d.slab : 1.0;
     c->plane_elems = (size_t)d.P * (size_t)(d.NY + 2 * NG);
     const size_t origin = (size_t)OY * d.P + OX;
     auto fail = [&](int code, const std::string &m) {
@@ -751,7 +786,7 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     build_metrics(*grid, d.NX, d.NY, hm);
     std::vector<const std::vector<double> *> mv = {&hm.idx_u, &hm.idx_c, &hm.dx_c, &hm.dx_u, &hm.r_u, &hm.r_c,
                                                    &hm.inv_r_u, &hm.inv_r_c, &hm.ring_wt_c,
-                                                   &hm.idy_v, &hm.idy_c, &hm.dy_c, &hm.dy_v};
+                                                   &hm.idy_v, &hm.idy_c, &hm.dy_c, &hm.dy_v, &hm.wx, &hm.wy};
     size_t mtot = 0;
     for (auto *v : mv) mtot += v->size();
     if (cudaMalloc(&c->metric_mem, mtot * sizeof(double)) != cudaSuccess) return fail(PVOF_ENOMEM, "cudaMalloc metrics");
@@ -767,6 +802,7 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     d.m.idx_u = mptr[0]; d.m.idx_c = mptr[1]; d.m.dx_c = mptr[2]; d.m.dx_u = mptr[3];
     d.m.r_u = mptr[4]; d.m.r_c = mptr[5]; d.m.inv_r_u = mptr[6]; d.m.inv_r_c = mptr[7]; d.m.ring_wt_c = mptr[8];
     d.m.idy_v = mptr[9]; d.m.idy_c = mptr[10]; d.m.dy_c = mptr[11]; d.m.dy_v = mptr[12];
+    d.m.wx = mptr[13]; d.m.wy = mptr[14];
     // ghost maps
     std::vector<int> srcs;
     std::vector<double> muls;
@@ -807,6 +843,8 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     if (ob < 1) return fail(PVOF_ECUDA, "persistent solver kernels do not fit on an SM");
     c->coop_blocks = ob * nsm;
     c->coop_threads = COOP_THREADS;
+    // cluster-resident pressure solver when the grid fits one cluster
+    c->cgc_smem = getenv("PVOF_NO_CLUSTER_SOLVER") ? 0 : cgc_pressure_setup(d.NX, d.NY);
     size_t npart = 4 * (size_t)std::max(c->coop_blocks, (int)(((d.NX + TBX - 1) / TBX) * ((d.NY + TBY - 1) / TBY)));
     if (cudaMalloc(&c->partials, npart * sizeof(double)) != cudaSuccess) return fail(PVOF_ENOMEM, "cudaMalloc partials");
     if (cudaMalloc(&c->scal, sizeof(DevScalars)) != cudaSuccess) return fail(PVOF_ENOMEM, "cudaMalloc scalars");

@@ -6,19 +6,25 @@
 // sums of each inner product in the same fixed order, so all blocks take the
 // same convergence decisions.  Cells are assigned to threads by the same
 // grid-stride mapping in every phase, so a thread reads back its own cells'
-// private vectors (diagonal, Ad, the new direction) without a barrier.
+// private values (diagonal, Ad) without a barrier.
+//
+// Two grid barriers per iteration: the new search direction d_k = z_k +
+// beta d_{k-1} is not written in a phase of its own; the matrix-vector phase
+// writes it for its own cells into the second direction buffer and evaluates
+// it on the fly at the stencil neighbours (from z and d_{k-1}, with the
+// reference's ghost update of d applied through the same source maps).  The
+// arithmetic per value is the reference's, so the iterates are those of the
+// reference's loop.
 //
 // The grid barrier is this file's own (not cooperative_groups::grid_group::
 // sync) so that its wait is bounded: if the other blocks never arrive it
 // records an error in DevScalars::error and every block leaves the solver.
-#include <cuda/atomic>
-
 #include "pvof_device.cuh"
 #include "pvof_kernels.cuh"
 
 namespace pvof {
 
-constexpr unsigned long long BARRIER_SPIN_LIMIT = 1ull << 25;
+constexpr unsigned long long BARRIER_SPIN_LIMIT = 1ull << 26;
 
 struct GridSync {
     DevScalars *s;
@@ -26,29 +32,31 @@ struct GridSync {
 };
 
 // Returns false (in every thread of the block) when the barrier gave up.
-__device__ bool grid_barrier(const GridSync &gs)
+__device__ __noinline__ bool grid_barrier(const GridSync &gs)
 {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(gs.s->bar_count);
-        cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(gs.s->bar_gen);
-        cuda::atomic_ref<int, cuda::thread_scope_device> err(gs.s->error);
-        int good = err.load(cuda::memory_order_relaxed) == 0;
-        unsigned g = gen.load(cuda::memory_order_acquire);
-        unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+        volatile unsigned *vgen = &gs.s->bar_gen;
+        volatile int *verr = &gs.s->error;
+        int good = (*verr == 0);
+        unsigned g = *vgen;
+        __threadfence();
+        unsigned arrived = atomicAdd(&gs.s->bar_count, 1u);
         if (arrived == gs.nblocks - 1) {
-            cnt.store(0u, cuda::memory_order_relaxed);
-            gen.fetch_add(1u, cuda::memory_order_release);
+            gs.s->bar_count = 0u;
+            __threadfence();
+            atomicAdd(&gs.s->bar_gen, 1u);
         } else {
             unsigned long long spins = 0;
-            while (gen.load(cuda::memory_order_acquire) == g) {
-                if (err.load(cuda::memory_order_relaxed) != 0 || ++spins > BARRIER_SPIN_LIMIT) {
-                    err.store(1, cuda::memory_order_relaxed);
+            while (*vgen == g) {
+                ++spins;
+                if ((spins & 1023ull) == 0 && (*verr != 0 || spins > BARRIER_SPIN_LIMIT)) {
+                    atomicExch(&gs.s->error, 1);
                     good = 0;
                     break;
                 }
-                __nanosleep(32);
+                if (spins > 4096) __nanosleep(64);
             }
         }
         __threadfence();
@@ -106,41 +114,67 @@ struct Range {
     __device__ __forceinline__ void ij(int q, int &i, int &j) const { i = i0 + q % w; j = j0 + q / w; }
 };
 
+// source of (i,j) under a ghost map (identity in the interior)
+__device__ __forceinline__ void src_of(const BcMap &m, int NX, int NY, int i, int j, int &si, int &sj, double &mul)
+{
+    if (i >= 1 && i <= NX - 2 && j >= 1 && j <= NY - 2) {
+        si = i; sj = j; mul = 1.0;
+        return;
+    }
+    si = m.x.src[i + NG];
+    sj = m.y.src[j + NG];
+    mul = m.x.mul[i + NG] * m.y.mul[j + NG];
+}
+
 // ---------------------------------------------------------------------------
 // diffuse_solve_biharmonic_pcg (Eulerian/VOF_DIFFUSE.c:339-429): CG on
-// [a_dt I + bih L.L] x = b over the G range, inner products weighted by the
-// cell measure and summed over the reference's nk identical planes.
+// [a_dt I + bih L.L] x = b.  The reference iterates over the G range, whose
+// half cells (i = NX-1, j = NY-1) hold exact copies of their boundary source
+// cells at every iteration; here every physical cell carries the summed
+// measure W of itself and its copies, and both Laplacians of the operator are
+// evaluated on the fly (with the scalar ghost update in between), so one
+// iteration needs two grid barriers.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_cg_biharmonic(BihArgs A)
+__global__ void __launch_bounds__(512) k_cg_biharmonic(BihArgs A)
 {
     const Dom &d = A.d;
     const int P = d.P, NX = d.NX, NY = d.NY;
     const GridSync gs{A.scal, gridDim.x};
-    const Range R{0, 0, NX, NX * NY};
+    const Range R{0, 0, NX - 1, (NX - 1) * (NY - 1)};
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
     const double nk = (double)d.nk;
     double *part0 = A.partials, *part1 = A.partials + gridDim.x;
     double *part2 = A.partials + 2 * gridDim.x, *part3 = A.partials + 3 * gridDim.x;
-    auto X = [&](int a, int b) { return remap(A.msc, A.x, P, NX, NY, a, b); };
 
-    // Ap = A x (two Laplacians with the scalar ghost update in between)
-    for (int q = tid; q < R.n; q += nth) {
-        int i, j;
-        R.ij(q, i, j);
-        AT_(A.aux, i, j) = lap_at(d, i, j, X);
-    }
-    if (!grid_barrier(gs)) return;
+    // L(L(f)) at (i,j) for a field given at sources: lap of the ghost-updated
+    // Laplacian of the ghost-updated f (VOF_DIFFUSE_compute_laplacian twice)
+    auto bilap = [&](int i, int j, auto fsrc) {
+        auto fv = [&](int a, int b) {
+            int si, sj;
+            double mul;
+            src_of(A.msc, NX, NY, a, b, si, sj, mul);
+            return fsrc(si, sj);
+        };
+        auto lapv = [&](int a, int b) {
+            int si, sj;
+            double mul;
+            src_of(A.msc, NX, NY, a, b, si, sj, mul);
+            return lap_at(d, si, sj, fv);
+        };
+        return lap_at(d, i, j, lapv);
+    };
+
     double sbb = 0.0, srr = 0.0;
     for (int q = tid; q < R.n; q += nth) {
         int i, j;
         R.ij(q, i, j);
-        double l2 = lap_at(d, i, j, [&](int a, int b) { return remap(A.msc, A.aux, P, NX, NY, a, b); });
+        double l2 = bilap(i, j, [&](int a, int b) { return AT_(A.x, a, b); });
         double ap = A.a_dt * AT_(A.x, i, j) + A.bih * l2;
         double bv = AT_(A.b, i, j);
         double rv = bv - ap;
         AT_(A.r, i, j) = rv;
         AT_(A.p1, i, j) = rv;
-        double m = cell_measure(d, i, j);
+        double m = d.m.wx[i] * d.m.wy[j] * d.wz;
         sbb += m * bv * bv;
         srr += m * rv * rv;
     }
@@ -156,45 +190,32 @@ __global__ void __launch_bounds__(256) k_cg_biharmonic(BihArgs A)
         if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->ch_iters = 0; A.scal->ch_rel = rel; }
         return;
     }
-    double *pcur = A.p1, *pold = A.p2;
+    double *pcur = A.p1, *pnxt = A.p2;
     double beta = 0.0;
     bool first = true;
     while (iter < A.maxit) {
-        // direction p = r + beta p_old (the first direction is r itself) and
-        // aux = L(p) with the scalar ghost update of p applied on the fly
-        if (!first) {
-            double *t = pold; pold = pcur; pcur = t;
-            for (int q = tid; q < R.n; q += nth) {
-                int i, j;
-                R.ij(q, i, j);
-                AT_(pcur, i, j) = AT_(A.r, i, j) + beta * AT_(pold, i, j);
-            }
-            for (int q = tid; q < R.n; q += nth) {
-                int i, j;
-                R.ij(q, i, j);
-                AT_(A.aux, i, j) = lap_at(d, i, j, [&](int a, int b) {
-                    return remap(A.msc, A.r, P, NX, NY, a, b) + beta * remap(A.msc, pold, P, NX, NY, a, b);
-                });
-            }
-        } else {
-            for (int q = tid; q < R.n; q += nth) {
-                int i, j;
-                R.ij(q, i, j);
-                AT_(A.aux, i, j) = lap_at(d, i, j, [&](int a, int b) { return remap(A.msc, pcur, P, NX, NY, a, b); });
-            }
-        }
-        first = false;
-        if (!grid_barrier(gs)) return;
+        // p = z + beta p (z = r); Ap = a_dt p + bih L(L(p))
         double spap = 0.0;
+        const double bt = beta;
+        const double *pold = pcur;
         for (int q = tid; q < R.n; q += nth) {
             int i, j;
             R.ij(q, i, j);
-            double l2 = lap_at(d, i, j, [&](int a, int b) { return remap(A.msc, A.aux, P, NX, NY, a, b); });
-            double pv = AT_(pcur, i, j);
+            double pv, l2;
+            if (first) {
+                pv = AT_(pold, i, j);
+                l2 = bilap(i, j, [&](int a, int b) { return AT_(pold, a, b); });
+            } else {
+                pv = AT_(A.r, i, j) + bt * AT_(pold, i, j);
+                AT_(pnxt, i, j) = pv;
+                l2 = bilap(i, j, [&](int a, int b) { return AT_(A.r, a, b) + bt * AT_(pold, a, b); });
+            }
             double ap = A.a_dt * pv + A.bih * l2;
             AT_(A.Ap, i, j) = ap;
-            spap += cell_measure(d, i, j) * pv * ap;
+            spap += d.m.wx[i] * d.m.wy[j] * d.wz * pv * ap;
         }
+        if (!first) { double *t = pcur; pcur = pnxt; pnxt = t; }
+        first = false;
         put_partial(part2, spap);
         if (!grid_barrier(gs)) return;
         double pAp = nk * grid_total(part2);
@@ -207,7 +228,7 @@ __global__ void __launch_bounds__(256) k_cg_biharmonic(BihArgs A)
             AT_(A.x, i, j) += alpha * AT_(pcur, i, j);
             double rv = AT_(A.r, i, j) - alpha * AT_(A.Ap, i, j);
             AT_(A.r, i, j) = rv;
-            srr2 += cell_measure(d, i, j) * rv * rv;
+            srr2 += d.m.wx[i] * d.m.wy[j] * d.wz * rv * rv;
         }
         put_partial(part3, srr2);
         if (!grid_barrier(gs)) return;
@@ -226,7 +247,7 @@ __global__ void __launch_bounds__(256) k_cg_biharmonic(BihArgs A)
 // Velocity_solve_cg (Eulerian/lsolver/msolve_cg.c:525-722): Jacobi PCG with
 // the RMS residual stop, one velocity component.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_cg_velocity(VelArgs A)
+__global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
 {
     const Dom &d = A.d;
     const int P = d.P, NX = d.NX, NY = d.NY;
@@ -236,6 +257,7 @@ __global__ void __launch_bounds__(256) k_cg_velocity(VelArgs A)
     const double EPS = 1e-14;
     double *part0 = A.partials, *part1 = A.partials + gridDim.x;
     double *part2 = A.partials + 2 * gridDim.x, *part3 = A.partials + 3 * gridDim.x;
+    auto active = [&](int a, int b) { return a >= A.i0 && a < A.i1 && b >= A.j0 && b < A.j1; };
 
     double srz = 0.0;
     for (int q = tid; q < R.n; q += nth) {
@@ -248,24 +270,51 @@ __global__ void __launch_bounds__(256) k_cg_velocity(VelArgs A)
         AT_(A.r, i, j) = rv;
         double dv = rv / dg;
         AT_(A.dir, i, j) = dv;
+        AT_(A.z, i, j) = dv;
         srz += rv * dv;
     }
     put_partial(part0, srz);
     if (!grid_barrier(gs)) return;
     double rz = grid_total(part0);
-    double RMS = 0.0;
+    double RMS = 0.0, beta = 0.0;
     int iters = 0;
+    double *dcur = A.dir, *dnxt = A.dir2;
+    bool first = true;
     while (iters < A.maxit) {
         iters++;
+        // d = M^-1 r + beta d, Ad = A d with the VEL_TYPE_CG ghost update of d
         double sdad = 0.0;
+        const double bt = beta;
+        const double *dold = dcur;
         for (int q = tid; q < R.n; q += nth) {
             int i, j;
             R.ij(q, i, j);
-            double ad = vel_op(d, A.comp, A.rho, A.mu, i, j, A.iRe, A.alpha_dt,
-                               [&](int a, int b) { return remap(A.mcg, A.dir, P, NX, NY, a, b); });
+            double dv, ad;
+            if (first) {
+                dv = AT_(dold, i, j);
+                ad = vel_op(d, A.comp, A.rho, A.mu, i, j, A.iRe, A.alpha_dt, [&](int a, int b) {
+                    int si, sj;
+                    double mul;
+                    src_of(A.mcg, NX, NY, a, b, si, sj, mul);
+                    if (mul == 0.0 || !active(si, sj)) return 0.0;
+                    return mul * AT_(dold, si, sj);
+                });
+            } else {
+                dv = AT_(A.z, i, j) + bt * AT_(dold, i, j);
+                AT_(dnxt, i, j) = dv;
+                ad = vel_op(d, A.comp, A.rho, A.mu, i, j, A.iRe, A.alpha_dt, [&](int a, int b) {
+                    int si, sj;
+                    double mul;
+                    src_of(A.mcg, NX, NY, a, b, si, sj, mul);
+                    if (mul == 0.0 || !active(si, sj)) return 0.0;
+                    return mul * (AT_(A.z, si, sj) + bt * AT_(dold, si, sj));
+                });
+            }
             AT_(A.Ad, i, j) = ad;
-            sdad += AT_(A.dir, i, j) * ad;
+            sdad += dv * ad;
         }
+        if (!first) { double *t = dcur; dcur = dnxt; dnxt = t; }
+        first = false;
         put_partial(part1, sdad);
         if (!grid_barrier(gs)) return;
         double dAd = grid_total(part1);
@@ -274,10 +323,12 @@ __global__ void __launch_bounds__(256) k_cg_velocity(VelArgs A)
         for (int q = tid; q < R.n; q += nth) {
             int i, j;
             R.ij(q, i, j);
-            AT_(A.x, i, j) += alpha * AT_(A.dir, i, j);
+            AT_(A.x, i, j) += alpha * AT_(dcur, i, j);
             double ri = AT_(A.r, i, j) - alpha * AT_(A.Ad, i, j);
             AT_(A.r, i, j) = ri;
-            s0 += ri * ri / AT_(A.diag, i, j);
+            double dg = AT_(A.diag, i, j);
+            AT_(A.z, i, j) = ri / dg;
+            s0 += ri * ri / dg;
             s1 += ri * ri;
         }
         put_partial(part2, s0);
@@ -286,14 +337,8 @@ __global__ void __launch_bounds__(256) k_cg_velocity(VelArgs A)
         double rz_new = grid_total(part2), rr = grid_total(part3);
         RMS = sqrt(A.in_tot * rr);
         if (RMS < A.tol) break;
-        double beta = rz_new / (rz + EPS);
+        beta = rz_new / (rz + EPS);
         rz = rz_new;
-        for (int q = tid; q < R.n; q += nth) {
-            int i, j;
-            R.ij(q, i, j);
-            AT_(A.dir, i, j) = AT_(A.r, i, j) / AT_(A.diag, i, j) + beta * AT_(A.dir, i, j);
-        }
-        if (!grid_barrier(gs)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->vel_iters[A.comp] = iters; A.scal->vel_rms[A.comp] = RMS; }
 }
@@ -303,7 +348,7 @@ __global__ void __launch_bounds__(256) k_cg_velocity(VelArgs A)
 // variable-density Poisson operator, absolute stop on sqrt(r.M^-1 r), mean
 // removed at the end.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_cg_pressure(PresArgs A)
+__global__ void __launch_bounds__(512) k_cg_pressure(PresArgs A)
 {
     const Dom &d = A.d;
     const int P = d.P, NX = d.NX, NY = d.NY;
@@ -321,25 +366,46 @@ __global__ void __launch_bounds__(256) k_cg_pressure(PresArgs A)
         AT_(A.res, i, j) = rv;
         double z = rv * AT_(A.M, i, j);
         AT_(A.dir, i, j) = z;
+        AT_(A.z, i, j) = z;
         sg += rv * z;
     }
     put_partial(part0, sg);
     if (!grid_barrier(gs)) return;
-    double gamma = grid_total(part0), gamma_new = 0.0;
+    double gamma = grid_total(part0), gamma_new = 0.0, beta = 0.0;
     if (sqrt(gamma) < A.tol) {
         if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->p_iters = 0; A.scal->p_res = sqrt(gamma); }
         return;
     }
+    double *dcur = A.dir, *dnxt = A.dir2;
+    bool first = true;
     int iters;
     for (iters = 1; iters <= A.maxit; iters++) {
+        // d = z + beta d (z = M r), Ad with the pressure ghost update of d
         double sdad = 0.0;
+        const double bt = beta;
+        const double *dold = dcur;
         for (int q = tid; q < R.n; q += nth) {
             int i, j;
             R.ij(q, i, j);
-            double ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, A.dir, P, NX, NY, a, b); });
+            double dv, ad;
+            if (first) {
+                dv = AT_(dold, i, j);
+                ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, dold, P, NX, NY, a, b); });
+            } else {
+                dv = AT_(A.z, i, j) + bt * AT_(dold, i, j);
+                AT_(dnxt, i, j) = dv;
+                ad = pressure_op(d, A.rho, i, j, [&](int a, int b) {
+                    int si, sj;
+                    double mul;
+                    src_of(A.mp, NX, NY, a, b, si, sj, mul);
+                    return AT_(A.z, si, sj) + bt * AT_(dold, si, sj);
+                });
+            }
             AT_(A.Ad, i, j) = ad;
-            sdad += AT_(A.dir, i, j) * ad;
+            sdad += dv * ad;
         }
+        if (!first) { double *t = dcur; dcur = dnxt; dnxt = t; }
+        first = false;
         put_partial(part1, sdad);
         if (!grid_barrier(gs)) return;
         double alpha = gamma / (grid_total(part1) + 1e-30);
@@ -347,22 +413,18 @@ __global__ void __launch_bounds__(256) k_cg_pressure(PresArgs A)
         for (int q = tid; q < R.n; q += nth) {
             int i, j;
             R.ij(q, i, j);
-            AT_(A.phi, i, j) += alpha * AT_(A.dir, i, j);
+            AT_(A.phi, i, j) += alpha * AT_(dcur, i, j);
             double rv = AT_(A.res, i, j) - alpha * AT_(A.Ad, i, j);
             AT_(A.res, i, j) = rv;
-            sgn += rv * (rv * AT_(A.M, i, j));
+            double z = rv * AT_(A.M, i, j);
+            AT_(A.z, i, j) = z;
+            sgn += rv * z;
         }
         put_partial(part2, sgn);
         if (!grid_barrier(gs)) return;
         gamma_new = grid_total(part2);
         if (sqrt(gamma_new) < A.tol) break;
-        double beta = gamma_new / (gamma + 1e-30);
-        for (int q = tid; q < R.n; q += nth) {
-            int i, j;
-            R.ij(q, i, j);
-            AT_(A.dir, i, j) = AT_(A.res, i, j) * AT_(A.M, i, j) + beta * AT_(A.dir, i, j);
-        }
-        if (!grid_barrier(gs)) return;
+        beta = gamma_new / (gamma + 1e-30);
         gamma = gamma_new;
     }
     // remove the mean (every face Neumann or periodic), psolve_cg.c:255-279

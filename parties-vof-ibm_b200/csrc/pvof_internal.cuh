@@ -58,6 +58,10 @@ struct Metrics {
     const double *idx_u, *idx_c, *dx_c, *dx_u;
     const double *idy_v, *idy_c, *dy_c, *dy_v;
     const double *r_u, *r_c, *inv_r_u, *inv_r_c, *ring_wt_c;
+    // inner-product weights of the physical cells: the measure of the cell
+    // plus the measures of the G-range half cells that copy it (x: times the
+    // ring weight in the axisymmetric mode); cell weight = wx[i] * wy[j] * wz
+    const double *wx, *wy;
 };
 
 struct Dom {
@@ -68,6 +72,7 @@ struct Dom {
     int perx, pery;   // XPERIODIC, YPERIODIC
     int nk;           // planes of the reference's G range in k (2 in 2D)
     double slab;      // dummy_z_slab_thickness
+    double wz;        // slab (planar) or 1 (axisymmetric) in the cell weights
     Metrics m;
 };
 
@@ -78,7 +83,7 @@ enum Scratch {
     SC_PSI = 0, SC_BULK_S, SC_CH_AUX1, SC_CH_RHS_NM1, SC_CH_RES, SC_CH_DIR, SC_CH_DIR2,
     SC_FLUX_X, SC_FLUX_Y, SC_P_RES, SC_P_D, SC_P_AD, SC_P_MINV,
     SC_U_R, SC_U_D, SC_U_AD, SC_U_DIAG, SC_V_R, SC_V_D, SC_V_AD, SC_V_DIAG,
-    SC_OLD, SC_COUNT
+    SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_COUNT
 };
 
 // device-side scalars written by solver kernels and read once per substep
@@ -119,6 +124,7 @@ struct Ctx {
     int stage;
     double dt;
     double time;
+    size_t cgc_smem;         // shared memory of the cluster pressure solver (0: grid solver)
     int coop_blocks;         // co-resident blocks for the persistent solvers
     int coop_threads;
     long long launches;      // kernels launched by this context

@@ -143,8 +143,10 @@ __device__ __forceinline__ void block_partial(double v, double *partials)
     }
 }
 
-// diffuse_bound_liquid_fraction (VOF_DIFFUSE.c:1093-1127); every thread of
-// the launch must reach block_partial, so out-of-range threads add zero.
+// diffuse_bound_liquid_fraction (VOF_DIFFUSE.c:1093-1127) over the G range;
+// the returned mass change counts the physical cells only (the half cells are
+// copies that the ghost update overwrites).  Every thread of the launch must
+// reach block_partial, so out-of-range threads add zero.
 __global__ void k_bound(Dom d, int i0, int i1, int j0, int j1, double *__restrict__ CL, const double *__restrict__ CS,
                         double *__restrict__ CG, double *partials)
 {
@@ -164,11 +166,8 @@ __global__ void k_bound(Dom d, int i0, int i1, int j0, int j1, double *__restric
         AT_(CL, i, j) = new_cl;
         double cg = 1.0 - new_cl - cs;
         AT_(CG, i, j) = cg < 0.0 ? 0.0 : (cg > 1.0 ? 1.0 : cg);
-        if (cs < 0.05) {
-            double m = cell_measure(d, i, j);
-            if (d.nk > 1) m /= (double)d.nk;
-            contrib = (new_cl - old_cl) * m * (double)d.nk;  // every plane of the reference
-        }
+        if (cs < 0.05 && i < d.NX - 1 && j < d.NY - 1)
+            contrib = (new_cl - old_cl) * cell_measure(d, i, j);
     }
     block_partial(contrib, partials);
 }
@@ -434,9 +433,20 @@ __global__ void k_project(Dom d, int i0, int i1, int j0, int j1, int comp, doubl
 __global__ void k_div_max(Dom d, int i0, int i1, int j0, int j1, const double *__restrict__ u,
                           const double *__restrict__ v, unsigned long long *out)
 {
-    KERNEL_2D_INDEX
-    double dc = fabs(cell_div(d, u, v, i, j, d.m.idx_u[i], d.m.idy_v[j]));
-    atomicMax(out, (unsigned long long)__double_as_longlong(dc));
+    const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = j0 + blockIdx.y * blockDim.y + threadIdx.y;
+    double dc = 0.0;
+    if (i < i1 && j < j1) dc = fabs(cell_div(d, u, v, i, j, d.m.idx_u[i], d.m.idy_v[j]));
+    __shared__ double sh[32];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int o = 16; o > 0; o >>= 1) dc = fmax(dc, __shfl_down_sync(0xffffffffu, dc, o));
+    if (lane == 0) sh[warp] = dc;
+    __syncthreads();
+    if (tid == 0) {
+        double m = sh[0];
+        for (int w = 1; w < (int)((blockDim.x * blockDim.y + 31) >> 5); w++) m = fmax(m, sh[w]);
+        atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    }
 }
 
 // liquid mass diagnostic over the physical cells

@@ -25,7 +25,7 @@ struct VelArgs {
     int i0, i1, j0, j1;    // solve range
     double *x;             // velocity component (updated in place)
     const double *rhs, *rho, *mu;
-    double *r, *dir, *Ad, *diag;
+    double *r, *dir, *dir2, *z, *Ad, *diag;
     double iRe, alpha_dt, in_tot, tol;
     int maxit;
     double *partials;
@@ -37,7 +37,7 @@ struct PresArgs {
     BcMap mp;              // Pressure_apply_BCs + exchange
     double *phi;           // deltap
     const double *rhs, *rho, *M;
-    double *res, *dir, *Ad;
+    double *res, *dir, *dir2, *z, *Ad;
     double tol;
     int maxit;
     double *partials;
@@ -83,6 +83,14 @@ __global__ void k_project(Dom d, int i0, int i1, int j0, int j1, int comp, doubl
                           const double *rho, double mdt);
 __global__ void k_div_max(Dom d, int i0, int i1, int j0, int j1, const double *u, const double *v, unsigned long long *out);
 __global__ void k_mass(Dom d, int i0, int i1, int j0, int j1, const double *CL, double *partials);
+
+// cluster-resident pressure solver (pvof_cgc.cu): shared memory it needs for
+// this grid after setting the kernel attributes (0: the grid does not fit one
+// cluster or the cluster cannot be scheduled), and its launch
+constexpr int CGC_CTAS = 16;
+constexpr int CGC_CPT = 8;
+size_t cgc_pressure_setup(int NX, int NY);
+cudaError_t cgc_pressure_launch(const PresArgs &A, size_t smem, cudaStream_t stream);
 
 __global__ void k_cg_biharmonic(BihArgs A);
 __global__ void k_cg_velocity(VelArgs A);

@@ -23,9 +23,17 @@ TIGHT = dict(ch_tol=1e-13, ch_iter_max=600, CG_ETOL=1e-15, CG_MAXIT=400, P_CG_ET
 STATE = ["C_L", "C_G", "RHO", "MU", "CH_RHS_N", "U", "V", "P"]
 
 
-def solver_for(grid, params, planes):
+def solver_for(grid, params, planes, grid_solver=False):
+    """grid_solver=True forces the grid-wide pressure PCG even where the
+    cluster-resident one fits."""
+    import os
     from pvof import runtime
-    g = runtime.Solver(grid, params, device=0)
+    if grid_solver:
+        os.environ["PVOF_NO_CLUSTER_SOLVER"] = "1"
+    try:
+        g = runtime.Solver(grid, params, device=0)
+    finally:
+        os.environ.pop("PVOF_NO_CLUSTER_SOLVER", None)
     g.set_planes(planes)
     g.initialize()
     return g
@@ -155,13 +163,15 @@ def test_solvers_match_oracle_routine_by_routine():
     compare(grid, g.get, o.get_field, ["P", "U", "V"], 1e-12, "Pressure_project_velocity")
 
 
-def test_planar_128x512_one_step_parity():
+@pytest.mark.parametrize("grid_solver", [False, True])
+def test_planar_128x512_one_step_parity(grid_solver):
     """The planar two-phase instability on its full 128x512 grid, one RK3
-    step, solver tolerances near machine precision in both codes."""
+    step, solver tolerances near machine precision in both codes; with the
+    cluster-resident and with the grid-wide pressure solver."""
     from pvof import cases
     kw = dict(TIGHT, P_CG_MAXIT=4000)
     grid, params, planes = cases.rayleigh_taylor(128, 512, Lx=1.0, Ly=4.0, Cn=0.01, **kw)
-    g = solver_for(grid, params, planes)
+    g = solver_for(grid, params, planes, grid_solver=grid_solver)
     o = oracle_for(grid, params, planes)
     sg = g.run_steps(1, 1e-4)
     so = o.run_steps(1, 1e-4)
