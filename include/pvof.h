@@ -241,6 +241,29 @@ int pvof_set_solver_timing(pvof_ctx *ctx, int enabled);
 int pvof_solver_timing(const pvof_ctx *ctx, int solver, double *ms, long long *launches, long long *iterations,
                        long long *cell_iters);
 
+/* --- no-allocation variant (no counterpart in the reference) -------------
+ * The pressure correction solve -- Pressure_compute_preconditioner,
+ * Pressure_solve_cg and the ghost exchange of the correction -- for callers
+ * that cannot allocate device memory (for example a host code that owns a
+ * fixed device pool, or runs where cudaMalloc may not be called).  The
+ * caller passes device planes in the reference's k = 0 plane layout
+ * ((NYM+7) rows of NXM+7 doubles, element (i,j) at (j+3)*(NXM+7) + i+3):
+ * rho with its ghost cells filled, the right-hand side, and phi (the initial
+ * guess on entry, normally zero; the correction on return).  Every temporary
+ * lives in one fixed device array of the library (about 3.7 MB, kept on each
+ * GPU that loads the library until the process exits); the call allocates
+ * nothing.  Limits: (NXM+7)*(NYM+7) <= 72000 and NXM, NYM <= 1024, else
+ * PVOF_EINVAL.  All calls on a device share that array: calls that overlap
+ * on the GPU race and must be serialised by the caller.  The first call on a
+ * device looks up the array's address with that device current; make it
+ * before any stream capture.  stream is a cudaStream_t (NULL: default
+ * stream); the call returns after the solve has finished, with the
+ * iteration count (also the return value) and the final sqrt(r.M^-1 r). */
+int pvof_Pressure_solve_cg_noalloc(const pvof_grid_desc *grid, const pvof_params *params, const double *rho,
+                                   const double *rhs, double *phi, void *stream, int *iterations,
+                                   double *residual);
+const char *pvof_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -112,6 +112,7 @@ EXPORTS = [
     "pvof_initialize",
     "pvof_launch_count", "pvof_timer_start", "pvof_timer_stop", "pvof_flush_l2",
     "pvof_set_solver_timing", "pvof_solver_timing",
+    "pvof_Pressure_solve_cg_noalloc", "pvof_noalloc_last_error",
 ]
 
 SOLVER_BIHARMONIC = 0
