@@ -44,7 +44,6 @@ WORKLOAD = ("planar two-phase instability 128x512 (x periodic, no-slip y), Atwoo
 # algorithmic bytes per cell and solver iteration (x, r, direction read+write,
 # plus the phase field that the coefficients are derived from)
 ALG_BYTES = {0: 48.0, 1: 56.0, 2: 56.0}
-SOLVER_NAMES = {0: "k_cg_biharmonic", 1: "k_cg_velocity", 2: "k_cg_pressure"}
 STATE_FIELDS = ["C_L", "U", "V", "P", "CH_RHS_N", "U_EXPLICIT_OLD", "V_EXPLICIT_OLD",
                 "U_VISC_EXPLICIT_OLD", "V_VISC_EXPLICIT_OLD"]
 
@@ -138,12 +137,12 @@ def measured_peak():
 
 
 def profile_traffic(kernel):
-    """DRAM bytes per cell-iteration of a solver kernel from the committed ncu
-    summary (profiles/ncu_traffic.json), or None."""
+    """DRAM bytes per launch of a solver kernel from the committed ncu capture
+    (profiles/ncu_traffic.json), or None."""
     try:
         with open(os.path.join(REPO, "profiles", "ncu_traffic.json")) as f:
             d = json.load(f)
-        return float(d[kernel]["dram_bytes_per_cell_iter"])
+        return float(d[kernel]["dram_bytes_per_launch"])
     except (OSError, KeyError, ValueError, TypeError):
         return None
 
@@ -228,6 +227,7 @@ def run_ours(args):
     barrier(dist)
     launches = g.launch_count() - l0
     timing = {k: g.solver_timing(k) for k in (0, 1, 2)}
+    names = {k: g.solver_kernel(k) for k in (0, 1, 2)}
     g.set_solver_timing(False)
     t_max = max_over_ranks(dist, total_ms)
     value = ws * cells * args.steps / (t_max * 1e-3)
@@ -264,9 +264,8 @@ def run_ours(args):
     t = timing[dom]
     peak, peak_kind = measured_peak()
     achieved = ALG_BYTES[dom] * t["cell_iters"] / (t["ms"] * 1e-3) / 1e9 if t["ms"] > 0 else 0.0
-    tr = profile_traffic(SOLVER_NAMES[dom])
-    traffic = tr * t["cell_iters"] / max(t["launches"], 1) if tr is not None else None
-    shares = {SOLVER_NAMES[k]: round(timing[k]["ms"] / total_ms, 4) for k in timing}
+    traffic = profile_traffic(names[dom])
+    shares = {names[k]: round(timing[k]["ms"] / total_ms, 4) for k in timing}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -284,12 +283,12 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "grid": "%dx%d" % (NXM, NYM), "cells": cells, "dt": DT,
                        "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "flushed before every timed step (memset of 2x L2, outside the timed intervals)",
-                       "solver_iterations": {SOLVER_NAMES[k]: timing[k]["iterations"] for k in timing},
+                       "solver_iterations": {names[k]: timing[k]["iterations"] for k in timing},
                        "solver_time_share": shares},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps},
             "gpu_launches": launches,
-            "roofline": {"kernel": SOLVER_NAMES[dom], "bound": "hbm", "achieved": achieved, "peak": peak,
+            "roofline": {"kernel": names[dom], "bound": "hbm", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "alg_bytes_per_cell_iter": ALG_BYTES[dom],
                          "avg_launch_ms": t["ms"] / max(t["launches"], 1)},

@@ -240,6 +240,10 @@ int pvof_flush_l2(pvof_ctx *ctx);
 int pvof_set_solver_timing(pvof_ctx *ctx, int enabled);
 int pvof_solver_timing(const pvof_ctx *ctx, int solver, double *ms, long long *launches, long long *iterations,
                        long long *cell_iters);
+/* Name of the kernel that runs solver PVOF_SOLVER_* for this context: the
+ * cluster-resident form when the solve range fits one thread-block cluster,
+ * else the grid-wide persistent form. */
+const char *pvof_solver_kernel(const pvof_ctx *ctx, int solver);
 
 /* --- no-allocation variant (no counterpart in the reference) -------------
  * The pressure correction solve -- Pressure_compute_preconditioner,

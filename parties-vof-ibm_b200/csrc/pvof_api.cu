@@ -232,7 +232,7 @@ int coop_blocks(pvof_ctx *c, int n)
 // Issue one solver launch, bracketed by timing events when enabled.
 // kind: PVOF_SOLVER_*; comp: velocity component (0/1); n: cells solved.
 template <class L>
-int timed_launch(pvof_ctx *c, int kind, int comp, int n, L launch)
+int timed_launch(pvof_ctx *c, int kind, int comp, int n, L launch, int n2 = 0)
 {
     int slot = -1;
     if (c->solver_timing && c->npend < Ctx::NPEND) {
@@ -240,6 +240,7 @@ int timed_launch(pvof_ctx *c, int kind, int comp, int n, L launch)
         c->pend_kind[slot] = kind;
         c->pend_comp[slot] = comp;
         c->pend_cells[slot] = n;
+        c->pend_cells2[slot] = n2;
         CK(cudaEventRecord(c->pend_ev[slot][0], c->stream));
     }
     CK(launch());
@@ -266,11 +267,15 @@ void collect_solver_timing(pvof_ctx *c)
     for (int q = 0; q < c->npend; q++) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, c->pend_ev[q][0], c->pend_ev[q][1]) != cudaSuccess) continue;
-        int k = c->pend_kind[q];
-        long long it = k == PVOF_SOLVER_BIHARMONIC ? h.ch_iters
-                     : (k == PVOF_SOLVER_VELOCITY ? h.vel_iters[c->pend_comp[q]] : h.p_iters);
+        int k = c->pend_kind[q], comp = c->pend_comp[q];
         c->sol_ms[k] += ms;
         c->sol_launches[k] += 1;
+        if (k == PVOF_SOLVER_VELOCITY && comp == 2) {   // both components in one launch
+            c->sol_iters[k] += (long long)h.vel_iters[0] + h.vel_iters[1];
+            c->sol_cell_iters[k] += h.vel_iters[0] * c->pend_cells[q] + h.vel_iters[1] * c->pend_cells2[q];
+            continue;
+        }
+        long long it = k == PVOF_SOLVER_BIHARMONIC ? h.ch_iters : (k == PVOF_SOLVER_VELOCITY ? h.vel_iters[comp] : h.p_iters);
         c->sol_iters[k] += it;
         c->sol_cell_iters[k] += it * c->pend_cells[q];
     }
@@ -513,7 +518,7 @@ int set_rhs(pvof_ctx *c, int comp)
                     F(c, PVOF_F_V_VISC_EXPLICIT_OLD), (const double *)F(c, PVOF_F_V_IMPLICIT), a_dt, s, -c->p.dp_dx);
 }
 
-int velocity_solve(pvof_ctx *c, int comp)
+VelArgs vel_args(pvof_ctx *c, int comp)
 {
     VelArgs A;
     A.d = c->dom;
@@ -540,7 +545,34 @@ int velocity_solve(pvof_ctx *c, int comp)
     A.maxit = c->p.CG_MAXIT;
     A.partials = c->partials;
     A.scal = c->scal;
-    return coop_launch(c, (const void *)k_cg_velocity, A, (A.i1 - A.i0) * (A.j1 - A.j0), PVOF_SOLVER_VELOCITY, comp);
+    return A;
+}
+
+// Velocity_solve_cg (msolve_cg.c:525-722) for one component
+int velocity_solve(pvof_ctx *c, int comp)
+{
+    VelPair V;
+    V.c[0] = vel_args(c, comp);
+    const int n = (V.c[0].i1 - V.c[0].i0) * (V.c[0].j1 - V.c[0].j0);
+    if (c->cgs_v_smem)
+        return timed_launch(c, PVOF_SOLVER_VELOCITY, comp, n,
+                            [&]() { return cgs_velocity_launch(V, 1, StripPlan{c->cgs_v_smem, c->cgs_v_threads}, c->stream); });
+    return coop_launch(c, (const void *)k_cg_velocity, V.c[0], n, PVOF_SOLVER_VELOCITY, comp);
+}
+
+// both components: one launch of two clusters when the ranges fit, else in turn
+int velocity_solve_both(pvof_ctx *c)
+{
+    if (!c->cgs_v_smem) {
+        TRY(velocity_solve(c, 0));
+        return velocity_solve(c, 1);
+    }
+    VelPair V;
+    V.c[0] = vel_args(c, 0);
+    V.c[1] = vel_args(c, 1);
+    const int n0 = (V.c[0].i1 - V.c[0].i0) * (V.c[0].j1 - V.c[0].j0);
+    const int n1 = (V.c[1].i1 - V.c[1].i0) * (V.c[1].j1 - V.c[1].j0);
+    return timed_launch(c, PVOF_SOLVER_VELOCITY, 2, n0, [&]() { return cgs_velocity_launch(V, 2, StripPlan{c->cgs_v_smem, c->cgs_v_threads}, c->stream); }, n1);
 }
 
 }  // namespace
@@ -590,8 +622,8 @@ int p_solve(pvof_ctx *c)
     A.partials = c->partials;
     A.scal = c->scal;
     const int n = (c->dom.NX - 1) * (c->dom.NY - 1);
-    if (c->cgc_smem)
-        TRY(timed_launch(c, PVOF_SOLVER_PRESSURE, 0, n, [&]() { return cgc_pressure_launch(A, c->cgc_smem, c->stream); }));
+    if (c->cgs_p_smem)
+        TRY(timed_launch(c, PVOF_SOLVER_PRESSURE, 0, n, [&]() { return cgs_pressure_launch(A, StripPlan{c->cgs_p_smem, c->cgs_p_threads}, c->stream); }));
     else
         TRY(coop_launch(c, (const void *)k_cg_pressure, A, n, PVOF_SOLVER_PRESSURE, 0));
     return fill(c, BK_WRAP_C, F(c, PVOF_F_DELTAP));
@@ -685,8 +717,7 @@ int substep(pvof_ctx *c, pvof_stats *st)
         TRY(apply_f_sigma_old(c));
     }
     if (c->p.gravity) TRY(add_gravity(c));
-    TRY(velocity_solve(c, 0));
-    TRY(velocity_solve(c, 1));
+    TRY(velocity_solve_both(c));
     TRY(fill(c, BK_U, F(c, PVOF_F_U)));
     TRY(fill(c, BK_V, F(c, PVOF_F_V)));
     int passes = 0, p_total = 0;
@@ -808,10 +839,13 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     std::vector<double> muls;
     std::vector<size_t> offx(BK_COUNT), offy(BK_COUNT);
     bool axis_lo = d.axisym;
+    std::vector<HostMap> hmaps(BK_COUNT);
     for (int k = 0; k < BK_COUNT; k++) {
         Map1 mx, my;
         axis_map(mx, k, d.NX, d.perx, grid->wall[PVOF_LEFT], grid->wall[PVOF_RIGHT], axis_lo, true, true);
         axis_map(my, k, d.NY, d.pery, grid->wall[PVOF_BOTTOM], grid->wall[PVOF_TOP], false, false, false);
+        hmaps[k].xsrc = mx.src; hmaps[k].xmul = mx.mul;
+        hmaps[k].ysrc = my.src; hmaps[k].ymul = my.mul;
         offx[k] = srcs.size();
         srcs.insert(srcs.end(), mx.src.begin(), mx.src.end());
         muls.insert(muls.end(), mx.mul.begin(), mx.mul.end());
@@ -844,7 +878,18 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     c->coop_blocks = ob * nsm;
     c->coop_threads = COOP_THREADS;
     // cluster-resident pressure solver when the grid fits one cluster
-    c->cgc_smem = getenv("PVOF_NO_CLUSTER_SOLVER") ? 0 : cgc_pressure_setup(d.NX, d.NY);
+    // cluster-resident solvers when the solve ranges fit one cluster
+    if (!getenv("PVOF_NO_CLUSTER_SOLVER")) {
+        StripPlan pp = cgs_pressure_setup(d.NX, d.NY, d.axisym, hmaps[BK_PRESSURE]);
+        c->cgs_p_smem = pp.smem;
+        c->cgs_p_threads = pp.threads;
+        int ru[4], rv[4];
+        u_range(c, ru[0], ru[1], ru[2], ru[3]);
+        v_range(c, rv[0], rv[1], rv[2], rv[3]);
+        StripPlan vp = cgs_velocity_setup(ru, hmaps[BK_U_CG], rv, hmaps[BK_V_CG], d.axisym);
+        c->cgs_v_smem = vp.smem;
+        c->cgs_v_threads = vp.threads;
+    }
     size_t npart = 4 * (size_t)std::max(c->coop_blocks, (int)(((d.NX + TBX - 1) / TBX) * ((d.NY + TBY - 1) / TBY)));
     if (cudaMalloc(&c->partials, npart * sizeof(double)) != cudaSuccess) return fail(PVOF_ENOMEM, "cudaMalloc partials");
     if (cudaMalloc(&c->scal, sizeof(DevScalars)) != cudaSuccess) return fail(PVOF_ENOMEM, "cudaMalloc scalars");
@@ -1118,6 +1163,17 @@ int pvof_set_solver_timing(pvof_ctx *c, int enabled)
     }
     c->npend = 0;
     return PVOF_OK;
+}
+
+const char *pvof_solver_kernel(const pvof_ctx *c, int solver)
+{
+    if (!c) return "";
+    switch (solver) {
+    case PVOF_SOLVER_BIHARMONIC: return "k_cg_biharmonic";
+    case PVOF_SOLVER_VELOCITY: return c->cgs_v_smem ? "k_cgs_velocity" : "k_cg_velocity";
+    case PVOF_SOLVER_PRESSURE: return c->cgs_p_smem ? "k_cgs_pressure" : "k_cg_pressure";
+    default: return "";
+    }
 }
 
 int pvof_solver_timing(const pvof_ctx *c, int solver, double *ms, long long *launches, long long *iterations,

@@ -124,7 +124,9 @@ struct Ctx {
     int stage;
     double dt;
     double time;
-    size_t cgc_smem;         // shared memory of the cluster pressure solver (0: grid solver)
+    size_t cgs_p_smem;       // shared memory of the cluster pressure solver (0: grid solver)
+    size_t cgs_v_smem;       // same, velocity solver for both components (0: grid solver)
+    int cgs_p_threads, cgs_v_threads;   // their threads per CTA
     int coop_blocks;         // co-resident blocks for the persistent solvers
     int coop_threads;
     long long launches;      // kernels launched by this context
@@ -136,7 +138,7 @@ struct Ctx {
     static constexpr int NPEND = 16;
     cudaEvent_t pend_ev[NPEND][2];
     int pend_kind[NPEND], pend_comp[NPEND];
-    long long pend_cells[NPEND];
+    long long pend_cells[NPEND], pend_cells2[NPEND];
     int npend;
     double sol_ms[3];
     long long sol_launches[3], sol_iters[3], sol_cell_iters[3];

@@ -2,6 +2,8 @@
 // host orchestration.
 #pragma once
 
+#include <vector>
+
 #include "pvof_internal.cuh"
 
 namespace pvof {
@@ -84,13 +86,35 @@ __global__ void k_project(Dom d, int i0, int i1, int j0, int j1, int comp, doubl
 __global__ void k_div_max(Dom d, int i0, int i1, int j0, int j1, const double *u, const double *v, unsigned long long *out);
 __global__ void k_mass(Dom d, int i0, int i1, int j0, int j1, const double *CL, double *partials);
 
-// cluster-resident pressure solver (pvof_cgc.cu): shared memory it needs for
-// this grid after setting the kernel attributes (0: the grid does not fit one
-// cluster or the cluster cannot be scheduled), and its launch
-constexpr int CGC_CTAS = 16;
-constexpr int CGC_CPT = 8;
-size_t cgc_pressure_setup(int NX, int NY);
-cudaError_t cgc_pressure_launch(const PresArgs &A, size_t smem, cudaStream_t stream);
+// Cluster-resident solvers (pvof_cgs.cu).  The setup functions return the
+// shared memory a solve range needs after setting the kernel attributes, or 0
+// when the range does not fit one cluster, its ghost maps do not have the
+// shape the strip layout assumes, or the cluster cannot be scheduled.
+constexpr int CGC_CTAS = 16;   // CTAs per cluster
+
+// host copy of one ghost-update kind: entry [i + NG] for i in [-NG, N + NG)
+struct HostMap {
+    std::vector<int> xsrc, ysrc;
+    std::vector<double> xmul, ymul;
+};
+
+// the two velocity components of one launch: cluster q solves c[q]
+struct VelPair {
+    VelArgs c[2];
+};
+
+// launch shape of a strip solver: threads per CTA (0: the range does not fit)
+// and dynamic shared memory
+struct StripPlan {
+    size_t smem;
+    int threads;
+};
+
+StripPlan cgs_pressure_setup(int NX, int NY, int axisym, const HostMap &mp);
+cudaError_t cgs_pressure_launch(const PresArgs &A, const StripPlan &plan, cudaStream_t stream);
+// ranges {i0, i1, j0, j1} of u and v; one plan serves both
+StripPlan cgs_velocity_setup(const int ru[4], const HostMap &mu, const int rv[4], const HostMap &mv, int axisym);
+cudaError_t cgs_velocity_launch(const VelPair &V, int ncomp, const StripPlan &plan, cudaStream_t stream);
 
 __global__ void k_cg_biharmonic(BihArgs A);
 __global__ void k_cg_velocity(VelArgs A);

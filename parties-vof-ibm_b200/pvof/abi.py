@@ -111,7 +111,7 @@ EXPORTS = [
     "pvof_substep", "pvof_run_steps", "pvof_liquid_mass",
     "pvof_initialize",
     "pvof_launch_count", "pvof_timer_start", "pvof_timer_stop", "pvof_flush_l2",
-    "pvof_set_solver_timing", "pvof_solver_timing",
+    "pvof_set_solver_timing", "pvof_solver_timing", "pvof_solver_kernel",
     "pvof_Pressure_solve_cg_noalloc", "pvof_noalloc_last_error",
 ]
 

@@ -65,6 +65,8 @@ def load():
     L.pvof_flush_l2.argtypes = [V]
     L.pvof_set_solver_timing.argtypes = [V, C.c_int]
     L.pvof_solver_timing.argtypes = [V, C.c_int, P(C.c_double), P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]
+    L.pvof_solver_kernel.argtypes = [V, C.c_int]
+    L.pvof_solver_kernel.restype = C.c_char_p
     _lib = L
     return L
 
@@ -168,6 +170,10 @@ class Solver:
 
     def set_solver_timing(self, on):
         check(load().pvof_set_solver_timing(self.h, 1 if on else 0), "pvof_set_solver_timing")
+
+    def solver_kernel(self, solver):
+        """Name of the kernel that runs solver abi.SOLVER_* in this context."""
+        return load().pvof_solver_kernel(self.h, solver).decode()
 
     def solver_timing(self, solver):
         ms, nl, it, ci = C.c_double(), C.c_longlong(), C.c_longlong(), C.c_longlong()
