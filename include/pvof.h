@@ -218,6 +218,44 @@ int pvof_run_steps(pvof_ctx *ctx, int nsteps, double dt, pvof_stats *stats);
  * VOF_DIFFUSE.c:1071-1091), computed on the device in FP64. */
 int pvof_liquid_mass(pvof_ctx *ctx, double *mass);
 
+/* --- resolved solid particles (planar mode) ------------------------------
+ * The reference keeps particles in two linked lists (p_mobile, p_fixed,
+ * PARTIES/src/Include/DataTypes.h:1327-1527) read from p_mobile.inp /
+ * p_fixed.inp.  Here the caller passes the owned particles once; the library
+ * derives markers, masses and the periodic copies itself. */
+typedef struct pvof_particle {
+    int mobile;         /* 1: mobile list, 0: fixed list */
+    double X[2];        /* centre (x, y) */
+    double R;           /* radius */
+    double U[2];        /* translational velocity */
+    double Omega_z;     /* spin about z */
+    double rho_s;       /* solid density ([particle] rho_s) */
+} pvof_particle;
+
+/* Replaces the particle lists; IDs as Particle_initialize assigns them (fixed
+ * first, then mobile; Lagrangian/Particle.c:213-221). */
+int pvof_set_particles(pvof_ctx *ctx, const pvof_particle *particles, int n);
+/* Particle_MPI_update of both lists on one rank (periodic copies) and
+ * Lagrangian_flag_points (Lagrangian/Lagrangian.c:2515-2627): markers of
+ * every list entry near the domain and their on/off flags. */
+int pvof_Lagrangian_flag_points(pvof_ctx *ctx);
+/* number of list entries after the last update (owned particles and copies,
+ * mobile list first) */
+int pvof_particle_entries(pvof_ctx *ctx);
+/* F and T (3 doubles per entry each) accumulated by pvof_Lagrangian_force */
+int pvof_particle_forces(pvof_ctx *ctx, double *F, double *T, int max_entries);
+/* markers of one entry: positions, control volumes, flags; returns the count */
+int pvof_particle_markers(pvof_ctx *ctx, int entry, double *x, double *y, double *vol, int *flag, int max_markers);
+/* Eulerian/VOF_DIFFUSE.c:685-813 VOF_DIFFUSE_compute_C_S: solid fraction, then
+ * the clamp of C_L and the phase cache */
+int pvof_VOF_DIFFUSE_compute_C_S(pvof_ctx *ctx);
+/* Eulerian/lsolver/msolve_direct.c:146-260 Velocity_solve_explicit (u or v) */
+int pvof_Velocity_solve_explicit(pvof_ctx *ctx, char component);
+/* Lagrangian/Lagrangian.c:1724-1871 Lagrangian_force: force_iter < 0 is the
+ * predictor on the momentum RHS, force_iter >= 0 that many corrector passes on
+ * the velocity; call pvof_Lagrangian_flag_points() first */
+int pvof_Lagrangian_force(pvof_ctx *ctx, int force_iter);
+
 /* --- measurement (no counterpart in the reference) ---------------------- */
 /* Number of CUDA kernels this context has launched so far. */
 long long pvof_launch_count(const pvof_ctx *ctx);

@@ -196,6 +196,42 @@ def run_reference(case, workdir, grid, params, planes, nsteps, dt, dump_every=1,
     return subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=timeout)
 
 
+def run_reference_ibm(workdir, grid, params, planes, fixed, mobile, dt, stage, case="ibm2d", timeout=600):
+    """Run the immersed-boundary routine driver (oracle/ref/ibm_driver.c) of
+    the reference build ``case``: particles are rows (X, Y, R, U, V, Omega_z)."""
+    os.makedirs(workdir, exist_ok=True)
+    write_parties_inp(os.path.join(workdir, "parties.inp"), grid, params)
+    names = {"F": "init_C.bin", "U": "init_u.bin", "V": "init_v.bin", "P": "init_p.bin"}
+    for k, fn in names.items():
+        if k in planes:
+            np.ascontiguousarray(planes[k], dtype="<f8").tofile(os.path.join(workdir, fn))
+    for fn, rows in (("particles_fixed.txt", fixed), ("particles_mobile.txt", mobile)):
+        with open(os.path.join(workdir, fn), "w") as f:
+            for r in rows:
+                f.write(" ".join("%.17g" % float(x) for x in r) + "\n")
+    cmd = [ref_binary(case), workdir, repr(float(dt)), str(int(stage))]
+    return subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=timeout)
+
+
+def read_reference_markers(workdir):
+    """Markers dumped by the routine driver: one (X_L, Y_L, Vol_L, flag) tuple
+    of arrays per list entry (mobile list first, then fixed)."""
+    a = np.fromfile(os.path.join(workdir, "out", "markers.bin"), dtype="<f8")
+    out, q = [], 0
+    while q < a.size:
+        n = int(a[q]); q += 1
+        xs = a[q:q + n]; ys = a[q + n:q + 2 * n]; vol = a[q + 2 * n:q + 3 * n]; fl = a[q + 3 * n:q + 4 * n]
+        q += 4 * n
+        out.append((xs, ys, vol, fl))
+    return out
+
+
+def read_reference_particles(workdir, tag):
+    """Per list entry F and T dumped by the routine driver, (n, 3) each."""
+    a = np.loadtxt(os.path.join(workdir, "out", "particles_%s.txt" % tag), ndmin=2)
+    return a[:, 0:3], a[:, 3:6]
+
+
 def read_reference_field(workdir, tag, name, grid, ng=False):
     """k = 0 plane of a dumped field (full ghosted plane for flow fields)."""
     a = np.fromfile(os.path.join(workdir, "out", "%s_%s.bin" % (tag, name)), dtype="<f8")

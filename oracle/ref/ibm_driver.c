@@ -1,0 +1,248 @@
+/*
+ * Oracle driver for the immersed-boundary routines of the reference, built
+ * from the reference's own sources with the resolved-particle flags
+ * (cfg/ibm2d.h: VOF_IBM, LAG_PARTICLE_RESOLVED).  It reuses the start-up of
+ * ref_driver.c, reads the particle lists through the reference's
+ * Particle_initialize (with the file reader below), and then calls, one by
+ * one and in the order of Temporal_int_all_the_equations
+ * (PARTIES/src/Temporal_int.c:948-1016), the routines of the IBM part of a
+ * substep, dumping their inputs and outputs:
+ *
+ *   i0   after start-up: C_S (VOF_DIFFUSE_compute_C_S inside VOF_DIFFUSE_init),
+ *        C_L, C_G, rho, mu, u, v
+ *   markers.bin  Particle_MPI_update of both lists and Lagrangian_flag_points,
+ *        as at the start of a substep: per particle (mobile list, then
+ *        fixed list) N_L_local, X_L, Y_L, Vol_L_marker, flag_L as doubles
+ *   r0   momentum RHS before the IBM (set_implicit_explicit, set_RHS, gravity)
+ *   r1   Velocity_solve_explicit of u and v (+ boundary update)
+ *   r2   Lagrangian_force(-1): RHS, particle F and T (particles_r2.txt)
+ *   r3   Velocity_solve (Jacobi-PCG) of u and v (+ boundary update)
+ *   r4   Lagrangian_force(N_forcing_loops) (+ boundary update): u, v, RHS,
+ *        particle F and T (particles_r4.txt)
+ *
+ * Usage: ibm_driver <case_dir> <dt> <stage>
+ *   files of ref_driver.c, plus particles_fixed.txt and particles_mobile.txt:
+ *   one particle per line, "X Y R U V Omega_z".
+ * Test infrastructure only.
+ */
+#define main ref_driver_main
+#include "ref_driver.c"
+#undef main
+
+#include "Lagrangian.h"
+#include "Particle.h"
+#include "ParticleInput.h"
+
+/*
+ * Particle file reader in place of the reference's ParticleInput_inp
+ * (PARTIES/src/IO/ParticleInput.c:24-334, whose translation unit needs HDF5):
+ * the same per-particle set-up -- in-plane position with z on the storage
+ * plane, identity rotation, Particle_initialize_nonessential_data,
+ * Particle_calc_derived_data, Particle_create_internal_arrays -- except that
+ * the velocities come from the file instead of zero.
+ */
+void ParticleInput_inp(Particle_list *p_list, MAC_grid *grid, Parameters *params, Debug_trace *dtrace)
+{
+    (void)dtrace;
+    const char *name = (p_list->type == FIXED) ? "particles_fixed.txt" : "particles_mobile.txt";
+    p_list->start = NULL;
+    p_list->Np = 0;
+    p_list->state = LIST_STATE_LOCAL;
+    FILE *f = fopen(name, "r");
+    if (!f) return;
+    Particle *last = NULL;
+    double x, y, r, u, v, om;
+    int n = 0;
+    while (fscanf(f, "%lf %lf %lf %lf %lf %lf", &x, &y, &r, &u, &v, &om) == 6) {
+        Particle *p = (Particle *)calloc(1, sizeof(Particle));
+        p->X[0] = x;
+        p->X[1] = y;
+        p->X[2] = grid->zc[grid->G_Ks];
+        p->R = r;
+        p->ID = n + p_list->ID_start;
+        p->U[0] = u;
+        p->U[1] = v;
+        p->Omega[2] = om;
+        p->Rotn[0][0] = p->Rotn[1][1] = p->Rotn[2][2] = 1.0;
+        p->particle_collision = NULL;
+        p->wall_collision = NULL;
+        Particle_initialize_nonessential_data(p);
+        Particle_calc_derived_data(p, grid, params);
+        Particle_create_internal_arrays(p);
+        p->next = NULL;
+        if (last) last->next = p;
+        else p_list->start = p;
+        last = p;
+        n++;
+    }
+    fclose(f);
+    p_list->Np = n;
+}
+
+static void dump_markers(Cart3d_bag *db)
+{
+    FILE *f = fopen("out/markers.bin", "wb");
+    if (!f) die("cannot open markers.bin");
+    Particle_list *lists[2] = {db->lag->p_mobile_list, db->lag->p_fixed_list};
+    for (int l = 0; l < 2; l++) {
+        for (Particle *p = lists[l]->start; p; p = p->next) {
+            double n = (double)p->N_L_local;
+            fwrite(&n, sizeof(double), 1, f);
+            fwrite(p->X_L, sizeof(double), (size_t)p->N_L_local, f);
+            fwrite(p->Y_L, sizeof(double), (size_t)p->N_L_local, f);
+            fwrite(p->Vol_L_marker, sizeof(double), (size_t)p->N_L_local, f);
+            for (int m = 0; m < p->N_L_local; m++) {
+                double fl = (double)p->flag_L[m];
+                fwrite(&fl, sizeof(double), 1, f);
+            }
+        }
+    }
+    fclose(f);
+}
+
+static void dump_particles(Cart3d_bag *db, const char *tag)
+{
+    char path[256];
+    snprintf(path, sizeof(path), "out/particles_%s.txt", tag);
+    FILE *f = fopen(path, "w");
+    if (!f) die("cannot open a particle output file");
+    Particle_list *lists[2] = {db->lag->p_mobile_list, db->lag->p_fixed_list};
+    for (int l = 0; l < 2; l++)
+        for (Particle *p = lists[l]->start; p; p = p->next)
+            fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g\n", p->F[0], p->F[1], p->F[2], p->T[0], p->T[1], p->T[2]);
+    fclose(f);
+}
+
+static void dump_fields(Cart3d_bag *db, const char *tag, int rhs)
+{
+    MAC_grid *g = db->grid;
+    char path[512];
+#define D(arr, name) do { snprintf(path, sizeof(path), "out/%s_%s.bin", tag, name); dump(arr, g, path); } while (0)
+#define DN(arr, name) do { snprintf(path, sizeof(path), "out/%s_%s.bin", tag, name); dump_ng(arr, g, path); } while (0)
+    D(db->u->data, "u");
+    D(db->v->data, "v");
+    if (rhs) {
+        DN(db->u->ng_rhs, "u_rhs");
+        DN(db->v->ng_rhs, "v_rhs");
+        DN(db->u->ng_implicit, "u_implicit");
+        DN(db->v->ng_implicit, "v_implicit");
+    }
+#undef D
+#undef DN
+}
+
+int main(int argc, char **argv)
+{
+    if (argc < 4) die("usage: ibm_driver <case_dir> <dt> <stage>");
+    const char *case_dir = argv[1];
+    double dt = atof(argv[2]);
+    int stage = atoi(argv[3]);
+    if (chdir(case_dir) != 0) die("cannot enter the case directory");
+    mkdir("out", 0755);
+
+    MPI_Init(&argc, &argv);
+    Debug_trace dtrace_parent = {"", "", 0, NULL, NULL};
+    Debug_trace *dtrace = &dtrace_parent;
+
+    Cart3d_bag *db = (Cart3d_bag *)calloc(1, sizeof(Cart3d_bag));
+    Parameters *params = (Parameters *)calloc(1, sizeof(Parameters));
+    params->size = 1;
+    params->rank = 0;
+    Input_set_parameters(params, PARTIES_INPUT_FILE);
+    db->params = params;
+
+    MAC_grid *grid = Grid_create(params, DTRACE("Grid_create"));
+    db->grid = grid;
+    Communication_new_xyz_communicator(grid, params);
+    db->timer = Timer_create(grid, params);
+    db->u = Velocity_create(grid, params, 'u', DTRACE("Velocity_create"));
+    db->v = Velocity_create(grid, params, 'v', DTRACE("Velocity_create"));
+    db->w = Velocity_create(grid, params, 'w', DTRACE("Velocity_create"));
+    db->p = Pressure_create(grid, params);
+    db->vof = VoF_create(grid, params);
+    db->lag = Lagrangian_create(grid, params);
+
+    int NX = grid->NX, NY = grid->NY;
+    double *plane;
+    if (!(plane = read_plane("init_C.bin", NX * NY))) die("missing init_C.bin");
+    inject(db->vof->F, plane, grid);
+    free(plane);
+    if ((plane = read_plane("init_u.bin", NX * NY))) { inject(db->u->data, plane, grid); free(plane); }
+    if ((plane = read_plane("init_v.bin", NX * NY))) { inject(db->v->data, plane, grid); free(plane); }
+    if ((plane = read_plane("init_p.bin", NX * NY))) { inject(db->p->p_data, plane, grid); free(plane); }
+
+    Velocity_update_boundaries(db->u->data, 'u', VEL_TYPE_NORMAL, db);
+    Velocity_update_boundaries(db->v->data, 'v', VEL_TYPE_NORMAL, db);
+    Velocity_update_boundaries(db->w->data, 'w', VEL_TYPE_NORMAL, db);
+    Pressure_apply_BCs(db->p->p_data, grid, params);
+    Communication_update_ghost_nodes_flow_variable(db->p->p_data, CONCENTRATION_PERTURBATION, 3, db);
+
+    /* particles before VOF_DIFFUSE_init, as Cart3d.c:488-496 does */
+    params->which_stage = 0;
+    params->dt = dt;
+    Particle_initialize(db, DTRACE("Particle_initialize"));
+    VOF_DIFFUSE_set_boundary_values(db->vof->F, db);
+    VOF_DIFFUSE_init(db);
+    VOF_update_density_viscosity(db);
+    Velocity_cell_center(db);
+
+    {
+        char path[512];
+#define D(arr, name) do { snprintf(path, sizeof(path), "out/i0_%s.bin", name); dump(arr, grid, path); } while (0)
+        D(db->vof->C_S, "C_S");
+        D(db->vof->C_L, "C_L");
+        D(db->vof->C_G, "C_G");
+        D(db->vof->rho, "rho");
+        D(db->vof->mu, "mu");
+        D(db->u->data, "u");
+        D(db->v->data, "v");
+#undef D
+    }
+
+    params->which_stage = stage;
+    params->dt = dt;
+    /* the list updates and marker flags at the start of a substep (Temporal_int.c:678-681) */
+    Particle_MPI_update(db->lag->p_mobile_list, db, DTRACE("Particle_MPI_update"));
+    Particle_MPI_update(db->lag->p_fixed_list, db, DTRACE("Particle_MPI_update"));
+    Lagrangian_flag_points(db, DTRACE("Lagrangian_flag_points"));
+    dump_markers(db);
+
+    Velocity_u_set_implicit_explicit(db);
+    Velocity_v_set_implicit_explicit(db);
+    Velocity_u_set_RHS(db);
+    Velocity_v_set_RHS(db);
+    Velocity_w_set_RHS(db);
+#ifdef VOF_GRAVITY
+    Velocity_add_gravity_2_RHS(db);
+#endif
+    dump_fields(db, "r0", 1);
+
+    Velocity_solve_explicit(db->u, db);
+    Velocity_solve_explicit(db->v, db);
+    Velocity_solve_explicit(db->w, db);
+    Velocity_update_boundaries(db->u->data, 'u', VEL_TYPE_NORMAL, db);
+    Velocity_update_boundaries(db->v->data, 'v', VEL_TYPE_NORMAL, db);
+    Velocity_update_boundaries(db->w->data, 'w', VEL_TYPE_NORMAL, db);
+    dump_fields(db, "r1", 0);
+
+    Lagrangian_force(-1, db, DTRACE("Lagrangian_force"));
+    dump_fields(db, "r2", 1);
+    dump_particles(db, "r2");
+
+    Velocity_solve(db->u, db);
+    Velocity_solve(db->v, db);
+    Velocity_solve(db->w, db);
+    Velocity_update_boundaries(db->u->data, 'u', VEL_TYPE_NORMAL, db);
+    Velocity_update_boundaries(db->v->data, 'v', VEL_TYPE_NORMAL, db);
+    Velocity_update_boundaries(db->w->data, 'w', VEL_TYPE_NORMAL, db);
+    dump_fields(db, "r3", 0);
+
+    Lagrangian_force(params->N_forcing_loops, db, DTRACE("Lagrangian_force"));
+    Velocity_update_boundaries(db->u->data, 'u', VEL_TYPE_NORMAL, db);
+    Velocity_update_boundaries(db->v->data, 'v', VEL_TYPE_NORMAL, db);
+    Velocity_update_boundaries(db->w->data, 'w', VEL_TYPE_NORMAL, db);
+    dump_fields(db, "r4", 1);
+    dump_particles(db, "r4");
+    printf("IBM_DONE N_forcing_loops=%d\n", params->N_forcing_loops);
+    return 0;
+}

@@ -745,6 +745,274 @@ int substep(pvof_ctx *c, pvof_stats *st)
     return rc;
 }
 
+// ---------------------------------------------------------------------------
+// resolved solid particles (kernels and list bookkeeping in pvof_ibm.cu)
+// ---------------------------------------------------------------------------
+}  // namespace
+
+struct pvof::IbmState {
+    std::vector<IbmEntry> mobile, fixed;   // owned particles, in list order
+    std::vector<IbmEntry> entries;         // lists after the last update (mobile, then fixed)
+    IbmMarkers markers;
+    HostMetrics hm;
+    IbmGrid grid;
+    double *d_coord = nullptr;             // xu, xc, yv, yc, each offset by NG
+    const double *xu = nullptr, *xc = nullptr, *yv = nullptr, *yc = nullptr;
+    IbmEntryDev *d_ent = nullptr;
+    size_t cap_ent = 0;
+    double *d_mk = nullptr;                // XL, YL, vol, UL, rhoL, FL
+    int *d_flag = nullptr;
+    size_t cap_mk = 0;
+    double *d_FT = nullptr;
+    double *d_geo = nullptr;
+    size_t cap_geo = 0;
+    int ngeo = 0;
+    bool flagged = false;
+    ~IbmState()
+    {
+        cudaFree(d_coord);
+        cudaFree(d_ent);
+        cudaFree(d_mk);
+        cudaFree(d_flag);
+        cudaFree(d_FT);
+        cudaFree(d_geo);
+    }
+};
+
+namespace {
+
+int ibm_state(pvof_ctx *c, IbmState **out)
+{
+    if (!c->dom.planar) return set_err(PVOF_EINVAL, "resolved particles are built for the planar mode only");
+    if (c->ibm) { *out = c->ibm; return PVOF_OK; }
+    IbmState *s = new IbmState();
+    build_metrics(c->g, c->dom.NX, c->dom.NY, s->hm);
+    const size_t nx = s->hm.xu.size(), ny = s->hm.yv.size();
+    if (cudaMalloc(&s->d_coord, (2 * nx + 2 * ny) * sizeof(double)) != cudaSuccess) {
+        delete s;
+        return set_err(PVOF_ENOMEM, "cudaMalloc particle coordinates");
+    }
+    std::vector<double> h;
+    for (auto *v : {&s->hm.xu, &s->hm.xc, &s->hm.yv, &s->hm.yc}) h.insert(h.end(), v->begin(), v->end());
+    CK(cudaMemcpy(s->d_coord, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    s->xu = s->d_coord + NG;
+    s->xc = s->d_coord + nx + NG;
+    s->yv = s->d_coord + 2 * nx + NG;
+    s->yc = s->d_coord + 2 * nx + ny + NG;
+    IbmGrid &g = s->grid;
+    g.NX = c->dom.NX;
+    g.NY = c->dom.NY;
+    g.periodic[0] = c->dom.perx;
+    g.periodic[1] = c->dom.pery;
+    g.xu = s->hm.xu.data() + NG;
+    g.yv = s->hm.yv.data() + NG;
+    g.h = s->hm.dx_u[1 + NG];
+    double dymin = s->hm.dy_v[NG];
+    for (int j = 0; j < c->dom.NY; j++) dymin = std::min(dymin, s->hm.dy_v[j + NG]);
+    g.dy_min = dymin;
+    g.slab = c->dom.slab;
+    g.twod_slab = c->g.slab_thickness;
+    g.Lx = c->g.xmax - c->g.xmin;
+    g.Ly = c->g.ymax - c->g.ymin;
+    c->ibm = s;
+    *out = s;
+    return PVOF_OK;
+}
+
+// Particle_MPI_update of both lists and Lagrangian_flag_points (Temporal_int.c:678-681)
+int ibm_flag_points(pvof_ctx *c)
+{
+    IbmState *s;
+    TRY(ibm_state(c, &s));
+    ibm_build(s->mobile, s->fixed, s->grid, c->p.Cn, s->entries, s->markers);
+    const size_t ne = s->entries.size(), nm = s->markers.x.size();
+    if (ne > s->cap_ent) {
+        cudaFree(s->d_ent);
+        cudaFree(s->d_FT);
+        s->d_ent = nullptr;
+        s->d_FT = nullptr;
+        if (cudaMalloc(&s->d_ent, ne * sizeof(IbmEntryDev)) != cudaSuccess ||
+            cudaMalloc(&s->d_FT, 6 * ne * sizeof(double)) != cudaSuccess) {
+            s->cap_ent = 0;
+            return set_err(PVOF_ENOMEM, "cudaMalloc particle entries");
+        }
+        s->cap_ent = ne;
+    }
+    if (nm > s->cap_mk) {
+        cudaFree(s->d_mk);
+        cudaFree(s->d_flag);
+        s->d_mk = nullptr;
+        s->d_flag = nullptr;
+        if (cudaMalloc(&s->d_mk, 6 * nm * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&s->d_flag, nm * sizeof(int)) != cudaSuccess) {
+            s->cap_mk = 0;
+            return set_err(PVOF_ENOMEM, "cudaMalloc particle markers");
+        }
+        s->cap_mk = nm;
+    }
+    std::vector<IbmEntryDev> ed(ne);
+    const double zs = c->g.zmin + 0.5 * (c->g.zmax - c->g.zmin);   // zc[G_Ks] of the storage plane
+    for (size_t q = 0; q < ne; q++) {
+        const IbmEntry &e = s->entries[q];
+        IbmEntryDev &o = ed[q];
+        for (int k = 0; k < 3; k++) { o.X[k] = e.X[k]; o.U[k] = e.U[k]; o.Omega[k] = e.Omega[k]; }
+        o.X[2] = zs;
+        o.Zs = zs;
+        o.moff = e.moff;
+        o.mcount = e.mcount;
+        for (int k = 0; k < 4; k++) o.box[k] = e.box[k];
+    }
+    if (ne) {
+        CK(cudaMemcpyAsync(s->d_ent, ed.data(), ne * sizeof(IbmEntryDev), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemsetAsync(s->d_FT, 0, 6 * ne * sizeof(double), c->stream));
+    }
+    if (nm) {
+        CK(cudaMemcpyAsync(s->d_mk, s->markers.x.data(), nm * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(s->d_mk + nm, s->markers.y.data(), nm * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(s->d_mk + 2 * nm, s->markers.vol.data(), nm * sizeof(double), cudaMemcpyHostToDevice,
+                           c->stream));
+        CK(cudaMemcpyAsync(s->d_flag, s->markers.flag.data(), nm * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));   // the host vectors may change with the next update
+    s->flagged = true;
+    return PVOF_OK;
+}
+
+IbmDev ibm_dev(pvof_ctx *c, IbmState *s)
+{
+    const size_t nm = s->markers.x.size();
+    IbmDev D;
+    D.ent = s->d_ent;
+    D.XL = s->d_mk;
+    D.YL = s->d_mk + nm;
+    D.vol = s->d_mk + 2 * nm;
+    D.UL = s->d_mk + 3 * nm;
+    D.rhoL = s->d_mk + 4 * nm;
+    D.FL = s->d_mk + 5 * nm;
+    D.flag = s->d_flag;
+    D.FT = s->d_FT;
+    const int NX = c->dom.NX, NY = c->dom.NY;
+    D.xlo = s->hm.xu[NG];
+    D.xhi = s->hm.xu[NX - 1 + NG];
+    D.ylo = s->hm.yv[NG];
+    D.yhi = s->hm.yv[NY - 1 + NG];
+    D.h = s->grid.h;
+    D.dxu1 = s->hm.dx_u[1 + NG];
+    D.slab = c->dom.slab > 0.0 ? c->dom.slab : D.dxu1;
+    D.dyv = c->dom.m.dy_v;
+    return D;
+}
+
+// Lagrangian_force (Lagrangian.c:1724-1871) without the squirmer, one-way and post-processing options
+int ibm_force(pvof_ctx *c, int force_iter)
+{
+    IbmState *s = c->ibm;
+    if (!s || !s->flagged) return set_err(PVOF_EINVAL, "pvof_Lagrangian_flag_points() first");
+    const Dom &d = c->dom;
+    const int NX = d.NX, NY = d.NY;
+    const double dtbeta = bet(c->stage) * c->dt;
+    const double idt2beta = 1.0 / (2.0 * bet(c->stage) * c->dt);
+    const int corrector = force_iter >= 0, iters = corrector ? force_iter : 1;
+    const int ne = (int)s->entries.size(), nm = (int)s->markers.x.size();
+    IbmDev D = ibm_dev(c, s);
+    const dim3 cb(128), cg((unsigned)((NX + 127) / 128), (unsigned)NY);
+    const unsigned mg = (unsigned)((nm + 127) / 128);
+    double *U = F(c, PVOF_F_U), *V = F(c, PVOF_F_V), *RU = F(c, PVOF_F_U_RHS), *RV = F(c, PVOF_F_V_RHS);
+    const double *rho = F(c, PVOF_F_RHO);
+    for (int ii = 0; ii < iters; ii++) {
+        TRY(fill(c, BK_WRAP_U, U));
+        TRY(fill(c, BK_WRAP_V, V));
+        if (corrector) {
+            k_ibm_ng_update<<<cg, cb, 0, c->stream>>>(d, RU, nullptr, 1);
+            CKL(c);
+            k_ibm_ng_update<<<cg, cb, 0, c->stream>>>(d, RV, nullptr, 1);
+            CKL(c);
+        }
+        if (nm > 0) {
+            k_ibm_interp<<<mg, 128, 0, c->stream>>>(d, rho, s->xc, s->yc, D.h, D.XL, D.YL, nm, D.rhoL);
+            CKL(c);
+        }
+        for (int comp = 0; comp < 2; comp++) {
+            const double *xs = comp == 0 ? s->xu : s->xc, *ys = comp == 0 ? s->yc : s->yv;
+            if (nm > 0) {
+                k_ibm_interp<<<mg, 128, 0, c->stream>>>(d, comp == 0 ? U : V, xs, ys, D.h, D.XL, D.YL, nm, D.UL);
+                CKL(c);
+            }
+            if (ne > 0) {
+                k_ibm_marker_force<<<(unsigned)((ne + 31) / 32), 32, 0, c->stream>>>(D, comp, ne, idt2beta,
+                                                                                   (!corrector && comp == 0) ? 1 : 0);
+                CKL(c);
+            }
+            for (int e = 0; e < ne; e++) {
+                k_ibm_spread<<<cg, cb, 0, c->stream>>>(d, D, e, comp, xs, ys, rho, comp == 0 ? RU : RV);
+                CKL(c);
+            }
+        }
+        if (corrector) {
+            k_ibm_correct<<<cg, cb, 0, c->stream>>>(d, 0, dtbeta, RU, rho, U);
+            CKL(c);
+            k_ibm_correct<<<cg, cb, 0, c->stream>>>(d, 1, dtbeta, RV, rho, V);
+            CKL(c);
+        }
+    }
+    if (!corrector) {
+        k_ibm_ng_update<<<cg, cb, 0, c->stream>>>(d, RU, F(c, PVOF_F_U_IMPLICIT), 0);
+        CKL(c);
+        k_ibm_ng_update<<<cg, cb, 0, c->stream>>>(d, RV, F(c, PVOF_F_V_IMPLICIT), 0);
+        CKL(c);
+    }
+    return PVOF_OK;
+}
+
+// Velocity_solve_explicit (msolve_direct.c:146-260)
+int vel_explicit(pvof_ctx *c, int comp)
+{
+    int i0, i1, j0, j1;
+    if (comp == 0) u_range(c, i0, i1, j0, j1);
+    else v_range(c, i0, i1, j0, j1);
+    if (i1 <= i0 || j1 <= j0) return PVOF_OK;
+    const dim3 cb(128), cg((unsigned)((i1 - i0 + 127) / 128), (unsigned)(j1 - j0));
+    k_vel_explicit<<<cg, cb, 0, c->stream>>>(c->dom, comp, i0, i1, j0, j1, bet(c->stage) * c->dt,
+                                              F(c, comp == 0 ? PVOF_F_U_RHS : PVOF_F_V_RHS), F(c, PVOF_F_RHO),
+                                              F(c, comp == 0 ? PVOF_F_U : PVOF_F_V));
+    CKL(c);
+    return PVOF_OK;
+}
+
+// VOF_DIFFUSE_compute_C_S (VOF_DIFFUSE.c:685-813)
+int compute_C_S(pvof_ctx *c)
+{
+    IbmState *s;
+    TRY(ibm_state(c, &s));
+    std::vector<double> geo;
+    ibm_solid_geometry(s->mobile, s->fixed, s->grid, geo);
+    if (geo.size() > s->cap_geo) {
+        cudaFree(s->d_geo);
+        s->d_geo = nullptr;
+        if (cudaMalloc(&s->d_geo, geo.size() * sizeof(double)) != cudaSuccess) {
+            s->cap_geo = 0;
+            return set_err(PVOF_ENOMEM, "cudaMalloc particle geometry");
+        }
+        s->cap_geo = geo.size();
+    }
+    s->ngeo = (int)(geo.size() / 3);
+    if (!geo.empty())
+        CK(cudaMemcpyAsync(s->d_geo, geo.data(), geo.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    double shift, denom, extra;
+    ibm_solid_constants(c->p.Cn, shift, denom, extra);
+    const Dom &d = c->dom;
+    const dim3 cb(128), cg((unsigned)((d.NX + 2 * NG + 127) / 128), (unsigned)(d.NY + 2 * NG));
+    k_compute_C_S<<<cg, cb, 0, c->stream>>>(d, s->xc, s->yc, s->d_geo, s->ngeo, shift, denom, extra, F(c, PVOF_F_C_S));
+    CKL(c);
+    TRY(fill(c, BK_SCALAR, F(c, PVOF_F_C_S)));
+    TRY(bound(c));
+    TRY(fill(c, BK_SCALAR, F(c, PVOF_F_C_L)));
+    TRY(phase_cache(c));
+    TRY(fill(c, BK_SCALAR, F(c, PVOF_F_C_G)));
+    CK(cudaStreamSynchronize(c->stream));   // the geometry host vector is released on return
+    return PVOF_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -925,6 +1193,7 @@ int pvof_destroy(pvof_ctx *c)
     for (int q = 0; q < 2; q++) if (c->timer_ev[q]) cudaEventDestroy(c->timer_ev[q]);
     for (int q = 0; q < Ctx::NPEND; q++)
         for (int e = 0; e < 2; e++) if (c->pend_ev[q][e]) cudaEventDestroy(c->pend_ev[q][e]);
+    delete c->ibm;
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PVOF_OK;
@@ -1185,6 +1454,101 @@ int pvof_solver_timing(const pvof_ctx *c, int solver, double *ms, long long *lau
     if (iterations) *iterations = c->sol_iters[solver];
     if (cell_iters) *cell_iters = c->sol_cell_iters[solver];
     return PVOF_OK;
+}
+
+
+// --- resolved solid particles --------------------------------------------
+int pvof_set_particles(pvof_ctx *c, const pvof_particle *parts, int n)
+{
+    ENTER(c);
+    if (n < 0 || (n > 0 && !parts)) return set_err(PVOF_EINVAL, "bad particle array");
+    IbmState *s;
+    TRY(ibm_state(c, &s));
+    s->mobile.clear();
+    s->fixed.clear();
+    for (int q = 0; q < n; q++) {
+        const pvof_particle &p = parts[q];
+        if (!(p.R > 0.0)) return set_err(PVOF_EINVAL, "particle radius must be positive");
+        IbmEntry e;
+        std::memset(&e, 0, sizeof(e));
+        e.X[0] = p.X[0];
+        e.X[1] = p.X[1];
+        e.R = p.R;
+        e.U[0] = p.U[0];
+        e.U[1] = p.U[1];
+        e.Omega[2] = p.Omega_z;
+        e.rho_s = p.rho_s;
+        (p.mobile ? s->mobile : s->fixed).push_back(e);
+    }
+    // IDs as Particle_initialize gives them: fixed first, then mobile (Particle.c:213-221)
+    int id = 0;
+    for (IbmEntry &e : s->fixed) e.id = id++;
+    for (IbmEntry &e : s->mobile) e.id = id++;
+    s->flagged = false;
+    return PVOF_OK;
+}
+
+int pvof_Lagrangian_flag_points(pvof_ctx *c) { ENTER(c); return ibm_flag_points(c); }
+
+int pvof_particle_entries(pvof_ctx *c)
+{
+    ENTER(c);
+    if (!c->ibm || !c->ibm->flagged) return set_err(PVOF_EINVAL, "pvof_Lagrangian_flag_points() first");
+    return (int)c->ibm->entries.size();
+}
+
+int pvof_particle_forces(pvof_ctx *c, double *Fo, double *To, int nmax)
+{
+    ENTER(c);
+    IbmState *s = c->ibm;
+    if (!s || !s->flagged) return set_err(PVOF_EINVAL, "pvof_Lagrangian_flag_points() first");
+    const int ne = (int)s->entries.size();
+    if (nmax < ne || !Fo || !To) return set_err(PVOF_EINVAL, "force arrays too small");
+    std::vector<double> h(6 * (size_t)ne);
+    if (ne) CK(cudaMemcpyAsync(h.data(), s->d_FT, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int e = 0; e < ne; e++)
+        for (int k = 0; k < 3; k++) {
+            Fo[3 * e + k] = h[6 * e + k];
+            To[3 * e + k] = h[6 * e + 3 + k];
+        }
+    return ne;
+}
+
+int pvof_particle_markers(pvof_ctx *c, int entry, double *x, double *y, double *vol, int *flag, int nmax)
+{
+    ENTER(c);
+    IbmState *s = c->ibm;
+    if (!s || !s->flagged) return set_err(PVOF_EINVAL, "pvof_Lagrangian_flag_points() first");
+    if (entry < 0 || entry >= (int)s->entries.size()) return set_err(PVOF_EINVAL, "bad particle entry");
+    const IbmEntry &e = s->entries[(size_t)entry];
+    if (nmax < e.mcount) return set_err(PVOF_EINVAL, "marker arrays too small");
+    for (int q = 0; q < e.mcount; q++) {
+        const size_t m = (size_t)(e.moff + q);
+        if (x) x[q] = s->markers.x[m];
+        if (y) y[q] = s->markers.y[m];
+        if (vol) vol[q] = s->markers.vol[m];
+        if (flag) flag[q] = s->markers.flag[m];
+    }
+    return e.mcount;
+}
+
+int pvof_VOF_DIFFUSE_compute_C_S(pvof_ctx *c) { ENTER(c); return compute_C_S(c); }
+
+int pvof_Velocity_solve_explicit(pvof_ctx *c, char component)
+{
+    ENTER(c);
+    NEED_DT(c);
+    int k = comp_of(component);
+    if (k < 0) return set_err(PVOF_EINVAL, "component must be 'u' or 'v' in the 2D modes");
+    return vel_explicit(c, k);
+}
+
+int pvof_Lagrangian_force(pvof_ctx *c, int force_iter)
+{
+    ENTER(c);
+    NEED_DT(c);
+    return ibm_force(c, force_iter);
 }
 
 }  // extern "C"

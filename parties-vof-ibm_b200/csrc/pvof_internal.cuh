@@ -102,6 +102,8 @@ struct DevScalars {
     unsigned bar_gen;
 };
 
+struct IbmState;
+
 struct Ctx {
     pvof_grid_desc g;
     pvof_params p;
@@ -140,6 +142,7 @@ struct Ctx {
     int pend_kind[NPEND], pend_comp[NPEND];
     long long pend_cells[NPEND], pend_cells2[NPEND];
     int npend;
+    IbmState *ibm;           // resolved particles (null until pvof_set_particles)
     double sol_ms[3];
     long long sol_launches[3], sol_iters[3], sol_cell_iters[3];
 };

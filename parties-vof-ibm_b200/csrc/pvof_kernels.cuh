@@ -116,6 +116,69 @@ cudaError_t cgs_pressure_launch(const PresArgs &A, const StripPlan &plan, cudaSt
 StripPlan cgs_velocity_setup(const int ru[4], const HostMap &mu, const int rv[4], const HostMap &mv, int axisym);
 cudaError_t cgs_velocity_launch(const VelPair &V, int ncomp, const StripPlan &plan, cudaStream_t stream);
 
+// ---------------------------------------------------------------------------
+// resolved solid particles (pvof_ibm.cu)
+// ---------------------------------------------------------------------------
+
+// one entry of a particle list after the update of a substep (an owned
+// particle or a periodic copy)
+struct IbmEntry {
+    int mobile, id, copy;
+    double X[3], U[3], Omega[3], R, rho_s;
+    double M, I_p, Vol_L;     // Particle_calc_derived_data
+    int N_L;                  // markers of the whole circle
+    int moff, mcount;         // this entry's markers near the domain
+    int box[4];               // cells [i0, i1) x [j0, j1) its marker supports can reach
+};
+
+struct IbmMarkers {
+    std::vector<double> x, y, vol;
+    std::vector<int> flag;
+};
+
+// grid data of the host-side particle bookkeeping; xu, yv offset so that
+// index 0 is the first G-range node, valid on [-NG, N + NG)
+struct IbmGrid {
+    int NX, NY;
+    int periodic[2];
+    const double *xu, *yv;
+    double h, dy_min, slab, twod_slab, Lx, Ly;
+};
+
+struct IbmEntryDev {
+    double X[3], U[3], Omega[3], Zs;
+    int moff, mcount;
+    int box[4];
+};
+
+struct IbmDev {
+    const IbmEntryDev *ent;
+    const double *XL, *YL, *vol;
+    const int *flag;
+    double *UL, *rhoL, *FL, *FT;   // FT: F[3], T[3] per entry
+    double xlo, xhi, ylo, yhi;     // Lagrangian_local_point_2d bounds
+    double h, dxu1, slab;
+    const double *dyv;
+};
+
+void ibm_build(const std::vector<IbmEntry> &mobile_local, const std::vector<IbmEntry> &fixed_local, const IbmGrid &g,
+               double Cn, std::vector<IbmEntry> &entries, IbmMarkers &m);
+void ibm_solid_geometry(const std::vector<IbmEntry> &mobile_local, const std::vector<IbmEntry> &fixed_local,
+                        const IbmGrid &g, std::vector<double> &geo);
+void ibm_solid_constants(double cn, double &shift, double &denom, double &extra);
+
+__global__ void k_ibm_interp(Dom d, const double *a, const double *xs, const double *ys, double h, const double *XL,
+                             const double *YL, int nm, double *out);
+__global__ void k_ibm_marker_force(IbmDev D, int comp, int nentries, double idt2beta, int reset);
+__global__ void k_ibm_spread(Dom d, IbmDev D, int e, int comp, const double *xs, const double *ys, const double *rho,
+                             double *rhs);
+__global__ void k_ibm_correct(Dom d, int comp, double dtbeta, const double *rhs, const double *rho, double *vel);
+__global__ void k_ibm_ng_update(Dom d, double *a, const double *b, int reset);
+__global__ void k_vel_explicit(Dom d, int comp, int i0, int i1, int j0, int j1, double dtimeb, const double *rhs,
+                               const double *rho, double *vel);
+__global__ void k_compute_C_S(Dom d, const double *xc, const double *yc, const double *geo, int ngeo, double shift,
+                              double denom, double extra, double *CS);
+
 __global__ void k_cg_biharmonic(BihArgs A);
 __global__ void k_cg_velocity(VelArgs A);
 __global__ void k_cg_pressure(PresArgs A);

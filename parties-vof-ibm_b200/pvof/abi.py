@@ -93,6 +93,14 @@ class Stats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class Particle(C.Structure):
+    """pvof_particle: one resolved solid particle of the planar mode."""
+    _fields_ = [
+        ("mobile", C.c_int), ("X", C.c_double * 2), ("R", C.c_double),
+        ("U", C.c_double * 2), ("Omega_z", C.c_double), ("rho_s", C.c_double),
+    ]
+
+
 # exported symbols of the C ABI (include/pvof.h), checked by the tests
 EXPORTS = [
     "pvof_abi_version", "pvof_last_error", "pvof_device_count",
@@ -113,6 +121,9 @@ EXPORTS = [
     "pvof_launch_count", "pvof_timer_start", "pvof_timer_stop", "pvof_flush_l2",
     "pvof_set_solver_timing", "pvof_solver_timing", "pvof_solver_kernel",
     "pvof_Pressure_solve_cg_noalloc", "pvof_noalloc_last_error",
+    "pvof_set_particles", "pvof_Lagrangian_flag_points", "pvof_particle_entries", "pvof_particle_forces",
+    "pvof_particle_markers", "pvof_VOF_DIFFUSE_compute_C_S", "pvof_Velocity_solve_explicit",
+    "pvof_Lagrangian_force",
 ]
 
 SOLVER_BIHARMONIC = 0

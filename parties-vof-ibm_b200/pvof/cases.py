@@ -153,3 +153,50 @@ def rayleigh_taylor(NXM=128, NYM=512, Lx=1.0, Ly=4.0, Cn=0.01, amp=0.05,
                             + 0.3 * rng.standard_normal((NY, NX)))
         p = velocity_amp * rng.standard_normal((NY, NX))
     return grid, params, {"F": C, "U": u, "V": v, "P": p}
+
+
+def axisym_grid(NXM, NYM, rmax, zmax):
+    """Axisymmetric (r, z) grid: the symmetry axis at r = 0 (left), no-slip
+    walls at r = rmax and at z = 0, zmax; full 2 pi ring."""
+    g = abi.GridDesc()
+    g.NXM, g.NYM, g.NZM = NXM, NYM, 1
+    g.ghost_nodes = G
+    g.geometry = abi.GEOM_AXISYM
+    g.periodic[0], g.periodic[1], g.periodic[2] = 0, 0, 1
+    for f in range(6):
+        g.wall[f] = abi.WALL_NOSLIP
+    g.xmin, g.xmax = 0.0, float(rmax)
+    g.ymin, g.ymax = 0.0, float(zmax)
+    hx = (g.xmax - g.xmin) / float(NXM)
+    hy = (g.ymax - g.ymin) / float(NYM)
+    g.slab_thickness = min(hx, hy)
+    g.zmin, g.zmax = 0.0, g.slab_thickness
+    g.theta_span = 2.0 * math.pi
+    return g
+
+
+def rising_bubble(NXM=64, NYM=128, rmax=2.0, zmax=4.0, radius=0.5, zc=1.0, Cn=0.04, rho_ratio=0.1,
+                  mu_ratio=0.1, Re=100.0, surface_tension=False, We=200.0, velocity_seed=None, velocity_amp=0.0,
+                  **param_kw):
+    """Axisymmetric bubble (C = 0 inside a sphere of ``radius`` on the axis at
+    z = zc) in liquid (C = 1); C = 0.5 (1 + tanh((d - radius) / (sqrt(2) Cn)))."""
+    grid = axisym_grid(NXM, NYM, rmax, zmax)
+    params = default_params(Re=Re, rho1=1.0, rho2=rho_ratio, mu1=1.0, mu2=mu_ratio, Cn=Cn, Pe_CH=1.0 / Cn,
+                            surface_tension=1 if surface_tension else 0, We=We, **param_kw)
+    xc, yc, xu, yv = cell_centres(grid)
+    X, Y = np.meshgrid(xc, yc)
+    dist = np.sqrt(X * X + (Y - zc) ** 2)
+    C = 0.5 * (1.0 + np.tanh((dist - radius) / (math.sqrt(2.0) * Cn)))
+    NX, NY, _ = dims(grid)
+    u = np.zeros((NY, NX))
+    v = np.zeros((NY, NX))
+    p = np.zeros((NY, NX))
+    if velocity_seed is not None:
+        rng = np.random.default_rng(velocity_seed)
+        Xu, Yc = np.meshgrid(xu, yc)
+        Xc, Yv = np.meshgrid(xc, yv)
+        u = velocity_amp * (np.sin(np.pi * Xu / rmax) * np.sin(np.pi * Yc / zmax) + 0.3 * rng.standard_normal((NY, NX)))
+        v = velocity_amp * (np.sin(np.pi * Xc / rmax) * np.sin(np.pi * Yv / zmax) + 0.3 * rng.standard_normal((NY, NX)))
+        p = velocity_amp * rng.standard_normal((NY, NX))
+    return grid, params, {"F": C, "U": u, "V": v, "P": p}
+

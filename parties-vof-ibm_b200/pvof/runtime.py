@@ -66,6 +66,14 @@ def load():
     L.pvof_set_solver_timing.argtypes = [V, C.c_int]
     L.pvof_solver_timing.argtypes = [V, C.c_int, P(C.c_double), P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]
     L.pvof_solver_kernel.argtypes = [V, C.c_int]
+    L.pvof_set_particles.argtypes = [V, P(abi.Particle), C.c_int]
+    L.pvof_Lagrangian_flag_points.argtypes = [V]
+    L.pvof_particle_entries.argtypes = [V]
+    L.pvof_particle_forces.argtypes = [V, P(C.c_double), P(C.c_double), C.c_int]
+    L.pvof_particle_markers.argtypes = [V, C.c_int, P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int), C.c_int]
+    L.pvof_VOF_DIFFUSE_compute_C_S.argtypes = [V]
+    L.pvof_Velocity_solve_explicit.argtypes = [V, C.c_char]
+    L.pvof_Lagrangian_force.argtypes = [V, C.c_int]
     L.pvof_solver_kernel.restype = C.c_char_p
     _lib = L
     return L
@@ -144,6 +152,37 @@ class Solver:
         st = abi.Stats()
         check(load().pvof_run_steps(self.h, n, dt, C.byref(st)), "pvof_run_steps")
         return st
+
+    # -- resolved solid particles -----------------------------------------
+    def set_particles(self, particles):
+        """particles: rows (mobile, x, y, R, u, v, omega_z, rho_s)."""
+        arr = (abi.Particle * max(len(particles), 1))()
+        for q, (mob, x, y, r, u, v, om, rs) in enumerate(particles):
+            p = arr[q]
+            p.mobile, p.R, p.Omega_z, p.rho_s = int(mob), float(r), float(om), float(rs)
+            p.X[0], p.X[1], p.U[0], p.U[1] = float(x), float(y), float(u), float(v)
+        check(load().pvof_set_particles(self.h, arr, len(particles)), "pvof_set_particles")
+
+    def flag_points(self):
+        check(load().pvof_Lagrangian_flag_points(self.h), "pvof_Lagrangian_flag_points")
+        return check(load().pvof_particle_entries(self.h), "pvof_particle_entries")
+
+    def particle_forces(self):
+        n = check(load().pvof_particle_entries(self.h), "pvof_particle_entries")
+        F = np.zeros(3 * max(n, 1))
+        T = np.zeros(3 * max(n, 1))
+        check(load().pvof_particle_forces(self.h, F.ctypes.data_as(C.POINTER(C.c_double)),
+                                          T.ctypes.data_as(C.POINTER(C.c_double)), n), "pvof_particle_forces")
+        return F[:3 * n].reshape(n, 3), T[:3 * n].reshape(n, 3)
+
+    def particle_markers(self, entry, nmax=100000):
+        x, y, vol = np.zeros(nmax), np.zeros(nmax), np.zeros(nmax)
+        fl = np.zeros(nmax, dtype=np.int32)
+        dp = C.POINTER(C.c_double)
+        n = check(load().pvof_particle_markers(self.h, entry, x.ctypes.data_as(dp), y.ctypes.data_as(dp),
+                                               vol.ctypes.data_as(dp), fl.ctypes.data_as(C.POINTER(C.c_int)), nmax),
+                  "pvof_particle_markers")
+        return x[:n], y[:n], vol[:n], fl[:n]
 
     def liquid_mass(self):
         m = C.c_double()

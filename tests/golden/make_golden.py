@@ -3,7 +3,9 @@
 Runs the reference's own time-step code, compiled from its sources by
 oracle/ref/Makefile into oracle/_ref/ref_<case>, on small seeded cases and
 stores the inputs, parameters, solver iteration counts and the fields after
-every RK substep in tests/golden/<name>.npz.
+every RK substep in tests/golden/<name>.npz.  The resolved-particle fixtures
+(IBM_CASES) hold the inputs and outputs of the immersed-boundary routines of
+one substep, from the routine driver oracle/ref/ibm_driver.c.
 
     python tests/golden/make_golden.py [--refsrc PATH]
 
@@ -44,6 +46,13 @@ CASES = [
      2, 1e-3, ["s0", "s1_0", "s1_2", "s2_2"]),
 ]
 
+# resolved-particle routine cases (oracle/ref/ibm_driver.c on the ibm2d build):
+# name, builder kwargs, particles (mobile, x, y, R, u, v, omega_z, rho_s), dt, stage
+IBM_CASES = [
+    ("ibm_small", dict(NXM=32, NYM=128, Lx=1.0, Ly=4.0, Cn=0.04, velocity_seed=7, velocity_amp=0.1),
+     [(0, 0.06, 1.2, 0.2, 0.0, 0.0, 0.0, 2.5), (1, 0.55, 2.7, 0.15, 0.2, -0.1, 0.7, 2.5)], 1e-3, 1),
+]
+
 PARAM_KEYS = [k for k, _ in abi.Params._fields_]
 GRID_KEYS = [k for k, _ in abi.GridDesc._fields_]
 
@@ -75,7 +84,9 @@ def g_range(grid, plane, ng):
 
 
 def make(name, refcase, kw, steps, dt, keep, outdir, refsrc=None):
-    grid, params, planes = cases.rayleigh_taylor(**kw)
+    build = dict(kw)
+    builder = getattr(cases, build.pop("_builder", "rayleigh_taylor"))
+    grid, params, planes = builder(**build)
     if not os.path.exists(po.ref_binary(refcase)):
         po.build_reference(refcase, refsrc)
     with tempfile.TemporaryDirectory() as wd:
@@ -105,13 +116,54 @@ def make(name, refcase, kw, steps, dt, keep, outdir, refsrc=None):
     return path
 
 
+def make_ibm(name, kw, particles, dt, stage, outdir, refsrc=None):
+    grid, params, planes = cases.rayleigh_taylor(**kw)
+    if not os.path.exists(po.ref_binary("ibm2d")):
+        po.build_reference("ibm2d", refsrc)
+    fixed = [p[1:7] for p in particles if not p[0]]
+    mobile = [p[1:7] for p in particles if p[0]]
+    data = {}
+    with tempfile.TemporaryDirectory() as wd:
+        cp = po.run_reference_ibm(wd, grid, params, planes, fixed, mobile, dt, stage)
+        for fname in ["C_S", "C_L", "rho", "mu", "u", "v"]:
+            data["i0/" + fname] = po.read_reference_field(wd, "i0", fname, grid)
+        for tag, rhs in (("r0", True), ("r1", False), ("r2", True), ("r3", False), ("r4", True)):
+            for fname in ["u", "v"]:
+                data["%s/%s" % (tag, fname)] = po.read_reference_field(wd, tag, fname, grid)
+            if rhs:
+                for fname in ["u_rhs", "v_rhs", "u_implicit", "v_implicit"]:
+                    data["%s/%s" % (tag, fname)] = po.read_reference_field(wd, tag, fname, grid, ng=True)
+        for tag in ("r2", "r4"):
+            F, T = po.read_reference_particles(wd, tag)
+            data[tag + "/F"], data[tag + "/T"] = F, T
+        mk = po.read_reference_markers(wd)
+        data["markers/count"] = np.array([len(m[0]) for m in mk], dtype=np.int64)
+        for q, key in enumerate(["x", "y", "vol", "flag"]):
+            data["markers/" + key] = np.concatenate([m[q] for m in mk]) if mk else np.zeros(0)
+        data["log"] = np.array(cp.stdout[-2000:])
+    for k, v in planes.items():
+        data["init/" + k] = v
+    meta = {"grid": struct_to_dict(grid), "params": struct_to_dict(params), "dt": dt, "stage": stage,
+            "particles": [list(p) for p in particles], "builder": kw, "refcase": "ibm2d"}
+    data["meta"] = np.array(repr(meta))
+    path = os.path.join(outdir, name + ".npz")
+    np.savez_compressed(path, **data)
+    return path
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--refsrc", default=None)
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--only", default=None, help="comma-separated fixture names")
     a = ap.parse_args()
+    ap_only = a.only.split(",") if a.only else None
     for name, refcase, kw, steps, dt, keep in CASES:
-        print(make(name, refcase, kw, steps, dt, keep, a.out, a.refsrc))
+        if ap_only is None or name in ap_only:
+            print(make(name, refcase, kw, steps, dt, keep, a.out, a.refsrc))
+    for name, kw, parts, dt, stage in IBM_CASES:
+        if ap_only is None or name in ap_only:
+            print(make_ibm(name, kw, parts, dt, stage, a.out, a.refsrc))
 
 
 if __name__ == "__main__":
