@@ -206,6 +206,13 @@ int pvof_Pressure_project_velocity(pvof_ctx *ctx);
 /* Pressure.c:475-597; writes the max |div| to *div_max */
 int pvof_Pressure_compute_velocity_divergence(pvof_ctx *ctx, double *div_max);
 
+/* Eulerian/lsolver/psolve_fft.c:638-983 Pressure_solve_xz_period: the
+ * constant-density Poisson equation lap(DELTAP) = P_RHS on the physical cells
+ * by a Fourier transform in x and tridiagonal solves in y (Neumann walls, the
+ * mean mode pinned at the first row); planar mode, x periodic, at most 2048
+ * cells in x.  Not on the variable-density path of the substep. */
+int pvof_Pressure_solve_fft(pvof_ctx *ctx);
+
 /* Temporal_int.c:563-1279 Temporal_int_all_the_equations for a case without
  * solids: one complete RK substep at the stage/dt set by pvof_set_stage. */
 int pvof_substep(pvof_ctx *ctx, pvof_stats *stats);

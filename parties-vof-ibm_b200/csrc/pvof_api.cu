@@ -1013,6 +1013,57 @@ int compute_C_S(pvof_ctx *c)
     return PVOF_OK;
 }
 
+// Pressure_solve_xz_period (psolve_fft.c:638-983) in the planar mode
+int p_solve_fft(pvof_ctx *c)
+{
+    const Dom &d = c->dom;
+    if (!d.planar || !d.perx || d.pery)
+        return set_err(PVOF_EINVAL, "the FFT Poisson solver needs the planar mode, x periodic and walls in y");
+    const int N = d.NX - 1, NYp = d.NY - 1;
+    if (N > 2048) return set_err(PVOF_EINVAL, "the FFT Poisson solver takes at most 2048 cells in x");
+    int logN = -1;
+    if ((N & (N - 1)) == 0) { logN = 0; while ((1 << logN) < N) logN++; }
+    if (!c->fft_coef) {
+        // Pressure_calc_coeff (psolve_fft.c:467-591), walls in y, x periodic
+        HostMetrics hm;
+        build_metrics(c->g, d.NX, d.NY, hm);
+        auto idy_v = [&](int j) { return hm.idy_v[j + NG]; };
+        auto idy_c = [&](int j) { return hm.idy_c[j + NG]; };
+        std::vector<double> co(3 * (size_t)NYp + (size_t)N, 0.0);
+        double *as_ = co.data(), *ap_ = as_ + NYp, *an_ = ap_ + NYp, *mw = an_ + NYp;
+        as_[0] = 0.0;
+        an_[NYp - 1] = 0.0;
+        for (int j = 0; j < NYp; j++) {
+            if (j > 0) as_[j] = idy_v(j) * idy_c(j - 1);
+            if (j < NYp - 1) an_[j] = idy_v(j) * idy_c(j);
+            ap_[j] = -as_[j] - an_[j];
+        }
+        an_[NYp - 1] = 0.0;
+        const double idx = hm.idx_u[NG];
+        const double pi = 3.14159265358979323846;
+        for (int i = 0; i < N; i++) {
+            const int wave = i < N / 2 ? i : N - i;   // Pressure_fft_setup wave ordering
+            mw[i] = 2.0 * (1 - cos(2. * pi * wave / N)) * (idx * idx);
+        }
+        if (cudaMalloc(&c->fft_coef, co.size() * sizeof(double)) != cudaSuccess) {
+            c->fft_coef = nullptr;
+            return set_err(PVOF_ENOMEM, "cudaMalloc FFT coefficients");
+        }
+        CK(cudaMemcpy(c->fft_coef, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    const double *as_ = c->fft_coef, *ap_ = as_ + NYp, *an_ = ap_ + NYp, *mw = an_ + NYp;
+    double *hc = S(c, SC_P_RES), *gam = S(c, SC_P_D);
+    const size_t smem = (size_t)N * sizeof(double2);
+    const double inx = 1.0 / (d.NX - 1.0);
+    k_fft_forward<<<(unsigned)NYp, 256, smem, c->stream>>>(d, N, logN, F(c, PVOF_F_P_RHS), hc, inx);
+    CKL(c);
+    k_fft_tridiag<<<(unsigned)((N + 127) / 128), 128, 0, c->stream>>>(d, N, NYp, as_, ap_, an_, mw, hc, gam);
+    CKL(c);
+    k_fft_inverse<<<(unsigned)NYp, 256, smem, c->stream>>>(d, N, logN, hc, F(c, PVOF_F_DELTAP));
+    CKL(c);
+    return PVOF_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1194,6 +1245,7 @@ int pvof_destroy(pvof_ctx *c)
     for (int q = 0; q < Ctx::NPEND; q++)
         for (int e = 0; e < 2; e++) if (c->pend_ev[q][e]) cudaEventDestroy(c->pend_ev[q][e]);
     delete c->ibm;
+    if (c->fft_coef) cudaFree(c->fft_coef);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PVOF_OK;
@@ -1550,5 +1602,8 @@ int pvof_Lagrangian_force(pvof_ctx *c, int force_iter)
     NEED_DT(c);
     return ibm_force(c, force_iter);
 }
+
+
+int pvof_Pressure_solve_fft(pvof_ctx *c) { ENTER(c); return p_solve_fft(c); }
 
 }  // extern "C"

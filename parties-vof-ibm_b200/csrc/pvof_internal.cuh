@@ -143,6 +143,7 @@ struct Ctx {
     long long pend_cells[NPEND], pend_cells2[NPEND];
     int npend;
     IbmState *ibm;           // resolved particles (null until pvof_set_particles)
+    double *fft_coef;        // as, ap, an (NY-1 each) and the modified wavenumbers (NX-1)
     double sol_ms[3];
     long long sol_launches[3], sol_iters[3], sol_cell_iters[3];
 };

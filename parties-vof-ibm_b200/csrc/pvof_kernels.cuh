@@ -179,6 +179,12 @@ __global__ void k_vel_explicit(Dom d, int comp, int i0, int i1, int j0, int j1, 
 __global__ void k_compute_C_S(Dom d, const double *xc, const double *yc, const double *geo, int ngeo, double shift,
                               double denom, double extra, double *CS);
 
+// constant-density Poisson solver (pvof_fft.cu)
+__global__ void k_fft_forward(Dom d, int N, int logN, const double *rhs, double *hc, double inx);
+__global__ void k_fft_tridiag(Dom d, int N, int NYp, const double *as_, const double *ap_, const double *an_,
+                              const double *mw, double *hc, double *gam);
+__global__ void k_fft_inverse(Dom d, int N, int logN, const double *hc, double *out);
+
 __global__ void k_cg_biharmonic(BihArgs A);
 __global__ void k_cg_velocity(VelArgs A);
 __global__ void k_cg_pressure(PresArgs A);

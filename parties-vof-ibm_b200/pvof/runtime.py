@@ -74,6 +74,7 @@ def load():
     L.pvof_VOF_DIFFUSE_compute_C_S.argtypes = [V]
     L.pvof_Velocity_solve_explicit.argtypes = [V, C.c_char]
     L.pvof_Lagrangian_force.argtypes = [V, C.c_int]
+    L.pvof_Pressure_solve_fft.argtypes = [V]
     L.pvof_solver_kernel.restype = C.c_char_p
     _lib = L
     return L

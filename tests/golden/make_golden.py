@@ -16,6 +16,7 @@ neither the tree nor the binaries.
 import argparse
 import os
 import re
+import subprocess
 import sys
 import tempfile
 
@@ -52,6 +53,10 @@ IBM_CASES = [
     ("ibm_small", dict(NXM=32, NYM=128, Lx=1.0, Ly=4.0, Cn=0.04, velocity_seed=7, velocity_amp=0.1),
      [(0, 0.06, 1.2, 0.2, 0.0, 0.0, 0.0, 2.5), (1, 0.55, 2.7, 0.15, 0.2, -0.1, 0.7, 2.5)], 1e-3, 1),
 ]
+
+# constant-density FFT Poisson cases (oracle/ref/fft_driver.c on the fft2d build):
+# name, NXM, NYM, Lx, Ly, seed
+FFT_CASES = [("fft_small", 32, 64, 1.0, 2.0, 1), ("fft_odd", 24, 40, 1.5, 2.5, 2)]
 
 PARAM_KEYS = [k for k, _ in abi.Params._fields_]
 GRID_KEYS = [k for k, _ in abi.GridDesc._fields_]
@@ -151,6 +156,36 @@ def make_ibm(name, kw, particles, dt, stage, outdir, refsrc=None):
     return path
 
 
+def make_fft(name, NXM, NYM, Lx, Ly, seed, outdir, refsrc=None):
+    """The reference's FFT solver runs in 3D with NZM = 2 (it needs an even
+    z count) on a z-independent right-hand side; its k = 0 plane is the 2D
+    solution.  The fixture keeps the 2D grid the library solves on."""
+    grid, params, _ = cases.rayleigh_taylor(NXM, NYM, Lx=Lx, Ly=Ly, Cn=0.04)
+    if not os.path.exists(po.ref_binary("fft2d")):
+        po.build_reference("fft2d", refsrc)
+    NX, NY, _ = cases.dims(grid)
+    rng = np.random.default_rng(seed)
+    rhs = np.zeros((NY, NX))
+    rhs[:NY - 1, :NX - 1] = rng.standard_normal((NY - 1, NX - 1))
+    rhs[:NY - 1, :NX - 1] -= rhs[:NY - 1, :NX - 1].mean()
+    grid3 = abi.GridDesc.from_buffer_copy(grid)
+    grid3.NZM = 2
+    grid3.zmax = grid3.zmin + 2.0 * (grid.xmax - grid.xmin) / NXM
+    with tempfile.TemporaryDirectory() as wd:
+        po.write_parties_inp(os.path.join(wd, "parties.inp"), grid3, params)
+        rhs.astype("<f8").tofile(os.path.join(wd, "rhs.bin"))
+        subprocess.run([po.ref_binary("fft2d"), wd], check=True, capture_output=True, text=True, timeout=600)
+        a = np.fromfile(os.path.join(wd, "out", "fft_deltap.bin"), dtype="<f8")
+    G = cases.G
+    blk = a.reshape(3 + 2 * G, NY + 2 * G, NX + 2 * G)
+    data = {"rhs": rhs, "deltap": blk[G, G:G + NY - 1, G:G + NX - 1]}
+    meta = {"grid": struct_to_dict(grid), "params": struct_to_dict(params), "refcase": "fft2d"}
+    data["meta"] = np.array(repr(meta))
+    path = os.path.join(outdir, name + ".npz")
+    np.savez_compressed(path, **data)
+    return path
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--refsrc", default=None)
@@ -164,6 +199,9 @@ def main():
     for name, kw, parts, dt, stage in IBM_CASES:
         if ap_only is None or name in ap_only:
             print(make_ibm(name, kw, parts, dt, stage, a.out, a.refsrc))
+    for name, NXM, NYM, Lx, Ly, seed in FFT_CASES:
+        if ap_only is None or name in ap_only:
+            print(make_fft(name, NXM, NYM, Lx, Ly, seed, a.out, a.refsrc))
 
 
 if __name__ == "__main__":
