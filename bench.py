@@ -18,6 +18,11 @@ HBM, the L2 flushed before every step (outside the timed intervals).  e2e:
 the same steps driven through the C ABI with the state uploaded from pinned
 host buffers before every step and downloaded after it.
 
+--batch-cases K additionally times K replicas of the workload advanced
+concurrently by pvof_run_steps_batched (the batched form: one host thread and
+stream per case, so the cluster-resident solvers of different cases run on
+different SMs) and adds a "batched" object to the line.
+
 --impl reference runs the reference's own time step (compiled from its
 sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host.
 With N > 1 (torchrun) every rank advances its own replica of the case
@@ -267,6 +272,31 @@ def run_ours(args):
     traffic = profile_traffic(names[dom])
     shares = {names[k]: round(timing[k]["ms"] / total_ms, 4) for k in timing}
 
+    # ---- batched form: K replicas advanced concurrently (optional) -----------
+    batched = None
+    if args.batch_cases > 1:
+        reps = []
+        for q in range(args.batch_cases):
+            r = runtime.Solver(grid, params, device=local)
+            r.set_planes(planes)
+            r.initialize()
+            reps.append(r)
+        runtime.run_steps_batched(reps, 1, DT)
+        bsteps = max(1, min(args.steps, args.batch_steps))
+        for r in reps:
+            r.flush_l2()
+        for r in reps:
+            r.timer_start()
+        runtime.run_steps_batched(reps, bsteps, DT)
+        span = max(r.timer_stop() for r in reps)
+        bvalue = args.batch_cases * cells * bsteps / (span * 1e-3)
+        batched = {"cases": args.batch_cases, "steps": bsteps, "value": bvalue, "unit": UNIT,
+                   "ms_per_step": span / bsteps, "vs_single": bvalue / (cells * args.steps / (total_ms * 1e-3)),
+                   "note": "replicas of the workload advanced concurrently by pvof_run_steps_batched "
+                           "(one host thread and stream per case); device time of the slowest case"}
+        for r in reps:
+            r.close()
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         r = reference_timing(args.cpu_steps)
@@ -297,6 +327,8 @@ def run_ours(args):
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if batched is not None:
+            line["batched"] = batched
         print(json.dumps(line))
     g.close()
     if dist is not None:
@@ -314,6 +346,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=5)
     ap.add_argument("--ref-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-cases", type=int, default=0,
+                    help="also time this many replicas advanced concurrently (batched form)")
+    ap.add_argument("--batch-steps", type=int, default=10)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         log("note: fewer than 3 warm-up steps")

@@ -221,6 +221,12 @@ int pvof_substep(pvof_ctx *ctx, pvof_stats *stats);
  * stats (optional) receives the last substep's statistics. */
 int pvof_run_steps(pvof_ctx *ctx, int nsteps, double dt, pvof_stats *stats);
 
+/* Batched form: advances n independent contexts by nsteps each
+ * (pvof_run_steps), concurrently -- one host thread per context, each on its
+ * own stream, so the solvers of different cases share the GPU's SMs.
+ * stats (optional) has n entries.  Returns the first failing case's code. */
+int pvof_run_steps_batched(pvof_ctx *const *ctxs, int n, int nsteps, double dt, pvof_stats *stats);
+
 /* Sum of C_L * cell measure over the physical cells (mass diagnostic,
  * VOF_DIFFUSE.c:1071-1091), computed on the device in FP64. */
 int pvof_liquid_mass(pvof_ctx *ctx, double *mass);

@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pvof_kernels.cuh"
@@ -1420,6 +1421,29 @@ int pvof_run_steps(pvof_ctx *c, int nsteps, double dt, pvof_stats *st)
             c->time += dt * bet2(rk);
         }
     }
+    return PVOF_OK;
+}
+
+int pvof_run_steps_batched(pvof_ctx *const *ctxs, int n, int nsteps, double dt, pvof_stats *stats)
+{
+    if (n < 0 || (n > 0 && !ctxs)) return set_err(PVOF_EINVAL, "bad context array");
+    for (int q = 0; q < n; q++) {
+        if (!ctxs[q]) return set_err(PVOF_EINVAL, "null context in the batch");
+        for (int r = 0; r < q; r++)
+            if (ctxs[r] == ctxs[q]) return set_err(PVOF_EINVAL, "a context appears twice in the batch");
+    }
+    std::vector<int> rc((size_t)n, PVOF_OK);
+    std::vector<std::string> msg((size_t)n);
+    std::vector<std::thread> workers;
+    workers.reserve((size_t)n);
+    for (int q = 0; q < n; q++)
+        workers.emplace_back([&, q]() {
+            rc[(size_t)q] = pvof_run_steps(ctxs[q], nsteps, dt, stats ? &stats[q] : nullptr);
+            if (rc[(size_t)q] < 0) msg[(size_t)q] = g_err;   // the message is per thread
+        });
+    for (std::thread &t : workers) t.join();
+    for (int q = 0; q < n; q++)
+        if (rc[(size_t)q] < 0) return set_err(rc[(size_t)q], "case " + std::to_string(q) + ": " + msg[(size_t)q]);
     return PVOF_OK;
 }
 

@@ -123,7 +123,7 @@ EXPORTS = [
     "pvof_Pressure_solve_cg_noalloc", "pvof_noalloc_last_error",
     "pvof_set_particles", "pvof_Lagrangian_flag_points", "pvof_particle_entries", "pvof_particle_forces",
     "pvof_particle_markers", "pvof_VOF_DIFFUSE_compute_C_S", "pvof_Velocity_solve_explicit",
-    "pvof_Lagrangian_force", "pvof_Pressure_solve_fft",
+    "pvof_Lagrangian_force", "pvof_Pressure_solve_fft", "pvof_run_steps_batched",
 ]
 
 SOLVER_BIHARMONIC = 0

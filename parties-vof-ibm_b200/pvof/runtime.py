@@ -75,6 +75,7 @@ def load():
     L.pvof_Velocity_solve_explicit.argtypes = [V, C.c_char]
     L.pvof_Lagrangian_force.argtypes = [V, C.c_int]
     L.pvof_Pressure_solve_fft.argtypes = [V]
+    L.pvof_run_steps_batched.argtypes = [P(V), C.c_int, C.c_int, C.c_double, P(abi.Stats)]
     L.pvof_solver_kernel.restype = C.c_char_p
     _lib = L
     return L
@@ -220,3 +221,14 @@ class Solver:
         check(load().pvof_solver_timing(self.h, solver, C.byref(ms), C.byref(nl), C.byref(it), C.byref(ci)),
               "pvof_solver_timing")
         return {"ms": ms.value, "launches": nl.value, "iterations": it.value, "cell_iters": ci.value}
+
+
+def run_steps_batched(solvers, nsteps, dt):
+    """Advance independent Solver objects concurrently (pvof_run_steps_batched);
+    returns their statistics."""
+    n = len(solvers)
+    handles = (C.c_void_p * max(n, 1))(*[s.h.value for s in solvers])
+    stats = (abi.Stats * max(n, 1))()
+    check(load().pvof_run_steps_batched(handles, n, nsteps, dt, stats), "pvof_run_steps_batched")
+    return [stats[q] for q in range(n)]
+
