@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define PVOF_ABI_VERSION 1
+#define PVOF_ABI_VERSION 2
 
 /* error codes */
 #define PVOF_OK 0
@@ -97,6 +97,9 @@ typedef struct pvof_params {
     double P_CG_ETOL;
     int surface_tension;        /* SURFACE_TENSION */
     int gravity;                /* VOF_GRAVITY */
+    /* resolved solids (used once pvof_set_particles has been called) */
+    double contact_angle_deg;   /* [vof] contact_angle_deg (default 90) */
+    int N_forcing_loops;        /* [particle] N_forcing_loops (default 2) */
 } pvof_params;
 
 /* Field identifiers for upload/download. */
@@ -113,6 +116,8 @@ enum pvof_field {
     PVOF_F_V_VISC_EXPLICIT, PVOF_F_V_VISC_EXPLICIT_OLD, PVOF_F_V_RHS,
     /* no-ghost surface-tension face forces */
     PVOF_F_FSIG_OLD_X, PVOF_F_FSIG_OLD_Y, PVOF_F_FSIG_NEW_X, PVOF_F_FSIG_NEW_Y,
+    /* solid normals of the contact-line projection (VolumeFraction nx_IBM, ny_IBM) */
+    PVOF_F_NX_IBM, PVOF_F_NY_IBM,
     PVOF_F_COUNT
 };
 
@@ -262,6 +267,17 @@ int pvof_particle_markers(pvof_ctx *ctx, int entry, double *x, double *y, double
 /* Eulerian/VOF_DIFFUSE.c:685-813 VOF_DIFFUSE_compute_C_S: solid fraction, then
  * the clamp of C_L and the phase cache */
 int pvof_VOF_DIFFUSE_compute_C_S(pvof_ctx *ctx);
+/* Eulerian/VOF_IBM_wetting.c:1021-1104 VOF_DIFFUSE_compute_solid_normals_MCL:
+ * solid normals into PVOF_F_NX_IBM / PVOF_F_NY_IBM */
+int pvof_VOF_DIFFUSE_compute_solid_normals_MCL(pvof_ctx *ctx);
+/* Eulerian/VOF_IBM_wetting.c:1946-2008 VOF_DIFFUSE_apply_contact_angle: the
+ * characteristic contact-angle projection of C_L in the solid cells along the
+ * contact line (no boundary update, as the reference) */
+int pvof_VOF_DIFFUSE_apply_contact_angle(pvof_ctx *ctx);
+/* Eulerian/VOF_IBM_wetting.c:2014-2131 VOF_DIFFUSE_extend_psi_LG_contact_angle:
+ * psi_LG in the same cells along the same characteristics, then its boundary
+ * values */
+int pvof_VOF_DIFFUSE_extend_psi_LG_contact_angle(pvof_ctx *ctx);
 /* Eulerian/lsolver/msolve_direct.c:146-260 Velocity_solve_explicit (u or v) */
 int pvof_Velocity_solve_explicit(pvof_ctx *ctx, char component);
 /* Lagrangian/Lagrangian.c:1724-1871 Lagrangian_force: force_iter < 0 is the

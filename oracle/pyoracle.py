@@ -157,8 +157,10 @@ def write_parties_inp(path, grid, params):
         "Cn = %.17g" % p.Cn, "Pe_CH = %.17g" % p.Pe_CH,
         "weno_order = %d" % p.weno_order, "ch_iter_max = %d" % p.ch_iter_max,
         "ch_tol = %.17g" % p.ch_tol,
+        "contact_angle_deg = %.17g" % p.contact_angle_deg,
         "[particle]",
         "grav = {%.17g, %.17g, %.17g}" % (p.grav[0], p.grav[1], p.grav[2]),
+        "N_forcing_loops = %d" % p.N_forcing_loops,
         "[conc]",
         "richardson = {%.17g, 0}" % p.richardson,
         "[lsolve]",
@@ -196,9 +198,11 @@ def run_reference(case, workdir, grid, params, planes, nsteps, dt, dump_every=1,
     return subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=timeout)
 
 
-def run_reference_ibm(workdir, grid, params, planes, fixed, mobile, dt, stage, case="ibm2d", timeout=600):
-    """Run the immersed-boundary routine driver (oracle/ref/ibm_driver.c) of
-    the reference build ``case``: particles are rows (X, Y, R, U, V, Omega_z)."""
+def run_reference_ibm(workdir, grid, params, planes, fixed, mobile, dt, stage, case="ibm2d", timeout=600,
+                      mode="routines", nsteps=1):
+    """Run the immersed-boundary driver (oracle/ref/ibm_driver.c) of the
+    reference build ``case``: particles are rows (X, Y, R, U, V, Omega_z);
+    ``mode`` is "routines", "mcl" or "steps" (``nsteps`` whole steps)."""
     os.makedirs(workdir, exist_ok=True)
     write_parties_inp(os.path.join(workdir, "parties.inp"), grid, params)
     names = {"F": "init_C.bin", "U": "init_u.bin", "V": "init_v.bin", "P": "init_p.bin"}
@@ -209,7 +213,7 @@ def run_reference_ibm(workdir, grid, params, planes, fixed, mobile, dt, stage, c
         with open(os.path.join(workdir, fn), "w") as f:
             for r in rows:
                 f.write(" ".join("%.17g" % float(x) for x in r) + "\n")
-    cmd = [ref_binary(case), workdir, repr(float(dt)), str(int(stage))]
+    cmd = [ref_binary(case), workdir, repr(float(dt)), str(int(stage)), mode, str(int(nsteps))]
     return subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=timeout)
 
 

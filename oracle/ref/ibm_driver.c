@@ -20,7 +20,28 @@
  *   r4   Lagrangian_force(N_forcing_loops) (+ boundary update): u, v, RHS,
  *        particle F and T (particles_r4.txt)
  *
- * Usage: ibm_driver <case_dir> <dt> <stage>
+ * Mode "mcl" instead dumps the contact-line routines of VOF_IBM_wetting.c
+ * (Liu & Ding characteristic projection):
+ *
+ *   m1   C_L, C_G, C_S before VOF_DIFFUSE_apply_contact_angle: the state
+ *        VOF_DIFFUSE_init has just before its own call of it (clamp of F,
+ *        bound to 1 - C_S, boundary values, phase cache)
+ *   m2   C_L right after VOF_DIFFUSE_apply_contact_angle (no boundary update)
+ *        and the solid normals nx_IBM, ny_IBM it computed
+ *   m3   psi_LG from VOF_DIFFUSE_compute_psi_LG after the boundary update and
+ *        phase cache of m2, and the C_L, C_G it was computed from
+ *   m4   psi_LG after VOF_DIFFUSE_extend_psi_LG_contact_angle
+ *
+ * Mode "steps" runs <nsteps> whole time steps through the reference's own
+ * substep routine Temporal_int_all_the_equations, as ref_driver.c does, and
+ * dumps the state (dump_state of ref_driver.c) after every step, plus the
+ * particle F and T (particles_s<n>.txt).
+ *
+ * The initial volume fraction goes into both F and C_L, as the reference's
+ * initialisers do (IO/VoF_Init.c), before Particle_initialize and
+ * VOF_DIFFUSE_init.
+ *
+ * Usage: ibm_driver <case_dir> <dt> <stage> [routines|mcl|steps] [nsteps]
  *   files of ref_driver.c, plus particles_fixed.txt and particles_mobile.txt:
  *   one particle per line, "X Y R U V Omega_z".
  * Test infrastructure only.
@@ -131,12 +152,96 @@ static void dump_fields(Cart3d_bag *db, const char *tag, int rhs)
 #undef DN
 }
 
+static void dump_tag(double ***a, MAC_grid *g, const char *tag, const char *name)
+{
+    char path[512];
+    snprintf(path, sizeof(path), "out/%s_%s.bin", tag, name);
+    dump(a, g, path);
+}
+
+/* the contact-line routines on the state VOF_DIFFUSE_init hands to its own
+ * VOF_DIFFUSE_apply_contact_angle call (VOF_DIFFUSE.c:523-568) */
+static void run_mcl(Cart3d_bag *db, const double *F0)
+{
+    MAC_grid *g = db->grid;
+    VolumeFraction *vof = db->vof;
+    inject(vof->F, F0, g);
+    VOF_DIFFUSE_set_boundary_values(vof->F, db);
+    for (int k = g->L_Ks; k < g->L_Ke; ++k)
+        for (int j = g->L_Js; j < g->L_Je; ++j)
+            for (int i = g->L_Is; i < g->L_Ie; ++i) {
+                double f = vof->F[k][j][i];
+                vof->C_L[k][j][i] = f < 0.0 ? 0.0 : (f > 1.0 ? 1.0 : f);
+            }
+    VOF_DIFFUSE_set_boundary_values(vof->C_L, db);
+    VOF_DIFFUSE_update_phase_cache(db);
+    /* diffuse_bound_liquid_fraction (VOF_DIFFUSE.c:1093-1127, static there) */
+    for (int k = g->G_Ks; k < g->G_Ke; ++k)
+        for (int j = g->G_Js; j < g->G_Je; ++j)
+            for (int i = g->G_Is; i < g->G_Ie; ++i) {
+                double cs = vof->C_S[k][j][i], cl = vof->C_L[k][j][i];
+                double mx = 1.0 - cs;
+                if (mx < 0.0) mx = 0.0;
+                if (mx > 1.0) mx = 1.0;
+                if (cl < 0.0) cl = 0.0;
+                if (cl > mx) cl = mx;
+                vof->C_L[k][j][i] = cl;
+                double cg = 1.0 - cl - cs;
+                vof->C_G[k][j][i] = cg < 0.0 ? 0.0 : (cg > 1.0 ? 1.0 : cg);
+            }
+    VOF_DIFFUSE_set_boundary_values(vof->C_L, db);
+    VOF_DIFFUSE_update_phase_cache(db);
+    dump_tag(vof->C_L, g, "m1", "C_L");
+    dump_tag(vof->C_G, g, "m1", "C_G");
+    dump_tag(vof->C_S, g, "m1", "C_S");
+    VOF_DIFFUSE_apply_contact_angle(db);
+    dump_tag(vof->C_L, g, "m2", "C_L");
+    dump_tag(vof->nx_IBM, g, "m2", "nx");
+    dump_tag(vof->ny_IBM, g, "m2", "ny");
+    VOF_DIFFUSE_set_boundary_values(vof->C_L, db);
+    VOF_DIFFUSE_update_phase_cache(db);
+    VOF_DIFFUSE_compute_psi_LG(db);
+    dump_tag(vof->psi_LG, g, "m3", "psi_LG");
+    dump_tag(vof->C_L, g, "m3", "C_L");
+    dump_tag(vof->C_G, g, "m3", "C_G");
+    VOF_DIFFUSE_extend_psi_LG_contact_angle(db);
+    dump_tag(vof->psi_LG, g, "m4", "psi_LG");
+}
+
+/* whole time steps as ref_driver.c takes them (Temporal_int.c:399-448) */
+static void run_steps(Cart3d_bag *db, int nsteps, double dt, Debug_trace *dtrace)
+{
+    Parameters *params = db->params;
+    const double BET2[] = {BETA2};
+    double time = 0.0;
+    params->time = 0.0;
+    dump_state(db, "s0");
+    for (int n = 1; n <= nsteps; n++) {
+        for (int rk = 0; rk < 3; rk++) {
+            if (time != 0 && rk == 0)
+                Velocity_cell_center(db);
+            params->which_stage = rk;
+            params->dt = dt;
+            Temporal_int_all_the_equations(db, DTRACE("Temporal_int_all_the_equations"));
+            time += dt * BET2[rk];
+            params->time = time;
+        }
+        params->ntime = n;
+        char tag[64];
+        snprintf(tag, sizeof(tag), "s%d", n);
+        dump_state(db, tag);
+        dump_particles(db, tag);
+    }
+}
+
 int main(int argc, char **argv)
 {
-    if (argc < 4) die("usage: ibm_driver <case_dir> <dt> <stage>");
+    if (argc < 4) die("usage: ibm_driver <case_dir> <dt> <stage> [routines|mcl|steps] [nsteps]");
     const char *case_dir = argv[1];
     double dt = atof(argv[2]);
     int stage = atoi(argv[3]);
+    const char *mode = (argc > 4) ? argv[4] : "routines";
+    int nsteps = (argc > 5) ? atoi(argv[5]) : 1;
     if (chdir(case_dir) != 0) die("cannot enter the case directory");
     mkdir("out", 0755);
 
@@ -164,9 +269,10 @@ int main(int argc, char **argv)
 
     int NX = grid->NX, NY = grid->NY;
     double *plane;
-    if (!(plane = read_plane("init_C.bin", NX * NY))) die("missing init_C.bin");
-    inject(db->vof->F, plane, grid);
-    free(plane);
+    double *F0;
+    if (!(F0 = read_plane("init_C.bin", NX * NY))) die("missing init_C.bin");
+    inject(db->vof->F, F0, grid);
+    inject(db->vof->C_L, F0, grid);
     if ((plane = read_plane("init_u.bin", NX * NY))) { inject(db->u->data, plane, grid); free(plane); }
     if ((plane = read_plane("init_v.bin", NX * NY))) { inject(db->v->data, plane, grid); free(plane); }
     if ((plane = read_plane("init_p.bin", NX * NY))) { inject(db->p->p_data, plane, grid); free(plane); }
@@ -184,6 +290,15 @@ int main(int argc, char **argv)
     VOF_DIFFUSE_set_boundary_values(db->vof->F, db);
     VOF_DIFFUSE_init(db);
     VOF_update_density_viscosity(db);
+#ifdef SURFACE_TENSION
+    /* Cart3d.c:1110-1125 */
+    VOF_DIFFUSE_compute_psi_LG(db);
+    VOF_DIFFUSE_extend_psi_LG_contact_angle(db);
+    VOF_DIFFUSE_compute_f_sigma(db);
+    Array_copy_noghost(db->vof->f_sigma_new_x, db->vof->f_sigma_old_x, grid, params);
+    Array_copy_noghost(db->vof->f_sigma_new_y, db->vof->f_sigma_old_y, grid, params);
+    Array_copy_noghost(db->vof->f_sigma_new_z, db->vof->f_sigma_old_z, grid, params);
+#endif
     Velocity_cell_center(db);
 
     {
@@ -198,6 +313,18 @@ int main(int argc, char **argv)
         D(db->v->data, "v");
 #undef D
     }
+
+    if (!strcmp(mode, "mcl")) {
+        run_mcl(db, F0);
+        printf("IBM_DONE mcl\n");
+        return 0;
+    }
+    if (!strcmp(mode, "steps")) {
+        run_steps(db, nsteps, dt, dtrace);
+        printf("IBM_DONE steps=%d\n", nsteps);
+        return 0;
+    }
+    if (strcmp(mode, "routines")) die("unknown mode");
 
     params->which_stage = stage;
     params->dt = dt;

@@ -195,6 +195,16 @@ void axis_map(Map1 &m, int kind, int N, bool periodic, int wall_lo, int wall_hi,
             m.set(N - 1, N - 2, wall_hi == PVOF_WALL_NOSLIP ? -1.0 : 1.0);
         }
         break;
+    case BK_NRM_X:
+    case BK_NRM_Y: {  // mcl_apply_normal_parity (VOF_IBM_wetting.c:914-1016), planar mode
+        // mirrored across a free-slip wall; the component normal to the wall flips
+        const double sgn = ((kind == BK_NRM_X) == is_x) ? -1.0 : 1.0;
+        if (wall_lo == PVOF_WALL_FREESLIP && !axisym_lo)
+            for (int g = 1; g <= NG; g++) m.set(-g, g - 1, sgn);
+        if (wall_hi == PVOF_WALL_FREESLIP)
+            for (int g = 0; g < NG; g++) m.set(N - 1 + g, N - 2 - g, sgn);
+        break;
+    }
     default:  // exchange-only kinds on a walled axis: nothing
         break;
     }
@@ -284,6 +294,9 @@ void collect_solver_timing(pvof_ctx *c)
 }
 
 double *F(pvof_ctx *c, int id) { return c->f[id]; }
+// resolved solid particles on (the reference's VOF_IBM and LAG_PARTICLE_RESOLVED
+// builds): from the first pvof_set_particles call on, even with no particles
+int resolved(const pvof_ctx *c) { return c->ibm != nullptr; }
 double *S(pvof_ctx *c, int id) { return c->s[id]; }
 
 // loop ranges of the face-centred arrays (e.g. Velocity.c:395-410)
@@ -345,8 +358,18 @@ int bound(pvof_ctx *c)
     return PVOF_OK;
 }
 
+// resolved-particle routines (defined with the particle bookkeeping below)
+int compute_C_S(pvof_ctx *c);
+int apply_contact_angle(pvof_ctx *c);
+int extend_psi_LG(pvof_ctx *c);
+int ibm_flag_points(pvof_ctx *c);
+int ibm_force(pvof_ctx *c, int force_iter);
+int vel_explicit(pvof_ctx *c, int comp);
+
+// VOF_DIFFUSE_init (VOF_DIFFUSE.c:523-568)
 int vof_diffuse_init(pvof_ctx *c)
 {
+    if (resolved(c)) TRY(compute_C_S(c));
     size_t n = c->plane_elems;
     k_clamp_from<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, c->base[PVOF_F_F], c->base[PVOF_F_C_L]);
     CKL(c);
@@ -355,6 +378,7 @@ int vof_diffuse_init(pvof_ctx *c)
     TRY(bound(c));
     TRY(fill(c, BK_SCALAR, F(c, PVOF_F_C_L)));
     TRY(phase_cache(c));
+    if (resolved(c)) TRY(apply_contact_angle(c));
     TRY(fill(c, BK_SCALAR, F(c, PVOF_F_C_L)));
     TRY(phase_cache(c));
     return fill(c, BK_SCALAR, F(c, PVOF_F_C_G));
@@ -405,6 +429,14 @@ int vof_diffuse_step(pvof_ctx *c)
     TRY(bound(c));
     TRY(fill(c, BK_SCALAR, CL));
     TRY(phase_cache(c));
+    if (resolved(c) && s == 2) {
+        // contact-angle projection once per time step, then C_L + C_S <= 1
+        TRY(apply_contact_angle(c));
+        TRY(fill(c, BK_SCALAR, CL));
+        TRY(bound(c));
+        TRY(fill(c, BK_SCALAR, CL));
+        TRY(phase_cache(c));
+    }
     size_t bytes = c->plane_elems * sizeof(double);
     CK(cudaMemcpyAsync(c->sbase[SC_CH_RHS_NM1], c->base[PVOF_F_CH_RHS_N], bytes,
                        cudaMemcpyDeviceToDevice, c->stream));
@@ -510,13 +542,14 @@ int set_rhs(pvof_ctx *c, int comp)
                         (const double *)F(c, PVOF_F_RHO), F(c, PVOF_F_U_RHS), (const double *)F(c, PVOF_F_U_EXPLICIT),
                         F(c, PVOF_F_U_EXPLICIT_OLD), (const double *)F(c, PVOF_F_U_VISC_EXPLICIT),
                         F(c, PVOF_F_U_VISC_EXPLICIT_OLD), (const double *)F(c, PVOF_F_U_IMPLICIT), a_dt, s,
-                        -c->p.dp_dx);
+                        -c->p.dp_dx, resolved(c));
     }
     v_range(c, i0, i1, j0, j1);
     return launch2d(c, k_set_rhs, i0, i1, j0, j1, 1, (const double *)F(c, PVOF_F_V), (const double *)F(c, PVOF_F_P),
                     (const double *)F(c, PVOF_F_RHO), F(c, PVOF_F_V_RHS), (const double *)F(c, PVOF_F_V_EXPLICIT),
                     F(c, PVOF_F_V_EXPLICIT_OLD), (const double *)F(c, PVOF_F_V_VISC_EXPLICIT),
-                    F(c, PVOF_F_V_VISC_EXPLICIT_OLD), (const double *)F(c, PVOF_F_V_IMPLICIT), a_dt, s, -c->p.dp_dx);
+                    F(c, PVOF_F_V_VISC_EXPLICIT_OLD), (const double *)F(c, PVOF_F_V_IMPLICIT), a_dt, s, -c->p.dp_dx,
+                    resolved(c));
 }
 
 VelArgs vel_args(pvof_ctx *c, int comp)
@@ -690,6 +723,7 @@ int initialize(pvof_ctx *c)
     TRY(update_density_viscosity(c));
     if (c->p.surface_tension) {
         TRY(compute_psi_LG(c));
+        if (resolved(c)) TRY(extend_psi_LG(c));
         TRY(compute_f_sigma(c));
         size_t bytes = c->plane_elems * sizeof(double);
         CK(cudaMemcpyAsync(c->base[PVOF_F_FSIG_OLD_X], c->base[PVOF_F_FSIG_NEW_X], bytes, cudaMemcpyDeviceToDevice, c->stream));
@@ -700,12 +734,18 @@ int initialize(pvof_ctx *c)
     return PVOF_OK;
 }
 
-// Temporal_int_all_the_equations (Temporal_int.c:563-1279), no solids
+// Temporal_int_all_the_equations (Temporal_int.c:563-1279); with resolved
+// particles the branches of VOF_IBM and LAG_PARTICLE_RESOLVED
 int substep(pvof_ctx *c, pvof_stats *st)
 {
+    const bool solids = resolved(c);
     if (c->stage > 0) TRY(cell_center(c));
     TRY(fill(c, BK_WRAP_C, F(c, PVOF_F_U_BC)));
     TRY(fill(c, BK_WRAP_C, F(c, PVOF_F_V_BC)));
+    if (solids) {
+        TRY(ibm_flag_points(c));   // Particle_MPI_update of both lists, Lagrangian_flag_points
+        TRY(compute_C_S(c));
+    }
     TRY(vof_diffuse_step(c));
     TRY(update_density_viscosity(c));
     TRY(implicit_explicit(c, 0));
@@ -714,13 +754,28 @@ int substep(pvof_ctx *c, pvof_stats *st)
     TRY(set_rhs(c, 1));
     if (c->p.surface_tension) {
         TRY(compute_psi_LG(c));
+        if (solids && c->stage == 2) TRY(extend_psi_LG(c));
         TRY(compute_f_sigma(c));
         TRY(apply_f_sigma_old(c));
     }
     if (c->p.gravity) TRY(add_gravity(c));
+    if (solids) {
+        // explicit predictor and direct forcing on the right-hand side (Temporal_int.c:948-980)
+        TRY(vel_explicit(c, 0));
+        TRY(vel_explicit(c, 1));
+        TRY(fill(c, BK_U, F(c, PVOF_F_U)));
+        TRY(fill(c, BK_V, F(c, PVOF_F_V)));
+        TRY(ibm_force(c, -1));
+    }
     TRY(velocity_solve_both(c));
     TRY(fill(c, BK_U, F(c, PVOF_F_U)));
     TRY(fill(c, BK_V, F(c, PVOF_F_V)));
+    if (solids) {
+        // forcing correctors on the velocity (Temporal_int.c:1008-1022)
+        TRY(ibm_force(c, c->p.N_forcing_loops));
+        TRY(fill(c, BK_U, F(c, PVOF_F_U)));
+        TRY(fill(c, BK_V, F(c, PVOF_F_V)));
+    }
     int passes = 0, p_total = 0;
     int rc = PVOF_OK;
     for (;;) {
@@ -768,9 +823,13 @@ struct pvof::IbmState {
     double *d_geo = nullptr;
     size_t cap_geo = 0;
     int ngeo = 0;
+    double *d_plist = nullptr;             // x, y, R, ID of the current list entries (contact-line normals)
+    size_t cap_plist = 0;
+    int n_plist = 0;
     bool flagged = false;
     ~IbmState()
     {
+        cudaFree(d_plist);
         cudaFree(d_coord);
         cudaFree(d_ent);
         cudaFree(d_mk);
@@ -820,11 +879,47 @@ int ibm_state(pvof_ctx *c, IbmState **out)
     return PVOF_OK;
 }
 
+// the particle state of a context in the resolved-particle mode
+int ibm_need(pvof_ctx *c, IbmState **out)
+{
+    if (!c->ibm) return set_err(PVOF_EINVAL, "pvof_set_particles() first");
+    *out = c->ibm;
+    return PVOF_OK;
+}
+
+// the entries the reference's particle lists hold at this point, in list
+// order (mobile list, then fixed), for mcl_nearest_particle_normal
+// (VOF_IBM_wetting.c:118-182): the owned particles until the first list
+// update of a substep, the updated lists (with periodic copies) after it
+int ibm_upload_plist(IbmState *s, const std::vector<const IbmEntry *> &list)
+{
+    std::vector<double> h;
+    h.reserve(4 * list.size());
+    for (const IbmEntry *e : list) {
+        h.push_back(e->X[0]);
+        h.push_back(e->X[1]);
+        h.push_back(e->R);
+        h.push_back((double)e->id);
+    }
+    if (h.size() > s->cap_plist) {
+        cudaFree(s->d_plist);
+        s->d_plist = nullptr;
+        if (cudaMalloc(&s->d_plist, h.size() * sizeof(double)) != cudaSuccess) {
+            s->cap_plist = 0;
+            return set_err(PVOF_ENOMEM, "cudaMalloc particle list");
+        }
+        s->cap_plist = h.size();
+    }
+    if (!h.empty()) CK(cudaMemcpy(s->d_plist, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    s->n_plist = (int)list.size();
+    return PVOF_OK;
+}
+
 // Particle_MPI_update of both lists and Lagrangian_flag_points (Temporal_int.c:678-681)
 int ibm_flag_points(pvof_ctx *c)
 {
     IbmState *s;
-    TRY(ibm_state(c, &s));
+    TRY(ibm_need(c, &s));
     ibm_build(s->mobile, s->fixed, s->grid, c->p.Cn, s->entries, s->markers);
     const size_t ne = s->entries.size(), nm = s->markers.x.size();
     if (ne > s->cap_ent) {
@@ -875,6 +970,9 @@ int ibm_flag_points(pvof_ctx *c)
         CK(cudaMemcpyAsync(s->d_flag, s->markers.flag.data(), nm * sizeof(int), cudaMemcpyHostToDevice, c->stream));
     }
     CK(cudaStreamSynchronize(c->stream));   // the host vectors may change with the next update
+    std::vector<const IbmEntry *> cur;
+    for (const IbmEntry &e : s->entries) cur.push_back(&e);
+    TRY(ibm_upload_plist(s, cur));
     s->flagged = true;
     return PVOF_OK;
 }
@@ -984,7 +1082,7 @@ int vel_explicit(pvof_ctx *c, int comp)
 int compute_C_S(pvof_ctx *c)
 {
     IbmState *s;
-    TRY(ibm_state(c, &s));
+    TRY(ibm_need(c, &s));
     std::vector<double> geo;
     ibm_solid_geometry(s->mobile, s->fixed, s->grid, geo);
     if (geo.size() > s->cap_geo) {
@@ -1015,6 +1113,84 @@ int compute_C_S(pvof_ctx *c)
 }
 
 // Pressure_solve_xz_period (psolve_fft.c:638-983) in the planar mode
+// contact-line projection (VOF_IBM_wetting.c:1021-2131; kernels in pvof_mcl.cu)
+int mcl_normals(pvof_ctx *c)
+{
+    IbmState *s;
+    TRY(ibm_need(c, &s));
+    const Dom &d = c->dom;
+    const double h_ref = (s->grid.dy_min > 0.0) ? s->grid.dy_min : 1.0e-14;
+    const double cn = (c->p.Cn > 0.0) ? c->p.Cn : 0.0;
+    const double support_width = 8.0 * ((cn > h_ref) ? cn : h_ref);
+    const dim3 blk(128), grd((unsigned)((d.NX + 2 * NG + 127) / 128), (unsigned)(d.NY + 2 * NG));
+    k_mcl_normals<<<grd, blk, 0, c->stream>>>(d, s->xc, s->yc, F(c, PVOF_F_C_S), s->d_plist, s->n_plist,
+                                              support_width, F(c, PVOF_F_NX_IBM), F(c, PVOF_F_NY_IBM));
+    CKL(c);
+    TRY(fill(c, BK_NRM_X, F(c, PVOF_F_NX_IBM)));
+    return fill(c, BK_NRM_Y, F(c, PVOF_F_NY_IBM));
+}
+
+MclView mcl_view(pvof_ctx *c, const double *CL, const double *field)
+{
+    IbmState *s = c->ibm;
+    MclView v;
+    v.NX = c->dom.NX;
+    v.NY = c->dom.NY;
+    v.perx = c->dom.perx;
+    v.pery = c->dom.pery;
+    v.free_lo_x = !v.perx && c->g.wall[PVOF_LEFT] == PVOF_WALL_FREESLIP;
+    v.free_hi_x = !v.perx && c->g.wall[PVOF_RIGHT] == PVOF_WALL_FREESLIP;
+    v.free_lo_y = !v.pery && c->g.wall[PVOF_BOTTOM] == PVOF_WALL_FREESLIP;
+    v.free_hi_y = !v.pery && c->g.wall[PVOF_TOP] == PVOF_WALL_FREESLIP;
+    v.xc = s->xc;
+    v.yc = s->yc;
+    // theta and its cosine and sine as the reference forms them (:1987-1988)
+    const double theta = c->p.contact_angle_deg * M_PI / 180.0;
+    v.ct = std::cos(theta);
+    v.st = std::sin(theta);
+    v.hydrophilic = theta <= 0.5 * M_PI;
+    // mcl_lg_band_limits (:862-877)
+    v.cmin = 0.005;
+    v.cmax = 0.995;
+    if (c->p.contact_angle_deg > 0.0 && c->p.contact_angle_deg < 45.0) {
+        v.cmin = 0.05;
+        v.cmax = 0.95;
+    }
+    v.CS = F(c, PVOF_F_C_S);
+    v.CG = F(c, PVOF_F_C_G);
+    v.CL = CL;
+    v.field = field;
+    return v;
+}
+
+// VOF_DIFFUSE_apply_contact_angle (:1946-2008): one pass over a snapshot of C_L
+int apply_contact_angle(pvof_ctx *c)
+{
+    TRY(mcl_normals(c));
+    double *CL = F(c, PVOF_F_C_L), *snap = S(c, SC_SNAP);
+    CK(cudaMemcpyAsync(c->sbase[SC_SNAP], c->base[PVOF_F_C_L], c->plane_elems * sizeof(double),
+                       cudaMemcpyDeviceToDevice, c->stream));
+    const MclView v = mcl_view(c, snap, snap);
+    const dim3 blk(128), grd((unsigned)((c->dom.NX + 127) / 128), (unsigned)c->dom.NY);
+    k_mcl_apply<<<grd, blk, 0, c->stream>>>(c->dom, v, F(c, PVOF_F_NX_IBM), F(c, PVOF_F_NY_IBM), CL);
+    CKL(c);
+    return PVOF_OK;
+}
+
+// VOF_DIFFUSE_extend_psi_LG_contact_angle (:2014-2131)
+int extend_psi_LG(pvof_ctx *c)
+{
+    TRY(mcl_normals(c));
+    double *psi = F(c, PVOF_F_PSI_LG), *snap = S(c, SC_SNAP);
+    CK(cudaMemcpyAsync(c->sbase[SC_SNAP], c->base[PVOF_F_PSI_LG], c->plane_elems * sizeof(double),
+                       cudaMemcpyDeviceToDevice, c->stream));
+    const MclView v = mcl_view(c, F(c, PVOF_F_C_L), snap);
+    const dim3 blk(128), grd((unsigned)((c->dom.NX + 127) / 128), (unsigned)c->dom.NY);
+    k_mcl_extend_psi<<<grd, blk, 0, c->stream>>>(c->dom, v, F(c, PVOF_F_NX_IBM), F(c, PVOF_F_NY_IBM), psi);
+    CKL(c);
+    return fill(c, BK_SCALAR, psi);
+}
+
 int p_solve_fft(pvof_ctx *c)
 {
     const Dom &d = c->dom;
@@ -1094,6 +1270,7 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     if (grid->NXM < 8 || grid->NYM < 8) return set_err(PVOF_EINVAL, "at least 8 cells per direction");
     if (grid->geometry == PVOF_GEOM_AXISYM && grid->periodic[0]) return set_err(PVOF_EINVAL, "the axis cannot be periodic");
     if (params->Re <= 0 || params->Pe_CH <= 0 || params->Cn <= 0) return set_err(PVOF_EINVAL, "Re, Pe_CH and Cn must be positive");
+    if (params->N_forcing_loops < 0) return set_err(PVOF_EINVAL, "N_forcing_loops must not be negative");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(PVOF_ENODEV, "no CUDA device");
     if (device < 0 || device >= ndev) return set_err(PVOF_EINVAL, "bad device index");
@@ -1561,7 +1738,10 @@ int pvof_set_particles(pvof_ctx *c, const pvof_particle *parts, int n)
     for (IbmEntry &e : s->fixed) e.id = id++;
     for (IbmEntry &e : s->mobile) e.id = id++;
     s->flagged = false;
-    return PVOF_OK;
+    std::vector<const IbmEntry *> cur;
+    for (const IbmEntry &e : s->mobile) cur.push_back(&e);
+    for (const IbmEntry &e : s->fixed) cur.push_back(&e);
+    return ibm_upload_plist(s, cur);
 }
 
 int pvof_Lagrangian_flag_points(pvof_ctx *c) { ENTER(c); return ibm_flag_points(c); }
@@ -1610,6 +1790,9 @@ int pvof_particle_markers(pvof_ctx *c, int entry, double *x, double *y, double *
 }
 
 int pvof_VOF_DIFFUSE_compute_C_S(pvof_ctx *c) { ENTER(c); return compute_C_S(c); }
+int pvof_VOF_DIFFUSE_compute_solid_normals_MCL(pvof_ctx *c) { ENTER(c); return mcl_normals(c); }
+int pvof_VOF_DIFFUSE_apply_contact_angle(pvof_ctx *c) { ENTER(c); return apply_contact_angle(c); }
+int pvof_VOF_DIFFUSE_extend_psi_LG_contact_angle(pvof_ctx *c) { ENTER(c); return extend_psi_LG(c); }
 
 int pvof_Velocity_solve_explicit(pvof_ctx *c, char component)
 {

@@ -39,6 +39,8 @@ enum BcKind {
     BK_WRAP_C,       // exchange only, scalar component (Communication.c:146-291)
     BK_WRAP_U,       // exchange only, x-face component (U_VELOCITY, FLUX_X)
     BK_WRAP_V,       // exchange only, y-face component (V_VELOCITY, FLUX_Y)
+    BK_NRM_X,        // contact-line solid normal, x component (VOF_IBM_wetting.c:914-1016)
+    BK_NRM_Y,        // same, y component
     BK_COUNT
 };
 
@@ -83,7 +85,7 @@ enum Scratch {
     SC_PSI = 0, SC_BULK_S, SC_CH_AUX1, SC_CH_RHS_NM1, SC_CH_RES, SC_CH_DIR, SC_CH_DIR2,
     SC_FLUX_X, SC_FLUX_Y, SC_P_RES, SC_P_D, SC_P_AD, SC_P_MINV,
     SC_U_R, SC_U_D, SC_U_AD, SC_U_DIAG, SC_V_R, SC_V_D, SC_V_AD, SC_V_DIAG,
-    SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_COUNT
+    SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_SNAP, SC_COUNT
 };
 
 // device-side scalars written by solver kernels and read once per substep

@@ -363,7 +363,8 @@ __global__ void k_v_impexp(Dom d, int i0, int i1, int j0, int j1, const double *
 __global__ void k_set_rhs(Dom d, int i0, int i1, int j0, int j1, int comp, const double *__restrict__ data,
                           const double *__restrict__ pd, const double *__restrict__ rho, double *__restrict__ rhs,
                           const double *__restrict__ ex, double *__restrict__ exo, const double *__restrict__ vx,
-                          double *__restrict__ vxo, const double *__restrict__ im, double a_dt, int s, double dp_src)
+                          double *__restrict__ vxo, const double *__restrict__ im, double a_dt, int s, double dp_src,
+                          int resolved)
 {
     KERNEL_2D_INDEX
     double dp, rf;
@@ -378,6 +379,9 @@ __global__ void k_set_rhs(Dom d, int i0, int i1, int j0, int j1, int comp, const
     double conv = gamb(s) * e + zetb(s) * eo;
     conv *= rf;
     double r = rf * a_dt * AT_(data, i, j) + conv + AT_(im, i, j) + (gamb(s) * v + zetb(s) * vo) - 2.0 * dp;
+    // with resolved particles the implicit part goes in twice; Lagrangian_force(-1)
+    // takes the second copy out again (Velocity.c:1665-1667, Lagrangian.c:1855-1867)
+    if (resolved) r += AT_(im, i, j);
     if (comp == 0 && d.perx) r += 2.0 * dp_src;
     AT_(rhs, i, j) = r;
     AT_(exo, i, j) = e;

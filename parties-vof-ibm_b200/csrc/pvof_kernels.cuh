@@ -77,7 +77,7 @@ __global__ void k_v_impexp(Dom d, int i0, int i1, int j0, int j1, const double *
                            const double *mu, double *ex, double *im, double *vx, double iRe);
 __global__ void k_set_rhs(Dom d, int i0, int i1, int j0, int j1, int comp, const double *data, const double *pd,
                           const double *rho, double *rhs, const double *ex, double *exo, const double *vx, double *vxo,
-                          const double *im, double a_dt, int s, double dp_src);
+                          const double *im, double a_dt, int s, double dp_src, int resolved);
 __global__ void k_p_rhs(Dom d, int i0, int i1, int j0, int j1, const double *u, const double *v, double *rhs, double ihdt);
 __global__ void k_p_precond(Dom d, int i0, int i1, int j0, int j1, const double *rho, double *M);
 __global__ void k_p_update(Dom d, int i0, int i1, int j0, int j1, double *pd, const double *dp);
@@ -166,6 +166,24 @@ void ibm_build(const std::vector<IbmEntry> &mobile_local, const std::vector<IbmE
 void ibm_solid_geometry(const std::vector<IbmEntry> &mobile_local, const std::vector<IbmEntry> &fixed_local,
                         const IbmGrid &g, std::vector<double> &geo);
 void ibm_solid_constants(double cn, double &shift, double &denom, double &extra);
+
+// contact-line projection (pvof_mcl.cu): the G-range scalars of one pass and
+// the case constants; CL and field are the pass's snapshots
+struct MclView {
+    int NX, NY;
+    int perx, pery;
+    int free_lo_x, free_hi_x, free_lo_y, free_hi_y;   // free-slip walls (mirror maps)
+    const double *xc, *yc;                            // offset by NG, valid on [-NG, N + NG)
+    double ct, st;                                    // cos, sin of the contact angle
+    int hydrophilic;                                  // theta <= pi / 2
+    double cmin, cmax;                                // liquid-gas band
+    const double *CS, *CG, *CL, *field;
+};
+
+__global__ void k_mcl_normals(Dom d, const double *xc, const double *yc, const double *CS, const double *plist,
+                              int np, double support_width, double *nxo, double *nyo);
+__global__ void k_mcl_apply(Dom d, MclView v, const double *nxa, const double *nya, double *CLout);
+__global__ void k_mcl_extend_psi(Dom d, MclView v, const double *nxa, const double *nya, double *PSIout);
 
 __global__ void k_ibm_interp(Dom d, const double *a, const double *xs, const double *ys, double h, const double *XL,
                              const double *YL, int nm, double *out);

@@ -5,7 +5,7 @@ field; tests/test_abi.py checks the exported symbols and the sizes.
 """
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 EINVAL = -1
@@ -34,6 +34,7 @@ FIELD_NAMES = [
     "V_EXPLICIT", "V_EXPLICIT_OLD", "V_IMPLICIT",
     "V_VISC_EXPLICIT", "V_VISC_EXPLICIT_OLD", "V_RHS",
     "FSIG_OLD_X", "FSIG_OLD_Y", "FSIG_NEW_X", "FSIG_NEW_Y",
+    "NX_IBM", "NY_IBM",
 ]
 FIELD = {name: idx for idx, name in enumerate(FIELD_NAMES)}
 FIELD_COUNT = len(FIELD_NAMES)
@@ -74,6 +75,8 @@ class Params(C.Structure):
         ("P_CG_ETOL", C.c_double),
         ("surface_tension", C.c_int),
         ("gravity", C.c_int),
+        ("contact_angle_deg", C.c_double),
+        ("N_forcing_loops", C.c_int),
     ]
 
 
@@ -124,6 +127,8 @@ EXPORTS = [
     "pvof_set_particles", "pvof_Lagrangian_flag_points", "pvof_particle_entries", "pvof_particle_forces",
     "pvof_particle_markers", "pvof_VOF_DIFFUSE_compute_C_S", "pvof_Velocity_solve_explicit",
     "pvof_Lagrangian_force", "pvof_Pressure_solve_fft", "pvof_run_steps_batched",
+    "pvof_VOF_DIFFUSE_compute_solid_normals_MCL", "pvof_VOF_DIFFUSE_apply_contact_angle",
+    "pvof_VOF_DIFFUSE_extend_psi_LG_contact_angle",
 ]
 
 SOLVER_BIHARMONIC = 0

@@ -80,6 +80,8 @@ def default_params(**kw):
     p.P_CG_ETOL = 1e-7
     p.surface_tension = 0
     p.gravity = 1
+    p.contact_angle_deg = 90.0
+    p.N_forcing_loops = 2
     for k, v in kw.items():
         setattr(p, k, v)
     return p

@@ -75,6 +75,9 @@ def load():
     L.pvof_Velocity_solve_explicit.argtypes = [V, C.c_char]
     L.pvof_Lagrangian_force.argtypes = [V, C.c_int]
     L.pvof_Pressure_solve_fft.argtypes = [V]
+    L.pvof_VOF_DIFFUSE_compute_solid_normals_MCL.argtypes = [V]
+    L.pvof_VOF_DIFFUSE_apply_contact_angle.argtypes = [V]
+    L.pvof_VOF_DIFFUSE_extend_psi_LG_contact_angle.argtypes = [V]
     L.pvof_run_steps_batched.argtypes = [P(V), C.c_int, C.c_int, C.c_double, P(abi.Stats)]
     L.pvof_solver_kernel.restype = C.c_char_p
     _lib = L

@@ -5,7 +5,9 @@ oracle/ref/Makefile into oracle/_ref/ref_<case>, on small seeded cases and
 stores the inputs, parameters, solver iteration counts and the fields after
 every RK substep in tests/golden/<name>.npz.  The resolved-particle fixtures
 (IBM_CASES) hold the inputs and outputs of the immersed-boundary routines of
-one substep, from the routine driver oracle/ref/ibm_driver.c.
+one substep, from the routine driver oracle/ref/ibm_driver.c; the contact-line
+fixtures (MCL_CASES) those of the contact-angle projection and the psi_LG
+extension, from the same driver's "mcl" mode.
 
     python tests/golden/make_golden.py [--refsrc PATH]
 
@@ -52,6 +54,28 @@ CASES = [
 IBM_CASES = [
     ("ibm_small", dict(NXM=32, NYM=128, Lx=1.0, Ly=4.0, Cn=0.04, velocity_seed=7, velocity_amp=0.1),
      [(0, 0.06, 1.2, 0.2, 0.0, 0.0, 0.0, 2.5), (1, 0.55, 2.7, 0.15, 0.2, -0.1, 0.7, 2.5)], 1e-3, 1),
+]
+
+# contact-line cases (oracle/ref/ibm_driver.c "mcl" mode on the ibm2d build):
+# name, builder arguments, particles, contact angle in degrees.  Two fixed
+# cylinders sit on the interface (one across the periodic x boundary) and a
+# small mobile one just below it.
+MCL_PARTICLES = [(0, 0.5, 1.0, 0.2, 0.0, 0.0, 0.0, 2.5), (0, 0.03, 1.04, 0.15, 0.0, 0.0, 0.0, 2.5),
+                 (1, 0.78, 0.98, 0.07, 0.0, 0.0, 0.0, 2.5)]
+MCL_GRID = dict(NXM=48, NYM=96, Lx=1.0, Ly=2.0, Cn=0.04)
+MCL_CASES = [("mcl_theta60", MCL_GRID, MCL_PARTICLES, 60.0),
+             ("mcl_theta120", MCL_GRID, MCL_PARTICLES, 120.0),
+             ("mcl_theta30", MCL_GRID, MCL_PARTICLES, 30.0)]
+
+# whole time steps with fixed resolved cylinders (oracle/ref/ibm_driver.c
+# "steps" mode): name, reference build, builder arguments, particles, contact
+# angle, steps, dt.  Solver tolerances near machine precision.
+IBM_STEP_PARTICLES = [(0, 0.5, 1.0, 0.2, 0.0, 0.0, 0.0, 2.5), (0, 0.03, 1.04, 0.15, 0.0, 0.0, 0.0, 2.5)]
+IBM_STEP_CASES = [
+    ("ibm_steps_st", "ibm2d_st", dict(NXM=32, NYM=64, Lx=1.0, Ly=2.0, Cn=0.04, surface_tension=True, We=100.0,
+                                      velocity_seed=13, velocity_amp=0.1, **TIGHT), IBM_STEP_PARTICLES, 60.0, 2, 1e-3),
+    ("ibm_steps", "ibm2d", dict(NXM=32, NYM=64, Lx=1.0, Ly=2.0, Cn=0.04, velocity_seed=17, velocity_amp=0.1, **TIGHT),
+     IBM_STEP_PARTICLES, 120.0, 2, 1e-3),
 ]
 
 # constant-density FFT Poisson cases (oracle/ref/fft_driver.c on the fft2d build):
@@ -156,6 +180,69 @@ def make_ibm(name, kw, particles, dt, stage, outdir, refsrc=None):
     return path
 
 
+def make_mcl(name, kw, particles, theta, outdir, refsrc=None):
+    grid, params, planes = cases.rayleigh_taylor(**kw)
+    params.contact_angle_deg = theta
+    if not os.path.exists(po.ref_binary("ibm2d")):
+        po.build_reference("ibm2d", refsrc)
+    fixed = [p[1:7] for p in particles if not p[0]]
+    mobile = [p[1:7] for p in particles if p[0]]
+    data = {}
+    with tempfile.TemporaryDirectory() as wd:
+        po.run_reference_ibm(wd, grid, params, planes, fixed, mobile, 1e-3, 0, mode="mcl")
+        for tag, names in (("i0", ["C_S", "C_L", "C_G"]), ("m1", ["C_L", "C_G", "C_S"]),
+                           ("m2", ["C_L", "nx", "ny"]), ("m3", ["psi_LG", "C_L", "C_G"]), ("m4", ["psi_LG"])):
+            for fname in names:
+                data["%s/%s" % (tag, fname)] = po.read_reference_field(wd, tag, fname, grid)
+    for k, v in planes.items():
+        data["init/" + k] = v
+    meta = {"grid": struct_to_dict(grid), "params": struct_to_dict(params), "particles": [list(p) for p in particles],
+            "builder": kw, "refcase": "ibm2d"}
+    data["meta"] = np.array(repr(meta))
+    path = os.path.join(outdir, name + ".npz")
+    np.savez_compressed(path, **data)
+    return path
+
+
+def make_ibm_steps(name, refcase, kw, particles, theta, steps, dt, outdir, refsrc=None):
+    grid, params, planes = cases.rayleigh_taylor(**kw)
+    params.contact_angle_deg = theta
+    if not os.path.exists(po.ref_binary(refcase)):
+        po.build_reference(refcase, refsrc)
+    fixed = [p[1:7] for p in particles if not p[0]]
+    mobile = [p[1:7] for p in particles if p[0]]
+    st = bool(params.surface_tension)
+    data = {}
+    with tempfile.TemporaryDirectory() as wd:
+        cp = po.run_reference_ibm(wd, grid, params, planes, fixed, mobile, dt, 0, case=refcase, mode="steps",
+                                  nsteps=steps)
+        for tag in ["s%d" % n for n in range(steps + 1)]:
+            flow = dict(FLOW_FIELDS, C_S="C_S", **(ST_FLOW if st else {}))
+            ngf = dict(NG_FIELDS, **(ST_NG if st else {}))
+            for fname, pname in flow.items():
+                if fname == "C_S":
+                    if tag != "s0":
+                        continue
+                    a = po.read_reference_field(wd, "i0", "C_S", grid)
+                else:
+                    a = po.read_reference_field(wd, tag, fname, grid)
+                data["%s/%s" % (tag, pname)] = g_range(grid, a, False)
+            for fname, pname in ngf.items():
+                data["%s/%s" % (tag, pname)] = po.read_reference_field(wd, tag, fname, grid, ng=True)
+            if tag != "s0":
+                F, T = po.read_reference_particles(wd, tag)
+                data[tag + "/F"], data[tag + "/T"] = F, T
+        data["iterations"] = parse_iterations(cp.stdout)
+    for k, v in planes.items():
+        data["init/" + k] = v
+    meta = {"grid": struct_to_dict(grid), "params": struct_to_dict(params), "particles": [list(p) for p in particles],
+            "steps": steps, "dt": dt, "builder": kw, "refcase": refcase}
+    data["meta"] = np.array(repr(meta))
+    path = os.path.join(outdir, name + ".npz")
+    np.savez_compressed(path, **data)
+    return path
+
+
 def make_fft(name, NXM, NYM, Lx, Ly, seed, outdir, refsrc=None):
     """The reference's FFT solver runs in 3D with NZM = 2 (it needs an even
     z count) on a z-independent right-hand side; its k = 0 plane is the 2D
@@ -199,6 +286,12 @@ def main():
     for name, kw, parts, dt, stage in IBM_CASES:
         if ap_only is None or name in ap_only:
             print(make_ibm(name, kw, parts, dt, stage, a.out, a.refsrc))
+    for name, kw, parts, theta in MCL_CASES:
+        if ap_only is None or name in ap_only:
+            print(make_mcl(name, kw, parts, theta, a.out, a.refsrc))
+    for name, refcase, kw, parts, theta, steps, dt in IBM_STEP_CASES:
+        if ap_only is None or name in ap_only:
+            print(make_ibm_steps(name, refcase, kw, parts, theta, steps, dt, a.out, a.refsrc))
     for name, NXM, NYM, Lx, Ly, seed in FFT_CASES:
         if ap_only is None or name in ap_only:
             print(make_fft(name, NXM, NYM, Lx, Ly, seed, a.out, a.refsrc))
