@@ -278,6 +278,22 @@ int pvof_VOF_DIFFUSE_apply_contact_angle(pvof_ctx *ctx);
  * psi_LG in the same cells along the same characteristics, then its boundary
  * values */
 int pvof_VOF_DIFFUSE_extend_psi_LG_contact_angle(pvof_ctx *ctx);
+/* Lagrangian/Particle.c:322-535 Particle_initialize_velocities: mobile
+ * particles take the volume-averaged fluid velocity and the fluid inside them
+ * is painted to that rigid motion (pvof_initialize calls it) */
+int pvof_Particle_initialize_velocities(pvof_ctx *ctx);
+/* Temporal_int.c:1186-1238 and Lagrangian/Lagrangian.c:283-1640 the end of a
+ * substep: momentum integrals over the particles, the contact-line capillary
+ * force, Lagrangian_advect_particles (fluid forces, then the substepped
+ * rigid-body motion).  PVOF_EINVAL when two particles, or a particle and a
+ * wall, come within the lubrication range (the collision models are not part
+ * of this library).  pvof_substep calls it. */
+int pvof_Lagrangian_advect_particles(pvof_ctx *ctx);
+/* the owned particles in list order (mobile list, then fixed): position,
+ * velocity and spin in `out` (R, rho_s and mobile as given), their IDs and the
+ * total fluid force and torque of the last substep (3 doubles each); any of
+ * ids, F, T may be NULL; returns the count */
+int pvof_get_particles(pvof_ctx *ctx, pvof_particle *out, int *ids, double *F, double *T, int max_particles);
 /* Eulerian/lsolver/msolve_direct.c:146-260 Velocity_solve_explicit (u or v) */
 int pvof_Velocity_solve_explicit(pvof_ctx *ctx, char component);
 /* Lagrangian/Lagrangian.c:1724-1871 Lagrangian_force: force_iter < 0 is the

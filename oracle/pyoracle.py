@@ -236,6 +236,12 @@ def read_reference_particles(workdir, tag):
     return a[:, 0:3], a[:, 3:6]
 
 
+def read_reference_particle_state(workdir, tag):
+    """Per particle (lists in order, mobile first) ID, (X, Y), (U, V), Omega_z."""
+    a = np.loadtxt(os.path.join(workdir, "out", "particles_%s.txt" % tag), ndmin=2)
+    return a[:, 6].astype(np.int64), a[:, 7:9], a[:, 9:11], a[:, 11]
+
+
 def read_reference_field(workdir, tag, name, grid, ng=False):
     """k = 0 plane of a dumped field (full ghosted plane for flow fields)."""
     a = np.fromfile(os.path.join(workdir, "out", "%s_%s.bin" % (tag, name)), dtype="<f8")

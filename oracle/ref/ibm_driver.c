@@ -32,10 +32,13 @@
  *        phase cache of m2, and the C_L, C_G it was computed from
  *   m4   psi_LG after VOF_DIFFUSE_extend_psi_LG_contact_angle
  *
- * Mode "steps" runs <nsteps> whole time steps through the reference's own
- * substep routine Temporal_int_all_the_equations, as ref_driver.c does, and
- * dumps the state (dump_state of ref_driver.c) after every step, plus the
- * particle F and T (particles_s<n>.txt).
+ * Mode "steps" sets the particle velocities from the fluid
+ * (Particle_initialize_velocities, as the reference's main does after the
+ * primitive data), then runs <nsteps> whole time steps through the
+ * reference's own substep routine Temporal_int_all_the_equations, as
+ * ref_driver.c does, and dumps the state (dump_state of ref_driver.c) after
+ * every step, plus per particle F, T, ID, X, U and Omega_z
+ * (particles_s<n>.txt).
  *
  * The initial volume fraction goes into both F and C_L, as the reference's
  * initialisers do (IO/VoF_Init.c), before Particle_initialize and
@@ -130,7 +133,8 @@ static void dump_particles(Cart3d_bag *db, const char *tag)
     Particle_list *lists[2] = {db->lag->p_mobile_list, db->lag->p_fixed_list};
     for (int l = 0; l < 2; l++)
         for (Particle *p = lists[l]->start; p; p = p->next)
-            fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g\n", p->F[0], p->F[1], p->F[2], p->T[0], p->T[1], p->T[2]);
+            fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g %d %.17g %.17g %.17g %.17g %.17g\n", p->F[0], p->F[1],
+                    p->F[2], p->T[0], p->T[1], p->T[2], p->ID, p->X[0], p->X[1], p->U[0], p->U[1], p->Omega[2]);
     fclose(f);
 }
 
@@ -215,7 +219,11 @@ static void run_steps(Cart3d_bag *db, int nsteps, double dt, Debug_trace *dtrace
     const double BET2[] = {BETA2};
     double time = 0.0;
     params->time = 0.0;
+    /* Cart3d.c:505-515, then the cell-centred velocity of Temporal_int.c:194 */
+    Particle_initialize_velocities(db, DTRACE("Particle_initialize_velocities"));
+    Velocity_cell_center(db);
     dump_state(db, "s0");
+    dump_particles(db, "s0");
     for (int n = 1; n <= nsteps; n++) {
         for (int rk = 0; rk < 3; rk++) {
             if (time != 0 && rk == 0)

@@ -365,6 +365,8 @@ int extend_psi_LG(pvof_ctx *c);
 int ibm_flag_points(pvof_ctx *c);
 int ibm_force(pvof_ctx *c, int force_iter);
 int vel_explicit(pvof_ctx *c, int comp);
+int ibm_advect(pvof_ctx *c);
+int ibm_velocity_init(pvof_ctx *c);
 
 // VOF_DIFFUSE_init (VOF_DIFFUSE.c:523-568)
 int vof_diffuse_init(pvof_ctx *c)
@@ -729,6 +731,7 @@ int initialize(pvof_ctx *c)
         CK(cudaMemcpyAsync(c->base[PVOF_F_FSIG_OLD_X], c->base[PVOF_F_FSIG_NEW_X], bytes, cudaMemcpyDeviceToDevice, c->stream));
         CK(cudaMemcpyAsync(c->base[PVOF_F_FSIG_OLD_Y], c->base[PVOF_F_FSIG_NEW_Y], bytes, cudaMemcpyDeviceToDevice, c->stream));
     }
+    if (resolved(c)) TRY(ibm_velocity_init(c));   // Cart3d.c:505-515
     TRY(cell_center(c));
     c->time = 0.0;
     return PVOF_OK;
@@ -793,6 +796,7 @@ int substep(pvof_ctx *c, pvof_stats *st)
         if (!(c->scal_host->div_max > 1e-6)) break;
     }
     if (c->p.surface_tension) swap_f_sigma(c);
+    if (solids && rc == PVOF_OK) TRY(ibm_advect(c));   // Temporal_int.c:1186-1238
     if (st) {
         fill_stats(c, st);
         st->p_iters_total = p_total;
@@ -820,6 +824,7 @@ struct pvof::IbmState {
     int *d_flag = nullptr;
     size_t cap_mk = 0;
     double *d_FT = nullptr;
+    double *d_sums = nullptr;              // k_ibm_particle_sums output, 6 per entry
     double *d_geo = nullptr;
     size_t cap_geo = 0;
     int ngeo = 0;
@@ -835,6 +840,7 @@ struct pvof::IbmState {
         cudaFree(d_mk);
         cudaFree(d_flag);
         cudaFree(d_FT);
+        cudaFree(d_sums);
         cudaFree(d_geo);
     }
 };
@@ -866,6 +872,8 @@ int ibm_state(pvof_ctx *c, IbmState **out)
     g.periodic[1] = c->dom.pery;
     g.xu = s->hm.xu.data() + NG;
     g.yv = s->hm.yv.data() + NG;
+    g.xc = s->hm.xc.data() + NG;
+    g.yc = s->hm.yc.data() + NG;
     g.h = s->hm.dx_u[1 + NG];
     double dymin = s->hm.dy_v[NG];
     for (int j = 0; j < c->dom.NY; j++) dymin = std::min(dymin, s->hm.dy_v[j + NG]);
@@ -925,10 +933,13 @@ int ibm_flag_points(pvof_ctx *c)
     if (ne > s->cap_ent) {
         cudaFree(s->d_ent);
         cudaFree(s->d_FT);
+        cudaFree(s->d_sums);
         s->d_ent = nullptr;
         s->d_FT = nullptr;
+        s->d_sums = nullptr;
         if (cudaMalloc(&s->d_ent, ne * sizeof(IbmEntryDev)) != cudaSuccess ||
-            cudaMalloc(&s->d_FT, 6 * ne * sizeof(double)) != cudaSuccess) {
+            cudaMalloc(&s->d_FT, 6 * ne * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&s->d_sums, 6 * ne * sizeof(double)) != cudaSuccess) {
             s->cap_ent = 0;
             return set_err(PVOF_ENOMEM, "cudaMalloc particle entries");
         }
@@ -957,6 +968,9 @@ int ibm_flag_points(pvof_ctx *c)
         o.moff = e.moff;
         o.mcount = e.mcount;
         for (int k = 0; k < 4; k++) o.box[k] = e.box[k];
+        o.R = e.R;
+        o.id = (double)e.id;
+        ibm_momentum_boxes(e, s->grid, s->hm.xc.data() + NG, s->hm.yc.data() + NG, o.mbox);
     }
     if (ne) {
         CK(cudaMemcpyAsync(s->d_ent, ed.data(), ne * sizeof(IbmEntryDev), cudaMemcpyHostToDevice, c->stream));
@@ -1113,6 +1127,139 @@ int compute_C_S(pvof_ctx *c)
 }
 
 // Pressure_solve_xz_period (psolve_fft.c:638-983) in the planar mode
+// per-entry momentum integrals (and with ccf the capillary contact force) of
+// the current list entries, read back into the host entries
+int ibm_sums(pvof_ctx *c, bool ccf)
+{
+    IbmState *s = c->ibm;
+    const int ne = (int)s->entries.size();
+    if (ne == 0) return PVOF_OK;
+    IbmSumArgs A;
+    A.ent = s->d_ent;
+    A.U = F(c, PVOF_F_U);
+    A.V = F(c, PVOF_F_V);
+    A.CL = F(c, PVOF_F_C_L);
+    A.CS = F(c, PVOF_F_C_S);
+    A.xu = s->xu;
+    A.xc = s->xc;
+    A.yv = s->yv;
+    A.yc = s->yc;
+    A.plist = s->d_plist;
+    A.np = s->n_plist;
+    A.h = s->grid.h;
+    A.slab = c->dom.slab > 0.0 ? c->dom.slab : s->grid.h;   // Interpolate_twod_cell_volume
+    A.sigma = 1.0 / c->p.We;
+    const double theta = c->p.contact_angle_deg * M_PI / 180.0;
+    A.ct = std::cos(theta);
+    A.st = std::sin(theta);
+    const double epsN = 1.0e-14;
+    const double h_ref = (s->grid.dy_min > epsN) ? s->grid.dy_min : epsN;
+    const double cn = (c->p.Cn > 0.0) ? c->p.Cn : 0.0;
+    A.support_width = 8.0 * ((cn > h_ref) ? cn : h_ref);
+    A.nk = c->dom.nk;
+    A.ccf = ccf ? 1 : 0;
+    A.out = s->d_sums;
+    k_ibm_particle_sums<<<(unsigned)ne, 256, 0, c->stream>>>(c->dom, A);
+    CKL(c);
+    std::vector<double> h(6 * (size_t)ne), ft(6 * (size_t)ne);
+    CK(cudaMemcpyAsync(h.data(), s->d_sums, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(ft.data(), s->d_FT, ft.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int q = 0; q < ne; q++) {
+        IbmEntry &e = s->entries[(size_t)q];
+        const double *o = h.data() + 6 * q;
+        for (int k = 0; k < 3; k++) {
+            e.F[k] = ft[6 * (size_t)q + (size_t)k];
+            e.T[k] = ft[6 * (size_t)q + 3 + (size_t)k];
+            e.Int_U[k] = e.Int_Omega[k] = e.F_CCF[k] = e.T_CCF[k] = 0.0;
+        }
+        e.Int_U[0] = o[0];
+        e.Int_U[1] = o[1];
+        e.Int_Omega[2] = o[2];
+        if (ccf) {
+            e.F_CCF[0] = o[3];
+            e.F_CCF[1] = o[4];
+            e.T_CCF[2] = o[5];
+        }
+    }
+    return PVOF_OK;
+}
+
+// the two lists of the current entries (mobile entries come first)
+void ibm_split(const IbmState *s, std::vector<IbmEntry> &mob, std::vector<IbmEntry> &fix)
+{
+    mob.clear();
+    fix.clear();
+    for (const IbmEntry &e : s->entries) (e.mobile ? mob : fix).push_back(e);
+}
+
+// the end of a substep with resolved particles (Temporal_int.c:1186-1238):
+// momentum integrals and contact-line forces of every list entry on the
+// device, then Lagrangian_advect_particles on the host
+int ibm_advect(pvof_ctx *c)
+{
+    IbmState *s = c->ibm;
+    if (!s || !s->flagged) return set_err(PVOF_EINVAL, "pvof_Lagrangian_flag_points() first");
+    TRY(ibm_sums(c, true));
+    std::vector<IbmEntry> mob, fix;
+    ibm_split(s, mob, fix);
+    s->mobile = ibm_collect(mob, s->grid);
+    s->fixed = ibm_collect(fix, s->grid);
+    std::string err;
+    if (!ibm_advance(s->mobile, s->fixed, s->grid, c->p.Cn, c->stage, c->dt, c->p.grav, err))
+        return set_err(PVOF_EINVAL, err);
+    return PVOF_OK;
+}
+
+// Particle_initialize_velocities (Lagrangian/Particle.c:322-535): mobile
+// particles take the volume-averaged fluid velocity, the fluid inside them is
+// painted to that rigid motion, and the momentum integrals of the painted
+// field become the reference for the first rigid-body force
+int ibm_velocity_init(pvof_ctx *c)
+{
+    IbmState *s = c->ibm;
+    TRY(ibm_flag_points(c));
+    TRY(ibm_sums(c, false));
+    std::vector<IbmEntry> mob, fix;
+    ibm_split(s, mob, fix);
+    s->mobile = ibm_collect(mob, s->grid);
+    s->fixed = ibm_collect(fix, s->grid);
+    for (IbmEntry &p : s->mobile) {
+        for (int i = 0; i < 3; i++) p.U[i] = p.Int_U[i] * p.rho_s / p.M;
+        for (int i = 0; i < 3; i++) p.Omega[i] = p.Int_Omega[i] * p.rho_s / p.I_p;
+        for (int i = 0; i < 3; i++) p.U_old[i] = p.U[i];
+        for (int i = 0; i < 3; i++) p.Omega_old[i] = p.Omega[i];
+    }
+    TRY(ibm_flag_points(c));
+    double *U = F(c, PVOF_F_U), *V = F(c, PVOF_F_V);
+    std::vector<IbmEntryDev> ed(s->entries.size());
+    CK(cudaMemcpy(ed.data(), s->d_ent, ed.size() * sizeof(IbmEntryDev), cudaMemcpyDeviceToHost));
+    for (size_t q = 0; q < s->entries.size(); q++) {
+        if (!s->entries[q].mobile) continue;
+        for (int comp = 0; comp < 2; comp++) {
+            const int *b = ed[q].mbox[comp];
+            if (b[1] <= b[0] || b[3] <= b[2]) continue;
+            const dim3 blk(16, 16), grd((unsigned)((b[1] - b[0] + 15) / 16), (unsigned)((b[3] - b[2] + 15) / 16));
+            k_ibm_paint<<<grd, blk, 0, c->stream>>>(c->dom, ed[q], comp, s->xu, s->xc, s->yv, s->yc,
+                                                    comp == 0 ? U : V);
+            CKL(c);
+        }
+    }
+    TRY(fill(c, BK_WRAP_U, U));
+    TRY(fill(c, BK_WRAP_V, V));
+    TRY(fill(c, BK_U, U));
+    TRY(fill(c, BK_V, V));
+    TRY(ibm_sums(c, false));
+    ibm_split(s, mob, fix);
+    s->mobile = ibm_collect(mob, s->grid);
+    s->fixed = ibm_collect(fix, s->grid);
+    for (IbmEntry &p : s->mobile) {
+        for (int i = 0; i < 3; i++) p.Int_U_old[i] = p.Int_U[i];
+        for (int i = 0; i < 3; i++) p.Int_Omega_old[i] = p.Int_Omega[i];
+    }
+    return PVOF_OK;
+}
+
 // contact-line projection (VOF_IBM_wetting.c:1021-2131; kernels in pvof_mcl.cu)
 int mcl_normals(pvof_ctx *c)
 {
@@ -1791,6 +1938,46 @@ int pvof_particle_markers(pvof_ctx *c, int entry, double *x, double *y, double *
 
 int pvof_VOF_DIFFUSE_compute_C_S(pvof_ctx *c) { ENTER(c); return compute_C_S(c); }
 int pvof_VOF_DIFFUSE_compute_solid_normals_MCL(pvof_ctx *c) { ENTER(c); return mcl_normals(c); }
+int pvof_Particle_initialize_velocities(pvof_ctx *c)
+{
+    ENTER(c);
+    if (!c->ibm) return set_err(PVOF_EINVAL, "pvof_set_particles() first");
+    return ibm_velocity_init(c);
+}
+int pvof_Lagrangian_advect_particles(pvof_ctx *c)
+{
+    ENTER(c);
+    NEED_DT(c);
+    return ibm_advect(c);
+}
+int pvof_get_particles(pvof_ctx *c, pvof_particle *out, int *ids, double *Fo, double *To, int nmax)
+{
+    ENTER(c);
+    if (!c->ibm) return set_err(PVOF_EINVAL, "pvof_set_particles() first");
+    const IbmState *s = c->ibm;
+    const int n = (int)(s->mobile.size() + s->fixed.size());
+    if (nmax < n || (n > 0 && !out)) return set_err(PVOF_EINVAL, "particle array too small");
+    int q = 0;
+    for (const std::vector<IbmEntry> *l : {&s->mobile, &s->fixed})
+        for (const IbmEntry &e : *l) {
+            pvof_particle &p = out[q];
+            p.mobile = l == &s->mobile ? 1 : 0;
+            p.X[0] = e.X[0];
+            p.X[1] = e.X[1];
+            p.R = e.R;
+            p.U[0] = e.U[0];
+            p.U[1] = e.U[1];
+            p.Omega_z = e.Omega[2];
+            p.rho_s = e.rho_s;
+            if (ids) ids[q] = e.id;
+            for (int k = 0; k < 3; k++) {
+                if (Fo) Fo[3 * q + k] = e.F[k];
+                if (To) To[3 * q + k] = e.T[k];
+            }
+            q++;
+        }
+    return n;
+}
 int pvof_VOF_DIFFUSE_apply_contact_angle(pvof_ctx *c) { ENTER(c); return apply_contact_angle(c); }
 int pvof_VOF_DIFFUSE_extend_psi_LG_contact_angle(pvof_ctx *c) { ENTER(c); return extend_psi_LG(c); }
 

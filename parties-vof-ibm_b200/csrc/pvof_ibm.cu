@@ -21,8 +21,10 @@
 // is the order in which the reference's scatter adds them, so the result is
 // the reference's to the last bit.
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <string>
 
 #include "pvof_device.cuh"
 #include "pvof_kernels.cuh"
@@ -79,10 +81,23 @@ static std::vector<IbmEntry> update_list(const std::vector<IbmEntry> &local, con
         const double hi = (axis == 0 ? g.xu[g.NX - 1] : g.yv[g.NY - 1]) - range;
         const double L = axis == 0 ? g.Lx : g.Ly;
         std::vector<IbmEntry> low, high;
+        // a copy carries the whole particle, its previous position shifted too
         for (const IbmEntry &p : list)
-            if (p.X[axis] - p.R < lo) { IbmEntry c = p; c.X[axis] += L; c.copy = 1; low.push_back(c); }
+            if (p.X[axis] - p.R < lo) {
+                IbmEntry c = p;
+                c.X[axis] += L;
+                c.X_old[axis] += L;
+                c.copy = 1;
+                low.push_back(c);
+            }
         for (const IbmEntry &p : list)
-            if (p.X[axis] + p.R > hi) { IbmEntry c = p; c.X[axis] -= L; c.copy = 1; high.push_back(c); }
+            if (p.X[axis] + p.R > hi) {
+                IbmEntry c = p;
+                c.X[axis] -= L;
+                c.X_old[axis] -= L;
+                c.copy = 1;
+                high.push_back(c);
+            }
         std::vector<IbmEntry> out = high;
         out.insert(out.end(), low.begin(), low.end());
         out.insert(out.end(), list.begin(), list.end());
@@ -236,6 +251,207 @@ void ibm_solid_constants(double cn, double &shift, double &denom, double &extra)
     const double atanh_x = 0.5 * log((1.0 + x) / (1.0 - x));
     const double e = -shift + denom * atanh_x;
     extra = e > 0.0 ? e : 0.0;
+}
+
+void ibm_derive(IbmEntry &e, const IbmGrid &g) { derived_data(e, g); }
+
+// cell ranges of Interpolate_integrate_momentum_twod and
+// Interpolate_paint_rigid_body_velocity_twod (Lagrangian/Interpolate.c:644-800):
+// u faces have cell edges at xc[i-1] and yv[j], v faces at xu[i] and yc[j-1]
+void ibm_momentum_boxes(const IbmEntry &e, const IbmGrid &g, const double *xc, const double *yc, int box[2][4])
+{
+    const double h = g.h;
+    for (int comp = 0; comp < 2; comp++) {
+        const double xe0 = comp == 0 ? xc[-1] : g.xu[0];
+        const double ye0 = comp == 0 ? g.yv[0] : yc[-1];
+        int i_start = (int)floor((e.X[0] - e.R - xe0) / h);
+        int j_start = (int)floor((e.X[1] - e.R - ye0) / h);
+        int i_end = (int)ceil((e.X[0] + e.R - xe0) / h);
+        int j_end = (int)ceil((e.X[1] + e.R - ye0) / h);
+        i_start = std::max(i_start, 0);
+        j_start = std::max(j_start, 0);
+        i_end = std::min(std::min(i_end, g.NX), g.NX - 1);
+        j_end = std::min(std::min(j_end, g.NY), g.NY - 1);
+        box[comp][0] = i_start;
+        box[comp][1] = i_end;
+        box[comp][2] = j_start;
+        box[comp][3] = j_end;
+    }
+}
+
+// Particle_list_remove (Lagrangian/Particle.c:991-1090), 2D: a centre outside
+// [xu[0], xu[NX-1]) x [yv[0], yv[NY-1]) belongs to a periodic copy
+static bool outside(const IbmEntry &p, const IbmGrid &g)
+{
+    return p.X[0] < g.xu[0] || p.X[0] >= g.xu[g.NX - 1] || p.X[1] < g.yv[0] || p.X[1] >= g.yv[g.NY - 1];
+}
+
+std::vector<IbmEntry> ibm_collect(const std::vector<IbmEntry> &both, const IbmGrid &g)
+{
+    std::vector<IbmEntry> local;
+    std::vector<const IbmEntry *> foreign;
+    for (const IbmEntry &p : both) {
+        if (outside(p, g)) foreign.push_back(&p);
+        else local.push_back(p);
+    }
+    for (IbmEntry &p : local) {
+        p.copy = 0;
+        for (const IbmEntry *pf : foreign) {
+            if (pf->id != p.id) continue;
+            for (int i = 0; i < 3; i++) p.F[i] += pf->F[i];
+            for (int i = 0; i < 3; i++) p.T[i] += pf->T[i];
+            for (int i = 0; i < 3; i++) p.F_CCF[i] += pf->F_CCF[i];
+            for (int i = 0; i < 3; i++) p.T_CCF[i] += pf->T_CCF[i];
+            for (int i = 0; i < 3; i++) p.Int_U[i] += pf->Int_U[i];
+            for (int i = 0; i < 3; i++) p.Int_Omega[i] += pf->Int_Omega[i];
+        }
+    }
+    return local;
+}
+
+namespace {
+
+// RK3 coefficients (Include/definitions.h:197-204)
+const double RK_BET[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
+const double RK_GAM[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+const double RK_ZET[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+
+// Lagrangian_apply_twod_particle_constraints (Lagrangian/Lagrangian.c:105-129), planar
+void twod_constraints(IbmEntry &p, double zs)
+{
+    p.X[2] = zs;
+    p.X_old[2] = p.X[2];
+    p.U[2] = 0.0;
+    p.U_old[2] = 0.0;
+    p.Omega[0] = 0.0;
+    p.Omega[1] = 0.0;
+    p.Omega_old[0] = 0.0;
+    p.Omega_old[1] = 0.0;
+}
+
+// The ranges at which Collision_particle / Collision_wall
+// (Lagrangian/Collision.c:277-720) start to act: contact, or a surface gap
+// within lub_range * h (LUBRICATION_NORMAL).  Returns false if any pair or
+// wall is that close.
+bool out_of_contact(const std::vector<IbmEntry> &mob_both, const std::vector<IbmEntry> &fix_both, const IbmGrid &g,
+                    std::string &err)
+{
+    const double range = LUB_RANGE * g.h;
+    char msg[256];
+    for (size_t a = 0; a < mob_both.size(); a++) {
+        const IbmEntry &p = mob_both[a];
+        auto check = [&](const IbmEntry &q) {
+            if (q.id == p.id) return true;
+            const double c = p.R + q.R + range;
+            const double d0 = p.X[0] - q.X[0], d1 = p.X[1] - q.X[1];
+            if (d0 * d0 + d1 * d1 <= c * c) {
+                snprintf(msg, sizeof(msg),
+                         "particles %d and %d within the lubrication range: the collision models are not built", p.id,
+                         q.id);
+                err = msg;
+                return false;
+            }
+            return true;
+        };
+        for (size_t b = 0; b < mob_both.size(); b++)
+            if (!check(mob_both[b])) return false;
+        for (const IbmEntry &q : fix_both)
+            if (!check(q)) return false;
+        for (int axis = 0; axis < 2; axis++) {
+            if (g.periodic[axis]) continue;
+            const double lo = axis == 0 ? g.xu[0] : g.yv[0];
+            const double hi = axis == 0 ? g.xu[g.NX - 1] : g.yv[g.NY - 1];
+            if (fabs(p.X[axis] - lo) - p.R <= range || fabs(hi - p.X[axis]) - p.R <= range) {
+                snprintf(msg, sizeof(msg),
+                         "particle %d within the lubrication range of a wall: the collision models are not built",
+                         p.id);
+                err = msg;
+                return false;
+            }
+        }
+    }
+    return true;
+}
+
+// the list updates and removals around Collision_evaluate
+// (Lagrangian/Lagrangian.c:1291-1303): copies across the periodic
+// boundaries, then the entries whose centre is in the domain, so a particle
+// that left through one side continues as its copy from the other
+bool relist(std::vector<IbmEntry> &mobile, std::vector<IbmEntry> &fixed, const IbmGrid &g, double Cn, std::string &err)
+{
+    std::vector<IbmEntry> mob = update_list(mobile, g, Cn), fix = update_list(fixed, g, Cn);
+    if (!out_of_contact(mob, fix, g, err)) return false;
+    mobile.clear();
+    for (const IbmEntry &p : mob)
+        if (!outside(p, g)) mobile.push_back(p);
+    fixed.clear();
+    for (const IbmEntry &p : fix)
+        if (!outside(p, g)) fixed.push_back(p);
+    for (IbmEntry &p : mobile) p.copy = 0;
+    for (IbmEntry &p : fixed) p.copy = 0;
+    return true;
+}
+
+}  // namespace
+
+bool ibm_advance(std::vector<IbmEntry> &mobile, std::vector<IbmEntry> &fixed, const IbmGrid &g, double Cn, int stage,
+                 double dt, const double grav[3], std::string &err)
+{
+    // Lagrangian_evaluate_fluid_forces (Lagrangian/Lagrangian.c:338-957), after
+    // the hydrodynamic collection; the diagnostic accumulators (F_IBM, F_rigid,
+    // F_CCF_cum, ...) change nothing downstream and are not kept
+    const double bt = RK_BET[stage];
+    const double idt2beta = 1.0 / (2.0 * bt * dt);
+    for (IbmEntry &p : mobile) {
+        const double int_rho = (p.rho_s > 0.0) ? p.M / p.rho_s : 0.0;   // Lagrangian_set_exact_solid_body_mass
+        for (int i = 0; i < 3; i++) p.F[i] += p.F_CCF[i];
+        for (int i = 0; i < 3; i++) p.T[i] += p.T_CCF[i];
+        for (int i = 0; i < 3; i++) p.F[i] += idt2beta * (p.Int_U[i] - p.Int_U_old[i]);
+        for (int i = 0; i < 3; i++) p.T[i] += idt2beta * (p.Int_Omega[i] - p.Int_Omega_old[i]);
+        for (int i = 0; i < 3; i++) p.Int_U_old[i] = p.Int_U[i];
+        for (int i = 0; i < 3; i++) p.Int_Omega_old[i] = p.Int_Omega[i];
+        for (int i = 0; i < 3; i++) p.F[i] += (p.M - int_rho) * grav[i];
+    }
+    for (IbmEntry &p : fixed) {
+        const double int_rho = (p.rho_s > 0.0) ? p.M / p.rho_s : 0.0;
+        for (int i = 0; i < 3; i++) p.F[i] += p.F_CCF[i];
+        for (int i = 0; i < 3; i++) p.T[i] += p.T_CCF[i];
+        for (int i = 0; i < 3; i++) p.Int_U_old[i] = p.Int_U[i];
+        for (int i = 0; i < 3; i++) p.Int_Omega_old[i] = p.Int_Omega[i];
+        for (int i = 0; i < 3; i++) p.F[i] += (p.M - int_rho) * grav[i];
+    }
+    // SUBSTEP (Lagrangian.c:293-318): 8, 2, 5 particle steps of dt / 15 per
+    // fluid stage, each a full RK3 of Lagrangian_integrate_particle_motion
+    // (Lagrangian.c:967-1640).  Out of contact range the collision forces and
+    // torques Fc, Tc are zero; the fixed particles keep their place.
+    const int nsub[3] = {8, 2, 5};
+    const double dts = dt / 15.0;
+    const double zs = mobile.empty() ? 0.0 : mobile[0].X[2];
+    for (int n = 0; n < nsub[stage]; n++)
+        for (int rk = 0; rk < 3; rk++) {
+            const double b = RK_BET[rk], gm = RK_GAM[rk], zt = RK_ZET[rk];
+            const double Fc = 0.0, Fc_old = 0.0;
+            for (IbmEntry &p : mobile) {   // predictor
+                const double dt_iM = dts / p.M, dt_iI = dts / p.I_p;
+                for (int i = 0; i < 3; i++) p.X_old[i] = p.X[i];
+                for (int i = 0; i < 3; i++) p.U_old[i] = p.U[i];
+                for (int i = 0; i < 3; i++) p.U[i] = p.U_old[i] + dt_iM * (2.0 * b * p.F[i] + gm * Fc + zt * Fc_old);
+                for (int i = 0; i < 3; i++) p.Omega_old[i] = p.Omega[i];
+                for (int i = 0; i < 3; i++)
+                    p.Omega[i] = p.Omega_old[i] + dt_iI * (2.0 * b * p.T[i] + gm * Fc + zt * Fc_old);
+                for (int i = 0; i < 3; i++) p.X[i] = p.X_old[i] + dts * b * (p.U[i] + p.U_old[i]);
+                twod_constraints(p, zs);
+            }
+            if (!relist(mobile, fixed, g, Cn, err)) return false;
+            for (IbmEntry &p : mobile) {   // corrector
+                const double dt_iM = dts / p.M, dt_iI = dts / p.I_p;
+                for (int i = 0; i < 3; i++) p.U[i] = p.U_old[i] + dt_iM * b * (2.0 * p.F[i] + Fc + Fc_old);
+                for (int i = 0; i < 3; i++) p.Omega[i] = p.Omega_old[i] + dt_iI * b * (2.0 * p.T[i] + Fc + Fc_old);
+                for (int i = 0; i < 3; i++) p.X[i] = p.X_old[i] + dts * b * (p.U[i] + p.U_old[i]);
+                twod_constraints(p, zs);
+            }
+        }
+    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -400,6 +616,188 @@ __global__ void k_compute_C_S(Dom d, const double *__restrict__ xc, const double
         if (cs > cs_max) cs_max = cs;
     }
     AT_(CS, i, j) = cs_max;
+}
+
+// Interpolate_twod_level_set (Interpolate.c:314-320)
+__device__ __forceinline__ double twod_level_set(double x, double y, double X0, double X1, double R)
+{
+    return sqrt((x - X0) * (x - X0) + (y - X1) * (y - X1)) / R - 1.0;
+}
+
+// Interpolate_twod_volume_fraction_from_phi (Interpolate.c:531-542)
+__device__ __forceinline__ double vf_from_phi(double phi00, double phi10, double phi01, double phi11)
+{
+    double vf_cell = 0.0;
+    const double sum_phi = fabs(phi00) + fabs(phi10) + fabs(phi01) + fabs(phi11);
+    if (phi00 < 0.0) vf_cell -= phi00;
+    if (phi10 < 0.0) vf_cell -= phi10;
+    if (phi01 < 0.0) vf_cell -= phi01;
+    if (phi11 < 0.0) vf_cell -= phi11;
+    return (sum_phi > 0.0) ? vf_cell / sum_phi : 0.0;
+}
+
+// solid fraction of face cell (i, j) of component comp from the level set at
+// its corners: u faces have corners at (xc[i-1..i], yv[j..j+1]), v faces at
+// (xu[i..i+1], yc[j-1..j]) (Interpolate.c:690-706)
+__device__ __forceinline__ double face_solid_fraction(int comp, int i, int j, double X0, double X1, double R,
+                                                      const double *xu, const double *xc, const double *yv,
+                                                      const double *yc)
+{
+    const double xa = comp == 0 ? xc[i - 1] : xu[i], xb = comp == 0 ? xc[i] : xu[i + 1];
+    const double ya = comp == 0 ? yv[j] : yc[j - 1], yb = comp == 0 ? yv[j + 1] : yc[j];
+    const double p00 = twod_level_set(xa, ya, X0, X1, R), p01 = twod_level_set(xb, ya, X0, X1, R);
+    const double p10 = twod_level_set(xa, yb, X0, X1, R), p11 = twod_level_set(xb, yb, X0, X1, R);
+    return vf_from_phi(p00, p01, p10, p11);
+}
+
+// mcl_particle_owns_diffuse_support (Eulerian/VOF_IBM_wetting.c:72-116): the
+// entry with ID `id` has the smallest surface gap among the list entries
+// whose support reaches (x, y), ties to the lower ID
+__device__ __forceinline__ bool owns_support(const double *plist, int np, double id, double x, double y,
+                                             double support_width)
+{
+    double best_gap = DBL_MAX, best_id = id;
+    bool found = false;
+    for (int q = 0; q < np; q++) {
+        const double *pq = plist + 4 * q;
+        const double support = pq[2] + support_width;
+        const double dx = x - pq[0], dy = y - pq[1], dz = 0.0;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 > support * support) continue;
+        const double gap = sqrt(d2) - pq[2];
+        if (!found || gap < best_gap - 1.0e-12 || (fabs(gap - best_gap) <= 1.0e-12 && pq[3] < best_id)) {
+            best_gap = gap;
+            best_id = pq[3];
+            found = true;
+        }
+    }
+    return !found || best_id == id;
+}
+
+// One block per list entry, at the end of a substep:
+//   Interpolate_integrate_momentum_twod (Interpolate.c:644-725) of u and v:
+//     Int_U[c] = sum vf * vel * dV, Int_Omega[2] = -sum_u dP r_y + sum_v dP r_x
+//   VOF_accumulate_solid_capillary_force (Eulerian/VOF_IBM_wetting.c:198-372),
+//     Washino's contact-line force sigma t_c (grad C_L . t_s)(grad C_S . n_s)
+//     over the cells of every G-range k plane within R + support of the centre
+//     that the entry owns; F_CCF and T_CCF[2]
+// The sums run as block reductions in a fixed order (run to run
+// reproducible); the reference adds the cells one by one, so the sums agree
+// to rounding.
+__global__ void __launch_bounds__(256) k_ibm_particle_sums(Dom d, IbmSumArgs A)
+{
+    const IbmEntryDev &E = A.ent[blockIdx.x];
+    const double X0 = E.X[0], X1 = E.X[1], R = E.R;
+    const int P = d.P;
+    double acc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int comp = 0; comp < 2; comp++) {
+        const int *b = E.mbox[comp];
+        const int w = b[1] - b[0], hgt = b[3] - b[2];
+        if (w <= 0 || hgt <= 0) continue;
+        const double *vel = comp == 0 ? A.U : A.V;
+        const double *xn = comp == 0 ? A.xu : A.xc, *yn = comp == 0 ? A.yc : A.yv;
+        for (int t = threadIdx.x; t < w * hgt; t += blockDim.x) {
+            const int i = b[0] + t % w, j = b[2] + t / w;
+            const double vf = face_solid_fraction(comp, i, j, X0, X1, R, A.xu, A.xc, A.yv, A.yc);
+            const double dV = A.h * d.m.dy_v[j] * A.slab;
+            const double dP = vf * AT_(vel, i, j) * dV;
+            acc[comp] += dP;
+            if (comp == 0) acc[2] += dP * (yn[j] - X1);
+            else acc[3] += dP * (xn[i] - X0);
+        }
+    }
+    if (A.ccf) {
+        const double sr = R + A.support_width, sr2 = sr * sr;
+        const double hx = A.xc[1] - A.xc[0], hy = A.yc[1] - A.yc[0];
+        const int i0 = max(0, (int)floor((X0 - sr - A.xc[0]) / hx) - 1);
+        const int i1 = min(d.NX, (int)ceil((X0 + sr - A.xc[0]) / hx) + 2);
+        const int j0 = max(0, (int)floor((X1 - sr - A.yc[0]) / hy) - 1);
+        const int j1 = min(d.NY, (int)ceil((X1 + sr - A.yc[0]) / hy) + 2);
+        const int w = i1 - i0, hgt = j1 - j0;
+        const int ncell = (w > 0 && hgt > 0) ? w * hgt : 0;
+        const double eps = 1.0e-14;
+        for (int t = threadIdx.x; t < ncell * A.nk; t += blockDim.x) {
+            const int c = t % ncell;
+            const int i = i0 + c % w, j = j0 + c / w;
+            const double r0 = A.xc[i] - X0, r1 = A.yc[j] - X1, r2 = 0.0;
+            const double dist2 = r0 * r0 + r1 * r1 + r2 * r2;
+            if (dist2 > sr2) continue;
+            if (!owns_support(A.plist, A.np, E.id, A.xc[i], A.yc[j], A.support_width)) continue;
+            const double i2dx = 1.0 / (A.xc[i + 1] - A.xc[i - 1]), i2dy = 1.0 / (A.yc[j + 1] - A.yc[j - 1]);
+            const double gl[3] = {(AT_(A.CL, i + 1, j) - AT_(A.CL, i - 1, j)) * i2dx,
+                                  (AT_(A.CL, i, j + 1) - AT_(A.CL, i, j - 1)) * i2dy, 0.0};
+            const double gs[3] = {(AT_(A.CS, i + 1, j) - AT_(A.CS, i - 1, j)) * i2dx,
+                                  (AT_(A.CS, i, j + 1) - AT_(A.CS, i, j - 1)) * i2dy, 0.0};
+            const double mag_l = sqrt(gl[0] * gl[0] + gl[1] * gl[1] + gl[2] * gl[2]);
+            const double mag_s = sqrt(gs[0] * gs[0] + gs[1] * gs[1] + gs[2] * gs[2]);
+            if (mag_l < eps || mag_s < eps) continue;
+            const double ns[3] = {gs[0] / mag_s, gs[1] / mag_s, gs[2] / mag_s};
+            const double gl_ns = gl[0] * ns[0] + gl[1] * ns[1] + gl[2] * ns[2];
+            double ts[3] = {gl[0] - gl_ns * ns[0], gl[1] - gl_ns * ns[1], gl[2] - gl_ns * ns[2]};
+            const double ts_len = sqrt(ts[0] * ts[0] + ts[1] * ts[1] + ts[2] * ts[2]);
+            if (ts_len < eps) continue;
+            ts[0] /= ts_len;
+            ts[1] /= ts_len;
+            ts[2] /= ts_len;
+            double tc[3] = {A.ct * ts[0] - A.st * ns[0], A.ct * ts[1] - A.st * ns[1], A.ct * ts[2] - A.st * ns[2]};
+            const double tc_len = sqrt(tc[0] * tc[0] + tc[1] * tc[1] + tc[2] * tc[2]);
+            if (tc_len < eps) continue;
+            tc[0] /= tc_len;
+            tc[1] /= tc_len;
+            const double term_l = gl[0] * ts[0] + gl[1] * ts[1] + gl[2] * ts[2];
+            const double term_s = gs[0] * ns[0] + gs[1] * ns[1] + gs[2] * ns[2];
+            const double f0 = A.sigma * term_l * term_s * tc[0], f1 = A.sigma * term_l * term_s * tc[1];
+            const double dV = d.m.dx_u[i] * d.m.dy_v[j] * A.slab;
+            const double dF0 = f0 * dV, dF1 = f1 * dV;
+            acc[4] += dF0;
+            acc[5] += dF1;
+            acc[6] += (dF0 * r1 - dF1 * r0);
+        }
+    }
+    // block reduction: warps, then the warp totals
+    __shared__ double red[8][7];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < 7; k++) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        const int k = threadIdx.x;
+        double v = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) v += red[q][k];
+        red[0][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double *o = A.out + 6 * blockIdx.x;
+        o[0] = red[0][0];
+        o[1] = red[0][1];
+        o[2] = (0.0 - red[0][2]) + red[0][3];
+        o[3] = red[0][4];
+        o[4] = red[0][5];
+        o[5] = red[0][6];
+    }
+}
+
+// Interpolate_paint_rigid_body_velocity_twod (Interpolate.c:734-800) of one
+// entry: vel = vf (U + Omega_z x r) + (1 - vf) vel on the face cells it covers
+__global__ void k_ibm_paint(Dom d, IbmEntryDev e, int comp, const double *__restrict__ xu,
+                            const double *__restrict__ xc, const double *__restrict__ yv,
+                            const double *__restrict__ yc, double *__restrict__ vel)
+{
+    const int *b = e.mbox[comp];
+    const int i = b[0] + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = b[2] + (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    if (i >= b[1] || j >= b[3]) return;
+    const double X0 = e.X[0], X1 = e.X[1];
+    const double vf = face_solid_fraction(comp, i, j, X0, X1, e.R, xu, xc, yv, yc);
+    if (vf <= 0.0) return;
+    const int P = d.P;
+    const double om = e.Omega[2];
+    const double u_rigid = comp == 0 ? e.U[0] - om * (yc[j] - X1) : e.U[1] + om * (xc[i] - X0);
+    AT_(vel, i, j) = vf * u_rigid + (1.0 - vf) * AT_(vel, i, j);
 }
 
 }  // namespace pvof

@@ -2,6 +2,7 @@
 // host orchestration.
 #pragma once
 
+#include <string>
 #include <vector>
 
 #include "pvof_internal.cuh"
@@ -129,6 +130,11 @@ struct IbmEntry {
     int N_L;                  // markers of the whole circle
     int moff, mcount;         // this entry's markers near the domain
     int box[4];               // cells [i0, i1) x [j0, j1) its marker supports can reach
+    // rigid-body state (the Particle fields of Include/DataTypes.h:1327-1527
+    // that the motion of a cylinder reads)
+    double X_old[3], U_old[3], Omega_old[3];
+    double Int_U[3], Int_Omega[3], Int_U_old[3], Int_Omega_old[3];
+    double F[3], T[3], F_CCF[3], T_CCF[3];
 };
 
 struct IbmMarkers {
@@ -141,14 +147,29 @@ struct IbmMarkers {
 struct IbmGrid {
     int NX, NY;
     int periodic[2];
-    const double *xu, *yv;
+    const double *xu, *yv, *xc, *yc;
     double h, dy_min, slab, twod_slab, Lx, Ly;
 };
 
 struct IbmEntryDev {
     double X[3], U[3], Omega[3], Zs;
+    double R, id;
     int moff, mcount;
     int box[4];
+    int mbox[2][4];           // cells of Interpolate_integrate_momentum_twod for u and v
+};
+
+// per-entry sums at the end of a substep (k_ibm_particle_sums): Int_U[0..1],
+// Int_Omega[2], and with ccf the capillary contact force F_CCF[0..1], T_CCF[2]
+struct IbmSumArgs {
+    const IbmEntryDev *ent;
+    const double *U, *V, *CL, *CS;
+    const double *xu, *xc, *yv, *yc;     // offset by NG
+    const double *plist;                 // x, y, R, ID of the list entries
+    int np;
+    double h, slab, sigma, ct, st, support_width;
+    int nk, ccf;
+    double *out;                         // 6 doubles per entry
 };
 
 struct IbmDev {
@@ -166,6 +187,18 @@ void ibm_build(const std::vector<IbmEntry> &mobile_local, const std::vector<IbmE
 void ibm_solid_geometry(const std::vector<IbmEntry> &mobile_local, const std::vector<IbmEntry> &fixed_local,
                         const IbmGrid &g, std::vector<double> &geo);
 void ibm_solid_constants(double cn, double &shift, double &denom, double &extra);
+void ibm_derive(IbmEntry &e, const IbmGrid &g);
+void ibm_momentum_boxes(const IbmEntry &e, const IbmGrid &g, const double *xc, const double *yc, int box[2][4]);
+// Lagrangian_collect_forces (LAG_COLLECT_HYDRO) after Particle_list_foreign_create:
+// the entries of a list whose centre lies in the domain, each with the
+// hydrodynamic sums of its periodic copies added
+std::vector<IbmEntry> ibm_collect(const std::vector<IbmEntry> &both, const IbmGrid &g);
+// Lagrangian_evaluate_fluid_forces and the substepped Lagrangian_integrate_particle_motion
+// (Lagrangian/Lagrangian.c:283-1640) for cylinders out of contact range; returns
+// false (with a message) when two particles or a particle and a wall come within
+// the lubrication range, where the collision models would act
+bool ibm_advance(std::vector<IbmEntry> &mobile, std::vector<IbmEntry> &fixed, const IbmGrid &g, double Cn,
+                 int stage, double dt, const double grav[3], std::string &err);
 
 // contact-line projection (pvof_mcl.cu): the G-range scalars of one pass and
 // the case constants; CL and field are the pass's snapshots
@@ -194,6 +227,9 @@ __global__ void k_ibm_correct(Dom d, int comp, double dtbeta, const double *rhs,
 __global__ void k_ibm_ng_update(Dom d, double *a, const double *b, int reset);
 __global__ void k_vel_explicit(Dom d, int comp, int i0, int i1, int j0, int j1, double dtimeb, const double *rhs,
                                const double *rho, double *vel);
+__global__ void k_ibm_particle_sums(Dom d, IbmSumArgs A);
+__global__ void k_ibm_paint(Dom d, IbmEntryDev e, int comp, const double *xu, const double *xc, const double *yv,
+                            const double *yc, double *vel);
 __global__ void k_compute_C_S(Dom d, const double *xc, const double *yc, const double *geo, int ngeo, double shift,
                               double denom, double extra, double *CS);
 

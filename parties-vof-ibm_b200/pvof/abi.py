@@ -129,6 +129,7 @@ EXPORTS = [
     "pvof_Lagrangian_force", "pvof_Pressure_solve_fft", "pvof_run_steps_batched",
     "pvof_VOF_DIFFUSE_compute_solid_normals_MCL", "pvof_VOF_DIFFUSE_apply_contact_angle",
     "pvof_VOF_DIFFUSE_extend_psi_LG_contact_angle",
+    "pvof_Particle_initialize_velocities", "pvof_Lagrangian_advect_particles", "pvof_get_particles",
 ]
 
 SOLVER_BIHARMONIC = 0

@@ -78,6 +78,9 @@ def load():
     L.pvof_VOF_DIFFUSE_compute_solid_normals_MCL.argtypes = [V]
     L.pvof_VOF_DIFFUSE_apply_contact_angle.argtypes = [V]
     L.pvof_VOF_DIFFUSE_extend_psi_LG_contact_angle.argtypes = [V]
+    L.pvof_Particle_initialize_velocities.argtypes = [V]
+    L.pvof_Lagrangian_advect_particles.argtypes = [V]
+    L.pvof_get_particles.argtypes = [V, P(abi.Particle), P(C.c_int), P(C.c_double), P(C.c_double), C.c_int]
     L.pvof_run_steps_batched.argtypes = [P(V), C.c_int, C.c_int, C.c_double, P(abi.Stats)]
     L.pvof_solver_kernel.restype = C.c_char_p
     _lib = L
@@ -179,6 +182,24 @@ class Solver:
         check(load().pvof_particle_forces(self.h, F.ctypes.data_as(C.POINTER(C.c_double)),
                                           T.ctypes.data_as(C.POINTER(C.c_double)), n), "pvof_particle_forces")
         return F[:3 * n].reshape(n, 3), T[:3 * n].reshape(n, 3)
+
+    def get_particles(self, nmax=4096):
+        """Owned particles in list order: dict of arrays id, mobile, X (n, 2),
+        U (n, 2), Omega (n,), R, F (n, 3), T (n, 3)."""
+        arr = (abi.Particle * nmax)()
+        ids = (C.c_int * nmax)()
+        F = np.zeros(3 * nmax)
+        T = np.zeros(3 * nmax)
+        dp = C.POINTER(C.c_double)
+        n = check(load().pvof_get_particles(self.h, arr, ids, F.ctypes.data_as(dp), T.ctypes.data_as(dp), nmax),
+                  "pvof_get_particles")
+        return {"id": np.array(ids[:n], dtype=np.int64),
+                "mobile": np.array([arr[q].mobile for q in range(n)], dtype=np.int64),
+                "X": np.array([[arr[q].X[0], arr[q].X[1]] for q in range(n)]).reshape(n, 2),
+                "U": np.array([[arr[q].U[0], arr[q].U[1]] for q in range(n)]).reshape(n, 2),
+                "Omega": np.array([arr[q].Omega_z for q in range(n)]),
+                "R": np.array([arr[q].R for q in range(n)]),
+                "F": F[:3 * n].reshape(n, 3), "T": T[:3 * n].reshape(n, 3)}
 
     def particle_markers(self, entry, nmax=100000):
         x, y, vol = np.zeros(nmax), np.zeros(nmax), np.zeros(nmax)

@@ -67,11 +67,17 @@ MCL_CASES = [("mcl_theta60", MCL_GRID, MCL_PARTICLES, 60.0),
              ("mcl_theta120", MCL_GRID, MCL_PARTICLES, 120.0),
              ("mcl_theta30", MCL_GRID, MCL_PARTICLES, 30.0)]
 
-# whole time steps with fixed resolved cylinders (oracle/ref/ibm_driver.c
-# "steps" mode): name, reference build, builder arguments, particles, contact
-# angle, steps, dt.  Solver tolerances near machine precision.
+# whole time steps with resolved cylinders (oracle/ref/ibm_driver.c "steps"
+# mode): name, reference build, builder arguments, particles, contact angle,
+# steps, dt.  Solver tolerances near machine precision.  The mobile case has
+# one cylinder across the periodic x boundary and one on the interface.
 IBM_STEP_PARTICLES = [(0, 0.5, 1.0, 0.2, 0.0, 0.0, 0.0, 2.5), (0, 0.03, 1.04, 0.15, 0.0, 0.0, 0.0, 2.5)]
+IBM_MOBILE_PARTICLES = [(0, 0.5, 1.0, 0.2, 0.0, 0.0, 0.0, 2.5), (1, 0.02, 1.5, 0.1, 0.0, 0.0, 0.0, 2.5),
+                        (1, 0.88, 1.0, 0.08, 0.0, 0.0, 0.0, 2.5)]
 IBM_STEP_CASES = [
+    ("ibm_mobile_st", "ibm2d_st", dict(NXM=32, NYM=64, Lx=1.0, Ly=2.0, Cn=0.04, surface_tension=True, We=100.0,
+                                       velocity_seed=19, velocity_amp=0.1, **TIGHT), IBM_MOBILE_PARTICLES, 70.0, 2,
+     1e-3),
     ("ibm_steps_st", "ibm2d_st", dict(NXM=32, NYM=64, Lx=1.0, Ly=2.0, Cn=0.04, surface_tension=True, We=100.0,
                                       velocity_seed=13, velocity_amp=0.1, **TIGHT), IBM_STEP_PARTICLES, 60.0, 2, 1e-3),
     ("ibm_steps", "ibm2d", dict(NXM=32, NYM=64, Lx=1.0, Ly=2.0, Cn=0.04, velocity_seed=17, velocity_amp=0.1, **TIGHT),
@@ -229,9 +235,10 @@ def make_ibm_steps(name, refcase, kw, particles, theta, steps, dt, outdir, refsr
                 data["%s/%s" % (tag, pname)] = g_range(grid, a, False)
             for fname, pname in ngf.items():
                 data["%s/%s" % (tag, pname)] = po.read_reference_field(wd, tag, fname, grid, ng=True)
-            if tag != "s0":
-                F, T = po.read_reference_particles(wd, tag)
-                data[tag + "/F"], data[tag + "/T"] = F, T
+            F, T = po.read_reference_particles(wd, tag)
+            data[tag + "/F"], data[tag + "/T"] = F, T
+            pid, X, U, Om = po.read_reference_particle_state(wd, tag)
+            data[tag + "/pid"], data[tag + "/pX"], data[tag + "/pU"], data[tag + "/pOmega"] = pid, X, U, Om
         data["iterations"] = parse_iterations(cp.stdout)
     for k, v in planes.items():
         data["init/" + k] = v
