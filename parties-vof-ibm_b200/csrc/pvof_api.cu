@@ -599,7 +599,7 @@ int velocity_solve(pvof_ctx *c, int comp)
 // both components: one launch of two clusters when the ranges fit, else in turn
 int velocity_solve_both(pvof_ctx *c)
 {
-    if (!c->cgs_v_smem) {
+    if (!c->cgs_v_smem || c->vel_one_cluster) {
         TRY(velocity_solve(c, 0));
         return velocity_solve(c, 1);
     }
@@ -1756,6 +1756,14 @@ int pvof_run_steps_batched(pvof_ctx *const *ctxs, int n, int nsteps, double dt, 
         for (int r = 0; r < q; r++)
             if (ctxs[r] == ctxs[q]) return set_err(PVOF_EINVAL, "a context appears twice in the batch");
     }
+    // with several cases on the GPU each case's momentum solve takes one
+    // cluster (u, then v) instead of two side by side, so more cases fit
+    const bool one = n > 1 && !std::getenv("PVOF_BATCH_VEL_PAIR");
+    std::vector<int> saved((size_t)n);
+    for (int q = 0; q < n; q++) {
+        saved[(size_t)q] = ctxs[q]->vel_one_cluster;
+        ctxs[q]->vel_one_cluster = one ? 1 : saved[(size_t)q];
+    }
     std::vector<int> rc((size_t)n, PVOF_OK);
     std::vector<std::string> msg((size_t)n);
     std::vector<std::thread> workers;
@@ -1766,6 +1774,7 @@ int pvof_run_steps_batched(pvof_ctx *const *ctxs, int n, int nsteps, double dt, 
             if (rc[(size_t)q] < 0) msg[(size_t)q] = g_err;   // the message is per thread
         });
     for (std::thread &t : workers) t.join();
+    for (int q = 0; q < n; q++) ctxs[q]->vel_one_cluster = saved[(size_t)q];
     for (int q = 0; q < n; q++)
         if (rc[(size_t)q] < 0) return set_err(rc[(size_t)q], "case " + std::to_string(q) + ": " + msg[(size_t)q]);
     return PVOF_OK;

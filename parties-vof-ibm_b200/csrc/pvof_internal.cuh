@@ -131,6 +131,7 @@ struct Ctx {
     size_t cgs_p_smem;       // shared memory of the cluster pressure solver (0: grid solver)
     size_t cgs_v_smem;       // same, velocity solver for both components (0: grid solver)
     int cgs_p_threads, cgs_v_threads;   // their threads per CTA
+    int vel_one_cluster;     // momentum solve as u then v on one cluster (batched runs)
     int coop_blocks;         // co-resident blocks for the persistent solvers
     int coop_threads;
     long long launches;      // kernels launched by this context
