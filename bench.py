@@ -24,7 +24,8 @@ stream per case, so the cluster-resident solvers of different cases run on
 different SMs) and adds a "batched" object to the line.
 
 --impl reference runs the reference's own time step (compiled from its
-sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host.
+sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host:
+--warmup untimed steps, then min(--steps, --ref-steps) timed ones.
 With N > 1 (torchrun) every rank advances its own replica of the case
 (replicas only; the case is not split across GPUs).
 """
@@ -152,8 +153,9 @@ def profile_traffic(kernel):
         return None
 
 
-def reference_timing(steps, timeout=1800):
-    """Run the reference build on the bench case; (cell-updates/s, seconds, steps)."""
+def reference_timing(steps, timeout=1800, warmup=0):
+    """Run the reference build on the bench case, ``warmup`` untimed steps then
+    ``steps`` timed ones; (cell-updates/s, seconds, steps)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import pyoracle as po  # checker / CPU baseline only
     binary = po.ref_binary("rt2d")
@@ -161,13 +163,15 @@ def reference_timing(steps, timeout=1800):
         return None
     grid, params, planes = case()
     with tempfile.TemporaryDirectory() as wd:
-        cp = po.run_reference("rt2d", wd, grid, params, planes, steps, DT, 0, timeout=timeout)
+        cp = po.run_reference("rt2d", wd, grid, params, planes, steps + warmup, DT, 0, timeout=timeout,
+                              warmup=warmup)
     for line in cp.stdout.splitlines():
         if line.startswith("REF_TIMING"):
             kv = dict(x.split("=") for x in line.split()[1:])
             secs = float(kv["seconds"])
             cells = int(kv["cells"])
-            return cells * steps / secs, secs, steps
+            timed = int(kv["steps"])
+            return cells * timed / secs, secs, timed
     return None
 
 
@@ -176,19 +180,20 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     steps = max(1, min(args.steps, args.ref_steps))
-    r = reference_timing(steps)
+    r = reference_timing(steps, warmup=max(0, args.warmup))
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/ref_rt2d is missing"}))
         return 0
     value, secs, n = r
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": n, "warmup": 0, "ms_per_step": 1e3 * secs / n, "higher_is_better": True, "scaling": "weak",
+        "steps": n, "warmup": max(0, args.warmup), "ms_per_step": 1e3 * secs / n, "higher_is_better": True,
+        "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "grid": "%dx%d" % (NXM, NYM), "cells": NXM * NYM, "dt": DT},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                         "sample": "%d time steps of the same case, single-rank reference build (no MPI on this "
-                                   "host), %.1f s" % (n, secs)},
+                         "sample": "%d time steps of the same case after %d untimed ones, single-rank reference "
+                                   "build (no MPI on this host), %.1f s" % (n, max(0, args.warmup), secs)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

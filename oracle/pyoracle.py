@@ -184,9 +184,10 @@ def build_reference(case, refsrc=None):
 
 
 def run_reference(case, workdir, grid, params, planes, nsteps, dt, dump_every=1,
-                  substeps=False, timeout=3600):
+                  substeps=False, timeout=3600, warmup=0):
     """Run the reference build ``case`` on the initial planes; returns the
-    completed process (stdout has the solver log and the REF_TIMING line)."""
+    completed process (stdout has the solver log and the REF_TIMING line,
+    which leaves out the first ``warmup`` of the ``nsteps`` steps)."""
     os.makedirs(workdir, exist_ok=True)
     write_parties_inp(os.path.join(workdir, "parties.inp"), grid, params)
     names = {"F": "init_C.bin", "U": "init_u.bin", "V": "init_v.bin", "P": "init_p.bin"}
@@ -194,7 +195,7 @@ def run_reference(case, workdir, grid, params, planes, nsteps, dt, dump_every=1,
         if k in planes:
             np.ascontiguousarray(planes[k], dtype="<f8").tofile(os.path.join(workdir, fn))
     cmd = [ref_binary(case), workdir, str(nsteps), repr(float(dt)), str(dump_every),
-           "1" if substeps else "0"]
+           "1" if substeps else "0", str(int(warmup))]
     return subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=timeout)
 
 

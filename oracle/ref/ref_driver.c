@@ -12,7 +12,7 @@
  * Temporal_int_all_the_equations (PARTIES/src/Temporal_int.c:563) exactly as
  * Temporal_int_rk3 calls it (Temporal_int.c:399-448) with a constant dt.
  *
- * Usage: ref_driver <case_dir> <nsteps> <dt> <dump_every> [substeps]
+ * Usage: ref_driver <case_dir> <nsteps> <dt> <dump_every> [substeps] [warmup]
  *   <case_dir>/parties.inp            INI parameters (reference format)
  *   <case_dir>/init_{C,u,v,p}.bin     doubles on the G range of one plane,
  *                                     [j][i] order, i fastest, NX*NY values
@@ -22,7 +22,7 @@
  *   block of the field (L ranges, [k][j][i], i fastest); "substeps" > 0 also
  *   dumps after every RK substep as s<step>_<rk>_<field>.bin.
  * The timing line "REF_TIMING steps=<n> cells=<c> seconds=<t>" covers the
- * step loop only.  Test infrastructure only.
+ * step loop only, after the first <warmup> steps (default 0).  Test infrastructure only.
  */
 #include "DataTypes.h"
 #include "definitions.h"
@@ -126,6 +126,7 @@ int main(int argc, char **argv)
     double dt = atof(argv[3]);
     int dump_every = atoi(argv[4]);
     int dump_substeps = (argc > 5) ? atoi(argv[5]) : 0;
+    int warm = (argc > 6) ? atoi(argv[6]) : 0;   /* leading steps left out of REF_TIMING */
     if (chdir(case_dir) != 0) die("cannot enter the case directory");
     mkdir("out", 0755);
 
@@ -191,6 +192,10 @@ int main(int argc, char **argv)
     double t0 = MPI_Wtime();
     double t_io = 0.0;
     for (int n = 1; n <= nsteps; n++) {
+        if (n == warm + 1) {
+            t0 = MPI_Wtime();
+            t_io = 0.0;
+        }
         for (int rk = 0; rk < 3; rk++) {
             if (time != 0 && rk == 0)
                 Velocity_cell_center(db);
@@ -217,7 +222,7 @@ int main(int argc, char **argv)
         }
     }
     double secs = MPI_Wtime() - t0 - t_io;
-    printf("REF_TIMING steps=%d cells=%ld seconds=%.6f\n", nsteps,
+    printf("REF_TIMING steps=%d cells=%ld seconds=%.6f\n", nsteps - (warm < nsteps ? warm : 0),
            (long)params->NXM * (long)params->NYM * (long)params->NZM, secs);
     return 0;
 }
