@@ -21,7 +21,9 @@ host buffers before every step and downloaded after it.
 --batch-cases K additionally times K replicas of the workload advanced
 concurrently by pvof_run_steps_batched (the batched form: one host thread and
 stream per case, so the cluster-resident solvers of different cases run on
-different SMs) and adds a "batched" object to the line.
+different SMs) and adds a "batched" object to the line; --batch-form fp32 runs
+the replicas in the FP32 stencil form and reports their error against the
+FP64 path.
 
 --impl reference runs the reference's own time step (compiled from its
 sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host:
@@ -280,9 +282,12 @@ def run_ours(args):
     # ---- batched form: K replicas advanced concurrently (optional) -----------
     batched = None
     if args.batch_cases > 1:
+        from pvof import abi
+        bparams = abi.Params.from_buffer_copy(params)
+        bparams.stencil_fp32 = 1 if args.batch_form == "fp32" else 0
         reps = []
         for q in range(args.batch_cases):
-            r = runtime.Solver(grid, params, device=local)
+            r = runtime.Solver(grid, bparams, device=local)
             r.set_planes(planes)
             r.initialize()
             reps.append(r)
@@ -298,7 +303,21 @@ def run_ours(args):
         batched = {"cases": args.batch_cases, "steps": bsteps, "value": bvalue, "unit": UNIT,
                    "ms_per_step": span / bsteps, "vs_single": bvalue / (cells * args.steps / (total_ms * 1e-3)),
                    "note": "replicas of the workload advanced concurrently by pvof_run_steps_batched "
-                           "(one host thread and stream per case); device time of the slowest case"}
+                           "(one host thread and stream per case); device time of the slowest case",
+                   "form": "fp32-stencils" if args.batch_form == "fp32" else "fp64"}
+        if args.batch_form == "fp32":
+            import numpy as np
+            # the error of the form: one replica against the FP64 path after the same steps
+            ref = runtime.Solver(grid, params, device=local)
+            ref.set_planes(planes)
+            ref.initialize()
+            ref.run_steps(1 + bsteps, DT)
+            vel = max(float(np.linalg.norm(reps[0].get(f) - ref.get(f)) / np.linalg.norm(ref.get(f)))
+                      for f in ("U", "V"))
+            m64 = ref.liquid_mass()
+            batched["error_vs_fp64"] = {"velocity_rel_l2": vel,
+                                        "volume_rel": abs(reps[0].liquid_mass() - m64) / abs(m64)}
+            ref.close()
         for r in reps:
             r.close()
 
@@ -354,6 +373,8 @@ def main():
     ap.add_argument("--batch-cases", type=int, default=0,
                     help="also time this many replicas advanced concurrently (batched form)")
     ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--batch-form", default="fp64", choices=["fp64", "fp32"],
+                    help="fp32: the batched replicas use the FP32 stencil form (error against FP64 reported)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         log("note: fewer than 3 warm-up steps")

@@ -100,6 +100,11 @@ typedef struct pvof_params {
     /* resolved solids (used once pvof_set_particles has been called) */
     double contact_angle_deg;   /* [vof] contact_angle_deg (default 90) */
     int N_forcing_loops;        /* [particle] N_forcing_loops (default 2) */
+    /* no counterpart in the reference: 1 selects the FP32 stencil form (WENO5
+     * fluxes, chemical potential and surface-tension force in single
+     * precision; fields, reductions and solvers stay FP64); 0 is the plain
+     * FP64 path that matches the reference */
+    int stencil_fp32;
 } pvof_params;
 
 /* Field identifiers for upload/download. */

@@ -315,11 +315,17 @@ void v_range(const pvof_ctx *c, int &i0, int &i1, int &j0, int &j1)
 // routines
 // ---------------------------------------------------------------------------
 
-// VOF_DIFFUSE_compute_laplacian (VOF_DIFFUSE.c:834-861)
-int compute_laplacian(pvof_ctx *c, double *in, double *out)
+// the FP32 stencil form: WENO5, chemical-potential and surface-tension
+// stencils in single precision (fields, reductions and solvers stay FP64)
+bool fp32_stencils(const pvof_ctx *c) { return c->p.stencil_fp32 != 0; }
+
+// VOF_DIFFUSE_compute_laplacian (VOF_DIFFUSE.c:834-861); fp32: the
+// single-precision stencil of the FP32 form
+int compute_laplacian(pvof_ctx *c, double *in, double *out, bool fp32 = false)
 {
     TRY(fill(c, BK_SCALAR, in));
-    TRY(launch2d(c, k_laplacian, 0, c->dom.NX, 0, c->dom.NY, (const double *)in, out));
+    if (fp32) TRY(launch2d(c, k_laplacian_f, 0, c->dom.NX, 0, c->dom.NY, (const double *)in, out));
+    else TRY(launch2d(c, k_laplacian, 0, c->dom.NX, 0, c->dom.NY, (const double *)in, out));
     return fill(c, BK_SCALAR, out);
 }
 
@@ -328,8 +334,12 @@ int advect(pvof_ctx *c, double *out)
     const int NX = c->dom.NX, NY = c->dom.NY;
     double *CL = F(c, PVOF_F_C_L);
     TRY(fill(c, BK_SCALAR, CL));
-    TRY(launch2d(c, k_weno_flux, 0, NX, 0, NY, (const double *)CL, (const double *)F(c, PVOF_F_U),
-                 (const double *)F(c, PVOF_F_V), S(c, SC_FLUX_X), S(c, SC_FLUX_Y), c->p.weno_order == 5 ? 1 : 0));
+    if (fp32_stencils(c))
+        TRY(launch2d(c, k_weno_flux_f, 0, NX, 0, NY, (const double *)CL, (const double *)F(c, PVOF_F_U),
+                     (const double *)F(c, PVOF_F_V), S(c, SC_FLUX_X), S(c, SC_FLUX_Y), c->p.weno_order == 5 ? 1 : 0));
+    else
+        TRY(launch2d(c, k_weno_flux, 0, NX, 0, NY, (const double *)CL, (const double *)F(c, PVOF_F_U),
+                     (const double *)F(c, PVOF_F_V), S(c, SC_FLUX_X), S(c, SC_FLUX_Y), c->p.weno_order == 5 ? 1 : 0));
     TRY(fill(c, BK_WRAP_U, S(c, SC_FLUX_X)));
     TRY(fill(c, BK_WRAP_V, S(c, SC_FLUX_Y)));
     TRY(launch2d(c, k_flux_div, 0, NX, 0, NY, (const double *)S(c, SC_FLUX_X), (const double *)S(c, SC_FLUX_Y), out));
@@ -396,9 +406,10 @@ int vof_diffuse_step(pvof_ctx *c)
     double *psiLG = F(c, PVOF_F_PSI_LG);
     // R(C) = -div(u C) + Pe^-1 L S(C)  (VOF_DIFFUSE.c:1287-1297)
     TRY(advect(c, cur));
-    TRY(launch2d(c, k_bulk_S, 0, NX, 0, NY, (const double *)CL, (const double *)F(c, PVOF_F_C_S), bS));
+    if (fp32_stencils(c)) TRY(launch2d(c, k_bulk_S_f, 0, NX, 0, NY, (const double *)CL, (const double *)F(c, PVOF_F_C_S), bS));
+    else TRY(launch2d(c, k_bulk_S, 0, NX, 0, NY, (const double *)CL, (const double *)F(c, PVOF_F_C_S), bS));
     TRY(fill(c, BK_SCALAR, bS));
-    TRY(compute_laplacian(c, bS, aux));
+    TRY(compute_laplacian(c, bS, aux, fp32_stencils(c)));
     TRY(launch2d(c, k_div_by, 0, NX, 0, NY, aux, c->p.Pe_CH));
     TRY(fill(c, BK_SCALAR, aux));
     TRY(launch2d(c, k_add, 0, NX, 0, NY, cur, (const double *)aux));
@@ -459,9 +470,13 @@ int update_density_viscosity(pvof_ctx *c)
 int compute_psi_LG(pvof_ctx *c)
 {
     double *CL = F(c, PVOF_F_C_L), *lap = F(c, PVOF_F_LAP_C), *psi = F(c, PVOF_F_PSI_LG);
-    TRY(compute_laplacian(c, CL, lap));
-    TRY(launch2d(c, k_psi_LG, 0, c->dom.NX, 0, c->dom.NY, (const double *)CL, (const double *)lap, psi,
-                 c->p.Cn * c->p.Cn));
+    TRY(compute_laplacian(c, CL, lap, fp32_stencils(c)));
+    if (fp32_stencils(c))
+        TRY(launch2d(c, k_psi_LG_f, 0, c->dom.NX, 0, c->dom.NY, (const double *)CL, (const double *)lap, psi,
+                     c->p.Cn * c->p.Cn));
+    else
+        TRY(launch2d(c, k_psi_LG, 0, c->dom.NX, 0, c->dom.NY, (const double *)CL, (const double *)lap, psi,
+                     c->p.Cn * c->p.Cn));
     return fill(c, BK_SCALAR, psi);
 }
 
@@ -471,6 +486,11 @@ int compute_f_sigma(pvof_ctx *c)
     u_range(c, ui0, ui1, uj0, uj1);
     v_range(c, vi0, vi1, vj0, vj1);
     const double scale = 2.0 * 6.0 * std::sqrt(2.0) / (c->p.Cn * c->p.We + 1e-30);
+    if (fp32_stencils(c))
+        return launch2d(c, k_f_sigma_f, 0, c->dom.NX, 0, c->dom.NY, (const double *)F(c, PVOF_F_C_L),
+                        (const double *)F(c, PVOF_F_C_G), (const double *)F(c, PVOF_F_C_S),
+                        (const double *)F(c, PVOF_F_PSI_LG), F(c, PVOF_F_FSIG_NEW_X), F(c, PVOF_F_FSIG_NEW_Y), scale,
+                        ui0, ui1, uj1, vj0, vi1, vj1);
     return launch2d(c, k_f_sigma, 0, c->dom.NX, 0, c->dom.NY, (const double *)F(c, PVOF_F_C_L),
                     (const double *)F(c, PVOF_F_C_G), (const double *)F(c, PVOF_F_C_S),
                     (const double *)F(c, PVOF_F_PSI_LG), F(c, PVOF_F_FSIG_NEW_X), F(c, PVOF_F_FSIG_NEW_Y), scale, ui0,

@@ -41,6 +41,42 @@ __device__ __forceinline__ double lap_at(const Dom &d, int i, int j, Get get)
     return (m.r_u[i + 1] * dfdxE - m.r_u[i] * dfdxW) * m.idx_u[i] * m.inv_r_c[i] + (dfdyN - dfdyS) * m.idy_v[j];
 }
 
+// The same Laplacian in single precision (the FP32 stencil form): the
+// operands are rounded to float on load, the metrics too.
+template <class Get>
+__device__ __forceinline__ float lap_at_f(const Dom &d, int i, int j, Get get)
+{
+    const Metrics &m = d.m;
+    const float c = (float)get(i, j);
+    const float dfdxE = ((float)get(i + 1, j) - c) * (float)m.idx_c[i];
+    const float dfdxW = (c - (float)get(i - 1, j)) * (float)((i != 0) ? m.idx_c[i - 1] : m.idx_c[i]);
+    const float dfdyN = ((float)get(i, j + 1) - c) * (float)m.idy_c[j];
+    const float dfdyS = (c - (float)get(i, j - 1)) * (float)((j != 0) ? m.idy_c[j - 1] : m.idy_c[j]);
+    if (d.planar)
+        return (dfdxE - dfdxW) * (float)m.idx_u[i] + (dfdyN - dfdyS) * (float)m.idy_v[j];
+    return ((float)m.r_u[i + 1] * dfdxE - (float)m.r_u[i] * dfdxW) * (float)m.idx_u[i] * (float)m.inv_r_c[i] +
+           (dfdyN - dfdyS) * (float)m.idy_v[j];
+}
+
+// diffuse_weno5_left in single precision (the FP32 stencil form)
+__device__ __forceinline__ float weno5_left_f(float v0, float v1, float v2, float v3, float v4)
+{
+    const float eps = 1e-6f;
+    const float q0 = (2.0f * v0 - 7.0f * v1 + 11.0f * v2) * (1.0f / 6.0f);
+    const float q1 = (-v1 + 5.0f * v2 + 2.0f * v3) * (1.0f / 6.0f);
+    const float q2 = (2.0f * v2 + 5.0f * v3 - v4) * (1.0f / 6.0f);
+    const float t0 = v0 - 2.0f * v1 + v2, t1 = v0 - 4.0f * v1 + 3.0f * v2;
+    const float b0 = (13.0f / 12.0f) * (t0 * t0) + 0.25f * (t1 * t1);
+    const float t2 = v1 - 2.0f * v2 + v3, t3 = v1 - v3;
+    const float b1 = (13.0f / 12.0f) * (t2 * t2) + 0.25f * (t3 * t3);
+    const float t4 = v2 - 2.0f * v3 + v4, t5 = 3.0f * v2 - 4.0f * v3 + v4;
+    const float b2 = (13.0f / 12.0f) * (t4 * t4) + 0.25f * (t5 * t5);
+    const float a0 = 0.1f / ((eps + b0) * (eps + b0));
+    const float a1 = 0.6f / ((eps + b1) * (eps + b1));
+    const float a2 = 0.3f / ((eps + b2) * (eps + b2));
+    return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+}
+
 // diffuse_weno5_left (Eulerian/VOF_DIFFUSE.c:431-451); pow(x, 2.0) is x*x
 __device__ __forceinline__ double weno5_left(double v0, double v1, double v2, double v3, double v4)
 {

@@ -66,6 +66,27 @@ __global__ void k_weno_flux(Dom d, int i0, int i1, int j0, int j1, const double 
     AT_(fy, i, j) = vel * st;
 }
 
+// the same face fluxes with the WENO5 states and the products in single
+// precision (the FP32 stencil form); each face flux is one stored value that
+// the two cells beside it share, so the divergence still telescopes
+__global__ void k_weno_flux_f(Dom d, int i0, int i1, int j0, int j1, const double *__restrict__ C,
+                              const double *__restrict__ u, const double *__restrict__ v,
+                              double *__restrict__ fx, double *__restrict__ fy, int weno5)
+{
+    KERNEL_2D_INDEX
+    auto c = [&](int a, int b) { return (float)AT_(C, a, b); };
+    float vel = (float)AT_(u, i, j), st;
+    if (weno5) st = (vel >= 0.0f) ? weno5_left_f(c(i - 3, j), c(i - 2, j), c(i - 1, j), c(i, j), c(i + 1, j))
+                                  : weno5_left_f(c(i + 2, j), c(i + 1, j), c(i, j), c(i - 1, j), c(i - 2, j));
+    else st = (vel >= 0.0f) ? c(i - 1, j) : c(i, j);
+    AT_(fx, i, j) = (double)(vel * st);
+    vel = (float)AT_(v, i, j);
+    if (weno5) st = (vel >= 0.0f) ? weno5_left_f(c(i, j - 3), c(i, j - 2), c(i, j - 1), c(i, j), c(i, j + 1))
+                                  : weno5_left_f(c(i, j + 2), c(i, j + 1), c(i, j), c(i, j - 1), c(i, j - 2));
+    else st = (vel >= 0.0f) ? c(i, j - 1) : c(i, j);
+    AT_(fy, i, j) = (double)(vel * st);
+}
+
 // rhs = -div(flux), TwodOps_scalar_flux_divergence (TwodOps.c:201-229)
 __global__ void k_flux_div(Dom d, int i0, int i1, int j0, int j1, const double *__restrict__ fx,
                            const double *__restrict__ fy, double *__restrict__ out)
@@ -86,6 +107,23 @@ __global__ void k_bulk_S(Dom d, int i0, int i1, int j0, int j1, const double *__
     KERNEL_2D_INDEX
     double c = AT_(CL, i, j), cs = AT_(CS, i, j);
     AT_(bS, i, j) = 0.5 * c - 1.5 * c * c + c * c * c - c * cs * (1.0 - c - cs);
+}
+
+// bulk S in single precision (the FP32 stencil form)
+__global__ void k_bulk_S_f(Dom d, int i0, int i1, int j0, int j1, const double *__restrict__ CL,
+                           const double *__restrict__ CS, double *__restrict__ bS)
+{
+    KERNEL_2D_INDEX
+    const float c = (float)AT_(CL, i, j), cs = (float)AT_(CS, i, j);
+    AT_(bS, i, j) = (double)(0.5f * c - 1.5f * c * c + c * c * c - c * cs * (1.0f - c - cs));
+}
+
+// the Laplacian in single precision (the FP32 stencil form)
+__global__ void k_laplacian_f(Dom d, int i0, int i1, int j0, int j1, const double *__restrict__ in,
+                              double *__restrict__ out)
+{
+    KERNEL_2D_INDEX
+    AT_(out, i, j) = (double)lap_at_f(d, i, j, [&](int a, int b) { return AT_(in, a, b); });
 }
 
 // TwodOps_scalar_laplacian over the G range (VOF_DIFFUSE.c:834-861)
@@ -228,6 +266,49 @@ __global__ void k_psi_LG(Dom d, int i0, int i1, int j0, int j1, const double *__
     KERNEL_2D_INDEX
     double c = AT_(CL, i, j);
     AT_(psi, i, j) = c * c * c - 1.5 * c * c + 0.5 * c - cn2 * AT_(lap, i, j);
+}
+
+// psi_LG in single precision (the FP32 stencil form)
+__global__ void k_psi_LG_f(Dom d, int i0, int i1, int j0, int j1, const double *__restrict__ CL,
+                           const double *__restrict__ lap, double *__restrict__ psi, double cn2)
+{
+    KERNEL_2D_INDEX
+    const float c = (float)AT_(CL, i, j);
+    AT_(psi, i, j) = (double)(c * c * c - 1.5f * c * c + 0.5f * c - (float)cn2 * (float)AT_(lap, i, j));
+}
+
+// f_sigma in single precision (the FP32 stencil form); the band test on the
+// averaged fractions stays as the reference's
+__global__ void k_f_sigma_f(Dom d, int i0, int i1, int j0, int j1, const double *__restrict__ CL,
+                            const double *__restrict__ CG, const double *__restrict__ CS,
+                            const double *__restrict__ psi, double *__restrict__ fx, double *__restrict__ fy,
+                            double scale, int ui0, int ui1, int uj1, int vj0, int vi1, int vj1)
+{
+    KERNEL_2D_INDEX
+    float vx = 0.0f, vy = 0.0f;
+    const float sc = (float)scale;
+    if (i >= ui0 && i < ui1 && j < uj1) {
+        const float cl = 0.5f * ((float)AT_(CL, i, j) + (float)AT_(CL, i - 1, j));
+        const float cg = 0.5f * ((float)AT_(CG, i, j) + (float)AT_(CG, i - 1, j));
+        const float cs = 0.5f * ((float)AT_(CS, i, j) + (float)AT_(CS, i - 1, j));
+        if (!(cl < 0.005f || cl > 0.995f || cg < 0.005f || cg > 0.995f || cs > 0.05f)) {
+            const float pf = 0.5f * ((float)AT_(psi, i, j) + (float)AT_(psi, i - 1, j));
+            const float gc = ((float)AT_(CL, i, j) - (float)AT_(CL, i - 1, j)) * (float)d.m.idx_c[i - 1];
+            vx = sc * pf * gc;
+        }
+    }
+    if (j >= vj0 && j < vj1 && i < vi1) {
+        const float cl = 0.5f * ((float)AT_(CL, i, j) + (float)AT_(CL, i, j - 1));
+        const float cg = 0.5f * ((float)AT_(CG, i, j) + (float)AT_(CG, i, j - 1));
+        const float cs = 0.5f * ((float)AT_(CS, i, j) + (float)AT_(CS, i, j - 1));
+        if (!(cl < 0.005f || cl > 0.995f || cg < 0.005f || cg > 0.995f || cs > 0.05f)) {
+            const float pf = 0.5f * ((float)AT_(psi, i, j) + (float)AT_(psi, i, j - 1));
+            const float gc = ((float)AT_(CL, i, j) - (float)AT_(CL, i, j - 1)) * (float)d.m.idy_c[j - 1];
+            vy = sc * pf * gc;
+        }
+    }
+    AT_(fx, i, j) = (double)vx;
+    AT_(fy, i, j) = (double)vy;
 }
 
 // VOF_DIFFUSE_compute_f_sigma (VOF_DIFFUSE.c:1364-1445): zero the G range,

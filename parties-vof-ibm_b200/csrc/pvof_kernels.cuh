@@ -50,6 +50,15 @@ struct PresArgs {
 __global__ void k_fill(Dom d, BcMap m, double *f);
 __global__ void k_weno_flux(Dom d, int i0, int i1, int j0, int j1, const double *C, const double *u, const double *v,
                             double *fx, double *fy, int weno5);
+__global__ void k_weno_flux_f(Dom d, int i0, int i1, int j0, int j1, const double *C, const double *u,
+                              const double *v, double *fx, double *fy, int weno5);
+__global__ void k_bulk_S_f(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *CS, double *bS);
+__global__ void k_laplacian_f(Dom d, int i0, int i1, int j0, int j1, const double *in, double *out);
+__global__ void k_psi_LG_f(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *lap, double *psi,
+                           double cn2);
+__global__ void k_f_sigma_f(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *CG,
+                            const double *CS, const double *psi, double *fx, double *fy, double scale, int ui0,
+                            int ui1, int uj1, int vj0, int vi1, int vj1);
 __global__ void k_flux_div(Dom d, int i0, int i1, int j0, int j1, const double *fx, const double *fy, double *out);
 __global__ void k_bulk_S(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *CS, double *bS);
 __global__ void k_laplacian(Dom d, int i0, int i1, int j0, int j1, const double *in, double *out);

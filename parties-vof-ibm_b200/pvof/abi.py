@@ -77,6 +77,7 @@ class Params(C.Structure):
         ("gravity", C.c_int),
         ("contact_angle_deg", C.c_double),
         ("N_forcing_loops", C.c_int),
+        ("stencil_fp32", C.c_int),
     ]
 
 

@@ -82,6 +82,7 @@ def default_params(**kw):
     p.gravity = 1
     p.contact_angle_deg = 90.0
     p.N_forcing_loops = 2
+    p.stencil_fp32 = 0
     for k, v in kw.items():
         setattr(p, k, v)
     return p
