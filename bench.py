@@ -21,9 +21,11 @@ host buffers before every step and downloaded after it.
 --batch-cases K additionally times K replicas of the workload advanced
 concurrently by pvof_run_steps_batched (the batched form: one host thread and
 stream per case, so the cluster-resident solvers of different cases run on
-different SMs) and adds a "batched" object to the line; --batch-form fp32 runs
-the replicas in the FP32 stencil form and reports their error against the
-FP64 path.
+different SMs) and adds a "batched" object to the line; --batch-form fp32
+(fp32-warm) runs the replicas in the FP32 stencil form (plus the pressure
+warm start) and reports their error against the FP64 path.  --forms adds a
+"forms" object: the workload in the FP32-stencil + warm-start form, its
+throughput against the plain path's and its error.
 
 --impl reference runs the reference's own time step (compiled from its
 sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host:
@@ -244,6 +246,39 @@ def run_ours(args):
     t_max = max_over_ranks(dist, total_ms)
     value = ws * cells * args.steps / (t_max * 1e-3)
 
+    # ---- the chosen forms on the same workload (optional) ---------------------
+    forms = None
+    if args.forms:
+        import numpy as np
+        snap = {f: g.get(f) for f in ("U", "V", "P", "C_L")}
+        m64 = g.liquid_mass()
+        fparams = abi.Params.from_buffer_copy(params)
+        fparams.stencil_fp32 = 1
+        fparams.pressure_warm_start = 1
+        fg = runtime.Solver(grid, fparams, device=local)
+        fg.set_planes(planes)
+        fg.initialize()
+        for _ in range(args.warmup):
+            fg.run_steps(1, DT)
+        fg.set_solver_timing(True)
+        f_ms = 0.0
+        for _ in range(args.steps):
+            fg.flush_l2()
+            fg.timer_start()
+            fg.run_steps(1, DT)
+            f_ms += fg.timer_stop()
+        fp_it = fg.solver_timing(2)["iterations"]
+        err = {"velocity_rel_l2": max(float(np.linalg.norm(fg.get(f) - snap[f]) / np.linalg.norm(snap[f]))
+                                      for f in ("U", "V")),
+               "pressure_rel_l2": float(np.linalg.norm(fg.get("P") - snap["P"]) / np.linalg.norm(snap["P"])),
+               "volume_rel": abs(fg.liquid_mass() - m64) / abs(m64)}
+        fvalue = cells * args.steps / (f_ms * 1e-3)
+        forms = {"form": "fp32 stencils + pressure warm start (same stage of the previous step)",
+                 "value": fvalue, "unit": UNIT, "ms_per_step": f_ms / args.steps, "vs_plain": fvalue / value,
+                 "pressure_iterations": fp_it, "pressure_iterations_plain": timing[2]["iterations"],
+                 "error_vs_fp64": err}
+        fg.close()
+
     # ---- end to end through the C ABI with host buffers ---------------------
     blocks = {f: pinned_like(g.block_count(f)) for f in STATE_FIELDS}
     for f in STATE_FIELDS:
@@ -284,7 +319,8 @@ def run_ours(args):
     if args.batch_cases > 1:
         from pvof import abi
         bparams = abi.Params.from_buffer_copy(params)
-        bparams.stencil_fp32 = 1 if args.batch_form == "fp32" else 0
+        bparams.stencil_fp32 = 1 if args.batch_form in ("fp32", "fp32-warm") else 0
+        bparams.pressure_warm_start = 1 if args.batch_form == "fp32-warm" else 0
         reps = []
         for q in range(args.batch_cases):
             r = runtime.Solver(grid, bparams, device=local)
@@ -304,8 +340,9 @@ def run_ours(args):
                    "ms_per_step": span / bsteps, "vs_single": bvalue / (cells * args.steps / (total_ms * 1e-3)),
                    "note": "replicas of the workload advanced concurrently by pvof_run_steps_batched "
                            "(one host thread and stream per case); device time of the slowest case",
-                   "form": "fp32-stencils" if args.batch_form == "fp32" else "fp64"}
-        if args.batch_form == "fp32":
+                   "form": {"fp64": "fp64", "fp32": "fp32-stencils",
+                            "fp32-warm": "fp32-stencils + pressure warm start"}[args.batch_form]}
+        if args.batch_form != "fp64":
             import numpy as np
             # the error of the form: one replica against the FP64 path after the same steps
             ref = runtime.Solver(grid, params, device=local)
@@ -353,6 +390,8 @@ def run_ours(args):
             line["cpu_baseline"] = cpu
         if batched is not None:
             line["batched"] = batched
+        if forms is not None:
+            line["forms"] = forms
         print(json.dumps(line))
     g.close()
     if dist is not None:
@@ -373,7 +412,9 @@ def main():
     ap.add_argument("--batch-cases", type=int, default=0,
                     help="also time this many replicas advanced concurrently (batched form)")
     ap.add_argument("--batch-steps", type=int, default=10)
-    ap.add_argument("--batch-form", default="fp64", choices=["fp64", "fp32"],
+    ap.add_argument("--forms", action="store_true",
+                    help="also time the FP32-stencil + pressure warm-start form on the workload (error against FP64)")
+    ap.add_argument("--batch-form", default="fp64", choices=["fp64", "fp32", "fp32-warm"],
                     help="fp32: the batched replicas use the FP32 stencil form (error against FP64 reported)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

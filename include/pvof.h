@@ -105,6 +105,11 @@ typedef struct pvof_params {
      * precision; fields, reductions and solvers stay FP64); 0 is the plain
      * FP64 path that matches the reference */
     int stencil_fp32;
+    /* no counterpart in the reference: 1 starts the first pressure solve of a
+     * substep from the correction of the same RK stage of the previous time
+     * step instead of zero; the solve still stops at the same absolute
+     * residual, so the result moves within that tolerance */
+    int pressure_warm_start;
 } pvof_params;
 
 /* Field identifiers for upload/download. */

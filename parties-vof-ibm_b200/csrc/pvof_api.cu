@@ -645,9 +645,16 @@ static double host_idx_u1(const pvof_ctx *c)
 
 namespace {
 
-int p_set_rhs(pvof_ctx *c)
+// warm: start from the correction of the same stage of the previous time
+// step instead of zero (the warm-start form)
+int p_set_rhs(pvof_ctx *c, bool warm = false)
 {
-    CK(cudaMemsetAsync(c->base[PVOF_F_DELTAP], 0, c->plane_elems * sizeof(double), c->stream));
+    if (warm) {
+        CK(cudaMemcpyAsync(c->base[PVOF_F_DELTAP], c->sbase[SC_PHI_PREV + c->stage], c->plane_elems * sizeof(double),
+                           cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+        CK(cudaMemsetAsync(c->base[PVOF_F_DELTAP], 0, c->plane_elems * sizeof(double), c->stream));
+    }
     double a_dt = 1.0 / (c->dt * 2.0 * bet(c->stage));
     double ihdt = host_idx_u1(c) * a_dt;
     return launch2d(c, k_p_rhs, 0, c->dom.NX - 1, 0, c->dom.NY - 1, (const double *)F(c, PVOF_F_U),
@@ -752,6 +759,7 @@ int initialize(pvof_ctx *c)
         CK(cudaMemcpyAsync(c->base[PVOF_F_FSIG_OLD_Y], c->base[PVOF_F_FSIG_NEW_Y], bytes, cudaMemcpyDeviceToDevice, c->stream));
     }
     if (resolved(c)) TRY(ibm_velocity_init(c));   // Cart3d.c:505-515
+    c->phi_prev_mask = 0;
     TRY(cell_center(c));
     c->time = 0.0;
     return PVOF_OK;
@@ -802,7 +810,7 @@ int substep(pvof_ctx *c, pvof_stats *st)
     int passes = 0, p_total = 0;
     int rc = PVOF_OK;
     for (;;) {
-        TRY(p_set_rhs(c));
+        TRY(p_set_rhs(c, passes == 0 && c->p.pressure_warm_start && (c->phi_prev_mask >> c->stage & 1)));
         TRY(p_precond(c));
         TRY(p_solve(c));
         TRY(p_project(c));
@@ -814,6 +822,11 @@ int substep(pvof_ctx *c, pvof_stats *st)
         p_total += c->scal_host->p_iters;
         if (passes > 10) { rc = set_err(PVOF_EDIVERGED, "Poisson solver did not converge"); break; }
         if (!(c->scal_host->div_max > 1e-6)) break;
+    }
+    if (c->p.pressure_warm_start && rc == PVOF_OK) {
+        CK(cudaMemcpyAsync(c->sbase[SC_PHI_PREV + c->stage], c->base[PVOF_F_DELTAP], c->plane_elems * sizeof(double),
+                           cudaMemcpyDeviceToDevice, c->stream));
+        c->phi_prev_mask |= 1 << c->stage;
     }
     if (c->p.surface_tension) swap_f_sigma(c);
     if (solids && rc == PVOF_OK) TRY(ibm_advect(c));   // Temporal_int.c:1186-1238

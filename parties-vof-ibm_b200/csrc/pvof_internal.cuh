@@ -85,7 +85,7 @@ enum Scratch {
     SC_PSI = 0, SC_BULK_S, SC_CH_AUX1, SC_CH_RHS_NM1, SC_CH_RES, SC_CH_DIR, SC_CH_DIR2,
     SC_FLUX_X, SC_FLUX_Y, SC_P_RES, SC_P_D, SC_P_AD, SC_P_MINV,
     SC_U_R, SC_U_D, SC_U_AD, SC_U_DIAG, SC_V_R, SC_V_D, SC_V_AD, SC_V_DIAG,
-    SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_SNAP, SC_COUNT
+    SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_SNAP, SC_PHI_PREV, SC_PHI_PREV1, SC_PHI_PREV2, SC_COUNT
 };
 
 // device-side scalars written by solver kernels and read once per substep
@@ -132,6 +132,7 @@ struct Ctx {
     size_t cgs_v_smem;       // same, velocity solver for both components (0: grid solver)
     int cgs_p_threads, cgs_v_threads;   // their threads per CTA
     int vel_one_cluster;     // momentum solve as u then v on one cluster (batched runs)
+    int phi_prev_mask;       // stages whose last correction is kept in SC_PHI_PREV + stage
     int coop_blocks;         // co-resident blocks for the persistent solvers
     int coop_threads;
     long long launches;      // kernels launched by this context

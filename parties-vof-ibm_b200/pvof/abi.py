@@ -78,6 +78,7 @@ class Params(C.Structure):
         ("contact_angle_deg", C.c_double),
         ("N_forcing_loops", C.c_int),
         ("stencil_fp32", C.c_int),
+        ("pressure_warm_start", C.c_int),
     ]
 
 

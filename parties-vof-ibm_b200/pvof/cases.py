@@ -83,6 +83,7 @@ def default_params(**kw):
     p.contact_angle_deg = 90.0
     p.N_forcing_loops = 2
     p.stencil_fp32 = 0
+    p.pressure_warm_start = 0
     for k, v in kw.items():
         setattr(p, k, v)
     return p
