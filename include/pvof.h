@@ -31,6 +31,7 @@
 #define PVOF_H
 
 #include <stddef.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -107,8 +108,10 @@ typedef struct pvof_params {
     int stencil_fp32;
     /* no counterpart in the reference: 1 starts the first pressure solve of a
      * substep from the correction of the same RK stage of the previous time
-     * step instead of zero; the solve still stops at the same absolute
-     * residual, so the result moves within that tolerance */
+     * step instead of zero; 2 adds to it the change predicted by the network
+     * set with pvof_set_pressure_network (the learned warm start); the solve
+     * still stops at the same absolute residual, so the result moves within
+     * that tolerance */
     int pressure_warm_start;
 } pvof_params;
 
@@ -310,6 +313,40 @@ int pvof_Velocity_solve_explicit(pvof_ctx *ctx, char component);
  * predictor on the momentum RHS, force_iter >= 0 that many corrector passes on
  * the velocity; call pvof_Lagrangian_flag_points() first */
 int pvof_Lagrangian_force(pvof_ctx *ctx, int force_iter);
+
+/* --- learned warm start (no counterpart in the reference) --------------- */
+/* The network: six 3x3 convolutions 3 -> 32 -> 32 -> 32 -> 32 -> 32 -> 1,
+ * zero padding, ReLU between them, BF16 weights with FP32 accumulation.
+ * Parameters are one flat FP32 array [w0, b0, ..., w5, b5], w_l laid out
+ * [cout][cin][3][3]; planes are channel-major [C][H][W] floats on the device.
+ * Inputs: rho, rhs / rms(rhs), phi_prev / rms(phi_prev); output: the change
+ * of the pressure correction over rms(phi_prev). */
+size_t pvof_cnn_param_count(void);
+/* floats of the work buffer (activations) for an H x W plane */
+size_t pvof_cnn_work_floats(int H, int W);
+/* forward pass; y may be NULL (the output stays in the work buffer) */
+int pvof_cnn_forward(const float *params, const uint16_t *params_bf16, const float *x, float *y, int H, int W,
+                     float *work, void *stream);
+/* backward pass after pvof_cnn_forward with the same work buffer: adds the
+ * parameter gradient of dL/dy to grad */
+int pvof_cnn_backward(const float *params, const uint16_t *params_bf16, const float *x, const float *dy, float *grad,
+                      int H, int W, float *work, void *stream);
+/* mean-square loss of y against t over n values (added to *loss on the
+ * device) and its gradient dy */
+int pvof_cnn_mse(const float *y, const float *t, float *dy, size_t n, double *loss, void *stream);
+/* one Adam step (step counts from 1) on the FP32 parameters and their BF16 copy */
+int pvof_cnn_adam(float *params, const float *grad, float *m, float *v, uint16_t *params_bf16, int step, float lr,
+                  void *stream);
+/* the BF16 copy of FP32 parameters */
+int pvof_cnn_to_bf16(const float *params, uint16_t *params_bf16, void *stream);
+/* the network the context's pressure_warm_start == 2 uses (host array of
+ * pvof_cnn_param_count() floats) */
+int pvof_set_pressure_network(pvof_ctx *ctx, const float *params, size_t n);
+/* a training sample from the last substep of `stage` (with
+ * pressure_warm_start on, once two time steps have run): the network inputs
+ * (x: 3 planes) and target (t: 1 plane) on the (NYM x NXM) physical cells,
+ * device arrays */
+int pvof_pressure_network_sample(pvof_ctx *ctx, int stage, float *x, float *t);
 
 /* --- measurement (no counterpart in the reference) ---------------------- */
 /* Number of CUDA kernels this context has launched so far. */

@@ -645,20 +645,71 @@ static double host_idx_u1(const pvof_ctx *c)
 
 namespace {
 
+int p_precond(pvof_ctx *c);
+
+// the learned warm start's network inputs (and target) from the density, the
+// pressure right-hand side and the kept corrections (pvof_cnn.cu)
+int cnn_prepare(pvof_ctx *c, const double *phi_prev, const double *phi, float *x, float *t)
+{
+    const unsigned nb = 148;
+    const int n = (c->dom.NX - 1) * (c->dom.NY - 1);
+    double *r0 = S(c, SC_SNAP);   // free during the pressure solve
+    k_cnn_residual<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->dom, c->maps[BK_PRESSURE], F(c, PVOF_F_RHO),
+                                                                      F(c, PVOF_F_P_RHS), phi_prev, r0);
+    CKL(c);
+    k_cnn_sumsq<<<nb, 256, 0, c->stream>>>(c->dom, r0, phi_prev, c->partials);
+    CKL(c);
+    k_finalize_sum<<<1, 256, 0, c->stream>>>(c->partials, (int)nb, &c->scal->cnn_ms[0]);
+    CKL(c);
+    k_finalize_sum<<<1, 256, 0, c->stream>>>(c->partials + nb, (int)nb, &c->scal->cnn_ms[1]);
+    CKL(c);
+    k_cnn_assemble<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->dom, F(c, PVOF_F_RHO), r0, phi_prev, phi,
+                                                                      c->scal, x, t);
+    CKL(c);
+    return PVOF_OK;
+}
+
 // warm: start from the correction of the same stage of the previous time
-// step instead of zero (the warm-start form)
+// step instead of zero (the warm-start form); with the network set and
+// pressure_warm_start == 2, from that correction plus the network's
+// predicted change
 int p_set_rhs(pvof_ctx *c, bool warm = false)
 {
-    if (warm) {
-        CK(cudaMemcpyAsync(c->base[PVOF_F_DELTAP], c->sbase[SC_PHI_PREV + c->stage], c->plane_elems * sizeof(double),
-                           cudaMemcpyDeviceToDevice, c->stream));
-    } else {
-        CK(cudaMemsetAsync(c->base[PVOF_F_DELTAP], 0, c->plane_elems * sizeof(double), c->stream));
-    }
     double a_dt = 1.0 / (c->dt * 2.0 * bet(c->stage));
     double ihdt = host_idx_u1(c) * a_dt;
-    return launch2d(c, k_p_rhs, 0, c->dom.NX - 1, 0, c->dom.NY - 1, (const double *)F(c, PVOF_F_U),
-                    (const double *)F(c, PVOF_F_V), F(c, PVOF_F_P_RHS), ihdt);
+    TRY(launch2d(c, k_p_rhs, 0, c->dom.NX - 1, 0, c->dom.NY - 1, (const double *)F(c, PVOF_F_U),
+                 (const double *)F(c, PVOF_F_V), F(c, PVOF_F_P_RHS), ihdt));
+    if (!warm) {
+        CK(cudaMemsetAsync(c->base[PVOF_F_DELTAP], 0, c->plane_elems * sizeof(double), c->stream));
+        return PVOF_OK;
+    }
+    CK(cudaMemcpyAsync(c->base[PVOF_F_DELTAP], c->sbase[SC_PHI_PREV + c->stage], c->plane_elems * sizeof(double),
+                       cudaMemcpyDeviceToDevice, c->stream));
+    if (c->p.pressure_warm_start == 2 && c->cnn_params) {
+        const double *prev = S(c, SC_PHI_PREV + c->stage);
+        TRY(cnn_prepare(c, prev, nullptr, c->cnn_x, nullptr));
+        const int rc = pvof_cnn_forward(c->cnn_params, c->cnn_bf16, c->cnn_x, c->cnn_y, c->dom.NY - 1, c->dom.NX - 1,
+                                        c->cnn_work, c->stream);
+        if (rc != PVOF_OK) return set_err(rc, "network forward pass");
+        c->launches += 7;
+        const int n = (c->dom.NX - 1) * (c->dom.NY - 1);
+        const unsigned nb = 148;
+        double *e = S(c, SC_P_D2);   // free until the solve starts
+        CK(cudaMemsetAsync(c->sbase[SC_P_D2], 0, c->plane_elems * sizeof(double), c->stream));
+        k_cnn_expand<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->dom, c->cnn_y, e);
+        CKL(c);
+        TRY(p_precond(c));   // M for the step; the loop computes it again from the same rho
+        k_cnn_galerkin<<<nb, 256, 0, c->stream>>>(c->dom, c->maps[BK_PRESSURE], F(c, PVOF_F_RHO), e, S(c, SC_SNAP),
+                                                  S(c, SC_P_MINV), c->partials);
+        CKL(c);
+        k_finalize_sum<<<1, 256, 0, c->stream>>>(c->partials, (int)nb, &c->scal->cnn_ms[0]);
+        CKL(c);
+        k_finalize_sum<<<1, 256, 0, c->stream>>>(c->partials + nb, (int)nb, &c->scal->cnn_ms[1]);
+        CKL(c);
+        k_cnn_apply<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->dom, e, prev, c->scal, F(c, PVOF_F_DELTAP));
+        CKL(c);
+    }
+    return PVOF_OK;
 }
 
 int p_precond(pvof_ctx *c)
@@ -760,6 +811,7 @@ int initialize(pvof_ctx *c)
     }
     if (resolved(c)) TRY(ibm_velocity_init(c));   // Cart3d.c:505-515
     c->phi_prev_mask = 0;
+    c->phi_old_mask = 0;
     TRY(cell_center(c));
     c->time = 0.0;
     return PVOF_OK;
@@ -824,8 +876,14 @@ int substep(pvof_ctx *c, pvof_stats *st)
         if (!(c->scal_host->div_max > 1e-6)) break;
     }
     if (c->p.pressure_warm_start && rc == PVOF_OK) {
-        CK(cudaMemcpyAsync(c->sbase[SC_PHI_PREV + c->stage], c->base[PVOF_F_DELTAP], c->plane_elems * sizeof(double),
-                           cudaMemcpyDeviceToDevice, c->stream));
+        const size_t bytes = c->plane_elems * sizeof(double);
+        if (c->phi_prev_mask >> c->stage & 1) {   // one generation back, for the network's samples
+            CK(cudaMemcpyAsync(c->sbase[SC_PHI_OLD + c->stage], c->sbase[SC_PHI_PREV + c->stage], bytes,
+                               cudaMemcpyDeviceToDevice, c->stream));
+            c->phi_old_mask |= 1 << c->stage;
+        }
+        CK(cudaMemcpyAsync(c->sbase[SC_PHI_PREV + c->stage], c->base[PVOF_F_DELTAP], bytes, cudaMemcpyDeviceToDevice,
+                           c->stream));
         c->phi_prev_mask |= 1 << c->stage;
     }
     if (c->p.surface_tension) swap_f_sigma(c);
@@ -1596,6 +1654,11 @@ int pvof_destroy(pvof_ctx *c)
     if (c->map_src_mem) cudaFree(c->map_src_mem);
     if (c->map_mul_mem) cudaFree(c->map_mul_mem);
     if (c->partials) cudaFree(c->partials);
+    cudaFree(c->cnn_params);
+    cudaFree(c->cnn_bf16);
+    cudaFree(c->cnn_x);
+    cudaFree(c->cnn_y);
+    cudaFree(c->cnn_work);
     if (c->scal) cudaFree(c->scal);
     if (c->scal_host) cudaFreeHost(c->scal_host);
     if (c->flush_buf) cudaFree(c->flush_buf);
@@ -1992,6 +2055,37 @@ int pvof_Lagrangian_advect_particles(pvof_ctx *c)
     NEED_DT(c);
     return ibm_advect(c);
 }
+int pvof_set_pressure_network(pvof_ctx *c, const float *params, size_t n)
+{
+    ENTER(c);
+    if (!params || n != pvof_cnn_param_count()) return set_err(PVOF_EINVAL, "network parameter count mismatch");
+    const int W = c->dom.NX - 1, H = c->dom.NY - 1;
+    const size_t plane = (size_t)W * H;
+    if (!c->cnn_params) {
+        if (cudaMalloc(&c->cnn_params, n * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&c->cnn_bf16, n * sizeof(uint16_t)) != cudaSuccess ||
+            cudaMalloc(&c->cnn_x, 3 * plane * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&c->cnn_y, plane * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&c->cnn_work, pvof_cnn_work_floats(H, W) * sizeof(float)) != cudaSuccess)
+            return set_err(PVOF_ENOMEM, "cudaMalloc network buffers");
+    }
+    CK(cudaMemcpyAsync(c->cnn_params, params, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    const int rc = pvof_cnn_to_bf16(c->cnn_params, c->cnn_bf16, c->stream);
+    if (rc != PVOF_OK) return set_err(rc, "network weights");
+    CK(cudaStreamSynchronize(c->stream));
+    return PVOF_OK;
+}
+
+int pvof_pressure_network_sample(pvof_ctx *c, int stage, float *x, float *t)
+{
+    ENTER(c);
+    if (stage < 0 || stage > 2 || !x || !t) return set_err(PVOF_EINVAL, "bad stage or null buffer");
+    if (!(c->phi_old_mask >> stage & 1)) return set_err(PVOF_EINVAL, "no two kept corrections for this stage yet");
+    TRY(cnn_prepare(c, S(c, SC_PHI_OLD + stage), S(c, SC_PHI_PREV + stage), x, t));
+    CK(cudaStreamSynchronize(c->stream));
+    return PVOF_OK;
+}
+
 int pvof_get_particles(pvof_ctx *c, pvof_particle *out, int *ids, double *Fo, double *To, int nmax)
 {
     ENTER(c);

@@ -1,0 +1,458 @@
+// The learned warm start of the pressure solve: a small convolutional network
+// that predicts the change of the pressure correction from the same RK stage
+// one time step earlier, trained on pairs the solver itself produces.  No
+// counterpart in the reference.
+//
+// Network (fixed): six 3x3 convolutions, 3 -> 32 -> 32 -> 32 -> 32 -> 32 -> 1
+// channels, zero padding, ReLU after all but the last; weights held in FP32
+// for training and used in BF16 by the forward pass, every product
+// accumulated in FP32.  Activations are channel-major planes [C][H][W].
+//
+// Inputs of a sample (all on the physical cells of the solve range):
+//   x0 = rho, x1 = r0 / rms(r0) with r0 = rhs - A phi_prev the residual the
+//   previous correction leaves, x2 = phi_prev / rms(phi_prev);
+// output y, the predicted change of the correction over rms(phi_prev); the
+// warm start takes the Galerkin step along it from phi_prev (k_cnn_apply);
+// training target t = (phi - phi_prev) / rms(phi_prev).
+//
+// Kernels: a shared-memory tiled direct convolution (one thread per pixel,
+// all output channels in registers, the tile and the layer's weights in
+// shared memory), its input gradient as the same convolution with the taps
+// flipped and the channels swapped, the weight gradient as per-block partial
+// sums, the mean-square loss, Adam, and the input assembly with the two root
+// mean squares.
+#include <cuda_bf16.h>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../include/pvof.h"
+#include "pvof_device.cuh"
+#include "pvof_kernels.cuh"
+
+namespace pvof {
+
+namespace {
+
+constexpr int CNN_TILE = 16;             // output tile edge of a block
+constexpr int CNN_HALO = CNN_TILE + 2;   // with the 3x3 halo
+constexpr int CNN_CMAX = 32;             // channels of the hidden layers
+
+// forward: out[co][p] = b[co] + sum_ci sum_tap w[co][ci][tap] * in[ci][p + tap]
+// (zero outside the H x W plane), then ReLU if relu
+template <int COUT>
+__global__ void __launch_bounds__(CNN_TILE * CNN_TILE) k_conv3x3(const float *__restrict__ in, int cin,
+                                                                 const __nv_bfloat16 *__restrict__ w,
+                                                                 const float *__restrict__ b, float *__restrict__ out,
+                                                                 int H, int W, int relu)
+{
+    extern __shared__ float cnn_smem[];
+    float (*tile)[CNN_HALO][CNN_HALO] = reinterpret_cast<float (*)[CNN_HALO][CNN_HALO]>(cnn_smem);
+    float *ws = cnn_smem + cin * CNN_HALO * CNN_HALO;   // the layer's weights, COUT * cin * 9
+    const int tx = threadIdx.x % CNN_TILE, ty = threadIdx.x / CNN_TILE;
+    const int i0 = blockIdx.x * CNN_TILE, j0 = blockIdx.y * CNN_TILE;
+    const size_t plane = (size_t)H * W;
+    for (int q = threadIdx.x; q < cin * CNN_HALO * CNN_HALO; q += blockDim.x) {
+        const int c = q / (CNN_HALO * CNN_HALO), r = q % (CNN_HALO * CNN_HALO);
+        const int i = i0 + r % CNN_HALO - 1, j = j0 + r / CNN_HALO - 1;
+        tile[c][r / CNN_HALO][r % CNN_HALO] = (i >= 0 && i < W && j >= 0 && j < H) ? in[c * plane + (size_t)j * W + i] : 0.0f;
+    }
+    for (int q = threadIdx.x; q < COUT * cin * 9; q += blockDim.x) ws[q] = __bfloat162float(w[q]);
+    __syncthreads();
+    const int i = i0 + tx, j = j0 + ty;
+    if (i >= W || j >= H) return;
+    float acc[COUT];
+#pragma unroll
+    for (int co = 0; co < COUT; co++) acc[co] = b ? b[co] : 0.0f;
+    for (int ci = 0; ci < cin; ci++)
+#pragma unroll
+        for (int t = 0; t < 9; t++) {
+            const float x = tile[ci][ty + t / 3][tx + t % 3];
+#pragma unroll
+            for (int co = 0; co < COUT; co++) acc[co] += x * ws[(co * cin + ci) * 9 + t];
+        }
+#pragma unroll
+    for (int co = 0; co < COUT; co++) {
+        float v = acc[co];
+        if (relu && v < 0.0f) v = 0.0f;
+        out[co * plane + (size_t)j * W + i] = v;
+    }
+}
+
+// the weights of the input-gradient convolution: wt[ci][co][8 - tap] = w[co][ci][tap]
+__global__ void k_conv_transpose_weights(const __nv_bfloat16 *__restrict__ w, __nv_bfloat16 *__restrict__ wt,
+                                         int cout, int cin)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= cout * cin * 9) return;
+    const int co = q / (cin * 9), ci = (q / 9) % cin, t = q % 9;
+    wt[(ci * cout + co) * 9 + (8 - t)] = w[q];
+}
+
+// dY *= (y > 0): the ReLU of a hidden layer, backwards
+__global__ void k_relu_back(float *__restrict__ dy, const float *__restrict__ y, size_t n)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n && !(y[q] > 0.0f)) dy[q] = 0.0f;
+}
+
+// weight and bias gradients of one layer: block (co, ci) sums
+// in[ci][p + tap] * dY[co][p] over the pixels for the nine taps; block
+// (co, cin) sums dY[co][p] for the bias
+__global__ void __launch_bounds__(256) k_conv_wgrad(const float *__restrict__ in, int cin,
+                                                    const float *__restrict__ dy, int H, int W,
+                                                    float *__restrict__ dw, float *__restrict__ db)
+{
+    const int co = blockIdx.y, ci = blockIdx.x;
+    const size_t plane = (size_t)H * W;
+    const float *g = dy + co * plane;
+    float acc[9];
+#pragma unroll
+    for (int t = 0; t < 9; t++) acc[t] = 0.0f;
+    const bool bias = ci == cin;
+    for (size_t p = threadIdx.x; p < plane; p += blockDim.x) {
+        const float gv = g[p];
+        if (gv == 0.0f) continue;
+        if (bias) {
+            acc[0] += gv;
+            continue;
+        }
+        const int i = (int)(p % W), j = (int)(p / W);
+        const float *x = in + ci * plane;
+#pragma unroll
+        for (int t = 0; t < 9; t++) {
+            const int a = i + t % 3 - 1, c = j + t / 3 - 1;
+            if (a >= 0 && a < W && c >= 0 && c < H) acc[t] += x[(size_t)c * W + a] * gv;
+        }
+    }
+    __shared__ float red[8][9];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int t = 0; t < 9; t++) {
+        float v = acc[t];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][t] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 9) {
+        float v = 0.0f;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) v += red[q][threadIdx.x];
+        if (bias) {
+            if (threadIdx.x == 0) db[co] += v;
+        } else {
+            dw[(co * cin + ci) * 9 + threadIdx.x] += v;
+        }
+    }
+}
+
+// mean-square loss and its gradient: dy = 2 (y - t) / n, loss partials per block
+__global__ void k_mse(const float *__restrict__ y, const float *__restrict__ t, size_t n, float *__restrict__ dy,
+                      double *__restrict__ loss)
+{
+    double s = 0.0;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const float e = y[q] - t[q];
+        dy[q] = 2.0f * e / (float)n;
+        s += (double)e * (double)e;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, s / (double)n);
+}
+
+// Adam (Kingma & Ba) on the FP32 master weights, then their BF16 copy
+__global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m, float *__restrict__ v,
+                       __nv_bfloat16 *__restrict__ wb, int n, float lr, float b1, float b2, float c1, float c2,
+                       float eps)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const float gq = g[q];
+    const float mq = b1 * m[q] + (1.0f - b1) * gq;
+    const float vq = b2 * v[q] + (1.0f - b2) * gq * gq;
+    m[q] = mq;
+    v[q] = vq;
+    const float wq = w[q] - lr * (mq / c1) / (sqrtf(vq / c2) + eps);
+    w[q] = wq;
+    wb[q] = __float2bfloat16(wq);
+}
+
+__global__ void k_to_bf16(const float *__restrict__ w, __nv_bfloat16 *__restrict__ wb, int n)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) wb[q] = __float2bfloat16(w[q]);
+}
+
+// layer shapes of the fixed network and their offsets in the flat parameter
+// array [w0, b0, w1, b1, ..., w5, b5] (w: [cout][cin][3][3])
+struct Layer {
+    int cin, cout;
+    size_t w, b;   // offsets
+};
+
+constexpr int CNN_LAYERS = 6;
+constexpr int CNN_IN = 3;
+
+void layers(Layer (&L)[CNN_LAYERS])
+{
+    size_t off = 0;
+    for (int l = 0; l < CNN_LAYERS; l++) {
+        L[l].cin = l == 0 ? CNN_IN : CNN_CMAX;
+        L[l].cout = l == CNN_LAYERS - 1 ? 1 : CNN_CMAX;
+        L[l].w = off;
+        off += (size_t)L[l].cout * L[l].cin * 9;
+        L[l].b = off;
+        off += (size_t)L[l].cout;
+    }
+}
+
+size_t param_count()
+{
+    Layer L[CNN_LAYERS];
+    layers(L);
+    return L[CNN_LAYERS - 1].b + 1;
+}
+
+// activation planes kept in the work buffer: the five hidden layers' outputs
+// (32 planes each) and the output plane, then two gradient buffers of 32
+// planes, then the transposed weights of one layer
+size_t work_floats(int H, int W)
+{
+    const size_t plane = (size_t)H * W;
+    return (5 * CNN_CMAX + 1 + 2 * CNN_CMAX) * plane + CNN_CMAX * CNN_CMAX * 9;
+}
+
+size_t conv_smem(int cin, int cout) { return sizeof(float) * ((size_t)cin * CNN_HALO * CNN_HALO + (size_t)cout * cin * 9); }
+
+int conv(const float *in, int cin, const __nv_bfloat16 *w, const float *b, float *out, int cout, int H, int W, int relu,
+         cudaStream_t st)
+{
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_conv3x3<CNN_CMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)conv_smem(CNN_CMAX, CNN_CMAX)) != cudaSuccess ||
+            cudaFuncSetAttribute(k_conv3x3<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)conv_smem(CNN_CMAX, 1)) != cudaSuccess)
+            return -1;
+        attr = true;
+    }
+    const dim3 grd((unsigned)((W + CNN_TILE - 1) / CNN_TILE), (unsigned)((H + CNN_TILE - 1) / CNN_TILE));
+    const size_t sm = conv_smem(cin, cout);
+    if (cout == CNN_CMAX) k_conv3x3<CNN_CMAX><<<grd, CNN_TILE * CNN_TILE, sm, st>>>(in, cin, w, b, out, H, W, relu);
+    else if (cout == 1) k_conv3x3<1><<<grd, CNN_TILE * CNN_TILE, sm, st>>>(in, cin, w, b, out, H, W, relu);
+    else return -1;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace
+
+// sums of squares over the physical cells (W x H) of two planes, per block
+__global__ void k_cnn_sumsq(Dom d, const double *__restrict__ a, const double *__restrict__ b,
+                            double *__restrict__ partials)
+{
+    const int W = d.NX - 1, H = d.NY - 1, P = d.P;
+    double sa = 0.0, sb = 0.0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < W * H; q += gridDim.x * blockDim.x) {
+        const int i = q % W, j = q / W;
+        const double x = AT_(a, i, j), y = AT_(b, i, j);
+        sa += x * x;
+        sb += y * y;
+    }
+    __shared__ double sh[2][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        sa += __shfl_down_sync(0xffffffffu, sa, o);
+        sb += __shfl_down_sync(0xffffffffu, sb, o);
+    }
+    if (lane == 0) { sh[0][warp] = sa; sh[1][warp] = sb; }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += sh[threadIdx.x][q];
+        partials[threadIdx.x * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// the residual of the previous correction under this substep's right-hand
+// side, r0 = rhs - A phi_prev (A: the variable-density operator of the
+// pressure solve with its ghost update), on the physical cells
+__global__ void k_cnn_residual(Dom d, BcMap mp, const double *__restrict__ rho, const double *__restrict__ rhs,
+                               const double *__restrict__ phi_prev, double *__restrict__ r0)
+{
+    const int W = d.NX - 1, H = d.NY - 1, P = d.P;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= W * H) return;
+    const int i = q % W, j = q / W;
+    const double a = pressure_op(d, rho, i, j, [&](int x, int y) { return remap(mp, phi_prev, P, d.NX, d.NY, x, y); });
+    AT_(r0, i, j) = AT_(rhs, i, j) - a;
+}
+
+// network inputs x = [rho, r0 / rms(r0), phi_prev / rms(phi_prev)] and, if
+// phi is given, the target t = (phi - phi_prev) / rms(phi_prev)
+__global__ void k_cnn_assemble(Dom d, const double *__restrict__ rho, const double *__restrict__ rhs,
+                               const double *__restrict__ phi_prev, const double *__restrict__ phi,
+                               const DevScalars *__restrict__ sc, float *__restrict__ x, float *__restrict__ t)
+{
+    const int W = d.NX - 1, H = d.NY - 1, P = d.P;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= W * H) return;
+    const int i = q % W, j = q / W;
+    const double n = (double)W * H;
+    const double rr = sqrt(sc->cnn_ms[0] / n) + 1e-300, rp = sqrt(sc->cnn_ms[1] / n) + 1e-300;
+    const size_t plane = (size_t)W * H;
+    x[q] = (float)AT_(rho, i, j);
+    x[plane + q] = (float)(AT_(rhs, i, j) / rr);
+    x[2 * plane + q] = (float)(AT_(phi_prev, i, j) / rp);
+    if (phi) t[q] = (float)((AT_(phi, i, j) - AT_(phi_prev, i, j)) / rp);
+}
+
+// the network's change as a plane of the solve's layout: e = y (ghosts zero)
+__global__ void k_cnn_expand(Dom d, const float *__restrict__ y, double *__restrict__ e)
+{
+    const int W = d.NX - 1, H = d.NY - 1, P = d.P;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= W * H) return;
+    AT_(e, q % W, q / W) = (double)y[q];
+}
+
+// the two inner products of the step along e that minimises the residual in
+// the solve's stopping norm (r . M r, M the Jacobi preconditioner): per block
+// sum (A e) M r0 and sum (A e) M (A e) over the physical cells
+__global__ void k_cnn_galerkin(Dom d, BcMap mp, const double *__restrict__ rho, const double *__restrict__ e,
+                               const double *__restrict__ r0, const double *__restrict__ M, double *__restrict__ partials)
+{
+    const int W = d.NX - 1, H = d.NY - 1, P = d.P;
+    double s0 = 0.0, s1 = 0.0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < W * H; q += gridDim.x * blockDim.x) {
+        const int i = q % W, j = q / W;
+        const double ae = pressure_op(d, rho, i, j, [&](int x, int y) { return remap(mp, e, P, d.NX, d.NY, x, y); });
+        const double m = AT_(M, i, j);
+        s0 += ae * m * AT_(r0, i, j);
+        s1 += ae * m * ae;
+    }
+    __shared__ double sh[2][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_down_sync(0xffffffffu, s0, o);
+        s1 += __shfl_down_sync(0xffffffffu, s1, o);
+    }
+    if (lane == 0) { sh[0][warp] = s0; sh[1][warp] = s1; }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += sh[threadIdx.x][q];
+        partials[threadIdx.x * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// the warm start phi = phi_prev + alpha e with alpha = (A e . M r0) /
+// (A e . M A e): of the corrections along e it leaves the smallest residual
+// in the solve's stopping norm, so the solve never starts further from its
+// stopping test than from phi_prev
+__global__ void k_cnn_apply(Dom d, const double *__restrict__ e, const double *__restrict__ phi_prev,
+                            const DevScalars *__restrict__ sc, double *__restrict__ phi)
+{
+    const int W = d.NX - 1, H = d.NY - 1, P = d.P;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= W * H) return;
+    const int i = q % W, j = q / W;
+    const double den = sc->cnn_ms[1];
+    const double alpha = (den != 0.0) ? sc->cnn_ms[0] / den : 0.0;
+    AT_(phi, i, j) = AT_(phi_prev, i, j) + alpha * AT_(e, i, j);
+}
+
+}  // namespace pvof
+
+using namespace pvof;
+
+extern "C" {
+
+size_t pvof_cnn_param_count(void) { return param_count(); }
+
+size_t pvof_cnn_work_floats(int H, int W) { return (H > 0 && W > 0) ? work_floats(H, W) : 0; }
+
+int pvof_cnn_forward(const float *params, const uint16_t *params_bf16, const float *x, float *y, int H, int W,
+                     float *work, void *stream)
+{
+    if (!params || !params_bf16 || !x || !work || H <= 0 || W <= 0) return PVOF_EINVAL;
+    cudaStream_t st = (cudaStream_t)stream;
+    Layer L[CNN_LAYERS];
+    layers(L);
+    const size_t plane = (size_t)H * W;
+    const __nv_bfloat16 *wb = reinterpret_cast<const __nv_bfloat16 *>(params_bf16);
+    const float *in = x;
+    for (int l = 0; l < CNN_LAYERS; l++) {
+        float *out = work + (size_t)l * CNN_CMAX * plane;   // layer l's output (the last: one plane)
+        if (conv(in, L[l].cin, wb + L[l].w, params + L[l].b, out, L[l].cout, H, W, l < CNN_LAYERS - 1, st))
+            return PVOF_ECUDA;
+        in = out;
+    }
+    if (y && cudaMemcpyAsync(y, in, plane * sizeof(float), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return PVOF_ECUDA;
+    return PVOF_OK;
+}
+
+int pvof_cnn_backward(const float *params, const uint16_t *params_bf16, const float *x, const float *dy, float *grad,
+                      int H, int W, float *work, void *stream)
+{
+    if (!params || !params_bf16 || !x || !dy || !grad || !work || H <= 0 || W <= 0) return PVOF_EINVAL;
+    (void)params;
+    cudaStream_t st = (cudaStream_t)stream;
+    Layer L[CNN_LAYERS];
+    layers(L);
+    const size_t plane = (size_t)H * W;
+    const __nv_bfloat16 *wb = reinterpret_cast<const __nv_bfloat16 *>(params_bf16);
+    float *gbuf[2] = {work + (5 * CNN_CMAX + 1) * plane, work + (6 * CNN_CMAX + 1) * plane};
+    __nv_bfloat16 *wt = reinterpret_cast<__nv_bfloat16 *>(work + (7 * CNN_CMAX + 1) * plane);
+    // gradient at the output of the last layer
+    if (cudaMemcpyAsync(gbuf[0], dy, plane * sizeof(float), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return PVOF_ECUDA;
+    int cur = 0;
+    for (int l = CNN_LAYERS - 1; l >= 0; l--) {
+        const float *lin = l == 0 ? x : work + (size_t)(l - 1) * CNN_CMAX * plane;
+        float *g = gbuf[cur];
+        if (l < CNN_LAYERS - 1) {   // through this layer's ReLU
+            const size_t n = (size_t)L[l].cout * plane;
+            k_relu_back<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, work + (size_t)l * CNN_CMAX * plane, n);
+        }
+        k_conv_wgrad<<<dim3((unsigned)L[l].cin + 1, (unsigned)L[l].cout), 256, 0, st>>>(lin, L[l].cin, g, H, W,
+                                                                                          grad + L[l].w, grad + L[l].b);
+        if (l > 0) {   // gradient at this layer's input: the flipped, transposed convolution
+            const int n = L[l].cout * L[l].cin * 9;
+            k_conv_transpose_weights<<<(n + 255) / 256, 256, 0, st>>>(wb + L[l].w, wt, L[l].cout, L[l].cin);
+            if (conv(g, L[l].cout, wt, nullptr, gbuf[1 - cur], L[l].cin, H, W, 0, st)) return PVOF_ECUDA;
+            cur = 1 - cur;
+        }
+    }
+    return cudaGetLastError() == cudaSuccess ? PVOF_OK : PVOF_ECUDA;
+}
+
+int pvof_cnn_mse(const float *y, const float *t, float *dy, size_t n, double *loss, void *stream)
+{
+    if (!y || !t || !dy || !loss || n == 0) return PVOF_EINVAL;
+    k_mse<<<296, 256, 0, (cudaStream_t)stream>>>(y, t, n, dy, loss);
+    return cudaGetLastError() == cudaSuccess ? PVOF_OK : PVOF_ECUDA;
+}
+
+int pvof_cnn_adam(float *params, const float *grad, float *m, float *v, uint16_t *params_bf16, int step, float lr,
+                  void *stream)
+{
+    if (!params || !grad || !m || !v || !params_bf16 || step < 1) return PVOF_EINVAL;
+    const int n = (int)param_count();
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    k_adam<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(params, grad, m, v,
+                                                             reinterpret_cast<__nv_bfloat16 *>(params_bf16), n, lr, b1,
+                                                             b2, c1, c2, 1e-8f);
+    return cudaGetLastError() == cudaSuccess ? PVOF_OK : PVOF_ECUDA;
+}
+
+int pvof_cnn_to_bf16(const float *params, uint16_t *params_bf16, void *stream)
+{
+    if (!params || !params_bf16) return PVOF_EINVAL;
+    const int n = (int)param_count();
+    k_to_bf16<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(params, reinterpret_cast<__nv_bfloat16 *>(params_bf16),
+                                                                 n);
+    return cudaGetLastError() == cudaSuccess ? PVOF_OK : PVOF_ECUDA;
+}
+
+}  // extern "C"

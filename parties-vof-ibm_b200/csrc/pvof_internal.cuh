@@ -85,7 +85,8 @@ enum Scratch {
     SC_PSI = 0, SC_BULK_S, SC_CH_AUX1, SC_CH_RHS_NM1, SC_CH_RES, SC_CH_DIR, SC_CH_DIR2,
     SC_FLUX_X, SC_FLUX_Y, SC_P_RES, SC_P_D, SC_P_AD, SC_P_MINV,
     SC_U_R, SC_U_D, SC_U_AD, SC_U_DIAG, SC_V_R, SC_V_D, SC_V_AD, SC_V_DIAG,
-    SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_SNAP, SC_PHI_PREV, SC_PHI_PREV1, SC_PHI_PREV2, SC_COUNT
+    SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_SNAP, SC_PHI_PREV, SC_PHI_PREV1, SC_PHI_PREV2, SC_PHI_OLD, SC_PHI_OLD1, SC_PHI_OLD2,
+    SC_COUNT
 };
 
 // device-side scalars written by solver kernels and read once per substep
@@ -98,6 +99,7 @@ struct DevScalars {
     double p_res;
     double div_max;
     double clamp_delta;
+    double cnn_ms[2];   // mean squares of the network's rhs and phi_prev inputs
     double mass;
     int error;          // non-zero: a grid barrier gave up (see pvof_cg.cu)
     unsigned bar_count; // grid barrier state
@@ -133,6 +135,12 @@ struct Ctx {
     int cgs_p_threads, cgs_v_threads;   // their threads per CTA
     int vel_one_cluster;     // momentum solve as u then v on one cluster (batched runs)
     int phi_prev_mask;       // stages whose last correction is kept in SC_PHI_PREV + stage
+    int phi_old_mask;        // stages whose correction one step before that is in SC_PHI_OLD + stage
+    // learned warm start (pvof_cnn.cu): FP32 and BF16 parameters, the input
+    // planes, the output plane and the activations
+    float *cnn_params;
+    uint16_t *cnn_bf16;
+    float *cnn_x, *cnn_y, *cnn_work;
     int coop_blocks;         // co-resident blocks for the persistent solvers
     int coop_threads;
     long long launches;      // kernels launched by this context

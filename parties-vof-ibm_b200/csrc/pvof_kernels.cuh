@@ -242,6 +242,17 @@ __global__ void k_ibm_paint(Dom d, IbmEntryDev e, int comp, const double *xu, co
 __global__ void k_compute_C_S(Dom d, const double *xc, const double *yc, const double *geo, int ngeo, double shift,
                               double denom, double extra, double *CS);
 
+// learned warm start (pvof_cnn.cu)
+__global__ void k_cnn_sumsq(Dom d, const double *a, const double *b, double *partials);
+__global__ void k_cnn_residual(Dom d, BcMap mp, const double *rho, const double *rhs, const double *phi_prev,
+                               double *r0);
+__global__ void k_cnn_assemble(Dom d, const double *rho, const double *rhs, const double *phi_prev, const double *phi,
+                               const DevScalars *sc, float *x, float *t);
+__global__ void k_cnn_expand(Dom d, const float *y, double *e);
+__global__ void k_cnn_galerkin(Dom d, BcMap mp, const double *rho, const double *e, const double *r0, const double *M,
+                               double *partials);
+__global__ void k_cnn_apply(Dom d, const double *e, const double *phi_prev, const DevScalars *sc, double *phi);
+
 // constant-density Poisson solver (pvof_fft.cu)
 __global__ void k_fft_forward(Dom d, int N, int logN, const double *rhs, double *hc, double inx);
 __global__ void k_fft_tridiag(Dom d, int N, int NYp, const double *as_, const double *ap_, const double *an_,

@@ -132,6 +132,8 @@ EXPORTS = [
     "pvof_VOF_DIFFUSE_compute_solid_normals_MCL", "pvof_VOF_DIFFUSE_apply_contact_angle",
     "pvof_VOF_DIFFUSE_extend_psi_LG_contact_angle",
     "pvof_Particle_initialize_velocities", "pvof_Lagrangian_advect_particles", "pvof_get_particles",
+    "pvof_cnn_param_count", "pvof_cnn_work_floats", "pvof_cnn_forward", "pvof_cnn_backward", "pvof_cnn_mse",
+    "pvof_cnn_adam", "pvof_cnn_to_bf16", "pvof_set_pressure_network", "pvof_pressure_network_sample",
 ]
 
 SOLVER_BIHARMONIC = 0

@@ -81,6 +81,17 @@ def load():
     L.pvof_Particle_initialize_velocities.argtypes = [V]
     L.pvof_Lagrangian_advect_particles.argtypes = [V]
     L.pvof_get_particles.argtypes = [V, P(abi.Particle), P(C.c_int), P(C.c_double), P(C.c_double), C.c_int]
+    L.pvof_cnn_param_count.restype = C.c_size_t
+    L.pvof_cnn_param_count.argtypes = []
+    L.pvof_cnn_work_floats.restype = C.c_size_t
+    L.pvof_cnn_work_floats.argtypes = [C.c_int, C.c_int]
+    L.pvof_cnn_forward.argtypes = [V, V, V, V, C.c_int, C.c_int, V, V]
+    L.pvof_cnn_backward.argtypes = [V, V, V, V, V, C.c_int, C.c_int, V, V]
+    L.pvof_cnn_mse.argtypes = [V, V, V, C.c_size_t, V, V]
+    L.pvof_cnn_adam.argtypes = [V, V, V, V, V, C.c_int, C.c_float, V]
+    L.pvof_cnn_to_bf16.argtypes = [V, V, V]
+    L.pvof_set_pressure_network.argtypes = [V, P(C.c_float), C.c_size_t]
+    L.pvof_pressure_network_sample.argtypes = [V, C.c_int, V, V]
     L.pvof_run_steps_batched.argtypes = [P(V), C.c_int, C.c_int, C.c_double, P(abi.Stats)]
     L.pvof_solver_kernel.restype = C.c_char_p
     _lib = L
@@ -209,6 +220,12 @@ class Solver:
                                                vol.ctypes.data_as(dp), fl.ctypes.data_as(C.POINTER(C.c_int)), nmax),
                   "pvof_particle_markers")
         return x[:n], y[:n], vol[:n], fl[:n]
+
+    def set_pressure_network(self, params):
+        """The learned warm start's parameters (flat float32 array)."""
+        a = np.ascontiguousarray(params, dtype=np.float32)
+        check(load().pvof_set_pressure_network(self.h, a.ctypes.data_as(C.POINTER(C.c_float)), a.size),
+              "pvof_set_pressure_network")
 
     def liquid_mass(self):
         m = C.c_double()
