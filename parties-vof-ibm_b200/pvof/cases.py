@@ -123,15 +123,16 @@ def cell_centres(grid):
 
 def rayleigh_taylor(NXM=128, NYM=512, Lx=1.0, Ly=4.0, Cn=0.01, amp=0.05,
                     atwood=0.5, Re=3000.0, surface_tension=False, We=100.0,
-                    velocity_seed=None, velocity_amp=0.0, **param_kw):
+                    velocity_seed=None, velocity_amp=0.0, wall_y=abi.WALL_NOSLIP, y0=None, **param_kw):
     """Planar two-phase instability: x periodic, no-slip walls in y, heavy
     fluid (C = 1) on top of an interface at mid-height perturbed by
     amp*cos(2 pi x / Lx); C = 0.5 (1 + tanh(d / (sqrt(2) Cn))).
 
     ``velocity_seed`` adds a seeded random divergence-carrying velocity of
     size ``velocity_amp`` (for parity cases that exercise the advection and
-    projection from the first substep)."""
-    grid = planar_grid(NXM, NYM, Lx, Ly)
+    projection from the first substep); ``wall_y`` is the wall type of both
+    y walls, ``y0`` the interface height (default mid-height)."""
+    grid = planar_grid(NXM, NYM, Lx, Ly, wall_y=wall_y)
     rho2 = (1.0 - atwood) / (1.0 + atwood)
     params = default_params(Re=Re, rho1=1.0, rho2=rho2, mu1=1.0, mu2=1.0,
                             Cn=Cn, Pe_CH=1.0 / Cn,
@@ -139,7 +140,7 @@ def rayleigh_taylor(NXM=128, NYM=512, Lx=1.0, Ly=4.0, Cn=0.01, amp=0.05,
                             We=We, **param_kw)
     xc, yc, xu, yv = cell_centres(grid)
     X, Y = np.meshgrid(xc, yc)
-    d = Y - (0.5 * Ly + amp * np.cos(2.0 * np.pi * X / Lx))
+    d = Y - ((0.5 * Ly if y0 is None else y0) + amp * np.cos(2.0 * np.pi * X / Lx))
     C = 0.5 * (1.0 + np.tanh(d / (math.sqrt(2.0) * Cn)))
     NX, NY, _ = dims(grid)
     u = np.zeros((NY, NX))

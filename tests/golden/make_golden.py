@@ -47,6 +47,9 @@ CASES = [
                                    velocity_seed=11, velocity_amp=0.1), 1, 1e-3, None),
     ("rt_tight", "rt2d", dict(NXM=24, NYM=48, Lx=1.0, Ly=2.0, Cn=0.04, velocity_seed=3, velocity_amp=0.1, **TIGHT),
      2, 1e-3, ["s0", "s1_0", "s1_2", "s2_2"]),
+    # free-slip walls in y (BOTTOM/TOP_WALL_VELOCITY_FREESLIP)
+    ("rt_fs_tight", "rt2d_fs", dict(NXM=24, NYM=48, Lx=1.0, Ly=2.0, Cn=0.04, velocity_seed=9, velocity_amp=0.1,
+                                    wall_y=abi.WALL_FREESLIP, **TIGHT), 2, 1e-3, ["s0", "s1_0", "s1_2", "s2_2"]),
 ]
 
 # resolved-particle routine cases (oracle/ref/ibm_driver.c on the ibm2d build):
@@ -65,7 +68,12 @@ MCL_PARTICLES = [(0, 0.5, 1.0, 0.2, 0.0, 0.0, 0.0, 2.5), (0, 0.03, 1.04, 0.15, 0
 MCL_GRID = dict(NXM=48, NYM=96, Lx=1.0, Ly=2.0, Cn=0.04)
 MCL_CASES = [("mcl_theta60", MCL_GRID, MCL_PARTICLES, 60.0),
              ("mcl_theta120", MCL_GRID, MCL_PARTICLES, 120.0),
-             ("mcl_theta30", MCL_GRID, MCL_PARTICLES, 30.0)]
+             ("mcl_theta30", MCL_GRID, MCL_PARTICLES, 30.0),
+             # free-slip walls in y (ibm2d_fs): the interface and two cylinders
+             # next to the bottom wall, so the characteristics cross it
+             ("mcl_fs_theta45", dict(NXM=48, NYM=48, Lx=1.0, Ly=1.0, Cn=0.04, y0=0.12, amp=0.02,
+                                     wall_y=abi.WALL_FREESLIP, _refcase="ibm2d_fs"),
+              [(0, 0.5, 0.13, 0.1, 0.0, 0.0, 0.0, 2.5), (0, 0.03, 0.15, 0.08, 0.0, 0.0, 0.0, 2.5)], 45.0)]
 
 # whole time steps with resolved cylinders (oracle/ref/ibm_driver.c "steps"
 # mode): name, reference build, builder arguments, particles, contact angle,
@@ -187,15 +195,17 @@ def make_ibm(name, kw, particles, dt, stage, outdir, refsrc=None):
 
 
 def make_mcl(name, kw, particles, theta, outdir, refsrc=None):
-    grid, params, planes = cases.rayleigh_taylor(**kw)
+    build = dict(kw)
+    refcase = build.pop("_refcase", "ibm2d")
+    grid, params, planes = cases.rayleigh_taylor(**build)
     params.contact_angle_deg = theta
-    if not os.path.exists(po.ref_binary("ibm2d")):
-        po.build_reference("ibm2d", refsrc)
+    if not os.path.exists(po.ref_binary(refcase)):
+        po.build_reference(refcase, refsrc)
     fixed = [p[1:7] for p in particles if not p[0]]
     mobile = [p[1:7] for p in particles if p[0]]
     data = {}
     with tempfile.TemporaryDirectory() as wd:
-        po.run_reference_ibm(wd, grid, params, planes, fixed, mobile, 1e-3, 0, mode="mcl")
+        po.run_reference_ibm(wd, grid, params, planes, fixed, mobile, 1e-3, 0, case=refcase, mode="mcl")
         for tag, names in (("i0", ["C_S", "C_L", "C_G"]), ("m1", ["C_L", "C_G", "C_S"]),
                            ("m2", ["C_L", "nx", "ny"]), ("m3", ["psi_LG", "C_L", "C_G"]), ("m4", ["psi_LG"])):
             for fname in names:
@@ -203,7 +213,7 @@ def make_mcl(name, kw, particles, theta, outdir, refsrc=None):
     for k, v in planes.items():
         data["init/" + k] = v
     meta = {"grid": struct_to_dict(grid), "params": struct_to_dict(params), "particles": [list(p) for p in particles],
-            "builder": kw, "refcase": "ibm2d"}
+            "builder": build, "refcase": refcase}
     data["meta"] = np.array(repr(meta))
     path = os.path.join(outdir, name + ".npz")
     np.savez_compressed(path, **data)

@@ -4,7 +4,9 @@ cylinders, against the reference.
 Routine fixtures (tests/golden/mcl_theta{60,120,30}.npz, oracle/ref/ibm_driver.c
 "mcl" mode on the ibm2d build): two fixed cylinders on a perturbed interface,
 one across the periodic x boundary, and a small mobile one; contact angles on
-both sides of 90 degrees and one below 45 (the narrower liquid-gas band).
+both sides of 90 degrees and one below 45 (the narrower liquid-gas band); and
+(mcl_fs_theta45, the ibm2d_fs build) free-slip y walls with the interface and
+two cylinders next to the bottom wall, so the characteristics cross it.
 Each routine gets the reference's input state and is compared with the
 reference's output over the whole ghosted plane:
 
@@ -33,7 +35,7 @@ from conftest import g_range, load_golden, physical, rel_l2
 
 pytestmark = pytest.mark.gpu
 
-MCL = ["mcl_theta60", "mcl_theta120", "mcl_theta30"]
+MCL = ["mcl_theta60", "mcl_theta120", "mcl_theta30", "mcl_fs_theta45"]
 
 
 def block(grid, plane):

@@ -58,7 +58,8 @@ def compare(grid, get_a, get_b, fields, tol, what):
     return worst
 
 
-@pytest.mark.parametrize("name,tol", [("rt_tight", 1e-12), ("rt_small", 1e-9), ("rt_st_small", 1e-9)])
+@pytest.mark.parametrize("name,tol", [("rt_tight", 1e-12), ("rt_small", 1e-9), ("rt_st_small", 1e-9),
+                                      ("rt_fs_tight", 1e-12)])
 def test_gpu_matches_reference_golden(name, tol):
     grid, params, planes, d, meta = load_golden(name)
     g = solver_for(grid, params, planes)
