@@ -27,6 +27,11 @@ warm start) and reports their error against the FP64 path.  --forms adds a
 "forms" object: the workload in the FP32-stencil + warm-start form, its
 throughput against the plain path's and its error.
 
+--particles adds a "particles" object: the workload with surface tension
+(We 100), a 70 degree contact angle and three resolved cylinders on the
+interface (two mobile, one fixed), timed against the same case without
+cylinders (run last, so a launch list of the command ends with its steps).
+
 --impl reference runs the reference's own time step (compiled from its
 sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host:
 --warmup untimed steps, then min(--steps, --ref-steps) timed ones.
@@ -54,6 +59,10 @@ WORKLOAD = ("planar two-phase instability 128x512 (x periodic, no-slip y), Atwoo
 # algorithmic bytes per cell and solver iteration (x, r, direction read+write,
 # plus the phase field that the coefficients are derived from)
 ALG_BYTES = {0: 48.0, 1: 56.0, 2: 56.0}
+# (mobile, x, y, R, u, v, omega_z, rho_s): two mobile cylinders cutting the
+# interface, a fixed one below it
+CYLINDERS = [(1, 0.25, 2.0, 0.08, 0, 0, 0, 2.5), (1, 0.75, 2.6, 0.08, 0, 0, 0, 2.5),
+             (0, 0.5, 1.2, 0.1, 0, 0, 0, 2.5)]
 STATE_FIELDS = ["C_L", "U", "V", "P", "CH_RHS_N", "U_EXPLICIT_OLD", "V_EXPLICIT_OLD",
                 "U_VISC_EXPLICIT_OLD", "V_VISC_EXPLICIT_OLD"]
 
@@ -202,6 +211,44 @@ def run_reference_arm(args):
     }
     print(json.dumps(line))
     return 0
+
+
+def particle_case(args, device):
+    """The workload with surface tension and three resolved cylinders, timed
+    like the main line (L2 flushed before every step), and the same case
+    without the cylinders.  Device time per step, solver iterations, the
+    cylinders' kernel launches per step."""
+    from pvof import cases, runtime
+    out = {}
+    for label, parts in (("without", None), ("with", CYLINDERS)):
+        grid, params, planes = cases.rayleigh_taylor(NXM, NYM, Lx=1.0, Ly=4.0, Cn=0.01, P_CG_MAXIT=2000,
+                                                     surface_tension=True, We=100.0)
+        params.contact_angle_deg = 70.0
+        s = runtime.Solver(grid, params, device=device)
+        if parts:
+            s.set_particles(parts)
+        s.set_planes(dict(planes, C_L=planes["F"]))
+        s.initialize()
+        for _ in range(args.warmup):
+            s.run_steps(1, DT)
+        s.set_solver_timing(True)
+        l0, ms = s.launch_count(), 0.0
+        for _ in range(args.steps):
+            s.flush_l2()
+            s.timer_start()
+            s.run_steps(1, DT)
+            ms += s.timer_stop()
+        out[label] = {"ms_per_step": ms / args.steps, "launches_per_step": (s.launch_count() - l0) / args.steps,
+                      "pressure_iterations": s.solver_timing(2)["iterations"],
+                      "pressure_ms_per_step": s.solver_timing(2)["ms"] / args.steps}
+        s.close()
+    w = out["with"]
+    return {"case": "the workload with surface tension (We 100), contact angle 70 degrees and three resolved "
+                    "cylinders on the interface (two mobile R 0.08, one fixed R 0.1, solid/liquid density 2.5)",
+            "value": NXM * NYM / (w["ms_per_step"] * 1e-3), "unit": UNIT, "steps": args.steps,
+            "ms_per_step": w["ms_per_step"], "launches_per_step": w["launches_per_step"],
+            "pressure_iterations": w["pressure_iterations"], "pressure_ms_per_step": w["pressure_ms_per_step"],
+            "without_cylinders": out["without"]}
 
 
 def pinned_like(n):
@@ -358,6 +405,8 @@ def run_ours(args):
         for r in reps:
             r.close()
 
+    particles = particle_case(args, local) if args.particles else None
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         r = reference_timing(args.cpu_steps)
@@ -392,6 +441,8 @@ def run_ours(args):
             line["batched"] = batched
         if forms is not None:
             line["forms"] = forms
+        if particles is not None:
+            line["particles"] = particles
         print(json.dumps(line))
     g.close()
     if dist is not None:
@@ -412,6 +463,8 @@ def main():
     ap.add_argument("--batch-cases", type=int, default=0,
                     help="also time this many replicas advanced concurrently (batched form)")
     ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--particles", action="store_true",
+                    help="also time the workload with surface tension and three resolved cylinders")
     ap.add_argument("--forms", action="store_true",
                     help="also time the FP32-stencil + pressure warm-start form on the workload (error against FP64)")
     ap.add_argument("--batch-form", default="fp64", choices=["fp64", "fp32", "fp32-warm"],

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define PVOF_ABI_VERSION 2
+#define PVOF_ABI_VERSION 3
 
 /* error codes */
 #define PVOF_OK 0
@@ -113,6 +113,15 @@ typedef struct pvof_params {
      * still stops at the same absolute residual, so the result moves within
      * that tolerance */
     int pressure_warm_start;
+    /* no counterpart in the reference: 1 preconditions the pressure PCG with
+     * the inverse of the constant-density Laplacian (an FFT along the periodic
+     * x rows and a tridiagonal solve per wavenumber along y) instead of the
+     * Jacobi diagonal; the solve still stops when sqrt(r^T D^-1 r), D the
+     * Jacobi diagonal, is below P_CG_ETOL, so the result moves within that
+     * tolerance.  Planar grids with x periodic, walls in y, a power-of-two x
+     * cell count up to 2048 and at most 1024 y cells; 0 is the reference's
+     * Jacobi-PCG */
+    int pressure_preconditioner;
 } pvof_params;
 
 /* Field identifiers for upload/download. */

@@ -717,8 +717,86 @@ int p_precond(pvof_ctx *c)
     return launch2d(c, k_p_precond, 0, c->dom.NX - 1, 0, c->dom.NY - 1, (const double *)F(c, PVOF_F_RHO), S(c, SC_P_MINV));
 }
 
+// the pressure PCG with the spectral preconditioner (pvof_spec.cu); the host
+// looks at the convergence flag every SPEC_BATCH iterations
+constexpr int SPEC_BATCH = 4;
+
+int p_solve_spectral(pvof_ctx *c)
+{
+    const Dom &d = c->dom;
+    const char *why = nullptr;
+    if (!spec_supported(d, &why)) return set_err(PVOF_EINVAL, why);
+    const int N = d.NX - 1, M = d.NY - 1;
+    if (!c->spec_mem) {
+        HostMetrics hm;   // the spacings the operator uses (idx_c[1], idy_c[1] on the device)
+        build_metrics(c->g, d.NX, d.NY, hm);
+        const double idx2 = hm.idx_c[1 + NG] * hm.idx_c[1 + NG], idy2 = hm.idy_c[1 + NG] * hm.idy_c[1 + NG];
+        c->spec_fscale = 1.0 / (idy2 * (double)N);
+        std::vector<double> lamx, tw;
+        spec_tables(N, idx2, idy2, lamx, tw);
+        std::vector<double> h(lamx);
+        h.insert(h.end(), tw.begin(), tw.end());
+        h.resize(h.size() + (size_t)M, 0.0);   // per-block sums
+        if (cudaMalloc(&c->spec_mem, h.size() * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&c->spec_s, sizeof(SpecScal)) != cudaSuccess ||
+            cudaMallocHost(&c->spec_done, sizeof(int)) != cudaSuccess)
+            return set_err(PVOF_ENOMEM, "allocating the spectral preconditioner");
+        CK(cudaMemcpy(c->spec_mem, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemset(c->spec_s, 0, sizeof(SpecScal)));
+    }
+    SpecArgs A;
+    A.d = d;
+    A.mp = c->maps[BK_PRESSURE];
+    A.phi = F(c, PVOF_F_DELTAP);
+    A.rhs = F(c, PVOF_F_P_RHS);
+    A.rho = F(c, PVOF_F_RHO);
+    A.MJ = S(c, SC_P_MINV);
+    A.res = S(c, SC_P_RES);
+    A.z = S(c, SC_P_Z);
+    A.Ad = S(c, SC_P_AD);
+    A.hat = S(c, SC_P_HAT);
+    A.lamx = c->spec_mem;
+    A.tw = reinterpret_cast<const double2 *>(c->spec_mem + N);
+    A.N = N;
+    A.logN = 0;
+    while ((1 << A.logN) < N) A.logN++;
+    A.M = M;
+    A.fscale = c->spec_fscale;
+    A.tol = c->p.P_CG_ETOL;
+    A.maxit = c->p.P_CG_MAXIT;
+    A.part = c->spec_mem + 2 * N;
+    A.s = c->spec_s;
+    A.scal = c->scal;
+    const int n = N * M;
+    long long kernels = 0;
+    TRY(timed_launch(c, PVOF_SOLVER_PRESSURE, 0, n, [&]() -> cudaError_t {
+        cudaError_t e = spec_launch_init(A, c->stream);
+        if (e != cudaSuccess) return e;
+        kernels += 3;
+        double *dcur = S(c, SC_P_D), *dnxt = S(c, SC_P_D2);
+        int it = 0;
+        while (it < A.maxit) {
+            for (int b = 0; b < SPEC_BATCH && it < A.maxit; b++, it++) {
+                e = spec_launch_iteration(A, dcur, dnxt, it == 0 ? 1 : 0, c->stream);
+                if (e != cudaSuccess) return e;
+                kernels += 4;
+                std::swap(dcur, dnxt);
+            }
+            e = cudaMemcpyAsync(c->spec_done, &c->spec_s->done, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+            if (e != cudaSuccess) return e;
+            if (*c->spec_done) break;
+        }
+        kernels += 2;
+        return spec_launch_mean(A, c->stream);
+    }));
+    c->launches += kernels - 1;
+    return fill(c, BK_WRAP_C, F(c, PVOF_F_DELTAP));
+}
+
 int p_solve(pvof_ctx *c)
 {
+    if (c->p.pressure_preconditioner == 1) return p_solve_spectral(c);
     PresArgs A;
     A.d = c->dom;
     A.mp = c->maps[BK_PRESSURE];
@@ -1042,7 +1120,7 @@ int ibm_flag_points(pvof_ctx *c)
         s->d_mk = nullptr;
         s->d_flag = nullptr;
         if (cudaMalloc(&s->d_mk, 6 * nm * sizeof(double)) != cudaSuccess ||
-            cudaMalloc(&s->d_flag, nm * sizeof(int)) != cudaSuccess) {
+            cudaMalloc(&s->d_flag, 3 * nm * sizeof(int)) != cudaSuccess) {
             s->cap_mk = 0;
             return set_err(PVOF_ENOMEM, "cudaMalloc particle markers");
         }
@@ -1094,6 +1172,8 @@ IbmDev ibm_dev(pvof_ctx *c, IbmState *s)
     D.rhoL = s->d_mk + 4 * nm;
     D.FL = s->d_mk + 5 * nm;
     D.flag = s->d_flag;
+    D.sup_i = s->d_flag + nm;
+    D.sup_j = s->d_flag + 2 * nm;
     D.FT = s->d_FT;
     const int NX = c->dom.NX, NY = c->dom.NY;
     D.xlo = s->hm.xu[NG];
@@ -1143,12 +1223,12 @@ int ibm_force(pvof_ctx *c, int force_iter)
                 CKL(c);
             }
             if (ne > 0) {
-                k_ibm_marker_force<<<(unsigned)((ne + 31) / 32), 32, 0, c->stream>>>(D, comp, ne, idt2beta,
-                                                                                   (!corrector && comp == 0) ? 1 : 0);
+                const double xs0 = comp == 0 ? s->hm.xu[NG] : s->hm.xc[NG];
+                const double ys0 = comp == 0 ? s->hm.yc[NG] : s->hm.yv[NG];
+                k_ibm_marker_force<<<(unsigned)ne, IBM_FORCE_THREADS, 0, c->stream>>>(D, comp, xs0, ys0, idt2beta,
+                                                                                     (!corrector && comp == 0) ? 1 : 0);
                 CKL(c);
-            }
-            for (int e = 0; e < ne; e++) {
-                k_ibm_spread<<<cg, cb, 0, c->stream>>>(d, D, e, comp, xs, ys, rho, comp == 0 ? RU : RV);
+                k_ibm_spread<<<cg, cb, 0, c->stream>>>(d, D, ne, comp, xs, ys, rho, comp == 0 ? RU : RV);
                 CKL(c);
             }
         }
@@ -1509,6 +1589,16 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     if (grid->geometry == PVOF_GEOM_AXISYM && grid->periodic[0]) return set_err(PVOF_EINVAL, "the axis cannot be periodic");
     if (params->Re <= 0 || params->Pe_CH <= 0 || params->Cn <= 0) return set_err(PVOF_EINVAL, "Re, Pe_CH and Cn must be positive");
     if (params->N_forcing_loops < 0) return set_err(PVOF_EINVAL, "N_forcing_loops must not be negative");
+    if (params->pressure_preconditioner < 0 || params->pressure_preconditioner > 1)
+        return set_err(PVOF_EINVAL, "pressure_preconditioner must be 0 (Jacobi) or 1 (spectral)");
+    if (params->pressure_preconditioner == 1) {
+        const int N = grid->NXM, M = grid->NYM;
+        if (grid->geometry != PVOF_GEOM_PLANAR || !grid->periodic[0] || grid->periodic[1])
+            return set_err(PVOF_EINVAL, "the spectral pressure preconditioner needs a planar grid, x periodic, walls in y");
+        if ((N & (N - 1)) != 0 || N > 2048 || M > 1024)
+            return set_err(PVOF_EINVAL, "the spectral pressure preconditioner needs a power-of-two x cell count up to 2048 "
+                                        "and at most 1024 y cells");
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(PVOF_ENODEV, "no CUDA device");
     if (device < 0 || device >= ndev) return set_err(PVOF_EINVAL, "bad device index");
@@ -1667,6 +1757,9 @@ int pvof_destroy(pvof_ctx *c)
         for (int e = 0; e < 2; e++) if (c->pend_ev[q][e]) cudaEventDestroy(c->pend_ev[q][e]);
     delete c->ibm;
     if (c->fft_coef) cudaFree(c->fft_coef);
+    if (c->spec_mem) cudaFree(c->spec_mem);
+    if (c->spec_s) cudaFree(c->spec_s);
+    if (c->spec_done) cudaFreeHost(c->spec_done);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PVOF_OK;

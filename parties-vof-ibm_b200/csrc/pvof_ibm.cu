@@ -494,68 +494,109 @@ __global__ void k_ibm_interp(Dom d, const double *__restrict__ a, const double *
 }
 
 // Marker forces of one velocity component and the particle reaction force
-// and torque (Lagrangian.c:2119-2170 for u, :2280-2335 for v): one thread per
-// particle, its markers in order.
-__global__ void k_ibm_marker_force(IbmDev D, int comp, int nentries, double idt2beta, int reset)
+// and torque (Lagrangian.c:2119-2170 for u, :2280-2335 for v): one block per
+// particle, its markers in chunks across the threads.  Each marker's force is
+// its own; its terms of the particle's force and torque go to shared memory
+// and one thread adds them in marker order, as the reference does.  The lower
+// corner of each marker's 3 x 3 spreading support on this component's grid is
+// stored for k_ibm_spread.
+__global__ void __launch_bounds__(IBM_FORCE_THREADS) k_ibm_marker_force(IbmDev D, int comp, double xs0, double ys0,
+                                                                       double idt2beta, int reset)
 {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nentries) return;
+    __shared__ double sh_f[IBM_FORCE_THREADS], sh_t[IBM_FORCE_THREADS];
+    __shared__ int sh_ok[IBM_FORCE_THREADS];
+    const int e = blockIdx.x, tid = threadIdx.x;
     const IbmEntryDev &p = D.ent[e];
-    double *F = D.FT + 6 * e, *T = F + 3;
-    if (reset) { F[0] = F[1] = F[2] = T[0] = T[1] = T[2] = 0.0; }
-    for (int q = p.moff; q < p.moff + p.mcount; q++) {
-        if (D.flag[q] == 0) { D.FL[q] = 0.0; continue; }
-        const double r0 = D.XL[q] - p.X[0], r1 = D.YL[q] - p.X[1], r2 = p.Zs - p.X[2];
-        const double Ud = comp == 0 ? p.U[0] + p.Omega[1] * r2 - p.Omega[2] * r1
-                                    : p.U[1] + p.Omega[2] * r0 - p.Omega[0] * r2;
-        const double rho_L = D.rhoL[q];
-        const double FL = idt2beta * (Ud - D.UL[q]);
-        const double x = D.XL[q], y = D.YL[q];
-        if (x >= D.xlo && x < D.xhi && y >= D.ylo && y < D.yhi) {   // Lagrangian_local_point_2d
-            const double M = D.vol[q];
-            if (comp == 0) {
-                F[0] -= rho_L * M * FL;
-                T[2] += rho_L * M * r1 * FL;
+    const double h = D.h;
+    double *Fp = D.FT + 6 * e, *Tp = Fp + 3;
+    double Fa = 0.0, Ta = 0.0;
+    if (tid == 0) {
+        if (reset) { Fp[0] = Fp[1] = Fp[2] = Tp[0] = Tp[1] = Tp[2] = 0.0; }
+        Fa = Fp[comp];
+        Ta = Tp[2];
+    }
+    const int end = p.moff + p.mcount;
+    for (int base = p.moff; base < end; base += IBM_FORCE_THREADS) {
+        const int q = base + tid;
+        int ok = 0;
+        if (q < end) {
+            const double x = D.XL[q], y = D.YL[q];
+            D.sup_i[q] = (int)round((x - xs0) / h) - 1;
+            D.sup_j[q] = (int)round((y - ys0) / h) - 1;
+            if (D.flag[q] == 0) {
+                D.FL[q] = 0.0;
             } else {
-                F[1] -= rho_L * M * FL;
-                T[2] -= rho_L * M * r0 * FL;
+                const double r0 = x - p.X[0], r1 = y - p.X[1], r2 = p.Zs - p.X[2];
+                const double Ud = comp == 0 ? p.U[0] + p.Omega[1] * r2 - p.Omega[2] * r1
+                                            : p.U[1] + p.Omega[2] * r0 - p.Omega[0] * r2;
+                const double rho_L = D.rhoL[q];
+                const double FL = idt2beta * (Ud - D.UL[q]);
+                if (x >= D.xlo && x < D.xhi && y >= D.ylo && y < D.yhi) {   // Lagrangian_local_point_2d
+                    const double M = D.vol[q];
+                    sh_f[tid] = rho_L * M * FL;
+                    sh_t[tid] = rho_L * M * (comp == 0 ? r1 : r0) * FL;
+                    ok = 1;
+                }
+                D.FL[q] = FL;
             }
         }
-        D.FL[q] = FL;
+        sh_ok[tid] = ok;
+        __syncthreads();
+        if (tid == 0) {
+            const int n = min(IBM_FORCE_THREADS, end - base);
+            for (int k = 0; k < n; k++) {
+                if (!sh_ok[k]) continue;
+                Fa -= sh_f[k];
+                if (comp == 0) Ta += sh_t[k];
+                else Ta -= sh_t[k];
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        Fp[comp] = Fa;
+        Tp[2] = Ta;
     }
 }
 
-// Interpolate_Lag_to_Eul_uniform_twod (Interpolate.c:390-475) of one particle
-// as a gather, then rhs += 2 rho_face temp (Lagrangian.c:2176-2190, :2338-2350)
-__global__ void k_ibm_spread(Dom d, IbmDev D, int e, int comp, const double *__restrict__ xs,
+// Interpolate_Lag_to_Eul_uniform_twod (Interpolate.c:390-475) of every
+// particle as a gather, then rhs += 2 rho_face temp per particle, in list
+// order (Lagrangian.c:2176-2190, :2338-2350).  A cell takes a marker when it
+// lies in the marker's 3 x 3 support (the support's corner from
+// k_ibm_marker_force; the reference clips the support to the interior, which
+// the cell already is); a cell outside a particle's box gets zero from it,
+// which leaves its sum as it is.
+__global__ void k_ibm_spread(Dom d, IbmDev D, int ne, int comp, const double *__restrict__ xs,
                              const double *__restrict__ ys, const double *__restrict__ rho, double *__restrict__ rhs)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= d.NX || j >= d.NY) return;
     const int P = d.P;
-    const IbmEntryDev &p = D.ent[e];
     const double h = D.h;
-    double temp = 0.0;
-    if (i >= p.box[0] && i < p.box[1] && j >= p.box[2] && j < p.box[3]) {
+    double r = 0.0;
+    bool touched = false;
+    for (int e = 0; e < ne; e++) {
+        const IbmEntryDev &p = D.ent[e];
+        if (!(i >= p.box[0] && i < p.box[1] && j >= p.box[2] && j < p.box[3])) continue;
+        if (!touched) {
+            r = AT_(rhs, i, j);
+            touched = true;
+        }
+        double temp = 0.0;
         const double cellv = D.dxu1 * D.dyv[j] * D.slab;   // Interpolate_twod_cell_volume, planar
         for (int q = p.moff; q < p.moff + p.mcount; q++) {
-            int i_start = (int)round((D.XL[q] - xs[0]) / h) - 1;
-            int j_start = (int)round((D.YL[q] - ys[0]) / h) - 1;
-            int i_end = i_start + 3, j_end = j_start + 3;
-            i_start = max(i_start, 0);
-            i_end = min(max(i_end, 0), d.NX);
-            j_start = min(max(j_start, 0), d.NY);
-            j_end = min(max(j_end, 0), d.NY);
-            if (i < i_start || i >= i_end || j < j_start || j >= j_end) continue;
+            if ((unsigned)(i - D.sup_i[q]) >= 3u || (unsigned)(j - D.sup_j[q]) >= 3u) continue;
             const double r1 = D.YL[q] - ys[j];
             const double r0 = D.XL[q] - xs[i];
             const double dV = D.vol[q] / cellv;
             temp += 1 * D.FL[q] * (ibm_delta(r0 / h) * ibm_delta(r1 / h)) * dV;
         }
+        const double rho_face = comp == 0 ? 0.5 * (AT_(rho, i, j) + AT_(rho, i - 1, j))
+                                          : 0.5 * (AT_(rho, i, j) + AT_(rho, i, j - 1));
+        r += 2.0 * rho_face * temp;
     }
-    const double rho_face = comp == 0 ? 0.5 * (AT_(rho, i, j) + AT_(rho, i - 1, j)) : 0.5 * (AT_(rho, i, j) + AT_(rho, i, j - 1));
-    AT_(rhs, i, j) += 2.0 * rho_face * temp;
+    if (touched) AT_(rhs, i, j) = r;
 }
 
 // corrector update u += beta dt rhs / rho_face over the G range (Lagrangian.c:1832-1851)

@@ -85,7 +85,7 @@ enum Scratch {
     SC_PSI = 0, SC_BULK_S, SC_CH_AUX1, SC_CH_RHS_NM1, SC_CH_RES, SC_CH_DIR, SC_CH_DIR2,
     SC_FLUX_X, SC_FLUX_Y, SC_P_RES, SC_P_D, SC_P_AD, SC_P_MINV,
     SC_U_R, SC_U_D, SC_U_AD, SC_U_DIAG, SC_V_R, SC_V_D, SC_V_AD, SC_V_DIAG,
-    SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_SNAP, SC_PHI_PREV, SC_PHI_PREV1, SC_PHI_PREV2, SC_PHI_OLD, SC_PHI_OLD1, SC_PHI_OLD2,
+    SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_SNAP, SC_PHI_PREV, SC_PHI_PREV1, SC_PHI_PREV2, SC_PHI_OLD, SC_PHI_OLD1, SC_PHI_OLD2, SC_P_HAT,
     SC_COUNT
 };
 
@@ -156,6 +156,10 @@ struct Ctx {
     int npend;
     IbmState *ibm;           // resolved particles (null until pvof_set_particles)
     double *fft_coef;        // as, ap, an (NY-1 each) and the modified wavenumbers (NX-1)
+    double *spec_mem;        // spectral pressure preconditioner: x eigenvalues, twiddles, block sums
+    struct SpecScal *spec_s; // its device scalars
+    int *spec_done;          // pinned host copy of its convergence flag
+    double spec_fscale;      // dy^2 / N
     double sol_ms[3];
     long long sol_launches[3], sol_iters[3], sol_cell_iters[3];
 };

@@ -47,6 +47,36 @@ struct PresArgs {
     DevScalars *scal;
 };
 
+// spectral-preconditioned pressure PCG (pvof_spec.cu)
+struct SpecScal {
+    double gamma, beta, alpha, res, avg;
+    int iters, done;
+    unsigned cnt[8];   // arrival counters of the per-launch reductions
+};
+
+struct SpecArgs {
+    Dom d;
+    BcMap mp;                 // the pressure ghost rules
+    double *phi;              // deltap
+    const double *rhs, *rho, *MJ;
+    double *res, *z, *Ad, *hat;
+    const double *lamx;       // dy^2 times the x eigenvalue of each half-complex index
+    const double2 *tw;        // exp(-2 pi i k / N), k < N / 2
+    int N, logN, M;           // x cells (a power of two), log2 N, y cells
+    double fscale;            // dy^2 / N
+    double tol;
+    int maxit;
+    double *part;             // per-block sums, M entries
+    SpecScal *s;
+    DevScalars *scal;
+};
+
+bool spec_supported(const Dom &d, const char **why);
+int spec_tables(int N, double idx2, double idy2, std::vector<double> &lamx, std::vector<double> &tw);
+cudaError_t spec_launch_init(const SpecArgs &A, cudaStream_t st);
+cudaError_t spec_launch_iteration(const SpecArgs &A, const double *dold, double *dnew, int first, cudaStream_t st);
+cudaError_t spec_launch_mean(const SpecArgs &A, cudaStream_t st);
+
 __global__ void k_fill(Dom d, BcMap m, double *f);
 __global__ void k_weno_flux(Dom d, int i0, int i1, int j0, int j1, const double *C, const double *u, const double *v,
                             double *fx, double *fy, int weno5);
@@ -185,6 +215,7 @@ struct IbmDev {
     const IbmEntryDev *ent;
     const double *XL, *YL, *vol;
     const int *flag;
+    int *sup_i, *sup_j;            // lower corner of each marker's spreading support
     double *UL, *rhoL, *FL, *FT;   // FT: F[3], T[3] per entry
     double xlo, xhi, ylo, yhi;     // Lagrangian_local_point_2d bounds
     double h, dxu1, slab;
@@ -229,8 +260,9 @@ __global__ void k_mcl_extend_psi(Dom d, MclView v, const double *nxa, const doub
 
 __global__ void k_ibm_interp(Dom d, const double *a, const double *xs, const double *ys, double h, const double *XL,
                              const double *YL, int nm, double *out);
-__global__ void k_ibm_marker_force(IbmDev D, int comp, int nentries, double idt2beta, int reset);
-__global__ void k_ibm_spread(Dom d, IbmDev D, int e, int comp, const double *xs, const double *ys, const double *rho,
+constexpr int IBM_FORCE_THREADS = 256;
+__global__ void k_ibm_marker_force(IbmDev D, int comp, double xs0, double ys0, double idt2beta, int reset);
+__global__ void k_ibm_spread(Dom d, IbmDev D, int ne, int comp, const double *xs, const double *ys, const double *rho,
                              double *rhs);
 __global__ void k_ibm_correct(Dom d, int comp, double dtbeta, const double *rhs, const double *rho, double *vel);
 __global__ void k_ibm_ng_update(Dom d, double *a, const double *b, int reset);

@@ -5,7 +5,7 @@ field; tests/test_abi.py checks the exported symbols and the sizes.
 """
 import ctypes as C
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 OK = 0
 EINVAL = -1
@@ -79,6 +79,7 @@ class Params(C.Structure):
         ("N_forcing_loops", C.c_int),
         ("stencil_fp32", C.c_int),
         ("pressure_warm_start", C.c_int),
+        ("pressure_preconditioner", C.c_int),
     ]
 
 

@@ -84,6 +84,7 @@ def default_params(**kw):
     p.N_forcing_loops = 2
     p.stencil_fp32 = 0
     p.pressure_warm_start = 0
+    p.pressure_preconditioner = 0
     for k, v in kw.items():
         setattr(p, k, v)
     return p
