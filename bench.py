@@ -24,7 +24,9 @@ stream per case, so the cluster-resident solvers of different cases run on
 different SMs) and adds a "batched" object to the line; --batch-form fp32
 (fp32-warm) runs the replicas in the FP32 stencil form (plus the pressure
 warm start) and reports their error against the FP64 path.  --forms adds a
-"forms" object: the workload in the FP32-stencil + warm-start form, its
+"forms" list: the workload in each form of FORMS (FP32 stencils + pressure
+warm start; the spectral pressure preconditioner; with it the momentum CG
+without the reference's step regularisation; all of them), each with its
 throughput against the plain path's and its error.
 
 --particles adds a "particles" object: the workload with surface tension
@@ -59,6 +61,15 @@ WORKLOAD = ("planar two-phase instability 128x512 (x periodic, no-slip y), Atwoo
 # algorithmic bytes per cell and solver iteration (x, r, direction read+write,
 # plus the phase field that the coefficients are derived from)
 ALG_BYTES = {0: 48.0, 1: 56.0, 2: 56.0}
+# the forms --forms times: (label, stencil_fp32, pressure_warm_start,
+# pressure_preconditioner, velocity_cg_unregularized)
+FORMS = [
+    ("fp32 stencils + pressure warm start (same stage of the previous step)", 1, 1, 0, 0),
+    ("spectral pressure preconditioner (FP64)", 0, 0, 1, 0),
+    ("spectral pressure preconditioner + unregularised momentum CG (FP64)", 0, 0, 1, 1),
+    ("spectral pressure preconditioner + unregularised momentum CG + fp32 stencils + pressure warm start",
+     1, 1, 1, 1),
+]
 # (mobile, x, y, R, u, v, omega_z, rho_s): two mobile cylinders cutting the
 # interface, a fixed one below it
 CYLINDERS = [(1, 0.25, 2.0, 0.08, 0, 0, 0, 2.5), (1, 0.75, 2.6, 0.08, 0, 0, 0, 2.5),
@@ -299,32 +310,39 @@ def run_ours(args):
         import numpy as np
         snap = {f: g.get(f) for f in ("U", "V", "P", "C_L")}
         m64 = g.liquid_mass()
-        fparams = abi.Params.from_buffer_copy(params)
-        fparams.stencil_fp32 = 1
-        fparams.pressure_warm_start = 1
-        fg = runtime.Solver(grid, fparams, device=local)
-        fg.set_planes(planes)
-        fg.initialize()
-        for _ in range(args.warmup):
-            fg.run_steps(1, DT)
-        fg.set_solver_timing(True)
-        f_ms = 0.0
-        for _ in range(args.steps):
-            fg.flush_l2()
-            fg.timer_start()
-            fg.run_steps(1, DT)
-            f_ms += fg.timer_stop()
-        fp_it = fg.solver_timing(2)["iterations"]
-        err = {"velocity_rel_l2": max(float(np.linalg.norm(fg.get(f) - snap[f]) / np.linalg.norm(snap[f]))
-                                      for f in ("U", "V")),
-               "pressure_rel_l2": float(np.linalg.norm(fg.get("P") - snap["P"]) / np.linalg.norm(snap["P"])),
-               "volume_rel": abs(fg.liquid_mass() - m64) / abs(m64)}
-        fvalue = cells * args.steps / (f_ms * 1e-3)
-        forms = {"form": "fp32 stencils + pressure warm start (same stage of the previous step)",
-                 "value": fvalue, "unit": UNIT, "ms_per_step": f_ms / args.steps, "vs_plain": fvalue / value,
-                 "pressure_iterations": fp_it, "pressure_iterations_plain": timing[2]["iterations"],
-                 "error_vs_fp64": err}
-        fg.close()
+        forms = []
+        for label, fp32, warm, precond, vel in FORMS:
+            fparams = abi.Params.from_buffer_copy(params)
+            fparams.stencil_fp32 = fp32
+            fparams.pressure_warm_start = warm
+            fparams.pressure_preconditioner = precond
+            fparams.velocity_cg_unregularized = vel
+            fg = runtime.Solver(grid, fparams, device=local)
+            fg.set_planes(planes)
+            fg.initialize()
+            for _ in range(args.warmup):
+                fg.run_steps(1, DT)
+            fg.set_solver_timing(True)
+            f_ms = 0.0
+            for _ in range(args.steps):
+                fg.flush_l2()
+                fg.timer_start()
+                fg.run_steps(1, DT)
+                f_ms += fg.timer_stop()
+            fp = fg.solver_timing(2)
+            err = {"velocity_rel_l2": max(float(np.linalg.norm(fg.get(f) - snap[f]) / np.linalg.norm(snap[f]))
+                                          for f in ("U", "V")),
+                   "pressure_rel_l2": float(np.linalg.norm(fg.get("P") - snap["P"]) / np.linalg.norm(snap["P"])),
+                   "volume_rel": abs(fg.liquid_mass() - m64) / abs(m64)}
+            fvalue = cells * args.steps / (f_ms * 1e-3)
+            forms.append({"form": label, "value": fvalue, "unit": UNIT, "ms_per_step": f_ms / args.steps,
+                          "vs_plain": fvalue / value, "pressure_iterations": fp["iterations"],
+                          "pressure_iterations_plain": timing[2]["iterations"],
+                          "pressure_ms_per_step": fp["ms"] / args.steps,
+                          "velocity_iterations": fg.solver_timing(1)["iterations"],
+                          "velocity_iterations_plain": timing[1]["iterations"],
+                          "error_vs_fp64": err})
+            fg.close()
 
     # ---- end to end through the C ABI with host buffers ---------------------
     blocks = {f: pinned_like(g.block_count(f)) for f in STATE_FIELDS}
@@ -366,8 +384,9 @@ def run_ours(args):
     if args.batch_cases > 1:
         from pvof import abi
         bparams = abi.Params.from_buffer_copy(params)
-        bparams.stencil_fp32 = 1 if args.batch_form in ("fp32", "fp32-warm") else 0
-        bparams.pressure_warm_start = 1 if args.batch_form == "fp32-warm" else 0
+        bparams.stencil_fp32 = 1 if args.batch_form.startswith("fp32") else 0
+        bparams.pressure_warm_start = 1 if args.batch_form in ("fp32-warm", "fp32-warm-spectral") else 0
+        bparams.pressure_preconditioner = 1 if args.batch_form.endswith("spectral") else 0
         reps = []
         for q in range(args.batch_cases):
             r = runtime.Solver(grid, bparams, device=local)
@@ -388,7 +407,10 @@ def run_ours(args):
                    "note": "replicas of the workload advanced concurrently by pvof_run_steps_batched "
                            "(one host thread and stream per case); device time of the slowest case",
                    "form": {"fp64": "fp64", "fp32": "fp32-stencils",
-                            "fp32-warm": "fp32-stencils + pressure warm start"}[args.batch_form]}
+                            "fp32-warm": "fp32-stencils + pressure warm start",
+                            "spectral": "spectral pressure preconditioner",
+                            "fp32-warm-spectral": "fp32-stencils + pressure warm start + spectral pressure "
+                                                  "preconditioner"}[args.batch_form]}
         if args.batch_form != "fp64":
             import numpy as np
             # the error of the form: one replica against the FP64 path after the same steps
@@ -467,7 +489,7 @@ def main():
                     help="also time the workload with surface tension and three resolved cylinders")
     ap.add_argument("--forms", action="store_true",
                     help="also time the FP32-stencil + pressure warm-start form on the workload (error against FP64)")
-    ap.add_argument("--batch-form", default="fp64", choices=["fp64", "fp32", "fp32-warm"],
+    ap.add_argument("--batch-form", default="fp64", choices=["fp64", "fp32", "fp32-warm", "spectral", "fp32-warm-spectral"],
                     help="fp32: the batched replicas use the FP32 stencil form (error against FP64 reported)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

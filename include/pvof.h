@@ -122,6 +122,13 @@ typedef struct pvof_params {
      * cell count up to 2048 and at most 1024 y cells; 0 is the reference's
      * Jacobi-PCG */
     int pressure_preconditioner;
+    /* no counterpart in the reference: 1 drops the 1e-14 that the momentum
+     * CG adds to its step-length and direction-update denominators
+     * (msolve_cg.c).  Once the preconditioned residual r^T D^-1 r falls near
+     * 1e-14 that constant shortens every step, so the reference's solve stalls
+     * above CG_ETOL and runs to CG_MAXIT; without it the solve stops at
+     * CG_ETOL.  0 is the reference's iteration */
+    int velocity_cg_unregularized;
 } pvof_params;
 
 /* Field identifiers for upload/download. */

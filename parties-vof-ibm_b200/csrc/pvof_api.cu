@@ -598,6 +598,9 @@ VelArgs vel_args(pvof_ctx *c, int comp)
     if (comp == 0) A.in_tot = c->dom.perx ? 1.0 / (double)((NX - 1) * (NY - 1) * (NZ - 1)) : 1.0 / (double)((NX - 2) * (NY - 1) * (NZ - 1));
     else A.in_tot = c->dom.pery ? 1.0 / (double)((NX - 1) * (NY - 1) * (NZ - 1)) : 1.0 / (double)((NX - 1) * (NY - 2) * (NZ - 1));
     A.tol = c->p.CG_ETOL;
+    // msolve_cg.c's 1e-14 in the step length and the direction update; the
+    // unregularised form keeps only a guard against 0 / 0
+    A.step_eps = c->p.velocity_cg_unregularized ? 1e-300 : 1e-14;
     A.maxit = c->p.CG_MAXIT;
     A.partials = c->partials;
     A.scal = c->scal;
@@ -1589,6 +1592,8 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     if (grid->geometry == PVOF_GEOM_AXISYM && grid->periodic[0]) return set_err(PVOF_EINVAL, "the axis cannot be periodic");
     if (params->Re <= 0 || params->Pe_CH <= 0 || params->Cn <= 0) return set_err(PVOF_EINVAL, "Re, Pe_CH and Cn must be positive");
     if (params->N_forcing_loops < 0) return set_err(PVOF_EINVAL, "N_forcing_loops must not be negative");
+    if (params->velocity_cg_unregularized < 0 || params->velocity_cg_unregularized > 1)
+        return set_err(PVOF_EINVAL, "velocity_cg_unregularized must be 0 or 1");
     if (params->pressure_preconditioner < 0 || params->pressure_preconditioner > 1)
         return set_err(PVOF_EINVAL, "pressure_preconditioner must be 0 (Jacobi) or 1 (spectral)");
     if (params->pressure_preconditioner == 1) {

@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
         put_partial(part1, sdad);
         if (!grid_barrier(gs)) return;
         double dAd = grid_total(part1);
-        double alpha = rz / (dAd + EPS);
+        double alpha = rz / (dAd + A.step_eps);
         double s0 = 0.0, s1 = 0.0;
         for (int q = tid; q < R.n; q += nth) {
             int i, j;
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
         double rz_new = grid_total(part2), rr = grid_total(part3);
         RMS = sqrt(A.in_tot * rr);
         if (RMS < A.tol) break;
-        beta = rz_new / (rz + EPS);
+        beta = rz_new / (rz + A.step_eps);
         rz = rz_new;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->vel_iters[A.comp] = iters; A.scal->vel_rms[A.comp] = RMS; }

@@ -584,7 +584,8 @@ __global__ void __launch_bounds__(NT, 1) k_cgs_velocity(const __grid_constant__ 
         {
             const double v1[1] = {sdad};
             const double g = rz;
-            cluster_reduce<NT>(cl, v1, slots, slot, out, [g, EPS](double *t) { t[0] = g / (t[0] + EPS); });
+            const double se = A.step_eps;
+            cluster_reduce<NT>(cl, v1, slots, slot, out, [g, se](double *t) { t[0] = g / (t[0] + se); });
         }
         slot = (slot + 1) & 3;
         const double alpha = out[0];
@@ -604,9 +605,10 @@ __global__ void __launch_bounds__(NT, 1) k_cgs_velocity(const __grid_constant__ 
         {
             const double v2[2] = {s0, s1};
             const double g = rz, in_tot = A.in_tot, tol = A.tol;
-            cluster_reduce<NT>(cl, v2, slots, slot, out, [g, in_tot, tol, EPS](double *t) {
+            const double se = A.step_eps;
+            cluster_reduce<NT>(cl, v2, slots, slot, out, [g, in_tot, tol, se](double *t) {
                 const double rms = sqrt(in_tot * t[1]);
-                t[1] = t[0] / (g + EPS);
+                t[1] = t[0] / (g + se);
                 t[2] = rms < tol ? 1.0 : 0.0;
                 t[3] = rms;
             });

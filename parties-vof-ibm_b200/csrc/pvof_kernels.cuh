@@ -30,6 +30,7 @@ struct VelArgs {
     const double *rhs, *rho, *mu;
     double *r, *dir, *dir2, *z, *Ad, *diag;
     double iRe, alpha_dt, in_tot, tol;
+    double step_eps;       // added to the step-length and direction denominators (1e-14 in the reference)
     int maxit;
     double *partials;
     DevScalars *scal;

@@ -80,6 +80,7 @@ class Params(C.Structure):
         ("stencil_fp32", C.c_int),
         ("pressure_warm_start", C.c_int),
         ("pressure_preconditioner", C.c_int),
+        ("velocity_cg_unregularized", C.c_int),
     ]
 
 

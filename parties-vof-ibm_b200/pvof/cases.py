@@ -85,6 +85,7 @@ def default_params(**kw):
     p.stencil_fp32 = 0
     p.pressure_warm_start = 0
     p.pressure_preconditioner = 0
+    p.velocity_cg_unregularized = 0
     for k, v in kw.items():
         setattr(p, k, v)
     return p
