@@ -119,7 +119,7 @@ typedef struct pvof_params {
      * Jacobi diagonal; the solve still stops when sqrt(r^T D^-1 r), D the
      * Jacobi diagonal, is below P_CG_ETOL, so the result moves within that
      * tolerance.  Planar grids with x periodic, walls in y, a power-of-two x
-     * cell count up to 2048 and at most 1024 y cells; 0 is the reference's
+     * cell count up to 1024 and at most 1024 y cells; 0 is the reference's
      * Jacobi-PCG */
     int pressure_preconditioner;
     /* no counterpart in the reference: 1 drops the 1e-14 that the momentum

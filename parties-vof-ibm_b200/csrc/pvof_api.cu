@@ -720,10 +720,8 @@ int p_precond(pvof_ctx *c)
     return launch2d(c, k_p_precond, 0, c->dom.NX - 1, 0, c->dom.NY - 1, (const double *)F(c, PVOF_F_RHO), S(c, SC_P_MINV));
 }
 
-// the pressure PCG with the spectral preconditioner (pvof_spec.cu); the host
-// looks at the convergence flag every SPEC_BATCH iterations
-constexpr int SPEC_BATCH = 4;
-
+// the pressure PCG with the spectral preconditioner (pvof_spec.cu), one
+// cooperative launch per solve
 int p_solve_spectral(pvof_ctx *c)
 {
     const Dom &d = c->dom;
@@ -735,14 +733,16 @@ int p_solve_spectral(pvof_ctx *c)
         build_metrics(c->g, d.NX, d.NY, hm);
         const double idx2 = hm.idx_c[1 + NG] * hm.idx_c[1 + NG], idy2 = hm.idy_c[1 + NG] * hm.idy_c[1 + NG];
         c->spec_fscale = 1.0 / (idy2 * (double)N);
-        std::vector<double> lamx, tw;
-        spec_tables(N, idx2, idy2, lamx, tw);
-        std::vector<double> h(lamx);
-        h.insert(h.end(), tw.begin(), tw.end());
-        h.resize(h.size() + (size_t)M, 0.0);   // per-block sums
+        c->spec_blocks = spec_pcg_blocks(c->device, N, M);
+        if (c->spec_blocks <= 0) return set_err(PVOF_ECUDA, "the spectral pressure solve needs a cooperative launch");
+        std::vector<double> tw, pcr;
+        c->spec_rounds = spec_tables(N, M, idx2, idy2, tw, pcr);
+        const size_t parts = 3 * (size_t)c->spec_blocks;
+        std::vector<double> h(tw);
+        h.resize(h.size() + parts, 0.0);
+        h.insert(h.end(), pcr.begin(), pcr.end());
         if (cudaMalloc(&c->spec_mem, h.size() * sizeof(double)) != cudaSuccess ||
-            cudaMalloc(&c->spec_s, sizeof(SpecScal)) != cudaSuccess ||
-            cudaMallocHost(&c->spec_done, sizeof(int)) != cudaSuccess)
+            cudaMalloc(&c->spec_s, sizeof(SpecScal)) != cudaSuccess)
             return set_err(PVOF_ENOMEM, "allocating the spectral preconditioner");
         CK(cudaMemcpy(c->spec_mem, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
         CK(cudaMemset(c->spec_s, 0, sizeof(SpecScal)));
@@ -758,42 +758,23 @@ int p_solve_spectral(pvof_ctx *c)
     A.z = S(c, SC_P_Z);
     A.Ad = S(c, SC_P_AD);
     A.hat = S(c, SC_P_HAT);
-    A.lamx = c->spec_mem;
-    A.tw = reinterpret_cast<const double2 *>(c->spec_mem + N);
+    A.tw = reinterpret_cast<const double2 *>(c->spec_mem);
+    A.part = c->spec_mem + N;
+    A.pcr = A.part + 3 * (size_t)c->spec_blocks;
     A.N = N;
     A.logN = 0;
     while ((1 << A.logN) < N) A.logN++;
     A.M = M;
+    A.rounds = c->spec_rounds;
     A.fscale = c->spec_fscale;
     A.tol = c->p.P_CG_ETOL;
     A.maxit = c->p.P_CG_MAXIT;
-    A.part = c->spec_mem + 2 * N;
     A.s = c->spec_s;
     A.scal = c->scal;
-    const int n = N * M;
-    long long kernels = 0;
-    TRY(timed_launch(c, PVOF_SOLVER_PRESSURE, 0, n, [&]() -> cudaError_t {
-        cudaError_t e = spec_launch_init(A, c->stream);
-        if (e != cudaSuccess) return e;
-        kernels += 3;
-        double *dcur = S(c, SC_P_D), *dnxt = S(c, SC_P_D2);
-        int it = 0;
-        while (it < A.maxit) {
-            for (int b = 0; b < SPEC_BATCH && it < A.maxit; b++, it++) {
-                e = spec_launch_iteration(A, dcur, dnxt, it == 0 ? 1 : 0, c->stream);
-                if (e != cudaSuccess) return e;
-                kernels += 4;
-                std::swap(dcur, dnxt);
-            }
-            e = cudaMemcpyAsync(c->spec_done, &c->spec_s->done, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-            if (e != cudaSuccess) return e;
-            if (*c->spec_done) break;
-        }
-        kernels += 2;
-        return spec_launch_mean(A, c->stream);
+    c->launches++;   // the barrier counter's reset
+    TRY(timed_launch(c, PVOF_SOLVER_PRESSURE, 0, N * M, [&]() {
+        return spec_launch_pcg(A, c->spec_blocks, S(c, SC_P_D), S(c, SC_P_D2), c->stream);
     }));
-    c->launches += kernels - 1;
     return fill(c, BK_WRAP_C, F(c, PVOF_F_DELTAP));
 }
 
@@ -852,6 +833,7 @@ int read_scalars(pvof_ctx *c)
     if (c->npend) collect_solver_timing(c);
     if (c->scal_host->error) {
         CK(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
+        if (c->spec_s) CK(cudaMemsetAsync(c->spec_s, 0, sizeof(SpecScal), c->stream));
         CK(cudaStreamSynchronize(c->stream));
         return set_err(PVOF_ECUDA, "solver grid barrier timed out");
     }
@@ -1600,8 +1582,8 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
         const int N = grid->NXM, M = grid->NYM;
         if (grid->geometry != PVOF_GEOM_PLANAR || !grid->periodic[0] || grid->periodic[1])
             return set_err(PVOF_EINVAL, "the spectral pressure preconditioner needs a planar grid, x periodic, walls in y");
-        if ((N & (N - 1)) != 0 || N > 2048 || M > 1024)
-            return set_err(PVOF_EINVAL, "the spectral pressure preconditioner needs a power-of-two x cell count up to 2048 "
+        if ((N & (N - 1)) != 0 || N > 1024 || M > 1024)
+            return set_err(PVOF_EINVAL, "the spectral pressure preconditioner needs a power-of-two x cell count up to 1024 "
                                         "and at most 1024 y cells");
     }
     int ndev = 0;
@@ -1764,7 +1746,6 @@ int pvof_destroy(pvof_ctx *c)
     if (c->fft_coef) cudaFree(c->fft_coef);
     if (c->spec_mem) cudaFree(c->spec_mem);
     if (c->spec_s) cudaFree(c->spec_s);
-    if (c->spec_done) cudaFreeHost(c->spec_done);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PVOF_OK;

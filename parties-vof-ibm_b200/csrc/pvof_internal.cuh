@@ -156,10 +156,11 @@ struct Ctx {
     int npend;
     IbmState *ibm;           // resolved particles (null until pvof_set_particles)
     double *fft_coef;        // as, ap, an (NY-1 each) and the modified wavenumbers (NX-1)
-    double *spec_mem;        // spectral pressure preconditioner: x eigenvalues, twiddles, block sums
-    struct SpecScal *spec_s; // its device scalars
-    int *spec_done;          // pinned host copy of its convergence flag
+    double *spec_mem;        // spectral pressure preconditioner: twiddles, block sums, reduction tables
+    struct SpecScal *spec_s; // its grid barrier state
     double spec_fscale;      // dy^2 / N
+    int spec_blocks;         // blocks of its cooperative launch
+    int spec_rounds;         // its cyclic-reduction rounds
     double sol_ms[3];
     long long sol_launches[3], sol_iters[3], sol_cell_iters[3];
 };

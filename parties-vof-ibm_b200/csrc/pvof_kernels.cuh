@@ -50,10 +50,11 @@ struct PresArgs {
 
 // spectral-preconditioned pressure PCG (pvof_spec.cu)
 struct SpecScal {
-    double gamma, beta, alpha, res, avg;
-    int iters, done;
-    unsigned cnt[8];   // arrival counters of the per-launch reductions
+    unsigned bar_count;   // grid barrier arrivals of the cooperative solve
 };
+
+constexpr int SPEC_PT = 1024;        // threads per block of the cooperative solve
+constexpr int SPEC_MAXROUNDS = 10;   // cyclic-reduction rounds for up to 1024 rows
 
 struct SpecArgs {
     Dom d;
@@ -61,22 +62,22 @@ struct SpecArgs {
     double *phi;              // deltap
     const double *rhs, *rho, *MJ;
     double *res, *z, *Ad, *hat;
-    const double *lamx;       // dy^2 times the x eigenvalue of each half-complex index
     const double2 *tw;        // exp(-2 pi i k / N), k < N / 2
+    const double *pcr;        // cyclic-reduction multipliers per round, then 1 / b ([2 rounds + 1][N][M])
     int N, logN, M;           // x cells (a power of two), log2 N, y cells
+    int rounds;               // cyclic-reduction rounds, ceil(log2 M)
     double fscale;            // dy^2 / N
     double tol;
     int maxit;
-    double *part;             // per-block sums, M entries
+    double *part;             // per-block sums, three slots of gridDim entries
     SpecScal *s;
     DevScalars *scal;
 };
 
 bool spec_supported(const Dom &d, const char **why);
-int spec_tables(int N, double idx2, double idy2, std::vector<double> &lamx, std::vector<double> &tw);
-cudaError_t spec_launch_init(const SpecArgs &A, cudaStream_t st);
-cudaError_t spec_launch_iteration(const SpecArgs &A, const double *dold, double *dnew, int first, cudaStream_t st);
-cudaError_t spec_launch_mean(const SpecArgs &A, cudaStream_t st);
+int spec_tables(int N, int M, double idx2, double idy2, std::vector<double> &tw, std::vector<double> &pcr);
+int spec_pcg_blocks(int device, int N, int M);
+cudaError_t spec_launch_pcg(const SpecArgs &A, int blocks, double *d0, double *d1, cudaStream_t st);
 
 __global__ void k_fill(Dom d, BcMap m, double *f);
 __global__ void k_weno_flux(Dom d, int i0, int i1, int j0, int j1, const double *C, const double *u, const double *v,

@@ -15,9 +15,12 @@
 //   2. every half-complex index m: parallel cyclic reduction (one thread per
 //      row, log2 M elimination rounds in shared memory) of
 //        -z_{j-1} + (b_j + dy^2 lambda_x(m)) z_j - z_{j+1} = rhs_j,
-//      b_j = 2 inside, 1 at the two walls; for the mean mode the first row is
-//      pinned and the column's mean removed afterwards, so the constant mode,
-//      the operator's null space, is projected out;
+//      b_j = 2 inside, 1 at the two walls.  The matrices do not change, so
+//      the rounds' multipliers and the final reciprocal diagonals are
+//      computed once per context on the host (spec_tables) and a round is
+//      two multiply-adds.  For the mean mode the first row is pinned and the
+//      right-hand side and the result are made mean-free, so the constant
+//      mode, the operator's null space, is projected out;
 //   3. every row: inverse transform.
 //
 // With the density ratio rho_max / rho_min the preconditioned operator's
@@ -27,13 +30,16 @@
 // so the solve stops at the same residual size; the iterates differ, so the
 // result moves within that tolerance of the reference's.
 //
-// One PCG iteration is four launches (matrix-vector product with the new
-// direction formed on the fly, update + forward row transforms, tridiagonal
-// solves, inverse row transforms + inner product); each launch's last block
-// (arrival counter) forms the iteration's scalars from the per-block sums in
-// block order, so the arithmetic does not depend on scheduling.  A device
-// flag set at convergence makes the later launches return at once; the host
-// looks at it every SPEC_BATCH iterations.
+// The whole solve is ONE cooperative launch: blocks of SPEC_PT threads, eight
+// 128-thread row groups in the row phases, SPEC_PT / Mp reduction systems per
+// block (Mp = M rounded up to 32), four grid barriers per iteration (after the
+// matrix-vector product, the update with its forward transforms, the
+// tridiagonal solves, the inverse transforms).  Every block adds the
+// per-block sums in block order, so all of them take the same decisions.  The
+// grid barrier is one arrival counter that only grows during a launch (the
+// host zeroes it before each), so a block waits for one atomic round trip;
+// its wait is bounded (on timeout the error flag in DevScalars is set and
+// every block leaves).
 #include <cmath>
 #include <vector>
 
@@ -45,6 +51,8 @@ namespace pvof {
 namespace {
 
 constexpr int ROW_THREADS = 128;
+constexpr int ROWG = SPEC_PT / ROW_THREADS;
+constexpr unsigned long long SPEC_SPIN_LIMIT = 1ull << 26;
 
 // sum over the block, in a fixed order; the total is valid in thread 0
 __device__ double block_sum(double v, double *sh)
@@ -60,39 +68,71 @@ __device__ double block_sum(double v, double *sh)
     return t;
 }
 
-// publish this block's sum; true in the block that arrives last, which then
-// adds all the block sums in block order (result valid in its thread 0)
-__device__ bool finish_sum(double v, double *part, unsigned *cnt, double *sh, double &total)
+// Grid barrier number `nth` (1, 2, ...) of this launch: every block adds one
+// to the arrival counter (zeroed by the host before the launch) and waits
+// until it reaches nth * gridDim.x.  Returns false (in every thread of the
+// block) when the wait gave up.
+__device__ __noinline__ bool spec_barrier(unsigned *count, unsigned nth, int *err)
 {
-    __shared__ bool last;
-    const double b = block_sum(v, sh);
-    const unsigned nb = gridDim.x;
+    __shared__ int ok;
+    __syncthreads();
     if (threadIdx.x == 0) {
-        part[blockIdx.x] = b;
+        volatile unsigned *vc = count;
+        volatile int *verr = err;
+        int good = (*verr == 0);
+        const unsigned target = nth * gridDim.x;
         __threadfence();
-        last = atomicAdd(cnt, 1u) == nb - 1;
+        atomicAdd(count, 1u);
+        unsigned long long spins = 0;
+        while ((int)(*vc - target) < 0) {
+            ++spins;
+            if ((spins & 1023ull) == 0 && (*verr != 0 || spins > SPEC_SPIN_LIMIT)) {
+                atomicExch(err, 1);
+                good = 0;
+                break;
+            }
+            if (spins > 4096) __nanosleep(64);
+        }
+        __threadfence();
+        ok = good;
     }
     __syncthreads();
-    if (!last) return false;
-    __threadfence();
-    double s = 0.0;
-    for (unsigned k = threadIdx.x; k < nb; k += blockDim.x) s += __ldcg(part + k);
-    total = block_sum(s, sh);
-    if (threadIdx.x == 0) *cnt = 0u;
-    return true;
+    return ok != 0;
 }
 
-// in-place complex FFT of a[0..N), N = 2^logN, by the block; sign -1 forward
-__device__ void fft(double2 *a, int N, int logN, const double2 *__restrict__ tw, double sign)
+// this block's sum of v into slot[blockIdx.x]
+__device__ void put_part(double v, double *slot, double *sh)
 {
-    for (int t = threadIdx.x; t < N; t += blockDim.x) {
+    const double b = block_sum(v, sh);
+    if (threadIdx.x == 0) slot[blockIdx.x] = b;
+}
+
+// the sum of a slot over all blocks, in block order, in every thread
+__device__ double slot_total(const double *slot, double *sh)
+{
+    __shared__ double res;
+    double s = 0.0;
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) s += __ldcg(slot + k);
+    const double t = block_sum(s, sh);
+    if (threadIdx.x == 0) res = t;
+    __syncthreads();
+    const double r = res;
+    __syncthreads();
+    return r;
+}
+
+// complex FFT of a[0..N), N = 2^logN, by the 128 threads of one row group
+// (lt = 0..127); sign -1 forward.  All groups of the block run it in lockstep.
+__device__ void fft_group(double2 *a, int N, int logN, const double2 *__restrict__ tw, double sign, int lt)
+{
+    for (int t = lt; t < N; t += ROW_THREADS) {
         const int r = (int)(__brev((unsigned)t) >> (32 - logN));
         if (r > t) { const double2 x = a[t]; a[t] = a[r]; a[r] = x; }
     }
     __syncthreads();
     for (int s = 0; s < logN; s++) {
         const int half = 1 << s, step = N >> (s + 1);
-        for (int t = threadIdx.x; t < N / 2; t += blockDim.x) {
+        for (int t = lt; t < N / 2; t += ROW_THREADS) {
             const int pos = t & (half - 1), i0 = ((t >> s) << (s + 1)) + pos, i1 = i0 + half;
             double2 w = tw[pos * step];
             w.y *= -sign;   // the table holds exp(-2 pi i k / N); the inverse takes its conjugate
@@ -105,206 +145,227 @@ __device__ void fft(double2 *a, int N, int logN, const double2 *__restrict__ tw,
     }
 }
 
-// sm holds a real row (imaginary parts zero): forward transform into the
-// half-complex row j of hat, times scale
-__device__ void row_forward(const SpecArgs &A, double2 *sm, int j)
+// forward transform of the group's row (already in a) into hat row j
+__device__ void group_forward(const SpecArgs &A, double2 *a, int j, bool active, int lt)
 {
     const int P = A.d.P, N = A.N;
     __syncthreads();
-    fft(sm, N, A.logN, A.tw, -1.0);
-    for (int k = threadIdx.x; k <= N / 2; k += blockDim.x) AT_(A.hat, k, j) = sm[k].x * A.fscale;
-    for (int k = 1 + threadIdx.x; k < N / 2; k += blockDim.x) AT_(A.hat, N - k, j) = sm[k].y * A.fscale;
+    fft_group(a, N, A.logN, A.tw, -1.0, lt);
+    if (active) {
+        for (int k = lt; k <= N / 2; k += ROW_THREADS) AT_(A.hat, k, j) = a[k].x * A.fscale;
+        for (int k = 1 + lt; k < N / 2; k += ROW_THREADS) AT_(A.hat, N - k, j) = a[k].y * A.fscale;
+    }
+    __syncthreads();   // the next row step overwrites a
 }
 
 __device__ __forceinline__ int src_x(const SpecArgs &A, int i) { return A.mp.x.src[i + NG]; }
 __device__ __forceinline__ int src_y(const SpecArgs &A, int j) { return A.mp.y.src[j + NG]; }
 
+// mean over the block's system 0 (threads sys == 0), broadcast to the block
+__device__ double system0_mean(double v, bool sys0, int M, double *sh)
+{
+    __shared__ double mean;
+    const double t = block_sum(sys0 ? v : 0.0, sh);
+    if (threadIdx.x == 0) mean = t / (double)M;
+    __syncthreads();
+    const double r = mean;
+    __syncthreads();
+    return r;
+}
+
+// the tridiagonal solves of every half-complex index, hat in place
+__device__ void tridiag_phase(const SpecArgs &A, double *smem, double *sh)
+{
+    const int P = A.d.P, N = A.N, M = A.M, Mp = (M + 31) / 32 * 32, S = SPEC_PT / Mp;
+    const int sys = threadIdx.x / Mp, j = threadIdx.x - sys * Mp;
+    const size_t NM = (size_t)N * M;
+    double *sd = smem + (size_t)sys * Mp;
+    for (int m0 = blockIdx.x * S; m0 < N; m0 += gridDim.x * S) {
+        const int m = m0 + sys;
+        const bool row = sys < S && m < N && j < M;
+        double r = row ? AT_(A.hat, m, j) : 0.0;
+        if (m0 == 0) {   // this block holds the mean mode as its system 0
+            const double mean = system0_mean(r, sys == 0, M, sh);
+            if (m == 0) r = j == 0 ? 0.0 : r - mean;   // mean-free, first row pinned
+        }
+        // this thread's multipliers, all loads in flight at once: round st
+        // k1 at [2 st NM], k2 at [(2 st + 1) NM], then 1 / b at [2 rounds NM]
+        const double *k = A.pcr + (size_t)m * M + j;
+        double kr[2 * SPEC_MAXROUNDS + 1];
+#pragma unroll
+        for (int q = 0; q < 2 * SPEC_MAXROUNDS + 1; q++) kr[q] = (row && q <= 2 * A.rounds) ? k[(size_t)q * NM] : 0.0;
+#pragma unroll
+        for (int st = 0; st < SPEC_MAXROUNDS; st++) {
+            if (st >= A.rounds) break;
+            const int s = 1 << st;
+            if (row) sd[j] = r;
+            __syncthreads();
+            if (row) {
+                double rn = r;
+                if (j - s >= 0) rn -= sd[j - s] * kr[2 * st];
+                if (j + s < M) rn -= sd[j + s] * kr[2 * st + 1];
+                r = rn;
+            }
+            __syncthreads();
+        }
+        double ib = 0.0;
+#pragma unroll
+        for (int q = 0; q < 2 * SPEC_MAXROUNDS + 1; q++)
+            if (q == 2 * A.rounds) ib = kr[q];
+        double x = row ? r * ib : 0.0;   // times the final 1 / b
+        if (m0 == 0) {
+            const double mean = system0_mean(x, sys == 0, M, sh);
+            if (m == 0) x -= mean;
+        }
+        if (row) AT_(A.hat, m, j) = x;
+    }
+}
+
 }  // namespace
 
-// r = rhs - A phi, the stopping test, forward transforms of r
-__global__ void __launch_bounds__(ROW_THREADS) k_spec_init_rows(SpecArgs A)
+__global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, double *d1)
 {
-    extern __shared__ double2 sm[];
+    extern __shared__ double smem[];   // the twiddles, then the row / reduction work area
     __shared__ double sh[32];
     const Dom &d = A.d;
-    const int P = d.P, NX = d.NX, NY = d.NY, j = blockIdx.x;
-    double sJ = 0.0;
-    for (int i = threadIdx.x; i < A.N; i += blockDim.x) {
-        const double ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, A.phi, P, NX, NY, a, b); });
-        const double rv = AT_(A.rhs, i, j) - ad;
-        AT_(A.res, i, j) = rv;
-        sJ += rv * (rv * AT_(A.MJ, i, j));
-        sm[i] = make_double2(rv, 0.0);
-    }
-    row_forward(A, sm, j);
-    double tot;
-    if (finish_sum(sJ, A.part, &A.s->cnt[0], sh, tot) && threadIdx.x == 0) {
-        A.s->iters = 0;
-        A.s->res = sqrt(tot);
-        A.s->done = sqrt(tot) < A.tol ? 1 : 0;
-    }
-}
-
-// tridiagonal solves along y by parallel cyclic reduction, one block per
-// half-complex index
-__global__ void k_spec_tridiag(SpecArgs A)
-{
-    if (A.s->done) return;
-    extern __shared__ double sbuf[];
-    __shared__ double sh[32];
-    const int P = A.d.P, M = A.M, m = blockIdx.x, j = threadIdx.x;
-    double *sa = sbuf, *sb = sa + M, *sc = sb + M, *sd = sc + M;
-    const bool row = j < M;
-    double a = 0.0, b = 1.0, c = 0.0, r = row ? AT_(A.hat, m, j) : 0.0;
-    if (m == 0) {   // the mean mode: a mean-free right-hand side, so the pinned row's equation holds too
-        __shared__ double rmean;
-        const double t = block_sum(r, sh);
-        if (threadIdx.x == 0) rmean = t / (double)M;
-        __syncthreads();
-        r -= rmean;
-    }
-    if (row && !(m == 0 && j == 0)) {
-        a = j > 0 ? -1.0 : 0.0;
-        c = j < M - 1 ? -1.0 : 0.0;
-        b = A.lamx[m] + (j > 0 ? 1.0 : 0.0) + (j < M - 1 ? 1.0 : 0.0);
-    } else {
-        r = 0.0;
-    }
-    for (int s = 1; s < M; s <<= 1) {
-        if (row) { sa[j] = a; sb[j] = b; sc[j] = c; sd[j] = r; }
-        __syncthreads();
-        if (row) {
-            double an = 0.0, cn = 0.0, bn = b, rn = r;
-            if (j - s >= 0) {
-                const double k1 = a / sb[j - s];
-                bn -= sc[j - s] * k1;
-                rn -= sd[j - s] * k1;
-                an = -sa[j - s] * k1;
-            }
-            if (j + s < M) {
-                const double k2 = c / sb[j + s];
-                bn -= sa[j + s] * k2;
-                rn -= sd[j + s] * k2;
-                cn = -sc[j + s] * k2;
-            }
-            a = an; b = bn; c = cn; r = rn;
-        }
-        __syncthreads();
-    }
-    double x = row ? r / b : 0.0;
-    if (m == 0) {   // project out the constant mode
-        __shared__ double mean;
-        const double t = block_sum(x, sh);
-        if (threadIdx.x == 0) mean = t / (double)M;
-        __syncthreads();
-        x -= mean;
-    }
-    if (row) AT_(A.hat, m, j) = x;
-}
-
-// z = inverse transform of the solved rows; gamma = r.z; first: gamma, beta = 0
-__global__ void __launch_bounds__(ROW_THREADS) k_spec_inverse_rows(SpecArgs A, int first)
-{
-    if (A.s->done) return;
-    extern __shared__ double2 sm[];
-    __shared__ double sh[32];
-    const int P = A.d.P, N = A.N, j = blockIdx.x;
-    for (int k = threadIdx.x; k < N; k += blockDim.x) {
-        double2 v;
-        if (k == 0 || 2 * k == N) v = make_double2(AT_(A.hat, k, j), 0.0);
-        else if (k < N / 2) v = make_double2(AT_(A.hat, k, j), AT_(A.hat, N - k, j));
-        else v = make_double2(AT_(A.hat, N - k, j), -AT_(A.hat, k, j));
-        sm[k] = v;
-    }
+    const int P = d.P, NX = d.NX, NY = d.NY, N = A.N, M = A.M;
+    const int grp = threadIdx.x / ROW_THREADS, lt = threadIdx.x - grp * ROW_THREADS;
+    double2 *tw = reinterpret_cast<double2 *>(smem);
+    double *work = smem + N;   // N / 2 complex twiddles before it
+    double2 *row = reinterpret_cast<double2 *>(work) + (size_t)grp * N;
+    double *slotA = A.part, *slotB = A.part + gridDim.x, *slotC = A.part + 2 * gridDim.x;
+    unsigned *count = &A.s->bar_count;
+    unsigned nb = 0;   // grid barriers passed
+    int *err = &A.scal->error;
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    for (int k = threadIdx.x; k < N / 2; k += blockDim.x) tw[k] = A.tw[k];
     __syncthreads();
-    fft(sm, N, A.logN, A.tw, 1.0);
-    double g = 0.0;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-        const double z = sm[i].x;
-        AT_(A.z, i, j) = z;
-        g += AT_(A.res, i, j) * z;
-    }
-    double tot;
-    if (finish_sum(g, A.part, &A.s->cnt[1], sh, tot) && threadIdx.x == 0) {
-        A.s->beta = first ? 0.0 : tot / (A.s->gamma + 1e-30);
-        A.s->gamma = tot;
-    }
-}
+    SpecArgs B = A;
+    B.tw = tw;
 
-// d = z + beta d_old (d = z on the first iteration) at every cell and its
-// neighbours, Ad, d.Ad; alpha = gamma / d.Ad
-__global__ void __launch_bounds__(ROW_THREADS) k_spec_matvec(SpecArgs A, const double *__restrict__ dold,
-                                                             double *__restrict__ dnew, int first)
-{
-    if (A.s->done) return;
-    __shared__ double sh[32];
-    const Dom &d = A.d;
-    const int P = d.P, NX = d.NX, NY = d.NY, j = blockIdx.x;
-    const double bt = A.s->beta;
-    auto dir = [&](int a, int b) {
-        int si = a, sj = b;
-        if (!(a >= 1 && a <= NX - 2 && b >= 1 && b <= NY - 2)) { si = src_x(A, a); sj = src_y(A, b); }
-        return first ? AT_(A.z, si, sj) : AT_(A.z, si, sj) + bt * AT_(dold, si, sj);
-    };
-    double s = 0.0;
-    for (int i = threadIdx.x; i < A.N; i += blockDim.x) {
-        const double dv = dir(i, j);
-        AT_(dnew, i, j) = dv;
-        const double ad = pressure_op(d, A.rho, i, j, dir);
-        AT_(A.Ad, i, j) = ad;
-        s += dv * ad;
-    }
-    double tot;
-    if (finish_sum(s, A.part, &A.s->cnt[2], sh, tot) && threadIdx.x == 0) A.s->alpha = A.s->gamma / (tot + 1e-30);
-}
-
-// phi += alpha d, r -= alpha Ad, the stopping test, forward transforms of r
-__global__ void __launch_bounds__(ROW_THREADS) k_spec_update_rows(SpecArgs A, const double *__restrict__ dcur)
-{
-    if (A.s->done) return;
-    extern __shared__ double2 sm[];
-    __shared__ double sh[32];
-    const int P = A.d.P, j = blockIdx.x;
-    const double alpha = A.s->alpha;
+    // r = rhs - A phi, the stopping sum, forward transforms
     double sJ = 0.0;
-    for (int i = threadIdx.x; i < A.N; i += blockDim.x) {
-        AT_(A.phi, i, j) += alpha * AT_(dcur, i, j);
-        const double rv = AT_(A.res, i, j) - alpha * AT_(A.Ad, i, j);
-        AT_(A.res, i, j) = rv;
-        sJ += rv * (rv * AT_(A.MJ, i, j));
-        sm[i] = make_double2(rv, 0.0);
+    for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
+        const int j = j0 + grp;
+        const bool active = j < M;
+        if (active) {
+            for (int i = lt; i < N; i += ROW_THREADS) {
+                const double ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, A.phi, P, NX, NY, a, b); });
+                const double rv = AT_(A.rhs, i, j) - ad;
+                AT_(A.res, i, j) = rv;
+                sJ += rv * (rv * AT_(A.MJ, i, j));
+                row[i] = make_double2(rv, 0.0);
+            }
+        }
+        group_forward(B, row, j, active, lt);
     }
-    row_forward(A, sm, j);
-    double tot;
-    if (finish_sum(sJ, A.part, &A.s->cnt[3], sh, tot) && threadIdx.x == 0) {
-        const int it = A.s->iters + 1;
-        A.s->iters = it;
-        A.s->res = sqrt(tot);
-        if (sqrt(tot) < A.tol || it >= A.maxit) A.s->done = 1;
+    put_part(sJ, slotA, sh);
+    if (!spec_barrier(count, ++nb, err)) return;
+    double tot = slot_total(slotA, sh);
+    int iters = 0;
+    double res = sqrt(tot);
+    if (sqrt(tot) < A.tol) {   // converged before the first iteration: phi stays as it is
+        if (lead) { A.scal->p_iters = 0; A.scal->p_res = res; }
+        return;
     }
-}
-
-// the mean of phi over the solve range (psolve_cg.c:255-279); a solve that
-// stops before its first iteration leaves phi as it is, as the reference does
-__global__ void __launch_bounds__(ROW_THREADS) k_spec_mean(SpecArgs A)
-{
-    __shared__ double sh[32];
-    const int P = A.d.P, j = blockIdx.x;
-    double s = 0.0;
-    for (int i = threadIdx.x; i < A.N; i += blockDim.x) s += AT_(A.phi, i, j);
-    double tot;
-    if (finish_sum(s, A.part, &A.s->cnt[4], sh, tot) && threadIdx.x == 0) {
-        A.s->avg = A.s->iters == 0 ? 0.0 : tot / ((double)A.N * (double)A.M);
-        A.scal->p_iters = A.s->iters;
-        A.scal->p_res = A.s->res;
+    double gamma = 0.0, beta = 0.0;
+    double *dold = d0, *dnew = d1;
+    for (int it = 0;; it++) {
+        // z = (-L)^-1 r
+        tridiag_phase(A, work, sh);
+        if (!spec_barrier(count, ++nb, err)) return;
+        double g = 0.0;
+        for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
+            const int j = j0 + grp;
+            const bool active = j < M;
+            if (active) {
+                for (int k = lt; k < N; k += ROW_THREADS) {
+                    double2 v;
+                    if (k == 0 || 2 * k == N) v = make_double2(AT_(A.hat, k, j), 0.0);
+                    else if (k < N / 2) v = make_double2(AT_(A.hat, k, j), AT_(A.hat, N - k, j));
+                    else v = make_double2(AT_(A.hat, N - k, j), -AT_(A.hat, k, j));
+                    row[k] = v;
+                }
+            }
+            __syncthreads();
+            fft_group(row, N, A.logN, tw, 1.0, lt);
+            if (active) {
+                for (int i = lt; i < N; i += ROW_THREADS) {
+                    const double z = row[i].x;
+                    AT_(A.z, i, j) = z;
+                    g += AT_(A.res, i, j) * z;
+                }
+            }
+            __syncthreads();
+        }
+        put_part(g, slotB, sh);
+        if (!spec_barrier(count, ++nb, err)) return;
+        const double gnew = slot_total(slotB, sh);
+        beta = it == 0 ? 0.0 : gnew / (gamma + 1e-30);
+        gamma = gnew;
+        if (it >= A.maxit) break;
+        // d = z + beta d_old at every cell and its neighbours, Ad, d.Ad
+        const bool first = it == 0;
+        auto dir = [&](int a, int b) {
+            int si = a, sj = b;
+            if (!(a >= 1 && a <= NX - 2 && b >= 1 && b <= NY - 2)) { si = src_x(A, a); sj = src_y(A, b); }
+            return first ? AT_(A.z, si, sj) : AT_(A.z, si, sj) + beta * AT_(dold, si, sj);
+        };
+        double sdad = 0.0;
+        for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
+            const int j = j0 + grp;
+            if (j >= M) continue;
+            for (int i = lt; i < N; i += ROW_THREADS) {
+                const double dv = dir(i, j);
+                AT_(dnew, i, j) = dv;
+                const double ad = pressure_op(d, A.rho, i, j, dir);
+                AT_(A.Ad, i, j) = ad;
+                sdad += dv * ad;
+            }
+        }
+        put_part(sdad, slotC, sh);
+        if (!spec_barrier(count, ++nb, err)) return;
+        const double alpha = gamma / (slot_total(slotC, sh) + 1e-30);
+        // phi += alpha d, r -= alpha Ad, the stopping sum, forward transforms
+        sJ = 0.0;
+        for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
+            const int j = j0 + grp;
+            const bool active = j < M;
+            if (active) {
+                for (int i = lt; i < N; i += ROW_THREADS) {
+                    AT_(A.phi, i, j) += alpha * AT_(dnew, i, j);
+                    const double rv = AT_(A.res, i, j) - alpha * AT_(A.Ad, i, j);
+                    AT_(A.res, i, j) = rv;
+                    sJ += rv * (rv * AT_(A.MJ, i, j));
+                    row[i] = make_double2(rv, 0.0);
+                }
+            }
+            group_forward(B, row, j, active, lt);
+        }
+        put_part(sJ, slotA, sh);
+        if (!spec_barrier(count, ++nb, err)) return;
+        tot = slot_total(slotA, sh);
+        iters = it + 1;
+        res = sqrt(tot);
+        if (sqrt(tot) < A.tol || iters >= A.maxit) break;
+        double *t = dold; dold = dnew; dnew = t;
     }
-}
-
-__global__ void __launch_bounds__(ROW_THREADS) k_spec_sub_mean(SpecArgs A)
-{
-    const int P = A.d.P, j = blockIdx.x;
-    const double avg = A.s->avg;
-    for (int i = threadIdx.x; i < A.N; i += blockDim.x) AT_(A.phi, i, j) -= avg;
+    // remove the mean (psolve_cg.c:255-279)
+    double ssum = 0.0;
+    for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
+        const int j = j0 + grp;
+        if (j >= M) continue;
+        for (int i = lt; i < N; i += ROW_THREADS) ssum += AT_(A.phi, i, j);
+    }
+    put_part(ssum, slotB, sh);
+    if (!spec_barrier(count, ++nb, err)) return;
+    const double avg = slot_total(slotB, sh) / ((double)N * (double)M);
+    for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
+        const int j = j0 + grp;
+        if (j >= M) continue;
+        for (int i = lt; i < N; i += ROW_THREADS) AT_(A.phi, i, j) -= avg;
+    }
+    if (lead) { A.scal->p_iters = iters; A.scal->p_res = res; }
 }
 
 // ---------------------------------------------------------------------------
@@ -315,52 +376,85 @@ bool spec_supported(const Dom &d, const char **why)
     const int N = d.NX - 1, M = d.NY - 1;
     if (!d.planar || d.axisym) { *why = "the spectral pressure preconditioner is built for the planar mode only"; return false; }
     if (!d.perx || d.pery) { *why = "the spectral pressure preconditioner needs x periodic and walls in y"; return false; }
-    if (N < 2 || (N & (N - 1)) != 0 || N > 2048) { *why = "the spectral pressure preconditioner needs a power-of-two x cell count (2..2048)"; return false; }
+    if (N < 2 || (N & (N - 1)) != 0 || N > 1024) { *why = "the spectral pressure preconditioner needs a power-of-two x cell count (2..1024)"; return false; }
     if (M < 1 || M > 1024) { *why = "the spectral pressure preconditioner needs at most 1024 y cells"; return false; }
     return true;
 }
 
-int spec_tables(int N, double idx2, double idy2, std::vector<double> &lamx, std::vector<double> &tw)
+int spec_tables(int N, int M, double idx2, double idy2, std::vector<double> &tw, std::vector<double> &pcr)
 {
-    lamx.assign(N, 0.0);
-    for (int m = 0; m < N; m++) {
-        const int wave = m <= N / 2 ? m : N - m;
-        lamx[m] = (2.0 - 2.0 * std::cos(2.0 * M_PI * wave / N)) * idx2 / idy2;
-    }
     tw.assign(N, 0.0);   // N / 2 complex entries exp(-2 pi i k / N)
     for (int k = 0; k < N / 2; k++) {
         tw[2 * k] = std::cos(2.0 * M_PI * k / N);
         tw[2 * k + 1] = -std::sin(2.0 * M_PI * k / N);
     }
-    return 0;
+    int nsteps = 0;
+    for (int s = 1; s < M; s <<= 1) nsteps++;
+    const size_t NM = (size_t)N * M;
+    pcr.assign((size_t)(2 * nsteps + 1) * NM, 0.0);
+    std::vector<double> a(M), b(M), c(M), a2(M), b2(M), c2(M);
+    for (int m = 0; m < N; m++) {
+        const int wave = m <= N / 2 ? m : N - m;
+        const double lam = (2.0 - 2.0 * std::cos(2.0 * M_PI * wave / N)) * idx2 / idy2;
+        for (int j = 0; j < M; j++) {
+            if (m == 0 && j == 0) { a[j] = 0.0; b[j] = 1.0; c[j] = 0.0; continue; }   // the pinned row
+            a[j] = j > 0 ? -1.0 : 0.0;
+            c[j] = j < M - 1 ? -1.0 : 0.0;
+            b[j] = lam + (j > 0 ? 1.0 : 0.0) + (j < M - 1 ? 1.0 : 0.0);
+        }
+        int st = 0;
+        for (int s = 1; s < M; s <<= 1, st++) {   // the elimination rounds of the device's cyclic reduction
+            for (int j = 0; j < M; j++) {
+                double an = 0.0, cn = 0.0, bn = b[j], k1 = 0.0, k2 = 0.0;
+                if (j - s >= 0) { k1 = a[j] / b[j - s]; bn -= c[j - s] * k1; an = -a[j - s] * k1; }
+                if (j + s < M) { k2 = c[j] / b[j + s]; bn -= a[j + s] * k2; cn = -c[j + s] * k2; }
+                pcr[(size_t)(2 * st) * NM + (size_t)m * M + j] = k1;
+                pcr[(size_t)(2 * st + 1) * NM + (size_t)m * M + j] = k2;
+                a2[j] = an; b2[j] = bn; c2[j] = cn;
+            }
+            a.swap(a2); b.swap(b2); c.swap(c2);
+        }
+        for (int j = 0; j < M; j++) pcr[(size_t)(2 * nsteps) * NM + (size_t)m * M + j] = 1.0 / b[j];
+    }
+    return nsteps;
 }
 
-cudaError_t spec_launch_init(const SpecArgs &A, cudaStream_t st)
+size_t spec_pcg_smem(int N, int M)
 {
-    const size_t row_smem = (size_t)A.N * sizeof(double2);
-    const unsigned tthreads = (unsigned)((A.M + 31) / 32 * 32);
-    k_spec_init_rows<<<(unsigned)A.M, ROW_THREADS, row_smem, st>>>(A);
-    k_spec_tridiag<<<(unsigned)A.N, tthreads, 4 * (size_t)A.M * sizeof(double), st>>>(A);
-    k_spec_inverse_rows<<<(unsigned)A.M, ROW_THREADS, row_smem, st>>>(A, 1);
-    return cudaGetLastError();
+    const size_t rows = (size_t)ROWG * N * sizeof(double2);
+    const int Mp = (M + 31) / 32 * 32;
+    const size_t tri = (size_t)(SPEC_PT / Mp) * Mp * sizeof(double);
+    return (size_t)N * sizeof(double) + (rows > tri ? rows : tri);   // twiddles first
 }
 
-cudaError_t spec_launch_iteration(const SpecArgs &A, const double *dold, double *dnew, int first, cudaStream_t st)
+// blocks for k_spec_pcg: enough for one pass over the rows and the systems,
+// at most what is co-resident; 0 if the launch cannot be cooperative
+int spec_pcg_blocks(int device, int N, int M)
 {
-    const size_t row_smem = (size_t)A.N * sizeof(double2);
-    const unsigned tthreads = (unsigned)((A.M + 31) / 32 * 32);
-    k_spec_matvec<<<(unsigned)A.M, ROW_THREADS, 0, st>>>(A, dold, dnew, first);
-    k_spec_update_rows<<<(unsigned)A.M, ROW_THREADS, row_smem, st>>>(A, dnew);
-    k_spec_tridiag<<<(unsigned)A.N, tthreads, 4 * (size_t)A.M * sizeof(double), st>>>(A);
-    k_spec_inverse_rows<<<(unsigned)A.M, ROW_THREADS, row_smem, st>>>(A, 0);
-    return cudaGetLastError();
+    const size_t smem = spec_pcg_smem(N, M);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_spec_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0;
+    int per_sm = 0, sms = 0, coop = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spec_pcg, SPEC_PT, smem) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop) return 0;
+    const int Mp = (M + 31) / 32 * 32, S = SPEC_PT / Mp;
+    int want = (M + ROWG - 1) / ROWG;
+    const int sys = (N + S - 1) / S;
+    if (sys > want) want = sys;
+    const int most = per_sm * sms;
+    return most < 1 ? 0 : (want < most ? want : most);
 }
 
-cudaError_t spec_launch_mean(const SpecArgs &A, cudaStream_t st)
+cudaError_t spec_launch_pcg(const SpecArgs &A, int blocks, double *d0, double *d1, cudaStream_t st)
 {
-    k_spec_mean<<<(unsigned)A.M, ROW_THREADS, 0, st>>>(A);
-    k_spec_sub_mean<<<(unsigned)A.M, ROW_THREADS, 0, st>>>(A);
-    return cudaGetLastError();
+    const cudaError_t e = cudaMemsetAsync(&A.s->bar_count, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    SpecArgs a = A;
+    void *args[] = {&a, &d0, &d1};
+    return cudaLaunchCooperativeKernel((const void *)k_spec_pcg, dim3((unsigned)blocks), dim3(SPEC_PT), args,
+                                       spec_pcg_smem(A.N, A.M), st);
 }
 
 }  // namespace pvof
