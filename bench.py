@@ -23,7 +23,9 @@ concurrently by pvof_run_steps_batched (the batched form: one host thread and
 stream per case, so the cluster-resident solvers of different cases run on
 different SMs) and adds a "batched" object to the line; --batch-form fp32
 (fp32-warm) runs the replicas in the FP32 stencil form (plus the pressure
-warm start) and reports their error against the FP64 path.  --forms adds a
+warm start), spectral / fp32-warm-spectral add the spectral pressure
+preconditioner, all adds the unregularised momentum CG too; every form but
+fp64 reports its error against the FP64 path.  --forms adds a
 "forms" list: the workload in each form of FORMS (FP32 stencils + pressure
 warm start; the spectral pressure preconditioner; with it the momentum CG
 without the reference's step regularisation; all of them), each with its
@@ -384,9 +386,10 @@ def run_ours(args):
     if args.batch_cases > 1:
         from pvof import abi
         bparams = abi.Params.from_buffer_copy(params)
-        bparams.stencil_fp32 = 1 if args.batch_form.startswith("fp32") else 0
-        bparams.pressure_warm_start = 1 if args.batch_form in ("fp32-warm", "fp32-warm-spectral") else 0
-        bparams.pressure_preconditioner = 1 if args.batch_form.endswith("spectral") else 0
+        bparams.stencil_fp32 = 1 if args.batch_form.startswith("fp32") or args.batch_form == "all" else 0
+        bparams.pressure_warm_start = 1 if args.batch_form in ("fp32-warm", "fp32-warm-spectral", "all") else 0
+        bparams.pressure_preconditioner = 1 if args.batch_form in ("spectral", "fp32-warm-spectral", "all") else 0
+        bparams.velocity_cg_unregularized = 1 if args.batch_form == "all" else 0
         reps = []
         for q in range(args.batch_cases):
             r = runtime.Solver(grid, bparams, device=local)
@@ -410,7 +413,9 @@ def run_ours(args):
                             "fp32-warm": "fp32-stencils + pressure warm start",
                             "spectral": "spectral pressure preconditioner",
                             "fp32-warm-spectral": "fp32-stencils + pressure warm start + spectral pressure "
-                                                  "preconditioner"}[args.batch_form]}
+                                                  "preconditioner",
+                            "all": "fp32-stencils + pressure warm start + spectral pressure preconditioner + "
+                                   "unregularised momentum CG"}[args.batch_form]}
         if args.batch_form != "fp64":
             import numpy as np
             # the error of the form: one replica against the FP64 path after the same steps
@@ -489,7 +494,7 @@ def main():
                     help="also time the workload with surface tension and three resolved cylinders")
     ap.add_argument("--forms", action="store_true",
                     help="also time the FP32-stencil + pressure warm-start form on the workload (error against FP64)")
-    ap.add_argument("--batch-form", default="fp64", choices=["fp64", "fp32", "fp32-warm", "spectral", "fp32-warm-spectral"],
+    ap.add_argument("--batch-form", default="fp64", choices=["fp64", "fp32", "fp32-warm", "spectral", "fp32-warm-spectral", "all"],
                     help="fp32: the batched replicas use the FP32 stencil form (error against FP64 reported)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
