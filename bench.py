@@ -18,15 +18,15 @@ HBM, the L2 flushed before every step (outside the timed intervals).  e2e:
 the same steps driven through the C ABI with the state uploaded from pinned
 host buffers before every step and downloaded after it.
 
---batch-cases K additionally times K replicas of the workload advanced
-concurrently by pvof_run_steps_batched (the batched form: one host thread and
-stream per case, so the cluster-resident solvers of different cases run on
-different SMs) and adds a "batched" object to the line; --batch-form fp32
-(fp32-warm) runs the replicas in the FP32 stencil form (plus the pressure
-warm start), spectral / fp32-warm-spectral add the spectral pressure
-preconditioner, all adds the unregularised momentum CG too; every form but
-fp64 reports its error against the FP64 path.  --forms adds a
-"forms" list: the workload in each form of FORMS (FP32 stencils + pressure
+--batch-cases K (default 6, 0 turns it off) additionally times K replicas of
+the workload advanced concurrently by pvof_run_steps_batched (the batched
+form: one host thread and stream per case, so the solvers of different cases
+run on different SMs) and adds a "batched" object to the line; --batch-form
+(default all) picks the replicas' form: fp32 (fp32-warm) the FP32 stencil
+form (plus the pressure warm start), spectral / fp32-warm-spectral add the
+spectral pressure preconditioner, all adds the unregularised momentum CG too;
+every form but fp64 reports its error against the FP64 path.  --forms (on by
+default, --no-forms turns it off) adds a "forms" list: the workload in each form of FORMS (FP32 stencils + pressure
 warm start; the spectral pressure preconditioner; with it the momentum CG
 without the reference's step regularisation; all of them), each with its
 throughput against the plain path's and its error.
@@ -269,6 +269,103 @@ def pinned_like(n):
     return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
 
 
+def time_forms(args, g, grid, params, planes, device, cells, value, timing):
+    """The workload in each form of FORMS, timed like the main line, with its
+    error against the plain path's state after the same steps (g)."""
+    from pvof import abi, runtime
+    import numpy as np
+    snap = {f: g.get(f) for f in ("U", "V", "P", "C_L")}
+    m64 = g.liquid_mass()
+    forms = []
+    for label, fp32, warm, precond, vel in FORMS:
+        fparams = abi.Params.from_buffer_copy(params)
+        fparams.stencil_fp32 = fp32
+        fparams.pressure_warm_start = warm
+        fparams.pressure_preconditioner = precond
+        fparams.velocity_cg_unregularized = vel
+        fg = runtime.Solver(grid, fparams, device=device)
+        fg.set_planes(planes)
+        fg.initialize()
+        for _ in range(args.warmup):
+            fg.run_steps(1, DT)
+        fg.set_solver_timing(True)
+        f_ms = 0.0
+        for _ in range(args.steps):
+            fg.flush_l2()
+            fg.timer_start()
+            fg.run_steps(1, DT)
+            f_ms += fg.timer_stop()
+        fp = fg.solver_timing(2)
+        err = {"velocity_rel_l2": max(float(np.linalg.norm(fg.get(f) - snap[f]) / np.linalg.norm(snap[f]))
+                                      for f in ("U", "V")),
+               "pressure_rel_l2": float(np.linalg.norm(fg.get("P") - snap["P"]) / np.linalg.norm(snap["P"])),
+               "volume_rel": abs(fg.liquid_mass() - m64) / abs(m64)}
+        fvalue = cells * args.steps / (f_ms * 1e-3)
+        forms.append({"form": label, "value": fvalue, "unit": UNIT, "ms_per_step": f_ms / args.steps,
+                      "vs_plain": fvalue / value, "pressure_iterations": fp["iterations"],
+                      "pressure_iterations_plain": timing[2]["iterations"],
+                      "pressure_ms_per_step": fp["ms"] / args.steps,
+                      "velocity_iterations": fg.solver_timing(1)["iterations"],
+                      "velocity_iterations_plain": timing[1]["iterations"],
+                      "error_vs_fp64": err})
+        fg.close()
+    return forms
+
+
+def time_batched(args, grid, params, planes, device, cells, total_ms):
+    """K replicas of the workload advanced concurrently in the chosen form."""
+    from pvof import runtime
+    from pvof import abi
+    bparams = abi.Params.from_buffer_copy(params)
+    bparams.stencil_fp32 = 1 if args.batch_form.startswith("fp32") or args.batch_form == "all" else 0
+    bparams.pressure_warm_start = 1 if args.batch_form in ("fp32-warm", "fp32-warm-spectral", "all") else 0
+    bparams.pressure_preconditioner = 1 if args.batch_form in ("spectral", "fp32-warm-spectral", "all") else 0
+    bparams.velocity_cg_unregularized = 1 if args.batch_form == "all" else 0
+    reps = []
+    for q in range(args.batch_cases):
+        r = runtime.Solver(grid, bparams, device=device)
+        r.set_planes(planes)
+        r.initialize()
+        reps.append(r)
+    runtime.run_steps_batched(reps, 1, DT)
+    bsteps = max(1, min(args.steps, args.batch_steps))
+    for r in reps:
+        r.flush_l2()
+    for r in reps:
+        r.timer_start()
+    runtime.run_steps_batched(reps, bsteps, DT)
+    span = max(r.timer_stop() for r in reps)
+    bvalue = args.batch_cases * cells * bsteps / (span * 1e-3)
+    batched = {"cases": args.batch_cases, "steps": bsteps, "value": bvalue, "unit": UNIT,
+               "ms_per_step": span / bsteps, "vs_single": bvalue / (cells * args.steps / (total_ms * 1e-3)),
+               "note": "replicas of the workload advanced concurrently by pvof_run_steps_batched "
+                       "(one host thread and stream per case); device time of the slowest case",
+               "form": {"fp64": "fp64", "fp32": "fp32-stencils",
+                        "fp32-warm": "fp32-stencils + pressure warm start",
+                        "spectral": "spectral pressure preconditioner",
+                        "fp32-warm-spectral": "fp32-stencils + pressure warm start + spectral pressure "
+                                              "preconditioner",
+                        "all": "fp32-stencils + pressure warm start + spectral pressure preconditioner + "
+                               "unregularised momentum CG"}[args.batch_form]}
+    if args.batch_form != "fp64":
+        import numpy as np
+        # the error of the form: one replica against the FP64 path after the same steps
+        ref = runtime.Solver(grid, params, device=device)
+        ref.set_planes(planes)
+        ref.initialize()
+        ref.run_steps(1 + bsteps, DT)
+        vel = max(float(np.linalg.norm(reps[0].get(f) - ref.get(f)) / np.linalg.norm(ref.get(f)))
+                  for f in ("U", "V"))
+        m64 = ref.liquid_mass()
+        batched["error_vs_fp64"] = {"velocity_rel_l2": vel,
+                                    "volume_rel": abs(reps[0].liquid_mass() - m64) / abs(m64)}
+        ref.close()
+    for r in reps:
+        r.close()
+
+    return batched
+
+
 def run_ours(args):
     ws, rank, local = dist_env()
     dist = init_dist(ws, local)
@@ -306,45 +403,13 @@ def run_ours(args):
     t_max = max_over_ranks(dist, total_ms)
     value = ws * cells * args.steps / (t_max * 1e-3)
 
-    # ---- the chosen forms on the same workload (optional) ---------------------
+    # ---- the chosen forms on the same workload (a failure here keeps the line) ----
     forms = None
     if args.forms:
-        import numpy as np
-        snap = {f: g.get(f) for f in ("U", "V", "P", "C_L")}
-        m64 = g.liquid_mass()
-        forms = []
-        for label, fp32, warm, precond, vel in FORMS:
-            fparams = abi.Params.from_buffer_copy(params)
-            fparams.stencil_fp32 = fp32
-            fparams.pressure_warm_start = warm
-            fparams.pressure_preconditioner = precond
-            fparams.velocity_cg_unregularized = vel
-            fg = runtime.Solver(grid, fparams, device=local)
-            fg.set_planes(planes)
-            fg.initialize()
-            for _ in range(args.warmup):
-                fg.run_steps(1, DT)
-            fg.set_solver_timing(True)
-            f_ms = 0.0
-            for _ in range(args.steps):
-                fg.flush_l2()
-                fg.timer_start()
-                fg.run_steps(1, DT)
-                f_ms += fg.timer_stop()
-            fp = fg.solver_timing(2)
-            err = {"velocity_rel_l2": max(float(np.linalg.norm(fg.get(f) - snap[f]) / np.linalg.norm(snap[f]))
-                                          for f in ("U", "V")),
-                   "pressure_rel_l2": float(np.linalg.norm(fg.get("P") - snap["P"]) / np.linalg.norm(snap["P"])),
-                   "volume_rel": abs(fg.liquid_mass() - m64) / abs(m64)}
-            fvalue = cells * args.steps / (f_ms * 1e-3)
-            forms.append({"form": label, "value": fvalue, "unit": UNIT, "ms_per_step": f_ms / args.steps,
-                          "vs_plain": fvalue / value, "pressure_iterations": fp["iterations"],
-                          "pressure_iterations_plain": timing[2]["iterations"],
-                          "pressure_ms_per_step": fp["ms"] / args.steps,
-                          "velocity_iterations": fg.solver_timing(1)["iterations"],
-                          "velocity_iterations_plain": timing[1]["iterations"],
-                          "error_vs_fp64": err})
-            fg.close()
+        try:
+            forms = time_forms(args, g, grid, params, planes, local, cells, value, timing)
+        except Exception as e:   # noqa: BLE001 -- reported in the line, the plain numbers stand
+            forms = {"error": "%s: %s" % (type(e).__name__, e)}
 
     # ---- end to end through the C ABI with host buffers ---------------------
     blocks = {f: pinned_like(g.block_count(f)) for f in STATE_FIELDS}
@@ -381,56 +446,13 @@ def run_ours(args):
     traffic = profile_traffic(names[dom])
     shares = {names[k]: round(timing[k]["ms"] / total_ms, 4) for k in timing}
 
-    # ---- batched form: K replicas advanced concurrently (optional) -----------
+    # ---- batched form: K replicas advanced concurrently (a failure keeps the line) ----
     batched = None
     if args.batch_cases > 1:
-        from pvof import abi
-        bparams = abi.Params.from_buffer_copy(params)
-        bparams.stencil_fp32 = 1 if args.batch_form.startswith("fp32") or args.batch_form == "all" else 0
-        bparams.pressure_warm_start = 1 if args.batch_form in ("fp32-warm", "fp32-warm-spectral", "all") else 0
-        bparams.pressure_preconditioner = 1 if args.batch_form in ("spectral", "fp32-warm-spectral", "all") else 0
-        bparams.velocity_cg_unregularized = 1 if args.batch_form == "all" else 0
-        reps = []
-        for q in range(args.batch_cases):
-            r = runtime.Solver(grid, bparams, device=local)
-            r.set_planes(planes)
-            r.initialize()
-            reps.append(r)
-        runtime.run_steps_batched(reps, 1, DT)
-        bsteps = max(1, min(args.steps, args.batch_steps))
-        for r in reps:
-            r.flush_l2()
-        for r in reps:
-            r.timer_start()
-        runtime.run_steps_batched(reps, bsteps, DT)
-        span = max(r.timer_stop() for r in reps)
-        bvalue = args.batch_cases * cells * bsteps / (span * 1e-3)
-        batched = {"cases": args.batch_cases, "steps": bsteps, "value": bvalue, "unit": UNIT,
-                   "ms_per_step": span / bsteps, "vs_single": bvalue / (cells * args.steps / (total_ms * 1e-3)),
-                   "note": "replicas of the workload advanced concurrently by pvof_run_steps_batched "
-                           "(one host thread and stream per case); device time of the slowest case",
-                   "form": {"fp64": "fp64", "fp32": "fp32-stencils",
-                            "fp32-warm": "fp32-stencils + pressure warm start",
-                            "spectral": "spectral pressure preconditioner",
-                            "fp32-warm-spectral": "fp32-stencils + pressure warm start + spectral pressure "
-                                                  "preconditioner",
-                            "all": "fp32-stencils + pressure warm start + spectral pressure preconditioner + "
-                                   "unregularised momentum CG"}[args.batch_form]}
-        if args.batch_form != "fp64":
-            import numpy as np
-            # the error of the form: one replica against the FP64 path after the same steps
-            ref = runtime.Solver(grid, params, device=local)
-            ref.set_planes(planes)
-            ref.initialize()
-            ref.run_steps(1 + bsteps, DT)
-            vel = max(float(np.linalg.norm(reps[0].get(f) - ref.get(f)) / np.linalg.norm(ref.get(f)))
-                      for f in ("U", "V"))
-            m64 = ref.liquid_mass()
-            batched["error_vs_fp64"] = {"velocity_rel_l2": vel,
-                                        "volume_rel": abs(reps[0].liquid_mass() - m64) / abs(m64)}
-            ref.close()
-        for r in reps:
-            r.close()
+        try:
+            batched = time_batched(args, grid, params, planes, local, cells, total_ms)
+        except Exception as e:   # noqa: BLE001
+            batched = {"error": "%s: %s" % (type(e).__name__, e)}
 
     particles = particle_case(args, local) if args.particles else None
 
@@ -487,14 +509,15 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=5)
     ap.add_argument("--ref-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch-cases", type=int, default=0,
-                    help="also time this many replicas advanced concurrently (batched form)")
+    ap.add_argument("--batch-cases", type=int, default=6,
+                    help="also time this many replicas advanced concurrently (batched form; 0: off)")
     ap.add_argument("--batch-steps", type=int, default=10)
     ap.add_argument("--particles", action="store_true",
                     help="also time the workload with surface tension and three resolved cylinders")
-    ap.add_argument("--forms", action="store_true",
-                    help="also time the FP32-stencil + pressure warm-start form on the workload (error against FP64)")
-    ap.add_argument("--batch-form", default="fp64", choices=["fp64", "fp32", "fp32-warm", "spectral", "fp32-warm-spectral", "all"],
+    ap.add_argument("--forms", action="store_true", default=True,
+                    help="also time each form of FORMS on the workload (error against FP64); on by default")
+    ap.add_argument("--no-forms", dest="forms", action="store_false")
+    ap.add_argument("--batch-form", default="all", choices=["fp64", "fp32", "fp32-warm", "spectral", "fp32-warm-spectral", "all"],
                     help="fp32: the batched replicas use the FP32 stencil form (error against FP64 reported)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
