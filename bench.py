@@ -14,9 +14,13 @@ not reach div < 1e-6 on this grid and aborts).
 
 One "step" = one time step (three RK substeps).  metric = N_cells x steps /
 seconds.  value: device time of the timed steps with the state resident in
-HBM, the L2 flushed before every step (outside the timed intervals).  e2e:
-the same steps driven through the C ABI with the state uploaded from pinned
-host buffers before every step and downloaded after it.
+HBM, the L2 flushed before every step (outside the timed intervals); the
+substeps replay their launches from CUDA graphs (pvof_set_graphs, on by
+default).  The per-solver times behind the roofline and the solver shares
+come from a following pass of --timing-steps steps issued launch by launch
+with CUDA events around every solver launch.  e2e: the same steps driven
+through the C ABI with the state uploaded from pinned host buffers before
+every step and downloaded after it.
 
 --batch-cases K (default 6, 0 turns it off) additionally times K replicas of
 the workload advanced concurrently by pvof_run_steps_batched (the batched
@@ -269,13 +273,29 @@ def pinned_like(n):
     return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
 
 
-def time_forms(args, g, grid, params, planes, device, cells, value, timing):
+def solver_timing_pass(g, nsteps):
+    """nsteps more steps with CUDA events around every solver launch: per
+    solver {ms, iterations, ...}, its kernel names, the steps' device time."""
+    g.set_solver_timing(True)
+    ms = 0.0
+    for _ in range(nsteps):
+        g.flush_l2()
+        g.timer_start()
+        g.run_steps(1, DT)
+        ms += g.timer_stop()
+    timing = {k: g.solver_timing(k) for k in (0, 1, 2)}
+    names = {k: g.solver_kernel(k) for k in (0, 1, 2)}
+    g.set_solver_timing(False)
+    return timing, names, ms
+
+
+def time_forms(args, snap, m64, grid, params, planes, device, cells, value, timing, tsteps):
     """The workload in each form of FORMS, timed like the main line, with its
-    error against the plain path's state after the same steps (g)."""
+    error against the plain path's state after the same steps (snap, m64);
+    solver iterations and pressure time from a following per-solver timing
+    pass of tsteps steps, like the plain path's (timing)."""
     from pvof import abi, runtime
     import numpy as np
-    snap = {f: g.get(f) for f in ("U", "V", "P", "C_L")}
-    m64 = g.liquid_mass()
     forms = []
     for label, fp32, warm, precond, vel in FORMS:
         fparams = abi.Params.from_buffer_copy(params)
@@ -288,24 +308,25 @@ def time_forms(args, g, grid, params, planes, device, cells, value, timing):
         fg.initialize()
         for _ in range(args.warmup):
             fg.run_steps(1, DT)
-        fg.set_solver_timing(True)
         f_ms = 0.0
         for _ in range(args.steps):
             fg.flush_l2()
             fg.timer_start()
             fg.run_steps(1, DT)
             f_ms += fg.timer_stop()
-        fp = fg.solver_timing(2)
         err = {"velocity_rel_l2": max(float(np.linalg.norm(fg.get(f) - snap[f]) / np.linalg.norm(snap[f]))
                                       for f in ("U", "V")),
                "pressure_rel_l2": float(np.linalg.norm(fg.get("P") - snap["P"]) / np.linalg.norm(snap["P"])),
                "volume_rel": abs(fg.liquid_mass() - m64) / abs(m64)}
         fvalue = cells * args.steps / (f_ms * 1e-3)
+        ft, _, _ = solver_timing_pass(fg, tsteps)
         forms.append({"form": label, "value": fvalue, "unit": UNIT, "ms_per_step": f_ms / args.steps,
-                      "vs_plain": fvalue / value, "pressure_iterations": fp["iterations"],
+                      "vs_plain": fvalue / value,
+                      "solver_timing_steps": tsteps,
+                      "pressure_iterations": ft[2]["iterations"],
                       "pressure_iterations_plain": timing[2]["iterations"],
-                      "pressure_ms_per_step": fp["ms"] / args.steps,
-                      "velocity_iterations": fg.solver_timing(1)["iterations"],
+                      "pressure_ms_per_step": ft[2]["ms"] / tsteps,
+                      "velocity_iterations": ft[1]["iterations"],
                       "velocity_iterations_plain": timing[1]["iterations"],
                       "error_vs_fp64": err})
         fg.close()
@@ -380,9 +401,8 @@ def run_ours(args):
         g.run_steps(1, DT)
     g.synchronize()
 
-    # ---- device-resident timing ------------------------------------------
+    # ---- device-resident timing (substeps replayed from CUDA graphs) --------
     clocks = Clocks(local)
-    g.set_solver_timing(True)
     barrier(dist)
     l0 = g.launch_count()
     clocks.start()
@@ -397,19 +417,11 @@ def run_ours(args):
     clk = clocks.stop()
     barrier(dist)
     launches = g.launch_count() - l0
-    timing = {k: g.solver_timing(k) for k in (0, 1, 2)}
-    names = {k: g.solver_kernel(k) for k in (0, 1, 2)}
-    g.set_solver_timing(False)
+    graph_steps = g.graph_replays()
     t_max = max_over_ranks(dist, total_ms)
     value = ws * cells * args.steps / (t_max * 1e-3)
-
-    # ---- the chosen forms on the same workload (a failure here keeps the line) ----
-    forms = None
-    if args.forms:
-        try:
-            forms = time_forms(args, g, grid, params, planes, local, cells, value, timing)
-        except Exception as e:   # noqa: BLE001 -- reported in the line, the plain numbers stand
-            forms = {"error": "%s: %s" % (type(e).__name__, e)}
+    snap = {f: g.get(f) for f in ("U", "V", "P", "C_L")}   # the forms' reference state
+    m64 = g.liquid_mass()
 
     # ---- end to end through the C ABI with host buffers ---------------------
     blocks = {f: pinned_like(g.block_count(f)) for f in STATE_FIELDS}
@@ -438,13 +450,26 @@ def run_ours(args):
     e2e_max = max_over_ranks(dist, e2e_ms)
     e2e_value = ws * cells * e2e_steps / (e2e_max * 1e-3)
 
+    # ---- per-solver timing: the next steps launch by launch, CUDA events
+    # around every solver launch (for the roofline and the solver shares) ----
+    tsteps = max(1, min(args.steps, args.timing_steps))
+    timing, names, ts_ms = solver_timing_pass(g, tsteps)
+
+    # ---- the chosen forms on the same workload (a failure here keeps the line) ----
+    forms = None
+    if args.forms:
+        try:
+            forms = time_forms(args, snap, m64, grid, params, planes, local, cells, value, timing, tsteps)
+        except Exception as e:   # noqa: BLE001 -- reported in the line, the plain numbers stand
+            forms = {"error": "%s: %s" % (type(e).__name__, e)}
+
     # ---- roofline of the dominant kernel ----------------------------------
     dom = max(timing, key=lambda k: timing[k]["ms"])
     t = timing[dom]
     peak, peak_kind = measured_peak()
     achieved = ALG_BYTES[dom] * t["cell_iters"] / (t["ms"] * 1e-3) / 1e9 if t["ms"] > 0 else 0.0
     traffic = profile_traffic(names[dom])
-    shares = {names[k]: round(timing[k]["ms"] / total_ms, 4) for k in timing}
+    shares = {names[k]: round(timing[k]["ms"] / ts_ms, 4) for k in timing}
 
     # ---- batched form: K replicas advanced concurrently (a failure keeps the line) ----
     batched = None
@@ -473,7 +498,10 @@ def run_ours(args):
                        "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "flushed before every timed step (memset of 2x L2, outside the timed intervals)",
                        "solver_iterations": {names[k]: timing[k]["iterations"] for k in timing},
-                       "solver_time_share": shares},
+                       "solver_time_share": shares,
+                       "solver_timing_steps": tsteps,
+                       "graphs": "substeps replayed from CUDA graphs in the timed steps: %d of %d"
+                                 % (graph_steps, 3 * (args.warmup + args.steps))},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps},
             "gpu_launches": launches,
@@ -512,6 +540,8 @@ def main():
     ap.add_argument("--batch-cases", type=int, default=6,
                     help="also time this many replicas advanced concurrently (batched form; 0: off)")
     ap.add_argument("--batch-steps", type=int, default=10)
+    ap.add_argument("--timing-steps", type=int, default=20,
+                    help="steps of the per-solver timing pass after the timed steps")
     ap.add_argument("--particles", action="store_true",
                     help="also time the workload with surface tension and three resolved cylinders")
     ap.add_argument("--forms", action="store_true", default=True,

@@ -384,6 +384,17 @@ int pvof_flush_l2(pvof_ctx *ctx);
 #define PVOF_SOLVER_VELOCITY 1
 #define PVOF_SOLVER_PRESSURE 2
 int pvof_set_solver_timing(pvof_ctx *ctx, int enabled);
+
+/* No counterpart in the reference: 1 (the default) replays the launches of
+ * pvof_substep up to its first Poisson pass's divergence check from a CUDA
+ * graph captured per (stage, dt, buffer parity, warm-start state); 0 issues
+ * them one by one.  Results are identical.  Cases with resolved particles,
+ * the learned warm start, and any substep run while solver timing is on
+ * issue them one by one. */
+int pvof_set_graphs(pvof_ctx *ctx, int enabled);
+/* No counterpart in the reference: how many substeps so far replayed their
+ * launches from a graph (-1 for a null context). */
+long long pvof_graph_replays(const pvof_ctx *ctx);
 int pvof_solver_timing(const pvof_ctx *ctx, int solver, double *ms, long long *launches, long long *iterations,
                        long long *cell_iters);
 /* Name of the kernel that runs solver PVOF_SOLVER_* for this context: the

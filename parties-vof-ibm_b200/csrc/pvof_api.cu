@@ -880,9 +880,12 @@ int initialize(pvof_ctx *c)
     return PVOF_OK;
 }
 
-// Temporal_int_all_the_equations (Temporal_int.c:563-1279); with resolved
-// particles the branches of VOF_IBM and LAG_PARTICLE_RESOLVED
-int substep(pvof_ctx *c, pvof_stats *st)
+int poisson_pass(pvof_ctx *c, bool warm);
+
+// Temporal_int_all_the_equations (Temporal_int.c:563-1279) up to the first
+// Poisson pass's divergence check; with resolved particles the branches of
+// VOF_IBM and LAG_PARTICLE_RESOLVED
+int substep_region(pvof_ctx *c, bool warm0)
 {
     const bool solids = resolved(c);
     if (c->stage > 0) TRY(cell_center(c));
@@ -922,16 +925,99 @@ int substep(pvof_ctx *c, pvof_stats *st)
         TRY(fill(c, BK_U, F(c, PVOF_F_U)));
         TRY(fill(c, BK_V, F(c, PVOF_F_V)));
     }
+    return poisson_pass(c, warm0);
+}
+
+// one pass of the outer Poisson loop up to its divergence check (read by the host)
+int poisson_pass(pvof_ctx *c, bool warm)
+{
+    TRY(p_set_rhs(c, warm));
+    TRY(p_precond(c));
+    TRY(p_solve(c));
+    TRY(p_project(c));
+    TRY(fill(c, BK_U, F(c, PVOF_F_U)));
+    TRY(fill(c, BK_V, F(c, PVOF_F_V)));
+    return p_divergence_async(c);
+}
+
+// The region above as a CUDA graph.  Its launches and their arguments depend
+// on the host state in GraphKey only (without resolved particles, whose list
+// bookkeeping reads the device, without the learned warm start, and without
+// solver timing, whose events must be recorded launch by launch); a key is
+// captured the second time it is seen, so lazy set-up (allocations, tables)
+// has run outside the capture, and replayed after that.  A key whose capture
+// fails runs its launches directly from then on.
+bool graph_key_equal(const GraphKey &a, const GraphKey &b)
+{
+    return a.stage == b.stage && a.dt == b.dt && a.fsig == b.fsig && a.warm == b.warm &&
+           a.one_cluster == b.one_cluster;
+}
+
+int run_region(pvof_ctx *c, bool warm0)
+{
+    if (!c->use_graphs || c->solver_timing || resolved(c) || c->p.pressure_warm_start == 2)
+        return substep_region(c, warm0);
+    GraphKey k;
+    k.stage = c->stage;
+    k.dt = c->dt;
+    k.fsig = c->f[PVOF_F_FSIG_OLD_X];
+    k.warm = warm0 ? 1 : 0;
+    k.one_cluster = c->vel_one_cluster;
+    GraphEntry *e = nullptr;
+    for (GraphEntry &g : c->graphs)
+        if (g.state != 0 && graph_key_equal(g.key, k)) { e = &g; break; }
+    if (!e) {   // first sight: remember the key, run directly
+        GraphEntry &g = c->graphs[c->graph_next];
+        c->graph_next = (c->graph_next + 1) % Ctx::NGRAPHS;
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = GraphEntry();
+        g.key = k;
+        g.state = 1;
+        return substep_region(c, warm0);
+    }
+    if (e->state == 3) return substep_region(c, warm0);
+    if (e->state == 1) {   // second sight: capture
+        const long long l0 = c->launches;
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            e->state = 3;
+            return substep_region(c, warm0);
+        }
+        const int rc = substep_region(c, warm0);
+        cudaGraph_t g = nullptr;
+        cudaError_t ee = cudaStreamEndCapture(c->stream, &g);
+        cudaGraphExec_t x = nullptr;
+        if (rc == PVOF_OK && ee == cudaSuccess && g) ee = cudaGraphInstantiate(&x, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (rc != PVOF_OK || ee != cudaSuccess || !x) {
+            if (x) cudaGraphExecDestroy(x);
+            cudaGetLastError();
+            e->state = 3;
+            c->launches = l0;
+            return substep_region(c, warm0);
+        }
+        e->exec = x;
+        e->state = 2;
+        e->launches = c->launches - l0;
+        c->launches = l0;
+    }
+    CK(cudaGraphLaunch(e->exec, c->stream));
+    c->graph_replays++;
+    c->launches += e->launches;
+    return PVOF_OK;
+}
+
+// Temporal_int_all_the_equations (Temporal_int.c:563-1279); with resolved
+// particles the branches of VOF_IBM and LAG_PARTICLE_RESOLVED
+int substep(pvof_ctx *c, pvof_stats *st)
+{
+    const bool solids = resolved(c);
+    const bool warm0 = c->p.pressure_warm_start && (c->phi_prev_mask >> c->stage & 1);
+    TRY(run_region(c, warm0));
     int passes = 0, p_total = 0;
     int rc = PVOF_OK;
     for (;;) {
-        TRY(p_set_rhs(c, passes == 0 && c->p.pressure_warm_start && (c->phi_prev_mask >> c->stage & 1)));
-        TRY(p_precond(c));
-        TRY(p_solve(c));
-        TRY(p_project(c));
-        TRY(fill(c, BK_U, F(c, PVOF_F_U)));
-        TRY(fill(c, BK_V, F(c, PVOF_F_V)));
-        TRY(p_divergence_async(c));
+        if (passes > 0) TRY(poisson_pass(c, false));
         TRY(read_scalars(c));
         passes++;
         p_total += c->scal_host->p_iters;
@@ -1593,6 +1679,7 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
 
     pvof_ctx *c = new pvof_ctx();
     std::memset(static_cast<Ctx *>(c), 0, sizeof(Ctx));
+    c->use_graphs = 1;
     c->g = *grid;
     c->p = *params;
     c->device = device;
@@ -1743,6 +1830,8 @@ int pvof_destroy(pvof_ctx *c)
     for (int q = 0; q < Ctx::NPEND; q++)
         for (int e = 0; e < 2; e++) if (c->pend_ev[q][e]) cudaEventDestroy(c->pend_ev[q][e]);
     delete c->ibm;
+    for (GraphEntry &g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     if (c->fft_coef) cudaFree(c->fft_coef);
     if (c->spec_mem) cudaFree(c->spec_mem);
     if (c->spec_s) cudaFree(c->spec_s);
@@ -2005,6 +2094,15 @@ int pvof_flush_l2(pvof_ctx *c)
     CK(cudaMemsetAsync(c->flush_buf, (int)(c->launches & 0xff), c->flush_bytes, c->stream));
     return PVOF_OK;
 }
+
+int pvof_set_graphs(pvof_ctx *c, int enabled)
+{
+    ENTER(c);
+    c->use_graphs = enabled ? 1 : 0;
+    return PVOF_OK;
+}
+
+long long pvof_graph_replays(const pvof_ctx *c) { return c ? c->graph_replays : -1; }
 
 int pvof_set_solver_timing(pvof_ctx *c, int enabled)
 {

@@ -108,6 +108,22 @@ struct DevScalars {
 
 struct IbmState;
 
+// host state that the launches of a substep (up to its first Poisson pass)
+// depend on, the key of its captured CUDA graph
+struct GraphKey {
+    int stage;
+    double dt;
+    const double *fsig;   // the f_sigma buffers swap every substep
+    int warm, one_cluster;
+};
+
+struct GraphEntry {
+    GraphKey key;
+    int state;   // 0 empty, 1 seen once, 2 captured, 3 runs directly
+    cudaGraphExec_t exec;
+    long long launches;   // kernels in the graph
+};
+
 struct Ctx {
     pvof_grid_desc g;
     pvof_params p;
@@ -163,6 +179,11 @@ struct Ctx {
     int spec_rounds;         // its cyclic-reduction rounds
     double sol_ms[3];
     long long sol_launches[3], sol_iters[3], sol_cell_iters[3];
+    int use_graphs;          // replay each substep's launches from a captured CUDA graph
+    static constexpr int NGRAPHS = 12;
+    GraphEntry graphs[NGRAPHS];
+    int graph_next;
+    long long graph_replays; // substeps whose launches came from a graph
 };
 
 }  // namespace pvof

@@ -64,6 +64,9 @@ def load():
     L.pvof_timer_stop.argtypes = [V, P(C.c_double)]
     L.pvof_flush_l2.argtypes = [V]
     L.pvof_set_solver_timing.argtypes = [V, C.c_int]
+    L.pvof_set_graphs.argtypes = [V, C.c_int]
+    L.pvof_graph_replays.argtypes = [V]
+    L.pvof_graph_replays.restype = C.c_longlong
     L.pvof_solver_timing.argtypes = [V, C.c_int, P(C.c_double), P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]
     L.pvof_solver_kernel.argtypes = [V, C.c_int]
     L.pvof_set_particles.argtypes = [V, P(abi.Particle), C.c_int]
@@ -252,6 +255,13 @@ class Solver:
 
     def set_solver_timing(self, on):
         check(load().pvof_set_solver_timing(self.h, 1 if on else 0), "pvof_set_solver_timing")
+
+    def set_graphs(self, on):
+        """Replay each substep's launches from captured CUDA graphs (default on)."""
+        check(load().pvof_set_graphs(self.h, 1 if on else 0), "pvof_set_graphs")
+
+    def graph_replays(self):
+        return load().pvof_graph_replays(self.h)
 
     def solver_kernel(self, solver):
         """Name of the kernel that runs solver abi.SOLVER_* in this context."""
