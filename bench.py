@@ -40,6 +40,10 @@ throughput against the plain path's and its error.
 interface (two mobile, one fixed), timed against the same case without
 cylinders (run last, so a launch list of the command ends with its steps).
 
+--large adds a "large" object: the instability on 1024x1024 at a density
+ratio of 1e-3 (--large-steps timed steps) in the plain path, with the
+spectral pressure preconditioner, and with it the unregularised momentum CG.
+
 --impl reference runs the reference's own time step (compiled from its
 sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host:
 --warmup untimed steps, then min(--steps, --ref-steps) timed ones.
@@ -268,6 +272,40 @@ def particle_case(args, device):
             "without_cylinders": out["without"]}
 
 
+def large_case(args, device):
+    """The planar instability on 1024 x 1024 with a density ratio of 1e-3
+    (Atwood 0.998, Cn 0.005, dt 2e-5): one untimed step, then --large-steps
+    timed steps (device time, L2 flushed) in the plain path, with the spectral
+    pressure preconditioner, and with it the unregularised momentum CG."""
+    from pvof import cases, runtime
+    ratio = 1e-3
+    nsteps = max(1, args.large_steps)
+    out = {"case": "planar instability 1024x1024, density ratio 1e-3 (Atwood 0.998), Cn 0.005, dt 2e-5",
+           "steps": nsteps, "unit": UNIT}
+    for label, precond, vel in (("plain", 0, 0), ("spectral", 1, 0), ("spectral + unregularised momentum", 1, 1)):
+        grid, params, planes = cases.rayleigh_taylor(1024, 1024, Lx=1.0, Ly=1.0, Cn=0.005,
+                                                     atwood=(1 - ratio) / (1 + ratio), P_CG_MAXIT=40000)
+        params.pressure_preconditioner = precond
+        params.velocity_cg_unregularized = vel
+        s = runtime.Solver(grid, params, device=device)
+        s.set_planes(planes)
+        s.initialize()
+        s.run_steps(1, 2e-5)
+        ms = 0.0
+        for _ in range(nsteps):
+            s.flush_l2()
+            s.timer_start()
+            s.run_steps(1, 2e-5)
+            ms += s.timer_stop()
+        t, _, _ = solver_timing_pass(s, 1)
+        out[label] = {"value": 1024 * 1024 / (ms / nsteps * 1e-3), "ms_per_step": ms / nsteps,
+                      "pressure_iterations_per_step": t[2]["iterations"],
+                      "velocity_iterations_per_step": t[1]["iterations"]}
+        s.close()
+    out["spectral_vs_plain"] = out["spectral + unregularised momentum"]["value"] / out["plain"]["value"]
+    return out
+
+
 def pinned_like(n):
     import torch
     return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
@@ -480,6 +518,12 @@ def run_ours(args):
             batched = {"error": "%s: %s" % (type(e).__name__, e)}
 
     particles = particle_case(args, local) if args.particles else None
+    large = None
+    if args.large:
+        try:
+            large = large_case(args, local)
+        except Exception as e:   # noqa: BLE001
+            large = {"error": "%s: %s" % (type(e).__name__, e)}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -520,6 +564,8 @@ def run_ours(args):
             line["forms"] = forms
         if particles is not None:
             line["particles"] = particles
+        if large is not None:
+            line["large"] = large
         print(json.dumps(line))
     g.close()
     if dist is not None:
@@ -542,6 +588,9 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=10)
     ap.add_argument("--timing-steps", type=int, default=20,
                     help="steps of the per-solver timing pass after the timed steps")
+    ap.add_argument("--large", action="store_true",
+                    help="also time 1024x1024 at density ratio 1e-3 (plain, spectral, spectral + momentum form)")
+    ap.add_argument("--large-steps", type=int, default=3)
     ap.add_argument("--particles", action="store_true",
                     help="also time the workload with surface tension and three resolved cylinders")
     ap.add_argument("--forms", action="store_true", default=True,

@@ -115,8 +115,9 @@ typedef struct pvof_params {
     int pressure_warm_start;
     /* no counterpart in the reference: 1 preconditions the pressure PCG with
      * the inverse of the constant-density Laplacian (an FFT along the periodic
-     * x rows and a tridiagonal solve per wavenumber along y) instead of the
-     * Jacobi diagonal; the solve still stops when sqrt(r^T D^-1 r), D the
+     * x rows and a tridiagonal solve per wavenumber along y), scaled on both
+     * sides by the square root of the Jacobi weights, instead of the Jacobi
+     * diagonal; the solve still stops when sqrt(r^T D^-1 r), D the
      * Jacobi diagonal, is below P_CG_ETOL, so the result moves within that
      * tolerance.  Planar grids with x periodic, walls in y, a power-of-two x
      * cell count up to 1024 and at most 1024 y cells; 0 is the reference's

@@ -780,7 +780,7 @@ int p_solve_spectral(pvof_ctx *c)
 
 int p_solve(pvof_ctx *c)
 {
-    if (c->p.pressure_preconditioner == 1) return p_solve_spectral(c);
+    if (c->p.pressure_preconditioner != 0) return p_solve_spectral(c);
     PresArgs A;
     A.d = c->dom;
     A.mp = c->maps[BK_PRESSURE];
@@ -1664,7 +1664,7 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
         return set_err(PVOF_EINVAL, "velocity_cg_unregularized must be 0 or 1");
     if (params->pressure_preconditioner < 0 || params->pressure_preconditioner > 1)
         return set_err(PVOF_EINVAL, "pressure_preconditioner must be 0 (Jacobi) or 1 (spectral)");
-    if (params->pressure_preconditioner == 1) {
+    if (params->pressure_preconditioner != 0) {
         const int N = grid->NXM, M = grid->NYM;
         if (grid->geometry != PVOF_GEOM_PLANAR || !grid->periodic[0] || grid->periodic[1])
             return set_err(PVOF_EINVAL, "the spectral pressure preconditioner needs a planar grid, x periodic, walls in y");
