@@ -19,7 +19,8 @@
 //        -z_{j-1} + (b_j + dy^2 lambda_x(m)) z_j - z_{j+1} = rhs_j,
 //      b_j = 2 inside, 1 at the two walls.  The matrices do not change, so
 //      the rounds' multipliers and the final reciprocal diagonals are
-//      computed once per context on the host (spec_tables) and a round is
+//      computed once per context on the host (spec_tables, one set per wave
+//      number: the half-complex indices m and N - m share it) and a round is
 //      two multiply-adds.  The mean mode's system is singular (the constant,
 //      the operator's null space): its first row is pinned, the right-hand
 //      side and the result are made mean-free, and the right-hand side's mean
@@ -130,6 +131,22 @@ __device__ double slot_total(const double *slot, double *sh)
 
 // complex FFT of a[0..N), N = 2^logN, by the 128 threads of one row group
 // (lt = 0..127); sign -1 forward.  All groups of the block run it in lockstep.
+// Radix-2 decimation in time after a bit reversal; two successive stages are
+// done per pass through shared memory (each thread keeps the four values of
+// both stages' butterflies in registers, the arithmetic is that of the two
+// radix-2 stages), a last odd stage on its own.
+__device__ __forceinline__ double2 cmul(double2 v, double2 w)
+{
+    return make_double2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
+}
+
+__device__ __forceinline__ double2 twid(const double2 *__restrict__ tw, int k, double sign)
+{
+    double2 w = tw[k];
+    w.y *= -sign;   // the table holds exp(-2 pi i k / N); the inverse takes its conjugate
+    return w;
+}
+
 __device__ void fft_group(double2 *a, int N, int logN, const double2 *__restrict__ tw, double sign, int lt)
 {
     for (int t = lt; t < N; t += ROW_THREADS) {
@@ -137,14 +154,32 @@ __device__ void fft_group(double2 *a, int N, int logN, const double2 *__restrict
         if (r > t) { const double2 x = a[t]; a[t] = a[r]; a[r] = x; }
     }
     __syncthreads();
-    for (int s = 0; s < logN; s++) {
+    int s = 0;
+    for (; s + 1 < logN; s += 2) {   // stages s and s + 1
+        const int h = 1 << s;
+        for (int t = lt; t < N / 4; t += ROW_THREADS) {
+            const int pos = t & (h - 1), i0 = ((t >> s) << (s + 2)) + pos, i1 = i0 + h, i2 = i1 + h, i3 = i2 + h;
+            const double2 w1 = twid(tw, pos * (N >> (s + 1)), sign);
+            const double2 w2 = twid(tw, pos * (N >> (s + 2)), sign), w3 = twid(tw, (pos + h) * (N >> (s + 2)), sign);
+            const double2 x0 = a[i0], x1 = a[i1], x2 = a[i2], x3 = a[i3];
+            double2 x = cmul(x1, w1);
+            const double2 y0 = make_double2(x0.x + x.x, x0.y + x.y), y1 = make_double2(x0.x - x.x, x0.y - x.y);
+            x = cmul(x3, w1);
+            const double2 y2 = make_double2(x2.x + x.x, x2.y + x.y), y3 = make_double2(x2.x - x.x, x2.y - x.y);
+            x = cmul(y2, w2);
+            a[i0] = make_double2(y0.x + x.x, y0.y + x.y);
+            a[i2] = make_double2(y0.x - x.x, y0.y - x.y);
+            x = cmul(y3, w3);
+            a[i1] = make_double2(y1.x + x.x, y1.y + x.y);
+            a[i3] = make_double2(y1.x - x.x, y1.y - x.y);
+        }
+        __syncthreads();
+    }
+    if (s < logN) {   // the last stage when log2 N is odd
         const int half = 1 << s, step = N >> (s + 1);
         for (int t = lt; t < N / 2; t += ROW_THREADS) {
             const int pos = t & (half - 1), i0 = ((t >> s) << (s + 1)) + pos, i1 = i0 + half;
-            double2 w = tw[pos * step];
-            w.y *= -sign;   // the table holds exp(-2 pi i k / N); the inverse takes its conjugate
-            const double2 u = a[i0], v = a[i1];
-            const double2 x = make_double2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
+            const double2 u = a[i0], x = cmul(a[i1], twid(tw, pos * step, sign));
             a[i0] = make_double2(u.x + x.x, u.y + x.y);
             a[i1] = make_double2(u.x - x.x, u.y - x.y);
         }
@@ -180,25 +215,36 @@ __device__ double system0_mean(double v, bool sys0, int M, double *sh)
     return r;
 }
 
+// half-complex index of the q-th system: 0, N/2, then 1, N-1, 2, N-2, ...,
+// so the two indices of one wave number (same matrix, same table rows) are
+// solved side by side
+__device__ __forceinline__ int system_index(int q, int N)
+{
+    if (q < 2) return q == 0 ? 0 : N / 2;
+    return (q & 1) ? N - (q >> 1) : (q >> 1);
+}
+
 // the tridiagonal solves of every half-complex index, hat in place
 __device__ void tridiag_phase(const SpecArgs &A, double *smem, double *sh)
 {
     const int P = A.d.P, N = A.N, M = A.M, Mp = (M + 31) / 32 * 32, S = SPEC_PT / Mp;
     const int sys = threadIdx.x / Mp, j = threadIdx.x - sys * Mp;
-    const size_t NM = (size_t)N * M;
+    const size_t NM = (size_t)(N / 2 + 1) * M;   // table rows per round: one per wave number
     double *sd = smem + (size_t)sys * Mp;
     for (int m0 = blockIdx.x * S; m0 < N; m0 += gridDim.x * S) {
-        const int m = m0 + sys;
-        const bool row = sys < S && m < N && j < M;
+        const int q = m0 + sys;
+        const int m = q < N ? system_index(q, N) : 0;
+        const int wave = m <= N / 2 ? m : N - m;
+        const bool row = sys < S && q < N && j < M;
         double r = row ? AT_(A.hat, m, j) : 0.0;
         double rmean = 0.0;
         if (m0 == 0) {   // this block holds the mean mode as its system 0
             rmean = system0_mean(r, sys == 0, M, sh);
-            if (m == 0) r = j == 0 ? 0.0 : r - rmean;   // mean-free, first row pinned
+            if (q == 0) r = j == 0 ? 0.0 : r - rmean;   // mean-free, first row pinned
         }
         // this thread's multipliers, all loads in flight at once: round st
         // k1 at [2 st NM], k2 at [(2 st + 1) NM], then 1 / b at [2 rounds NM]
-        const double *k = A.pcr + (size_t)m * M + j;
+        const double *k = A.pcr + (size_t)wave * M + j;
         double kr[2 * SPEC_MAXROUNDS + 1];
 #pragma unroll
         for (int q = 0; q < 2 * SPEC_MAXROUNDS + 1; q++) kr[q] = (row && q <= 2 * A.rounds) ? k[(size_t)q * NM] : 0.0;
@@ -227,7 +273,7 @@ __device__ void tridiag_phase(const SpecArgs &A, double *smem, double *sh)
             // the right-hand side's mean, so the scaled preconditioner stays
             // positive definite
             const double mean = system0_mean(x, sys == 0, M, sh);
-            if (m == 0) x = x - mean + rmean;
+            if (q == 0) x = x - mean + rmean;
         }
         if (row) AT_(A.hat, m, j) = x;
     }
@@ -406,12 +452,11 @@ int spec_tables(int N, int M, double idx2, double idy2, std::vector<double> &tw,
     }
     int nsteps = 0;
     for (int s = 1; s < M; s <<= 1) nsteps++;
-    const size_t NM = (size_t)N * M;
+    const size_t NM = (size_t)(N / 2 + 1) * M;   // one matrix per wave number 0 .. N/2
     pcr.assign((size_t)(2 * nsteps + 1) * NM, 0.0);
     std::vector<double> a(M), b(M), c(M), a2(M), b2(M), c2(M);
-    for (int m = 0; m < N; m++) {
-        const int wave = m <= N / 2 ? m : N - m;
-        const double lam = (2.0 - 2.0 * std::cos(2.0 * M_PI * wave / N)) * idx2 / idy2;
+    for (int m = 0; m <= N / 2; m++) {   // m: the wave number
+        const double lam = (2.0 - 2.0 * std::cos(2.0 * M_PI * m / N)) * idx2 / idy2;
         for (int j = 0; j < M; j++) {
             if (m == 0 && j == 0) { a[j] = 0.0; b[j] = 1.0; c[j] = 0.0; continue; }   // the pinned row
             a[j] = j > 0 ? -1.0 : 0.0;
