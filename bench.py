@@ -241,10 +241,13 @@ def particle_case(args, device):
     cylinders' kernel launches per step."""
     from pvof import cases, runtime
     out = {}
-    for label, parts in (("without", None), ("with", CYLINDERS)):
+    for label, parts, forms in (("without", None, 0), ("with", CYLINDERS, 0), ("with, all forms", CYLINDERS, 1)):
         grid, params, planes = cases.rayleigh_taylor(NXM, NYM, Lx=1.0, Ly=4.0, Cn=0.01, P_CG_MAXIT=2000,
                                                      surface_tension=True, We=100.0)
         params.contact_angle_deg = 70.0
+        if forms:
+            params.stencil_fp32 = params.pressure_warm_start = 1
+            params.pressure_preconditioner = params.velocity_cg_unregularized = 1
         s = runtime.Solver(grid, params, device=device)
         if parts:
             s.set_particles(parts)
@@ -269,7 +272,7 @@ def particle_case(args, device):
             "value": NXM * NYM / (w["ms_per_step"] * 1e-3), "unit": UNIT, "steps": args.steps,
             "ms_per_step": w["ms_per_step"], "launches_per_step": w["launches_per_step"],
             "pressure_iterations": w["pressure_iterations"], "pressure_ms_per_step": w["pressure_ms_per_step"],
-            "without_cylinders": out["without"]}
+            "without_cylinders": out["without"], "with_all_forms": out["with, all forms"]}
 
 
 def large_case(args, device):
