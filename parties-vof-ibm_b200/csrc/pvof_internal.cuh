@@ -180,7 +180,7 @@ struct Ctx {
     double sol_ms[3];
     long long sol_launches[3], sol_iters[3], sol_cell_iters[3];
     int use_graphs;          // replay each substep's launches from a captured CUDA graph
-    static constexpr int NGRAPHS = 12;
+    static constexpr int NGRAPHS = 24;   // 3 stages x 2 buffer parities x warm start x one or two clusters
     GraphEntry graphs[NGRAPHS];
     int graph_next;
     long long graph_replays; // substeps whose launches came from a graph
