@@ -40,6 +40,11 @@ throughput against the plain path's and its error.
 interface (two mobile, one fixed), timed against the same case without
 cylinders (run last, so a launch list of the command ends with its steps).
 
+--batch-mixed adds a "batched_mixed" object: eight instability cases of four
+sizes (two each of 64x128, 128x256, 256x512, 512x1024) in all four forms,
+advanced concurrently by pvof_run_steps_batched, against the same cases
+advanced one after another.
+
 --large adds a "large" object: the instability on 1024x1024 at a density
 ratio of 1e-3 (--large-steps timed steps) in the plain path, with the
 spectral pressure preconditioner, and with it the unregularised momentum CG.
@@ -309,6 +314,53 @@ def large_case(args, device):
     return out
 
 
+# uneven batch: the planar instability at four sizes, two cases each
+MIXED_SIZES = [(64, 128), (64, 128), (128, 256), (128, 256), (256, 512), (256, 512), (512, 1024), (512, 1024)]
+
+
+def mixed_batch(args, device):
+    """Cases of uneven size (MIXED_SIZES, domain 1 x 2, Cn 2 / NXM) in all
+    four forms, advanced concurrently by pvof_run_steps_batched, against the
+    same cases advanced one after another; device time, L2 flushed first."""
+    from pvof import cases, runtime
+    nsteps = max(1, min(args.steps, args.batch_steps))
+
+    def make():
+        out = []
+        for nx, ny in MIXED_SIZES:
+            grid, params, planes = cases.rayleigh_taylor(nx, ny, Lx=1.0, Ly=2.0, Cn=2.0 / nx, P_CG_MAXIT=4000)
+            params.stencil_fp32 = params.pressure_warm_start = 1
+            params.pressure_preconditioner = params.velocity_cg_unregularized = 1
+            s = runtime.Solver(grid, params, device=device)
+            s.set_planes(planes)
+            s.initialize()
+            out.append(s)
+        return out
+
+    cells = sum(nx * ny for nx, ny in MIXED_SIZES)
+    reps = make()
+    runtime.run_steps_batched(reps, 2, DT)
+    for r in reps:
+        r.flush_l2()
+    for r in reps:
+        r.timer_start()
+    runtime.run_steps_batched(reps, nsteps, DT)
+    span = max(r.timer_stop() for r in reps)
+    seq_ms = 0.0
+    for r in reps:   # the same cases one after another
+        r.flush_l2()
+        r.timer_start()
+        r.run_steps(nsteps, DT)
+        seq_ms += r.timer_stop()
+    for r in reps:
+        r.close()
+    return {"cases": ["%dx%d" % sz for sz in MIXED_SIZES], "cells": cells, "steps": nsteps,
+            "form": "fp32-stencils + pressure warm start + spectral pressure preconditioner + unregularised momentum CG",
+            "value": cells * nsteps / (span * 1e-3), "unit": UNIT, "ms_per_step": span / nsteps,
+            "sequential_value": cells * nsteps / (seq_ms * 1e-3),
+            "vs_sequential": seq_ms / span}
+
+
 def pinned_like(n):
     import torch
     return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
@@ -521,6 +573,12 @@ def run_ours(args):
             batched = {"error": "%s: %s" % (type(e).__name__, e)}
 
     particles = particle_case(args, local) if args.particles else None
+    mixed = None
+    if args.batch_mixed:
+        try:
+            mixed = mixed_batch(args, local)
+        except Exception as e:   # noqa: BLE001
+            mixed = {"error": "%s: %s" % (type(e).__name__, e)}
     large = None
     if args.large:
         try:
@@ -569,6 +627,8 @@ def run_ours(args):
             line["particles"] = particles
         if large is not None:
             line["large"] = large
+        if mixed is not None:
+            line["batched_mixed"] = mixed
         print(json.dumps(line))
     g.close()
     if dist is not None:
@@ -591,6 +651,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=10)
     ap.add_argument("--timing-steps", type=int, default=20,
                     help="steps of the per-solver timing pass after the timed steps")
+    ap.add_argument("--batch-mixed", action="store_true",
+                    help="also time eight cases of four sizes (64x128 .. 512x1024) in all forms, batched")
     ap.add_argument("--large", action="store_true",
                     help="also time 1024x1024 at density ratio 1e-3 (plain, spectral, spectral + momentum form)")
     ap.add_argument("--large-steps", type=int, default=3)
