@@ -396,6 +396,15 @@ int pvof_set_graphs(pvof_ctx *ctx, int enabled);
 /* No counterpart in the reference: how many substeps so far replayed their
  * launches from a graph (-1 for a null context). */
 long long pvof_graph_replays(const pvof_ctx *ctx);
+
+/* No counterpart in the reference: the host-computed tables of the spectral
+ * pressure preconditioner's cyclic reduction for an N x M grid (x spacing
+ * squared inverse idx2, y idy2), without a GPU: for each round st = 0 ..
+ * R - 1 (R = ceil(log2 M)) the multipliers k1 then k2, each [N/2 + 1][M] (one
+ * row per wave number), then the reciprocal diagonals [N/2 + 1][M].  Returns
+ * the number of doubles, (2 R + 1) (N/2 + 1) M, and writes them to out when
+ * cap is at least that; -1 on invalid sizes. */
+long long pvof_spectral_tables(int N, int M, double idx2, double idy2, double *out, long long cap);
 int pvof_solver_timing(const pvof_ctx *ctx, int solver, double *ms, long long *launches, long long *iterations,
                        long long *cell_iters);
 /* Name of the kernel that runs solver PVOF_SOLVER_* for this context: the

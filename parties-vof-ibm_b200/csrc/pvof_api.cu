@@ -2104,6 +2104,19 @@ int pvof_set_graphs(pvof_ctx *c, int enabled)
 
 long long pvof_graph_replays(const pvof_ctx *c) { return c ? c->graph_replays : -1; }
 
+long long pvof_spectral_tables(int N, int M, double idx2, double idy2, double *out, long long cap)
+{
+    if (N < 2 || (N & (N - 1)) != 0 || M < 1 || !(idx2 > 0.0) || !(idy2 > 0.0)) {
+        set_err(PVOF_EINVAL, "pvof_spectral_tables: N a power of two >= 2, M >= 1, positive spacings");
+        return -1;
+    }
+    std::vector<double> tw, pcr;
+    spec_tables(N, M, idx2, idy2, tw, pcr);
+    const long long n = (long long)pcr.size();
+    if (out && cap >= n) std::memcpy(out, pcr.data(), pcr.size() * sizeof(double));
+    return n;
+}
+
 int pvof_set_solver_timing(pvof_ctx *c, int enabled)
 {
     ENTER(c);
