@@ -232,10 +232,12 @@ int fill(pvof_ctx *c, int kind, double *f)
     return PVOF_OK;
 }
 
-int coop_blocks(pvof_ctx *c, int n)
+// blocks for a grid-wide solver launch of kind PVOF_SOLVER_*: enough for n
+// cells, at most what that kernel keeps co-resident
+int coop_blocks(pvof_ctx *c, int n, int kind)
 {
     int b = (n + COOP_THREADS - 1) / COOP_THREADS;
-    if (b > c->coop_blocks) b = c->coop_blocks;
+    if (b > c->coop_blocks_of[kind]) b = c->coop_blocks_of[kind];
     if (b < 1) b = 1;
     return b;
 }
@@ -263,7 +265,7 @@ int timed_launch(pvof_ctx *c, int kind, int comp, int n, L launch, int n2 = 0)
 template <class A>
 int coop_launch(pvof_ctx *c, const void *fn, A &args, int n, int kind, int comp)
 {
-    int nb = coop_blocks(c, n);
+    int nb = coop_blocks(c, n, kind);
     return timed_launch(c, kind, comp, n, [&]() {
         void *params[] = {&args};
         return cudaLaunchCooperativeKernel(fn, dim3((unsigned)nb), dim3(COOP_THREADS), params, 0, c->stream);
@@ -744,8 +746,12 @@ int p_solve_spectral(pvof_ctx *c)
         if (cudaMalloc(&c->spec_mem, h.size() * sizeof(double)) != cudaSuccess ||
             cudaMalloc(&c->spec_s, sizeof(SpecScal)) != cudaSuccess)
             return set_err(PVOF_ENOMEM, "allocating the spectral preconditioner");
-        CK(cudaMemcpy(c->spec_mem, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemset(c->spec_s, 0, sizeof(SpecScal)));
+        // on the context's (non-blocking) stream, so the solve's launches are
+        // ordered after them; a copy or memset on the legacy default stream
+        // is not, and a zeroing of the barrier state landing in the middle of
+        // the first solve erased arrivals (a grid barrier timeout)
+        CK(cudaMemcpyAsync(c->spec_mem, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemsetAsync(c->spec_s, 0, sizeof(SpecScal), c->stream));
     }
     SpecArgs A;
     A.d = d;
@@ -771,7 +777,6 @@ int p_solve_spectral(pvof_ctx *c)
     A.maxit = c->p.P_CG_MAXIT;
     A.s = c->spec_s;
     A.scal = c->scal;
-    c->launches++;   // the barrier counter's reset
     TRY(timed_launch(c, PVOF_SOLVER_PRESSURE, 0, N * M, [&]() {
         return spec_launch_pcg(A, c->spec_blocks, S(c, SC_P_D), S(c, SC_P_D2), c->stream);
     }));
@@ -832,10 +837,13 @@ int read_scalars(pvof_ctx *c)
     CK(cudaStreamSynchronize(c->stream));
     if (c->npend) collect_solver_timing(c);
     if (c->scal_host->error) {
+        const int code = c->scal_host->error;
         CK(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
         if (c->spec_s) CK(cudaMemsetAsync(c->spec_s, 0, sizeof(SpecScal), c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        return set_err(PVOF_ECUDA, "solver grid barrier timed out");
+        return set_err(PVOF_ECUDA, code == 3 ? "cluster solver: a slab edge outside the owner's boundary rows"
+                                              : code == 2 ? "solver grid barrier timed out (spectral pressure solve)"
+                                                          : "solver grid barrier timed out (grid-wide solver)");
     }
     return PVOF_OK;
 }
@@ -953,6 +961,35 @@ bool graph_key_equal(const GraphKey &a, const GraphKey &b)
            a.one_cluster == b.one_cluster;
 }
 
+// The solver kernels whose blocks wait on one another (grid barriers) must
+// stay cooperative launches, all blocks co-resident, when replayed from a
+// graph: mark their kernel nodes so explicitly.  False if a node could not be
+// read or marked.
+bool keep_cooperative(cudaGraph_t g)
+{
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return false;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n && cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return false;
+    const void *coop[] = {(const void *)k_cg_biharmonic, (const void *)k_cg_velocity, (const void *)k_cg_pressure,
+                          spec_pcg_kernel()};
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) != cudaSuccess) return false;
+        if (t != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp;
+        if (cudaGraphKernelNodeGetParams(nd, &kp) != cudaSuccess) return false;
+        for (const void *f : coop) {
+            if (kp.func != f) continue;
+            cudaLaunchAttributeValue v;
+            std::memset(&v, 0, sizeof(v));
+            v.cooperative = 1;
+            if (cudaGraphKernelNodeSetAttribute(nd, cudaLaunchAttributeCooperative, &v) != cudaSuccess) return false;
+        }
+    }
+    return true;
+}
+
 int run_region(pvof_ctx *c, bool warm0)
 {
     if (!c->use_graphs || c->solver_timing || resolved(c) || c->p.pressure_warm_start == 2)
@@ -987,6 +1024,7 @@ int run_region(pvof_ctx *c, bool warm0)
         cudaGraph_t g = nullptr;
         cudaError_t ee = cudaStreamEndCapture(c->stream, &g);
         cudaGraphExec_t x = nullptr;
+        if (rc == PVOF_OK && ee == cudaSuccess && g && !keep_cooperative(g)) ee = cudaErrorUnknown;
         if (rc == PVOF_OK && ee == cudaSuccess && g) ee = cudaGraphInstantiate(&x, g, 0);
         if (g) cudaGraphDestroy(g);
         if (rc != PVOF_OK || ee != cudaSuccess || !x) {
@@ -1100,7 +1138,7 @@ int ibm_state(pvof_ctx *c, IbmState **out)
     }
     std::vector<double> h;
     for (auto *v : {&s->hm.xu, &s->hm.xc, &s->hm.yv, &s->hm.yc}) h.insert(h.end(), v->begin(), v->end());
-    CK(cudaMemcpy(s->d_coord, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(s->d_coord, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     s->xu = s->d_coord + NG;
     s->xc = s->d_coord + nx + NG;
     s->yv = s->d_coord + 2 * nx + NG;
@@ -1139,7 +1177,7 @@ int ibm_need(pvof_ctx *c, IbmState **out)
 // order (mobile list, then fixed), for mcl_nearest_particle_normal
 // (VOF_IBM_wetting.c:118-182): the owned particles until the first list
 // update of a substep, the updated lists (with periodic copies) after it
-int ibm_upload_plist(IbmState *s, const std::vector<const IbmEntry *> &list)
+int ibm_upload_plist(IbmState *s, const std::vector<const IbmEntry *> &list, cudaStream_t stream)
 {
     std::vector<double> h;
     h.reserve(4 * list.size());
@@ -1158,7 +1196,7 @@ int ibm_upload_plist(IbmState *s, const std::vector<const IbmEntry *> &list)
         }
         s->cap_plist = h.size();
     }
-    if (!h.empty()) CK(cudaMemcpy(s->d_plist, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (!h.empty()) CK(cudaMemcpyAsync(s->d_plist, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
     s->n_plist = (int)list.size();
     return PVOF_OK;
 }
@@ -1226,7 +1264,7 @@ int ibm_flag_points(pvof_ctx *c)
     CK(cudaStreamSynchronize(c->stream));   // the host vectors may change with the next update
     std::vector<const IbmEntry *> cur;
     for (const IbmEntry &e : s->entries) cur.push_back(&e);
-    TRY(ibm_upload_plist(s, cur));
+    TRY(ibm_upload_plist(s, cur, c->stream));
     s->flagged = true;
     return PVOF_OK;
 }
@@ -1615,7 +1653,7 @@ int p_solve_fft(pvof_ctx *c)
             c->fft_coef = nullptr;
             return set_err(PVOF_ENOMEM, "cudaMalloc FFT coefficients");
         }
-        CK(cudaMemcpy(c->fft_coef, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(c->fft_coef, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     }
     const double *as_ = c->fft_coef, *ap_ = as_ + NYp, *an_ = ap_ + NYp, *mw = an_ + NYp;
     double *hc = S(c, SC_P_RES), *gam = S(c, SC_P_D);
@@ -1774,7 +1812,10 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, k_cg_pressure, COOP_THREADS, 0);
     ob = std::min(o1, std::min(o2, o3));
     if (ob < 1) return fail(PVOF_ECUDA, "persistent solver kernels do not fit on an SM");
-    c->coop_blocks = ob * nsm;
+    c->coop_blocks_of[PVOF_SOLVER_BIHARMONIC] = o1 * nsm;   // each as many as it keeps co-resident
+    c->coop_blocks_of[PVOF_SOLVER_VELOCITY] = o2 * nsm;
+    c->coop_blocks_of[PVOF_SOLVER_PRESSURE] = o3 * nsm;
+    c->coop_blocks = std::max(o1, std::max(o2, o3)) * nsm;
     c->coop_threads = COOP_THREADS;
     // cluster-resident pressure solver when the grid fits one cluster
     // cluster-resident solvers when the solve ranges fit one cluster
@@ -2183,7 +2224,7 @@ int pvof_set_particles(pvof_ctx *c, const pvof_particle *parts, int n)
     std::vector<const IbmEntry *> cur;
     for (const IbmEntry &e : s->mobile) cur.push_back(&e);
     for (const IbmEntry &e : s->fixed) cur.push_back(&e);
-    return ibm_upload_plist(s, cur);
+    return ibm_upload_plist(s, cur, c->stream);
 }
 
 int pvof_Lagrangian_flag_points(pvof_ctx *c) { ENTER(c); return ibm_flag_points(c); }

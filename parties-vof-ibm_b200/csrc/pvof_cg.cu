@@ -52,7 +52,7 @@ __device__ __noinline__ bool grid_barrier(const GridSync &gs)
             while (*vgen == g) {
                 ++spins;
                 if ((spins & 1023ull) == 0 && (*verr != 0 || spins > BARRIER_SPIN_LIMIT)) {
-                    atomicExch(&gs.s->error, 1);
+                    atomicCAS(&gs.s->error, 0, 1);   // 1: a grid-wide solver's barrier
                     good = 0;
                     break;
                 }

@@ -90,7 +90,7 @@ __device__ inline SlabEdge slab_edge(const int *ysrc, const double *ymul, int rj
         const int nro = slab_row0(e.owner + 1, H, nb) - slab_row0(e.owner, H, nb);
         if (e.lrow == 0) e.zsel = 0;
         else if (e.lrow == nro - 1) e.zsel = 1;
-        else { e.mul = 0.0; e.local = 1; e.lrow = 0; atomicExch(error, 1); }   // excluded by the host check
+        else { e.mul = 0.0; e.local = 1; e.lrow = 0; atomicCAS(error, 0, 3); }   // excluded by the host check
     }
     return e;
 }

@@ -157,7 +157,8 @@ struct Ctx {
     float *cnn_params;
     uint16_t *cnn_bf16;
     float *cnn_x, *cnn_y, *cnn_work;
-    int coop_blocks;         // co-resident blocks for the persistent solvers
+    int coop_blocks;         // the most co-resident blocks of any grid-wide solver (sizes the partial sums)
+    int coop_blocks_of[3];   // co-resident blocks of each grid-wide solver, by PVOF_SOLVER_*
     int coop_threads;
     long long launches;      // kernels launched by this context
     // measurement

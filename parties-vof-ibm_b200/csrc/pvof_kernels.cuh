@@ -50,7 +50,7 @@ struct PresArgs {
 
 // spectral-preconditioned pressure PCG (pvof_spec.cu)
 struct SpecScal {
-    unsigned bar_count;   // grid barrier arrivals of the cooperative solve
+    unsigned bar_count, bar_gen;   // grid barrier of the cooperative solve (arrivals, generation)
 };
 
 constexpr int SPEC_PT = 1024;        // threads per block of the cooperative solve
@@ -78,6 +78,7 @@ bool spec_supported(const Dom &d, const char **why);
 int spec_tables(int N, int M, double idx2, double idy2, std::vector<double> &tw, std::vector<double> &pcr);
 int spec_pcg_blocks(int device, int N, int M);
 cudaError_t spec_launch_pcg(const SpecArgs &A, int blocks, double *d0, double *d1, cudaStream_t st);
+const void *spec_pcg_kernel();   // k_spec_pcg, for marking graph nodes cooperative
 
 __global__ void k_fill(Dom d, BcMap m, double *f);
 __global__ void k_weno_flux(Dom d, int i0, int i1, int j0, int j1, const double *C, const double *u, const double *v,

@@ -44,10 +44,9 @@
 // matrix-vector product, the update with its forward transforms, the
 // tridiagonal solves, the inverse transforms).  Every block adds the
 // per-block sums in block order, so all of them take the same decisions.  The
-// grid barrier is one arrival counter that only grows during a launch (the
-// host zeroes it before each), so a block waits for one atomic round trip;
-// its wait is bounded (on timeout the error flag in DevScalars is set and
-// every block leaves).
+// grid barrier resets itself (the last arriver zeroes the count and advances
+// a generation); its wait is bounded (on timeout the error flag in DevScalars
+// is set and every block leaves).
 #include <cmath>
 #include <vector>
 
@@ -76,30 +75,36 @@ __device__ double block_sum(double v, double *sh)
     return t;
 }
 
-// Grid barrier number `nth` (1, 2, ...) of this launch: every block adds one
-// to the arrival counter (zeroed by the host before the launch) and waits
-// until it reaches nth * gridDim.x.  Returns false (in every thread of the
-// block) when the wait gave up.
-__device__ __noinline__ bool spec_barrier(unsigned *count, unsigned nth, int *err)
+// Grid barrier: the last block to arrive resets the arrival count and
+// advances the generation that the others wait on, so the barrier needs no
+// reset between launches.  The wait is bounded; returns false (in every
+// thread of the block) when it gave up or another block did.
+__device__ __noinline__ bool spec_barrier(SpecScal *s, int *err)
 {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned *vc = count;
+        volatile unsigned *vgen = &s->bar_gen;
         volatile int *verr = err;
         int good = (*verr == 0);
-        const unsigned target = nth * gridDim.x;
+        const unsigned g = *vgen;
         __threadfence();
-        atomicAdd(count, 1u);
-        unsigned long long spins = 0;
-        while ((int)(*vc - target) < 0) {
-            ++spins;
-            if ((spins & 1023ull) == 0 && (*verr != 0 || spins > SPEC_SPIN_LIMIT)) {
-                atomicExch(err, 1);
-                good = 0;
-                break;
+        const unsigned arrived = atomicAdd(&s->bar_count, 1u);
+        if (arrived == gridDim.x - 1) {
+            s->bar_count = 0u;
+            __threadfence();
+            atomicAdd(&s->bar_gen, 1u);
+        } else {
+            unsigned long long spins = 0;
+            while (*vgen == g) {
+                ++spins;
+                if ((spins & 1023ull) == 0 && (*verr != 0 || spins > SPEC_SPIN_LIMIT)) {
+                    atomicCAS(err, 0, 2);   // 2: the spectral solve's barrier
+                    good = 0;
+                    break;
+                }
+                if (spins > 4096) __nanosleep(64);
             }
-            if (spins > 4096) __nanosleep(64);
         }
         __threadfence();
         ok = good;
@@ -292,8 +297,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
     double *work = smem + N;   // N / 2 complex twiddles before it
     double2 *row = reinterpret_cast<double2 *>(work) + (size_t)grp * N;
     double *slotA = A.part, *slotB = A.part + gridDim.x, *slotC = A.part + 2 * gridDim.x;
-    unsigned *count = &A.s->bar_count;
-    unsigned nb = 0;   // grid barriers passed
+    SpecScal *S = A.s;
     int *err = &A.scal->error;
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
     for (int k = threadIdx.x; k < N / 2; k += blockDim.x) tw[k] = A.tw[k];
@@ -318,7 +322,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
         group_forward(B, row, j, active, lt);
     }
     put_part(sJ, slotA, sh);
-    if (!spec_barrier(count, ++nb, err)) return;
+    if (!spec_barrier(S, err)) return;
     double tot = slot_total(slotA, sh);
     int iters = 0;
     double res = sqrt(tot);
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
     for (int it = 0;; it++) {
         // z = (-L)^-1 r
         tridiag_phase(A, work, sh);
-        if (!spec_barrier(count, ++nb, err)) return;
+        if (!spec_barrier(S, err)) return;
         double g = 0.0;
         for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
             const int j = j0 + grp;
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
             __syncthreads();
         }
         put_part(g, slotB, sh);
-        if (!spec_barrier(count, ++nb, err)) return;
+        if (!spec_barrier(S, err)) return;
         const double gnew = slot_total(slotB, sh);
         // guards against 0 / 0 only: with the scaling r.z is about the Jacobi
         // weight times smaller than in the reference's iteration, so a guard
@@ -386,7 +390,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
             }
         }
         put_part(sdad, slotC, sh);
-        if (!spec_barrier(count, ++nb, err)) return;
+        if (!spec_barrier(S, err)) return;
         const double alpha = gamma / (slot_total(slotC, sh) + 1e-300);
         // phi += alpha d, r -= alpha Ad, the stopping sum, forward transforms
         sJ = 0.0;
@@ -405,7 +409,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
             group_forward(B, row, j, active, lt);
         }
         put_part(sJ, slotA, sh);
-        if (!spec_barrier(count, ++nb, err)) return;
+        if (!spec_barrier(S, err)) return;
         tot = slot_total(slotA, sh);
         iters = it + 1;
         res = sqrt(tot);
@@ -420,7 +424,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
         for (int i = lt; i < N; i += ROW_THREADS) ssum += AT_(A.phi, i, j);
     }
     put_part(ssum, slotB, sh);
-    if (!spec_barrier(count, ++nb, err)) return;
+    if (!spec_barrier(S, err)) return;
     const double avg = slot_total(slotB, sh) / ((double)N * (double)M);
     for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
         const int j = j0 + grp;
@@ -508,10 +512,10 @@ int spec_pcg_blocks(int device, int N, int M)
     return most < 1 ? 0 : (want < most ? want : most);
 }
 
+const void *spec_pcg_kernel() { return (const void *)k_spec_pcg; }
+
 cudaError_t spec_launch_pcg(const SpecArgs &A, int blocks, double *d0, double *d1, cudaStream_t st)
 {
-    const cudaError_t e = cudaMemsetAsync(&A.s->bar_count, 0, sizeof(unsigned), st);
-    if (e != cudaSuccess) return e;
     SpecArgs a = A;
     void *args[] = {&a, &d0, &d1};
     return cudaLaunchCooperativeKernel((const void *)k_spec_pcg, dim3((unsigned)blocks), dim3(SPEC_PT), args,

@@ -1,7 +1,7 @@
 """Substeps replayed from CUDA graphs (pvof_set_graphs, on by default)
 against the same substeps issued launch by launch: the fields, the solver
 statistics and the launch count are identical, bit for bit, in the plain
-path and in the forms; the graphs are used from the second step on."""
+path and in the forms; the graphs are used from the third step on."""
 import numpy as np
 import pytest
 
