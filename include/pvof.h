@@ -396,6 +396,13 @@ int pvof_set_graphs(pvof_ctx *ctx, int enabled);
 /* No counterpart in the reference: how many substeps so far replayed their
  * launches from a graph (-1 for a null context). */
 long long pvof_graph_replays(const pvof_ctx *ctx);
+/* No counterpart in the reference: 1 (the default) solves the pressure and
+ * momentum systems with the cluster-resident kernels wherever their solve
+ * ranges fit one thread-block cluster; 0 selects the grid-wide persistent
+ * kernels for every size.  Both run the reference's iteration; results agree
+ * to rounding (their inner products are summed in different orders).  Waits
+ * for the context's stream and drops its captured substep graphs. */
+int pvof_set_cluster_solvers(pvof_ctx *ctx, int enabled);
 
 /* No counterpart in the reference: the host-computed tables of the spectral
  * pressure preconditioner's cyclic reduction for an N x M grid (x spacing
@@ -429,7 +436,11 @@ const char *pvof_solver_kernel(const pvof_ctx *ctx, int solver);
  * device looks up the array's address with that device current; make it
  * before any stream capture.  stream is a cudaStream_t (NULL: default
  * stream); the call returns after the solve has finished, with the
- * iteration count (also the return value) and the final sqrt(r.M^-1 r). */
+ * iteration count (also the return value) and the final sqrt(r.M^-1 r).
+ * As in the reference, a solve that reaches P_CG_MAXIT stops there and still
+ * returns its (positive) iteration count: the solve converged only if
+ * *residual < P_CG_ETOL, so a caller that needs a converged correction
+ * compares the two. */
 int pvof_Pressure_solve_cg_noalloc(const pvof_grid_desc *grid, const pvof_params *params, const double *rho,
                                    const double *rhs, double *phi, void *stream, int *iterations,
                                    double *residual);

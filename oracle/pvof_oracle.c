@@ -1093,8 +1093,16 @@ static int pressure_solve_cg(orc_t *o, double *res_out)
     bc_pressure(o, phi);
     comm(o, phi, 'c');
     pressure_operator(o, Ad, phi);
+    /* the right-hand side carries the operator's row weight r_c in the
+     * axisymmetric mode, as the reference's HYPRE path forms it
+     * (psolve_hypre.c:184-200); its in-tree CG leaves it out and then solves
+     * r_c L phi = rhs, which is not the projection's system (the oracle build
+     * of the reference adds the weight too, oracle/ref/shim/axisym_rhs.c) */
     for (int j = 0; j < NYp; j++)
-        for (int i = 0; i < NXp; i++) AT(o, res, i, j) = AT(o, rhs, i, j) - AT(o, Ad, i, j);
+        for (int i = 0; i < NXp; i++) {
+            double b = o->axisym ? AT(o, rhs, i, j) * row_weight(o, i) : AT(o, rhs, i, j);
+            AT(o, res, i, j) = b - AT(o, Ad, i, j);
+        }
     for (int j = 0; j < NYp; j++)
         for (int i = 0; i < NXp; i++) {
             AT(o, z, i, j) = AT(o, res, i, j) * AT(o, M, i, j);

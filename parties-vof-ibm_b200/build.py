@@ -40,9 +40,26 @@ def up_to_date():
 
 
 def build(force=False, verbose=False):
+    """Compile every source to an object in parallel (objects under
+    _build/, git-ignored), then link the shared library."""
     if not force and up_to_date():
         return OUT
-    cmd = [nvcc()] + NVCC_FLAGS + ["-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES]
+    from concurrent.futures import ThreadPoolExecutor
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+
+    def one(src):
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc()] + compile_flags + ["-c", "-o", obj, os.path.join(CSRC, src)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        objs = list(ex.map(one, SOURCES))
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", OUT] + objs
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -1817,18 +1817,18 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     c->coop_blocks_of[PVOF_SOLVER_PRESSURE] = o3 * nsm;
     c->coop_blocks = std::max(o1, std::max(o2, o3)) * nsm;
     c->coop_threads = COOP_THREADS;
-    // cluster-resident pressure solver when the grid fits one cluster
     // cluster-resident solvers when the solve ranges fit one cluster
-    if (!getenv("PVOF_NO_CLUSTER_SOLVER")) {
-        StripPlan pp = cgs_pressure_setup(d.NX, d.NY, d.axisym, hmaps[BK_PRESSURE]);
-        c->cgs_p_smem = pp.smem;
-        c->cgs_p_threads = pp.threads;
+    // (pvof_set_cluster_solvers selects the grid-wide forms instead)
+    {
+        c->cgs_p_fit = cgs_pressure_setup(d.NX, d.NY, d.axisym, hmaps[BK_PRESSURE]);
+        c->cgs_p_smem = c->cgs_p_fit.smem;
+        c->cgs_p_threads = c->cgs_p_fit.threads;
         int ru[4], rv[4];
         u_range(c, ru[0], ru[1], ru[2], ru[3]);
         v_range(c, rv[0], rv[1], rv[2], rv[3]);
-        StripPlan vp = cgs_velocity_setup(ru, hmaps[BK_U_CG], rv, hmaps[BK_V_CG], d.axisym);
-        c->cgs_v_smem = vp.smem;
-        c->cgs_v_threads = vp.threads;
+        c->cgs_v_fit = cgs_velocity_setup(ru, hmaps[BK_U_CG], rv, hmaps[BK_V_CG], d.axisym);
+        c->cgs_v_smem = c->cgs_v_fit.smem;
+        c->cgs_v_threads = c->cgs_v_fit.threads;
     }
     size_t npart = 4 * (size_t)std::max(c->coop_blocks, (int)(((d.NX + TBX - 1) / TBX) * ((d.NY + TBY - 1) / TBY)));
     if (cudaMalloc(&c->partials, npart * sizeof(double)) != cudaSuccess) return fail(PVOF_ENOMEM, "cudaMalloc partials");
@@ -2063,7 +2063,7 @@ int pvof_run_steps_batched(pvof_ctx *const *ctxs, int n, int nsteps, double dt, 
     }
     // with several cases on the GPU each case's momentum solve takes one
     // cluster (u, then v) instead of two side by side, so more cases fit
-    const bool one = n > 1 && !std::getenv("PVOF_BATCH_VEL_PAIR");
+    const bool one = n > 1;
     std::vector<int> saved((size_t)n);
     for (int q = 0; q < n; q++) {
         saved[(size_t)q] = ctxs[q]->vel_one_cluster;
@@ -2144,6 +2144,26 @@ int pvof_set_graphs(pvof_ctx *c, int enabled)
 }
 
 long long pvof_graph_replays(const pvof_ctx *c) { return c ? c->graph_replays : -1; }
+
+int pvof_set_cluster_solvers(pvof_ctx *c, int enabled)
+{
+    ENTER(c);
+    // the captured substeps hold the old solver launches: wait for them and drop them
+    CK(cudaStreamSynchronize(c->stream));
+    for (GraphEntry &g : c->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = GraphEntry();
+    }
+    c->graph_next = 0;
+    const StripPlan none = {0, 0};
+    const StripPlan &pp = enabled ? c->cgs_p_fit : none;
+    const StripPlan &vp = enabled ? c->cgs_v_fit : none;
+    c->cgs_p_smem = pp.smem;
+    c->cgs_p_threads = pp.threads;
+    c->cgs_v_smem = vp.smem;
+    c->cgs_v_threads = vp.threads;
+    return PVOF_OK;
+}
 
 long long pvof_spectral_tables(int N, int M, double idx2, double idy2, double *out, long long cap)
 {

@@ -362,7 +362,9 @@ __global__ void __launch_bounds__(512) k_cg_pressure(PresArgs A)
         int i, j;
         R.ij(q, i, j);
         double ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, A.phi, P, NX, NY, a, b); });
-        double rv = AT_(A.rhs, i, j) - ad;
+        // the axisymmetric right-hand side carries the row weight r_c of the
+        // operator (psolve_hypre.c:184-200)
+        double rv = (d.axisym ? AT_(A.rhs, i, j) * d.m.r_c[i] : AT_(A.rhs, i, j)) - ad;
         AT_(A.res, i, j) = rv;
         double z = rv * AT_(A.M, i, j);
         AT_(A.dir, i, j) = z;

@@ -272,9 +272,12 @@ __global__ void __launch_bounds__(NT, 1) k_cgs_pressure(PresArgs A)
         cxp[lr * W + ci] = b;
         if (lr == 0) cy[ci] = c2;               // cym of a row = cyp of the row below
         cy[(lr + 1) * W + ci] = e;
-        // initial residual r = rhs - A phi (phi with its ghost update)
+        // initial residual r = rhs - A phi (phi with its ghost update); the
+        // axisymmetric right-hand side carries the operator's row weight r_c
+        // (as psolve_hypre.c:184-200 forms it; the reference's in-tree CG
+        // leaves it out and its projection then diverges)
         double ad0 = pressure_op(d, A.rho, i, j, [&](int x, int y) { return remap(A.mp, A.phi, P, NX, NY, x, y); });
-        double rv = AT_(A.rhs, i, j) - ad0;
+        double rv = (AXI ? AT_(A.rhs, i, j) * rw : AT_(A.rhs, i, j)) - ad0;
         double m = AT_(A.M, i, j);
         double z = rv * m;
         rr[k] = rv;
@@ -709,13 +712,6 @@ static bool identity_on(const std::vector<int> &src, const std::vector<double> &
     return true;
 }
 
-// the thread counts tried, most warps first; PVOF_STRIP_THREADS pins one
-static int strip_threads_allowed(int nt)
-{
-    const char *e = getenv("PVOF_STRIP_THREADS");
-    return !e || atoi(e) == nt;
-}
-
 StripPlan cgs_pressure_setup(int NX, int NY, int axisym, const HostMap &mp)
 {
     StripPlan plan = {0, 0};
@@ -724,11 +720,11 @@ StripPlan cgs_pressure_setup(int NX, int NY, int axisym, const HostMap &mp)
     if (!strip_edges_ok(mp.ysrc, mp.ymul, 0, H)) return plan;
     size_t smem;
     // 512 threads first: the 1024-thread form spills at 64 registers per thread
-    if (strip_threads_allowed(512) && (smem = strip_smem(W, H, 0, 512, 8)) &&
+    if ((smem = strip_smem(W, H, 0, 512, 8)) &&
         (axisym ? strip_kernel_fits(k_cgs_pressure<512, 8, true>, 512, smem)
                 : strip_kernel_fits(k_cgs_pressure<512, 8, false>, 512, smem)))
         return StripPlan{smem, 512};
-    if (strip_threads_allowed(1024) && (smem = strip_smem(W, H, 0, 1024, 4)) &&
+    if ((smem = strip_smem(W, H, 0, 1024, 4)) &&
         (axisym ? strip_kernel_fits(k_cgs_pressure<1024, 4, true>, 1024, smem)
                 : strip_kernel_fits(k_cgs_pressure<1024, 4, false>, 1024, smem)))
         return StripPlan{smem, 1024};
@@ -759,7 +755,6 @@ StripPlan cgs_velocity_setup(const int ru[4], const HostMap &mu, const int rv[4]
     if (!velocity_range_ok(ru, mu) || !velocity_range_ok(rv, mv)) return plan;
     const int Wu = ru[1] - ru[0], Hu = ru[3] - ru[2], Wv = rv[1] - rv[0], Hv = rv[3] - rv[2];
     for (int nt : {1024, 512}) {
-        if (!strip_threads_allowed(nt)) continue;
         const int cpt = nt == 1024 ? 4 : 8;
         const size_t su = strip_smem(Wu, Hu, 1, nt, cpt), sv = strip_smem(Wv, Hv, 1, nt, cpt);
         if (!su || !sv) continue;

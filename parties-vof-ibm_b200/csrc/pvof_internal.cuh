@@ -106,6 +106,13 @@ struct DevScalars {
     unsigned bar_gen;
 };
 
+// launch shape of a strip solver: threads per CTA (0: the range does not fit)
+// and dynamic shared memory
+struct StripPlan {
+    size_t smem;
+    int threads;
+};
+
 struct IbmState;
 
 // host state that the launches of a substep (up to its first Poisson pass)
@@ -149,6 +156,7 @@ struct Ctx {
     size_t cgs_p_smem;       // shared memory of the cluster pressure solver (0: grid solver)
     size_t cgs_v_smem;       // same, velocity solver for both components (0: grid solver)
     int cgs_p_threads, cgs_v_threads;   // their threads per CTA
+    StripPlan cgs_p_fit, cgs_v_fit;     // the cluster plans that fit this grid (kept for pvof_set_cluster_solvers)
     int vel_one_cluster;     // momentum solve as u then v on one cluster (batched runs)
     int phi_prev_mask;       // stages whose last correction is kept in SC_PHI_PREV + stage
     int phi_old_mask;        // stages whose correction one step before that is in SC_PHI_OLD + stage

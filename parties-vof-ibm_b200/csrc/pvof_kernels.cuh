@@ -146,12 +146,6 @@ struct VelPair {
     VelArgs c[2];
 };
 
-// launch shape of a strip solver: threads per CTA (0: the range does not fit)
-// and dynamic shared memory
-struct StripPlan {
-    size_t smem;
-    int threads;
-};
 
 StripPlan cgs_pressure_setup(int NX, int NY, int axisym, const HostMap &mp);
 cudaError_t cgs_pressure_launch(const PresArgs &A, const StripPlan &plan, cudaStream_t stream);

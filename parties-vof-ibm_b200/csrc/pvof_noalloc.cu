@@ -153,6 +153,8 @@ extern "C" int pvof_Pressure_solve_cg_noalloc(const pvof_grid_desc *grid, const 
     if (grid->ghost_nodes != NG || grid->NZM != 1 ||
         (grid->geometry != PVOF_GEOM_PLANAR && grid->geometry != PVOF_GEOM_AXISYM))
         return na_err(PVOF_EINVAL, "needs a 2D grid with 3 ghost layers");
+    if (grid->geometry == PVOF_GEOM_AXISYM && grid->periodic[0])
+        return na_err(PVOF_EINVAL, "an axisymmetric grid has the symmetry axis on its left: x cannot be periodic");
     if (grid->NXM < 8 || grid->NYM < 8 || grid->NXM > NOALLOC_AXIS_MAX || grid->NYM > NOALLOC_AXIS_MAX ||
         (size_t)(grid->NXM + 7) * (size_t)(grid->NYM + 7) > NOALLOC_PLANE_MAX)
         return na_err(PVOF_EINVAL, "grid exceeds the fixed scratch: (NXM+7)*(NYM+7) must be <= 72000 "

@@ -67,6 +67,7 @@ def load():
     L.pvof_set_graphs.argtypes = [V, C.c_int]
     L.pvof_graph_replays.argtypes = [V]
     L.pvof_graph_replays.restype = C.c_longlong
+    L.pvof_set_cluster_solvers.argtypes = [V, C.c_int]
     L.pvof_solver_timing.argtypes = [V, C.c_int, P(C.c_double), P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]
     L.pvof_solver_kernel.argtypes = [V, C.c_int]
     L.pvof_set_particles.argtypes = [V, P(abi.Particle), C.c_int]
@@ -262,6 +263,10 @@ class Solver:
 
     def graph_replays(self):
         return load().pvof_graph_replays(self.h)
+
+    def set_cluster_solvers(self, on):
+        """Cluster-resident solvers where they fit (default), or the grid-wide ones."""
+        check(load().pvof_set_cluster_solvers(self.h, 1 if on else 0), "pvof_set_cluster_solvers")
 
     def solver_kernel(self, solver):
         """Name of the kernel that runs solver abi.SOLVER_* in this context."""

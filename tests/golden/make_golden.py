@@ -40,6 +40,8 @@ ST_NG = {"f_sigma_old_x": "FSIG_OLD_X", "f_sigma_old_y": "FSIG_OLD_Y"}
 
 TIGHT = dict(ch_tol=1e-13, ch_iter_max=600, CG_ETOL=1e-15, CG_MAXIT=400, P_CG_ETOL=1e-13, P_CG_MAXIT=1000)
 
+AXI_GRID = dict(NXM=24, NYM=48, rmax=1.0, zmax=2.0, radius=0.3, zc=0.7, Cn=0.04)
+
 # name, reference case, builder kwargs, steps, dt, snapshots kept (None = all)
 CASES = [
     ("rt_small", "rt2d", dict(NXM=24, NYM=48, Lx=1.0, Ly=2.0, Cn=0.04, velocity_seed=5, velocity_amp=0.1), 2, 1e-3, None),
@@ -50,6 +52,24 @@ CASES = [
     # free-slip walls in y (BOTTOM/TOP_WALL_VELOCITY_FREESLIP)
     ("rt_fs_tight", "rt2d_fs", dict(NXM=24, NYM=48, Lx=1.0, Ly=2.0, Cn=0.04, velocity_seed=9, velocity_amp=0.1,
                                     wall_y=abi.WALL_FREESLIP, **TIGHT), 2, 1e-3, ["s0", "s1_0", "s1_2", "s2_2"]),
+    # axisymmetric (r, z) bubble on the axis (AXISYM_RZ builds; the pressure
+    # right-hand side carries the operator's row weight, oracle/ref/shim/axisym_rhs.c)
+    ("axi_small", "axi2d", dict(_builder="rising_bubble", **AXI_GRID, velocity_seed=5, velocity_amp=0.1), 2, 1e-3,
+     None),
+    ("axi_tight", "axi2d", dict(_builder="rising_bubble", **AXI_GRID, velocity_seed=3, velocity_amp=0.1, **TIGHT), 2,
+     1e-3, ["s0", "s1_0", "s1_2", "s2_2"]),
+    ("axi_st_tight", "axi2d_st", dict(_builder="rising_bubble", **AXI_GRID, surface_tension=True, We=200.0,
+                                      velocity_seed=21, velocity_amp=0.1, **TIGHT), 2, 1e-3,
+     ["s0", "s1_0", "s1_2", "s2_2"]),
+]
+
+# long runs on a benchmark grid, only the end state kept (physical cells of
+# C_L, u, v, p): name, reference case, builder kwargs, steps, dt.  The first is
+# the planar instability on its full 128x512 grid (dt 1e-4, zero initial
+# velocity), solver tolerances near machine precision.
+LONG_CASES = [
+    ("rt128x512_100steps", "rt2d", dict(NXM=128, NYM=512, Lx=1.0, Ly=4.0, Cn=0.01, **dict(TIGHT, P_CG_MAXIT=4000)),
+     100, 1e-4),
 ]
 
 # resolved-particle routine cases (oracle/ref/ibm_driver.c on the ibm2d build):
@@ -153,6 +173,29 @@ def make(name, refcase, kw, steps, dt, keep, outdir, refsrc=None):
         data["init/" + k] = v
     meta = {"grid": struct_to_dict(grid), "params": struct_to_dict(params), "steps": steps, "dt": dt,
             "refcase": refcase, "builder": kw}
+    data["meta"] = np.array(repr(meta))
+    path = os.path.join(outdir, name + ".npz")
+    np.savez_compressed(path, **data)
+    return path
+
+
+def make_long(name, refcase, kw, steps, dt, outdir, refsrc=None):
+    build = dict(kw)
+    builder = getattr(cases, build.pop("_builder", "rayleigh_taylor"))
+    grid, params, planes = builder(**build)
+    if not os.path.exists(po.ref_binary(refcase)):
+        po.build_reference(refcase, refsrc)
+    NX, NY, _ = cases.dims(grid)
+    data = {}
+    with tempfile.TemporaryDirectory() as wd:
+        cp = po.run_reference(refcase, wd, grid, params, planes, steps, dt, steps, substeps=False, timeout=7200)
+        tag = "s%d" % steps
+        for fname, pname in (("C_L", "C_L"), ("u", "U"), ("v", "V"), ("p", "P")):
+            a = g_range(grid, po.read_reference_field(wd, tag, fname, grid), False)
+            data["%s/%s" % (tag, pname)] = a[:NY - 1, :NX - 1]
+        data["iterations"] = parse_iterations(cp.stdout)
+    meta = {"grid": struct_to_dict(grid), "params": struct_to_dict(params), "steps": steps, "dt": dt,
+            "refcase": refcase, "builder": kw, "physical_only": True}
     data["meta"] = np.array(repr(meta))
     path = os.path.join(outdir, name + ".npz")
     np.savez_compressed(path, **data)
@@ -300,6 +343,9 @@ def main():
     for name, refcase, kw, steps, dt, keep in CASES:
         if ap_only is None or name in ap_only:
             print(make(name, refcase, kw, steps, dt, keep, a.out, a.refsrc))
+    for name, refcase, kw, steps, dt in LONG_CASES:
+        if ap_only is not None and name in ap_only:   # minutes of CPU: only on request
+            print(make_long(name, refcase, kw, steps, dt, a.out, a.refsrc))
     for name, kw, parts, dt, stage in IBM_CASES:
         if ap_only is None or name in ap_only:
             print(make_ibm(name, kw, parts, dt, stage, a.out, a.refsrc))

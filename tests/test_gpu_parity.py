@@ -26,14 +26,10 @@ STATE = ["C_L", "C_G", "RHO", "MU", "CH_RHS_N", "U", "V", "P"]
 def solver_for(grid, params, planes, grid_solver=False):
     """grid_solver=True forces the grid-wide pressure PCG even where the
     cluster-resident one fits."""
-    import os
     from pvof import runtime
+    g = runtime.Solver(grid, params, device=0)
     if grid_solver:
-        os.environ["PVOF_NO_CLUSTER_SOLVER"] = "1"
-    try:
-        g = runtime.Solver(grid, params, device=0)
-    finally:
-        os.environ.pop("PVOF_NO_CLUSTER_SOLVER", None)
+        g.set_cluster_solvers(False)
     g.set_planes(planes)
     g.initialize()
     return g
@@ -59,7 +55,8 @@ def compare(grid, get_a, get_b, fields, tol, what):
 
 
 @pytest.mark.parametrize("name,tol", [("rt_tight", 1e-12), ("rt_small", 1e-9), ("rt_st_small", 1e-9),
-                                      ("rt_fs_tight", 1e-12)])
+                                      ("rt_fs_tight", 1e-12), ("axi_tight", 1e-12), ("axi_small", 1e-9),
+                                      ("axi_st_tight", 1e-12)])
 def test_gpu_matches_reference_golden(name, tol):
     grid, params, planes, d, meta = load_golden(name)
     g = solver_for(grid, params, planes)
@@ -88,12 +85,18 @@ def test_gpu_matches_reference_golden(name, tol):
     assert np.all(np.abs(got[:, 3] - ref_iters[:, 3]) <= 2), (got, ref_iters)
 
 
-def test_stencil_routines_bitwise_on_equal_inputs():
+@pytest.mark.parametrize("geometry", ["planar", "axisym"])
+def test_stencil_routines_bitwise_on_equal_inputs(geometry):
     """Every routine that is not an iterative solve rounds exactly like the
-    oracle (the library is built without FMA contraction)."""
+    oracle (the library is built without FMA contraction), in the planar and
+    in the axisymmetric mode."""
     from pvof import cases
-    grid, params, planes = cases.rayleigh_taylor(32, 64, Lx=1.0, Ly=2.0, Cn=0.04, surface_tension=True,
-                                                 velocity_seed=5, velocity_amp=0.1)
+    if geometry == "planar":
+        grid, params, planes = cases.rayleigh_taylor(32, 64, Lx=1.0, Ly=2.0, Cn=0.04, surface_tension=True,
+                                                     velocity_seed=5, velocity_amp=0.1)
+    else:
+        grid, params, planes = cases.rising_bubble(NXM=32, NYM=64, rmax=1.0, zmax=2.0, radius=0.3, zc=0.7, Cn=0.04,
+                                                   surface_tension=True, velocity_seed=5, velocity_amp=0.1)
     g = solver_for(grid, params, planes)
     o = oracle_for(grid, params, planes)
     for f in STATE + ["U_BC", "V_BC", "F"]:
@@ -127,10 +130,15 @@ def test_stencil_routines_bitwise_on_equal_inputs():
             assert np.array_equal(a, b), "%s/%s max diff %.3e" % (name, f, np.abs(a - b).max())
 
 
-def test_solvers_match_oracle_routine_by_routine():
+@pytest.mark.parametrize("geometry", ["planar", "axisym"])
+def test_solvers_match_oracle_routine_by_routine(geometry):
     from pvof import cases
-    grid, params, planes = cases.rayleigh_taylor(32, 64, Lx=1.0, Ly=2.0, Cn=0.04, surface_tension=True,
-                                                 velocity_seed=9, velocity_amp=0.1, **TIGHT)
+    if geometry == "planar":
+        grid, params, planes = cases.rayleigh_taylor(32, 64, Lx=1.0, Ly=2.0, Cn=0.04, surface_tension=True,
+                                                     velocity_seed=9, velocity_amp=0.1, **TIGHT)
+    else:
+        grid, params, planes = cases.rising_bubble(NXM=32, NYM=64, rmax=1.0, zmax=2.0, radius=0.3, zc=0.7, Cn=0.04,
+                                                   surface_tension=True, velocity_seed=9, velocity_amp=0.1, **TIGHT)
     g = solver_for(grid, params, planes)
     o = oracle_for(grid, params, planes)
     g.set_stage(0, 1e-3)
@@ -189,6 +197,24 @@ def test_hundred_steps_parity():
     g.run_steps(100, 5e-4)
     o.run_steps(100, 5e-4)
     compare(grid, g.get, o.get_field, STATE, 1e-10, "100 steps")
+
+
+def test_hundred_steps_128x512_against_reference():
+    """The planar instability on its full 128x512 grid (the benchmark
+    workload), 100 RK3 steps at dt 1e-4, solver tolerances near machine
+    precision: C_L, u, v and p on the physical cells within 1e-10 relative L2
+    of the reference's own time step (fixture rt128x512_100steps, written by
+    the reference build)."""
+    grid, params, planes, d, meta = load_golden("rt128x512_100steps")
+    g = solver_for(grid, params, planes)
+    g.run_steps(meta["steps"], meta["dt"])
+    from pvof import cases
+    NX, NY, _ = cases.dims(grid)
+    worst = {}
+    for f in ("C_L", "U", "V", "P"):
+        a = g_range(grid, g.get(f))[:NY - 1, :NX - 1]
+        worst[f] = rel_l2(a, d["s%d/%s" % (meta["steps"], f)])
+    assert all(r <= 1e-10 for r in worst.values()), worst
 
 
 def test_liquid_mass_conserved():

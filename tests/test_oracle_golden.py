@@ -47,7 +47,8 @@ def run_case(name):
     return d, snaps, np.array(iters)
 
 
-@pytest.mark.parametrize("name", ["rt_small", "rt_st_small", "rt_tight", "rt_fs_tight"])
+@pytest.mark.parametrize("name", ["rt_small", "rt_st_small", "rt_tight", "rt_fs_tight", "axi_small", "axi_tight",
+                                  "axi_st_tight"])
 def test_oracle_matches_reference_bitwise(name):
     d, snaps, iters = run_case(name)
     assert np.array_equal(iters, d["iterations"]), (iters, d["iterations"])

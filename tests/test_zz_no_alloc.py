@@ -11,7 +11,6 @@ solver converged to near machine precision).  The test allocates its device
 buffers with torch; the entry point itself allocates nothing.
 """
 import ctypes as C
-import os
 
 import numpy as np
 import pytest
@@ -21,17 +20,25 @@ from conftest import rel_l2
 pytestmark = pytest.mark.gpu
 
 
-def test_noalloc_pressure_solve_matches_context_solve():
+def _case(kind):
+    from pvof import cases
+    if kind == "planar":
+        return cases.rayleigh_taylor(128, 512, Lx=1.0, Ly=4.0, Cn=0.01, velocity_seed=6, velocity_amp=0.05,
+                                     P_CG_ETOL=1e-6, P_CG_MAXIT=4000)
+    # axisymmetric: the radius tables (r_u, r_c, 1/r_c) and the row-weighted
+    # right-hand side take a branch of their own
+    return cases.rising_bubble(NXM=96, NYM=192, rmax=1.0, zmax=2.0, radius=0.3, zc=0.7, Cn=0.02, velocity_seed=4,
+                               velocity_amp=0.05, P_CG_ETOL=1e-9, P_CG_MAXIT=4000)
+
+
+@pytest.mark.parametrize("kind", ["planar", "axisym"])
+def test_noalloc_pressure_solve_matches_context_solve(kind):
     import torch
     from pvof import abi, cases, runtime
 
-    grid, params, planes = cases.rayleigh_taylor(128, 512, Lx=1.0, Ly=4.0, Cn=0.01, velocity_seed=6,
-                                                 velocity_amp=0.05, P_CG_ETOL=1e-6, P_CG_MAXIT=4000)
-    os.environ["PVOF_NO_CLUSTER_SOLVER"] = "1"
-    try:
-        g = runtime.Solver(grid, params, device=0)
-    finally:
-        os.environ.pop("PVOF_NO_CLUSTER_SOLVER", None)
+    grid, params, planes = _case(kind)
+    g = runtime.Solver(grid, params, device=0)
+    g.set_cluster_solvers(False)   # the grid-wide kernel, as the entry point uses
     g.set_planes(planes)
     g.initialize()
     g.set_stage(1, 1e-4)
@@ -74,3 +81,11 @@ def test_noalloc_pressure_solve_matches_context_solve():
                                           d_rho.data_ptr(), None, None, None)
     assert rc == abi.EINVAL
     assert b"72000" in L.pvof_noalloc_last_error()
+    # so is an axisymmetric grid whose radial direction is marked periodic
+    if kind == "axisym":
+        bad = abi.GridDesc.from_buffer_copy(grid)
+        bad.periodic[0] = 1
+        rc = L.pvof_Pressure_solve_cg_noalloc(C.byref(bad), C.byref(params), d_rho.data_ptr(), d_rhs.data_ptr(),
+                                              d_rho.data_ptr(), None, None, None)
+        assert rc == abi.EINVAL
+        assert b"axis" in L.pvof_noalloc_last_error()
