@@ -49,6 +49,11 @@ advanced one after another.
 ratio of 1e-3 (--large-steps timed steps) in the plain path, with the
 spectral pressure preconditioner, and with it the unregularised momentum CG.
 
+--axisym adds an "axisym" object: the axisymmetric bubble rising towards a
+fixed sphere on the axis (256x512, density ratio 1e-3, surface tension,
+contact angle 90 degrees) for --axisym-steps steps, with the reference build
+(AXISYM_RZ, resolved particles) on the host for --axisym-ref-steps steps.
+
 --impl reference runs the reference's own time step (compiled from its
 sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host:
 --warmup untimed steps, then min(--steps, --ref-steps) timed ones.
@@ -311,6 +316,84 @@ def large_case(args, device):
                       "velocity_iterations_per_step": t[1]["iterations"]}
         s.close()
     out["spectral_vs_plain"] = out["spectral + unregularised momentum"]["value"] / out["plain"]["value"]
+    return out
+
+
+# the axisymmetric benchmark case: a bubble (R 0.5 at z = 1) rising towards a
+# fixed sphere (R 0.25 at z = 2.5) on the axis, 256 x 512 cells over
+# r in [0, 2], z in [0, 4]
+AXI_SPHERE = [(0, 0.0, 2.5, 0.25, 0, 0, 0, 2.5)]
+AXI_DT = 1e-4
+
+
+def axisym_setup():
+    from pvof import cases
+    grid, params, planes = cases.rising_bubble(NXM=256, NYM=512, rmax=2.0, zmax=4.0, radius=0.5, zc=1.0, Cn=0.01,
+                                               rho_ratio=1e-3, mu_ratio=1e-2, Re=100.0, surface_tension=True,
+                                               We=200.0, P_CG_MAXIT=40000)
+    params.contact_angle_deg = 90.0
+    return grid, params, planes
+
+
+def axisym_reference(steps, timeout=3600):
+    """The reference build with AXISYM_RZ and resolved particles
+    (oracle/_ref/ref_ibm_axi_st) on the axisymmetric case for ``steps``
+    steps on the host; (cell-updates/s, seconds) or None."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle as po  # checker / CPU baseline only
+    if not os.path.exists(po.ref_binary("ibm_axi_st")):
+        return None
+    grid, params, planes = axisym_setup()
+    fixed = [p[1:7] for p in AXI_SPHERE if not p[0]]
+    mobile = [p[1:7] for p in AXI_SPHERE if p[0]]
+    with tempfile.TemporaryDirectory() as wd:
+        cp = po.run_reference_ibm(wd, grid, params, planes, fixed, mobile, AXI_DT, 0, case="ibm_axi_st",
+                                  mode="steps", nsteps=steps, timeout=timeout)
+    for line in cp.stdout.splitlines():
+        if line.startswith("REF_TIMING"):
+            kv = dict(x.split("=") for x in line.split()[1:])
+            secs = float(kv["seconds"])
+            return int(kv["cells"]) * int(kv["steps"]) / secs, secs
+    return None
+
+
+def axisym_case(args, device):
+    """The axisymmetric bubble-and-sphere case (density ratio 1e-3, viscosity
+    ratio 1e-2, Re 100, We 200, Cn 0.01, contact angle 90 degrees): one
+    untimed step, then --axisym-steps timed steps (device time, L2 flushed),
+    and the reference build on the host for --axisym-ref-steps steps."""
+    from pvof import runtime
+    grid, params, planes = axisym_setup()
+    cells = grid.NXM * grid.NYM
+    s = runtime.Solver(grid, params, device=device)
+    s.set_particles(AXI_SPHERE)
+    s.set_planes(dict(planes, C_L=planes["F"]))
+    s.initialize()
+    s.run_steps(1, AXI_DT)
+    nsteps = max(1, args.axisym_steps)
+    s.set_solver_timing(True)
+    l0, ms = s.launch_count(), 0.0
+    for _ in range(nsteps):
+        s.flush_l2()
+        s.timer_start()
+        s.run_steps(1, AXI_DT)
+        ms += s.timer_stop()
+    t = s.solver_timing(2)
+    out = {"case": "axisymmetric bubble (R 0.5, z 1) below a fixed sphere on the axis (R 0.25, z 2.5), 256x512, "
+                   "r in [0,2], z in [0,4], density ratio 1e-3, viscosity ratio 1e-2, Re 100, We 200, Cn 0.01, "
+                   "contact angle 90 degrees, dt 1e-4",
+           "value": cells * nsteps / (ms * 1e-3), "unit": UNIT, "steps": nsteps, "ms_per_step": ms / nsteps,
+           "launches_per_step": (s.launch_count() - l0) / nsteps,
+           "pressure_iterations_per_step": t["iterations"] / nsteps, "pressure_kernel": s.solver_kernel(2)}
+    s.close()
+    if args.axisym_ref_steps > 0:
+        r = axisym_reference(args.axisym_ref_steps)
+        if r is not None:
+            out["cpu_reference"] = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
+                                    "sample": "%d time steps of the same case (after the start-up) by the "
+                                              "single-rank reference build with AXISYM_RZ and resolved "
+                                              "particles, %.1f s" % (args.axisym_ref_steps, r[1])}
+            out["vs_cpu_reference"] = out["value"] / r[0]
     return out
 
 
@@ -579,6 +662,12 @@ def run_ours(args):
             mixed = mixed_batch(args, local)
         except Exception as e:   # noqa: BLE001
             mixed = {"error": "%s: %s" % (type(e).__name__, e)}
+    axisym = None
+    if args.axisym:
+        try:
+            axisym = axisym_case(args, local)
+        except Exception as e:   # noqa: BLE001
+            axisym = {"error": "%s: %s" % (type(e).__name__, e)}
     large = None
     if args.large:
         try:
@@ -627,6 +716,8 @@ def run_ours(args):
             line["particles"] = particles
         if large is not None:
             line["large"] = large
+        if axisym is not None:
+            line["axisym"] = axisym
         if mixed is not None:
             line["batched_mixed"] = mixed
         print(json.dumps(line))
@@ -656,6 +747,10 @@ def main():
     ap.add_argument("--large", action="store_true",
                     help="also time 1024x1024 at density ratio 1e-3 (plain, spectral, spectral + momentum form)")
     ap.add_argument("--large-steps", type=int, default=3)
+    ap.add_argument("--axisym", action="store_true",
+                    help="also time the axisymmetric bubble-and-sphere case (256x512) and the reference on it")
+    ap.add_argument("--axisym-steps", type=int, default=10)
+    ap.add_argument("--axisym-ref-steps", type=int, default=2)
     ap.add_argument("--particles", action="store_true",
                     help="also time the workload with surface tension and three resolved cylinders")
     ap.add_argument("--forms", action="store_true", default=True,

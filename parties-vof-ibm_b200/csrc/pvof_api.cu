@@ -1127,7 +1127,6 @@ namespace {
 
 int ibm_state(pvof_ctx *c, IbmState **out)
 {
-    if (!c->dom.planar) return set_err(PVOF_EINVAL, "resolved particles are built for the planar mode only");
     if (c->ibm) { *out = c->ibm; return PVOF_OK; }
     IbmState *s = new IbmState();
     build_metrics(c->g, c->dom.NX, c->dom.NY, s->hm);
@@ -1148,6 +1147,7 @@ int ibm_state(pvof_ctx *c, IbmState **out)
     g.NY = c->dom.NY;
     g.periodic[0] = c->dom.perx;
     g.periodic[1] = c->dom.pery;
+    g.axisym = c->dom.axisym;
     g.xu = s->hm.xu.data() + NG;
     g.yv = s->hm.yv.data() + NG;
     g.xc = s->hm.xc.data() + NG;
@@ -1293,6 +1293,8 @@ IbmDev ibm_dev(pvof_ctx *c, IbmState *s)
     D.dxu1 = s->hm.dx_u[1 + NG];
     D.slab = c->dom.slab > 0.0 ? c->dom.slab : D.dxu1;
     D.dyv = c->dom.m.dy_v;
+    D.axisym = c->dom.axisym;
+    D.theta_span = c->g.theta_span;
     return D;
 }
 
@@ -1322,13 +1324,15 @@ int ibm_force(pvof_ctx *c, int force_iter)
             CKL(c);
         }
         if (nm > 0) {
-            k_ibm_interp<<<mg, 128, 0, c->stream>>>(d, rho, s->xc, s->yc, D.h, D.XL, D.YL, nm, D.rhoL);
+            k_ibm_interp<<<mg, 128, 0, c->stream>>>(d, rho, s->xc, s->yc, D.h, D.XL, D.YL, nm,
+                                                    d.axisym ? IBM_AXIS_EVEN : IBM_AXIS_NONE, D.rhoL);
             CKL(c);
         }
         for (int comp = 0; comp < 2; comp++) {
             const double *xs = comp == 0 ? s->xu : s->xc, *ys = comp == 0 ? s->yc : s->yv;
             if (nm > 0) {
-                k_ibm_interp<<<mg, 128, 0, c->stream>>>(d, comp == 0 ? U : V, xs, ys, D.h, D.XL, D.YL, nm, D.UL);
+                const int axis = !d.axisym ? IBM_AXIS_NONE : (comp == 0 ? IBM_AXIS_ODD : IBM_AXIS_EVEN);
+                k_ibm_interp<<<mg, 128, 0, c->stream>>>(d, comp == 0 ? U : V, xs, ys, D.h, D.XL, D.YL, nm, axis, D.UL);
                 CKL(c);
             }
             if (ne > 0) {
@@ -1438,6 +1442,8 @@ int ibm_sums(pvof_ctx *c, bool ccf)
     A.support_width = 8.0 * ((cn > h_ref) ? cn : h_ref);
     A.nk = c->dom.nk;
     A.ccf = ccf ? 1 : 0;
+    A.axisym = c->dom.axisym;
+    A.theta_span = c->g.theta_span;
     A.out = s->d_sums;
     k_ibm_particle_sums<<<(unsigned)ne, 256, 0, c->stream>>>(c->dom, A);
     CKL(c);
@@ -1553,6 +1559,11 @@ int mcl_normals(pvof_ctx *c)
     k_mcl_normals<<<grd, blk, 0, c->stream>>>(d, s->xc, s->yc, F(c, PVOF_F_C_S), s->d_plist, s->n_plist,
                                               support_width, F(c, PVOF_F_NX_IBM), F(c, PVOF_F_NY_IBM));
     CKL(c);
+    if (d.axisym) {
+        k_mcl_axis_normals<<<(unsigned)((d.NY + 2 * NG + 127) / 128), 128, 0, c->stream>>>(d, F(c, PVOF_F_NX_IBM),
+                                                                                         F(c, PVOF_F_NY_IBM));
+        CKL(c);
+    }
     TRY(fill(c, BK_NRM_X, F(c, PVOF_F_NX_IBM)));
     return fill(c, BK_NRM_Y, F(c, PVOF_F_NY_IBM));
 }
@@ -2225,6 +2236,10 @@ int pvof_set_particles(pvof_ctx *c, const pvof_particle *parts, int n)
     for (int q = 0; q < n; q++) {
         const pvof_particle &p = parts[q];
         if (!(p.R > 0.0)) return set_err(PVOF_EINVAL, "particle radius must be positive");
+        // Lagrangian_generate_points_2d (Lagrangian.c:2948-2959): axisymmetric
+        // particles are spheres centred on the axis
+        if (c->dom.axisym && std::fabs(p.X[0]) > 1.0e-14)
+            return set_err(PVOF_EINVAL, "an axisymmetric particle must sit on the axis (X[0] = 0)");
         IbmEntry e;
         std::memset(&e, 0, sizeof(e));
         e.X[0] = p.X[0];

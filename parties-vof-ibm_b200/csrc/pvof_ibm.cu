@@ -1,6 +1,7 @@
 // Immersed-boundary routines of the diffuse-interface substep for resolved
-// solid particles in the planar 2D mode (the reference's VOF_IBM +
-// LAG_PARTICLE_RESOLVED + TWOD_CARTESIAN build):
+// solid particles in the 2D modes (the reference's VOF_IBM +
+// LAG_PARTICLE_RESOLVED build with TWOD_CARTESIAN: cylinders; with AXISYM_RZ:
+// spheres on the symmetry axis, their markers full rings):
 //
 //   particle lists at the start of a substep   Particle_MPI_update (single rank,
 //                                              Lagrangian/Particle.c:2042-2500)
@@ -40,11 +41,21 @@ constexpr double LUB_RANGE = 2.0;                   // [particle] lub_range defa
 // host: particle lists, markers and flags
 // ---------------------------------------------------------------------------
 
-// Particle_calc_derived_data (Lagrangian/Particle.c:663-733), planar branch
+// Particle_calc_derived_data (Lagrangian/Particle.c:663-733): planar
+// cylinders per slab thickness; axisymmetric spheres keep the sphere's mass
+// and moment of inertia, with one ring marker per ceil(pi R / h) (at least 4)
 static void derived_data(IbmEntry &e, const IbmGrid &g)
 {
     const double h = g.dy_min;
-    const double R2 = e.R * e.R;
+    const double R = e.R, R2 = R * R;
+    if (g.axisym) {
+        e.M = e.rho_s * 4.0 / 3.0 * IBM_PI * R2 * R;
+        e.I_p = e.rho_s * 8.0 / 15.0 * IBM_PI * R2 * R2 * R;
+        int N_L = (int)ceil(IBM_PI * R / h);
+        e.N_L = N_L > 4 ? N_L : 4;
+        e.Vol_L = 4.0 * IBM_PI * R2 * h / e.N_L;
+        return;
+    }
     double slab = g.slab > 0.0 ? g.slab : g.twod_slab;
     if (slab <= 0.0) slab = h;
     int N_L = (int)ceil(2.0 * IBM_PI * e.R / h);
@@ -113,11 +124,34 @@ static bool near_point(double x, double y, double range, const IbmGrid &g)
     return xs - x < range && x - xe < range && ys - y < range && y - ye < range;
 }
 
-// Lagrangian_generate_points_2d, planar branch (Lagrangian/Lagrangian.c:2900-2947)
+// Lagrangian_generate_points_2d (Lagrangian/Lagrangian.c:2900-2991): planar
+// markers on the circle, line segment x slab x h each; axisymmetric markers on
+// the meridian of a sphere centred on the axis, midpoints in the polar angle,
+// each the spherical band 2 pi R^2 (cos theta_m - cos theta_p) times h
 static void generate_points(IbmEntry &e, const IbmGrid &g, IbmMarkers &m)
 {
     const double h = g.h;
     const double range = DELTA_FUNC_RADIUS * h;
+    if (g.axisym) {
+        const double dtheta = IBM_PI / e.N_L;
+        e.moff = (int)m.x.size();
+        for (int mv = 0; mv < e.N_L; mv++) {
+            const double theta = (mv + 0.5) * dtheta;
+            const double theta_m = mv * dtheta;
+            const double theta_p = (mv + 1) * dtheta;
+            const double r_ring = e.R * sin(theta);
+            const double z_axial = e.X[1] + e.R * cos(theta);
+            const double ring_volume = (2.0 * IBM_PI) * e.R * e.R * (cos(theta_m) - cos(theta_p)) * h;
+            if (near_point(r_ring, z_axial, range, g)) {
+                m.x.push_back(r_ring);
+                m.y.push_back(z_axial);
+                m.vol.push_back(ring_volume);
+                m.flag.push_back(1);
+            }
+        }
+        e.mcount = (int)m.x.size() - e.moff;
+        return;
+    }
     const double dtheta = 2.0 * IBM_PI / e.N_L;
     const double ds = e.R * dtheta;
     double slab = g.slab;
@@ -171,7 +205,7 @@ static void flag_walls(const IbmEntry &p, const IbmGrid &g, IbmMarkers &m)
         }
     };
     if (!g.periodic[0]) {
-        wall(0, g.xu[0]);
+        if (!g.axisym) wall(0, g.xu[0]);   // the axis is no wall (Lagrangian.c:2723)
         wall(0, g.xu[g.NX - 1]);
     }
     if (!g.periodic[1]) {
@@ -316,13 +350,24 @@ const double RK_BET[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
 const double RK_GAM[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
 const double RK_ZET[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
 
-// Lagrangian_apply_twod_particle_constraints (Lagrangian/Lagrangian.c:105-129), planar
-void twod_constraints(IbmEntry &p, double zs)
+// Lagrangian_apply_twod_particle_constraints (Lagrangian/Lagrangian.c:105-129):
+// planar cylinders keep the spin about z only; axisymmetric spheres stay on
+// the axis and do not rotate
+void twod_constraints(IbmEntry &p, double zs, bool axisym)
 {
     p.X[2] = zs;
     p.X_old[2] = p.X[2];
     p.U[2] = 0.0;
     p.U_old[2] = 0.0;
+    if (axisym) {
+        p.X[0] = 0.0;
+        p.X_old[0] = 0.0;
+        p.U[0] = 0.0;
+        p.U_old[0] = 0.0;
+        for (int i = 0; i < 3; i++) p.Omega[i] = 0.0;
+        for (int i = 0; i < 3; i++) p.Omega_old[i] = 0.0;
+        return;
+    }
     p.Omega[0] = 0.0;
     p.Omega[1] = 0.0;
     p.Omega_old[0] = 0.0;
@@ -402,6 +447,22 @@ bool ibm_advance(std::vector<IbmEntry> &mobile, std::vector<IbmEntry> &fixed, co
     // F_CCF_cum, ...) change nothing downstream and are not kept
     const double bt = RK_BET[stage];
     const double idt2beta = 1.0 / (2.0 * bt * dt);
+    // axisymmetric: markers are full rings, so on an on-axis sphere the radial
+    // and azimuthal components and every torque cancel (Lagrangian.c:525-543,
+    // :819-837); only the axial force moves it
+    if (g.axisym)
+        for (std::vector<IbmEntry> *l : {&mobile, &fixed})
+            for (IbmEntry &p : *l) {
+                p.F[0] = 0.0;
+                p.F[2] = 0.0;
+                for (int i = 0; i < 3; i++) p.T[i] = 0.0;
+                p.Int_U[0] = 0.0;
+                p.Int_U[2] = 0.0;
+                for (int i = 0; i < 3; i++) p.Int_Omega[i] = 0.0;
+                p.F_CCF[0] = 0.0;
+                p.F_CCF[2] = 0.0;
+                for (int i = 0; i < 3; i++) p.T_CCF[i] = 0.0;
+            }
     for (IbmEntry &p : mobile) {
         const double int_rho = (p.rho_s > 0.0) ? p.M / p.rho_s : 0.0;   // Lagrangian_set_exact_solid_body_mass
         for (int i = 0; i < 3; i++) p.F[i] += p.F_CCF[i];
@@ -440,7 +501,7 @@ bool ibm_advance(std::vector<IbmEntry> &mobile, std::vector<IbmEntry> &fixed, co
                 for (int i = 0; i < 3; i++)
                     p.Omega[i] = p.Omega_old[i] + dt_iI * (2.0 * b * p.T[i] + gm * Fc + zt * Fc_old);
                 for (int i = 0; i < 3; i++) p.X[i] = p.X_old[i] + dts * b * (p.U[i] + p.U_old[i]);
-                twod_constraints(p, zs);
+                twod_constraints(p, zs, g.axisym != 0);
             }
             if (!relist(mobile, fixed, g, Cn, err)) return false;
             for (IbmEntry &p : mobile) {   // corrector
@@ -448,7 +509,7 @@ bool ibm_advance(std::vector<IbmEntry> &mobile, std::vector<IbmEntry> &fixed, co
                 for (int i = 0; i < 3; i++) p.U[i] = p.U_old[i] + dt_iM * b * (2.0 * p.F[i] + Fc + Fc_old);
                 for (int i = 0; i < 3; i++) p.Omega[i] = p.Omega_old[i] + dt_iI * b * (2.0 * p.T[i] + Fc + Fc_old);
                 for (int i = 0; i < 3; i++) p.X[i] = p.X_old[i] + dts * b * (p.U[i] + p.U_old[i]);
-                twod_constraints(p, zs);
+                twod_constraints(p, zs, g.axisym != 0);
             }
         }
     return true;
@@ -467,10 +528,30 @@ __device__ __forceinline__ double ibm_delta(double r)
     return 0;
 }
 
+// Interpolate_axis_index_for_sample / _for_spread (Interpolate.c:334-388):
+// across the symmetry axis (axis == IBM_AXIS_ODD for u faces, radial parity
+// odd; IBM_AXIS_EVEN for every other quantity) an index left of the axis
+// folds back onto its mirror cell, u with the sign flipped; the u face on the
+// axis itself maps to -1.  axis == IBM_AXIS_NONE: the identity.
+__device__ __forceinline__ int axis_fold(int i, int axis, int &sign)
+{
+    sign = 1;
+    if (axis == IBM_AXIS_NONE) return i;
+    if (i < 0) {
+        if (axis == IBM_AXIS_ODD) {
+            sign = -1;
+            return -i;
+        }
+        return -1 - i;
+    }
+    if (axis == IBM_AXIS_ODD && i == 0) return -1;
+    return i;
+}
+
 // Interpolate_Eul_to_Lag_twod (Interpolate.c:477-529): one marker per thread
 __global__ void k_ibm_interp(Dom d, const double *__restrict__ a, const double *__restrict__ xs,
                              const double *__restrict__ ys, double h, const double *__restrict__ XL,
-                             const double *__restrict__ YL, int nm, double *__restrict__ out)
+                             const double *__restrict__ YL, int nm, int axis, double *__restrict__ out)
 {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= nm) return;
@@ -486,8 +567,11 @@ __global__ void k_ibm_interp(Dom d, const double *__restrict__ a, const double *
     for (int j = j_start; j < j_end; j++) {
         const double r1 = YL[m] - ys[j];
         for (int i = i_start; i < i_end; i++) {
+            int parity;
+            const int ii = axis_fold(i, axis, parity);
+            if (ii < -NG || ii >= d.NX + NG) continue;
             const double r0 = XL[m] - xs[i];
-            A += 1 * AT_(a, i, j) * (ibm_delta(r0 / h) * ibm_delta(r1 / h));
+            A += parity * AT_(a, ii, j) * (ibm_delta(r0 / h) * ibm_delta(r1 / h));
         }
     }
     out[m] = A;
@@ -547,6 +631,7 @@ __global__ void __launch_bounds__(IBM_FORCE_THREADS) k_ibm_marker_force(IbmDev D
             for (int k = 0; k < n; k++) {
                 if (!sh_ok[k]) continue;
                 Fa -= sh_f[k];
+                if (D.axisym) continue;   // the torque is the planar spin's only (Lagrangian.c:2157-2159)
                 if (comp == 0) Ta += sh_t[k];
                 else Ta -= sh_t[k];
             }
@@ -566,6 +651,21 @@ __global__ void __launch_bounds__(IBM_FORCE_THREADS) k_ibm_marker_force(IbmDev D
 // k_ibm_marker_force; the reference clips the support to the interior, which
 // the cell already is); a cell outside a particle's box gets zero from it,
 // which leaves its sum as it is.
+// Interpolate_twod_cell_volume (Interpolate.c:288-312): the planar cell times
+// the slab; in the axisymmetric mode the full ring, dx dy theta_span r with r
+// the face radius for u and the cell-centre radius otherwise (xs), 2 pi times
+// half a cell on the axis
+__device__ __forceinline__ double ibm_cell_volume(const IbmDev &D, int comp, const double *xs, int i, int j)
+{
+    if (!D.axisym) return D.dxu1 * D.dyv[j] * D.slab;
+    (void)comp;
+    double radius = fabs(xs[i]);
+    if (radius < 1.0e-14) radius = 0.5 * D.dxu1;
+    double ring = D.theta_span * fabs(xs[i]);
+    if (ring < 1.0e-14) ring = (2.0 * 3.14159265358979323846) * radius;
+    return D.dxu1 * D.dyv[j] * ring;
+}
+
 __global__ void k_ibm_spread(Dom d, IbmDev D, int ne, int comp, const double *__restrict__ xs,
                              const double *__restrict__ ys, const double *__restrict__ rho, double *__restrict__ rhs)
 {
@@ -574,6 +674,11 @@ __global__ void k_ibm_spread(Dom d, IbmDev D, int ne, int comp, const double *__
     if (i >= d.NX || j >= d.NY) return;
     const int P = d.P;
     const double h = D.h;
+    // axisymmetric: the cell also takes the supports of its mirror index left
+    // of the axis, which the reference's scatter visits first (ascending i)
+    const int axis = D.axisym ? (comp == 0 ? IBM_AXIS_ODD : IBM_AXIS_EVEN) : IBM_AXIS_NONE;
+    const int im = axis == IBM_AXIS_ODD ? (i >= 1 ? -i : 1 << 30) : (axis == IBM_AXIS_EVEN ? -1 - i : 1 << 30);
+    const bool direct = !(axis == IBM_AXIS_ODD && i == 0);   // the axis face takes nothing
     double r = 0.0;
     bool touched = false;
     for (int e = 0; e < ne; e++) {
@@ -584,12 +689,18 @@ __global__ void k_ibm_spread(Dom d, IbmDev D, int ne, int comp, const double *__
             touched = true;
         }
         double temp = 0.0;
-        const double cellv = D.dxu1 * D.dyv[j] * D.slab;   // Interpolate_twod_cell_volume, planar
+        const double cellv = ibm_cell_volume(D, comp, xs, i, j);
         for (int q = p.moff; q < p.moff + p.mcount; q++) {
-            if ((unsigned)(i - D.sup_i[q]) >= 3u || (unsigned)(j - D.sup_j[q]) >= 3u) continue;
+            if ((unsigned)(j - D.sup_j[q]) >= 3u) continue;
             const double r1 = D.YL[q] - ys[j];
-            const double r0 = D.XL[q] - xs[i];
             const double dV = D.vol[q] / cellv;
+            if (axis != IBM_AXIS_NONE && (unsigned)(im - D.sup_i[q]) < 3u && im >= -NG) {
+                const double r0 = D.XL[q] - xs[im];
+                const double sgn = axis == IBM_AXIS_ODD ? -1.0 : 1.0;
+                temp += sgn * D.FL[q] * (ibm_delta(r0 / h) * ibm_delta(r1 / h)) * dV;
+            }
+            if (!direct || (unsigned)(i - D.sup_i[q]) >= 3u) continue;
+            const double r0 = D.XL[q] - xs[i];
             temp += 1 * D.FL[q] * (ibm_delta(r0 / h) * ibm_delta(r1 / h)) * dV;
         }
         const double rho_face = comp == 0 ? 0.5 * (AT_(rho, i, j) + AT_(rho, i - 1, j))
@@ -740,7 +851,14 @@ __global__ void __launch_bounds__(256) k_ibm_particle_sums(Dom d, IbmSumArgs A)
         for (int t = threadIdx.x; t < w * hgt; t += blockDim.x) {
             const int i = b[0] + t % w, j = b[2] + t / w;
             const double vf = face_solid_fraction(comp, i, j, X0, X1, R, A.xu, A.xc, A.yv, A.yc);
-            const double dV = A.h * d.m.dy_v[j] * A.slab;
+            double ring = A.slab;   // Interpolate_twod_cell_volume: slab, or the ring at the face radius
+            if (A.axisym) {
+                double radius = fabs(xn[i]);
+                if (radius < 1.0e-14) radius = 0.5 * A.h;
+                ring = A.theta_span * fabs(xn[i]);
+                if (ring < 1.0e-14) ring = (2.0 * 3.14159265358979323846) * radius;
+            }
+            const double dV = A.h * d.m.dy_v[j] * ring;
             const double dP = vf * AT_(vel, i, j) * dV;
             acc[comp] += dP;
             if (comp == 0) acc[2] += dP * (yn[j] - X1);
@@ -788,7 +906,9 @@ __global__ void __launch_bounds__(256) k_ibm_particle_sums(Dom d, IbmSumArgs A)
             const double term_l = gl[0] * ts[0] + gl[1] * ts[1] + gl[2] * ts[2];
             const double term_s = gs[0] * ns[0] + gs[1] * ns[1] + gs[2] * ns[2];
             const double f0 = A.sigma * term_l * term_s * tc[0], f1 = A.sigma * term_l * term_s * tc[1];
-            const double dV = d.m.dx_u[i] * d.m.dy_v[j] * A.slab;
+            // TwodOps_cell_measure_c (TwodOps.c:326-347)
+            const double dV = A.axisym ? d.m.dx_u[i] * d.m.dy_v[j] * d.m.ring_wt_c[i]
+                                       : d.m.dx_u[i] * d.m.dy_v[j] * A.slab;
             const double dF0 = f0 * dV, dF1 = f1 * dV;
             acc[4] += dF0;
             acc[5] += dF1;

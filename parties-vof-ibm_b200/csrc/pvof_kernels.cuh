@@ -183,6 +183,7 @@ struct IbmMarkers {
 struct IbmGrid {
     int NX, NY;
     int periodic[2];
+    int axisym;               // AXISYM_RZ: spheres on the axis, ring markers
     const double *xu, *yv, *xc, *yc;
     double h, dy_min, slab, twod_slab, Lx, Ly;
 };
@@ -205,8 +206,14 @@ struct IbmSumArgs {
     int np;
     double h, slab, sigma, ct, st, support_width;
     int nk, ccf;
+    int axisym;                          // ring measures, no in-plane spin
+    double theta_span;
     double *out;                         // 6 doubles per entry
 };
+
+// parity of a quantity across the symmetry axis for the marker gathers and
+// spreads (Interpolate.c:334-388): none (planar), odd (u faces), even
+constexpr int IBM_AXIS_NONE = 0, IBM_AXIS_ODD = 1, IBM_AXIS_EVEN = 2;
 
 struct IbmDev {
     const IbmEntryDev *ent;
@@ -217,6 +224,8 @@ struct IbmDev {
     double xlo, xhi, ylo, yhi;     // Lagrangian_local_point_2d bounds
     double h, dxu1, slab;
     const double *dyv;
+    int axisym;                    // fold supports across the axis, ring cell volumes
+    double theta_span;
 };
 
 void ibm_build(const std::vector<IbmEntry> &mobile_local, const std::vector<IbmEntry> &fixed_local, const IbmGrid &g,
@@ -253,10 +262,11 @@ struct MclView {
 __global__ void k_mcl_normals(Dom d, const double *xc, const double *yc, const double *CS, const double *plist,
                               int np, double support_width, double *nxo, double *nyo);
 __global__ void k_mcl_apply(Dom d, MclView v, const double *nxa, const double *nya, double *CLout);
+__global__ void k_mcl_axis_normals(Dom d, double *nx, double *ny);
 __global__ void k_mcl_extend_psi(Dom d, MclView v, const double *nxa, const double *nya, double *PSIout);
 
 __global__ void k_ibm_interp(Dom d, const double *a, const double *xs, const double *ys, double h, const double *XL,
-                             const double *YL, int nm, double *out);
+                             const double *YL, int nm, int axis, double *out);
 constexpr int IBM_FORCE_THREADS = 256;
 __global__ void k_ibm_marker_force(IbmDev D, int comp, double xs0, double ys0, double idt2beta, int reset);
 __global__ void k_ibm_spread(Dom d, IbmDev D, int ne, int comp, const double *xs, const double *ys, const double *rho,

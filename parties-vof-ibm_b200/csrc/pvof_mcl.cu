@@ -379,6 +379,23 @@ __global__ void k_mcl_normals(Dom d, const double *__restrict__ xc, const double
     mcl_normal_cell(d, xc, yc, CS, plist, np, support_width, nxo, nyo, i, j);
 }
 
+// VOF_DIFFUSE_compute_solid_normals_MCL and mcl_apply_normal_parity on the
+// symmetry axis (VOF_IBM_wetting.c:938-953, :1092-1099): the radial component
+// is zero in the first cell column, and the ghost columns mirror it, the
+// radial component with its sign flipped; one thread per row of the ghosted
+// plane
+__global__ void k_mcl_axis_normals(Dom d, double *__restrict__ nx, double *__restrict__ ny)
+{
+    const int j = -NG + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (j >= d.NY + NG) return;
+    const int P = d.P;
+    AT_(nx, 0, j) = 0.0;
+    for (int g = 1; g <= NG; ++g) {
+        AT_(nx, -g, j) = -AT_(nx, g - 1, j);
+        AT_(ny, -g, j) = AT_(ny, g - 1, j);
+    }
+}
+
 __global__ void k_mcl_apply(Dom d, MclView v, const double *__restrict__ nxa, const double *__restrict__ nya,
                             double *__restrict__ CLout)
 {

@@ -41,6 +41,15 @@ ST_NG = {"f_sigma_old_x": "FSIG_OLD_X", "f_sigma_old_y": "FSIG_OLD_Y"}
 TIGHT = dict(ch_tol=1e-13, ch_iter_max=600, CG_ETOL=1e-15, CG_MAXIT=400, P_CG_ETOL=1e-13, P_CG_MAXIT=1000)
 
 AXI_GRID = dict(NXM=24, NYM=48, rmax=1.0, zmax=2.0, radius=0.3, zc=0.7, Cn=0.04)
+# axisymmetric cases with a resolved sphere on the axis: the bubble's top
+# reaches into the sphere's diffuse shell
+AXI_GRID_IBM = dict(NXM=32, NYM=64, rmax=1.0, zmax=2.0, radius=0.3, zc=0.7, Cn=0.04)
+AXI_SPHERE = [(0, 0.0, 1.15, 0.2, 0.0, 0.0, 0.0, 2.5)]
+# In the axisymmetric mode the pressure residual sqrt(r.M^-1 r) stalls at
+# 2e-13 to 5e-13 (its rounding floor; the rows carry the weight r_c), where
+# 1e-13 would make the stopping iteration depend on rounding: the tight
+# axisymmetric cases stop the pressure solve at 1e-12, above that floor.
+AXI_TIGHT = dict(TIGHT, P_CG_ETOL=1e-12)
 
 # name, reference case, builder kwargs, steps, dt, snapshots kept (None = all)
 CASES = [
@@ -56,10 +65,10 @@ CASES = [
     # right-hand side carries the operator's row weight, oracle/ref/shim/axisym_rhs.c)
     ("axi_small", "axi2d", dict(_builder="rising_bubble", **AXI_GRID, velocity_seed=5, velocity_amp=0.1), 2, 1e-3,
      None),
-    ("axi_tight", "axi2d", dict(_builder="rising_bubble", **AXI_GRID, velocity_seed=3, velocity_amp=0.1, **TIGHT), 2,
+    ("axi_tight", "axi2d", dict(_builder="rising_bubble", **AXI_GRID, velocity_seed=3, velocity_amp=0.1, **AXI_TIGHT), 2,
      1e-3, ["s0", "s1_0", "s1_2", "s2_2"]),
     ("axi_st_tight", "axi2d_st", dict(_builder="rising_bubble", **AXI_GRID, surface_tension=True, We=200.0,
-                                      velocity_seed=21, velocity_amp=0.1, **TIGHT), 2, 1e-3,
+                                      velocity_seed=21, velocity_amp=0.1, **AXI_TIGHT), 2, 1e-3,
      ["s0", "s1_0", "s1_2", "s2_2"]),
 ]
 
@@ -77,6 +86,12 @@ LONG_CASES = [
 IBM_CASES = [
     ("ibm_small", dict(NXM=32, NYM=128, Lx=1.0, Ly=4.0, Cn=0.04, velocity_seed=7, velocity_amp=0.1),
      [(0, 0.06, 1.2, 0.2, 0.0, 0.0, 0.0, 2.5), (1, 0.55, 2.7, 0.15, 0.2, -0.1, 0.7, 2.5)], 1e-3, 1),
+    # axisymmetric (ibm_axi_st build): a fixed sphere on the axis cutting the
+    # top of a bubble, its ring markers folded across the axis by the gathers
+    # and spreads
+    ("ibm_axi_small", dict(_builder="rising_bubble", _refcase="ibm_axi_st", **AXI_GRID_IBM, surface_tension=True,
+                           We=200.0, velocity_seed=7, velocity_amp=0.1, _theta=90.0),
+     AXI_SPHERE, 1e-3, 1),
 ]
 
 # contact-line cases (oracle/ref/ibm_driver.c "mcl" mode on the ibm2d build):
@@ -93,7 +108,13 @@ MCL_CASES = [("mcl_theta60", MCL_GRID, MCL_PARTICLES, 60.0),
              # next to the bottom wall, so the characteristics cross it
              ("mcl_fs_theta45", dict(NXM=48, NYM=48, Lx=1.0, Ly=1.0, Cn=0.04, y0=0.12, amp=0.02,
                                      wall_y=abi.WALL_FREESLIP, _refcase="ibm2d_fs"),
-              [(0, 0.5, 0.13, 0.1, 0.0, 0.0, 0.0, 2.5), (0, 0.03, 0.15, 0.08, 0.0, 0.0, 0.0, 2.5)], 45.0)]
+              [(0, 0.5, 0.13, 0.1, 0.0, 0.0, 0.0, 2.5), (0, 0.03, 0.15, 0.08, 0.0, 0.0, 0.0, 2.5)], 45.0),
+             # axisymmetric: the sphere on the axis in the bubble's top, the
+             # characteristics folded at the axis
+             ("mcl_axi_theta60", dict(_builder="rising_bubble", _refcase="ibm_axi_st", **AXI_GRID_IBM), AXI_SPHERE,
+              60.0),
+             ("mcl_axi_theta120", dict(_builder="rising_bubble", _refcase="ibm_axi_st", **AXI_GRID_IBM), AXI_SPHERE,
+              120.0)]
 
 # whole time steps with resolved cylinders (oracle/ref/ibm_driver.c "steps"
 # mode): name, reference build, builder arguments, particles, contact angle,
@@ -110,6 +131,11 @@ IBM_STEP_CASES = [
                                       velocity_seed=13, velocity_amp=0.1, **TIGHT), IBM_STEP_PARTICLES, 60.0, 2, 1e-3),
     ("ibm_steps", "ibm2d", dict(NXM=32, NYM=64, Lx=1.0, Ly=2.0, Cn=0.04, velocity_seed=17, velocity_amp=0.1, **TIGHT),
      IBM_STEP_PARTICLES, 120.0, 2, 1e-3),
+    # axisymmetric: the static sphere on the axis in the top of a bubble
+    # (the bubble-and-sphere benchmark case in small), surface tension
+    ("ibm_axi_steps_st", "ibm_axi_st", dict(_builder="rising_bubble", **AXI_GRID_IBM, surface_tension=True, We=200.0,
+                                            velocity_seed=23, velocity_amp=0.1, **AXI_TIGHT), AXI_SPHERE, 90.0, 2,
+     1e-3),
 ]
 
 # constant-density FFT Poisson cases (oracle/ref/fft_driver.c on the fft2d build):
@@ -146,10 +172,22 @@ def g_range(grid, plane, ng):
     return plane[G:G + NY, G:G + NX]
 
 
-def make(name, refcase, kw, steps, dt, keep, outdir, refsrc=None):
+def build_case(kw):
+    """(grid, params, planes, reference build) of a builder-kwargs dict whose
+    optional keys _builder (a pvof.cases function, default rayleigh_taylor)
+    and _refcase (default None) select the case."""
     build = dict(kw)
     builder = getattr(cases, build.pop("_builder", "rayleigh_taylor"))
+    refcase = build.pop("_refcase", None)
+    theta = build.pop("_theta", None)
     grid, params, planes = builder(**build)
+    if theta is not None:
+        params.contact_angle_deg = theta
+    return grid, params, planes, refcase
+
+
+def make(name, refcase, kw, steps, dt, keep, outdir, refsrc=None):
+    grid, params, planes, _ = build_case(kw)
     if not os.path.exists(po.ref_binary(refcase)):
         po.build_reference(refcase, refsrc)
     with tempfile.TemporaryDirectory() as wd:
@@ -203,14 +241,15 @@ def make_long(name, refcase, kw, steps, dt, outdir, refsrc=None):
 
 
 def make_ibm(name, kw, particles, dt, stage, outdir, refsrc=None):
-    grid, params, planes = cases.rayleigh_taylor(**kw)
-    if not os.path.exists(po.ref_binary("ibm2d")):
-        po.build_reference("ibm2d", refsrc)
+    grid, params, planes, refcase = build_case(kw)
+    refcase = refcase or "ibm2d"
+    if not os.path.exists(po.ref_binary(refcase)):
+        po.build_reference(refcase, refsrc)
     fixed = [p[1:7] for p in particles if not p[0]]
     mobile = [p[1:7] for p in particles if p[0]]
     data = {}
     with tempfile.TemporaryDirectory() as wd:
-        cp = po.run_reference_ibm(wd, grid, params, planes, fixed, mobile, dt, stage)
+        cp = po.run_reference_ibm(wd, grid, params, planes, fixed, mobile, dt, stage, case=refcase)
         for fname in ["C_S", "C_L", "rho", "mu", "u", "v"]:
             data["i0/" + fname] = po.read_reference_field(wd, "i0", fname, grid)
         for tag, rhs in (("r0", True), ("r1", False), ("r2", True), ("r3", False), ("r4", True)):
@@ -230,7 +269,7 @@ def make_ibm(name, kw, particles, dt, stage, outdir, refsrc=None):
     for k, v in planes.items():
         data["init/" + k] = v
     meta = {"grid": struct_to_dict(grid), "params": struct_to_dict(params), "dt": dt, "stage": stage,
-            "particles": [list(p) for p in particles], "builder": kw, "refcase": "ibm2d"}
+            "particles": [list(p) for p in particles], "builder": kw, "refcase": refcase}
     data["meta"] = np.array(repr(meta))
     path = os.path.join(outdir, name + ".npz")
     np.savez_compressed(path, **data)
@@ -238,9 +277,9 @@ def make_ibm(name, kw, particles, dt, stage, outdir, refsrc=None):
 
 
 def make_mcl(name, kw, particles, theta, outdir, refsrc=None):
-    build = dict(kw)
-    refcase = build.pop("_refcase", "ibm2d")
-    grid, params, planes = cases.rayleigh_taylor(**build)
+    grid, params, planes, refcase = build_case(kw)
+    refcase = refcase or "ibm2d"
+    build = {k: v for k, v in kw.items() if k != "_refcase"}
     params.contact_angle_deg = theta
     if not os.path.exists(po.ref_binary(refcase)):
         po.build_reference(refcase, refsrc)
@@ -264,7 +303,7 @@ def make_mcl(name, kw, particles, theta, outdir, refsrc=None):
 
 
 def make_ibm_steps(name, refcase, kw, particles, theta, steps, dt, outdir, refsrc=None):
-    grid, params, planes = cases.rayleigh_taylor(**kw)
+    grid, params, planes, _ = build_case(kw)
     params.contact_angle_deg = theta
     if not os.path.exists(po.ref_binary(refcase)):
         po.build_reference(refcase, refsrc)

@@ -3,9 +3,10 @@ against the reference's own routines (fixture tests/golden/ibm_small.npz,
 made by oracle/ref/ibm_driver.c on the reference build with VOF_IBM and
 LAG_PARTICLE_RESOLVED).
 
-The case has a fixed cylinder crossing the periodic x boundary (so the list
-update adds a periodic copy that carries markers) and a mobile cylinder with
-velocity and spin.  Each routine gets the reference's inputs and is compared
+The planar case has a fixed cylinder crossing the periodic x boundary (so the
+list update adds a periodic copy that carries markers) and a mobile cylinder
+with velocity and spin; the axisymmetric case (ibm_axi_small, the ibm_axi_st
+build) a fixed sphere on the symmetry axis in the top of a bubble.  Each routine gets the reference's inputs and is compared
 with the reference's outputs:
 
   markers and flags        Lagrangian_flag_points        bit for bit
@@ -47,9 +48,12 @@ def assert_same(a, b, what, tol=0.0):
     assert err <= tol * scale, "%s: max abs diff %.3e (scale %.3e)" % (what, err, scale)
 
 
-@pytest.fixture(scope="module")
-def case():
-    return load_golden("ibm_small")
+@pytest.fixture(scope="module", params=["ibm_small", "ibm_axi_small"])
+def case(request):
+    """ibm_small: planar cylinders; ibm_axi_small: a sphere on the symmetry
+    axis of an axisymmetric case (ring markers, supports folded across the
+    axis, ring cell volumes)."""
+    return load_golden(request.param)
 
 
 def test_solid_fraction_matches_reference(case):
