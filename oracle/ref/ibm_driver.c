@@ -219,24 +219,39 @@ static void run_steps(Cart3d_bag *db, int nsteps, double dt, Debug_trace *dtrace
     const double BET2[] = {BETA2};
     double time = 0.0;
     params->time = 0.0;
+#if defined(PVOF_BRIDGE_DRIVER) && PVOF_BRIDGE_DRIVER == 1
+    /* the device takes the case from here: its start-up sets the particle
+     * velocities and paints them (Particle_initialize_velocities) itself */
+    (void)dtrace;
+    bridge_check(pvof_bridge_start(db, 0), "pvof_bridge_start");
+    bridge_check(pvof_bridge_download(db), "pvof_bridge_download");
+#else
     /* Cart3d.c:505-515, then the cell-centred velocity of Temporal_int.c:194 */
     Particle_initialize_velocities(db, DTRACE("Particle_initialize_velocities"));
     Velocity_cell_center(db);
+#endif
     dump_state(db, "s0");
     dump_particles(db, "s0");
     double t0 = MPI_Wtime(), t_io = 0.0;
     for (int n = 1; n <= nsteps; n++) {
         for (int rk = 0; rk < 3; rk++) {
-            if (time != 0 && rk == 0)
-                Velocity_cell_center(db);
             params->which_stage = rk;
             params->dt = dt;
+#if defined(PVOF_BRIDGE_DRIVER) && PVOF_BRIDGE_DRIVER == 1
+            bridge_check(pvof_bridge_substep(db), "pvof_bridge_substep");
+#else
+            if (time != 0 && rk == 0)
+                Velocity_cell_center(db);
             Temporal_int_all_the_equations(db, DTRACE("Temporal_int_all_the_equations"));
+#endif
             time += dt * BET2[rk];
             params->time = time;
         }
         params->ntime = n;
         double a = MPI_Wtime();
+#if defined(PVOF_BRIDGE_DRIVER) && PVOF_BRIDGE_DRIVER == 1
+        bridge_check(pvof_bridge_download(db), "pvof_bridge_download");
+#endif
         char tag[64];
         snprintf(tag, sizeof(tag), "s%d", n);
         dump_state(db, tag);

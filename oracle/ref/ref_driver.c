@@ -22,7 +22,22 @@
  *   block of the field (L ranges, [k][j][i], i fastest); "substeps" > 0 also
  *   dumps after every RK substep as s<step>_<rk>_<field>.bin.
  * The timing line "REF_TIMING steps=<n> cells=<c> seconds=<t>" covers the
- * step loop only, after the first <warmup> steps (default 0).  Test infrastructure only.
+ * step loop only, after the first <warmup> steps (default 0).
+ *
+ * Built with -DPVOF_BRIDGE_DRIVER (oracle/ref/Makefile, BRIDGE=substep or
+ * BRIDGE=routines) the same program drives the B200 library through the
+ * PARTIES-side bridge (parties-vof-ibm_b200/bridge/pvof_bridge.c):
+ *   PVOF_BRIDGE_DRIVER == 1: after the reference's start-up, pvof_bridge_start
+ *     hands the case to the device, and every substep is pvof_bridge_substep
+ *     in place of Velocity_cell_center + Temporal_int_all_the_equations (the
+ *     drop-in of the whole substep); the fields are brought back with
+ *     pvof_bridge_download before every dump;
+ *   PVOF_BRIDGE_DRIVER == 2: the reference's routines that the bridge
+ *     defines under their own names (PVOF_BRIDGE_ROUTINES) replace the
+ *     reference's CPU definitions (made weak in this build), and the
+ *     reference's own start-up and Temporal_int_all_the_equations run
+ *     unchanged around them.
+ * Test infrastructure only.
  */
 #include "DataTypes.h"
 #include "definitions.h"
@@ -44,6 +59,17 @@
 #include <string.h>
 #include <unistd.h>
 #include <sys/stat.h>
+
+#ifdef PVOF_BRIDGE_DRIVER
+#include "pvof_bridge.h"
+static void bridge_check(int rc, const char *what)
+{
+    if (rc < 0) {
+        fprintf(stderr, "ref_driver: %s: %s\n", what, pvof_last_error());
+        exit(3);
+    }
+}
+#endif
 
 static void die(const char *msg)
 {
@@ -161,6 +187,11 @@ int main(int argc, char **argv)
     if ((plane = read_plane("init_u.bin", NX * NY))) { inject(db->u->data, plane, grid); free(plane); }
     if ((plane = read_plane("init_v.bin", NX * NY))) { inject(db->v->data, plane, grid); free(plane); }
     if ((plane = read_plane("init_p.bin", NX * NY))) { inject(db->p->p_data, plane, grid); free(plane); }
+#if defined(PVOF_BRIDGE_DRIVER) && PVOF_BRIDGE_DRIVER == 2
+    /* the bridged routines below work on the device copy from here on */
+    params->dt = dt;
+    bridge_check(pvof_bridge_start(db, 0), "pvof_bridge_start");
+#endif
 
     Velocity_update_boundaries(db->u->data, 'u', VEL_TYPE_NORMAL, db);
     Velocity_update_boundaries(db->v->data, 'v', VEL_TYPE_NORMAL, db);
@@ -183,6 +214,10 @@ int main(int argc, char **argv)
 #endif
     /* cell-centred velocity for the first substep (Temporal_int.c:420-424) */
     Velocity_cell_center(db);
+#if defined(PVOF_BRIDGE_DRIVER) && PVOF_BRIDGE_DRIVER == 1
+    bridge_check(pvof_bridge_start(db, 0), "pvof_bridge_start");
+    bridge_check(pvof_bridge_download(db), "pvof_bridge_download");
+#endif
 
     dump_state(db, "s0");
 
@@ -197,15 +232,22 @@ int main(int argc, char **argv)
             t_io = 0.0;
         }
         for (int rk = 0; rk < 3; rk++) {
-            if (time != 0 && rk == 0)
-                Velocity_cell_center(db);
             params->which_stage = rk;
             params->dt = dt;
+#if defined(PVOF_BRIDGE_DRIVER) && PVOF_BRIDGE_DRIVER == 1
+            bridge_check(pvof_bridge_substep(db), "pvof_bridge_substep");
+#else
+            if (time != 0 && rk == 0)
+                Velocity_cell_center(db);
             Temporal_int_all_the_equations(db, DTRACE("Temporal_int_all_the_equations"));
+#endif
             time += dt * BET2[rk];
             params->time = time;
             if (dump_substeps > 0 && dump_every > 0 && n % dump_every == 0) {
                 double a = MPI_Wtime();
+#if defined(PVOF_BRIDGE_DRIVER) && PVOF_BRIDGE_DRIVER == 1
+                bridge_check(pvof_bridge_download(db), "pvof_bridge_download");
+#endif
                 char tag[64];
                 snprintf(tag, sizeof(tag), "s%d_%d", n, rk);
                 dump_state(db, tag);
@@ -215,6 +257,9 @@ int main(int argc, char **argv)
         params->ntime = n;
         if (dump_every > 0 && n % dump_every == 0) {
             double a = MPI_Wtime();
+#if defined(PVOF_BRIDGE_DRIVER) && PVOF_BRIDGE_DRIVER == 1
+            bridge_check(pvof_bridge_download(db), "pvof_bridge_download");
+#endif
             char tag[64];
             snprintf(tag, sizeof(tag), "s%d", n);
             dump_state(db, tag);

@@ -232,6 +232,7 @@ def make_long(name, refcase, kw, steps, dt, outdir, refsrc=None):
             a = g_range(grid, po.read_reference_field(wd, tag, fname, grid), False)
             data["%s/%s" % (tag, pname)] = a[:NY - 1, :NX - 1]
         data["iterations"] = parse_iterations(cp.stdout)
+    # the initial planes are the builder's (deterministic); they are not stored
     meta = {"grid": struct_to_dict(grid), "params": struct_to_dict(params), "steps": steps, "dt": dt,
             "refcase": refcase, "builder": kw, "physical_only": True}
     data["meta"] = np.array(repr(meta))
