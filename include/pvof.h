@@ -333,7 +333,9 @@ int pvof_Lagrangian_force(pvof_ctx *ctx, int force_iter);
 
 /* --- learned warm start (no counterpart in the reference) --------------- */
 /* The network: six 3x3 convolutions 3 -> 32 -> 32 -> 32 -> 32 -> 32 -> 1,
- * zero padding, ReLU between them, BF16 weights with FP32 accumulation.
+ * zero padding, ReLU between them, BF16 weights with FP32 accumulation; the
+ * four hidden 32 -> 32 layers run on the tensor cores with BF16 activations
+ * (their input gradients too).
  * Parameters are one flat FP32 array [w0, b0, ..., w5, b5], w_l laid out
  * [cout][cin][3][3]; planes are channel-major [C][H][W] floats on the device.
  * Inputs: rho, rhs / rms(rhs), phi_prev / rms(phi_prev); output: the change
@@ -356,6 +358,17 @@ int pvof_cnn_adam(float *params, const float *grad, float *m, float *v, uint16_t
                   void *stream);
 /* the BF16 copy of FP32 parameters */
 int pvof_cnn_to_bf16(const float *params, uint16_t *params_bf16, void *stream);
+/* one hidden-layer convolution on the tensor cores, as the network runs it:
+ * y[co] = b[co] + sum_ci sum_tap w[co][ci][tap] x[ci][p + tap] (zero outside
+ * the H x W plane) with x rounded to BF16, w in BF16 ([32][32][3][3]), FP32
+ * accumulation, then the ReLU if relu; x, y: 32 planes [32][H][W]; b may be
+ * NULL */
+int pvof_cnn_conv32(const float *x, const uint16_t *w_bf16, const float *b, float *y, int H, int W, int relu,
+                    void *stream);
+/* waits for the stream; PVOF_ECUDA (and the flag cleared) if a tensor-core
+ * convolution since the last call gave up waiting for its matrix
+ * multiplications, else 0 */
+int pvof_cnn_status(void *stream);
 /* the network the context's pressure_warm_start == 2 uses (host array of
  * pvof_cnn_param_count() floats) */
 int pvof_set_pressure_network(pvof_ctx *ctx, const float *params, size_t n);

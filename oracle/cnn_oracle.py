@@ -3,7 +3,11 @@
 The same fixed network as parties-vof-ibm_b200/csrc/pvof_cnn.cu: six 3x3
 convolutions 3 -> 32 -> 32 -> 32 -> 32 -> 32 -> 1 with zero padding and ReLU
 between them; weights rounded to BF16 (round to nearest even) for the
-forward and backward passes, biases in FP32; here every sum is in FP64.
+forward and backward passes, biases in FP32; the four hidden 32 -> 32 layers
+(TC_LAYERS, the tensor-core layers of the CUDA code) also take their input
+activations, and in the backward pass the output gradient of their input
+convolution, rounded to BF16 (through FP32, as the device holds them); here
+every sum is in FP64.
 Parameters are one flat array [w0, b0, ..., w5, b5], w_l laid out
 [cout][cin][3][3]; planes are channel-major [C][H][W].
 
@@ -15,6 +19,7 @@ import numpy as np
 CIN = 3
 CMAX = 32
 LAYERS = 6
+TC_LAYERS = (1, 2, 3, 4)   # 32 -> 32: BF16 operands on the device's tensor cores
 
 
 def shapes():
@@ -41,6 +46,12 @@ def unpack(params):
         off += co
         out.append((w, b))
     return out
+
+
+def bf16_operand(a):
+    """An FP64 activation plane as the tensor cores take it: to FP32, then to
+    the nearest BF16, back in FP64."""
+    return to_bf16(np.asarray(a, dtype=np.float32)).astype(np.float64)
 
 
 def to_bf16(a):
@@ -76,22 +87,26 @@ def conv(x, w, b):
     return out
 
 
-def forward(params, x):
-    """Output (H, W) and the activations of every layer (after ReLU)."""
+def forward(params, x, tc_bf16=True):
+    """Output (H, W) and the activations of every layer (after ReLU).
+    tc_bf16=False keeps the hidden layers' activations unrounded (the smooth
+    function whose gradient finite differences can check)."""
     acts = []
     a = np.asarray(x, dtype=np.float64)
     for l, (w, b) in enumerate(unpack(params)):
-        a = conv(a, to_bf16(w).astype(np.float64), b)
+        a = conv(bf16_operand(a) if (tc_bf16 and l in TC_LAYERS) else a, to_bf16(w).astype(np.float64), b)
         if l < LAYERS - 1:
             a = np.maximum(a, 0.0)
         acts.append(a)
     return a[0], acts
 
 
-def backward(params, x, dy):
-    """Gradient of sum(dy * y) with respect to the flat parameters."""
+def backward(params, x, dy, tc_bf16=True):
+    """Gradient of sum(dy * y) with respect to the flat parameters; with
+    tc_bf16 the device's: the BF16 rounding of the hidden layers' operands is
+    passed straight through."""
     layers = unpack(params)
-    _, acts = forward(params, x)
+    _, acts = forward(params, x, tc_bf16)
     grads = [None] * LAYERS
     g = np.asarray(dy, dtype=np.float64)[None]
     for l in range(LAYERS - 1, -1, -1):
@@ -100,6 +115,8 @@ def backward(params, x, dy):
         if l < LAYERS - 1:
             g = g * (acts[l] > 0.0)
         inp = np.asarray(x, dtype=np.float64) if l == 0 else acts[l - 1]
+        if tc_bf16 and l in TC_LAYERS:
+            inp = bf16_operand(inp)
         ci, H, W = inp.shape
         ip = np.pad(inp, ((0, 0), (1, 1), (1, 1)))
         gw = np.zeros(wb.shape)
@@ -109,7 +126,7 @@ def backward(params, x, dy):
         grads[l] = (gw, g.sum(axis=(1, 2)))
         if l > 0:   # the input gradient: the transposed convolution
             wt = wb[:, :, ::-1, ::-1].transpose(1, 0, 2, 3)
-            g = conv(g, wt, None)
+            g = conv(bf16_operand(g) if (tc_bf16 and l in TC_LAYERS) else g, wt, None)
     return np.concatenate([np.concatenate([gw.ravel(), gb]) for gw, gb in grads])
 
 

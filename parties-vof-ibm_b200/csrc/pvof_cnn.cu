@@ -15,12 +15,15 @@
 // warm start takes the Galerkin step along it from phi_prev (k_cnn_apply);
 // training target t = (phi - phi_prev) / rms(phi_prev).
 //
-// Kernels: a shared-memory tiled direct convolution (one thread per pixel,
-// all output channels in registers, the tile and the layer's weights in
-// shared memory), its input gradient as the same convolution with the taps
-// flipped and the channels swapped, the weight gradient as per-block partial
-// sums, the mean-square loss, Adam, and the input assembly with the two root
-// mean squares.
+// Kernels: the four hidden 32 -> 32 layers run on the tensor cores
+// (k_conv_umma: tcgen05.mma implicit GEMM, BF16 activations and weights, FP32
+// accumulation in tensor memory), forward and input gradient; the first
+// (3 -> 32) and last (32 -> 1) layers, too narrow for an MMA tile, are a
+// shared-memory tiled direct convolution on the FP32 pipes (one thread per
+// pixel, all output channels in registers); the input gradient is the same
+// convolution with the taps flipped and the channels swapped, the weight
+// gradient per-block partial sums; then the mean-square loss, Adam, and the
+// input assembly with the two root mean squares.
 #include <cuda_bf16.h>
 #include <cstdint>
 #include <cstring>
@@ -79,6 +82,166 @@ __global__ void __launch_bounds__(CNN_TILE * CNN_TILE) k_conv3x3(const float *__
     }
 }
 
+// ---------------------------------------------------------------------------
+// 32 -> 32 channel 3x3 convolutions on the tensor cores (tcgen05, kind::f16)
+// ---------------------------------------------------------------------------
+// An implicit GEMM D[p][co] = sum_k A[p][k] B[co][k] over k = tap * 32 + ci
+// (288 = 18 MMAs of K = 16): one CTA of 128 threads takes 128 consecutive
+// pixels of the flattened H x W plane (the MMA's M = 128, N = 32).  Every
+// thread gathers its pixel's im2col row, rounded to BF16, into shared memory,
+// the CTA the layer's BF16 weights; both in the K-major canonical layout
+// without swizzle (core matrices of 8 rows x 16 bytes: rows 16 bytes apart,
+// the two K halves of an MMA 128 bytes apart, groups of 8 rows 256 bytes
+// apart).  One thread issues the 18 MMAs into a 128 x 32 FP32 accumulator in
+// tensor memory and commits them to an mbarrier; each warp then reads its 32
+// rows (pixels) back with tcgen05.ld and writes the 32 channels, plus the
+// bias and the ReLU.  The input-gradient convolution of the same layers is
+// this kernel with the flipped, transposed weights.
+constexpr int UM_M = 128;                          // pixels per CTA (MMA M)
+constexpr int UM_N = 32;                           // output channels (MMA N)
+constexpr int UM_KSTEPS = 9 * CNN_CMAX / 16;       // 18 MMAs of K = 16
+constexpr int UM_A_STEP = UM_M * 16 * 2;           // bytes of A per MMA: 4096
+constexpr int UM_B_STEP = UM_N * 16 * 2;           // bytes of B per MMA: 1024
+constexpr size_t UM_SMEM = (size_t)UM_KSTEPS * (UM_A_STEP + UM_B_STEP) + 1024;   // + alignment slack
+constexpr long long UM_WAIT_LIMIT = 1LL << 26;     // bounded wait on the MMAs' mbarrier
+
+// tcgen05.mma instruction descriptor: D F32 (bits 4-5 = 1), A and B BF16
+// (bits 7-9, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at bits
+// 17-22, M >> 4 at bits 24-28
+constexpr uint32_t UM_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(UM_N >> 3) << 17) |
+                              ((uint32_t)(UM_M >> 4) << 24);
+
+// shared-memory matrix descriptor of a K-major operand without swizzle:
+// start address, leading (K) and stride (8-row group) byte offsets, each in
+// 16-byte units; version 1 at bit 46; layout type 0 (no swizzle) at bits 61-63
+__device__ __forceinline__ uint64_t um_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ uint32_t um_pack(float a, float b)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);   // a in the low half: the lower address
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+__global__ void __launch_bounds__(UM_M) k_conv_umma(const float *__restrict__ in, const __nv_bfloat16 *__restrict__ w,
+                                                    const float *__restrict__ b, float *__restrict__ out, int H, int W,
+                                                    int relu, int *__restrict__ err)
+{
+    extern __shared__ unsigned char um_raw[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_holder;
+    unsigned char *As = reinterpret_cast<unsigned char *>(((uintptr_t)um_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char *Bs = As + UM_KSTEPS * UM_A_STEP;
+    const int t = threadIdx.x, warp = t >> 5;
+    const long long plane = (long long)H * W;
+    const long long p = (long long)blockIdx.x * UM_M + t;
+    const bool live = p < plane;
+    const int y = live ? (int)(p / W) : 0, x = live ? (int)(p % W) : 0;
+    const uint32_t mbar_a = (uint32_t)__cvta_generic_to_shared(&mbar);
+
+    if (warp == 0) {   // 32 columns of tensor memory: the 128 x 32 FP32 accumulator
+        const uint32_t holder = (uint32_t)__cvta_generic_to_shared(&tmem_holder);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(holder) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // A: the pixel's im2col row, 16 input channels of one tap per MMA
+#pragma unroll 1
+    for (int s = 0; s < UM_KSTEPS; s++) {
+        const int tap = s >> 1, c0 = (s & 1) * 16;
+        const int xx = x + tap % 3 - 1, yy = y + tap / 3 - 1;
+        const bool ok = live && xx >= 0 && xx < W && yy >= 0 && yy < H;
+        const size_t at = ok ? (size_t)c0 * (size_t)plane + (size_t)yy * W + xx : 0;
+        uint32_t pk[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const float v0 = ok ? in[at + (size_t)(2 * e) * (size_t)plane] : 0.0f;
+            const float v1 = ok ? in[at + (size_t)(2 * e + 1) * (size_t)plane] : 0.0f;
+            pk[e] = um_pack(v0, v1);
+        }
+        unsigned char *row = As + s * UM_A_STEP + (t >> 3) * 256 + (t & 7) * 16;
+        *reinterpret_cast<uint4 *>(row) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        *reinterpret_cast<uint4 *>(row + 128) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+    }
+    // B: w[co][ci][tap] as rows co of K = tap * 32 + ci, 16-byte chunks (step, co, half)
+    for (int q = t; q < UM_KSTEPS * UM_N * 2; q += UM_M) {
+        const int s = q >> 6, co = (q >> 1) & 31, half = q & 1;
+        const int tap = s >> 1, c0 = (s & 1) * 16 + half * 8;
+        uint16_t v[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const __nv_bfloat16 wv = w[(co * CNN_CMAX + c0 + e) * 9 + tap];
+            v[e] = *reinterpret_cast<const uint16_t *>(&wv);
+        }
+        unsigned char *dst = Bs + s * UM_B_STEP + (co >> 3) * 256 + half * 128 + (co & 7) * 16;
+        *reinterpret_cast<uint4 *>(dst) = make_uint4(v[0] | ((uint32_t)v[1] << 16), v[2] | ((uint32_t)v[3] << 16),
+                                                     v[4] | ((uint32_t)v[5] << 16), v[6] | ((uint32_t)v[7] << 16));
+    }
+    // the generic-proxy stores above become visible to the tensor cores' async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_holder;
+    if (t == 0) {
+        const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(As), b0 = (uint32_t)__cvta_generic_to_shared(Bs);
+#pragma unroll 1
+        for (int s = 0; s < UM_KSTEPS; s++) {
+            const uint64_t ad = um_desc(a0 + s * UM_A_STEP, 128, 256), bd = um_desc(b0 + s * UM_B_STEP, 128, 256);
+            const uint32_t acc = s > 0 ? 1u : 0u;
+            asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                         ::"r"(tmem), "l"(ad), "l"(bd), "r"(UM_IDESC), "r"(acc) : "memory");
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar_a)
+                     : "memory");
+    }
+    // bounded wait for the MMAs (phase 0 of the mbarrier)
+    int done = 0;
+    for (long long it = 0; it < UM_WAIT_LIMIT && !done; it++) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(ok) : "r"(mbar_a), "r"(0u) : "memory");
+        done = (int)ok;
+    }
+    done = __syncthreads_and(done);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (done) {
+        uint32_t r[32];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                     "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+                     "%30, %31}, [%32];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                       "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                       "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+                       "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+                       "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                     : "r"(taddr)
+                     : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (live) {
+#pragma unroll
+            for (int co = 0; co < UM_N; co++) {
+                float v = __uint_as_float(r[co]) + (b ? b[co] : 0.0f);
+                if (relu && v < 0.0f) v = 0.0f;
+                out[(size_t)co * (size_t)plane + (size_t)p] = v;
+            }
+        }
+    } else if (t == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
+}
+
 // the weights of the input-gradient convolution: wt[ci][co][8 - tap] = w[co][ci][tap]
 __global__ void k_conv_transpose_weights(const __nv_bfloat16 *__restrict__ w, __nv_bfloat16 *__restrict__ wt,
                                          int cout, int cin)
@@ -101,7 +264,7 @@ __global__ void k_relu_back(float *__restrict__ dy, const float *__restrict__ y,
 // (co, cin) sums dY[co][p] for the bias
 __global__ void __launch_bounds__(256) k_conv_wgrad(const float *__restrict__ in, int cin,
                                                     const float *__restrict__ dy, int H, int W,
-                                                    float *__restrict__ dw, float *__restrict__ db)
+                                                    float *__restrict__ dw, float *__restrict__ db, int bf16_in)
 {
     const int co = blockIdx.y, ci = blockIdx.x;
     const size_t plane = (size_t)H * W;
@@ -122,7 +285,11 @@ __global__ void __launch_bounds__(256) k_conv_wgrad(const float *__restrict__ in
 #pragma unroll
         for (int t = 0; t < 9; t++) {
             const int a = i + t % 3 - 1, c = j + t / 3 - 1;
-            if (a >= 0 && a < W && c >= 0 && c < H) acc[t] += x[(size_t)c * W + a] * gv;
+            if (a >= 0 && a < W && c >= 0 && c < H) {
+                float xv = x[(size_t)c * W + a];
+                if (bf16_in) xv = __bfloat162float(__float2bfloat16(xv));   // the tensor-core layers' operand
+                acc[t] += xv * gv;
+            }
         }
     }
     __shared__ float red[8][9];
@@ -223,9 +390,25 @@ size_t work_floats(int H, int W)
 
 size_t conv_smem(int cin, int cout) { return sizeof(float) * ((size_t)cin * CNN_HALO * CNN_HALO + (size_t)cout * cin * 9); }
 
+__device__ int g_cnn_err;   // set when a tensor-core convolution gave up waiting for its MMAs
+
 int conv(const float *in, int cin, const __nv_bfloat16 *w, const float *b, float *out, int cout, int H, int W, int relu,
          cudaStream_t st)
 {
+    if (cin == CNN_CMAX && cout == CNN_CMAX) {   // the hidden layers: tensor cores
+        static bool um_attr = false;
+        if (!um_attr) {
+            if (cudaFuncSetAttribute(k_conv_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UM_SMEM) !=
+                cudaSuccess)
+                return -1;
+            um_attr = true;
+        }
+        int *err = nullptr;
+        if (cudaGetSymbolAddress((void **)&err, g_cnn_err) != cudaSuccess) return -1;
+        const long long n = (long long)H * W;
+        k_conv_umma<<<(unsigned)((n + UM_M - 1) / UM_M), UM_M, UM_SMEM, st>>>(in, w, b, out, H, W, relu, err);
+        return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    }
     static bool attr = false;
     if (!attr) {
         if (cudaFuncSetAttribute(k_conv3x3<CNN_CMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -414,8 +597,10 @@ int pvof_cnn_backward(const float *params, const uint16_t *params_bf16, const fl
             const size_t n = (size_t)L[l].cout * plane;
             k_relu_back<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, work + (size_t)l * CNN_CMAX * plane, n);
         }
+        const int tc = L[l].cin == CNN_CMAX && L[l].cout == CNN_CMAX;   // a tensor-core layer: BF16 inputs
         k_conv_wgrad<<<dim3((unsigned)L[l].cin + 1, (unsigned)L[l].cout), 256, 0, st>>>(lin, L[l].cin, g, H, W,
-                                                                                          grad + L[l].w, grad + L[l].b);
+                                                                                          grad + L[l].w, grad + L[l].b,
+                                                                                          tc);
         if (l > 0) {   // gradient at this layer's input: the flipped, transposed convolution
             const int n = L[l].cout * L[l].cin * 9;
             k_conv_transpose_weights<<<(n + 255) / 256, 256, 0, st>>>(wb + L[l].w, wt, L[l].cout, L[l].cin);
@@ -444,6 +629,28 @@ int pvof_cnn_adam(float *params, const float *grad, float *m, float *v, uint16_t
                                                              reinterpret_cast<__nv_bfloat16 *>(params_bf16), n, lr, b1,
                                                              b2, c1, c2, 1e-8f);
     return cudaGetLastError() == cudaSuccess ? PVOF_OK : PVOF_ECUDA;
+}
+
+int pvof_cnn_conv32(const float *x, const uint16_t *w_bf16, const float *b, float *y, int H, int W, int relu,
+                    void *stream)
+{
+    if (!x || !w_bf16 || !y || H <= 0 || W <= 0) return PVOF_EINVAL;
+    return conv(x, CNN_CMAX, reinterpret_cast<const __nv_bfloat16 *>(w_bf16), b, y, CNN_CMAX, H, W, relu,
+                (cudaStream_t)stream)
+               ? PVOF_ECUDA
+               : PVOF_OK;
+}
+
+int pvof_cnn_status(void *stream)
+{
+    int *err = nullptr, h = 0;
+    if (cudaGetSymbolAddress((void **)&err, g_cnn_err) != cudaSuccess) return PVOF_ECUDA;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return PVOF_ECUDA;
+    if (h && cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return PVOF_ECUDA;
+    return h ? PVOF_ECUDA : PVOF_OK;
 }
 
 int pvof_cnn_to_bf16(const float *params, uint16_t *params_bf16, void *stream)

@@ -136,7 +136,7 @@ EXPORTS = [
     "pvof_VOF_DIFFUSE_extend_psi_LG_contact_angle",
     "pvof_Particle_initialize_velocities", "pvof_Lagrangian_advect_particles", "pvof_get_particles",
     "pvof_cnn_param_count", "pvof_cnn_work_floats", "pvof_cnn_forward", "pvof_cnn_backward", "pvof_cnn_mse",
-    "pvof_cnn_adam", "pvof_cnn_to_bf16", "pvof_set_pressure_network", "pvof_pressure_network_sample",
+    "pvof_cnn_adam", "pvof_cnn_to_bf16", "pvof_cnn_status", "pvof_cnn_conv32", "pvof_set_pressure_network", "pvof_pressure_network_sample",
 ]
 
 SOLVER_BIHARMONIC = 0

@@ -69,6 +69,11 @@ class Network:
                                       _ptr(self.work), self.stream), "pvof_cnn_forward")
         return self.y
 
+    def status(self):
+        """Raises if a tensor-core convolution since the last call gave up
+        waiting for its matrix multiplications."""
+        check(load().pvof_cnn_status(self.stream), "pvof_cnn_status")
+
     def gradient(self, x, dy):
         """Parameter gradient of sum(dy * y) at x (a fresh buffer)."""
         self.g.zero_()

@@ -92,6 +92,8 @@ def load():
     L.pvof_cnn_forward.argtypes = [V, V, V, V, C.c_int, C.c_int, V, V]
     L.pvof_cnn_backward.argtypes = [V, V, V, V, V, C.c_int, C.c_int, V, V]
     L.pvof_cnn_mse.argtypes = [V, V, V, C.c_size_t, V, V]
+    L.pvof_cnn_status.argtypes = [V]
+    L.pvof_cnn_conv32.argtypes = [V, V, V, V, C.c_int, C.c_int, C.c_int, V]
     L.pvof_cnn_adam.argtypes = [V, V, V, V, V, C.c_int, C.c_float, V]
     L.pvof_cnn_to_bf16.argtypes = [V, V, V]
     L.pvof_set_pressure_network.argtypes = [V, P(C.c_float), C.c_size_t]

@@ -2,9 +2,18 @@
 (oracle/cnn_oracle.py), training on the solver's own samples, and the warm
 start in the solve against the same-stage warm start it is built on.
 
-  forward pass                  relative max error <= 1e-5 (FP32 sums vs FP64)
-  parameter gradient            relative max error <= 1e-5
+  one hidden layer on the       relative max error <= 1e-5 on BF16-exact inputs
+  tensor cores                  (FP32 accumulation in tensor memory vs FP64)
+  forward pass                  relative L2 error <= 3e-3
+  parameter gradient            relative L2 error <= 2e-2
   mean-square loss and dy       <= 1e-6
+
+The hidden layers take their operands in BF16; the device rounds its FP32
+activations, the oracle its FP64 ones (through FP32), and a value near a
+rounding boundary can round to neighbouring BF16 numbers in the two (a step
+of 2^-8 relative), so the whole network agrees to a few 1e-4 and its
+gradient, through the ReLU masks as well, to a few 1e-3; the single layer on
+BF16-exact inputs isolates the tensor-core arithmetic itself.
   training                      the loss falls below that of predicting no change
   learned warm start            the fields stay within the pressure tolerance of
                                 the plain path (1e-7 relative L2); the pressure
@@ -16,6 +25,32 @@ import pytest
 from conftest import g_range, physical
 
 pytestmark = pytest.mark.gpu
+
+
+def test_tensor_core_layer_matches_oracle():
+    """pvof_cnn_conv32: a 32 -> 32 layer as tcgen05 MMAs on BF16 operands,
+    on pixel counts that are and are not multiples of the 128-pixel tile."""
+    import torch
+    import cnn_oracle as co
+    from pvof.cnn import _ptr
+    from pvof.runtime import check, load
+    rng = np.random.default_rng(11)
+    for H, W in ((16, 8), (13, 29), (70, 50)):
+        x = co.to_bf16(rng.standard_normal((32, H, W)).astype(np.float32))
+        w = co.to_bf16((rng.standard_normal((32, 32, 3, 3)) * 0.1).astype(np.float32))
+        b = rng.standard_normal(32).astype(np.float32)
+        wb = torch.tensor((w.view(np.uint32) >> 16).astype(np.int16).ravel(), device="cuda")
+        xt = torch.tensor(x.ravel(), device="cuda")
+        bt = torch.tensor(b, device="cuda")
+        yt = torch.empty(32 * H * W, dtype=torch.float32, device="cuda")
+        for relu in (0, 1):
+            check(load().pvof_cnn_conv32(_ptr(xt), _ptr(wb), _ptr(bt), _ptr(yt), H, W, relu, None), "conv32")
+            check(load().pvof_cnn_status(None), "status")
+            ref = co.conv(x.astype(np.float64), w.astype(np.float64), b)
+            if relu:
+                ref = np.maximum(ref, 0.0)
+            y = yt.cpu().numpy().reshape(32, H, W)
+            assert np.abs(y - ref).max() <= 1e-5 * np.abs(ref).max(), (H, W, relu, np.abs(y - ref).max())
 
 
 def test_network_kernels_match_oracle():
@@ -30,11 +65,17 @@ def test_network_kernels_match_oracle():
     net = cnn.Network(H, W, params=p)
     xt = torch.tensor(x.ravel(), device="cuda")
     y = net.forward(xt).cpu().numpy().reshape(H, W)
+    net.status()
     y_ref, _ = co.forward(p, x)
-    assert np.abs(y - y_ref).max() <= 1e-5 * np.abs(y_ref).max()
+    y_smooth, _ = co.forward(p, x, tc_bf16=False)
+    err = np.linalg.norm(y - y_ref) / np.linalg.norm(y_ref)
+    assert err <= 3e-3, err
+    # closer to the BF16-operand network than that is to the unrounded one
+    assert err < np.linalg.norm(y_smooth - y_ref) / np.linalg.norm(y_ref)
     g = net.gradient(xt, torch.tensor(dy.ravel(), device="cuda")).cpu().numpy()
+    net.status()
     g_ref = co.backward(p, x, dy)
-    assert np.abs(g - g_ref).max() <= 1e-5 * np.abs(g_ref).max()
+    assert np.linalg.norm(g - g_ref) <= 2e-2 * np.linalg.norm(g_ref)
     # the loss kernel
     t = rng.standard_normal(H * W).astype(np.float32)
     loss_ref, dy_ref = co.mse(y.ravel(), t)
