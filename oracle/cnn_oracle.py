@@ -5,8 +5,9 @@ convolutions 3 -> 32 -> 32 -> 32 -> 32 -> 32 -> 1 with zero padding and ReLU
 between them; weights rounded to BF16 (round to nearest even) for the
 forward and backward passes, biases in FP32; the four hidden 32 -> 32 layers
 (TC_LAYERS, the tensor-core layers of the CUDA code) also take their input
-activations, and in the backward pass the output gradient of their input
-convolution, rounded to BF16 (through FP32, as the device holds them); here
+activations, and in the backward pass their output gradient (the operand of
+the input-gradient and weight-gradient GEMMs; the bias gradient sums it
+unrounded), rounded to BF16 (through FP32, as the device holds them); here
 every sum is in FP64.
 Parameters are one flat array [w0, b0, ..., w5, b5], w_l laid out
 [cout][cin][3][3]; planes are channel-major [C][H][W].
@@ -120,9 +121,10 @@ def backward(params, x, dy, tc_bf16=True):
         ci, H, W = inp.shape
         ip = np.pad(inp, ((0, 0), (1, 1), (1, 1)))
         gw = np.zeros(wb.shape)
+        gg = bf16_operand(g) if (tc_bf16 and l in TC_LAYERS) else g   # the weight gradient's GEMM operand
         for dyy in range(3):
             for dxx in range(3):
-                gw[:, :, dyy, dxx] = np.einsum("ohw,chw->oc", g, ip[:, dyy:dyy + H, dxx:dxx + W])
+                gw[:, :, dyy, dxx] = np.einsum("ohw,chw->oc", gg, ip[:, dyy:dyy + H, dxx:dxx + W])
         grads[l] = (gw, g.sum(axis=(1, 2)))
         if l > 0:   # the input gradient: the transposed convolution
             wt = wb[:, :, ::-1, ::-1].transpose(1, 0, 2, 3)

@@ -17,7 +17,8 @@
 //
 // Kernels: the four hidden 32 -> 32 layers run on the tensor cores
 // (k_conv_umma: tcgen05.mma implicit GEMM, BF16 activations and weights, FP32
-// accumulation in tensor memory), forward and input gradient; the first
+// accumulation in tensor memory), forward and input gradient, and their
+// weight gradients (k_conv_wgrad_umma, the pixels as the GEMM's K); the first
 // (3 -> 32) and last (32 -> 1) layers, too narrow for an MMA tile, are a
 // shared-memory tiled direct convolution on the FP32 pipes (one thread per
 // pixel, all output channels in registers); the input gradient is the same
@@ -242,6 +243,177 @@ __global__ void __launch_bounds__(UM_M) k_conv_umma(const float *__restrict__ in
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
 }
 
+// Weight gradient of a 32 -> 32 layer on the tensor cores: the GEMM
+// D[m][co] = sum_p A[m][p] G[co][p] over the pixels, m = tap * 32 + ci
+// (288 rows in three M = 128 tiles, the last one padded with zeros),
+// A[m][p] = in[ci][p + tap] and G the layer's output gradient, both rounded to
+// BF16.  Each CTA takes 128-pixel chunks of the plane (grid-stride), gathers
+// them into shared memory in the K-major canonical layout (K = pixels),
+// issues 3 x 8 MMAs per chunk into three 128 x 32 FP32 accumulators in tensor
+// memory, and at the end writes its 288 x 32 partial sums; k_wgrad_reduce adds
+// the CTAs' partials in a fixed order.
+constexpr int UW_PIX = 128;                                   // pixels per chunk
+constexpr int UW_TILES = 3;                                   // M tiles of 128 (288 rows)
+constexpr int UW_A_TILE_STEP = UM_M * 16 * 2;                 // bytes of one tile for one MMA: 4096
+constexpr int UW_A_BYTES = UW_TILES * (UW_PIX / 16) * UW_A_TILE_STEP;   // 98304
+constexpr int UW_B_BYTES = (UW_PIX / 16) * UM_B_STEP;         // 8192
+constexpr size_t UW_SMEM = (size_t)UW_A_BYTES + UW_B_BYTES + 1024;
+
+__global__ void __launch_bounds__(UM_M) k_conv_wgrad_umma(const float *__restrict__ in, const float *__restrict__ g,
+                                                          int H, int W, float *__restrict__ partial,
+                                                          int *__restrict__ err)
+{
+    extern __shared__ unsigned char uw_raw[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_holder;
+    unsigned char *As = reinterpret_cast<unsigned char *>(((uintptr_t)uw_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char *Bs = As + UW_A_BYTES;
+    const int t = threadIdx.x, warp = t >> 5;
+    const long long plane = (long long)H * W;
+    const long long nchunk = (plane + UW_PIX - 1) / UW_PIX;
+    const uint32_t mbar_a = (uint32_t)__cvta_generic_to_shared(&mbar);
+    if (warp == 0) {   // 3 x 32 columns: the three accumulators (allocated as 128)
+        const uint32_t holder = (uint32_t)__cvta_generic_to_shared(&tmem_holder);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(holder) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // rows 288..383 (rows 32..127 of the last tile: row groups 4..15) stay zero
+    for (int q = t; q < (UW_PIX / 16) * 12 * 2 * 8; q += UM_M) {   // steps x 12 row groups x 2 halves x 8 rows
+        const int s = q / 192, rest = q % 192;
+        unsigned char *dst = As + (2 * (UW_PIX / 16) + s) * UW_A_TILE_STEP + (4 + rest / 16) * 256 +
+                             ((rest / 8) & 1) * 128 + (rest & 7) * 16;
+        *reinterpret_cast<uint4 *>(dst) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_holder;
+    const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(As), b0 = (uint32_t)__cvta_generic_to_shared(Bs);
+    int ok_all = 1;
+    uint32_t phase = 0;
+    bool first = true;
+#pragma unroll 1
+    for (long long c = blockIdx.x; c < nchunk; c += gridDim.x) {
+        const long long p0 = c * UW_PIX;
+        // A: 288 rows (tap, ci) x 128 pixels, 16-byte chunks of 8 pixels
+#pragma unroll 1
+        for (int q = t; q < 288 * (UW_PIX / 8); q += UM_M) {
+            const int m = q / (UW_PIX / 8), k8 = q % (UW_PIX / 8);
+            const int tap = m >> 5, ci = m & 31, dx = tap % 3 - 1, dy = tap / 3 - 1;
+            uint32_t pk[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                float v[2];
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const long long pp = p0 + k8 * 8 + 2 * e + h;
+                    v[h] = 0.0f;
+                    if (pp < plane) {
+                        const int y = (int)(pp / W) + dy, x = (int)(pp % W) + dx;
+                        if (x >= 0 && x < W && y >= 0 && y < H) v[h] = in[(size_t)ci * plane + (size_t)y * W + x];
+                    }
+                }
+                pk[e] = um_pack(v[0], v[1]);
+            }
+            const int tile = m >> 7, row = m & 127, s = k8 >> 1, half = k8 & 1;
+            unsigned char *dst = As + (tile * (UW_PIX / 16) + s) * UW_A_TILE_STEP + (row >> 3) * 256 + half * 128 +
+                                 (row & 7) * 16;
+            *reinterpret_cast<uint4 *>(dst) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        }
+        // B: the output gradient, 32 rows (co) x 128 pixels
+        for (int q = t; q < UM_N * (UW_PIX / 8); q += UM_M) {
+            const int co = q / (UW_PIX / 8), k8 = q % (UW_PIX / 8);
+            uint32_t pk[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const long long pp = p0 + k8 * 8 + 2 * e;
+                const float v0 = pp < plane ? g[(size_t)co * plane + (size_t)pp] : 0.0f;
+                const float v1 = pp + 1 < plane ? g[(size_t)co * plane + (size_t)pp + 1] : 0.0f;
+                pk[e] = um_pack(v0, v1);
+            }
+            const int s = k8 >> 1, half = k8 & 1;
+            unsigned char *dst = Bs + s * UM_B_STEP + (co >> 3) * 256 + half * 128 + (co & 7) * 16;
+            *reinterpret_cast<uint4 *>(dst) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (t == 0) {
+#pragma unroll 1
+            for (int tile = 0; tile < UW_TILES; tile++)
+#pragma unroll 1
+                for (int s = 0; s < UW_PIX / 16; s++) {
+                    const uint64_t ad = um_desc(a0 + (tile * (UW_PIX / 16) + s) * UW_A_TILE_STEP, 128, 256);
+                    const uint64_t bd = um_desc(b0 + s * UM_B_STEP, 128, 256);
+                    const uint32_t acc = (first && s == 0) ? 0u : 1u;
+                    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                                 ::"r"(tmem + (uint32_t)(tile * UM_N)), "l"(ad), "l"(bd), "r"(UM_IDESC), "r"(acc)
+                                 : "memory");
+                }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar_a)
+                         : "memory");
+        }
+        first = false;
+        // the MMAs read the shared tiles: wait before the next chunk overwrites them
+        int done = 0;
+        for (long long it = 0; it < UM_WAIT_LIMIT && !done; it++) {
+            uint32_t okw;
+            asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                         "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(okw) : "r"(mbar_a), "r"(phase) : "memory");
+            done = (int)okw;
+        }
+        phase ^= 1u;
+        ok_all = __syncthreads_and(done);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (!ok_all) break;
+    }
+    if (ok_all && !first) {
+        float *out = partial + (size_t)blockIdx.x * 288 * UM_N;
+#pragma unroll 1
+        for (int tile = 0; tile < UW_TILES; tile++) {
+            uint32_t r[32];
+            const uint32_t taddr = tmem + (uint32_t)(tile * UM_N) + ((uint32_t)(warp * 32) << 16);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                         "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+                         "%30, %31}, [%32];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                           "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+                           "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+                           "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                         : "r"(taddr)
+                         : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const int m = tile * UM_M + t;
+            if (m < 288)
+#pragma unroll
+                for (int co = 0; co < UM_N; co++) out[(size_t)m * UM_N + co] = __uint_as_float(r[co]);
+        }
+    } else if (t == 0 && !ok_all) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tmem) : "memory");
+}
+
+// dw[co][ci][tap] += sum over the CTAs (in order) of partial[cta][tap * 32 + ci][co]
+__global__ void k_wgrad_reduce(const float *__restrict__ partial, int nparts, float *__restrict__ dw)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;   // q = m * 32 + co
+    if (q >= 288 * UM_N) return;
+    float s = 0.0f;
+    for (int c = 0; c < nparts; c++) s += partial[(size_t)c * 288 * UM_N + q];
+    const int m = q / UM_N, co = q % UM_N, tap = m >> 5, ci = m & 31;
+    dw[(co * CNN_CMAX + ci) * 9 + tap] += s;
+}
+
 // the weights of the input-gradient convolution: wt[ci][co][8 - tap] = w[co][ci][tap]
 __global__ void k_conv_transpose_weights(const __nv_bfloat16 *__restrict__ w, __nv_bfloat16 *__restrict__ wt,
                                          int cout, int cin)
@@ -264,7 +436,7 @@ __global__ void k_relu_back(float *__restrict__ dy, const float *__restrict__ y,
 // (co, cin) sums dY[co][p] for the bias
 __global__ void __launch_bounds__(256) k_conv_wgrad(const float *__restrict__ in, int cin,
                                                     const float *__restrict__ dy, int H, int W,
-                                                    float *__restrict__ dw, float *__restrict__ db, int bf16_in)
+                                                    float *__restrict__ dw, float *__restrict__ db)
 {
     const int co = blockIdx.y, ci = blockIdx.x;
     const size_t plane = (size_t)H * W;
@@ -285,11 +457,7 @@ __global__ void __launch_bounds__(256) k_conv_wgrad(const float *__restrict__ in
 #pragma unroll
         for (int t = 0; t < 9; t++) {
             const int a = i + t % 3 - 1, c = j + t / 3 - 1;
-            if (a >= 0 && a < W && c >= 0 && c < H) {
-                float xv = x[(size_t)c * W + a];
-                if (bf16_in) xv = __bfloat162float(__float2bfloat16(xv));   // the tensor-core layers' operand
-                acc[t] += xv * gv;
-            }
+            if (a >= 0 && a < W && c >= 0 && c < H) acc[t] += x[(size_t)c * W + a] * gv;
         }
     }
     __shared__ float red[8][9];
@@ -382,15 +550,38 @@ size_t param_count()
 // activation planes kept in the work buffer: the five hidden layers' outputs
 // (32 planes each) and the output plane, then two gradient buffers of 32
 // planes, then the transposed weights of one layer
+__device__ int g_cnn_err;   // set when a tensor-core convolution gave up waiting for its MMAs
+
+constexpr int UW_MAX_CTAS = 296;   // tensor-core weight-gradient CTAs (two per SM of a B200)
+
 size_t work_floats(int H, int W)
 {
     const size_t plane = (size_t)H * W;
-    return (5 * CNN_CMAX + 1 + 2 * CNN_CMAX) * plane + CNN_CMAX * CNN_CMAX * 9;
+    return (5 * CNN_CMAX + 1 + 2 * CNN_CMAX) * plane + CNN_CMAX * CNN_CMAX * 9 + (size_t)UW_MAX_CTAS * 288 * UM_N;
+}
+
+// weight and bias gradient of a 32 -> 32 layer: the weights on the tensor
+// cores, the bias by per-block sums
+int wgrad32(const float *in, const float *g, float *dw, float *db, int H, int W, float *partial, cudaStream_t st)
+{
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_conv_wgrad_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UW_SMEM) !=
+            cudaSuccess)
+            return -1;
+        attr = true;
+    }
+    int *err = nullptr;
+    if (cudaGetSymbolAddress((void **)&err, g_cnn_err) != cudaSuccess) return -1;
+    const long long n = (long long)H * W, nchunk = (n + UW_PIX - 1) / UW_PIX;
+    const int nb = (int)(nchunk < UW_MAX_CTAS ? nchunk : UW_MAX_CTAS);   // every CTA gets a chunk
+    k_conv_wgrad_umma<<<(unsigned)nb, UM_M, UW_SMEM, st>>>(in, g, H, W, partial, err);
+    k_wgrad_reduce<<<(288 * UM_N + 255) / 256, 256, 0, st>>>(partial, nb, dw);
+    k_conv_wgrad<<<dim3(1u, (unsigned)CNN_CMAX), 256, 0, st>>>(in, 0, g, H, W, dw, db);   // bias only
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 size_t conv_smem(int cin, int cout) { return sizeof(float) * ((size_t)cin * CNN_HALO * CNN_HALO + (size_t)cout * cin * 9); }
-
-__device__ int g_cnn_err;   // set when a tensor-core convolution gave up waiting for its MMAs
 
 int conv(const float *in, int cin, const __nv_bfloat16 *w, const float *b, float *out, int cout, int H, int W, int relu,
          cudaStream_t st)
@@ -586,6 +777,7 @@ int pvof_cnn_backward(const float *params, const uint16_t *params_bf16, const fl
     const __nv_bfloat16 *wb = reinterpret_cast<const __nv_bfloat16 *>(params_bf16);
     float *gbuf[2] = {work + (5 * CNN_CMAX + 1) * plane, work + (6 * CNN_CMAX + 1) * plane};
     __nv_bfloat16 *wt = reinterpret_cast<__nv_bfloat16 *>(work + (7 * CNN_CMAX + 1) * plane);
+    float *partial = work + (7 * CNN_CMAX + 1) * plane + CNN_CMAX * CNN_CMAX * 9;
     // gradient at the output of the last layer
     if (cudaMemcpyAsync(gbuf[0], dy, plane * sizeof(float), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
         return PVOF_ECUDA;
@@ -597,10 +789,12 @@ int pvof_cnn_backward(const float *params, const uint16_t *params_bf16, const fl
             const size_t n = (size_t)L[l].cout * plane;
             k_relu_back<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, work + (size_t)l * CNN_CMAX * plane, n);
         }
-        const int tc = L[l].cin == CNN_CMAX && L[l].cout == CNN_CMAX;   // a tensor-core layer: BF16 inputs
-        k_conv_wgrad<<<dim3((unsigned)L[l].cin + 1, (unsigned)L[l].cout), 256, 0, st>>>(lin, L[l].cin, g, H, W,
-                                                                                          grad + L[l].w, grad + L[l].b,
-                                                                                          tc);
+        if (L[l].cin == CNN_CMAX && L[l].cout == CNN_CMAX) {   // a tensor-core layer
+            if (wgrad32(lin, g, grad + L[l].w, grad + L[l].b, H, W, partial, st)) return PVOF_ECUDA;
+        } else {
+            k_conv_wgrad<<<dim3((unsigned)L[l].cin + 1, (unsigned)L[l].cout), 256, 0, st>>>(
+                lin, L[l].cin, g, H, W, grad + L[l].w, grad + L[l].b);
+        }
         if (l > 0) {   // gradient at this layer's input: the flipped, transposed convolution
             const int n = L[l].cout * L[l].cin * 9;
             k_conv_transpose_weights<<<(n + 255) / 256, 256, 0, st>>>(wb + L[l].w, wt, L[l].cout, L[l].cin);
