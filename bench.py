@@ -54,6 +54,12 @@ fixed sphere on the axis (256x512, density ratio 1e-3, surface tension,
 contact angle 90 degrees) for --axisym-steps steps, with the reference build
 (AXISYM_RZ, resolved particles) on the host for --axisym-ref-steps steps.
 
+--learned adds a "learned" object: the learned warm start on its benchmark
+case (1024x1024, three mobile cylinders on a flat interface, density ratio
+1e-3): the network trained on about --learned-samples 64x64 crops of the
+solver's own samples, then pressure iterations and time per step with a cold
+start, the same-stage warm start and the learned one.
+
 --impl reference runs the reference's own time step (compiled from its
 sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host:
 --warmup untimed steps, then min(--steps, --ref-steps) timed ones.
@@ -85,6 +91,8 @@ ALG_BYTES = {0: 48.0, 1: 56.0, 2: 56.0}
 # pressure_preconditioner, velocity_cg_unregularized)
 FORMS = [
     ("fp32 stencils + pressure warm start (same stage of the previous step)", 1, 1, 0, 0),
+    ("fp32 stencils + learned pressure warm start (the network on the tensor cores, trained on this run's own "
+     "samples)", 1, 2, 0, 0),
     ("spectral pressure preconditioner (FP64)", 0, 0, 1, 0),
     ("spectral pressure preconditioner + unregularised momentum CG (FP64)", 0, 0, 1, 1),
     ("spectral pressure preconditioner + unregularised momentum CG + fp32 stencils + pressure warm start",
@@ -94,6 +102,9 @@ FORMS = [
 # interface, a fixed one below it
 CYLINDERS = [(1, 0.25, 2.0, 0.08, 0, 0, 0, 2.5), (1, 0.75, 2.6, 0.08, 0, 0, 0, 2.5),
              (0, 0.5, 1.2, 0.1, 0, 0, 0, 2.5)]
+# the learned form's network: trained on the solver's samples of this run
+LEARNED_SAMPLE_STEPS = 12
+LEARNED_EPOCHS = 15
 STATE_FIELDS = ["C_L", "U", "V", "P", "CH_RHS_N", "U_EXPLICIT_OLD", "V_EXPLICIT_OLD",
                 "U_VISC_EXPLICIT_OLD", "V_VISC_EXPLICIT_OLD"]
 
@@ -397,6 +408,80 @@ def axisym_case(args, device):
     return out
 
 
+def learned_case(args, device):
+    """The learned warm start on its benchmark case: three mobile cylinders
+    (R 0.1, solid density 2.5, contact angle 110 degrees) on a flat
+    interface, 1024 x 1024, density ratio 1e-3, Jacobi-PCG pressure solve.
+    The network is trained on random 64 x 64 crops of the solver's own
+    samples (the same-stage warm start's run), then the case is advanced with
+    a cold start, the same-stage warm start and the learned one: pressure
+    iterations and device time per step of --learned-steps steps after two
+    (which fill the kept corrections)."""
+    import numpy as np
+    from pvof import cases, cnn, runtime
+    dt = 2e-5
+    grid, params, planes, parts = cases.sinking_cylinders(P_CG_MAXIT=40000)
+    planes_cl = dict(planes, C_L=planes["F"])
+    t0 = time.time()
+    nplanes = 3 * (args.learned_sample_steps - 2)
+    per_plane = max(1, -(-args.learned_samples // max(nplanes, 1)))
+    samples = cnn.generate_crop_samples(grid, params, planes, parts, args.learned_sample_steps, dt, 64, per_plane,
+                                        device=device)
+    t_samples = time.time() - t0
+    t0 = time.time()
+    net, hist = cnn.train(samples, 64, 64, epochs=args.learned_epochs, batch=32, lr=1e-3, device=device)
+    loss, base = net.evaluate(samples[: min(len(samples), 2000)])
+    t_train = time.time() - t0
+    P = net.params()
+    del samples, net
+    out = {"case": "planar 1024x1024, x periodic, three mobile cylinders (R 0.1, rho_s 2.5, contact angle 110 deg) "
+                   "on a flat interface at y 0.6, density ratio 1e-3, We 100, Re 100, Cn 0.005, dt 2e-5, "
+                   "Jacobi-PCG pressure solve to the reference's absolute tolerance 1e-7",
+           "network": {"crops": nplanes * per_plane, "crop": "64x64", "epochs": args.learned_epochs,
+                       "loss": loss, "loss_predicting_no_change": base, "sampling_s": t_samples,
+                       "training_s": t_train},
+           "steps": args.learned_steps}
+    fields = {}
+    for label, warm in (("cold", 0), ("same_stage", 1), ("learned", 2)):
+        from pvof import abi
+        p = abi.Params.from_buffer_copy(params)
+        p.pressure_warm_start = warm
+        s = runtime.Solver(grid, p, device=device)
+        s.set_particles(parts)
+        if warm == 2:
+            s.set_pressure_network(P)
+        s.set_planes(planes_cl)
+        s.initialize()
+        iters = 0
+        for n in range(2 + args.learned_steps):
+            timed = n >= 2
+            if timed and n == 2:
+                ms = 0.0
+            if timed:
+                s.flush_l2()
+                s.timer_start()
+            for rk in range(3):
+                if n > 0 and rk == 0:
+                    s.call("Velocity_cell_center")
+                s.set_stage(rk, dt)
+                st = s.substep()
+                if timed:
+                    iters += st.p_iters_total
+            if timed:
+                ms += s.timer_stop()
+        out[label] = {"pressure_iterations": iters, "ms_per_step": ms / args.learned_steps}
+        fields[label] = {f: s.get(f) for f in ("U", "V", "P")}
+        s.close()
+    for label in ("same_stage", "learned"):
+        out[label]["velocity_rel_l2_vs_cold"] = max(
+            float(np.linalg.norm(fields[label][f] - fields["cold"][f]) / np.linalg.norm(fields["cold"][f]))
+            for f in ("U", "V"))
+    out["learned_vs_cold_iterations"] = out["learned"]["pressure_iterations"] / max(1, out["cold"]["pressure_iterations"])
+    out["learned_vs_same_stage_iterations"] = (out["learned"]["pressure_iterations"] /
+                                              max(1, out["same_stage"]["pressure_iterations"]))
+    return out
+
+
 # uneven batch: the planar instability at four sizes, two cases each
 MIXED_SIZES = [(64, 128), (64, 128), (128, 256), (128, 256), (256, 512), (256, 512), (512, 1024), (512, 1024)]
 
@@ -470,16 +555,30 @@ def time_forms(args, snap, m64, grid, params, planes, device, cells, value, timi
     error against the plain path's state after the same steps (snap, m64);
     solver iterations and pressure time from a following per-solver timing
     pass of tsteps steps, like the plain path's (timing)."""
-    from pvof import abi, runtime
+    from pvof import abi, cnn, runtime
     import numpy as np
     forms = []
+    net_params, net_info = None, None
     for label, fp32, warm, precond, vel in FORMS:
         fparams = abi.Params.from_buffer_copy(params)
         fparams.stencil_fp32 = fp32
         fparams.pressure_warm_start = warm
         fparams.pressure_preconditioner = precond
         fparams.velocity_cg_unregularized = vel
+        if warm == 2 and net_params is None:
+            # samples from the solver on this workload, then training on the device
+            t0 = time.time()
+            samples = cnn.generate_samples(grid, params, planes, LEARNED_SAMPLE_STEPS, DT, device=device)
+            net, hist = cnn.train(samples, grid.NYM, grid.NXM, epochs=LEARNED_EPOCHS, batch=6, lr=2e-3,
+                                  device=device)
+            loss, base = net.evaluate(samples)
+            net_params = net.params()
+            net_info = {"samples": len(samples), "epochs": LEARNED_EPOCHS, "loss": loss, "loss_predicting_no_change": base,
+                        "training_s": time.time() - t0}
+            del samples, net
         fg = runtime.Solver(grid, fparams, device=device)
+        if warm == 2:
+            fg.set_pressure_network(net_params)
         fg.set_planes(planes)
         fg.initialize()
         for _ in range(args.warmup):
@@ -505,6 +604,8 @@ def time_forms(args, snap, m64, grid, params, planes, device, cells, value, timi
                       "velocity_iterations": ft[1]["iterations"],
                       "velocity_iterations_plain": timing[1]["iterations"],
                       "error_vs_fp64": err})
+        if warm == 2:
+            forms[-1]["network"] = net_info
         fg.close()
     return forms
 
@@ -662,6 +763,12 @@ def run_ours(args):
             mixed = mixed_batch(args, local)
         except Exception as e:   # noqa: BLE001
             mixed = {"error": "%s: %s" % (type(e).__name__, e)}
+    learned = None
+    if args.learned:
+        try:
+            learned = learned_case(args, local)
+        except Exception as e:   # noqa: BLE001
+            learned = {"error": "%s: %s" % (type(e).__name__, e)}
     axisym = None
     if args.axisym:
         try:
@@ -718,6 +825,8 @@ def run_ours(args):
             line["large"] = large
         if axisym is not None:
             line["axisym"] = axisym
+        if learned is not None:
+            line["learned"] = learned
         if mixed is not None:
             line["batched_mixed"] = mixed
         print(json.dumps(line))
@@ -751,6 +860,12 @@ def main():
                     help="also time the axisymmetric bubble-and-sphere case (256x512) and the reference on it")
     ap.add_argument("--axisym-steps", type=int, default=10)
     ap.add_argument("--axisym-ref-steps", type=int, default=2)
+    ap.add_argument("--learned", action="store_true",
+                    help="also train the warm-start network on the 1024x1024 three-cylinder case and time it")
+    ap.add_argument("--learned-steps", type=int, default=4)
+    ap.add_argument("--learned-sample-steps", type=int, default=8)
+    ap.add_argument("--learned-samples", type=int, default=20000)
+    ap.add_argument("--learned-epochs", type=int, default=3)
     ap.add_argument("--particles", action="store_true",
                     help="also time the workload with surface tension and three resolved cylinders")
     ap.add_argument("--forms", action="store_true", default=True,

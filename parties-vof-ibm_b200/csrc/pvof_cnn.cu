@@ -657,7 +657,8 @@ __global__ void k_cnn_residual(Dom d, BcMap mp, const double *__restrict__ rho, 
     if (q >= W * H) return;
     const int i = q % W, j = q / W;
     const double a = pressure_op(d, rho, i, j, [&](int x, int y) { return remap(mp, phi_prev, P, d.NX, d.NY, x, y); });
-    AT_(r0, i, j) = AT_(rhs, i, j) - a;
+    // the right-hand side with the operator's axisymmetric row weight, as the solve forms its residual
+    AT_(r0, i, j) = (d.axisym ? AT_(rhs, i, j) * d.m.r_c[i] : AT_(rhs, i, j)) - a;
 }
 
 // network inputs x = [rho, r0 / rms(r0), phi_prev / rms(phi_prev)] and, if

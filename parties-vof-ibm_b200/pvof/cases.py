@@ -207,3 +207,21 @@ def rising_bubble(NXM=64, NYM=128, rmax=2.0, zmax=4.0, radius=0.5, zc=1.0, Cn=0.
         p = velocity_amp * rng.standard_normal((NY, NX))
     return grid, params, {"F": C, "U": u, "V": v, "P": p}
 
+
+
+def sinking_cylinders(NXM=1024, NYM=1024, L=1.0, Cn=0.005, rho_ratio=1e-3, R=0.1, rho_s=2.5, theta=110.0,
+                      Re=100.0, We=100.0, y0=0.6, **param_kw):
+    """Three mobile cylinders (radius R, solid/liquid density rho_s) centred on
+    a flat interface at y0 of an L x L box (x periodic, no-slip walls in y),
+    liquid (C = 1) below, gas of density ratio rho_ratio above, surface
+    tension with contact angle theta (degrees): the learned-warm-start
+    benchmark case.  Returns (grid, params, planes, particles), particles as
+    rows (mobile, x, y, R, u, v, omega_z, rho_s)."""
+    grid, params, planes = rayleigh_taylor(NXM, NYM, Lx=L, Ly=L, Cn=Cn, amp=0.0, atwood=(1 - rho_ratio) /
+                                           (1 + rho_ratio), Re=Re, surface_tension=True, We=We, y0=y0, **param_kw)
+    # liquid below the interface: flip the heavy-fluid-on-top profile
+    planes["F"] = 1.0 - planes["F"]
+    params.rho1, params.rho2 = 1.0, rho_ratio
+    params.contact_angle_deg = theta
+    parts = [(1, L * x, y0, R, 0.0, 0.0, 0.0, rho_s) for x in (0.2, 0.5, 0.8)]
+    return grid, params, planes, parts

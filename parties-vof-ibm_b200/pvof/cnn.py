@@ -155,3 +155,52 @@ def train(samples, H, W, epochs=30, batch=8, lr=1e-3, seed=0, device=0, log=None
         if log:
             log("epoch %d loss %.4e" % (ep, hist[-1]))
     return net, hist
+
+
+def crops(x, t, H, W, size, count, rng):
+    """count random size x size windows of a full-plane sample (x: 3 planes,
+    t: 1 plane, flat device tensors), as (x, t) pairs of flat tensors."""
+    xs = x.view(3, H, W)
+    ts = t.view(H, W)
+    out = []
+    for _ in range(count):
+        j = int(rng.integers(0, H - size + 1))
+        i = int(rng.integers(0, W - size + 1))
+        out.append((xs[:, j:j + size, i:i + size].contiguous().view(-1), ts[j:j + size, i:i + size].contiguous().view(-1)))
+    return out
+
+
+def generate_crop_samples(grid, params, planes, particles, nsteps, dt, size, per_plane, seed=0, device=0, log=None):
+    """Run the case (with resolved particles if given) with the same-stage
+    warm start; from the third step on, every substep's full-plane sample
+    gives per_plane random size x size crops."""
+    import torch
+    from . import abi
+    p = abi.Params.from_buffer_copy(params)
+    p.pressure_warm_start = 1
+    s = runtime.Solver(grid, p, device=device)
+    if particles:
+        s.set_particles(particles)
+        s.set_planes(dict(planes, C_L=planes["F"]))
+    else:
+        s.set_planes(planes)
+    s.initialize()
+    H, W = grid.NYM, grid.NXM
+    dev = torch.device("cuda", device)
+    rng = np.random.default_rng(seed)
+    x = torch.empty(3 * H * W, dtype=torch.float32, device=dev)
+    t = torch.empty(H * W, dtype=torch.float32, device=dev)
+    out = []
+    for n in range(nsteps):
+        for rk in range(3):
+            if n > 0 and rk == 0:
+                s.call("Velocity_cell_center")
+            s.set_stage(rk, dt)
+            s.substep()
+            if n >= 2:
+                check(load().pvof_pressure_network_sample(s.h, rk, _ptr(x), _ptr(t)), "pvof_pressure_network_sample")
+                out += crops(x, t, H, W, size, per_plane, rng)
+        if log:
+            log("sample step %d: %d crops" % (n, len(out)))
+    s.close()
+    return out
