@@ -682,6 +682,7 @@ def run_ours(args):
     clocks = Clocks(local)
     barrier(dist)
     l0 = g.launch_count()
+    clamp0, mass0 = g.clamp_mass_total(), g.liquid_mass()
     clocks.start()
     wall0 = time.time()
     total_ms = 0.0
@@ -699,6 +700,10 @@ def run_ours(args):
     value = ws * cells * args.steps / (t_max * 1e-3)
     snap = {f: g.get(f) for f in ("U", "V", "P", "C_L")}   # the forms' reference state
     m64 = g.liquid_mass()
+    # liquid volume over the timed steps: the change the C_L clamp made (the
+    # only non-conservative operation of the substep) and the total change
+    mass_report = {"clamp_mass_timed_steps": g.clamp_mass_total() - clamp0, "liquid_mass_change": m64 - mass0,
+                   "liquid_mass": mass0}
 
     # ---- end to end through the C ABI with host buffers ---------------------
     blocks = {f: pinned_like(g.block_count(f)) for f in STATE_FIELDS}
@@ -806,6 +811,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps},
             "gpu_launches": launches,
+            "mass": mass_report,
             "roofline": {"kernel": names[dom], "bound": "hbm", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "alg_bytes_per_cell_iter": ALG_BYTES[dom],

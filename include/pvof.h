@@ -409,6 +409,9 @@ int pvof_set_graphs(pvof_ctx *ctx, int enabled);
 /* No counterpart in the reference: how many substeps so far replayed their
  * launches from a graph (-1 for a null context). */
 long long pvof_graph_replays(const pvof_ctx *ctx);
+/* The liquid mass the C_L clamp changed (pvof_stats.clamp_mass,
+ * VOF_DIFFUSE.c:1093-1127) summed over every substep since pvof_initialize. */
+int pvof_clamp_mass_total(const pvof_ctx *ctx, double *total);
 /* No counterpart in the reference: 1 (the default) solves the pressure and
  * momentum systems with the cluster-resident kernels wherever their solve
  * ranges fit one thread-block cluster; 0 selects the grid-wide persistent

@@ -885,6 +885,7 @@ int initialize(pvof_ctx *c)
     c->phi_old_mask = 0;
     TRY(cell_center(c));
     c->time = 0.0;
+    c->clamp_total = 0.0;
     return PVOF_OK;
 }
 
@@ -1073,6 +1074,7 @@ int substep(pvof_ctx *c, pvof_stats *st)
                            c->stream));
         c->phi_prev_mask |= 1 << c->stage;
     }
+    c->clamp_total += c->scal_host->clamp_delta;
     if (c->p.surface_tension) swap_f_sigma(c);
     if (solids && rc == PVOF_OK) TRY(ibm_advect(c));   // Temporal_int.c:1186-1238
     if (st) {
@@ -2155,6 +2157,13 @@ int pvof_set_graphs(pvof_ctx *c, int enabled)
 }
 
 long long pvof_graph_replays(const pvof_ctx *c) { return c ? c->graph_replays : -1; }
+
+int pvof_clamp_mass_total(const pvof_ctx *c, double *total)
+{
+    if (!c || !total) return set_err(PVOF_EINVAL, "null context or output");
+    *total = c->clamp_total;
+    return PVOF_OK;
+}
 
 int pvof_set_cluster_solvers(pvof_ctx *c, int enabled)
 {

@@ -153,6 +153,7 @@ struct Ctx {
     int stage;
     double dt;
     double time;
+    double clamp_total;      // clamp_mass summed over the substeps since pvof_initialize
     size_t cgs_p_smem;       // shared memory of the cluster pressure solver (0: grid solver)
     size_t cgs_v_smem;       // same, velocity solver for both components (0: grid solver)
     int cgs_p_threads, cgs_v_threads;   // their threads per CTA

@@ -68,6 +68,7 @@ def load():
     L.pvof_graph_replays.argtypes = [V]
     L.pvof_graph_replays.restype = C.c_longlong
     L.pvof_set_cluster_solvers.argtypes = [V, C.c_int]
+    L.pvof_clamp_mass_total.argtypes = [V, P(C.c_double)]
     L.pvof_solver_timing.argtypes = [V, C.c_int, P(C.c_double), P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]
     L.pvof_solver_kernel.argtypes = [V, C.c_int]
     L.pvof_set_particles.argtypes = [V, P(abi.Particle), C.c_int]
@@ -265,6 +266,12 @@ class Solver:
 
     def graph_replays(self):
         return load().pvof_graph_replays(self.h)
+
+    def clamp_mass_total(self):
+        """The clamp's liquid mass change summed over the substeps since initialize()."""
+        t = C.c_double()
+        check(load().pvof_clamp_mass_total(self.h, C.byref(t)), "pvof_clamp_mass_total")
+        return t.value
 
     def set_cluster_solvers(self, on):
         """Cluster-resident solvers where they fit (default), or the grid-wide ones."""

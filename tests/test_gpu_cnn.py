@@ -16,8 +16,10 @@ gradient, through the ReLU masks as well, to a few 1e-3; the single layer on
 BF16-exact inputs isolates the tensor-core arithmetic itself.
   training                      the loss falls below that of predicting no change
   learned warm start            the fields stay within the pressure tolerance of
-                                the plain path (1e-7 relative L2); the pressure
-                                iterations of both warm starts are reported
+                                the plain path (1e-7 relative L2); the trained
+                                network takes fewer pressure iterations than the
+                                cold start (it does not beat the same-stage warm
+                                start it is built on); both counts are reported
 """
 import numpy as np
 import pytest
@@ -121,3 +123,5 @@ def test_learned_warm_start_trains_and_stays_within_tolerance():
             a, b = out[mode][1][f], out[0][1][f]
             assert np.linalg.norm(a - b) <= 1e-7 * np.linalg.norm(b), (mode, f)
     assert out[1][0] < out[0][0]
+    # what the trained network gains over the Jacobi-PCG without a warm start
+    assert out[2][0] < out[0][0], (out[2][0], out[0][0])
