@@ -20,7 +20,8 @@ default).  The per-solver times behind the roofline and the solver shares
 come from a following pass of --timing-steps steps issued launch by launch
 with CUDA events around every solver launch.  e2e: the same steps driven
 through the C ABI with the state uploaded from pinned host buffers before
-every step and downloaded after it.
+every step and downloaded after it, timed by the host's clock around the
+calls (the device-event time of the same interval is reported beside it).
 
 --batch-cases K (default 6, 0 turns it off) additionally times K replicas of
 the workload advanced concurrently by pvof_run_steps_batched (the batched
@@ -324,6 +325,8 @@ def large_case(args, device):
         t, _, _ = solver_timing_pass(s, 1)
         out[label] = {"value": 1024 * 1024 / (ms / nsteps * 1e-3), "ms_per_step": ms / nsteps,
                       "pressure_iterations_per_step": t[2]["iterations"],
+                      "pressure_ms_per_step": t[2]["ms"],
+                      "pressure_us_per_iteration": 1e3 * t[2]["ms"] / max(1, t[2]["iterations"]),
                       "velocity_iterations_per_step": t[1]["iterations"]}
         s.close()
     out["spectral_vs_plain"] = out["spectral + unregularised momentum"]["value"] / out["plain"]["value"]
@@ -720,6 +723,8 @@ def run_ours(args):
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
     barrier(dist)
     e2e_ms = 0.0
+    g.synchronize()
+    host0 = time.perf_counter()
     for _ in range(e2e_steps):
         g.timer_start()
         for f in STATE_FIELDS:
@@ -728,8 +733,12 @@ def run_ours(args):
         for f in STATE_FIELDS:
             g.download(f, out=blocks[f])
         e2e_ms += g.timer_stop()
+    # the downloads are synchronous: the host holds every step's state when
+    # its call returns, so the host clock here is what a caller observes
+    e2e_host_ms = (time.perf_counter() - host0) * 1e3
     barrier(dist)
-    e2e_max = max_over_ranks(dist, e2e_ms)
+    e2e_max = max_over_ranks(dist, e2e_host_ms)
+    e2e_device_max = max_over_ranks(dist, e2e_ms)
     e2e_value = ws * cells * e2e_steps / (e2e_max * 1e-3)
 
     # ---- per-solver timing: the next steps launch by launch, CUDA events
@@ -809,7 +818,8 @@ def run_ours(args):
                        "graphs": "substeps replayed from CUDA graphs in the timed steps: %d of %d"
                                  % (graph_steps, 3 * (args.warmup + args.steps))},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "steps": e2e_steps},
+                    "steps": e2e_steps, "clock": "host wall clock around the C ABI calls",
+                    "ms_per_step": e2e_max / e2e_steps, "device_ms_per_step": e2e_device_max / e2e_steps},
             "gpu_launches": launches,
             "mass": mass_report,
             "roofline": {"kernel": names[dom], "bound": "hbm", "achieved": achieved, "peak": peak,

@@ -420,13 +420,21 @@ int pvof_clamp_mass_total(const pvof_ctx *ctx, double *total);
  * for the context's stream and drops its captured substep graphs. */
 int pvof_set_cluster_solvers(pvof_ctx *ctx, int enabled);
 
-/* No counterpart in the reference: the host-computed tables of the spectral
- * pressure preconditioner's cyclic reduction for an N x M grid (x spacing
- * squared inverse idx2, y idy2), without a GPU: for each round st = 0 ..
- * R - 1 (R = ceil(log2 M)) the multipliers k1 then k2, each [N/2 + 1][M] (one
- * row per wave number), then the reciprocal diagonals [N/2 + 1][M].  Returns
- * the number of doubles, (2 R + 1) (N/2 + 1) M, and writes them to out when
- * cap is at least that; -1 on invalid sizes. */
+/* No counterpart in the reference: the host-computed table of the spectral
+ * pressure preconditioner's tridiagonal solves for an N x M grid (x spacing
+ * squared inverse idx2, y idy2), without a GPU.  The systems
+ * a_j z_{j-1} + b_j z_j + c_j z_{j+1} = r_j (a = c = -1 inside,
+ * b_j = lambda_m + 2 inside, lambda_m + 1 at the walls; the mean mode's
+ * first row pinned) are solved by a partition method: the M rows split into
+ * P = min(32, M / 2) chunks, chunk l starting at l base + min(l, rem) with
+ * base + (l < rem) rows (base = M / P, rem = M mod P; K the longest).  Per
+ * wave number m = 0 .. N/2, (2K + 4) rows of 32 doubles, entry [row][l]:
+ * row i (1 <= i < chunk length) the elimination pivot r_i, row K + i the
+ * coupling A_i to the chunk's first unknown, row 0 the chunk's c_0, row K its
+ * a_0, rows 2K .. 2K + 3 the Thomas pivot and c' of the reduced system's
+ * equations 2l and 2l + 1.  Returns the number of doubles, (N/2 + 1)(2K + 4)
+ * 32, and writes them to out when cap is at least that; -1 on invalid sizes
+ * (N a power of two >= 2, M >= 2). */
 long long pvof_spectral_tables(int N, int M, double idx2, double idy2, double *out, long long cap);
 int pvof_solver_timing(const pvof_ctx *ctx, int solver, double *ms, long long *launches, long long *iterations,
                        long long *cell_iters);

@@ -14,7 +14,7 @@
 #include <thread>
 #include <vector>
 
-#include "pvof_kernels.cuh"
+#include "pvof_particles.cuh"
 
 using namespace pvof;
 
@@ -737,12 +737,12 @@ int p_solve_spectral(pvof_ctx *c)
         c->spec_fscale = 1.0 / (idy2 * (double)N);
         c->spec_blocks = spec_pcg_blocks(c->device, N, M);
         if (c->spec_blocks <= 0) return set_err(PVOF_ECUDA, "the spectral pressure solve needs a cooperative launch");
-        std::vector<double> tw, pcr;
-        c->spec_rounds = spec_tables(N, M, idx2, idy2, tw, pcr);
+        std::vector<double> tw, tri;
+        spec_tables(N, M, idx2, idy2, tw, tri);
         const size_t parts = 3 * (size_t)c->spec_blocks;
         std::vector<double> h(tw);
         h.resize(h.size() + parts, 0.0);
-        h.insert(h.end(), pcr.begin(), pcr.end());
+        h.insert(h.end(), tri.begin(), tri.end());
         if (cudaMalloc(&c->spec_mem, h.size() * sizeof(double)) != cudaSuccess ||
             cudaMalloc(&c->spec_s, sizeof(SpecScal)) != cudaSuccess)
             return set_err(PVOF_ENOMEM, "allocating the spectral preconditioner");
@@ -766,12 +766,11 @@ int p_solve_spectral(pvof_ctx *c)
     A.hat = S(c, SC_P_HAT);
     A.tw = reinterpret_cast<const double2 *>(c->spec_mem);
     A.part = c->spec_mem + N;
-    A.pcr = A.part + 3 * (size_t)c->spec_blocks;
+    A.tri = A.part + 3 * (size_t)c->spec_blocks;
     A.N = N;
     A.logN = 0;
     while ((1 << A.logN) < N) A.logN++;
     A.M = M;
-    A.rounds = c->spec_rounds;
     A.fscale = c->spec_fscale;
     A.tol = c->p.P_CG_ETOL;
     A.maxit = c->p.P_CG_MAXIT;
@@ -950,9 +949,11 @@ int poisson_pass(pvof_ctx *c, bool warm)
 }
 
 // The region above as a CUDA graph.  Its launches and their arguments depend
-// on the host state in GraphKey only (without resolved particles, whose list
-// bookkeeping reads the device, without the learned warm start, and without
-// solver timing, whose events must be recorded launch by launch); a key is
+// on the host state in GraphKey only (resolved particles included: their
+// bookkeeping runs on the device, its launches cover the capacities set by
+// pvof_set_particles, which drops the captured graphs; without the learned
+// warm start, and without solver timing, whose events must be recorded
+// launch by launch); a key is
 // captured the second time it is seen, so lazy set-up (allocations, tables)
 // has run outside the capture, and replayed after that.  A key whose capture
 // fails runs its launches directly from then on.
@@ -991,9 +992,21 @@ bool keep_cooperative(cudaGraph_t g)
     return true;
 }
 
+// waits for the context's stream and drops its captured substeps (after a
+// change of the launches or buffers they hold)
+void drop_graphs(pvof_ctx *c)
+{
+    cudaStreamSynchronize(c->stream);
+    for (GraphEntry &g : c->graphs) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g = GraphEntry();
+    }
+    c->graph_next = 0;
+}
+
 int run_region(pvof_ctx *c, bool warm0)
 {
-    if (!c->use_graphs || c->solver_timing || resolved(c) || c->p.pressure_warm_start == 2)
+    if (!c->use_graphs || c->solver_timing || c->p.pressure_warm_start == 2)
         return substep_region(c, warm0);
     GraphKey k;
     k.stage = c->stage;
@@ -1091,37 +1104,18 @@ int substep(pvof_ctx *c, pvof_stats *st)
 }  // namespace
 
 struct pvof::IbmState {
-    std::vector<IbmEntry> mobile, fixed;   // owned particles, in list order
-    std::vector<IbmEntry> entries;         // lists after the last update (mobile, then fixed)
-    IbmMarkers markers;
     HostMetrics hm;
-    IbmGrid grid;
+    PSet P;                                // host copy: pointers, capacities, grid; counts as last set by the host
+    PSet *d_ps = nullptr;                  // the device copy the kernels update
     double *d_coord = nullptr;             // xu, xc, yv, yc, each offset by NG
     const double *xu = nullptr, *xc = nullptr, *yv = nullptr, *yc = nullptr;
-    IbmEntryDev *d_ent = nullptr;
-    size_t cap_ent = 0;
-    double *d_mk = nullptr;                // XL, YL, vol, UL, rhoL, FL
-    int *d_flag = nullptr;
-    size_t cap_mk = 0;
-    double *d_FT = nullptr;
-    double *d_sums = nullptr;              // k_ibm_particle_sums output, 6 per entry
-    double *d_geo = nullptr;
-    size_t cap_geo = 0;
-    int ngeo = 0;
-    double *d_plist = nullptr;             // x, y, R, ID of the current list entries (contact-line normals)
-    size_t cap_plist = 0;
-    int n_plist = 0;
+    char *d_mem = nullptr;                 // every buffer of P, one allocation
     bool flagged = false;
     ~IbmState()
     {
-        cudaFree(d_plist);
+        cudaFree(d_mem);
+        cudaFree(d_ps);
         cudaFree(d_coord);
-        cudaFree(d_ent);
-        cudaFree(d_mk);
-        cudaFree(d_flag);
-        cudaFree(d_FT);
-        cudaFree(d_sums);
-        cudaFree(d_geo);
     }
 };
 
@@ -1131,37 +1125,44 @@ int ibm_state(pvof_ctx *c, IbmState **out)
 {
     if (c->ibm) { *out = c->ibm; return PVOF_OK; }
     IbmState *s = new IbmState();
+    std::memset(&s->P, 0, sizeof(PSet));
     build_metrics(c->g, c->dom.NX, c->dom.NY, s->hm);
     const size_t nx = s->hm.xu.size(), ny = s->hm.yv.size();
-    if (cudaMalloc(&s->d_coord, (2 * nx + 2 * ny) * sizeof(double)) != cudaSuccess) {
+    if (cudaMalloc(&s->d_coord, (2 * nx + 2 * ny) * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&s->d_ps, sizeof(PSet)) != cudaSuccess) {
         delete s;
-        return set_err(PVOF_ENOMEM, "cudaMalloc particle coordinates");
+        return set_err(PVOF_ENOMEM, "cudaMalloc particle state");
     }
     std::vector<double> h;
     for (auto *v : {&s->hm.xu, &s->hm.xc, &s->hm.yv, &s->hm.yc}) h.insert(h.end(), v->begin(), v->end());
     CK(cudaMemcpyAsync(s->d_coord, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     s->xu = s->d_coord + NG;
     s->xc = s->d_coord + nx + NG;
     s->yv = s->d_coord + 2 * nx + NG;
     s->yc = s->d_coord + 2 * nx + ny + NG;
-    IbmGrid &g = s->grid;
-    g.NX = c->dom.NX;
-    g.NY = c->dom.NY;
+    PGrid &g = s->P.g;
+    const int NX = c->dom.NX, NY = c->dom.NY;
+    g.NX = NX;
+    g.NY = NY;
     g.periodic[0] = c->dom.perx;
     g.periodic[1] = c->dom.pery;
     g.axisym = c->dom.axisym;
-    g.xu = s->hm.xu.data() + NG;
-    g.yv = s->hm.yv.data() + NG;
-    g.xc = s->hm.xc.data() + NG;
-    g.yc = s->hm.yc.data() + NG;
     g.h = s->hm.dx_u[1 + NG];
     double dymin = s->hm.dy_v[NG];
-    for (int j = 0; j < c->dom.NY; j++) dymin = std::min(dymin, s->hm.dy_v[j + NG]);
+    for (int j = 0; j < NY; j++) dymin = std::min(dymin, s->hm.dy_v[j + NG]);
     g.dy_min = dymin;
     g.slab = c->dom.slab;
     g.twod_slab = c->g.slab_thickness;
     g.Lx = c->g.xmax - c->g.xmin;
     g.Ly = c->g.ymax - c->g.ymin;
+    g.zs = c->g.zmin + 0.5 * (c->g.zmax - c->g.zmin);   // zc[G_Ks] of the storage plane
+    g.xu0 = s->hm.xu[NG];
+    g.xuN = s->hm.xu[NX - 1 + NG];
+    g.yv0 = s->hm.yv[NG];
+    g.yvN = s->hm.yv[NY - 1 + NG];
+    g.xcm1 = s->hm.xc[NG - 1];
+    g.ycm1 = s->hm.yc[NG - 1];
     c->ibm = s;
     *out = s;
     return PVOF_OK;
@@ -1170,128 +1171,73 @@ int ibm_state(pvof_ctx *c, IbmState **out)
 // the particle state of a context in the resolved-particle mode
 int ibm_need(pvof_ctx *c, IbmState **out)
 {
-    if (!c->ibm) return set_err(PVOF_EINVAL, "pvof_set_particles() first");
+    if (!c->ibm || !c->ibm->d_mem) return set_err(PVOF_EINVAL, "pvof_set_particles() first");
     *out = c->ibm;
     return PVOF_OK;
 }
 
-// the entries the reference's particle lists hold at this point, in list
-// order (mobile list, then fixed), for mcl_nearest_particle_normal
-// (VOF_IBM_wetting.c:118-182): the owned particles until the first list
-// update of a substep, the updated lists (with periodic copies) after it
-int ibm_upload_plist(IbmState *s, const std::vector<const IbmEntry *> &list, cudaStream_t stream)
+// the device copy's counts and error state (waits for the stream)
+int ibm_read(pvof_ctx *c, IbmState *s, PSet &h)
 {
-    std::vector<double> h;
-    h.reserve(4 * list.size());
-    for (const IbmEntry *e : list) {
-        h.push_back(e->X[0]);
-        h.push_back(e->X[1]);
-        h.push_back(e->R);
-        h.push_back((double)e->id);
-    }
-    if (h.size() > s->cap_plist) {
-        cudaFree(s->d_plist);
-        s->d_plist = nullptr;
-        if (cudaMalloc(&s->d_plist, h.size() * sizeof(double)) != cudaSuccess) {
-            s->cap_plist = 0;
-            return set_err(PVOF_ENOMEM, "cudaMalloc particle list");
-        }
-        s->cap_plist = h.size();
-    }
-    if (!h.empty()) CK(cudaMemcpyAsync(s->d_plist, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-    s->n_plist = (int)list.size();
+    CK(cudaMemcpyAsync(&h, s->d_ps, sizeof(PSet), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return PVOF_OK;
 }
 
-// Particle_MPI_update of both lists and Lagrangian_flag_points (Temporal_int.c:678-681)
+// the bookkeeping's error state as an error code and message
+int ibm_check(pvof_ctx *c, IbmState *s)
+{
+    PSet h;
+    TRY(ibm_read(c, s, h));
+    if (h.err == 0) return PVOF_OK;
+    char msg[256];
+    if (h.err == 1 && h.err_b >= 0)
+        snprintf(msg, sizeof(msg), "particles %d and %d within the lubrication range: the collision models are not built",
+                 h.err_a, h.err_b);
+    else if (h.err == 1)
+        snprintf(msg, sizeof(msg), "particle %d within the lubrication range of a wall: the collision models are not built",
+                 h.err_a);
+    else
+        snprintf(msg, sizeof(msg), "the particle lists or markers outgrew their capacity");
+    return set_err(PVOF_EINVAL, msg);
+}
+
+// Particle_MPI_update of both lists and Lagrangian_flag_points
+// (Temporal_int.c:678-681), on the device
 int ibm_flag_points(pvof_ctx *c)
 {
     IbmState *s;
     TRY(ibm_need(c, &s));
-    ibm_build(s->mobile, s->fixed, s->grid, c->p.Cn, s->entries, s->markers);
-    const size_t ne = s->entries.size(), nm = s->markers.x.size();
-    if (ne > s->cap_ent) {
-        cudaFree(s->d_ent);
-        cudaFree(s->d_FT);
-        cudaFree(s->d_sums);
-        s->d_ent = nullptr;
-        s->d_FT = nullptr;
-        s->d_sums = nullptr;
-        if (cudaMalloc(&s->d_ent, ne * sizeof(IbmEntryDev)) != cudaSuccess ||
-            cudaMalloc(&s->d_FT, 6 * ne * sizeof(double)) != cudaSuccess ||
-            cudaMalloc(&s->d_sums, 6 * ne * sizeof(double)) != cudaSuccess) {
-            s->cap_ent = 0;
-            return set_err(PVOF_ENOMEM, "cudaMalloc particle entries");
-        }
-        s->cap_ent = ne;
-    }
-    if (nm > s->cap_mk) {
-        cudaFree(s->d_mk);
-        cudaFree(s->d_flag);
-        s->d_mk = nullptr;
-        s->d_flag = nullptr;
-        if (cudaMalloc(&s->d_mk, 6 * nm * sizeof(double)) != cudaSuccess ||
-            cudaMalloc(&s->d_flag, 3 * nm * sizeof(int)) != cudaSuccess) {
-            s->cap_mk = 0;
-            return set_err(PVOF_ENOMEM, "cudaMalloc particle markers");
-        }
-        s->cap_mk = nm;
-    }
-    std::vector<IbmEntryDev> ed(ne);
-    const double zs = c->g.zmin + 0.5 * (c->g.zmax - c->g.zmin);   // zc[G_Ks] of the storage plane
-    for (size_t q = 0; q < ne; q++) {
-        const IbmEntry &e = s->entries[q];
-        IbmEntryDev &o = ed[q];
-        for (int k = 0; k < 3; k++) { o.X[k] = e.X[k]; o.U[k] = e.U[k]; o.Omega[k] = e.Omega[k]; }
-        o.X[2] = zs;
-        o.Zs = zs;
-        o.moff = e.moff;
-        o.mcount = e.mcount;
-        for (int k = 0; k < 4; k++) o.box[k] = e.box[k];
-        o.R = e.R;
-        o.id = (double)e.id;
-        ibm_momentum_boxes(e, s->grid, s->hm.xc.data() + NG, s->hm.yc.data() + NG, o.mbox);
-    }
-    if (ne) {
-        CK(cudaMemcpyAsync(s->d_ent, ed.data(), ne * sizeof(IbmEntryDev), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemsetAsync(s->d_FT, 0, 6 * ne * sizeof(double), c->stream));
-    }
-    if (nm) {
-        CK(cudaMemcpyAsync(s->d_mk, s->markers.x.data(), nm * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(s->d_mk + nm, s->markers.y.data(), nm * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(s->d_mk + 2 * nm, s->markers.vol.data(), nm * sizeof(double), cudaMemcpyHostToDevice,
-                           c->stream));
-        CK(cudaMemcpyAsync(s->d_flag, s->markers.flag.data(), nm * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    }
-    CK(cudaStreamSynchronize(c->stream));   // the host vectors may change with the next update
-    std::vector<const IbmEntry *> cur;
-    for (const IbmEntry &e : s->entries) cur.push_back(&e);
-    TRY(ibm_upload_plist(s, cur, c->stream));
+    k_ps_update<<<1, 32, 0, c->stream>>>(s->d_ps);
+    CKL(c);
+    k_ps_markers<<<1, PS_MARKER_THREADS, 0, c->stream>>>(s->d_ps);
+    CKL(c);
     s->flagged = true;
     return PVOF_OK;
 }
 
 IbmDev ibm_dev(pvof_ctx *c, IbmState *s)
 {
-    const size_t nm = s->markers.x.size();
+    const PSet &P = s->P;
+    const size_t cap = (size_t)P.cap_mk;
     IbmDev D;
-    D.ent = s->d_ent;
-    D.XL = s->d_mk;
-    D.YL = s->d_mk + nm;
-    D.vol = s->d_mk + 2 * nm;
-    D.UL = s->d_mk + 3 * nm;
-    D.rhoL = s->d_mk + 4 * nm;
-    D.FL = s->d_mk + 5 * nm;
-    D.flag = s->d_flag;
-    D.sup_i = s->d_flag + nm;
-    D.sup_j = s->d_flag + 2 * nm;
-    D.FT = s->d_FT;
-    const int NX = c->dom.NX, NY = c->dom.NY;
-    D.xlo = s->hm.xu[NG];
-    D.xhi = s->hm.xu[NX - 1 + NG];
-    D.ylo = s->hm.yv[NG];
-    D.yhi = s->hm.yv[NY - 1 + NG];
-    D.h = s->grid.h;
+    D.ent = P.dent;
+    D.ne = &s->d_ps->ne;
+    D.XL = P.mk;
+    D.YL = P.mk + cap;
+    D.vol = P.mk + 2 * cap;
+    D.UL = P.mk + 3 * cap;
+    D.rhoL = P.mk + 4 * cap;
+    D.FL = P.mk + 5 * cap;
+    D.flag = P.mflag;
+    D.sup_i = P.mflag + cap;
+    D.sup_j = P.mflag + 2 * cap;
+    D.FT = P.FT;
+    D.xlo = P.g.xu0;
+    D.xhi = P.g.xuN;
+    D.ylo = P.g.yv0;
+    D.yhi = P.g.yvN;
+    D.h = P.g.h;
     D.dxu1 = s->hm.dx_u[1 + NG];
     D.slab = c->dom.slab > 0.0 ? c->dom.slab : D.dxu1;
     D.dyv = c->dom.m.dy_v;
@@ -1300,7 +1246,9 @@ IbmDev ibm_dev(pvof_ctx *c, IbmState *s)
     return D;
 }
 
-// Lagrangian_force (Lagrangian.c:1724-1871) without the squirmer, one-way and post-processing options
+// Lagrangian_force (Lagrangian.c:1724-1871) without the squirmer, one-way and
+// post-processing options.  The marker and entry launches cover the
+// capacities and read the counts on the device.
 int ibm_force(pvof_ctx *c, int force_iter)
 {
     IbmState *s = c->ibm;
@@ -1310,10 +1258,10 @@ int ibm_force(pvof_ctx *c, int force_iter)
     const double dtbeta = bet(c->stage) * c->dt;
     const double idt2beta = 1.0 / (2.0 * bet(c->stage) * c->dt);
     const int corrector = force_iter >= 0, iters = corrector ? force_iter : 1;
-    const int ne = (int)s->entries.size(), nm = (int)s->markers.x.size();
     IbmDev D = ibm_dev(c, s);
+    const int *nm = &s->d_ps->nm;
     const dim3 cb(128), cg((unsigned)((NX + 127) / 128), (unsigned)NY);
-    const unsigned mg = (unsigned)((nm + 127) / 128);
+    const unsigned mg = (unsigned)((s->P.cap_mk + 127) / 128), eg = (unsigned)s->P.cap_ent;
     double *U = F(c, PVOF_F_U), *V = F(c, PVOF_F_V), *RU = F(c, PVOF_F_U_RHS), *RV = F(c, PVOF_F_V_RHS);
     const double *rho = F(c, PVOF_F_RHO);
     for (int ii = 0; ii < iters; ii++) {
@@ -1325,27 +1273,21 @@ int ibm_force(pvof_ctx *c, int force_iter)
             k_ibm_ng_update<<<cg, cb, 0, c->stream>>>(d, RV, nullptr, 1);
             CKL(c);
         }
-        if (nm > 0) {
-            k_ibm_interp<<<mg, 128, 0, c->stream>>>(d, rho, s->xc, s->yc, D.h, D.XL, D.YL, nm,
-                                                    d.axisym ? IBM_AXIS_EVEN : IBM_AXIS_NONE, D.rhoL);
-            CKL(c);
-        }
+        k_ibm_interp<<<mg, 128, 0, c->stream>>>(d, rho, s->xc, s->yc, D.h, D.XL, D.YL, nm,
+                                                d.axisym ? IBM_AXIS_EVEN : IBM_AXIS_NONE, D.rhoL);
+        CKL(c);
         for (int comp = 0; comp < 2; comp++) {
             const double *xs = comp == 0 ? s->xu : s->xc, *ys = comp == 0 ? s->yc : s->yv;
-            if (nm > 0) {
-                const int axis = !d.axisym ? IBM_AXIS_NONE : (comp == 0 ? IBM_AXIS_ODD : IBM_AXIS_EVEN);
-                k_ibm_interp<<<mg, 128, 0, c->stream>>>(d, comp == 0 ? U : V, xs, ys, D.h, D.XL, D.YL, nm, axis, D.UL);
-                CKL(c);
-            }
-            if (ne > 0) {
-                const double xs0 = comp == 0 ? s->hm.xu[NG] : s->hm.xc[NG];
-                const double ys0 = comp == 0 ? s->hm.yc[NG] : s->hm.yv[NG];
-                k_ibm_marker_force<<<(unsigned)ne, IBM_FORCE_THREADS, 0, c->stream>>>(D, comp, xs0, ys0, idt2beta,
-                                                                                     (!corrector && comp == 0) ? 1 : 0);
-                CKL(c);
-                k_ibm_spread<<<cg, cb, 0, c->stream>>>(d, D, ne, comp, xs, ys, rho, comp == 0 ? RU : RV);
-                CKL(c);
-            }
+            const int axis = !d.axisym ? IBM_AXIS_NONE : (comp == 0 ? IBM_AXIS_ODD : IBM_AXIS_EVEN);
+            k_ibm_interp<<<mg, 128, 0, c->stream>>>(d, comp == 0 ? U : V, xs, ys, D.h, D.XL, D.YL, nm, axis, D.UL);
+            CKL(c);
+            const double xs0 = comp == 0 ? s->hm.xu[NG] : s->hm.xc[NG];
+            const double ys0 = comp == 0 ? s->hm.yc[NG] : s->hm.yv[NG];
+            k_ibm_marker_force<<<eg, IBM_FORCE_THREADS, 0, c->stream>>>(D, comp, xs0, ys0, idt2beta,
+                                                                        (!corrector && comp == 0) ? 1 : 0);
+            CKL(c);
+            k_ibm_spread<<<cg, cb, 0, c->stream>>>(d, D, comp, xs, ys, rho, comp == 0 ? RU : RV);
+            CKL(c);
         }
         if (corrector) {
             k_ibm_correct<<<cg, cb, 0, c->stream>>>(d, 0, dtbeta, RU, rho, U);
@@ -1378,50 +1320,36 @@ int vel_explicit(pvof_ctx *c, int comp)
     return PVOF_OK;
 }
 
-// VOF_DIFFUSE_compute_C_S (VOF_DIFFUSE.c:685-813)
+// VOF_DIFFUSE_compute_C_S (VOF_DIFFUSE.c:685-813): the particles' geometry
+// from the owned lists on the device, then the field
 int compute_C_S(pvof_ctx *c)
 {
     IbmState *s;
     TRY(ibm_need(c, &s));
-    std::vector<double> geo;
-    ibm_solid_geometry(s->mobile, s->fixed, s->grid, geo);
-    if (geo.size() > s->cap_geo) {
-        cudaFree(s->d_geo);
-        s->d_geo = nullptr;
-        if (cudaMalloc(&s->d_geo, geo.size() * sizeof(double)) != cudaSuccess) {
-            s->cap_geo = 0;
-            return set_err(PVOF_ENOMEM, "cudaMalloc particle geometry");
-        }
-        s->cap_geo = geo.size();
-    }
-    s->ngeo = (int)(geo.size() / 3);
-    if (!geo.empty())
-        CK(cudaMemcpyAsync(s->d_geo, geo.data(), geo.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    k_ps_geo<<<1, 32, 0, c->stream>>>(s->d_ps);
+    CKL(c);
     double shift, denom, extra;
     ibm_solid_constants(c->p.Cn, shift, denom, extra);
     const Dom &d = c->dom;
     const dim3 cb(128), cg((unsigned)((d.NX + 2 * NG + 127) / 128), (unsigned)(d.NY + 2 * NG));
-    k_compute_C_S<<<cg, cb, 0, c->stream>>>(d, s->xc, s->yc, s->d_geo, s->ngeo, shift, denom, extra, F(c, PVOF_F_C_S));
+    k_compute_C_S<<<cg, cb, 0, c->stream>>>(d, s->xc, s->yc, s->P.geo, &s->d_ps->ngeo, shift, denom, extra,
+                                             F(c, PVOF_F_C_S));
     CKL(c);
     TRY(fill(c, BK_SCALAR, F(c, PVOF_F_C_S)));
     TRY(bound(c));
     TRY(fill(c, BK_SCALAR, F(c, PVOF_F_C_L)));
     TRY(phase_cache(c));
-    TRY(fill(c, BK_SCALAR, F(c, PVOF_F_C_G)));
-    CK(cudaStreamSynchronize(c->stream));   // the geometry host vector is released on return
-    return PVOF_OK;
+    return fill(c, BK_SCALAR, F(c, PVOF_F_C_G));
 }
 
-// Pressure_solve_xz_period (psolve_fft.c:638-983) in the planar mode
 // per-entry momentum integrals (and with ccf the capillary contact force) of
-// the current list entries, read back into the host entries
+// the current list entries, into the device's sums
 int ibm_sums(pvof_ctx *c, bool ccf)
 {
     IbmState *s = c->ibm;
-    const int ne = (int)s->entries.size();
-    if (ne == 0) return PVOF_OK;
     IbmSumArgs A;
-    A.ent = s->d_ent;
+    A.ent = s->P.dent;
+    A.ne = &s->d_ps->ne;
     A.U = F(c, PVOF_F_U);
     A.V = F(c, PVOF_F_V);
     A.CL = F(c, PVOF_F_C_L);
@@ -1430,73 +1358,40 @@ int ibm_sums(pvof_ctx *c, bool ccf)
     A.xc = s->xc;
     A.yv = s->yv;
     A.yc = s->yc;
-    A.plist = s->d_plist;
-    A.np = s->n_plist;
-    A.h = s->grid.h;
-    A.slab = c->dom.slab > 0.0 ? c->dom.slab : s->grid.h;   // Interpolate_twod_cell_volume
+    A.plist = s->P.plist;
+    A.np = &s->d_ps->np;
+    A.h = s->P.g.h;
+    A.slab = c->dom.slab > 0.0 ? c->dom.slab : s->P.g.h;   // Interpolate_twod_cell_volume
     A.sigma = 1.0 / c->p.We;
     const double theta = c->p.contact_angle_deg * M_PI / 180.0;
     A.ct = std::cos(theta);
     A.st = std::sin(theta);
     const double epsN = 1.0e-14;
-    const double h_ref = (s->grid.dy_min > epsN) ? s->grid.dy_min : epsN;
+    const double h_ref = (s->P.g.dy_min > epsN) ? s->P.g.dy_min : epsN;
     const double cn = (c->p.Cn > 0.0) ? c->p.Cn : 0.0;
     A.support_width = 8.0 * ((cn > h_ref) ? cn : h_ref);
     A.nk = c->dom.nk;
     A.ccf = ccf ? 1 : 0;
     A.axisym = c->dom.axisym;
     A.theta_span = c->g.theta_span;
-    A.out = s->d_sums;
-    k_ibm_particle_sums<<<(unsigned)ne, 256, 0, c->stream>>>(c->dom, A);
+    A.out = s->P.sums;
+    k_ibm_particle_sums<<<(unsigned)s->P.cap_ent, 256, 0, c->stream>>>(c->dom, A);
     CKL(c);
-    std::vector<double> h(6 * (size_t)ne), ft(6 * (size_t)ne);
-    CK(cudaMemcpyAsync(h.data(), s->d_sums, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(ft.data(), s->d_FT, ft.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    for (int q = 0; q < ne; q++) {
-        IbmEntry &e = s->entries[(size_t)q];
-        const double *o = h.data() + 6 * q;
-        for (int k = 0; k < 3; k++) {
-            e.F[k] = ft[6 * (size_t)q + (size_t)k];
-            e.T[k] = ft[6 * (size_t)q + 3 + (size_t)k];
-            e.Int_U[k] = e.Int_Omega[k] = e.F_CCF[k] = e.T_CCF[k] = 0.0;
-        }
-        e.Int_U[0] = o[0];
-        e.Int_U[1] = o[1];
-        e.Int_Omega[2] = o[2];
-        if (ccf) {
-            e.F_CCF[0] = o[3];
-            e.F_CCF[1] = o[4];
-            e.T_CCF[2] = o[5];
-        }
-    }
     return PVOF_OK;
 }
 
-// the two lists of the current entries (mobile entries come first)
-void ibm_split(const IbmState *s, std::vector<IbmEntry> &mob, std::vector<IbmEntry> &fix)
-{
-    mob.clear();
-    fix.clear();
-    for (const IbmEntry &e : s->entries) (e.mobile ? mob : fix).push_back(e);
-}
-
 // the end of a substep with resolved particles (Temporal_int.c:1186-1238):
-// momentum integrals and contact-line forces of every list entry on the
-// device, then Lagrangian_advect_particles on the host
+// momentum integrals and contact-line forces of every list entry, their
+// collection into the owned particles and Lagrangian_advect_particles, all on
+// the device; the host reads back only the error state
 int ibm_advect(pvof_ctx *c)
 {
     IbmState *s = c->ibm;
     if (!s || !s->flagged) return set_err(PVOF_EINVAL, "pvof_Lagrangian_flag_points() first");
     TRY(ibm_sums(c, true));
-    std::vector<IbmEntry> mob, fix;
-    ibm_split(s, mob, fix);
-    s->mobile = ibm_collect(mob, s->grid);
-    s->fixed = ibm_collect(fix, s->grid);
-    std::string err;
-    if (!ibm_advance(s->mobile, s->fixed, s->grid, c->p.Cn, c->stage, c->dt, c->p.grav, err))
-        return set_err(PVOF_EINVAL, err);
-    return PVOF_OK;
+    k_ps_collect<<<1, 32, 0, c->stream>>>(s->d_ps, PS_ADVANCE, 1, c->stage, c->dt);
+    CKL(c);
+    return ibm_check(c, s);
 }
 
 // Particle_initialize_velocities (Lagrangian/Particle.c:322-535): mobile
@@ -1508,44 +1403,23 @@ int ibm_velocity_init(pvof_ctx *c)
     IbmState *s = c->ibm;
     TRY(ibm_flag_points(c));
     TRY(ibm_sums(c, false));
-    std::vector<IbmEntry> mob, fix;
-    ibm_split(s, mob, fix);
-    s->mobile = ibm_collect(mob, s->grid);
-    s->fixed = ibm_collect(fix, s->grid);
-    for (IbmEntry &p : s->mobile) {
-        for (int i = 0; i < 3; i++) p.U[i] = p.Int_U[i] * p.rho_s / p.M;
-        for (int i = 0; i < 3; i++) p.Omega[i] = p.Int_Omega[i] * p.rho_s / p.I_p;
-        for (int i = 0; i < 3; i++) p.U_old[i] = p.U[i];
-        for (int i = 0; i < 3; i++) p.Omega_old[i] = p.Omega[i];
-    }
+    k_ps_collect<<<1, 32, 0, c->stream>>>(s->d_ps, PS_INIT_VELOCITY, 0, 0, 0.0);
+    CKL(c);
     TRY(ibm_flag_points(c));
     double *U = F(c, PVOF_F_U), *V = F(c, PVOF_F_V);
-    std::vector<IbmEntryDev> ed(s->entries.size());
-    CK(cudaMemcpy(ed.data(), s->d_ent, ed.size() * sizeof(IbmEntryDev), cudaMemcpyDeviceToHost));
-    for (size_t q = 0; q < s->entries.size(); q++) {
-        if (!s->entries[q].mobile) continue;
-        for (int comp = 0; comp < 2; comp++) {
-            const int *b = ed[q].mbox[comp];
-            if (b[1] <= b[0] || b[3] <= b[2]) continue;
-            const dim3 blk(16, 16), grd((unsigned)((b[1] - b[0] + 15) / 16), (unsigned)((b[3] - b[2] + 15) / 16));
-            k_ibm_paint<<<grd, blk, 0, c->stream>>>(c->dom, ed[q], comp, s->xu, s->xc, s->yv, s->yc,
-                                                    comp == 0 ? U : V);
-            CKL(c);
-        }
+    const dim3 blk(16, 16), grd((unsigned)((c->dom.NX + 15) / 16), (unsigned)((c->dom.NY + 15) / 16));
+    for (int comp = 0; comp < 2; comp++) {
+        k_ps_paint<<<grd, blk, 0, c->stream>>>(c->dom, s->d_ps, comp, s->xu, s->xc, s->yv, s->yc, comp == 0 ? U : V);
+        CKL(c);
     }
     TRY(fill(c, BK_WRAP_U, U));
     TRY(fill(c, BK_WRAP_V, V));
     TRY(fill(c, BK_U, U));
     TRY(fill(c, BK_V, V));
     TRY(ibm_sums(c, false));
-    ibm_split(s, mob, fix);
-    s->mobile = ibm_collect(mob, s->grid);
-    s->fixed = ibm_collect(fix, s->grid);
-    for (IbmEntry &p : s->mobile) {
-        for (int i = 0; i < 3; i++) p.Int_U_old[i] = p.Int_U[i];
-        for (int i = 0; i < 3; i++) p.Int_Omega_old[i] = p.Int_Omega[i];
-    }
-    return PVOF_OK;
+    k_ps_collect<<<1, 32, 0, c->stream>>>(s->d_ps, PS_INIT_MOMENTUM, 0, 0, 0.0);
+    CKL(c);
+    return ibm_check(c, s);
 }
 
 // contact-line projection (VOF_IBM_wetting.c:1021-2131; kernels in pvof_mcl.cu)
@@ -1554,11 +1428,11 @@ int mcl_normals(pvof_ctx *c)
     IbmState *s;
     TRY(ibm_need(c, &s));
     const Dom &d = c->dom;
-    const double h_ref = (s->grid.dy_min > 0.0) ? s->grid.dy_min : 1.0e-14;
+    const double h_ref = (s->P.g.dy_min > 0.0) ? s->P.g.dy_min : 1.0e-14;
     const double cn = (c->p.Cn > 0.0) ? c->p.Cn : 0.0;
     const double support_width = 8.0 * ((cn > h_ref) ? cn : h_ref);
     const dim3 blk(128), grd((unsigned)((d.NX + 2 * NG + 127) / 128), (unsigned)(d.NY + 2 * NG));
-    k_mcl_normals<<<grd, blk, 0, c->stream>>>(d, s->xc, s->yc, F(c, PVOF_F_C_S), s->d_plist, s->n_plist,
+    k_mcl_normals<<<grd, blk, 0, c->stream>>>(d, s->xc, s->yc, F(c, PVOF_F_C_S), s->P.plist, &s->d_ps->np,
                                               support_width, F(c, PVOF_F_NX_IBM), F(c, PVOF_F_NY_IBM));
     CKL(c);
     if (d.axisym) {
@@ -2170,11 +2044,7 @@ int pvof_set_cluster_solvers(pvof_ctx *c, int enabled)
     ENTER(c);
     // the captured substeps hold the old solver launches: wait for them and drop them
     CK(cudaStreamSynchronize(c->stream));
-    for (GraphEntry &g : c->graphs) {
-        if (g.exec) cudaGraphExecDestroy(g.exec);
-        g = GraphEntry();
-    }
-    c->graph_next = 0;
+    drop_graphs(c);
     const StripPlan none = {0, 0};
     const StripPlan &pp = enabled ? c->cgs_p_fit : none;
     const StripPlan &vp = enabled ? c->cgs_v_fit : none;
@@ -2187,14 +2057,14 @@ int pvof_set_cluster_solvers(pvof_ctx *c, int enabled)
 
 long long pvof_spectral_tables(int N, int M, double idx2, double idy2, double *out, long long cap)
 {
-    if (N < 2 || (N & (N - 1)) != 0 || M < 1 || !(idx2 > 0.0) || !(idy2 > 0.0)) {
-        set_err(PVOF_EINVAL, "pvof_spectral_tables: N a power of two >= 2, M >= 1, positive spacings");
+    if (N < 2 || (N & (N - 1)) != 0 || M < 2 || !(idx2 > 0.0) || !(idy2 > 0.0)) {
+        set_err(PVOF_EINVAL, "pvof_spectral_tables: N a power of two >= 2, M >= 2, positive spacings");
         return -1;
     }
-    std::vector<double> tw, pcr;
-    spec_tables(N, M, idx2, idy2, tw, pcr);
-    const long long n = (long long)pcr.size();
-    if (out && cap >= n) std::memcpy(out, pcr.data(), pcr.size() * sizeof(double));
+    std::vector<double> tw, tri;
+    spec_tables(N, M, idx2, idy2, tw, tri);
+    const long long n = (long long)tri.size();
+    if (out && cap >= n) std::memcpy(out, tri.data(), tri.size() * sizeof(double));
     return n;
 }
 
@@ -2238,18 +2108,23 @@ int pvof_set_particles(pvof_ctx *c, const pvof_particle *parts, int n)
 {
     ENTER(c);
     if (n < 0 || (n > 0 && !parts)) return set_err(PVOF_EINVAL, "bad particle array");
-    IbmState *s;
-    TRY(ibm_state(c, &s));
-    s->mobile.clear();
-    s->fixed.clear();
     for (int q = 0; q < n; q++) {
-        const pvof_particle &p = parts[q];
-        if (!(p.R > 0.0)) return set_err(PVOF_EINVAL, "particle radius must be positive");
+        if (!(parts[q].R > 0.0)) return set_err(PVOF_EINVAL, "particle radius must be positive");
         // Lagrangian_generate_points_2d (Lagrangian.c:2948-2959): axisymmetric
         // particles are spheres centred on the axis
-        if (c->dom.axisym && std::fabs(p.X[0]) > 1.0e-14)
+        if (c->dom.axisym && std::fabs(parts[q].X[0]) > 1.0e-14)
             return set_err(PVOF_EINVAL, "an axisymmetric particle must sit on the axis (X[0] = 0)");
-        IbmEntry e;
+    }
+    IbmState *s;
+    TRY(ibm_state(c, &s));
+    CK(cudaStreamSynchronize(c->stream));   // the buffers below may be in use
+    PGrid &g = s->P.g;
+    g.Cn = c->p.Cn;
+    for (int k = 0; k < 3; k++) g.grav[k] = c->p.grav[k];
+    std::vector<PEnt> mob, fix;
+    for (int q = 0; q < n; q++) {
+        const pvof_particle &p = parts[q];
+        PEnt e;
         std::memset(&e, 0, sizeof(e));
         e.X[0] = p.X[0];
         e.X[1] = p.X[1];
@@ -2258,17 +2133,86 @@ int pvof_set_particles(pvof_ctx *c, const pvof_particle *parts, int n)
         e.U[1] = p.U[1];
         e.Omega[2] = p.Omega_z;
         e.rho_s = p.rho_s;
-        (p.mobile ? s->mobile : s->fixed).push_back(e);
+        (p.mobile ? mob : fix).push_back(e);
     }
     // IDs as Particle_initialize gives them: fixed first, then mobile (Particle.c:213-221)
     int id = 0;
-    for (IbmEntry &e : s->fixed) e.id = id++;
-    for (IbmEntry &e : s->mobile) e.id = id++;
+    for (PEnt &e : fix) e.id = id++;
+    for (PEnt &e : mob) e.id = id++;
+    std::vector<const PEnt *> by_id(n);
+    for (PEnt &e : fix) by_id[e.id] = &e;
+    for (PEnt &e : mob) by_id[e.id] = &e;
+    for (PEnt &e : mob) { e.mobile = 1; ps_derived(e, g); }
+    for (PEnt &e : fix) { e.mobile = 0; ps_derived(e, g); }
+    std::vector<double> trig;
+    std::vector<int> trig_off(n > 0 ? n : 1, 0);
+    long long nl = 0;
+    for (int q = 0; q < n; q++) {
+        trig_off[q] = (int)nl;
+        ps_marker_table(*by_id[q], g, trig);
+        nl += by_id[q]->N_L;
+    }
+    // capacities: a particle has at most two copies per periodic axis, so at
+    // most nine entries; markers likewise
+    PSet &P = s->P;
+    P.cap_own = n > 0 ? n : 1;
+    P.cap_ent = 9 * P.cap_own;
+    P.cap_mk = (int)std::max(9 * nl, 1LL);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+    const size_t o_mob = take(sizeof(PEnt) * P.cap_own), o_fix = take(sizeof(PEnt) * P.cap_own);
+    const size_t o_ent = take(sizeof(PEnt) * P.cap_ent), o_tmp = take(sizeof(PEnt) * 3 * (size_t)P.cap_ent);
+    const size_t o_dent = take(sizeof(IbmEntryDev) * P.cap_ent);
+    const size_t o_mk = take(sizeof(double) * 6 * (size_t)P.cap_mk), o_flag = take(sizeof(int) * 4 * (size_t)P.cap_mk);
+    const size_t o_trig = take(sizeof(double) * std::max<size_t>(trig.size(), 1));
+    const size_t o_toff = take(sizeof(int) * trig_off.size());
+    const size_t o_plist = take(sizeof(double) * 4 * (size_t)P.cap_ent);
+    const size_t o_geo = take(sizeof(double) * 3 * (size_t)P.cap_own);
+    const size_t o_FT = take(sizeof(double) * 6 * (size_t)P.cap_ent), o_sums = take(sizeof(double) * 6 * (size_t)P.cap_ent);
+    cudaFree(s->d_mem);
+    s->d_mem = nullptr;
+    if (cudaMalloc(&s->d_mem, off) != cudaSuccess) return set_err(PVOF_ENOMEM, "cudaMalloc particle state");
+    char *m = s->d_mem;
+    P.mob = (PEnt *)(m + o_mob);
+    P.fix = (PEnt *)(m + o_fix);
+    P.ent = (PEnt *)(m + o_ent);
+    P.tmp = (PEnt *)(m + o_tmp);
+    P.dent = (IbmEntryDev *)(m + o_dent);
+    P.mk = (double *)(m + o_mk);
+    P.mflag = (int *)(m + o_flag);
+    P.trig = (const double *)(m + o_trig);
+    P.trig_off = (const int *)(m + o_toff);
+    P.plist = (double *)(m + o_plist);
+    P.geo = (double *)(m + o_geo);
+    P.FT = (double *)(m + o_FT);
+    P.sums = (double *)(m + o_sums);
+    P.nmob = (int)mob.size();
+    P.nfix = (int)fix.size();
+    P.ne = P.nm = P.ngeo = P.err = 0;
+    P.err_a = P.err_b = -1;
+    // the contact-line list before the first update: the owned lists
+    std::vector<double> pl;
+    for (const std::vector<PEnt> *l : {&mob, &fix})
+        for (const PEnt &e : *l) {
+            pl.push_back(e.X[0]);
+            pl.push_back(e.X[1]);
+            pl.push_back(e.R);
+            pl.push_back((double)e.id);
+        }
+    P.np = n;
+    CK(cudaMemsetAsync(s->d_mem, 0, off, c->stream));
+    if (!mob.empty()) CK(cudaMemcpyAsync(P.mob, mob.data(), mob.size() * sizeof(PEnt), cudaMemcpyHostToDevice, c->stream));
+    if (!fix.empty()) CK(cudaMemcpyAsync(P.fix, fix.data(), fix.size() * sizeof(PEnt), cudaMemcpyHostToDevice, c->stream));
+    if (!trig.empty())
+        CK(cudaMemcpyAsync((void *)P.trig, trig.data(), trig.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync((void *)P.trig_off, trig_off.data(), trig_off.size() * sizeof(int), cudaMemcpyHostToDevice,
+                       c->stream));
+    if (!pl.empty()) CK(cudaMemcpyAsync(P.plist, pl.data(), pl.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(s->d_ps, &P, sizeof(PSet), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));   // the host vectors are released on return
     s->flagged = false;
-    std::vector<const IbmEntry *> cur;
-    for (const IbmEntry &e : s->mobile) cur.push_back(&e);
-    for (const IbmEntry &e : s->fixed) cur.push_back(&e);
-    return ibm_upload_plist(s, cur, c->stream);
+    drop_graphs(c);
+    return PVOF_OK;
 }
 
 int pvof_Lagrangian_flag_points(pvof_ctx *c) { ENTER(c); return ibm_flag_points(c); }
@@ -2277,7 +2221,9 @@ int pvof_particle_entries(pvof_ctx *c)
 {
     ENTER(c);
     if (!c->ibm || !c->ibm->flagged) return set_err(PVOF_EINVAL, "pvof_Lagrangian_flag_points() first");
-    return (int)c->ibm->entries.size();
+    PSet h;
+    TRY(ibm_read(c, c->ibm, h));
+    return h.ne;
 }
 
 int pvof_particle_forces(pvof_ctx *c, double *Fo, double *To, int nmax)
@@ -2285,10 +2231,12 @@ int pvof_particle_forces(pvof_ctx *c, double *Fo, double *To, int nmax)
     ENTER(c);
     IbmState *s = c->ibm;
     if (!s || !s->flagged) return set_err(PVOF_EINVAL, "pvof_Lagrangian_flag_points() first");
-    const int ne = (int)s->entries.size();
+    PSet hs;
+    TRY(ibm_read(c, s, hs));
+    const int ne = hs.ne;
     if (nmax < ne || !Fo || !To) return set_err(PVOF_EINVAL, "force arrays too small");
     std::vector<double> h(6 * (size_t)ne);
-    if (ne) CK(cudaMemcpyAsync(h.data(), s->d_FT, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (ne) CK(cudaMemcpyAsync(h.data(), s->P.FT, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     for (int e = 0; e < ne; e++)
         for (int k = 0; k < 3; k++) {
@@ -2303,15 +2251,18 @@ int pvof_particle_markers(pvof_ctx *c, int entry, double *x, double *y, double *
     ENTER(c);
     IbmState *s = c->ibm;
     if (!s || !s->flagged) return set_err(PVOF_EINVAL, "pvof_Lagrangian_flag_points() first");
-    if (entry < 0 || entry >= (int)s->entries.size()) return set_err(PVOF_EINVAL, "bad particle entry");
-    const IbmEntry &e = s->entries[(size_t)entry];
+    PSet hs;
+    TRY(ibm_read(c, s, hs));
+    if (entry < 0 || entry >= hs.ne) return set_err(PVOF_EINVAL, "bad particle entry");
+    PEnt e;
+    CK(cudaMemcpy(&e, s->P.ent + entry, sizeof(PEnt), cudaMemcpyDeviceToHost));
     if (nmax < e.mcount) return set_err(PVOF_EINVAL, "marker arrays too small");
-    for (int q = 0; q < e.mcount; q++) {
-        const size_t m = (size_t)(e.moff + q);
-        if (x) x[q] = s->markers.x[m];
-        if (y) y[q] = s->markers.y[m];
-        if (vol) vol[q] = s->markers.vol[m];
-        if (flag) flag[q] = s->markers.flag[m];
+    const size_t cap = (size_t)s->P.cap_mk;
+    if (e.mcount > 0) {
+        if (x) CK(cudaMemcpy(x, s->P.mk + e.moff, e.mcount * sizeof(double), cudaMemcpyDeviceToHost));
+        if (y) CK(cudaMemcpy(y, s->P.mk + cap + e.moff, e.mcount * sizeof(double), cudaMemcpyDeviceToHost));
+        if (vol) CK(cudaMemcpy(vol, s->P.mk + 2 * cap + e.moff, e.mcount * sizeof(double), cudaMemcpyDeviceToHost));
+        if (flag) CK(cudaMemcpy(flag, s->P.mflag + e.moff, e.mcount * sizeof(int), cudaMemcpyDeviceToHost));
     }
     return e.mcount;
 }
@@ -2364,15 +2315,20 @@ int pvof_pressure_network_sample(pvof_ctx *c, int stage, float *x, float *t)
 int pvof_get_particles(pvof_ctx *c, pvof_particle *out, int *ids, double *Fo, double *To, int nmax)
 {
     ENTER(c);
-    if (!c->ibm) return set_err(PVOF_EINVAL, "pvof_set_particles() first");
-    const IbmState *s = c->ibm;
-    const int n = (int)(s->mobile.size() + s->fixed.size());
+    IbmState *s;
+    TRY(ibm_need(c, &s));
+    PSet h;
+    TRY(ibm_read(c, s, h));
+    const int n = h.nmob + h.nfix;
     if (nmax < n || (n > 0 && !out)) return set_err(PVOF_EINVAL, "particle array too small");
+    std::vector<PEnt> mob(h.nmob), fix(h.nfix);
+    if (h.nmob) CK(cudaMemcpy(mob.data(), s->P.mob, h.nmob * sizeof(PEnt), cudaMemcpyDeviceToHost));
+    if (h.nfix) CK(cudaMemcpy(fix.data(), s->P.fix, h.nfix * sizeof(PEnt), cudaMemcpyDeviceToHost));
     int q = 0;
-    for (const std::vector<IbmEntry> *l : {&s->mobile, &s->fixed})
-        for (const IbmEntry &e : *l) {
+    for (const std::vector<PEnt> *l : {&mob, &fix})
+        for (const PEnt &e : *l) {
             pvof_particle &p = out[q];
-            p.mobile = l == &s->mobile ? 1 : 0;
+            p.mobile = l == &mob ? 1 : 0;
             p.X[0] = e.X[0];
             p.X[1] = e.X[1];
             p.R = e.R;

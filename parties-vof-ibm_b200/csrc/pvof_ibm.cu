@@ -15,9 +15,12 @@
 //                                              Interpolate_Eul_to_Lag_twod / _Lag_to_Eul_uniform_twod
 //                                              and delta (Lagrangian/Interpolate.c:390-560)
 //
-// Particle bookkeeping (lists, periodic copies, markers, flags) is host work on
-// a few hundred markers; the gathers, the per-particle force and torque sums
-// and the spreads run on the device.  The spread is written as a gather: each
+// Everything runs on the device: the particle bookkeeping (lists, periodic
+// copies, markers, flags, rigid-body motion; the list logic is shared with
+// the host in pvof_particles.cuh) in one-thread or one-block kernels over a
+// handful of particles and a few hundred markers, the gathers, the
+// per-particle force and torque sums and the spreads.  Only the marker
+// tables of each particle are made on the host, once.  The spread is written as a gather: each
 // cell adds the contributions of a particle's markers in marker order, which
 // is the order in which the reference's scatter adds them, so the result is
 // the reference's to the last bit.
@@ -28,23 +31,20 @@
 #include <string>
 
 #include "pvof_device.cuh"
-#include "pvof_kernels.cuh"
+#include "pvof_particles.cuh"
 
 namespace pvof {
 
-constexpr double IBM_PI = 3.14159265358979323846;   // PI, Include/definitions.h:7
-constexpr double DELTA_FUNC_RADIUS = 1.5;           // Include/definitions.h:58
-constexpr double LAG_FLAG_RANGE = 3.0;              // Include/definitions.h:61
-constexpr double LUB_RANGE = 2.0;                   // [particle] lub_range default (IO/default.inp)
+constexpr double IBM_PI = PS_PI;
 
 // ---------------------------------------------------------------------------
-// host: particle lists, markers and flags
+// host: per-particle constants
 // ---------------------------------------------------------------------------
 
 // Particle_calc_derived_data (Lagrangian/Particle.c:663-733): planar
 // cylinders per slab thickness; axisymmetric spheres keep the sphere's mass
 // and moment of inertia, with one ring marker per ceil(pi R / h) (at least 4)
-static void derived_data(IbmEntry &e, const IbmGrid &g)
+void ps_derived(PEnt &e, const PGrid &g)
 {
     const double h = g.dy_min;
     const double R = e.R, R2 = R * R;
@@ -65,212 +65,38 @@ static void derived_data(IbmEntry &e, const IbmGrid &g)
     e.Vol_L = (2.0 * IBM_PI * e.R / e.N_L) * slab * h;
 }
 
-// Particle_ibm_exchange_range (Lagrangian/Particle.c:26-47) plus the marker-flag
-// and lubrication ranges added in Particle_MPI_update (:2052-2060)
-static double exchange_range(const IbmGrid &g, double Cn)
-{
-    const double h = g.h;
-    double range = DELTA_FUNC_RADIUS * h;
-    const double h_ref = (g.dy_min > 0.0) ? g.dy_min : h;
-    const double cn = (Cn > 0.0) ? Cn : 0.0;
-    const double wetting = 8.0 * ((cn > h_ref) ? cn : h_ref);
-    if (wetting > range) range = wetting;
-    range += LAG_FLAG_RANGE * h;
-    const double lub = 0.5 * LUB_RANGE * h;
-    return range > lub ? range : lub;
-}
-
-// One list of Particle_MPI_update on a single rank: local -> local + periodic
-// copies; copies are prepended in the order the exchanges add them.
-static std::vector<IbmEntry> update_list(const std::vector<IbmEntry> &local, const IbmGrid &g, double Cn)
-{
-    std::vector<IbmEntry> list = local;
-    const double range = exchange_range(g, Cn);
-    for (int axis = 0; axis < 2; axis++) {
-        if (!g.periodic[axis]) continue;
-        const double lo = (axis == 0 ? g.xu[0] : g.yv[0]) + range;
-        const double hi = (axis == 0 ? g.xu[g.NX - 1] : g.yv[g.NY - 1]) - range;
-        const double L = axis == 0 ? g.Lx : g.Ly;
-        std::vector<IbmEntry> low, high;
-        // a copy carries the whole particle, its previous position shifted too
-        for (const IbmEntry &p : list)
-            if (p.X[axis] - p.R < lo) {
-                IbmEntry c = p;
-                c.X[axis] += L;
-                c.X_old[axis] += L;
-                c.copy = 1;
-                low.push_back(c);
-            }
-        for (const IbmEntry &p : list)
-            if (p.X[axis] + p.R > hi) {
-                IbmEntry c = p;
-                c.X[axis] -= L;
-                c.X_old[axis] -= L;
-                c.copy = 1;
-                high.push_back(c);
-            }
-        std::vector<IbmEntry> out = high;
-        out.insert(out.end(), low.begin(), low.end());
-        out.insert(out.end(), list.begin(), list.end());
-        list.swap(out);
-    }
-    return list;
-}
-
-// Lagrangian_near_point_2d (Lagrangian/Lagrangian.c:86-96)
-static bool near_point(double x, double y, double range, const IbmGrid &g)
-{
-    const double xs = g.xu[0], xe = g.xu[g.NX - 1], ys = g.yv[0], ye = g.yv[g.NY - 1];
-    return xs - x < range && x - xe < range && ys - y < range && y - ye < range;
-}
-
+// The marker table of one particle for k_ps_markers, after
 // Lagrangian_generate_points_2d (Lagrangian/Lagrangian.c:2900-2991): planar
-// markers on the circle, line segment x slab x h each; axisymmetric markers on
-// the meridian of a sphere centred on the axis, midpoints in the polar angle,
-// each the spherical band 2 pi R^2 (cos theta_m - cos theta_p) times h
-static void generate_points(IbmEntry &e, const IbmGrid &g, IbmMarkers &m)
+// markers on the circle at the angle midpoints, (cos, sin, segment x slab x h);
+// axisymmetric markers on the meridian at the polar-angle midpoints,
+// (sin, cos, the spherical band 2 pi R^2 (cos theta_m - cos theta_p) times h)
+void ps_marker_table(const PEnt &e, const PGrid &g, std::vector<double> &tab)
 {
     const double h = g.h;
-    const double range = DELTA_FUNC_RADIUS * h;
     if (g.axisym) {
         const double dtheta = IBM_PI / e.N_L;
-        e.moff = (int)m.x.size();
         for (int mv = 0; mv < e.N_L; mv++) {
             const double theta = (mv + 0.5) * dtheta;
             const double theta_m = mv * dtheta;
             const double theta_p = (mv + 1) * dtheta;
-            const double r_ring = e.R * sin(theta);
-            const double z_axial = e.X[1] + e.R * cos(theta);
-            const double ring_volume = (2.0 * IBM_PI) * e.R * e.R * (cos(theta_m) - cos(theta_p)) * h;
-            if (near_point(r_ring, z_axial, range, g)) {
-                m.x.push_back(r_ring);
-                m.y.push_back(z_axial);
-                m.vol.push_back(ring_volume);
-                m.flag.push_back(1);
-            }
+            tab.push_back(sin(theta));
+            tab.push_back(cos(theta));
+            tab.push_back((2.0 * IBM_PI) * e.R * e.R * (cos(theta_m) - cos(theta_p)) * h);
+            tab.push_back(0.0);
         }
-        e.mcount = (int)m.x.size() - e.moff;
         return;
     }
     const double dtheta = 2.0 * IBM_PI / e.N_L;
     const double ds = e.R * dtheta;
     double slab = g.slab;
     if (slab <= 0.0) slab = h;
-    e.moff = (int)m.x.size();
     for (int mv = 0; mv < e.N_L; mv++) {
         const double theta = (mv + 0.5) * dtheta;
-        const double nx = cos(theta), ny = sin(theta);
-        const double x = e.X[0] + e.R * nx;
-        const double y = e.X[1] + e.R * ny;
-        if (near_point(x, y, range, g)) {
-            m.x.push_back(x);
-            m.y.push_back(y);
-            m.vol.push_back(ds * slab * h);
-            m.flag.push_back(1);
-        }
+        tab.push_back(cos(theta));
+        tab.push_back(sin(theta));
+        tab.push_back(ds * slab * h);
+        tab.push_back(0.0);
     }
-    e.mcount = (int)m.x.size() - e.moff;
-}
-
-// Lagrangian_flag_points_individual (Lagrangian/Lagrangian.c:2629-2690), 2D
-static void flag_individual(const IbmEntry &p, const IbmEntry &p2, const IbmGrid &g, IbmMarkers &m)
-{
-    const double h = g.h;
-    double dpp = p.R + p2.R + LAG_FLAG_RANGE * h;
-    dpp = dpp * dpp;
-    double dlp = p2.R + LAG_FLAG_RANGE * h;
-    dlp = dlp * dlp;
-    double r0 = p2.X[0] - p.X[0], r1 = p2.X[1] - p.X[1];
-    if (!(r0 * r0 + r1 * r1 < dpp)) return;
-    for (int q = p.moff; q < p.moff + p.mcount; q++) {
-        r0 = p2.X[0] - m.x[q];
-        r1 = p2.X[1] - m.y[q];
-        const double d2 = r0 * r0 + r1 * r1;
-        if (m.flag[q] == 1 && d2 < dlp) m.flag[q] = 0;
-    }
-}
-
-// Lagrangian_flag_points_wall (Lagrangian/Lagrangian.c:2697-2795), x and y walls
-static void flag_walls(const IbmEntry &p, const IbmGrid &g, IbmMarkers &m)
-{
-    const double h = g.h;
-    const double dpw = p.R + 0.5 * LAG_FLAG_RANGE * h;
-    const double dlw = 0.5 * LAG_FLAG_RANGE * h;
-    auto wall = [&](int axis, double pos) {
-        const double c = axis == 0 ? p.X[0] : p.X[1];
-        if (!(fabs(c - pos) < dpw)) return;
-        for (int q = p.moff; q < p.moff + p.mcount; q++) {
-            const double v = axis == 0 ? m.x[q] : m.y[q];
-            if (m.flag[q] == 1 && fabs(v - pos) < dlw) m.flag[q] = 0;
-        }
-    };
-    if (!g.periodic[0]) {
-        if (!g.axisym) wall(0, g.xu[0]);   // the axis is no wall (Lagrangian.c:2723)
-        wall(0, g.xu[g.NX - 1]);
-    }
-    if (!g.periodic[1]) {
-        wall(1, g.yv[0]);
-        wall(1, g.yv[g.NY - 1]);
-    }
-}
-
-void ibm_build(const std::vector<IbmEntry> &mobile_local, const std::vector<IbmEntry> &fixed_local, const IbmGrid &g,
-               double Cn, std::vector<IbmEntry> &entries, IbmMarkers &m)
-{
-    std::vector<IbmEntry> mob = update_list(mobile_local, g, Cn);
-    std::vector<IbmEntry> fix = update_list(fixed_local, g, Cn);
-    for (IbmEntry &e : mob) { e.mobile = 1; derived_data(e, g); }
-    for (IbmEntry &e : fix) { e.mobile = 0; derived_data(e, g); }
-    m = IbmMarkers();
-    // Lagrangian_flag_points: mobile list first, then fixed
-    for (IbmEntry &p : mob) {
-        generate_points(p, g, m);
-        for (const IbmEntry &p2 : mob)
-            if (p2.id != p.id) flag_individual(p, p2, g, m);
-        for (const IbmEntry &p2 : fix) flag_individual(p, p2, g, m);
-        flag_walls(p, g, m);
-    }
-    for (IbmEntry &p : fix) {
-        generate_points(p, g, m);
-        for (const IbmEntry &p2 : mob) flag_individual(p, p2, g, m);
-        for (const IbmEntry &p2 : fix)
-            if (p2.id != p.id) flag_individual(p, p2, g, m);
-        flag_walls(p, g, m);
-    }
-    entries = mob;
-    entries.insert(entries.end(), fix.begin(), fix.end());
-    // cell box of every particle's marker supports (3 x 3 stencils), for the spread
-    for (IbmEntry &e : entries) {
-        e.box[0] = e.box[2] = 1 << 30;
-        e.box[1] = e.box[3] = -(1 << 30);
-        for (int q = e.moff; q < e.moff + e.mcount; q++) {
-            const int i = (int)floor((m.x[q] - g.xu[0]) / g.h), j = (int)floor((m.y[q] - g.yv[0]) / g.h);
-            e.box[0] = std::min(e.box[0], i - 3);
-            e.box[1] = std::max(e.box[1], i + 4);
-            e.box[2] = std::min(e.box[2], j - 3);
-            e.box[3] = std::max(e.box[3], j + 4);
-        }
-    }
-}
-
-// VOF_DIFFUSE_compute_C_S geometry (VOF_DIFFUSE.c:57-85 through
-// Particle_collect_owned_overlaps, Lagrangian/Particle.c:1697-1786): on one
-// rank every particle whose centre the rank owns, unshifted -- the overlap
-// test takes the first shift that overlaps and the unshifted one always does
-// -- so a particle crossing a periodic boundary has no copy in C_S.  The
-// maximum over particles does not depend on their order.
-void ibm_solid_geometry(const std::vector<IbmEntry> &mobile_local, const std::vector<IbmEntry> &fixed_local,
-                        const IbmGrid &g, std::vector<double> &geo)
-{
-    geo.clear();
-    const double x0 = g.xu[0], x1 = g.xu[g.NX - 1], y0 = g.yv[0], y1 = g.yv[g.NY - 1];
-    for (const std::vector<IbmEntry> *l : {&mobile_local, &fixed_local})
-        for (const IbmEntry &p : *l) {
-            if (!(p.X[0] >= x0 && p.X[0] <= x1 && p.X[1] >= y0 && p.X[1] <= y1)) continue;
-            geo.push_back(p.X[0]);
-            geo.push_back(p.X[1]);
-            geo.push_back(p.R);
-        }
 }
 
 // diffuse_solid_support_extra (Eulerian/VOF_DIFFUSE.c:42-55) and the profile constants
@@ -287,237 +113,283 @@ void ibm_solid_constants(double cn, double &shift, double &denom, double &extra)
     extra = e > 0.0 ? e : 0.0;
 }
 
-void ibm_derive(IbmEntry &e, const IbmGrid &g) { derived_data(e, g); }
+// ---------------------------------------------------------------------------
+// device: particle bookkeeping
+// ---------------------------------------------------------------------------
 
-// cell ranges of Interpolate_integrate_momentum_twod and
-// Interpolate_paint_rigid_body_velocity_twod (Lagrangian/Interpolate.c:644-800):
-// u faces have cell edges at xc[i-1] and yv[j], v faces at xu[i] and yc[j-1]
-void ibm_momentum_boxes(const IbmEntry &e, const IbmGrid &g, const double *xc, const double *yc, int box[2][4])
+// Particle_MPI_update of both lists (mobile, then fixed), the entries'
+// momentum boxes, and the contact-line list (mcl_nearest_particle_normal,
+// VOF_IBM_wetting.c:118-182, reads the lists as they stand after the update)
+__global__ void k_ps_update(PSet *ps)
 {
-    const double h = g.h;
-    for (int comp = 0; comp < 2; comp++) {
-        const double xe0 = comp == 0 ? xc[-1] : g.xu[0];
-        const double ye0 = comp == 0 ? g.yv[0] : yc[-1];
-        int i_start = (int)floor((e.X[0] - e.R - xe0) / h);
-        int j_start = (int)floor((e.X[1] - e.R - ye0) / h);
-        int i_end = (int)ceil((e.X[0] + e.R - xe0) / h);
-        int j_end = (int)ceil((e.X[1] + e.R - ye0) / h);
-        i_start = std::max(i_start, 0);
-        j_start = std::max(j_start, 0);
-        i_end = std::min(std::min(i_end, g.NX), g.NX - 1);
-        j_end = std::min(std::min(j_end, g.NY), g.NY - 1);
-        box[comp][0] = i_start;
-        box[comp][1] = i_end;
-        box[comp][2] = j_start;
-        box[comp][3] = j_end;
-    }
-}
-
-// Particle_list_remove (Lagrangian/Particle.c:991-1090), 2D: a centre outside
-// [xu[0], xu[NX-1]) x [yv[0], yv[NY-1]) belongs to a periodic copy
-static bool outside(const IbmEntry &p, const IbmGrid &g)
-{
-    return p.X[0] < g.xu[0] || p.X[0] >= g.xu[g.NX - 1] || p.X[1] < g.yv[0] || p.X[1] >= g.yv[g.NY - 1];
-}
-
-std::vector<IbmEntry> ibm_collect(const std::vector<IbmEntry> &both, const IbmGrid &g)
-{
-    std::vector<IbmEntry> local;
-    std::vector<const IbmEntry *> foreign;
-    for (const IbmEntry &p : both) {
-        if (outside(p, g)) foreign.push_back(&p);
-        else local.push_back(p);
-    }
-    for (IbmEntry &p : local) {
-        p.copy = 0;
-        for (const IbmEntry *pf : foreign) {
-            if (pf->id != p.id) continue;
-            for (int i = 0; i < 3; i++) p.F[i] += pf->F[i];
-            for (int i = 0; i < 3; i++) p.T[i] += pf->T[i];
-            for (int i = 0; i < 3; i++) p.F_CCF[i] += pf->F_CCF[i];
-            for (int i = 0; i < 3; i++) p.T_CCF[i] += pf->T_CCF[i];
-            for (int i = 0; i < 3; i++) p.Int_U[i] += pf->Int_U[i];
-            for (int i = 0; i < 3; i++) p.Int_Omega[i] += pf->Int_Omega[i];
-        }
-    }
-    return local;
-}
-
-namespace {
-
-// RK3 coefficients (Include/definitions.h:197-204)
-const double RK_BET[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
-const double RK_GAM[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
-const double RK_ZET[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
-
-// Lagrangian_apply_twod_particle_constraints (Lagrangian/Lagrangian.c:105-129):
-// planar cylinders keep the spin about z only; axisymmetric spheres stay on
-// the axis and do not rotate
-void twod_constraints(IbmEntry &p, double zs, bool axisym)
-{
-    p.X[2] = zs;
-    p.X_old[2] = p.X[2];
-    p.U[2] = 0.0;
-    p.U_old[2] = 0.0;
-    if (axisym) {
-        p.X[0] = 0.0;
-        p.X_old[0] = 0.0;
-        p.U[0] = 0.0;
-        p.U_old[0] = 0.0;
-        for (int i = 0; i < 3; i++) p.Omega[i] = 0.0;
-        for (int i = 0; i < 3; i++) p.Omega_old[i] = 0.0;
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    PSet &S = *ps;
+    const PGrid &g = S.g;
+    const int m = ps_update_list(S.mob, S.nmob, S.ent, S.tmp, S.cap_ent, g);
+    const int f = m < 0 ? -1 : ps_update_list(S.fix, S.nfix, S.ent + m, S.tmp, S.cap_ent - m, g);
+    if (m < 0 || f < 0) {
+        S.err = 2;
+        S.ne = S.np = 0;
         return;
     }
-    p.Omega[0] = 0.0;
-    p.Omega[1] = 0.0;
-    p.Omega_old[0] = 0.0;
-    p.Omega_old[1] = 0.0;
+    S.ne = m + f;
+    for (int q = 0; q < S.ne; q++) {
+        PEnt &e = S.ent[q];
+        e.mobile = q < m ? 1 : 0;
+        ps_momentum_boxes(e, g);
+        double *pl = S.plist + 4 * q;
+        pl[0] = e.X[0];
+        pl[1] = e.X[1];
+        pl[2] = e.R;
+        pl[3] = (double)e.id;
+    }
+    S.np = S.ne;
 }
 
-// The ranges at which Collision_particle / Collision_wall
-// (Lagrangian/Collision.c:277-720) start to act: contact, or a surface gap
-// within lub_range * h (LUBRICATION_NORMAL).  Returns false if any pair or
-// wall is that close.
-bool out_of_contact(const std::vector<IbmEntry> &mob_both, const std::vector<IbmEntry> &fix_both, const IbmGrid &g,
-                    std::string &err)
+// Lagrangian_flag_points (Lagrangian/Lagrangian.c:2515-2800) for the entries
+// in list order: each entry's markers near the domain
+// (Lagrangian_generate_points_2d), compacted in marker order by a block scan;
+// then every marker's flag, cleared within LAG_FLAG_RANGE h of another
+// particle (Lagrangian_flag_points_individual, :2629-2690) or of an x or y
+// wall (Lagrangian_flag_points_wall, :2697-2795; the axis is no wall) -- the
+// flags only go from 1 to 0, so the order of the tests does not matter; then
+// each entry's cell box of its marker supports (3 x 3 stencils, for the
+// spread) and the entry as the force kernels read it.
+__global__ void __launch_bounds__(PS_MARKER_THREADS) k_ps_markers(PSet *ps)
 {
-    const double range = LUB_RANGE * g.h;
-    char msg[256];
-    for (size_t a = 0; a < mob_both.size(); a++) {
-        const IbmEntry &p = mob_both[a];
-        auto check = [&](const IbmEntry &q) {
-            if (q.id == p.id) return true;
-            const double c = p.R + q.R + range;
-            const double d0 = p.X[0] - q.X[0], d1 = p.X[1] - q.X[1];
-            if (d0 * d0 + d1 * d1 <= c * c) {
-                snprintf(msg, sizeof(msg),
-                         "particles %d and %d within the lubrication range: the collision models are not built", p.id,
-                         q.id);
-                err = msg;
-                return false;
+    __shared__ int s_cnt[PS_MARKER_THREADS / 32];
+    __shared__ int s_total, s_over;
+    __shared__ int s_box[4];
+    PSet &S = *ps;
+    const PGrid &g = S.g;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int ne = S.ne, cap = S.cap_mk;
+    double *mx = S.mk, *my = S.mk + cap, *mvol = S.mk + 2 * cap;
+    int *mflag = S.mflag, *mown = S.mflag + 3 * cap;
+    const double h = g.h, range = PS_DELTA_FUNC_RADIUS * h;
+    if (tid == 0) s_over = 0;
+    int base = 0;
+    for (int e = 0; e < ne; e++) {
+        const PEnt &E = S.ent[e];
+        const double *tab = S.trig + (size_t)S.trig_off[E.id] * PS_TRIG;
+        const int start = base;
+        for (int c0 = 0; c0 < E.N_L; c0 += blockDim.x) {
+            const int mv = c0 + tid;
+            bool near = false;
+            double x = 0.0, y = 0.0, vol = 0.0;
+            if (mv < E.N_L) {
+                const double *t = tab + (size_t)mv * PS_TRIG;
+                x = g.axisym ? E.R * t[0] : E.X[0] + E.R * t[0];
+                y = E.X[1] + E.R * t[1];
+                vol = t[2];
+                near = ps_near_point(x, y, range, g);
             }
-            return true;
-        };
-        for (size_t b = 0; b < mob_both.size(); b++)
-            if (!check(mob_both[b])) return false;
-        for (const IbmEntry &q : fix_both)
-            if (!check(q)) return false;
-        for (int axis = 0; axis < 2; axis++) {
+            const unsigned bal = __ballot_sync(0xffffffffu, near);
+            if (lane == 0) s_cnt[warp] = __popc(bal);
+            __syncthreads();
+            if (tid == 0) {
+                int run = 0;
+                for (int w = 0; w < nw; w++) {
+                    const int n = s_cnt[w];
+                    s_cnt[w] = run;
+                    run += n;
+                }
+                s_total = run;
+            }
+            __syncthreads();
+            if (near) {
+                const int pos = base + s_cnt[warp] + __popc(bal & ((1u << lane) - 1u));
+                if (pos < cap) {
+                    mx[pos] = x;
+                    my[pos] = y;
+                    mvol[pos] = vol;
+                    mflag[pos] = 1;
+                    mown[pos] = e;
+                } else {
+                    s_over = 1;
+                }
+            }
+            base += s_total;
+            __syncthreads();
+        }
+        if (tid == 0) {
+            S.ent[e].moff = start;
+            S.ent[e].mcount = base - start;
+        }
+    }
+    __syncthreads();
+    if (s_over || base > cap) {
+        if (tid == 0) {
+            S.err = 2;
+            S.nm = 0;
+            for (int e = 0; e < ne; e++) S.ent[e].mcount = 0;
+        }
+        base = 0;
+    }
+    __syncthreads();
+    const int nm = base;
+    for (int q = tid; q < nm; q += blockDim.x) {
+        const PEnt &P = S.ent[mown[q]];
+        int flag = mflag[q];
+        for (int e2 = 0; e2 < ne; e2++) {
+            const PEnt &P2 = S.ent[e2];
+            if (P2.id == P.id) continue;
+            double dpp = P.R + P2.R + PS_LAG_FLAG_RANGE * h;
+            dpp = dpp * dpp;
+            double dlp = P2.R + PS_LAG_FLAG_RANGE * h;
+            dlp = dlp * dlp;
+            double r0 = P2.X[0] - P.X[0], r1 = P2.X[1] - P.X[1];
+            if (!(r0 * r0 + r1 * r1 < dpp)) continue;
+            r0 = P2.X[0] - mx[q];
+            r1 = P2.X[1] - my[q];
+            const double d2 = r0 * r0 + r1 * r1;
+            if (flag == 1 && d2 < dlp) flag = 0;
+        }
+        const double dpw = P.R + 0.5 * PS_LAG_FLAG_RANGE * h;
+        const double dlw = 0.5 * PS_LAG_FLAG_RANGE * h;
+        for (int w = 0; w < 4; w++) {
+            const int axis = w >> 1;
             if (g.periodic[axis]) continue;
-            const double lo = axis == 0 ? g.xu[0] : g.yv[0];
-            const double hi = axis == 0 ? g.xu[g.NX - 1] : g.yv[g.NY - 1];
-            if (fabs(p.X[axis] - lo) - p.R <= range || fabs(hi - p.X[axis]) - p.R <= range) {
-                snprintf(msg, sizeof(msg),
-                         "particle %d within the lubrication range of a wall: the collision models are not built",
-                         p.id);
-                err = msg;
-                return false;
-            }
+            if (w == 0 && g.axisym) continue;   // the axis is no wall (Lagrangian.c:2723)
+            const double pos = w == 0 ? g.xu0 : (w == 1 ? g.xuN : (w == 2 ? g.yv0 : g.yvN));
+            const double c = axis == 0 ? P.X[0] : P.X[1];
+            if (!(fabs(c - pos) < dpw)) continue;
+            const double v = axis == 0 ? mx[q] : my[q];
+            if (flag == 1 && fabs(v - pos) < dlw) flag = 0;
+        }
+        mflag[q] = flag;
+    }
+    for (int e = 0; e < ne; e++) {
+        if (tid == 0) {
+            s_box[0] = s_box[2] = 1 << 30;
+            s_box[1] = s_box[3] = -(1 << 30);
+        }
+        __syncthreads();
+        const PEnt &E = S.ent[e];
+        int b0 = 1 << 30, b1 = -(1 << 30), b2 = 1 << 30, b3 = -(1 << 30);
+        for (int q = E.moff + tid; q < E.moff + E.mcount; q += blockDim.x) {
+            const int i = (int)floor((mx[q] - g.xu0) / h), j = (int)floor((my[q] - g.yv0) / h);
+            b0 = min(b0, i - 3);
+            b1 = max(b1, i + 4);
+            b2 = min(b2, j - 3);
+            b3 = max(b3, j + 4);
+        }
+        atomicMin(&s_box[0], b0);
+        atomicMax(&s_box[1], b1);
+        atomicMin(&s_box[2], b2);
+        atomicMax(&s_box[3], b3);
+        __syncthreads();
+        if (tid == 0)
+            for (int k = 0; k < 4; k++) S.ent[e].box[k] = s_box[k];
+        __syncthreads();
+    }
+    for (int e = tid; e < ne; e += blockDim.x) {
+        const PEnt &E = S.ent[e];
+        IbmEntryDev &o = S.dent[e];
+        for (int k = 0; k < 3; k++) { o.X[k] = E.X[k]; o.U[k] = E.U[k]; o.Omega[k] = E.Omega[k]; }
+        o.X[2] = g.zs;
+        o.Zs = g.zs;
+        o.moff = E.moff;
+        o.mcount = E.mcount;
+        for (int k = 0; k < 4; k++) o.box[k] = E.box[k];
+        o.R = E.R;
+        o.id = (double)E.id;
+        for (int c = 0; c < 2; c++)
+            for (int k = 0; k < 4; k++) o.mbox[c][k] = E.mbox[c][k];
+        for (int k = 0; k < 6; k++) S.FT[6 * e + k] = 0.0;
+    }
+    if (tid == 0) S.nm = nm;
+}
+
+// VOF_DIFFUSE_compute_C_S geometry (VOF_DIFFUSE.c:57-85 through
+// Particle_collect_owned_overlaps, Lagrangian/Particle.c:1697-1786): on one
+// rank every particle whose centre the rank owns, unshifted -- the overlap
+// test takes the first shift that overlaps and the unshifted one always does
+// -- so a particle crossing a periodic boundary has no copy in C_S.  The
+// maximum over particles does not depend on their order.
+__global__ void k_ps_geo(PSet *ps)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    PSet &S = *ps;
+    const PGrid &g = S.g;
+    int n = 0;
+    for (int q = 0; q < S.nmob + S.nfix; q++) {
+        const PEnt &p = q < S.nmob ? S.mob[q] : S.fix[q - S.nmob];
+        if (!(p.X[0] >= g.xu0 && p.X[0] <= g.xuN && p.X[1] >= g.yv0 && p.X[1] <= g.yvN)) continue;
+        S.geo[3 * n] = p.X[0];
+        S.geo[3 * n + 1] = p.X[1];
+        S.geo[3 * n + 2] = p.R;
+        n++;
+    }
+    S.ngeo = n;
+}
+
+// The end of a substep (Temporal_int.c:1186-1238) after k_ibm_particle_sums:
+// every entry takes its direct-forcing reaction (F, T of Lagrangian_force),
+// its momentum integrals (Int_U[0..1], Int_Omega[2]) and, with ccf, its
+// capillary contact force (F_CCF[0..1], T_CCF[2]); the two lists are
+// collected into the owned particles (the mobile entries come first); then
+// the mode's step.
+__global__ void k_ps_collect(PSet *ps, int mode, int ccf, int stage, double dt)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    PSet &S = *ps;
+    const PGrid &g = S.g;
+    if (S.err) return;
+    const int ne = S.ne;
+    int nmob_e = 0;
+    for (int q = 0; q < ne; q++) {
+        PEnt &e = S.ent[q];
+        const double *o = S.sums + 6 * q;
+        for (int k = 0; k < 3; k++) {
+            e.F[k] = S.FT[6 * q + k];
+            e.T[k] = S.FT[6 * q + 3 + k];
+            e.Int_U[k] = e.Int_Omega[k] = e.F_CCF[k] = e.T_CCF[k] = 0.0;
+        }
+        e.Int_U[0] = o[0];
+        e.Int_U[1] = o[1];
+        e.Int_Omega[2] = o[2];
+        if (ccf) {
+            e.F_CCF[0] = o[3];
+            e.F_CCF[1] = o[4];
+            e.T_CCF[2] = o[5];
+        }
+        if (e.mobile) nmob_e = q + 1;
+    }
+    const int m = ps_collect(S.ent, nmob_e, S.mob, S.cap_own, g);
+    const int f = ps_collect(S.ent + nmob_e, ne - nmob_e, S.fix, S.cap_own, g);
+    if (m < 0 || f < 0) {
+        S.err = 2;
+        return;
+    }
+    S.nmob = m;
+    S.nfix = f;
+    if (mode == PS_INIT_VELOCITY) {
+        for (int q = 0; q < m; q++) {
+            PEnt &p = S.mob[q];
+            for (int i = 0; i < 3; i++) p.U[i] = p.Int_U[i] * p.rho_s / p.M;
+            for (int i = 0; i < 3; i++) p.Omega[i] = p.Int_Omega[i] * p.rho_s / p.I_p;
+            for (int i = 0; i < 3; i++) p.U_old[i] = p.U[i];
+            for (int i = 0; i < 3; i++) p.Omega_old[i] = p.Omega[i];
+        }
+    } else if (mode == PS_INIT_MOMENTUM) {
+        for (int q = 0; q < m; q++) {
+            PEnt &p = S.mob[q];
+            for (int i = 0; i < 3; i++) p.Int_U_old[i] = p.Int_U[i];
+            for (int i = 0; i < 3; i++) p.Int_Omega_old[i] = p.Int_Omega[i];
+        }
+    } else if (mode == PS_ADVANCE) {
+        int nm = m, nf = f, who[2] = {-1, -1};
+        const int rc = ps_advance(S.mob, nm, S.fix, nf, S.tmp, S.cap_ent, S.cap_own, g, stage, dt, who);
+        S.nmob = nm;
+        S.nfix = nf;
+        if (rc) {
+            S.err = rc;
+            S.err_a = who[0];
+            S.err_b = who[1];
         }
     }
-    return true;
 }
-
-// the list updates and removals around Collision_evaluate
-// (Lagrangian/Lagrangian.c:1291-1303): copies across the periodic
-// boundaries, then the entries whose centre is in the domain, so a particle
-// that left through one side continues as its copy from the other
-bool relist(std::vector<IbmEntry> &mobile, std::vector<IbmEntry> &fixed, const IbmGrid &g, double Cn, std::string &err)
-{
-    std::vector<IbmEntry> mob = update_list(mobile, g, Cn), fix = update_list(fixed, g, Cn);
-    if (!out_of_contact(mob, fix, g, err)) return false;
-    mobile.clear();
-    for (const IbmEntry &p : mob)
-        if (!outside(p, g)) mobile.push_back(p);
-    fixed.clear();
-    for (const IbmEntry &p : fix)
-        if (!outside(p, g)) fixed.push_back(p);
-    for (IbmEntry &p : mobile) p.copy = 0;
-    for (IbmEntry &p : fixed) p.copy = 0;
-    return true;
-}
-
-}  // namespace
-
-bool ibm_advance(std::vector<IbmEntry> &mobile, std::vector<IbmEntry> &fixed, const IbmGrid &g, double Cn, int stage,
-                 double dt, const double grav[3], std::string &err)
-{
-    // Lagrangian_evaluate_fluid_forces (Lagrangian/Lagrangian.c:338-957), after
-    // the hydrodynamic collection; the diagnostic accumulators (F_IBM, F_rigid,
-    // F_CCF_cum, ...) change nothing downstream and are not kept
-    const double bt = RK_BET[stage];
-    const double idt2beta = 1.0 / (2.0 * bt * dt);
-    // axisymmetric: markers are full rings, so on an on-axis sphere the radial
-    // and azimuthal components and every torque cancel (Lagrangian.c:525-543,
-    // :819-837); only the axial force moves it
-    if (g.axisym)
-        for (std::vector<IbmEntry> *l : {&mobile, &fixed})
-            for (IbmEntry &p : *l) {
-                p.F[0] = 0.0;
-                p.F[2] = 0.0;
-                for (int i = 0; i < 3; i++) p.T[i] = 0.0;
-                p.Int_U[0] = 0.0;
-                p.Int_U[2] = 0.0;
-                for (int i = 0; i < 3; i++) p.Int_Omega[i] = 0.0;
-                p.F_CCF[0] = 0.0;
-                p.F_CCF[2] = 0.0;
-                for (int i = 0; i < 3; i++) p.T_CCF[i] = 0.0;
-            }
-    for (IbmEntry &p : mobile) {
-        const double int_rho = (p.rho_s > 0.0) ? p.M / p.rho_s : 0.0;   // Lagrangian_set_exact_solid_body_mass
-        for (int i = 0; i < 3; i++) p.F[i] += p.F_CCF[i];
-        for (int i = 0; i < 3; i++) p.T[i] += p.T_CCF[i];
-        for (int i = 0; i < 3; i++) p.F[i] += idt2beta * (p.Int_U[i] - p.Int_U_old[i]);
-        for (int i = 0; i < 3; i++) p.T[i] += idt2beta * (p.Int_Omega[i] - p.Int_Omega_old[i]);
-        for (int i = 0; i < 3; i++) p.Int_U_old[i] = p.Int_U[i];
-        for (int i = 0; i < 3; i++) p.Int_Omega_old[i] = p.Int_Omega[i];
-        for (int i = 0; i < 3; i++) p.F[i] += (p.M - int_rho) * grav[i];
-    }
-    for (IbmEntry &p : fixed) {
-        const double int_rho = (p.rho_s > 0.0) ? p.M / p.rho_s : 0.0;
-        for (int i = 0; i < 3; i++) p.F[i] += p.F_CCF[i];
-        for (int i = 0; i < 3; i++) p.T[i] += p.T_CCF[i];
-        for (int i = 0; i < 3; i++) p.Int_U_old[i] = p.Int_U[i];
-        for (int i = 0; i < 3; i++) p.Int_Omega_old[i] = p.Int_Omega[i];
-        for (int i = 0; i < 3; i++) p.F[i] += (p.M - int_rho) * grav[i];
-    }
-    // SUBSTEP (Lagrangian.c:293-318): 8, 2, 5 particle steps of dt / 15 per
-    // fluid stage, each a full RK3 of Lagrangian_integrate_particle_motion
-    // (Lagrangian.c:967-1640).  Out of contact range the collision forces and
-    // torques Fc, Tc are zero; the fixed particles keep their place.
-    const int nsub[3] = {8, 2, 5};
-    const double dts = dt / 15.0;
-    const double zs = mobile.empty() ? 0.0 : mobile[0].X[2];
-    for (int n = 0; n < nsub[stage]; n++)
-        for (int rk = 0; rk < 3; rk++) {
-            const double b = RK_BET[rk], gm = RK_GAM[rk], zt = RK_ZET[rk];
-            const double Fc = 0.0, Fc_old = 0.0;
-            for (IbmEntry &p : mobile) {   // predictor
-                const double dt_iM = dts / p.M, dt_iI = dts / p.I_p;
-                for (int i = 0; i < 3; i++) p.X_old[i] = p.X[i];
-                for (int i = 0; i < 3; i++) p.U_old[i] = p.U[i];
-                for (int i = 0; i < 3; i++) p.U[i] = p.U_old[i] + dt_iM * (2.0 * b * p.F[i] + gm * Fc + zt * Fc_old);
-                for (int i = 0; i < 3; i++) p.Omega_old[i] = p.Omega[i];
-                for (int i = 0; i < 3; i++)
-                    p.Omega[i] = p.Omega_old[i] + dt_iI * (2.0 * b * p.T[i] + gm * Fc + zt * Fc_old);
-                for (int i = 0; i < 3; i++) p.X[i] = p.X_old[i] + dts * b * (p.U[i] + p.U_old[i]);
-                twod_constraints(p, zs, g.axisym != 0);
-            }
-            if (!relist(mobile, fixed, g, Cn, err)) return false;
-            for (IbmEntry &p : mobile) {   // corrector
-                const double dt_iM = dts / p.M, dt_iI = dts / p.I_p;
-                for (int i = 0; i < 3; i++) p.U[i] = p.U_old[i] + dt_iM * b * (2.0 * p.F[i] + Fc + Fc_old);
-                for (int i = 0; i < 3; i++) p.Omega[i] = p.Omega_old[i] + dt_iI * b * (2.0 * p.T[i] + Fc + Fc_old);
-                for (int i = 0; i < 3; i++) p.X[i] = p.X_old[i] + dts * b * (p.U[i] + p.U_old[i]);
-                twod_constraints(p, zs, g.axisym != 0);
-            }
-        }
-    return true;
-}
-
-// ---------------------------------------------------------------------------
-// device
-// ---------------------------------------------------------------------------
 
 // delta (Lagrangian/Interpolate.c:551-560)
 __device__ __forceinline__ double ibm_delta(double r)
@@ -551,10 +423,10 @@ __device__ __forceinline__ int axis_fold(int i, int axis, int &sign)
 // Interpolate_Eul_to_Lag_twod (Interpolate.c:477-529): one marker per thread
 __global__ void k_ibm_interp(Dom d, const double *__restrict__ a, const double *__restrict__ xs,
                              const double *__restrict__ ys, double h, const double *__restrict__ XL,
-                             const double *__restrict__ YL, int nm, int axis, double *__restrict__ out)
+                             const double *__restrict__ YL, const int *nm, int axis, double *__restrict__ out)
 {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= nm) return;
+    if (m >= *nm) return;
     const int P = d.P;
     int i_start = (int)round((XL[m] - xs[0]) / h) - 1;
     int j_start = (int)round((YL[m] - ys[0]) / h) - 1;
@@ -590,6 +462,7 @@ __global__ void __launch_bounds__(IBM_FORCE_THREADS) k_ibm_marker_force(IbmDev D
     __shared__ double sh_f[IBM_FORCE_THREADS], sh_t[IBM_FORCE_THREADS];
     __shared__ int sh_ok[IBM_FORCE_THREADS];
     const int e = blockIdx.x, tid = threadIdx.x;
+    if (e >= *D.ne) return;   // launched for the capacity; the block's exit is uniform
     const IbmEntryDev &p = D.ent[e];
     const double h = D.h;
     double *Fp = D.FT + 6 * e, *Tp = Fp + 3;
@@ -666,7 +539,7 @@ __device__ __forceinline__ double ibm_cell_volume(const IbmDev &D, int comp, con
     return D.dxu1 * D.dyv[j] * ring;
 }
 
-__global__ void k_ibm_spread(Dom d, IbmDev D, int ne, int comp, const double *__restrict__ xs,
+__global__ void k_ibm_spread(Dom d, IbmDev D, int comp, const double *__restrict__ xs,
                              const double *__restrict__ ys, const double *__restrict__ rho, double *__restrict__ rhs)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -681,6 +554,7 @@ __global__ void k_ibm_spread(Dom d, IbmDev D, int ne, int comp, const double *__
     const bool direct = !(axis == IBM_AXIS_ODD && i == 0);   // the axis face takes nothing
     double r = 0.0;
     bool touched = false;
+    const int ne = *D.ne;
     for (int e = 0; e < ne; e++) {
         const IbmEntryDev &p = D.ent[e];
         if (!(i >= p.box[0] && i < p.box[1] && j >= p.box[2] && j < p.box[3])) continue;
@@ -749,9 +623,10 @@ __global__ void k_vel_explicit(Dom d, int comp, int i0, int i1, int j0, int j1, 
 // VOF_DIFFUSE_compute_C_S cell loop (VOF_DIFFUSE.c:714-770), planar: every cell
 // of the ghosted plane starts at 0 and takes the maximum over the particles
 __global__ void k_compute_C_S(Dom d, const double *__restrict__ xc, const double *__restrict__ yc,
-                              const double *__restrict__ geo, int ngeo, double shift, double denom, double extra,
-                              double *__restrict__ CS)
+                              const double *__restrict__ geo, const int *ngeo_p, double shift, double denom,
+                              double extra, double *__restrict__ CS)
 {
+    const int ngeo = *ngeo_p;
     const int i = -NG + (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int j = -NG + (int)blockIdx.y;
     if (i >= d.NX + NG || j >= d.NY + NG) return;
@@ -838,7 +713,9 @@ __device__ __forceinline__ bool owns_support(const double *plist, int np, double
 // to rounding.
 __global__ void __launch_bounds__(256) k_ibm_particle_sums(Dom d, IbmSumArgs A)
 {
+    if ((int)blockIdx.x >= *A.ne) return;   // launched for the capacity; the block's exit is uniform
     const IbmEntryDev &E = A.ent[blockIdx.x];
+    const int np = *A.np;
     const double X0 = E.X[0], X1 = E.X[1], R = E.R;
     const int P = d.P;
     double acc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -881,7 +758,7 @@ __global__ void __launch_bounds__(256) k_ibm_particle_sums(Dom d, IbmSumArgs A)
             const double r0 = A.xc[i] - X0, r1 = A.yc[j] - X1, r2 = 0.0;
             const double dist2 = r0 * r0 + r1 * r1 + r2 * r2;
             if (dist2 > sr2) continue;
-            if (!owns_support(A.plist, A.np, E.id, A.xc[i], A.yc[j], A.support_width)) continue;
+            if (!owns_support(A.plist, np, E.id, A.xc[i], A.yc[j], A.support_width)) continue;
             const double i2dx = 1.0 / (A.xc[i + 1] - A.xc[i - 1]), i2dy = 1.0 / (A.yc[j + 1] - A.yc[j - 1]);
             const double gl[3] = {(AT_(A.CL, i + 1, j) - AT_(A.CL, i - 1, j)) * i2dx,
                                   (AT_(A.CL, i, j + 1) - AT_(A.CL, i, j - 1)) * i2dy, 0.0};
@@ -942,23 +819,34 @@ __global__ void __launch_bounds__(256) k_ibm_particle_sums(Dom d, IbmSumArgs A)
     }
 }
 
-// Interpolate_paint_rigid_body_velocity_twod (Interpolate.c:734-800) of one
-// entry: vel = vf (U + Omega_z x r) + (1 - vf) vel on the face cells it covers
-__global__ void k_ibm_paint(Dom d, IbmEntryDev e, int comp, const double *__restrict__ xu,
-                            const double *__restrict__ xc, const double *__restrict__ yv,
-                            const double *__restrict__ yc, double *__restrict__ vel)
+// Interpolate_paint_rigid_body_velocity_twod (Interpolate.c:734-800) of every
+// mobile entry in list order: vel = vf (U + Omega_z x r) + (1 - vf) vel on the
+// face cells of its box
+__global__ void k_ps_paint(Dom d, const PSet *ps, int comp, const double *__restrict__ xu,
+                           const double *__restrict__ xc, const double *__restrict__ yv,
+                           const double *__restrict__ yc, double *__restrict__ vel)
 {
-    const int *b = e.mbox[comp];
-    const int i = b[0] + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    const int j = b[2] + (int)(blockIdx.y * blockDim.y + threadIdx.y);
-    if (i >= b[1] || j >= b[3]) return;
-    const double X0 = e.X[0], X1 = e.X[1];
-    const double vf = face_solid_fraction(comp, i, j, X0, X1, e.R, xu, xc, yv, yc);
-    if (vf <= 0.0) return;
+    const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = (int)(blockIdx.y * blockDim.y + threadIdx.y);
+    if (i >= d.NX || j >= d.NY) return;
     const int P = d.P;
-    const double om = e.Omega[2];
-    const double u_rigid = comp == 0 ? e.U[0] - om * (yc[j] - X1) : e.U[1] + om * (xc[i] - X0);
-    AT_(vel, i, j) = vf * u_rigid + (1.0 - vf) * AT_(vel, i, j);
+    const PSet &S = *ps;
+    for (int q = 0; q < S.ne; q++) {
+        const PEnt &e = S.ent[q];
+        if (!e.mobile) continue;
+        const int *b = e.mbox[comp];
+        if (i < b[0] || i >= b[1] || j < b[2] || j >= b[3]) continue;
+        const double X0 = e.X[0], X1 = e.X[1];
+        const double vf = face_solid_fraction(comp, i, j, X0, X1, e.R, xu, xc, yv, yc);
+        if (vf <= 0.0) continue;
+        const double om = e.Omega[2];
+        const double u_rigid = comp == 0 ? e.U[0] - om * (yc[j] - X1) : e.U[1] + om * (xc[i] - X0);
+        AT_(vel, i, j) = vf * u_rigid + (1.0 - vf) * AT_(vel, i, j);
+    }
 }
+
+// ---------------------------------------------------------------------------
+// device
+// ---------------------------------------------------------------------------
 
 }  // namespace pvof

@@ -186,7 +186,6 @@ struct Ctx {
     struct SpecScal *spec_s; // its grid barrier state
     double spec_fscale;      // dy^2 / N
     int spec_blocks;         // blocks of its cooperative launch
-    int spec_rounds;         // its cyclic-reduction rounds
     double sol_ms[3];
     long long sol_launches[3], sol_iters[3], sol_cell_iters[3];
     int use_graphs;          // replay each substep's launches from a captured CUDA graph

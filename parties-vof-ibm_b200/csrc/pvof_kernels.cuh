@@ -54,7 +54,6 @@ struct SpecScal {
 };
 
 constexpr int SPEC_PT = 1024;        // threads per block of the cooperative solve
-constexpr int SPEC_MAXROUNDS = 10;   // cyclic-reduction rounds for up to 1024 rows
 
 struct SpecArgs {
     Dom d;
@@ -63,9 +62,8 @@ struct SpecArgs {
     const double *rhs, *rho, *MJ;
     double *res, *z, *Ad, *hat;
     const double2 *tw;        // exp(-2 pi i k / N), k < N / 2
-    const double *pcr;        // cyclic-reduction multipliers per round, then 1 / b ([2 rounds + 1][N][M])
+    const double *tri;        // the tridiagonal phase's coefficients, one set per wave number (spec_tables)
     int N, logN, M;           // x cells (a power of two), log2 N, y cells
-    int rounds;               // cyclic-reduction rounds, ceil(log2 M)
     double fscale;            // dy^2 / N
     double tol;
     int maxit;
@@ -75,7 +73,7 @@ struct SpecArgs {
 };
 
 bool spec_supported(const Dom &d, const char **why);
-int spec_tables(int N, int M, double idx2, double idy2, std::vector<double> &tw, std::vector<double> &pcr);
+int spec_tables(int N, int M, double idx2, double idy2, std::vector<double> &tw, std::vector<double> &tri);
 int spec_pcg_blocks(int device, int N, int M);
 cudaError_t spec_launch_pcg(const SpecArgs &A, int blocks, double *d0, double *d1, cudaStream_t st);
 const void *spec_pcg_kernel();   // k_spec_pcg, for marking graph nodes cooperative
@@ -159,35 +157,6 @@ cudaError_t cgs_velocity_launch(const VelPair &V, int ncomp, const StripPlan &pl
 
 // one entry of a particle list after the update of a substep (an owned
 // particle or a periodic copy)
-struct IbmEntry {
-    int mobile, id, copy;
-    double X[3], U[3], Omega[3], R, rho_s;
-    double M, I_p, Vol_L;     // Particle_calc_derived_data
-    int N_L;                  // markers of the whole circle
-    int moff, mcount;         // this entry's markers near the domain
-    int box[4];               // cells [i0, i1) x [j0, j1) its marker supports can reach
-    // rigid-body state (the Particle fields of Include/DataTypes.h:1327-1527
-    // that the motion of a cylinder reads)
-    double X_old[3], U_old[3], Omega_old[3];
-    double Int_U[3], Int_Omega[3], Int_U_old[3], Int_Omega_old[3];
-    double F[3], T[3], F_CCF[3], T_CCF[3];
-};
-
-struct IbmMarkers {
-    std::vector<double> x, y, vol;
-    std::vector<int> flag;
-};
-
-// grid data of the host-side particle bookkeeping; xu, yv offset so that
-// index 0 is the first G-range node, valid on [-NG, N + NG)
-struct IbmGrid {
-    int NX, NY;
-    int periodic[2];
-    int axisym;               // AXISYM_RZ: spheres on the axis, ring markers
-    const double *xu, *yv, *xc, *yc;
-    double h, dy_min, slab, twod_slab, Lx, Ly;
-};
-
 struct IbmEntryDev {
     double X[3], U[3], Omega[3], Zs;
     double R, id;
@@ -200,10 +169,11 @@ struct IbmEntryDev {
 // Int_Omega[2], and with ccf the capillary contact force F_CCF[0..1], T_CCF[2]
 struct IbmSumArgs {
     const IbmEntryDev *ent;
+    const int *ne;                       // entries (device count; the launch covers the capacity)
     const double *U, *V, *CL, *CS;
     const double *xu, *xc, *yv, *yc;     // offset by NG
     const double *plist;                 // x, y, R, ID of the list entries
-    int np;
+    const int *np;                       // their count (device)
     double h, slab, sigma, ct, st, support_width;
     int nk, ccf;
     int axisym;                          // ring measures, no in-plane spin
@@ -217,6 +187,7 @@ constexpr int IBM_AXIS_NONE = 0, IBM_AXIS_ODD = 1, IBM_AXIS_EVEN = 2;
 
 struct IbmDev {
     const IbmEntryDev *ent;
+    const int *ne;                 // entries (device count; the launches cover the capacity)
     const double *XL, *YL, *vol;
     const int *flag;
     int *sup_i, *sup_j;            // lower corner of each marker's spreading support
@@ -228,23 +199,7 @@ struct IbmDev {
     double theta_span;
 };
 
-void ibm_build(const std::vector<IbmEntry> &mobile_local, const std::vector<IbmEntry> &fixed_local, const IbmGrid &g,
-               double Cn, std::vector<IbmEntry> &entries, IbmMarkers &m);
-void ibm_solid_geometry(const std::vector<IbmEntry> &mobile_local, const std::vector<IbmEntry> &fixed_local,
-                        const IbmGrid &g, std::vector<double> &geo);
 void ibm_solid_constants(double cn, double &shift, double &denom, double &extra);
-void ibm_derive(IbmEntry &e, const IbmGrid &g);
-void ibm_momentum_boxes(const IbmEntry &e, const IbmGrid &g, const double *xc, const double *yc, int box[2][4]);
-// Lagrangian_collect_forces (LAG_COLLECT_HYDRO) after Particle_list_foreign_create:
-// the entries of a list whose centre lies in the domain, each with the
-// hydrodynamic sums of its periodic copies added
-std::vector<IbmEntry> ibm_collect(const std::vector<IbmEntry> &both, const IbmGrid &g);
-// Lagrangian_evaluate_fluid_forces and the substepped Lagrangian_integrate_particle_motion
-// (Lagrangian/Lagrangian.c:283-1640) for cylinders out of contact range; returns
-// false (with a message) when two particles or a particle and a wall come within
-// the lubrication range, where the collision models would act
-bool ibm_advance(std::vector<IbmEntry> &mobile, std::vector<IbmEntry> &fixed, const IbmGrid &g, double Cn,
-                 int stage, double dt, const double grav[3], std::string &err);
 
 // contact-line projection (pvof_mcl.cu): the G-range scalars of one pass and
 // the case constants; CL and field are the pass's snapshots
@@ -260,26 +215,24 @@ struct MclView {
 };
 
 __global__ void k_mcl_normals(Dom d, const double *xc, const double *yc, const double *CS, const double *plist,
-                              int np, double support_width, double *nxo, double *nyo);
+                              const int *np, double support_width, double *nxo, double *nyo);
 __global__ void k_mcl_apply(Dom d, MclView v, const double *nxa, const double *nya, double *CLout);
 __global__ void k_mcl_axis_normals(Dom d, double *nx, double *ny);
 __global__ void k_mcl_extend_psi(Dom d, MclView v, const double *nxa, const double *nya, double *PSIout);
 
 __global__ void k_ibm_interp(Dom d, const double *a, const double *xs, const double *ys, double h, const double *XL,
-                             const double *YL, int nm, int axis, double *out);
+                             const double *YL, const int *nm, int axis, double *out);
 constexpr int IBM_FORCE_THREADS = 256;
 __global__ void k_ibm_marker_force(IbmDev D, int comp, double xs0, double ys0, double idt2beta, int reset);
-__global__ void k_ibm_spread(Dom d, IbmDev D, int ne, int comp, const double *xs, const double *ys, const double *rho,
+__global__ void k_ibm_spread(Dom d, IbmDev D, int comp, const double *xs, const double *ys, const double *rho,
                              double *rhs);
 __global__ void k_ibm_correct(Dom d, int comp, double dtbeta, const double *rhs, const double *rho, double *vel);
 __global__ void k_ibm_ng_update(Dom d, double *a, const double *b, int reset);
 __global__ void k_vel_explicit(Dom d, int comp, int i0, int i1, int j0, int j1, double dtimeb, const double *rhs,
                                const double *rho, double *vel);
 __global__ void k_ibm_particle_sums(Dom d, IbmSumArgs A);
-__global__ void k_ibm_paint(Dom d, IbmEntryDev e, int comp, const double *xu, const double *xc, const double *yv,
-                            const double *yc, double *vel);
-__global__ void k_compute_C_S(Dom d, const double *xc, const double *yc, const double *geo, int ngeo, double shift,
-                              double denom, double extra, double *CS);
+__global__ void k_compute_C_S(Dom d, const double *xc, const double *yc, const double *geo, const int *ngeo,
+                              double shift, double denom, double extra, double *CS);
 
 // learned warm start (pvof_cnn.cu)
 __global__ void k_cnn_sumsq(Dom d, const double *a, const double *b, double *partials);

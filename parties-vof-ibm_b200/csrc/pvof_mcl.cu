@@ -370,13 +370,14 @@ __host__ __device__ void mcl_extend_cell(const Dom &d, const MclView &v, const d
 }
 
 __global__ void k_mcl_normals(Dom d, const double *__restrict__ xc, const double *__restrict__ yc,
-                              const double *__restrict__ CS, const double *__restrict__ plist, int np,
-                              double support_width, double *__restrict__ nxo, double *__restrict__ nyo)
+                              const double *__restrict__ CS, const double *__restrict__ plist,
+                              const int *np, double support_width, double *__restrict__ nxo,
+                              double *__restrict__ nyo)
 {
     const int i = -NG + (int)(blockIdx.x * blockDim.x + threadIdx.x);
     const int j = -NG + (int)blockIdx.y;
     if (i >= d.NX + NG) return;
-    mcl_normal_cell(d, xc, yc, CS, plist, np, support_width, nxo, nyo, i, j);
+    mcl_normal_cell(d, xc, yc, CS, plist, *np, support_width, nxo, nyo, i, j);
 }
 
 // VOF_DIFFUSE_compute_solid_normals_MCL and mcl_apply_normal_parity on the

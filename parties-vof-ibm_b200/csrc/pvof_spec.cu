@@ -14,19 +14,25 @@
 //   1. every row j: forward complex FFT of the residual row (radix 2 in shared
 //      memory, twiddles from a table), stored in FFTW's half-complex order
 //      (Re X_0 .. Re X_{N/2}, Im X_{N/2-1} .. Im X_1) times dy^2 / N;
-//   2. every half-complex index m: parallel cyclic reduction (one thread per
-//      row, log2 M elimination rounds in shared memory) of
+//   2. every half-complex index m: the tridiagonal system
 //        -z_{j-1} + (b_j + dy^2 lambda_x(m)) z_j - z_{j+1} = rhs_j,
-//      b_j = 2 inside, 1 at the two walls.  The matrices do not change, so
-//      the rounds' multipliers and the final reciprocal diagonals are
-//      computed once per context on the host (spec_tables, one set per wave
-//      number: the half-complex indices m and N - m share it) and a round is
-//      two multiply-adds.  The mean mode's system is singular (the constant,
-//      the operator's null space): its first row is pinned, the right-hand
-//      side and the result are made mean-free, and the right-hand side's mean
-//      is added back, i.e. the constant mode is given eigenvalue 1 (the
-//      inverse of L + P, P the projector on constants), which keeps the
-//      scaled preconditioner positive definite;
+//      b_j = 2 inside, 1 at the two walls, by a partition method: one warp
+//      per system, the column staged in shared memory, each lane owning a
+//      chunk of consecutive rows.  A lane eliminates its chunk's sub- and
+//      super-diagonals down to two equations in the chunk's first and last
+//      unknowns; the 2P equations of the P chunks form a tridiagonal system
+//      that one lane solves by the Thomas algorithm; each lane then fills in
+//      its chunk's interior by back substitution.  The matrices do not change,
+//      so every pivot and coupling coefficient, those of the reduced system
+//      included, is computed once per context on the host (spec_tables, one
+//      set per wave number: the half-complex indices m and N - m share it);
+//      per iteration a row costs an add and a multiply or two.  The mean
+//      mode's system is singular (the constant, the operator's null space):
+//      its first row is pinned, the right-hand side and the result are made
+//      mean-free, and the right-hand side's mean is added back, i.e. the
+//      constant mode is given eigenvalue 1 (the inverse of L + P, P the
+//      projector on constants), which keeps the scaled preconditioner
+//      positive definite;
 //   3. every row: inverse transform.
 //
 // Without the scaling the preconditioned operator's condition number is at
@@ -39,8 +45,8 @@
 // result moves within that tolerance of the reference's.
 //
 // The whole solve is ONE cooperative launch: blocks of SPEC_PT threads, eight
-// 128-thread row groups in the row phases, SPEC_PT / Mp reduction systems per
-// block (Mp = M rounded up to 32), four grid barriers per iteration (after the
+// 128-thread row groups in the row phases, eight warps of one tridiagonal
+// system each per block in the solve phase, four grid barriers per iteration (after the
 // matrix-vector product, the update with its forward transforms, the
 // tridiagonal solves, the inverse transforms).  Every block adds the
 // per-block sums in block order, so all of them take the same decisions.  The
@@ -57,9 +63,32 @@ namespace pvof {
 
 namespace {
 
-constexpr int ROW_THREADS = 128;
-constexpr int ROWG = SPEC_PT / ROW_THREADS;
+constexpr int ROW_THREADS = 256;
+constexpr int ROWG = SPEC_PT / ROW_THREADS;   // row groups per block, one pair of rows each
 constexpr unsigned long long SPEC_SPIN_LIMIT = 1ull << 26;
+constexpr int SPEC_SYS = 8;          // tridiagonal systems per block and pass, one warp each
+constexpr int SPEC_CHUNKS = 32;      // chunks of a system, one per lane
+
+// The rows of a column of M (>= 2) unknowns split into P = min(32, M / 2)
+// chunks of base or base + 1 rows (at least two each): chunk l starts at
+// l base + min(l, rem) and has base + (l < rem) rows; K = the longest chunk.
+struct Chunks {
+    int P, base, rem, K;
+};
+
+__host__ __device__ inline Chunks spec_chunks(int M)
+{
+    Chunks c;
+    c.P = M / 2 < SPEC_CHUNKS ? M / 2 : SPEC_CHUNKS;
+    c.base = M / c.P;
+    c.rem = M - c.base * c.P;
+    c.K = c.base + (c.rem > 0 ? 1 : 0);
+    return c;
+}
+
+// shared-memory column index of row j: one pad double per 32 rows, so the
+// lanes' chunks (about 32 rows apart) fall in different banks
+__device__ __forceinline__ int cidx(int j) { return j + (j >> 5); }
 
 // sum over the block, in a fixed order; the total is valid in thread 0
 __device__ double block_sum(double v, double *sh)
@@ -192,95 +221,177 @@ __device__ void fft_group(double2 *a, int N, int logN, const double2 *__restrict
     }
 }
 
-// forward transform of the group's row (already in a) into hat row j
-__device__ void group_forward(const SpecArgs &A, double2 *a, int j, bool active, int lt)
+// Two real rows in one complex transform: the group's pair of rows ja, jb
+// sits in a as a + i b.  Forward: Z = FFT(a + i b) gives both spectra,
+// X_a[k] = (Z[k] + conj Z[N-k]) / 2, X_b[k] = (Z[k] - conj Z[N-k]) / 2i,
+// stored in half-complex order into hat rows ja and jb (each if active).
+// Every group of the block calls it (the transform synchronises the block).
+__device__ void pair_forward(const SpecArgs &A, double2 *a, int ja, bool acta, bool actb, int lt)
 {
-    const int P = A.d.P, N = A.N;
+    const int P = A.d.P, N = A.N, jb = ja + 1;
+    const double sc = 0.5 * A.fscale;
     __syncthreads();
     fft_group(a, N, A.logN, A.tw, -1.0, lt);
-    if (active) {
-        for (int k = lt; k <= N / 2; k += ROW_THREADS) AT_(A.hat, k, j) = a[k].x * A.fscale;
-        for (int k = 1 + lt; k < N / 2; k += ROW_THREADS) AT_(A.hat, N - k, j) = a[k].y * A.fscale;
-    }
-    __syncthreads();   // the next row step overwrites a
+    if (acta)
+        for (int k = lt; k <= N / 2; k += ROW_THREADS) {
+            const double2 zk = a[k], zn = a[(N - k) & (N - 1)];
+            AT_(A.hat, k, ja) = (zk.x + zn.x) * sc;
+            if (actb) AT_(A.hat, k, jb) = (zk.y + zn.y) * sc;
+            if (k > 0 && k < N / 2) {
+                AT_(A.hat, N - k, ja) = (zk.y - zn.y) * sc;
+                if (actb) AT_(A.hat, N - k, jb) = (zn.x - zk.x) * sc;
+            }
+        }
+    __syncthreads();   // the next pair overwrites a
+}
+
+// the spectrum X[k] (k = 0 .. N-1) of a real row from its half-complex row j
+__device__ __forceinline__ double2 half_complex(const SpecArgs &A, int k, int j)
+{
+    const int P = A.d.P, N = A.N;
+    if (k == 0 || 2 * k == N) return make_double2(AT_(A.hat, k, j), 0.0);
+    if (k < N / 2) return make_double2(AT_(A.hat, k, j), AT_(A.hat, N - k, j));
+    return make_double2(AT_(A.hat, N - k, j), -AT_(A.hat, k, j));
 }
 
 __device__ __forceinline__ int src_x(const SpecArgs &A, int i) { return A.mp.x.src[i + NG]; }
 __device__ __forceinline__ int src_y(const SpecArgs &A, int j) { return A.mp.y.src[j + NG]; }
 
-// mean over the block's system 0 (threads sys == 0), broadcast to the block
-__device__ double system0_mean(double v, bool sys0, int M, double *sh)
-{
-    __shared__ double mean;
-    const double t = block_sum(sys0 ? v : 0.0, sh);
-    if (threadIdx.x == 0) mean = t / (double)M;
-    __syncthreads();
-    const double r = mean;
-    __syncthreads();
-    return r;
-}
-
 // half-complex index of the q-th system: 0, N/2, then 1, N-1, 2, N-2, ...,
-// so the two indices of one wave number (same matrix, same table rows) are
-// solved side by side
+// so the two indices of one wave number (same matrix, same table entries)
+// sit in neighbouring lanes
 __device__ __forceinline__ int system_index(int q, int N)
 {
     if (q < 2) return q == 0 ? 0 : N / 2;
     return (q & 1) ? N - (q >> 1) : (q >> 1);
 }
 
-// the tridiagonal solves of every half-complex index, hat in place
-__device__ void tridiag_phase(const SpecArgs &A, double *smem, double *sh)
+__device__ __forceinline__ double warp_total(double v)
 {
-    const int P = A.d.P, N = A.N, M = A.M, Mp = (M + 31) / 32 * 32, S = SPEC_PT / Mp;
-    const int sys = threadIdx.x / Mp, j = threadIdx.x - sys * Mp;
-    const size_t NM = (size_t)(N / 2 + 1) * M;   // table rows per round: one per wave number
-    double *sd = smem + (size_t)sys * Mp;
-    for (int m0 = blockIdx.x * S; m0 < N; m0 += gridDim.x * S) {
-        const int q = m0 + sys;
-        const int m = q < N ? system_index(q, N) : 0;
-        const int wave = m <= N / 2 ? m : N - m;
-        const bool row = sys < S && q < N && j < M;
-        double r = row ? AT_(A.hat, m, j) : 0.0;
-        double rmean = 0.0;
-        if (m0 == 0) {   // this block holds the mean mode as its system 0
-            rmean = system0_mean(r, sys == 0, M, sh);
-            if (q == 0) r = j == 0 ? 0.0 : r - rmean;   // mean-free, first row pinned
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// The tridiagonal solves of every half-complex index, hat in place.  A
+// block takes SPEC_SYS systems at a time: their columns are loaded into
+// shared memory (coalesced: the systems are enumerated so that a group holds
+// two runs of neighbouring indices), warp s solves system s, and the columns
+// go back.  Per warp, with the table T of the system's wave number
+// (spec_tables: for chunk row i >= 1 the elimination pivot r_i in
+// T[i][lane] and the first-unknown coupling A_i in T[K + i][lane]; the
+// chunk's c_0 in T[0][lane], a_0 in T[K][lane]; the reduced system's Thomas
+// pivots in T[2K .. 2K + 3][lane]):
+//   lane l, rows s_l .. s_l + L - 1 of its chunk:
+//     down   D_1 = r_1 d_1, D_i = r_i (d_i + D_{i-1}): row i now reads
+//            x_i + A_i x_first + C_i x_{i+1} = D_i (C_i = -r_i inside)
+//     up     E_{L-1} = 0, E_i = D_i + r_i E_{i+1} down to E_1
+//     the chunk's two equations: row 0 with x_1 eliminated (right-hand side
+//     d_0 - c_0 E_1) and row L - 1 as it stands after the down sweep
+//   lane 0: the Thomas algorithm over the 2P equations, pivots from the table
+//   lane l: x_first, x_last from it, then x_i = D_i - A_i x_first + r_i x_{i+1}
+//           for i = L - 2 .. 1
+// The mean mode (m = 0) is made mean-free with its first row pinned on the
+// way in, and given the right-hand side's mean back on the way out.
+__device__ void tridiag_phase(const SpecArgs &A, double *area)
+{
+    const int N = A.N, M = A.M, P = A.d.P;
+    const Chunks ch = spec_chunks(M);
+    const int K = ch.K, TW = (2 * K + 4) * 32;
+    const int CP = M + (M >> 5) + 1;
+    double *cols = area;                      // SPEC_SYS columns of CP doubles
+    double *red = area + SPEC_SYS * CP;       // per warp: rhs, lower coupling, pivot, c' of the 2P equations
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int q0 = blockIdx.x * SPEC_SYS; q0 < N; q0 += gridDim.x * SPEC_SYS) {
+        __syncthreads();   // the previous group's columns are stored
+        for (int e = threadIdx.x; e < SPEC_SYS * M; e += blockDim.x) {
+            const int j = e / SPEC_SYS, s = e - j * SPEC_SYS;
+            if (q0 + s < N) cols[s * CP + cidx(j)] = AT_(A.hat, system_index(q0 + s, N), j);
         }
-        // this thread's multipliers, all loads in flight at once: round st
-        // k1 at [2 st NM], k2 at [(2 st + 1) NM], then 1 / b at [2 rounds NM]
-        const double *k = A.pcr + (size_t)wave * M + j;
-        double kr[2 * SPEC_MAXROUNDS + 1];
-#pragma unroll
-        for (int q = 0; q < 2 * SPEC_MAXROUNDS + 1; q++) kr[q] = (row && q <= 2 * A.rounds) ? k[(size_t)q * NM] : 0.0;
-#pragma unroll
-        for (int st = 0; st < SPEC_MAXROUNDS; st++) {
-            if (st >= A.rounds) break;
-            const int s = 1 << st;
-            if (row) sd[j] = r;
-            __syncthreads();
-            if (row) {
-                double rn = r;
-                if (j - s >= 0) rn -= sd[j - s] * kr[2 * st];
-                if (j + s < M) rn -= sd[j + s] * kr[2 * st + 1];
-                r = rn;
+        __syncthreads();
+        const int q = q0 + warp;
+        if (warp < SPEC_SYS && q < N) {
+            double *col = cols + warp * CP;
+            double *rw = red + warp * 256;
+            const int m = system_index(q, N);
+            const int wave = m <= N / 2 ? m : N - m;
+            const double *__restrict__ T = A.tri + (size_t)wave * TW;
+            double rmean = 0.0;
+            if (m == 0) {   // mean-free, first row pinned
+                double sum = 0.0;
+                for (int j = lane; j < M; j += 32) sum += col[cidx(j)];
+                rmean = warp_total(sum) / (double)M;
+                for (int j = lane; j < M; j += 32) col[cidx(j)] = j == 0 ? 0.0 : col[cidx(j)] - rmean;
+                __syncwarp();
             }
-            __syncthreads();
+            const int len = lane < ch.P ? ch.base + (lane < ch.rem ? 1 : 0) : 0;
+            const int st = lane * ch.base + (lane < ch.rem ? lane : ch.rem);
+            if (len > 0) {
+                double Dp = 0.0;
+#pragma unroll 4
+                for (int i = 1; i < len; i++) {
+                    const int c = cidx(st + i);
+                    const double r = T[i * 32 + lane], dv = col[c];
+                    Dp = i == 1 ? r * dv : r * (dv + Dp);
+                    col[c] = Dp;
+                }
+                double E = 0.0;
+#pragma unroll 4
+                for (int i = len - 2; i >= 1; i--) E = col[cidx(st + i)] + T[i * 32 + lane] * E;
+                rw[2 * lane] = col[cidx(st)] - T[lane] * E;
+                rw[2 * lane + 1] = Dp;
+                rw[64 + 2 * lane] = T[K * 32 + lane];
+                rw[64 + 2 * lane + 1] = T[(K + len - 1) * 32 + lane];
+                rw[128 + 2 * lane] = T[(2 * K) * 32 + lane];
+                rw[192 + 2 * lane] = T[(2 * K + 1) * 32 + lane];
+                rw[128 + 2 * lane + 1] = T[(2 * K + 2) * 32 + lane];
+                rw[192 + 2 * lane + 1] = T[(2 * K + 3) * 32 + lane];
+            }
+            __syncwarp();
+            if (lane == 0) {   // the reduced system: 2P equations, Thomas
+                const int n2 = 2 * ch.P;
+                double prev = 0.0;
+#pragma unroll 8
+                for (int k = 0; k < n2; k++) {
+                    prev = (rw[k] - rw[64 + k] * prev) * rw[128 + k];
+                    rw[k] = prev;
+                }
+                double nxt = 0.0;
+#pragma unroll 8
+                for (int k = n2 - 1; k >= 0; k--) {
+                    nxt = rw[k] - rw[192 + k] * nxt;
+                    rw[k] = nxt;
+                }
+            }
+            __syncwarp();
+            if (len > 0) {
+                const double x0 = rw[2 * lane], x1 = rw[2 * lane + 1];
+                col[cidx(st)] = x0;
+                col[cidx(st + len - 1)] = x1;
+                double xn = x1;
+#pragma unroll 4
+                for (int i = len - 2; i >= 1; i--) {
+                    const int c = cidx(st + i);
+                    xn = col[c] - T[(K + i) * 32 + lane] * x0 + T[i * 32 + lane] * xn;
+                    col[c] = xn;
+                }
+            }
+            if (m == 0) {
+                // the constant mode, the operator's null space, gets eigenvalue
+                // 1 (in units of 1 / dy^2) instead of 0: the mean-free solution
+                // plus the right-hand side's mean, so the scaled
+                // preconditioner stays positive definite
+                __syncwarp();
+                double sum = 0.0;
+                for (int j = lane; j < M; j += 32) sum += col[cidx(j)];
+                const double mean = warp_total(sum) / (double)M;
+                for (int j = lane; j < M; j += 32) col[cidx(j)] = col[cidx(j)] - mean + rmean;
+            }
         }
-        double ib = 0.0;
-#pragma unroll
-        for (int q = 0; q < 2 * SPEC_MAXROUNDS + 1; q++)
-            if (q == 2 * A.rounds) ib = kr[q];
-        double x = row ? r * ib : 0.0;   // times the final 1 / b
-        if (m0 == 0) {
-            // the constant mode, the operator's null space, gets eigenvalue 1
-            // (in units of 1 / dy^2) instead of 0: the mean-free solution plus
-            // the right-hand side's mean, so the scaled preconditioner stays
-            // positive definite
-            const double mean = system0_mean(x, sys == 0, M, sh);
-            if (q == 0) x = x - mean + rmean;
+        __syncthreads();
+        for (int e = threadIdx.x; e < SPEC_SYS * M; e += blockDim.x) {
+            const int j = e / SPEC_SYS, s = e - j * SPEC_SYS;
+            if (q0 + s < N) AT_(A.hat, system_index(q0 + s, N), j) = cols[s * CP + cidx(j)];
         }
-        if (row) AT_(A.hat, m, j) = x;
     }
 }
 
@@ -294,7 +405,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
     const int P = d.P, NX = d.NX, NY = d.NY, N = A.N, M = A.M;
     const int grp = threadIdx.x / ROW_THREADS, lt = threadIdx.x - grp * ROW_THREADS;
     double2 *tw = reinterpret_cast<double2 *>(smem);
-    double *work = smem + N;   // N / 2 complex twiddles before it
+    double *work = smem + N;   // N / 2 complex twiddles before it; the row groups' rows, or the systems' columns
     double2 *row = reinterpret_cast<double2 *>(work) + (size_t)grp * N;
     double *slotA = A.part, *slotB = A.part + gridDim.x, *slotC = A.part + 2 * gridDim.x;
     SpecScal *S = A.s;
@@ -306,20 +417,23 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
     B.tw = tw;
 
     // r = rhs - A phi, the stopping sum, forward transforms
+    auto residual = [&](int i, int j, double &sum) {
+        const double ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, A.phi, P, NX, NY, a, b); });
+        const double rv = AT_(A.rhs, i, j) - ad;
+        AT_(A.res, i, j) = rv;
+        sum += rv * (rv * AT_(A.MJ, i, j));
+        return rv * sqrt(AT_(A.MJ, i, j));
+    };
     double sJ = 0.0;
-    for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
-        const int j = j0 + grp;
-        const bool active = j < M;
-        if (active) {
+    for (int p0 = blockIdx.x * ROWG; 2 * p0 < M; p0 += gridDim.x * ROWG) {
+        const int ja = 2 * (p0 + grp), jb = ja + 1;
+        const bool acta = ja < M, actb = jb < M;
+        if (acta)
             for (int i = lt; i < N; i += ROW_THREADS) {
-                const double ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, A.phi, P, NX, NY, a, b); });
-                const double rv = AT_(A.rhs, i, j) - ad;
-                AT_(A.res, i, j) = rv;
-                sJ += rv * (rv * AT_(A.MJ, i, j));
-                row[i] = make_double2(rv * sqrt(AT_(A.MJ, i, j)), 0.0);
+                const double va = residual(i, ja, sJ);
+                row[i] = make_double2(va, actb ? residual(i, jb, sJ) : 0.0);
             }
-        }
-        group_forward(B, row, j, active, lt);
+        pair_forward(B, row, ja, acta, actb, lt);
     }
     put_part(sJ, slotA, sh);
     if (!spec_barrier(S, err)) return;
@@ -334,30 +448,32 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
     double *dold = d0, *dnew = d1;
     for (int it = 0;; it++) {
         // z = (-L)^-1 r
-        tridiag_phase(A, work, sh);
+        tridiag_phase(A, work);
         if (!spec_barrier(S, err)) return;
         double g = 0.0;
-        for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
-            const int j = j0 + grp;
-            const bool active = j < M;
-            if (active) {
+        for (int p0 = blockIdx.x * ROWG; 2 * p0 < M; p0 += gridDim.x * ROWG) {
+            const int ja = 2 * (p0 + grp), jb = ja + 1;
+            const bool acta = ja < M, actb = jb < M;
+            if (acta)
                 for (int k = lt; k < N; k += ROW_THREADS) {
-                    double2 v;
-                    if (k == 0 || 2 * k == N) v = make_double2(AT_(A.hat, k, j), 0.0);
-                    else if (k < N / 2) v = make_double2(AT_(A.hat, k, j), AT_(A.hat, N - k, j));
-                    else v = make_double2(AT_(A.hat, N - k, j), -AT_(A.hat, k, j));
-                    row[k] = v;
+                    const double2 xa = half_complex(A, k, ja);
+                    const double2 xb = actb ? half_complex(A, k, jb) : make_double2(0.0, 0.0);
+                    row[k] = make_double2(xa.x - xb.y, xa.y + xb.x);   // X_a + i X_b
                 }
-            }
             __syncthreads();
             fft_group(row, N, A.logN, tw, 1.0, lt);
-            if (active) {
+            if (acta)
                 for (int i = lt; i < N; i += ROW_THREADS) {
-                    const double z = row[i].x * sqrt(AT_(A.MJ, i, j));
-                    AT_(A.z, i, j) = z;
-                    g += AT_(A.res, i, j) * z;
+                    const double2 v = row[i];
+                    const double za = v.x * sqrt(AT_(A.MJ, i, ja));
+                    AT_(A.z, i, ja) = za;
+                    g += AT_(A.res, i, ja) * za;
+                    if (actb) {
+                        const double zb = v.y * sqrt(AT_(A.MJ, i, jb));
+                        AT_(A.z, i, jb) = zb;
+                        g += AT_(A.res, i, jb) * zb;
+                    }
                 }
-            }
             __syncthreads();
         }
         put_part(g, slotB, sh);
@@ -378,35 +494,39 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
             return first ? AT_(A.z, si, sj) : AT_(A.z, si, sj) + beta * AT_(dold, si, sj);
         };
         double sdad = 0.0;
-        for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
-            const int j = j0 + grp;
-            if (j >= M) continue;
-            for (int i = lt; i < N; i += ROW_THREADS) {
-                const double dv = dir(i, j);
-                AT_(dnew, i, j) = dv;
-                const double ad = pressure_op(d, A.rho, i, j, dir);
-                AT_(A.Ad, i, j) = ad;
-                sdad += dv * ad;
+        for (int p0 = blockIdx.x * ROWG; 2 * p0 < M; p0 += gridDim.x * ROWG)
+            for (int h = 0; h < 2; h++) {
+                const int j = 2 * (p0 + grp) + h;
+                if (j >= M) continue;
+                for (int i = lt; i < N; i += ROW_THREADS) {
+                    const double dv = dir(i, j);
+                    AT_(dnew, i, j) = dv;
+                    const double ad = pressure_op(d, A.rho, i, j, dir);
+                    AT_(A.Ad, i, j) = ad;
+                    sdad += dv * ad;
+                }
             }
-        }
         put_part(sdad, slotC, sh);
         if (!spec_barrier(S, err)) return;
         const double alpha = gamma / (slot_total(slotC, sh) + 1e-300);
         // phi += alpha d, r -= alpha Ad, the stopping sum, forward transforms
+        auto update = [&](int i, int j, double &sum) {
+            AT_(A.phi, i, j) += alpha * AT_(dnew, i, j);
+            const double rv = AT_(A.res, i, j) - alpha * AT_(A.Ad, i, j);
+            AT_(A.res, i, j) = rv;
+            sum += rv * (rv * AT_(A.MJ, i, j));
+            return rv * sqrt(AT_(A.MJ, i, j));
+        };
         sJ = 0.0;
-        for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
-            const int j = j0 + grp;
-            const bool active = j < M;
-            if (active) {
+        for (int p0 = blockIdx.x * ROWG; 2 * p0 < M; p0 += gridDim.x * ROWG) {
+            const int ja = 2 * (p0 + grp), jb = ja + 1;
+            const bool acta = ja < M, actb = jb < M;
+            if (acta)
                 for (int i = lt; i < N; i += ROW_THREADS) {
-                    AT_(A.phi, i, j) += alpha * AT_(dnew, i, j);
-                    const double rv = AT_(A.res, i, j) - alpha * AT_(A.Ad, i, j);
-                    AT_(A.res, i, j) = rv;
-                    sJ += rv * (rv * AT_(A.MJ, i, j));
-                    row[i] = make_double2(rv * sqrt(AT_(A.MJ, i, j)), 0.0);
+                    const double va = update(i, ja, sJ);
+                    row[i] = make_double2(va, actb ? update(i, jb, sJ) : 0.0);
                 }
-            }
-            group_forward(B, row, j, active, lt);
+            pair_forward(B, row, ja, acta, actb, lt);
         }
         put_part(sJ, slotA, sh);
         if (!spec_barrier(S, err)) return;
@@ -418,19 +538,21 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
     }
     // remove the mean (psolve_cg.c:255-279)
     double ssum = 0.0;
-    for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
-        const int j = j0 + grp;
-        if (j >= M) continue;
-        for (int i = lt; i < N; i += ROW_THREADS) ssum += AT_(A.phi, i, j);
-    }
+    for (int p0 = blockIdx.x * ROWG; 2 * p0 < M; p0 += gridDim.x * ROWG)
+        for (int h = 0; h < 2; h++) {
+            const int j = 2 * (p0 + grp) + h;
+            if (j >= M) continue;
+            for (int i = lt; i < N; i += ROW_THREADS) ssum += AT_(A.phi, i, j);
+        }
     put_part(ssum, slotB, sh);
     if (!spec_barrier(S, err)) return;
     const double avg = slot_total(slotB, sh) / ((double)N * (double)M);
-    for (int j0 = blockIdx.x * ROWG; j0 < M; j0 += gridDim.x * ROWG) {
-        const int j = j0 + grp;
-        if (j >= M) continue;
-        for (int i = lt; i < N; i += ROW_THREADS) AT_(A.phi, i, j) -= avg;
-    }
+    for (int p0 = blockIdx.x * ROWG; 2 * p0 < M; p0 += gridDim.x * ROWG)
+        for (int h = 0; h < 2; h++) {
+            const int j = 2 * (p0 + grp) + h;
+            if (j >= M) continue;
+            for (int i = lt; i < N; i += ROW_THREADS) AT_(A.phi, i, j) -= avg;
+        }
     if (lead) { A.scal->p_iters = iters; A.scal->p_res = res; }
 }
 
@@ -443,53 +565,75 @@ bool spec_supported(const Dom &d, const char **why)
     if (!d.planar || d.axisym) { *why = "the spectral pressure preconditioner is built for the planar mode only"; return false; }
     if (!d.perx || d.pery) { *why = "the spectral pressure preconditioner needs x periodic and walls in y"; return false; }
     if (N < 2 || (N & (N - 1)) != 0 || N > 1024) { *why = "the spectral pressure preconditioner needs a power-of-two x cell count (2..1024)"; return false; }
-    if (M < 1 || M > 1024) { *why = "the spectral pressure preconditioner needs at most 1024 y cells"; return false; }
+    if (M < 2 || M > 1024) { *why = "the spectral pressure preconditioner needs 2 to 1024 y cells"; return false; }
     return true;
 }
 
-int spec_tables(int N, int M, double idx2, double idy2, std::vector<double> &tw, std::vector<double> &pcr)
+int spec_tables(int N, int M, double idx2, double idy2, std::vector<double> &tw, std::vector<double> &tri)
 {
     tw.assign(N, 0.0);   // N / 2 complex entries exp(-2 pi i k / N)
     for (int k = 0; k < N / 2; k++) {
         tw[2 * k] = std::cos(2.0 * M_PI * k / N);
         tw[2 * k + 1] = -std::sin(2.0 * M_PI * k / N);
     }
-    int nsteps = 0;
-    for (int s = 1; s < M; s <<= 1) nsteps++;
-    const size_t NM = (size_t)(N / 2 + 1) * M;   // one matrix per wave number 0 .. N/2
-    pcr.assign((size_t)(2 * nsteps + 1) * NM, 0.0);
-    std::vector<double> a(M), b(M), c(M), a2(M), b2(M), c2(M);
-    for (int m = 0; m <= N / 2; m++) {   // m: the wave number
-        const double lam = (2.0 - 2.0 * std::cos(2.0 * M_PI * m / N)) * idx2 / idy2;
-        for (int j = 0; j < M; j++) {
-            if (m == 0 && j == 0) { a[j] = 0.0; b[j] = 1.0; c[j] = 0.0; continue; }   // the pinned row
-            a[j] = j > 0 ? -1.0 : 0.0;
-            c[j] = j < M - 1 ? -1.0 : 0.0;
-            b[j] = lam + (j > 0 ? 1.0 : 0.0) + (j < M - 1 ? 1.0 : 0.0);
-        }
-        int st = 0;
-        for (int s = 1; s < M; s <<= 1, st++) {   // the elimination rounds of the device's cyclic reduction
-            for (int j = 0; j < M; j++) {
-                double an = 0.0, cn = 0.0, bn = b[j], k1 = 0.0, k2 = 0.0;
-                if (j - s >= 0) { k1 = a[j] / b[j - s]; bn -= c[j - s] * k1; an = -a[j - s] * k1; }
-                if (j + s < M) { k2 = c[j] / b[j + s]; bn -= a[j + s] * k2; cn = -c[j + s] * k2; }
-                pcr[(size_t)(2 * st) * NM + (size_t)m * M + j] = k1;
-                pcr[(size_t)(2 * st + 1) * NM + (size_t)m * M + j] = k2;
-                a2[j] = an; b2[j] = bn; c2[j] = cn;
+    // per wave number, (2K + 4) rows of 32 (one entry per chunk): the
+    // coefficients of tridiag_phase for a_j z_{j-1} + b_j z_j + c_j z_{j+1} = r_j
+    // (a = c = -1 inside)
+    const Chunks ch = spec_chunks(M);
+    const int K = ch.K, TW = (2 * K + 4) * 32, NW = N / 2 + 1;
+    tri.assign((size_t)NW * TW, 0.0);
+    std::vector<double> R(K), Ac(K), Cc(K), lo(2 * ch.P), di(2 * ch.P), up(2 * ch.P);
+    for (int w = 0; w < NW; w++) {
+        const double lam = (2.0 - 2.0 * std::cos(2.0 * M_PI * w / N)) * idx2 / idy2;
+        auto coef = [&](int j, double &a, double &b, double &c) {
+            if (w == 0 && j == 0) { a = 0.0; b = 1.0; c = 0.0; return; }   // the pinned row
+            a = j > 0 ? -1.0 : 0.0;
+            c = j < M - 1 ? -1.0 : 0.0;
+            b = lam + (j > 0 ? 1.0 : 0.0) + (j < M - 1 ? 1.0 : 0.0);
+        };
+        double *T = tri.data() + (size_t)w * TW;
+        for (int l = 0; l < ch.P; l++) {
+            const int L = ch.base + (l < ch.rem ? 1 : 0), s = l * ch.base + (l < ch.rem ? l : ch.rem);
+            // down: row i (>= 1) becomes x_i + A_i x_0 + C_i x_{i+1} = D_i
+            for (int i = 1; i < L; i++) {
+                double a, b, c;
+                coef(s + i, a, b, c);
+                R[i] = i == 1 ? 1.0 / b : 1.0 / (b - a * Cc[i - 1]);
+                Ac[i] = i == 1 ? a * R[i] : -a * R[i] * Ac[i - 1];
+                Cc[i] = c * R[i];
+                T[i * 32 + l] = R[i];
+                T[(K + i) * 32 + l] = Ac[i];
             }
-            a.swap(a2); b.swap(b2); c.swap(c2);
+            // up: x_1 = E_1 - F_1 x_0 - G_1 x_{L-1}
+            double F = 0.0, G = -1.0;
+            for (int i = L - 2; i >= 1; i--) {
+                F = Ac[i] - Cc[i] * F;
+                G = -Cc[i] * G;
+            }
+            double a0, b0, c0;
+            coef(s, a0, b0, c0);
+            T[l] = c0;
+            T[K * 32 + l] = a0;
+            lo[2 * l] = a0;  di[2 * l] = b0 - c0 * F;  up[2 * l] = -c0 * G;
+            lo[2 * l + 1] = Ac[L - 1];  di[2 * l + 1] = 1.0;  up[2 * l + 1] = Cc[L - 1];
         }
-        for (int j = 0; j < M; j++) pcr[(size_t)(2 * nsteps) * NM + (size_t)m * M + j] = 1.0 / b[j];
+        // the reduced system's Thomas pivots
+        double cprev = 0.0;
+        for (int k = 0; k < 2 * ch.P; k++) {
+            const double inv = 1.0 / (di[k] - lo[k] * cprev);
+            cprev = up[k] * inv;
+            T[(2 * K + 2 * (k & 1)) * 32 + k / 2] = inv;
+            T[(2 * K + 2 * (k & 1) + 1) * 32 + k / 2] = cprev;
+        }
     }
-    return nsteps;
+    return M;
 }
 
 size_t spec_pcg_smem(int N, int M)
 {
     const size_t rows = (size_t)ROWG * N * sizeof(double2);
-    const int Mp = (M + 31) / 32 * 32;
-    const size_t tri = (size_t)(SPEC_PT / Mp) * Mp * sizeof(double);
-    return (size_t)N * sizeof(double) + (rows > tri ? rows : tri);   // twiddles first
+    const size_t cols = (size_t)SPEC_SYS * ((size_t)M + (M >> 5) + 1 + 256) * sizeof(double);
+    return (size_t)N * sizeof(double) + (rows > cols ? rows : cols);   // twiddles, then the work area
 }
 
 // blocks for k_spec_pcg: enough for one pass over the rows and the systems,
@@ -504,10 +648,7 @@ int spec_pcg_blocks(int device, int N, int M)
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spec_pcg, SPEC_PT, smem) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) != cudaSuccess || !coop) return 0;
-    const int Mp = (M + 31) / 32 * 32, S = SPEC_PT / Mp;
-    int want = (M + ROWG - 1) / ROWG;
-    const int sys = (N + S - 1) / S;
-    if (sys > want) want = sys;
+    int want = (M + 2 * ROWG - 1) / (2 * ROWG);   // the tridiagonal phase loops over its systems: any block count works
     const int most = per_sm * sms;
     return most < 1 ? 0 : (want < most ? want : most);
 }
