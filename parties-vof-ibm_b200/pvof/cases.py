@@ -225,3 +225,65 @@ def sinking_cylinders(NXM=1024, NYM=1024, L=1.0, Cn=0.005, rho_ratio=1e-3, R=0.1
     params.contact_angle_deg = theta
     parts = [(1, L * x, y0, R, 0.0, 0.0, 0.0, rho_s) for x in (0.2, 0.5, 0.8)]
     return grid, params, planes, parts
+
+
+def droplet_on_cylinder(NXM=128, Rd=0.5, Rs=0.3, theta=90.0, Cn=0.01, rho_ratio=1e-3, mu_ratio=1e-2, Re=100.0,
+                        We=10.0, **param_kw):
+    """Sessile droplet on a static cylinder, the synthetic stand-in for the
+    reference's VoF_init_planar_droplet_on_static_cylinder_theta
+    (IO/VoF_Init.c:2496-2597) with seeded radii: that case is the half of a
+    symmetric problem on a free-slip symmetry plane; here the whole problem
+    sits in a box x in [0, 2] (periodic) by y in [0, 4] (no-slip walls) of
+    NXM x 2 NXM square cells.  The fixed cylinder of radius Rs is centred at
+    (1, 1), the liquid droplet of radius Rd at (1, 1 + 0.75 (Rs + Rd)) (the
+    reference's centre distance 0.75 at Rs = Rd = 0.5); gas of density ratio
+    rho_ratio and viscosity ratio mu_ratio around, surface tension with
+    contact angle theta (degrees), no gravity.  C is the reference's cell
+    average over 5 x 5 sub-samples of 0.5 (1 + tanh(s / (2 sqrt 2 Cn))), s the
+    signed distance to the droplet's circle, capped by 1 - C_S of the
+    cylinder's diffuse profile.  Cn is raised to 0.75 h where h is too coarse
+    to resolve it (the reference's own value for an unset Cn).  Returns
+    (grid, params, planes, particles), particles as rows (mobile, x, y, R, u,
+    v, omega_z, rho_s)."""
+    NYM = 2 * NXM
+    grid = planar_grid(NXM, NYM, 2.0, 4.0)
+    h = 2.0 / NXM
+    cn = max(Cn, 0.75 * h)
+    params = default_params(Re=Re, rho1=1.0, rho2=rho_ratio, mu1=1.0, mu2=mu_ratio, Cn=cn, Pe_CH=1.0 / cn,
+                            surface_tension=1, We=We, **param_kw)
+    params.grav[0], params.grav[1], params.grav[2] = 0.0, 0.0, 0.0
+    params.contact_angle_deg = theta
+    xs, ys = 1.0, 1.0
+    xd, yd = xs, ys + 0.75 * (Rs + Rd)
+    xc, yc, _, _ = cell_centres(grid)
+    S = 5
+    off = (np.arange(S) + 0.5) / S - 0.5
+    bw = 2.0 * math.sqrt(2.0) * cn
+    shift_S = math.sqrt(2.0) * math.log(19.0) * cn
+    denom_S = 2.0 * math.sqrt(2.0) * cn
+    C = np.zeros((yc.size, xc.size))
+    for oy in off:
+        Y = (yc + oy * h)[:, None]
+        for ox in off:
+            X = (xc + ox * h)[None, :]
+            cl = 0.5 * (1.0 + np.tanh((Rd - np.sqrt((X - xd) ** 2 + (Y - yd) ** 2)) / bw))
+            cs = 0.5 - 0.5 * np.tanh((np.sqrt((X - xs) ** 2 + (Y - ys) ** 2) - (Rs - shift_S)) / denom_S)
+            C += np.clip(np.minimum(cl, np.maximum(1.0 - cs, 0.0)), 0.0, None) / (S * S)
+    z = np.zeros_like(C)
+    return grid, params, {"F": C, "U": z, "V": z.copy(), "P": z.copy()}, [(0, xs, ys, Rs, 0.0, 0.0, 0.0, 1.0)]
+
+
+def droplet_batch(n=64, seed=0, nxm_min=64, nxm_max=512, **kw):
+    """The batching form's cases: n sessile droplets on static cylinders
+    (droplet_on_cylinder) with NXM log-uniform in [nxm_min, nxm_max] (a
+    multiple of 8, NYM = 2 NXM), droplet radius U(0.3, 0.6), cylinder radius
+    U(0.2, 0.4), contact angle U(30, 150) degrees, all seeded.  Returns a list
+    of (grid, params, planes, particles)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nxm = int(round(math.exp(rng.uniform(math.log(nxm_min), math.log(nxm_max))) / 8.0)) * 8
+        nxm = min(max(nxm, nxm_min), nxm_max)
+        Rd, Rs, th = rng.uniform(0.3, 0.6), rng.uniform(0.2, 0.4), rng.uniform(30.0, 150.0)
+        out.append(droplet_on_cylinder(nxm, Rd=Rd, Rs=Rs, theta=th, **kw))
+    return out

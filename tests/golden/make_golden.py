@@ -136,6 +136,10 @@ IBM_STEP_CASES = [
     ("ibm_axi_steps_st", "ibm_axi_st", dict(_builder="rising_bubble", **AXI_GRID_IBM, surface_tension=True, We=200.0,
                                             velocity_seed=23, velocity_amp=0.1, **AXI_TIGHT), AXI_SPHERE, 90.0, 2,
      1e-3),
+    # the batching form's case in small: a sessile droplet on a static
+    # cylinder (pvof.cases.droplet_on_cylinder), contact angle 60 degrees
+    ("drop_cyl_st", "ibm2d_st", dict(_builder="droplet_on_cylinder", NXM=32, Rd=0.5, Rs=0.3, theta=60.0, **TIGHT),
+     [(0, 1.0, 1.0, 0.3, 0.0, 0.0, 0.0, 1.0)], 60.0, 3, 1e-3),
 ]
 
 # constant-density FFT Poisson cases (oracle/ref/fft_driver.c on the fft2d build):
@@ -180,7 +184,7 @@ def build_case(kw):
     builder = getattr(cases, build.pop("_builder", "rayleigh_taylor"))
     refcase = build.pop("_refcase", None)
     theta = build.pop("_theta", None)
-    grid, params, planes = builder(**build)
+    grid, params, planes = builder(**build)[:3]
     if theta is not None:
         params.contact_angle_deg = theta
     return grid, params, planes, refcase

@@ -83,3 +83,57 @@ def test_particles_in_lubrication_range_are_refused():
     s.set_stage(0, 1e-3)
     with pytest.raises(runtime.PvofError, match="lubrication range"):
         s.substep()
+
+
+def test_droplet_on_cylinder_matches_reference():
+    """The batching form's case in small (a sessile droplet on a static
+    cylinder, contact angle 60 degrees; fixture tests/golden/drop_cyl_st.npz
+    from the ibm2d_st reference build): three whole steps, state fields
+    within 1e-12, the cylinder's reaction force and torque within 1e-10."""
+    from pvof import runtime
+    grid, params, planes, d, meta = load_golden("drop_cyl_st")
+    s = runtime.Solver(grid, params, device=0)
+    s.set_particles([tuple(p) for p in meta["particles"]])
+    s.set_planes(dict(planes, C_L=planes["F"]))
+    s.initialize()
+    for n in range(1, meta["steps"] + 1):
+        for rk in range(3):
+            if n > 1 and rk == 0:
+                s.call("Velocity_cell_center")
+            s.set_stage(rk, meta["dt"])
+            s.substep()
+        worst = {f: rel_l2(physical(grid, g_range(grid, s.get(f)), f), physical(grid, d["s%d/%s" % (n, f)], f))
+                 for f in STATE}
+        bad = {f: r for f, r in worst.items() if not r <= 1e-12}
+        assert not bad, "s%d: %s" % (n, bad)
+        check_particles(s, d, "s%d" % n, 0.0, 1e-10, True)
+
+
+def test_droplet_on_cylinder_fp32_form_and_graphs():
+    """The same case as the batching form runs it: FP32 stencils, substeps
+    replayed from CUDA graphs (the particle bookkeeping on the device), 6
+    steps, against the FP64 path launched step by step: velocity within
+    1e-5 relative L2, the liquid volume within 1e-6 relative, the graphs
+    replayed."""
+    from pvof import cases, runtime
+    out = {}
+    for fp32 in (0, 1):
+        grid, params, planes, parts = cases.droplet_on_cylinder(48, Rd=0.45, Rs=0.3, theta=120.0,
+                                                                 P_CG_MAXIT=4000, stencil_fp32=fp32)
+        s = runtime.Solver(grid, params, device=0)
+        s.set_graphs(bool(fp32))
+        s.set_particles(parts)
+        s.set_planes(dict(planes, C_L=planes["F"]))
+        s.initialize()
+        s.run_steps(6, 2e-4)
+        out[fp32] = ({f: physical(grid, g_range(grid, s.get(f)), f) for f in ("U", "V", "C_L")}, s.liquid_mass(),
+                     s.graph_replays())
+        s.close()
+    (a, ma, _), (b, mb, replays) = out[0], out[1]
+    for f in ("U", "V"):
+        r = rel_l2(b[f], a[f])
+        print("%s rel L2 %.2e" % (f, r))
+        assert r <= 1e-5, (f, r)
+    print("volume rel %.2e, graph replays %d" % (abs(mb - ma) / ma, replays))
+    assert abs(mb - ma) <= 1e-6 * ma
+    assert replays > 0
