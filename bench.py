@@ -532,6 +532,121 @@ def mixed_batch(args, device):
             "vs_sequential": seq_ms / span}
 
 
+DROP_DT = 1e-4
+
+
+def droplet_reference(case, steps, timeout=1800):
+    """The reference build with resolved particles and surface tension
+    (oracle/_ref/ref_ibm2d_st) on one droplet case for ``steps`` steps on the
+    host; (cell-updates/s, seconds) or None."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle as po  # checker / CPU baseline only
+    if not os.path.exists(po.ref_binary("ibm2d_st")):
+        return None
+    grid, params, planes, parts = case
+    fixed = [p[1:7] for p in parts if not p[0]]
+    mobile = [p[1:7] for p in parts if p[0]]
+    with tempfile.TemporaryDirectory() as wd:
+        cp = po.run_reference_ibm(wd, grid, params, planes, fixed, mobile, DROP_DT, 0, case="ibm2d_st",
+                                  mode="steps", nsteps=steps, timeout=timeout)
+    for line in cp.stdout.splitlines():
+        if line.startswith("REF_TIMING"):
+            kv = dict(x.split("=") for x in line.split()[1:])
+            secs = float(kv["seconds"])
+            return int(kv["cells"]) * int(kv["steps"]) / secs, secs
+    return None
+
+
+def droplet_batch(args, dist, device, ws, rank):
+    """The batching form's workload: --droplets seeded sessile droplets on
+    static cylinders (pvof.cases.droplet_batch: grids log-uniform from 64x128
+    to 512x1024, droplet radius U(0.3,0.6), cylinder radius U(0.2,0.4),
+    contact angle U(30,150) degrees, density ratio 1e-3, Cn 0.01) in the FP32
+    stencil form with the pressure warm start.  The cases are split over the
+    ranks by cell count (pvof.dist.run_sharded_batch, no collective on the
+    data path); each rank advances its shard concurrently with
+    pvof_run_steps_batched, every substep replayed from CUDA graphs, timed by
+    the host clock (max over ranks).  Rank 0 also runs the two smallest cases
+    in FP64 for the form's error and times the reference on the smallest."""
+    from pvof import cases, runtime
+    from pvof import dist as pdist
+    kw = dict(P_CG_MAXIT=20000, stencil_fp32=1, pressure_warm_start=1)
+    allc = cases.droplet_batch(args.droplets, seed=args.droplet_seed, **kw)
+    costs = [float(g.NXM * g.NYM) for g, _, _, _ in allc]
+    nsteps = max(1, min(args.steps, args.droplet_steps))
+
+    def start(case):
+        g, p, pl, parts = case
+        s = runtime.Solver(g, p, device=device)
+        s.set_particles(parts)
+        s.set_planes(dict(pl, C_L=pl["F"]))
+        s.initialize()
+        return s
+
+    def run_batch(idx):
+        solvers = [start(allc[q]) for q in idx]
+        if solvers:
+            runtime.run_steps_batched(solvers, max(1, args.droplet_warmup), DROP_DT)
+        m0 = [s.liquid_mass() for s in solvers]
+        c0 = [s.clamp_mass_total() for s in solvers]
+        r0 = [s.graph_replays() for s in solvers]
+        barrier(dist)
+        t0 = time.perf_counter()
+        if solvers:
+            runtime.run_steps_batched(solvers, nsteps, DROP_DT)
+        secs = time.perf_counter() - t0
+        res = {}
+        for q, s, m, c, r in zip(idx, solvers, m0, c0, r0):
+            res[q] = {"grid": "%dx%d" % (allc[q][0].NXM, allc[q][0].NYM),
+                      "volume_change": (s.liquid_mass() - m) / m, "clamp_change": (s.clamp_mass_total() - c) / m,
+                      "graph_replays": s.graph_replays() - r, "substeps": 3 * nsteps}
+            s.close()
+        return res, secs
+
+    merged, shard, secs = pdist.run_sharded_batch(dist, costs, run_batch, device="cuda")
+    cells = int(sum(costs))
+    out = {"cases": len(allc), "cells": cells, "steps": nsteps, "warmup_steps": max(1, args.droplet_warmup),
+           "dt": DROP_DT, "value": cells * nsteps / secs, "unit": UNIT, "seconds": secs,
+           "clock": "host wall clock around pvof_run_steps_batched, max over ranks",
+           "form": "fp32 stencils + same-stage pressure warm start, Jacobi-PCG pressure (FP64)",
+           "sharding": "%d rank(s), cases split by cell count" % ws,
+           "graph_replayed_substeps": sum(v["graph_replays"] for v in merged.values()),
+           "substeps": sum(v["substeps"] for v in merged.values()),
+           "max_abs_volume_change_net_of_clamp": max(abs(v["volume_change"] - v["clamp_change"])
+                                                     for v in merged.values()),
+           "grids": {"min": min(merged.values(), key=lambda v: int(v["grid"].split("x")[0]))["grid"],
+                     "max": max(merged.values(), key=lambda v: int(v["grid"].split("x")[0]))["grid"]}}
+    if rank == 0:
+        small = sorted(range(len(allc)), key=lambda q: (costs[q], q))[:2]
+        errs = []
+        for q in small:
+            st = {}
+            for fp32 in (0, 1):
+                g, p, pl, parts = cases.droplet_batch(args.droplets, seed=args.droplet_seed,
+                                                      **dict(kw, stencil_fp32=fp32, pressure_warm_start=fp32))[q]
+                s = start((g, p, pl, parts))
+                s.run_steps(max(1, args.droplet_warmup) + nsteps, DROP_DT)
+                st[fp32] = ({f: s.get(f) for f in ("U", "V")}, s.liquid_mass())
+                s.close()
+            import numpy as np
+            vel = max(float(np.linalg.norm(st[1][0][f] - st[0][0][f]) / max(np.linalg.norm(st[0][0][f]), 1e-300))
+                      for f in ("U", "V"))
+            errs.append({"grid": "%dx%d" % (allc[q][0].NXM, allc[q][0].NYM), "velocity_rel_l2": vel,
+                         "volume_rel": abs(st[1][1] - st[0][1]) / st[0][1]})
+        out["error_vs_fp64"] = errs
+        if args.droplet_ref_steps > 0:
+            q = small[0]
+            r = droplet_reference(cases.droplet_batch(args.droplets, seed=args.droplet_seed)[q],
+                                  args.droplet_ref_steps)
+            if r is not None:
+                out["cpu_reference"] = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
+                                        "sample": "%d time step(s) of the smallest case (%dx%d) by the single-rank "
+                                                  "reference build with resolved particles and surface tension, "
+                                                  "%.1f s" % (args.droplet_ref_steps, allc[q][0].NXM, allc[q][0].NYM,
+                                                              r[1])}
+    return out
+
+
 def pinned_like(n):
     import torch
     return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
@@ -789,6 +904,12 @@ def run_ours(args):
             axisym = axisym_case(args, local)
         except Exception as e:   # noqa: BLE001
             axisym = {"error": "%s: %s" % (type(e).__name__, e)}
+    droplets = None
+    if args.droplets > 0:
+        try:
+            droplets = droplet_batch(args, dist, local, ws, rank)
+        except Exception as e:   # noqa: BLE001
+            droplets = {"error": "%s: %s" % (type(e).__name__, e)}
     large = None
     if args.large:
         try:
@@ -845,6 +966,8 @@ def run_ours(args):
             line["learned"] = learned
         if mixed is not None:
             line["batched_mixed"] = mixed
+        if droplets is not None:
+            line["batched_droplets"] = droplets
         print(json.dumps(line))
     g.close()
     if dist is not None:
@@ -867,6 +990,16 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=10)
     ap.add_argument("--timing-steps", type=int, default=20,
                     help="steps of the per-solver timing pass after the timed steps")
+    ap.add_argument("--droplets", type=int, default=64,
+                    help="also time this many seeded droplet-on-cylinder cases (the batching form's workload: 64; "
+                         "0: off), split over the ranks and advanced concurrently")
+    ap.add_argument("--droplet-steps", type=int, default=3)
+    ap.add_argument("--droplet-warmup", type=int, default=6,
+                    help="untimed steps first: a substep replays from a CUDA graph from the third time its launches "
+                         "recur (stage x surface-tension buffer parity x warm start: about six steps)")
+    ap.add_argument("--droplet-seed", type=int, default=0)
+    ap.add_argument("--droplet-ref-steps", type=int, default=1,
+                    help="steps of the reference build on the smallest droplet case (0: off)")
     ap.add_argument("--batch-mixed", action="store_true",
                     help="also time eight cases of four sizes (64x128 .. 512x1024) in all forms, batched")
     ap.add_argument("--large", action="store_true",

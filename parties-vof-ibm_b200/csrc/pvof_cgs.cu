@@ -34,6 +34,7 @@
 // reference's: the same operands in the same order.
 #include <cooperative_groups.h>
 #include <cstdlib>
+#include <mutex>
 
 #include "pvof_device.cuh"
 #include "pvof_kernels.cuh"
@@ -687,10 +688,25 @@ static cudaLaunchConfig_t strip_config(int nclusters, int nt, size_t smem, cudaS
     return cfg;
 }
 
+// The dynamic shared memory limit is an attribute of the kernel, shared by
+// every context of the process: contexts of different grid sizes need
+// different amounts, so the limit only ever grows (to the largest any
+// context launches with; a launch with less is unaffected), under a lock, as
+// contexts may be created from several threads.
+bool raise_dynamic_smem(const void *fn, size_t bytes)
+{
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) return false;
+    if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return true;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess;
+}
+
 template <class K>
 static bool strip_kernel_fits(K fn, int nt, size_t smem)
 {
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+    if (!raise_dynamic_smem((const void *)fn, smem) ||
         cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
         cudaGetLastError();
         return false;

@@ -72,6 +72,9 @@ struct SpecArgs {
     DevScalars *scal;
 };
 
+// raise a kernel's dynamic shared memory limit to at least bytes (never lower it)
+bool raise_dynamic_smem(const void *fn, size_t bytes);
+
 bool spec_supported(const Dom &d, const char **why);
 int spec_tables(int N, int M, double idx2, double idy2, std::vector<double> &tw, std::vector<double> &tri);
 int spec_pcg_blocks(int device, int N, int M);

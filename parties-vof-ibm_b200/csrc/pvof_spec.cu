@@ -642,7 +642,7 @@ int spec_pcg_blocks(int device, int N, int M)
 {
     const size_t smem = spec_pcg_smem(N, M);
     if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(k_spec_pcg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        !raise_dynamic_smem((const void *)k_spec_pcg, smem))
         return 0;
     int per_sm = 0, sms = 0, coop = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spec_pcg, SPEC_PT, smem) != cudaSuccess) return 0;

@@ -79,3 +79,18 @@ def run_sharded(dist, costs, run_case, rank=None, world_size=None):
     shard = balanced_shards(costs, ws)[rk]
     local = {idx: run_case(idx) for idx in shard}
     return gather_results(dist, local), shard
+
+
+def run_sharded_batch(dist, costs, run_batch, rank=None, world_size=None, device=None):
+    """Run run_batch(indices) once on this rank's shard of the cases (the
+    shard advances together, e.g. through pvof_run_steps_batched); run_batch
+    returns ({index: result}, seconds) for exactly those indices.  Returns the
+    merged results of all ranks, this rank's shard and the max over ranks of
+    the seconds.  Every rank calls it once (it holds collectives)."""
+    ws = world_size if world_size is not None else (dist.get_world_size() if dist else 1)
+    rk = rank if rank is not None else (dist.get_rank() if dist else 0)
+    shard = balanced_shards(costs, ws)[rk]
+    local, secs = run_batch(shard)
+    if sorted(local) != sorted(shard):
+        raise RuntimeError("run_batch returned cases %r for the shard %r" % (sorted(local), shard))
+    return gather_results(dist, local), shard, max_over_ranks(dist, secs, device=device)
