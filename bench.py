@@ -307,7 +307,10 @@ def large_case(args, device):
     nsteps = max(1, args.large_steps)
     out = {"case": "planar instability 1024x1024, density ratio 1e-3 (Atwood 0.998), Cn 0.005, dt 2e-5",
            "steps": nsteps, "unit": UNIT}
-    for label, precond, vel in (("plain", 0, 0), ("spectral", 1, 0), ("spectral + unregularised momentum", 1, 1)):
+    forms = (("plain", 0, 0), ("spectral", 1, 0), ("spectral + unregularised momentum", 1, 1))
+    pick = {"plain": 0, "spectral": 1, "spectral-unreg": 2}
+    wanted = [forms[pick[f]] for f in args.large_forms.split(",")]
+    for label, precond, vel in wanted:
         grid, params, planes = cases.rayleigh_taylor(1024, 1024, Lx=1.0, Ly=1.0, Cn=0.005,
                                                      atwood=(1 - ratio) / (1 + ratio), P_CG_MAXIT=40000)
         params.pressure_preconditioner = precond
@@ -329,7 +332,8 @@ def large_case(args, device):
                       "pressure_us_per_iteration": 1e3 * t[2]["ms"] / max(1, t[2]["iterations"]),
                       "velocity_iterations_per_step": t[1]["iterations"]}
         s.close()
-    out["spectral_vs_plain"] = out["spectral + unregularised momentum"]["value"] / out["plain"]["value"]
+    if "plain" in out and "spectral + unregularised momentum" in out:
+        out["spectral_vs_plain"] = out["spectral + unregularised momentum"]["value"] / out["plain"]["value"]
     return out
 
 
@@ -585,6 +589,14 @@ def droplet_batch(args, dist, device, ws, rank):
 
     def run_batch(idx):
         solvers = [start(allc[q]) for q in idx]
+        # stencil tiles: each case tuned alone on the GPU (launch times taken
+        # while other cases run would include their waits), a few steps each
+        for s in solvers:
+            s.set_autotune(True)
+            for _ in range(8):
+                if not s.autotune_active():
+                    break
+                s.run_steps(1, DROP_DT)
         if solvers:
             runtime.run_steps_batched(solvers, max(1, args.droplet_warmup), DROP_DT)
         m0 = [s.liquid_mass() for s in solvers]
@@ -597,9 +609,13 @@ def droplet_batch(args, dist, device, ws, rank):
         secs = time.perf_counter() - t0
         res = {}
         for q, s, m, c, r in zip(idx, solvers, m0, c0, r0):
+            rep = s.autotune_report()
             res[q] = {"grid": "%dx%d" % (allc[q][0].NXM, allc[q][0].NYM),
                       "volume_change": (s.liquid_mass() - m) / m, "clamp_change": (s.clamp_mass_total() - c) / m,
-                      "graph_replays": s.graph_replays() - r, "substeps": 3 * nsteps}
+                      "graph_replays": s.graph_replays() - r, "substeps": 3 * nsteps,
+                      "tuned": sum(1 for e in rep if e["decided"]), "tunable": len(rep),
+                      "tiles": {e["kernel"]: [e["tile"], round(e["best_us"], 2), round(e["default_us"], 2)]
+                                for e in rep}}
             s.close()
         return res, secs
 
@@ -615,7 +631,14 @@ def droplet_batch(args, dist, device, ws, rank):
            "max_abs_volume_change_net_of_clamp": max(abs(v["volume_change"] - v["clamp_change"])
                                                      for v in merged.values()),
            "grids": {"min": min(merged.values(), key=lambda v: int(v["grid"].split("x")[0]))["grid"],
-                     "max": max(merged.values(), key=lambda v: int(v["grid"].split("x")[0]))["grid"]}}
+                     "max": max(merged.values(), key=lambda v: int(v["grid"].split("x")[0]))["grid"]},
+           "autotune": {"kernels_decided": sum(v["tuned"] for v in merged.values()),
+                        "kernels_met": sum(v["tunable"] for v in merged.values()),
+                        "note": "stencil tile per kernel and case, picked by the autotuner (pvof_set_autotune) with "
+                                "the case alone on the GPU before the warm-up; kernel: [tile, mean us there, mean us "
+                                "at the default 32x8]",
+                        "smallest_case": merged[min(merged, key=lambda q: (costs[q], q))]["tiles"],
+                        "largest_case": merged[max(merged, key=lambda q: (costs[q], q))]["tiles"]}}
     if rank == 0:
         small = sorted(range(len(allc)), key=lambda q: (costs[q], q))[:2]
         errs = []
@@ -995,8 +1018,9 @@ def main():
                          "0: off), split over the ranks and advanced concurrently")
     ap.add_argument("--droplet-steps", type=int, default=3)
     ap.add_argument("--droplet-warmup", type=int, default=6,
-                    help="untimed steps first: a substep replays from a CUDA graph from the third time its launches "
-                         "recur (stage x surface-tension buffer parity x warm start: about six steps)")
+                    help="untimed concurrent steps after the cases' tile tuning: a substep replays from a CUDA graph "
+                         "from the third time its launches recur (stage x surface-tension buffer parity x warm "
+                         "start: about six steps)")
     ap.add_argument("--droplet-seed", type=int, default=0)
     ap.add_argument("--droplet-ref-steps", type=int, default=1,
                     help="steps of the reference build on the smallest droplet case (0: off)")
@@ -1005,6 +1029,8 @@ def main():
     ap.add_argument("--large", action="store_true",
                     help="also time 1024x1024 at density ratio 1e-3 (plain, spectral, spectral + momentum form)")
     ap.add_argument("--large-steps", type=int, default=3)
+    ap.add_argument("--large-forms", default="plain,spectral,spectral-unreg",
+                    help="comma-separated forms of --large: plain, spectral, spectral-unreg")
     ap.add_argument("--axisym", action="store_true",
                     help="also time the axisymmetric bubble-and-sphere case (256x512) and the reference on it")
     ap.add_argument("--axisym-steps", type=int, default=10)

@@ -399,6 +399,28 @@ int pvof_flush_l2(pvof_ctx *ctx);
 #define PVOF_SOLVER_PRESSURE 2
 int pvof_set_solver_timing(pvof_ctx *ctx, int enabled);
 
+/* No counterpart in the reference: the stencil tile autotuner.  The
+ * cell-wise stencil kernels compute every cell alike whatever their
+ * thread-block shape; with enabled = 1 the next substeps time each such
+ * kernel's launches over a set of candidate tiles (32x8, 64x4, 128x2, 256x1,
+ * 32x4, 64x8; two launches each, CUDA events) and keep for each kernel the
+ * tile of the smallest mean time.  Results are bit for bit those of the
+ * default tile.  While tuning, substeps run launch by launch; tuning ends by
+ * itself once every kernel met so far is decided.  Tune a context while it
+ * has the GPU to itself: a launch's event time includes its waits behind
+ * other streams' work.  enabled = 0 stops it and
+ * returns every kernel to the default tile.  Drops the captured substep
+ * graphs. */
+int pvof_set_autotune(pvof_ctx *ctx, int enabled);
+/* 1 while the autotuner is still sampling, else 0. */
+int pvof_autotune_active(const pvof_ctx *ctx);
+/* Kernels the autotuner has met; entry q: the kernel's name, its tile, its
+ * mean launch time there and at the default tile (ms).  Returns 1 when the
+ * kernel is decided, 0 while undecided (the default tile), <0 on error. */
+int pvof_autotune_entries(const pvof_ctx *ctx);
+int pvof_autotune_entry(const pvof_ctx *ctx, int q, const char **name, int *bx, int *by, double *best_ms,
+                        double *default_ms);
+
 /* No counterpart in the reference: 1 (the default) replays the launches of
  * pvof_substep up to its first Poisson pass's divergence check from a CUDA
  * graph captured per (stage, dt, buffer parity, warm-start state); 0 issues

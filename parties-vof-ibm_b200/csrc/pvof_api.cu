@@ -213,14 +213,154 @@ void axis_map(Map1 &m, int kind, int N, bool periodic, int wall_lo, int wall_hi,
 // ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
+// --- stencil tile autotuner -----------------------------------------------
+// The cell-wise kernels issued through launch2d compute every cell with the
+// same arithmetic whatever the thread-block shape, so their tile is free.
+// pvof_set_autotune starts an online tuning over the context's next
+// substeps: each launch of a tunable kernel takes the candidate tile with
+// the fewest samples so far, bracketed by events; after every candidate has
+// TUNE_SAMPLES samples the kernel keeps the tile of the smallest mean time.
+// While tuning, substeps run launch by launch (no graph capture); the
+// results are bit for bit those of the default tile.
+struct Tile {
+    int bx, by;
+};
+constexpr Tile TUNE_TILES[] = {{TBX, TBY}, {64, 4}, {128, 2}, {256, 1}, {32, 4}, {64, 8}};
+constexpr int NTILES = sizeof(TUNE_TILES) / sizeof(TUNE_TILES[0]);
+constexpr int TUNE_SAMPLES = 2;
+constexpr int TUNE_EVENTS = 64;
+
+struct TuneRec {
+    const void *fn;
+    const char *name;
+    double ms[NTILES];
+    int n[NTILES];
+    int chosen;   // index into TUNE_TILES, -1 while undecided
+};
+
+}  // namespace
+
+struct pvof::TuneState {
+    bool active = false;
+    std::vector<TuneRec> recs;
+    cudaEvent_t ev[TUNE_EVENTS][2];
+    int pend_rec[TUNE_EVENTS], pend_tile[TUNE_EVENTS];
+    int npend = 0;
+    bool events = false;
+    ~TuneState()
+    {
+        if (events)
+            for (int q = 0; q < TUNE_EVENTS; q++) {
+                cudaEventDestroy(ev[q][0]);
+                cudaEventDestroy(ev[q][1]);
+            }
+    }
+};
+
+namespace {
+
+// the kernels the autotuner may retile (cell-wise, no block-level reductions)
+const TuneRec *tunable(const void *fn)
+{
+    static const std::vector<TuneRec> table = [] {
+        std::vector<TuneRec> t;
+        auto add = [&](const void *fn, const char *name) {
+            TuneRec r;
+            std::memset(&r, 0, sizeof(r));
+            r.fn = fn;
+            r.name = name;
+            r.chosen = -1;
+            t.push_back(r);
+        };
+#define PVOF_TUNABLE(k) add((const void *)k, #k)
+        PVOF_TUNABLE(k_weno_flux); PVOF_TUNABLE(k_weno_flux_f); PVOF_TUNABLE(k_flux_div);
+        PVOF_TUNABLE(k_laplacian); PVOF_TUNABLE(k_laplacian_f); PVOF_TUNABLE(k_bulk_S); PVOF_TUNABLE(k_bulk_S_f);
+        PVOF_TUNABLE(k_psi_LG); PVOF_TUNABLE(k_psi_LG_f); PVOF_TUNABLE(k_f_sigma); PVOF_TUNABLE(k_f_sigma_f);
+        PVOF_TUNABLE(k_u_impexp); PVOF_TUNABLE(k_v_impexp); PVOF_TUNABLE(k_set_rhs); PVOF_TUNABLE(k_rhs_vec);
+        PVOF_TUNABLE(k_p_rhs); PVOF_TUNABLE(k_p_precond); PVOF_TUNABLE(k_p_update); PVOF_TUNABLE(k_project);
+        PVOF_TUNABLE(k_density); PVOF_TUNABLE(k_cell_center); PVOF_TUNABLE(k_gravity); PVOF_TUNABLE(k_add);
+        PVOF_TUNABLE(k_add_to); PVOF_TUNABLE(k_sub_scaled); PVOF_TUNABLE(k_div_by);
+#undef PVOF_TUNABLE
+        return t;
+    }();
+    for (const TuneRec &r : table)
+        if (r.fn == fn) return &r;
+    return nullptr;
+}
+
+// the tile of a launch; with the tuner active, a candidate and an event slot
+// (slot >= 0: record ev[slot][1] after the launch)
+Tile tune_pick(pvof_ctx *c, const void *fn, int &slot)
+{
+    slot = -1;
+    TuneState *t = c->tune;
+    if (!t) return TUNE_TILES[0];
+    int q = -1;
+    for (size_t k = 0; k < t->recs.size(); k++)
+        if (t->recs[k].fn == fn) { q = (int)k; break; }
+    if (q < 0) {
+        const TuneRec *r = tunable(fn);
+        if (!r) return TUNE_TILES[0];
+        t->recs.push_back(*r);
+        q = (int)t->recs.size() - 1;
+    }
+    TuneRec &r = t->recs[(size_t)q];
+    if (r.chosen >= 0) return TUNE_TILES[r.chosen];
+    if (!t->active || !t->events || t->npend >= TUNE_EVENTS) return TUNE_TILES[0];
+    int best = 0;
+    for (int k = 1; k < NTILES; k++)
+        if (r.n[k] < r.n[best]) best = k;
+    slot = t->npend++;
+    t->pend_rec[slot] = q;
+    t->pend_tile[slot] = best;
+    if (cudaEventRecord(t->ev[slot][0], c->stream) != cudaSuccess) {
+        t->npend--;
+        slot = -1;
+        return TUNE_TILES[0];
+    }
+    return TUNE_TILES[best];
+}
+
+// after a stream synchronisation: the finished samples into their kernels,
+// decisions for the kernels with every candidate sampled; the tuner stops
+// when every kernel seen so far is decided
+void collect_tune(pvof_ctx *c)
+{
+    TuneState *t = c->tune;
+    if (!t || !t->active) return;
+    for (int q = 0; q < t->npend; q++) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, t->ev[q][0], t->ev[q][1]) != cudaSuccess) continue;
+        TuneRec &r = t->recs[(size_t)t->pend_rec[q]];
+        r.ms[t->pend_tile[q]] += ms;
+        r.n[t->pend_tile[q]] += 1;
+    }
+    t->npend = 0;
+    bool all = !t->recs.empty();
+    for (TuneRec &r : t->recs) {
+        if (r.chosen >= 0) continue;
+        bool done = true;
+        for (int k = 0; k < NTILES; k++) done = done && r.n[k] >= TUNE_SAMPLES;
+        if (!done) { all = false; continue; }
+        int best = 0;
+        for (int k = 1; k < NTILES; k++)
+            if (r.ms[k] / r.n[k] < r.ms[best] / r.n[best]) best = k;
+        r.chosen = best;
+    }
+    if (all) t->active = false;
+}
+
 template <class K, class... Args>
 int launch2d(pvof_ctx *c, K kernel, int i0, int i1, int j0, int j1, Args... args)
 {
     if (i1 <= i0 || j1 <= j0) return PVOF_OK;
-    dim3 blk(TBX, TBY);
-    dim3 grd((unsigned)((i1 - i0 + TBX - 1) / TBX), (unsigned)((j1 - j0 + TBY - 1) / TBY));
+    int slot;
+    const Tile t = tune_pick(c, (const void *)kernel, slot);
+    dim3 blk((unsigned)t.bx, (unsigned)t.by);
+    dim3 grd((unsigned)((i1 - i0 + t.bx - 1) / t.bx), (unsigned)((j1 - j0 + t.by - 1) / t.by));
     kernel<<<grd, blk, 0, c->stream>>>(c->dom, i0, i1, j0, j1, args...);
     CKL(c);
+    if (slot >= 0) CK(cudaEventRecord(c->tune->ev[slot][1], c->stream));
     return PVOF_OK;
 }
 
@@ -743,6 +883,7 @@ int p_solve_spectral(pvof_ctx *c)
         std::vector<double> h(tw);
         h.resize(h.size() + parts, 0.0);
         h.insert(h.end(), tri.begin(), tri.end());
+        h.resize(h.size() + 3 * c->plane_elems, 0.0);   // the face coefficients and weight roots of a solve
         if (cudaMalloc(&c->spec_mem, h.size() * sizeof(double)) != cudaSuccess ||
             cudaMalloc(&c->spec_s, sizeof(SpecScal)) != cudaSuccess)
             return set_err(PVOF_ENOMEM, "allocating the spectral preconditioner");
@@ -767,6 +908,15 @@ int p_solve_spectral(pvof_ctx *c)
     A.tw = reinterpret_cast<const double2 *>(c->spec_mem);
     A.part = c->spec_mem + N;
     A.tri = A.part + 3 * (size_t)c->spec_blocks;
+    {
+        const int NW = N / 2 + 1;
+        const int P = M / 2 < 32 ? M / 2 : 32;   // spec_tables' chunk rule: P chunks, K the longest
+        const int K = M / P + (M % P ? 1 : 0);
+        double *planes = const_cast<double *>(A.tri) + (size_t)NW * (2 * K + 4) * 32;
+        A.cx = planes + (size_t)OY * c->dom.P + OX;
+        A.cy = A.cx + c->plane_elems;
+        A.sm = A.cy + c->plane_elems;
+    }
     A.N = N;
     A.logN = 0;
     while ((1 << A.logN) < N) A.logN++;
@@ -835,6 +985,7 @@ int read_scalars(pvof_ctx *c)
     CK(cudaMemcpyAsync(c->scal_host, c->scal, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (c->npend) collect_solver_timing(c);
+    collect_tune(c);
     if (c->scal_host->error) {
         const int code = c->scal_host->error;
         CK(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
@@ -1006,7 +1157,7 @@ void drop_graphs(pvof_ctx *c)
 
 int run_region(pvof_ctx *c, bool warm0)
 {
-    if (!c->use_graphs || c->solver_timing || c->p.pressure_warm_start == 2)
+    if (!c->use_graphs || c->solver_timing || (c->tune && c->tune->active) || c->p.pressure_warm_start == 2)
         return substep_region(c, warm0);
     GraphKey k;
     k.stage = c->stage;
@@ -1758,6 +1909,7 @@ int pvof_destroy(pvof_ctx *c)
     for (int q = 0; q < Ctx::NPEND; q++)
         for (int e = 0; e < 2; e++) if (c->pend_ev[q][e]) cudaEventDestroy(c->pend_ev[q][e]);
     delete c->ibm;
+    delete c->tune;
     for (GraphEntry &g : c->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     if (c->fft_coef) cudaFree(c->fft_coef);
@@ -2066,6 +2218,46 @@ long long pvof_spectral_tables(int N, int M, double idx2, double idy2, double *o
     const long long n = (long long)tri.size();
     if (out && cap >= n) std::memcpy(out, tri.data(), tri.size() * sizeof(double));
     return n;
+}
+
+int pvof_set_autotune(pvof_ctx *c, int enabled)
+{
+    ENTER(c);
+    drop_graphs(c);   // they hold the launches' tiles
+    if (!c->tune) {
+        c->tune = new TuneState();
+        bool ok = true;
+        for (int q = 0; q < TUNE_EVENTS && ok; q++)
+            ok = cudaEventCreate(&c->tune->ev[q][0]) == cudaSuccess && cudaEventCreate(&c->tune->ev[q][1]) == cudaSuccess;
+        if (!ok) {
+            delete c->tune;
+            c->tune = nullptr;
+            return set_err(PVOF_ECUDA, "cudaEventCreate for the autotuner");
+        }
+        c->tune->events = true;
+    }
+    c->tune->recs.clear();
+    c->tune->npend = 0;
+    c->tune->active = enabled != 0;
+    return PVOF_OK;
+}
+
+int pvof_autotune_active(const pvof_ctx *c) { return c && c->tune && c->tune->active ? 1 : 0; }
+
+int pvof_autotune_entries(const pvof_ctx *c) { return c && c->tune ? (int)c->tune->recs.size() : 0; }
+
+int pvof_autotune_entry(const pvof_ctx *c, int q, const char **name, int *bx, int *by, double *best_ms,
+                        double *default_ms)
+{
+    if (!c || !c->tune || q < 0 || q >= (int)c->tune->recs.size()) return set_err(PVOF_EINVAL, "bad autotuner entry");
+    const TuneRec &r = c->tune->recs[(size_t)q];
+    if (name) *name = r.name;
+    const int k = r.chosen >= 0 ? r.chosen : 0;
+    if (bx) *bx = TUNE_TILES[k].bx;
+    if (by) *by = TUNE_TILES[k].by;
+    if (best_ms) *best_ms = r.n[k] ? r.ms[k] / r.n[k] : 0.0;
+    if (default_ms) *default_ms = r.n[0] ? r.ms[0] / r.n[0] : 0.0;
+    return r.chosen >= 0 ? 1 : 0;
 }
 
 int pvof_set_solver_timing(pvof_ctx *c, int enabled)

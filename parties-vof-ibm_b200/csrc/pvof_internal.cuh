@@ -193,6 +193,7 @@ struct Ctx {
     GraphEntry graphs[NGRAPHS];
     int graph_next;
     long long graph_replays; // substeps whose launches came from a graph
+    struct TuneState *tune;  // stencil tile autotuner (null until pvof_set_autotune)
 };
 
 }  // namespace pvof

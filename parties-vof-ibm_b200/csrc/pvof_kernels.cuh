@@ -63,6 +63,7 @@ struct SpecArgs {
     double *res, *z, *Ad, *hat;
     const double2 *tw;        // exp(-2 pi i k / N), k < N / 2
     const double *tri;        // the tridiagonal phase's coefficients, one set per wave number (spec_tables)
+    double *cx, *cy, *sm;     // per solve: x and y face coefficients of the operator, sqrt of the Jacobi weights
     int N, logN, M;           // x cells (a power of two), log2 N, y cells
     double fscale;            // dy^2 / N
     double tol;

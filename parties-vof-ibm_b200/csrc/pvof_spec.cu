@@ -48,7 +48,8 @@
 // 128-thread row groups in the row phases, eight warps of one tridiagonal
 // system each per block in the solve phase, four grid barriers per iteration (after the
 // matrix-vector product, the update with its forward transforms, the
-// tridiagonal solves, the inverse transforms).  Every block adds the
+// tridiagonal solves, the inverse transforms), one more per solve after the
+// solve's constants (face coefficients, weight roots).  Every block adds the
 // per-block sums in block order, so all of them take the same decisions.  The
 // grid barrier resets itself (the last arriver zeroes the count and advances
 // a generation); its wait is bounded (on timeout the error flag in DevScalars
@@ -254,6 +255,21 @@ __device__ __forceinline__ double2 half_complex(const SpecArgs &A, int k, int j)
     return make_double2(AT_(A.hat, N - k, j), -AT_(A.hat, k, j));
 }
 
+// pressure_op (Pressure_operator_variableCoeff, psolve_cg.c:302-344) in the
+// planar mode from the solve's face coefficients: cx(i, j) is the x face
+// between cells i and i+1, (2 / (rho_i + rho_i+1)) idx^2, the same value as
+// pressure_op's cxp at i and cxm at i+1 (the sum in the division commutes);
+// cy likewise in y.  Bit for bit pressure_op's result.
+template <class Get>
+__device__ __forceinline__ double spec_op(const SpecArgs &A, int i, int j, Get get)
+{
+    const int P = A.d.P;
+    const double c = get(i, j);
+    const double val = AT_(A.cx, i, j) * (get(i + 1, j) - c) - AT_(A.cx, i - 1, j) * (c - get(i - 1, j)) +
+                       AT_(A.cy, i, j) * (get(i, j + 1) - c) - AT_(A.cy, i, j - 1) * (c - get(i, j - 1));
+    return 1.0 * val;
+}
+
 __device__ __forceinline__ int src_x(const SpecArgs &A, int i) { return A.mp.x.src[i + NG]; }
 __device__ __forceinline__ int src_y(const SpecArgs &A, int j) { return A.mp.y.src[j + NG]; }
 
@@ -292,21 +308,59 @@ __device__ __forceinline__ double warp_total(double v)
 //           for i = L - 2 .. 1
 // The mean mode (m = 0) is made mean-free with its first row pinned on the
 // way in, and given the right-hand side's mean back on the way out.
-__device__ void tridiag_phase(const SpecArgs &A, double *area)
+// asynchronous 8-byte global -> shared copies (cp.async): all of a thread's
+// copies are in flight together, and no register holds them
+__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gmem_src)
+{
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// shared-memory layout of the solve phase (doubles after the twiddles): the
+// row groups' rows overlap the systems' columns and reduction scratch; the
+// tables come after both
+__host__ __device__ inline size_t spec_tab_offset(int N, int M)
+{
+    const size_t rows = (size_t)ROWG * N * 2;
+    const size_t cols = (size_t)SPEC_SYS * ((size_t)M + (M >> 5) + 1 + 256);
+    return rows > cols ? rows : cols;
+}
+
+// the table rows of the sweeps (pivots and couplings, 2K x 32 per system) of
+// the block's systems q0 .. q0 + SPEC_SYS - 1 into shared memory
+__device__ void stage_tables(const SpecArgs &A, double *tabs, int q0)
+{
+    const int N = A.N;
+    const int K = spec_chunks(A.M).K, TW = (2 * K + 4) * 32, TS = 2 * K * 32;
+    for (int e = threadIdx.x; e < SPEC_SYS * TS; e += blockDim.x) {
+        const int s = e / TS, r = e - s * TS;
+        if (q0 + s >= N) continue;
+        const int m = system_index(q0 + s, N);
+        cp_async8(tabs + e, A.tri + (size_t)(m <= N / 2 ? m : N - m) * TW + r);
+    }
+}
+
+__device__ void tridiag_phase(const SpecArgs &A, double *area, bool resident)
 {
     const int N = A.N, M = A.M, P = A.d.P;
     const Chunks ch = spec_chunks(M);
-    const int K = ch.K, TW = (2 * K + 4) * 32;
+    const int K = ch.K, TW = (2 * K + 4) * 32, TS = 2 * K * 32;
     const int CP = M + (M >> 5) + 1;
     double *cols = area;                      // SPEC_SYS columns of CP doubles
     double *red = area + SPEC_SYS * CP;       // per warp: rhs, lower coupling, pivot, c' of the 2P equations
+    double *tabs = area + spec_tab_offset(N, M);   // per system: the table's pivot and coupling rows (2K x 32)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int q0 = blockIdx.x * SPEC_SYS; q0 < N; q0 += gridDim.x * SPEC_SYS) {
         __syncthreads();   // the previous group's columns are stored
         for (int e = threadIdx.x; e < SPEC_SYS * M; e += blockDim.x) {
             const int j = e / SPEC_SYS, s = e - j * SPEC_SYS;
-            if (q0 + s < N) cols[s * CP + cidx(j)] = AT_(A.hat, system_index(q0 + s, N), j);
+            if (q0 + s < N) cp_async8(cols + s * CP + cidx(j), &AT_(A.hat, system_index(q0 + s, N), j));
         }
+        // with one group per block the tables stay in shared memory for the
+        // whole solve (staged before the first iteration)
+        if (!resident) stage_tables(A, tabs, q0);
+        cp_async_wait_all();
         __syncthreads();
         const int q = q0 + warp;
         if (warp < SPEC_SYS && q < N) {
@@ -314,7 +368,8 @@ __device__ void tridiag_phase(const SpecArgs &A, double *area)
             double *rw = red + warp * 256;
             const int m = system_index(q, N);
             const int wave = m <= N / 2 ? m : N - m;
-            const double *__restrict__ T = A.tri + (size_t)wave * TW;
+            const double *__restrict__ T = A.tri + (size_t)wave * TW;   // rows 2K.. (the reduced system)
+            const double *St = tabs + warp * TS;                          // rows 0 .. 2K-1, staged
             double rmean = 0.0;
             if (m == 0) {   // mean-free, first row pinned
                 double sum = 0.0;
@@ -330,17 +385,17 @@ __device__ void tridiag_phase(const SpecArgs &A, double *area)
 #pragma unroll 4
                 for (int i = 1; i < len; i++) {
                     const int c = cidx(st + i);
-                    const double r = T[i * 32 + lane], dv = col[c];
+                    const double r = St[i * 32 + lane], dv = col[c];
                     Dp = i == 1 ? r * dv : r * (dv + Dp);
                     col[c] = Dp;
                 }
                 double E = 0.0;
 #pragma unroll 4
-                for (int i = len - 2; i >= 1; i--) E = col[cidx(st + i)] + T[i * 32 + lane] * E;
-                rw[2 * lane] = col[cidx(st)] - T[lane] * E;
+                for (int i = len - 2; i >= 1; i--) E = col[cidx(st + i)] + St[i * 32 + lane] * E;
+                rw[2 * lane] = col[cidx(st)] - St[lane] * E;
                 rw[2 * lane + 1] = Dp;
-                rw[64 + 2 * lane] = T[K * 32 + lane];
-                rw[64 + 2 * lane + 1] = T[(K + len - 1) * 32 + lane];
+                rw[64 + 2 * lane] = St[K * 32 + lane];
+                rw[64 + 2 * lane + 1] = St[(K + len - 1) * 32 + lane];
                 rw[128 + 2 * lane] = T[(2 * K) * 32 + lane];
                 rw[192 + 2 * lane] = T[(2 * K + 1) * 32 + lane];
                 rw[128 + 2 * lane + 1] = T[(2 * K + 2) * 32 + lane];
@@ -371,7 +426,7 @@ __device__ void tridiag_phase(const SpecArgs &A, double *area)
 #pragma unroll 4
                 for (int i = len - 2; i >= 1; i--) {
                     const int c = cidx(st + i);
-                    xn = col[c] - T[(K + i) * 32 + lane] * x0 + T[i * 32 + lane] * xn;
+                    xn = col[c] - St[(K + i) * 32 + lane] * x0 + St[i * 32 + lane] * xn;
                     col[c] = xn;
                 }
             }
@@ -416,13 +471,34 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
     SpecArgs B = A;
     B.tw = tw;
 
+    // the solve's constants: face coefficients (x faces i = -1 .. N-1 of rows
+    // 0 .. M-1, y faces j = -1 .. M-1 of columns 0 .. N-1) and the square roots
+    // of the Jacobi weights, from the density's ghosted plane
+    {
+        const double idx2 = d.m.idx_c[1] * d.m.idx_c[1], idy2 = d.m.idy_c[1] * d.m.idy_c[1];
+        const int W = N + 1, cells = W * (M + 1);
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < cells; e += gridDim.x * blockDim.x) {
+            const int j = e / W - 1, i = e - (j + 1) * W - 1;
+            if (j >= 0) AT_(A.cx, i, j) = (2.0 / (AT_(A.rho, i, j) + AT_(A.rho, i + 1, j))) * idx2;
+            if (i >= 0) AT_(A.cy, i, j) = (2.0 / (AT_(A.rho, i, j) + AT_(A.rho, i, j + 1))) * idy2;
+            if (i >= 0 && j >= 0) AT_(A.sm, i, j) = sqrt(AT_(A.MJ, i, j));
+        }
+    }
+    // one group of systems per block: its tables are staged once for the solve
+    const bool resident = (int)gridDim.x * SPEC_SYS >= N;
+    if (resident) {
+        stage_tables(A, work + spec_tab_offset(N, M), blockIdx.x * SPEC_SYS);
+        cp_async_wait_all();
+    }
+    if (!spec_barrier(S, err)) return;
+
     // r = rhs - A phi, the stopping sum, forward transforms
     auto residual = [&](int i, int j, double &sum) {
-        const double ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, A.phi, P, NX, NY, a, b); });
+        const double ad = spec_op(A, i, j, [&](int a, int b) { return remap(A.mp, A.phi, P, NX, NY, a, b); });
         const double rv = AT_(A.rhs, i, j) - ad;
         AT_(A.res, i, j) = rv;
         sum += rv * (rv * AT_(A.MJ, i, j));
-        return rv * sqrt(AT_(A.MJ, i, j));
+        return rv * AT_(A.sm, i, j);
     };
     double sJ = 0.0;
     for (int p0 = blockIdx.x * ROWG; 2 * p0 < M; p0 += gridDim.x * ROWG) {
@@ -448,7 +524,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
     double *dold = d0, *dnew = d1;
     for (int it = 0;; it++) {
         // z = (-L)^-1 r
-        tridiag_phase(A, work);
+        tridiag_phase(A, work, resident);
         if (!spec_barrier(S, err)) return;
         double g = 0.0;
         for (int p0 = blockIdx.x * ROWG; 2 * p0 < M; p0 += gridDim.x * ROWG) {
@@ -465,11 +541,11 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
             if (acta)
                 for (int i = lt; i < N; i += ROW_THREADS) {
                     const double2 v = row[i];
-                    const double za = v.x * sqrt(AT_(A.MJ, i, ja));
+                    const double za = v.x * AT_(A.sm, i, ja);
                     AT_(A.z, i, ja) = za;
                     g += AT_(A.res, i, ja) * za;
                     if (actb) {
-                        const double zb = v.y * sqrt(AT_(A.MJ, i, jb));
+                        const double zb = v.y * AT_(A.sm, i, jb);
                         AT_(A.z, i, jb) = zb;
                         g += AT_(A.res, i, jb) * zb;
                     }
@@ -501,7 +577,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
                 for (int i = lt; i < N; i += ROW_THREADS) {
                     const double dv = dir(i, j);
                     AT_(dnew, i, j) = dv;
-                    const double ad = pressure_op(d, A.rho, i, j, dir);
+                    const double ad = spec_op(A, i, j, dir);
                     AT_(A.Ad, i, j) = ad;
                     sdad += dv * ad;
                 }
@@ -515,7 +591,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
             const double rv = AT_(A.res, i, j) - alpha * AT_(A.Ad, i, j);
             AT_(A.res, i, j) = rv;
             sum += rv * (rv * AT_(A.MJ, i, j));
-            return rv * sqrt(AT_(A.MJ, i, j));
+            return rv * AT_(A.sm, i, j);
         };
         sJ = 0.0;
         for (int p0 = blockIdx.x * ROWG; 2 * p0 < M; p0 += gridDim.x * ROWG) {
@@ -631,9 +707,8 @@ int spec_tables(int N, int M, double idx2, double idy2, std::vector<double> &tw,
 
 size_t spec_pcg_smem(int N, int M)
 {
-    const size_t rows = (size_t)ROWG * N * sizeof(double2);
-    const size_t cols = (size_t)SPEC_SYS * ((size_t)M + (M >> 5) + 1 + 256) * sizeof(double);
-    return (size_t)N * sizeof(double) + (rows > cols ? rows : cols);   // twiddles, then the work area
+    // twiddles, the rows / columns area, the tables
+    return ((size_t)N + spec_tab_offset(N, M) + (size_t)SPEC_SYS * 64 * spec_chunks(M).K) * sizeof(double);
 }
 
 // blocks for k_spec_pcg: enough for one pass over the rows and the systems,

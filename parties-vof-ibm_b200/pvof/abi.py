@@ -126,7 +126,8 @@ EXPORTS = [
     "pvof_substep", "pvof_run_steps", "pvof_liquid_mass",
     "pvof_initialize",
     "pvof_launch_count", "pvof_timer_start", "pvof_timer_stop", "pvof_flush_l2",
-    "pvof_set_solver_timing", "pvof_solver_timing", "pvof_solver_kernel", "pvof_set_graphs", "pvof_graph_replays", "pvof_spectral_tables",
+    "pvof_set_solver_timing", "pvof_solver_timing", "pvof_set_autotune", "pvof_autotune_active",
+    "pvof_autotune_entries", "pvof_autotune_entry", "pvof_solver_kernel", "pvof_set_graphs", "pvof_graph_replays", "pvof_spectral_tables",
     "pvof_set_cluster_solvers", "pvof_clamp_mass_total",
     "pvof_Pressure_solve_cg_noalloc", "pvof_noalloc_last_error",
     "pvof_set_particles", "pvof_Lagrangian_flag_points", "pvof_particle_entries", "pvof_particle_forces",

@@ -64,6 +64,11 @@ def load():
     L.pvof_timer_stop.argtypes = [V, P(C.c_double)]
     L.pvof_flush_l2.argtypes = [V]
     L.pvof_set_solver_timing.argtypes = [V, C.c_int]
+    L.pvof_set_autotune.argtypes = [V, C.c_int]
+    L.pvof_autotune_active.argtypes = [V]
+    L.pvof_autotune_entries.argtypes = [V]
+    L.pvof_autotune_entry.argtypes = [V, C.c_int, P(C.c_char_p), P(C.c_int), P(C.c_int), P(C.c_double),
+                                      P(C.c_double)]
     L.pvof_set_graphs.argtypes = [V, C.c_int]
     L.pvof_graph_replays.argtypes = [V]
     L.pvof_graph_replays.restype = C.c_longlong
@@ -259,6 +264,25 @@ class Solver:
 
     def set_solver_timing(self, on):
         check(load().pvof_set_solver_timing(self.h, 1 if on else 0), "pvof_set_solver_timing")
+
+    def set_autotune(self, on):
+        """Start (or stop) the stencil tile autotuner over the next substeps."""
+        check(load().pvof_set_autotune(self.h, 1 if on else 0), "pvof_set_autotune")
+
+    def autotune_active(self):
+        return bool(load().pvof_autotune_active(self.h))
+
+    def autotune_report(self):
+        """[{kernel, tile, best_us, default_us, decided}] of the kernels the tuner met."""
+        L = load()
+        out = []
+        for q in range(L.pvof_autotune_entries(self.h)):
+            name, bx, by, best, dflt = C.c_char_p(), C.c_int(), C.c_int(), C.c_double(), C.c_double()
+            rc = L.pvof_autotune_entry(self.h, q, C.byref(name), C.byref(bx), C.byref(by), C.byref(best), C.byref(dflt))
+            check(min(rc, 0), "pvof_autotune_entry")
+            out.append({"kernel": name.value.decode(), "tile": "%dx%d" % (bx.value, by.value),
+                        "best_us": 1e3 * best.value, "default_us": 1e3 * dflt.value, "decided": rc == 1})
+        return out
 
     def set_graphs(self, on):
         """Replay each substep's launches from captured CUDA graphs (default on)."""
