@@ -377,9 +377,11 @@ def axisym_reference(steps, timeout=3600):
 
 def axisym_case(args, device):
     """The axisymmetric bubble-and-sphere case (density ratio 1e-3, viscosity
-    ratio 1e-2, Re 100, We 200, Cn 0.01, contact angle 90 degrees): one
-    untimed step, then --axisym-steps timed steps (device time, L2 flushed),
-    and the reference build on the host for --axisym-ref-steps steps."""
+    ratio 1e-2, Re 100, We 200, Cn 0.01, contact angle 90 degrees):
+    --axisym-warmup untimed steps, then --axisym-steps timed steps replayed
+    from CUDA graphs (device time, L2 flushed), one more step launch by launch
+    for the solver counts, and the reference build on the host for
+    --axisym-ref-steps steps."""
     from pvof import runtime
     grid, params, planes = axisym_setup()
     cells = grid.NXM * grid.NYM
@@ -387,22 +389,27 @@ def axisym_case(args, device):
     s.set_particles(AXI_SPHERE)
     s.set_planes(dict(planes, C_L=planes["F"]))
     s.initialize()
-    s.run_steps(1, AXI_DT)
+    # untimed steps first: a substep replays from a CUDA graph (the sphere's
+    # bookkeeping included) from the third time its launches recur
+    s.run_steps(max(1, args.axisym_warmup), AXI_DT)
     nsteps = max(1, args.axisym_steps)
-    s.set_solver_timing(True)
-    l0, ms = s.launch_count(), 0.0
+    l0, r0, ms = s.launch_count(), s.graph_replays(), 0.0
     for _ in range(nsteps):
         s.flush_l2()
         s.timer_start()
         s.run_steps(1, AXI_DT)
         ms += s.timer_stop()
-    t = s.solver_timing(2)
+    replays = s.graph_replays() - r0
+    launches = s.launch_count() - l0
+    timing, _, _ = solver_timing_pass(s, 1)   # one more step, launch by launch, for the solver counts
+    t = timing[2]
     out = {"case": "axisymmetric bubble (R 0.5, z 1) below a fixed sphere on the axis (R 0.25, z 2.5), 256x512, "
                    "r in [0,2], z in [0,4], density ratio 1e-3, viscosity ratio 1e-2, Re 100, We 200, Cn 0.01, "
                    "contact angle 90 degrees, dt 1e-4",
            "value": cells * nsteps / (ms * 1e-3), "unit": UNIT, "steps": nsteps, "ms_per_step": ms / nsteps,
-           "launches_per_step": (s.launch_count() - l0) / nsteps,
-           "pressure_iterations_per_step": t["iterations"] / nsteps, "pressure_kernel": s.solver_kernel(2)}
+           "launches_per_step": launches / nsteps, "graph_replayed_substeps": "%d of %d" % (replays, 3 * nsteps),
+           "pressure_iterations_per_step": t["iterations"], "pressure_ms_per_step": t["ms"],
+           "pressure_kernel": s.solver_kernel(2)}
     s.close()
     if args.axisym_ref_steps > 0:
         r = axisym_reference(args.axisym_ref_steps)
@@ -564,17 +571,20 @@ def droplet_reference(case, steps, timeout=1800):
 def droplet_batch(args, dist, device, ws, rank):
     """The batching form's workload: --droplets seeded sessile droplets on
     static cylinders (pvof.cases.droplet_batch: grids log-uniform from 64x128
-    to 512x1024, droplet radius U(0.3,0.6), cylinder radius U(0.2,0.4),
-    contact angle U(30,150) degrees, density ratio 1e-3, Cn 0.01) in the FP32
-    stencil form with the pressure warm start.  The cases are split over the
+    to 512x1024 on the widths 2^a, 3 2^a, 5 2^a, droplet radius U(0.3,0.6),
+    cylinder radius U(0.2,0.4), contact angle U(30,150) degrees, density
+    ratio 1e-3, Cn 0.01) in all four forms (FP32 stencils, warm start,
+    spectral preconditioner, unregularised momentum CG).  The cases are split over the
     ranks by cell count (pvof.dist.run_sharded_batch, no collective on the
     data path); each rank advances its shard concurrently with
     pvof_run_steps_batched, every substep replayed from CUDA graphs, timed by
     the host clock (max over ranks).  Rank 0 also runs the two smallest cases
-    in FP64 for the form's error and times the reference on the smallest."""
+    in the plain FP64 path for the forms' error and times the reference on the
+    smallest."""
     from pvof import cases, runtime
     from pvof import dist as pdist
-    kw = dict(P_CG_MAXIT=20000, stencil_fp32=1, pressure_warm_start=1)
+    kw = dict(P_CG_MAXIT=20000, stencil_fp32=1, pressure_warm_start=1, pressure_preconditioner=1,
+              velocity_cg_unregularized=1)
     allc = cases.droplet_batch(args.droplets, seed=args.droplet_seed, **kw)
     costs = [float(g.NXM * g.NYM) for g, _, _, _ in allc]
     nsteps = max(1, min(args.steps, args.droplet_steps))
@@ -624,7 +634,8 @@ def droplet_batch(args, dist, device, ws, rank):
     out = {"cases": len(allc), "cells": cells, "steps": nsteps, "warmup_steps": max(1, args.droplet_warmup),
            "dt": DROP_DT, "value": cells * nsteps / secs, "unit": UNIT, "seconds": secs,
            "clock": "host wall clock around pvof_run_steps_batched, max over ranks",
-           "form": "fp32 stencils + same-stage pressure warm start, Jacobi-PCG pressure (FP64)",
+           "form": "all four forms: fp32 stencils, same-stage pressure warm start, spectral pressure "
+                   "preconditioner, unregularised momentum CG (solves and reductions in FP64)",
            "sharding": "%d rank(s), cases split by cell count" % ws,
            "graph_replayed_substeps": sum(v["graph_replays"] for v in merged.values()),
            "substeps": sum(v["substeps"] for v in merged.values()),
@@ -645,8 +656,9 @@ def droplet_batch(args, dist, device, ws, rank):
         for q in small:
             st = {}
             for fp32 in (0, 1):
-                g, p, pl, parts = cases.droplet_batch(args.droplets, seed=args.droplet_seed,
-                                                      **dict(kw, stencil_fp32=fp32, pressure_warm_start=fp32))[q]
+                forms = dict(stencil_fp32=fp32, pressure_warm_start=fp32, pressure_preconditioner=fp32,
+                             velocity_cg_unregularized=fp32)
+                g, p, pl, parts = cases.droplet_batch(args.droplets, seed=args.droplet_seed, **dict(kw, **forms))[q]
                 s = start((g, p, pl, parts))
                 s.run_steps(max(1, args.droplet_warmup) + nsteps, DROP_DT)
                 st[fp32] = ({f: s.get(f) for f in ("U", "V")}, s.liquid_mass())
@@ -1028,6 +1040,7 @@ def main():
                     help="also time eight cases of four sizes (64x128 .. 512x1024) in all forms, batched")
     ap.add_argument("--large", action="store_true",
                     help="also time 1024x1024 at density ratio 1e-3 (plain, spectral, spectral + momentum form)")
+    ap.add_argument("--axisym-warmup", type=int, default=6)
     ap.add_argument("--large-steps", type=int, default=3)
     ap.add_argument("--large-forms", default="plain,spectral,spectral-unreg",
                     help="comma-separated forms of --large: plain, spectral, spectral-unreg")

@@ -456,7 +456,7 @@ int pvof_set_cluster_solvers(pvof_ctx *ctx, int enabled);
  * a_0, rows 2K .. 2K + 3 the Thomas pivot and c' of the reduced system's
  * equations 2l and 2l + 1.  Returns the number of doubles, (N/2 + 1)(2K + 4)
  * 32, and writes them to out when cap is at least that; -1 on invalid sizes
- * (N a power of two >= 2, M >= 2). */
+ * (N = 2^a, 3 2^a or 5 2^a and even, M >= 2). */
 long long pvof_spectral_tables(int N, int M, double idx2, double idy2, double *out, long long cap);
 int pvof_solver_timing(const pvof_ctx *ctx, int solver, double *ms, long long *launches, long long *iterations,
                        long long *cell_iters);

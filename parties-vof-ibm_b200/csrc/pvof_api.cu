@@ -918,8 +918,10 @@ int p_solve_spectral(pvof_ctx *c)
         A.sm = A.cy + c->plane_elems;
     }
     A.N = N;
+    A.R = N % 3 == 0 ? 3 : (N % 5 == 0 ? 5 : 1);
+    A.n = N / A.R;
     A.logN = 0;
-    while ((1 << A.logN) < N) A.logN++;
+    while ((1 << A.logN) < A.n) A.logN++;
     A.M = M;
     A.fscale = c->spec_fscale;
     A.tol = c->p.P_CG_ETOL;
@@ -1744,9 +1746,11 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
         const int N = grid->NXM, M = grid->NYM;
         if (grid->geometry != PVOF_GEOM_PLANAR || !grid->periodic[0] || grid->periodic[1])
             return set_err(PVOF_EINVAL, "the spectral pressure preconditioner needs a planar grid, x periodic, walls in y");
-        if ((N & (N - 1)) != 0 || N > 1024 || M > 1024)
-            return set_err(PVOF_EINVAL, "the spectral pressure preconditioner needs a power-of-two x cell count up to 1024 "
-                                        "and at most 1024 y cells");
+        int odd = N;
+        while (odd % 2 == 0 && odd > 1) odd /= 2;
+        if (N < 2 || N % 2 != 0 || (odd != 1 && odd != 3 && odd != 5) || N > 1024 || M < 2 || M > 1024)
+            return set_err(PVOF_EINVAL, "the spectral pressure preconditioner needs an x cell count of 2^a, 3 2^a or "
+                                        "5 2^a up to 1024 and 2 to 1024 y cells");
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(PVOF_ENODEV, "no CUDA device");
@@ -2209,8 +2213,10 @@ int pvof_set_cluster_solvers(pvof_ctx *c, int enabled)
 
 long long pvof_spectral_tables(int N, int M, double idx2, double idy2, double *out, long long cap)
 {
-    if (N < 2 || (N & (N - 1)) != 0 || M < 2 || !(idx2 > 0.0) || !(idy2 > 0.0)) {
-        set_err(PVOF_EINVAL, "pvof_spectral_tables: N a power of two >= 2, M >= 2, positive spacings");
+    int odd = N;
+    while (odd % 2 == 0 && odd > 1) odd /= 2;
+    if (N < 2 || N % 2 != 0 || (odd != 1 && odd != 3 && odd != 5) || M < 2 || !(idx2 > 0.0) || !(idy2 > 0.0)) {
+        set_err(PVOF_EINVAL, "pvof_spectral_tables: N = 2^a, 3 2^a or 5 2^a (even), M >= 2, positive spacings");
         return -1;
     }
     std::vector<double> tw, tri;

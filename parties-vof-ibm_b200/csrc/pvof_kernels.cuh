@@ -64,7 +64,8 @@ struct SpecArgs {
     const double2 *tw;        // exp(-2 pi i k / N), k < N / 2
     const double *tri;        // the tridiagonal phase's coefficients, one set per wave number (spec_tables)
     double *cx, *cy, *sm;     // per solve: x and y face coefficients of the operator, sqrt of the Jacobi weights
-    int N, logN, M;           // x cells (a power of two), log2 N, y cells
+    int N, logN, M;           // x cells (R n), log2 n, y cells
+    int R, n;                 // N = R n: R = 1, 3 or 5, n a power of two
     double fscale;            // dy^2 / N
     double tol;
     int maxit;

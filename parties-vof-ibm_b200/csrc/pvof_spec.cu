@@ -164,12 +164,19 @@ __device__ double slot_total(const double *slot, double *sh)
     return r;
 }
 
-// complex FFT of a[0..N), N = 2^logN, by the 128 threads of one row group
-// (lt = 0..127); sign -1 forward.  All groups of the block run it in lockstep.
-// Radix-2 decimation in time after a bit reversal; two successive stages are
-// done per pass through shared memory (each thread keeps the four values of
-// both stages' butterflies in registers, the arithmetic is that of the two
-// radix-2 stages), a last odd stage on its own.
+// Complex FFTs of rows of N = R n points (R = 1, 3 or 5, n = 2^logn) by the
+// ROW_THREADS threads of one row group (lt = their index); sign -1 forward.
+// All groups of the block run them in lockstep.  The row is stored
+// decimated by R (point i at (i mod R) n + i / R, row_slot): the R
+// interleaved subsequences are transformed as R rows of n points (radix-2
+// decimation in time after a bit reversal, two stages per pass through
+// shared memory with the four values of both stages' butterflies in
+// registers, a last odd stage on its own), then one radix-R pass combines
+// them in place into the N-point transform in natural order (the R outputs
+// k, k + n, .. of one column come from the column's R inputs).  Twiddles
+// come from the N-point table exp(-2 pi i k / N), k < N/2 (the other half by
+// symmetry); a subsequence's twiddle exp(-2 pi i e / n) is the table's
+// entry e R.
 __device__ __forceinline__ double2 cmul(double2 v, double2 w)
 {
     return make_double2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
@@ -182,41 +189,72 @@ __device__ __forceinline__ double2 twid(const double2 *__restrict__ tw, int k, d
     return w;
 }
 
-__device__ void fft_group(double2 *a, int N, int logN, const double2 *__restrict__ tw, double sign, int lt)
+// exp(sign 2 pi i k / N) for any k >= 0
+__device__ __forceinline__ double2 twid_full(const double2 *__restrict__ tw, int k, int N, double sign)
 {
-    for (int t = lt; t < N; t += ROW_THREADS) {
-        const int r = (int)(__brev((unsigned)t) >> (32 - logN));
-        if (r > t) { const double2 x = a[t]; a[t] = a[r]; a[r] = x; }
+    k %= N;
+    double2 w = k < N / 2 ? tw[k] : make_double2(-tw[k - N / 2].x, -tw[k - N / 2].y);
+    w.y *= -sign;
+    return w;
+}
+
+// where point i of a row goes before the transform
+__device__ __forceinline__ int row_slot(const SpecArgs &A, int i) { return A.R == 1 ? i : (i % A.R) * A.n + i / A.R; }
+
+__device__ void fft_rows(double2 *a, int N, int n, int logn, int R, const double2 *__restrict__ tw, double sign, int lt)
+{
+    for (int t = lt; t < R * n; t += ROW_THREADS) {
+        const int c = t / n, u = t - c * n, r = (int)(__brev((unsigned)u) >> (32 - logn));
+        if (r > u) { const double2 x = a[c * n + u]; a[c * n + u] = a[c * n + r]; a[c * n + r] = x; }
     }
     __syncthreads();
     int s = 0;
-    for (; s + 1 < logN; s += 2) {   // stages s and s + 1
+    for (; s + 1 < logn; s += 2) {   // stages s and s + 1
         const int h = 1 << s;
-        for (int t = lt; t < N / 4; t += ROW_THREADS) {
-            const int pos = t & (h - 1), i0 = ((t >> s) << (s + 2)) + pos, i1 = i0 + h, i2 = i1 + h, i3 = i2 + h;
+        for (int t = lt; t < R * (n / 4); t += ROW_THREADS) {
+            const int c = t / (n / 4), tt = t - c * (n / 4);
+            double2 *b = a + c * n;
+            const int pos = tt & (h - 1), i0 = ((tt >> s) << (s + 2)) + pos, i1 = i0 + h, i2 = i1 + h, i3 = i2 + h;
             const double2 w1 = twid(tw, pos * (N >> (s + 1)), sign);
             const double2 w2 = twid(tw, pos * (N >> (s + 2)), sign), w3 = twid(tw, (pos + h) * (N >> (s + 2)), sign);
-            const double2 x0 = a[i0], x1 = a[i1], x2 = a[i2], x3 = a[i3];
+            const double2 x0 = b[i0], x1 = b[i1], x2 = b[i2], x3 = b[i3];
             double2 x = cmul(x1, w1);
             const double2 y0 = make_double2(x0.x + x.x, x0.y + x.y), y1 = make_double2(x0.x - x.x, x0.y - x.y);
             x = cmul(x3, w1);
             const double2 y2 = make_double2(x2.x + x.x, x2.y + x.y), y3 = make_double2(x2.x - x.x, x2.y - x.y);
             x = cmul(y2, w2);
-            a[i0] = make_double2(y0.x + x.x, y0.y + x.y);
-            a[i2] = make_double2(y0.x - x.x, y0.y - x.y);
+            b[i0] = make_double2(y0.x + x.x, y0.y + x.y);
+            b[i2] = make_double2(y0.x - x.x, y0.y - x.y);
             x = cmul(y3, w3);
-            a[i1] = make_double2(y1.x + x.x, y1.y + x.y);
-            a[i3] = make_double2(y1.x - x.x, y1.y - x.y);
+            b[i1] = make_double2(y1.x + x.x, y1.y + x.y);
+            b[i3] = make_double2(y1.x - x.x, y1.y - x.y);
         }
         __syncthreads();
     }
-    if (s < logN) {   // the last stage when log2 N is odd
+    if (s < logn) {   // the last stage when log2 n is odd
         const int half = 1 << s, step = N >> (s + 1);
-        for (int t = lt; t < N / 2; t += ROW_THREADS) {
-            const int pos = t & (half - 1), i0 = ((t >> s) << (s + 1)) + pos, i1 = i0 + half;
-            const double2 u = a[i0], x = cmul(a[i1], twid(tw, pos * step, sign));
-            a[i0] = make_double2(u.x + x.x, u.y + x.y);
-            a[i1] = make_double2(u.x - x.x, u.y - x.y);
+        for (int t = lt; t < R * (n / 2); t += ROW_THREADS) {
+            const int c = t / (n / 2), tt = t - c * (n / 2);
+            double2 *b = a + c * n;
+            const int pos = tt & (half - 1), i0 = ((tt >> s) << (s + 1)) + pos, i1 = i0 + half;
+            const double2 u = b[i0], x = cmul(b[i1], twid(tw, pos * step, sign));
+            b[i0] = make_double2(u.x + x.x, u.y + x.y);
+            b[i1] = make_double2(u.x - x.x, u.y - x.y);
+        }
+        __syncthreads();
+    }
+    if (R > 1) {   // X[k + t n] = sum_r exp(sign 2 pi i r (k + t n) / N) F_r[k]
+        for (int k = lt; k < n; k += ROW_THREADS) {
+            double2 f[5];   // (local memory: only the R > 1 rows pass here)
+            for (int r = 0; r < R; r++) f[r] = r == 0 ? a[k] : cmul(a[r * n + k], twid_full(tw, r * k, N, sign));
+            for (int t = 0; t < R; t++) {
+                double2 x = f[0];
+                for (int r = 1; r < R; r++) {
+                    const double2 y = cmul(f[r], twid_full(tw, r * t * n, N, sign));
+                    x = make_double2(x.x + y.x, x.y + y.y);
+                }
+                a[t * n + k] = x;
+            }
         }
         __syncthreads();
     }
@@ -232,10 +270,10 @@ __device__ void pair_forward(const SpecArgs &A, double2 *a, int ja, bool acta, b
     const int P = A.d.P, N = A.N, jb = ja + 1;
     const double sc = 0.5 * A.fscale;
     __syncthreads();
-    fft_group(a, N, A.logN, A.tw, -1.0, lt);
+    fft_rows(a, N, A.n, A.logN, A.R, A.tw, -1.0, lt);
     if (acta)
         for (int k = lt; k <= N / 2; k += ROW_THREADS) {
-            const double2 zk = a[k], zn = a[(N - k) & (N - 1)];
+            const double2 zk = a[k], zn = a[k == 0 ? 0 : N - k];
             AT_(A.hat, k, ja) = (zk.x + zn.x) * sc;
             if (actb) AT_(A.hat, k, jb) = (zk.y + zn.y) * sc;
             if (k > 0 && k < N / 2) {
@@ -507,7 +545,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
         if (acta)
             for (int i = lt; i < N; i += ROW_THREADS) {
                 const double va = residual(i, ja, sJ);
-                row[i] = make_double2(va, actb ? residual(i, jb, sJ) : 0.0);
+                row[row_slot(A, i)] = make_double2(va, actb ? residual(i, jb, sJ) : 0.0);
             }
         pair_forward(B, row, ja, acta, actb, lt);
     }
@@ -534,10 +572,10 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
                 for (int k = lt; k < N; k += ROW_THREADS) {
                     const double2 xa = half_complex(A, k, ja);
                     const double2 xb = actb ? half_complex(A, k, jb) : make_double2(0.0, 0.0);
-                    row[k] = make_double2(xa.x - xb.y, xa.y + xb.x);   // X_a + i X_b
+                    row[row_slot(A, k)] = make_double2(xa.x - xb.y, xa.y + xb.x);   // X_a + i X_b
                 }
             __syncthreads();
-            fft_group(row, N, A.logN, tw, 1.0, lt);
+            fft_rows(row, N, A.n, A.logN, A.R, tw, 1.0, lt);
             if (acta)
                 for (int i = lt; i < N; i += ROW_THREADS) {
                     const double2 v = row[i];
@@ -600,7 +638,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
             if (acta)
                 for (int i = lt; i < N; i += ROW_THREADS) {
                     const double va = update(i, ja, sJ);
-                    row[i] = make_double2(va, actb ? update(i, jb, sJ) : 0.0);
+                    row[row_slot(A, i)] = make_double2(va, actb ? update(i, jb, sJ) : 0.0);
                 }
             pair_forward(B, row, ja, acta, actb, lt);
         }
@@ -640,7 +678,12 @@ bool spec_supported(const Dom &d, const char **why)
     const int N = d.NX - 1, M = d.NY - 1;
     if (!d.planar || d.axisym) { *why = "the spectral pressure preconditioner is built for the planar mode only"; return false; }
     if (!d.perx || d.pery) { *why = "the spectral pressure preconditioner needs x periodic and walls in y"; return false; }
-    if (N < 2 || (N & (N - 1)) != 0 || N > 1024) { *why = "the spectral pressure preconditioner needs a power-of-two x cell count (2..1024)"; return false; }
+    int n = N;
+    while (n % 2 == 0 && n > 1) n /= 2;   // the odd factor
+    if (N < 2 || N > 1024 || N % 2 != 0 || (n != 1 && n != 3 && n != 5) || N / n < 2) {
+        *why = "the spectral pressure preconditioner needs an x cell count of 2^a, 3 2^a or 5 2^a (2..1024)";
+        return false;
+    }
     if (M < 2 || M > 1024) { *why = "the spectral pressure preconditioner needs 2 to 1024 y cells"; return false; }
     return true;
 }

@@ -273,17 +273,33 @@ def droplet_on_cylinder(NXM=128, Rd=0.5, Rs=0.3, theta=90.0, Cn=0.01, rho_ratio=
     return grid, params, {"F": C, "U": z, "V": z.copy(), "P": z.copy()}, [(0, xs, ys, Rs, 0.0, 0.0, 0.0, 1.0)]
 
 
+def smooth_widths(lo, hi):
+    """x cell counts in [lo, hi] of the form 2^a, 3 2^a or 5 2^a (the widths
+    the spectral pressure preconditioner's row transforms take)."""
+    out = set()
+    for r in (1, 3, 5):
+        w = r * 2
+        while w <= hi:
+            if w >= lo:
+                out.add(w)
+            w *= 2
+    return sorted(out)
+
+
 def droplet_batch(n=64, seed=0, nxm_min=64, nxm_max=512, **kw):
     """The batching form's cases: n sessile droplets on static cylinders
-    (droplet_on_cylinder) with NXM log-uniform in [nxm_min, nxm_max] (a
-    multiple of 8, NYM = 2 NXM), droplet radius U(0.3, 0.6), cylinder radius
-    U(0.2, 0.4), contact angle U(30, 150) degrees, all seeded.  Returns a list
-    of (grid, params, planes, particles)."""
+    (droplet_on_cylinder) with NXM drawn log-uniformly in [nxm_min, nxm_max]
+    and taken to the nearest (in log) of smooth_widths (64, 80, 96, 128, 160,
+    192, 256, 320, 384, 512 for the default range; NYM = 2 NXM), droplet
+    radius U(0.3, 0.6), cylinder radius U(0.2, 0.4), contact angle
+    U(30, 150) degrees, all seeded.  Returns a list of (grid, params, planes,
+    particles)."""
     rng = np.random.default_rng(seed)
+    widths = smooth_widths(nxm_min, nxm_max)
     out = []
     for _ in range(n):
-        nxm = int(round(math.exp(rng.uniform(math.log(nxm_min), math.log(nxm_max))) / 8.0)) * 8
-        nxm = min(max(nxm, nxm_min), nxm_max)
+        x = rng.uniform(math.log(nxm_min), math.log(nxm_max))
+        nxm = min(widths, key=lambda w: (abs(math.log(w) - x), w))
         Rd, Rs, th = rng.uniform(0.3, 0.6), rng.uniform(0.2, 0.4), rng.uniform(30.0, 150.0)
         out.append(droplet_on_cylinder(nxm, Rd=Rd, Rs=Rs, theta=th, **kw))
     return out

@@ -79,6 +79,9 @@ CASES = [
 LONG_CASES = [
     ("rt128x512_100steps", "rt2d", dict(NXM=128, NYM=512, Lx=1.0, Ly=4.0, Cn=0.01, **dict(TIGHT, P_CG_MAXIT=4000)),
      100, 1e-4),
+    # the axisymmetric bubble with surface tension, 100 steps
+    ("axi_st_100steps", "axi2d_st", dict(_builder="rising_bubble", NXM=32, NYM=64, rmax=1.0, zmax=2.0, radius=0.3,
+                                         zc=0.7, Cn=0.04, surface_tension=True, We=200.0, **AXI_TIGHT), 100, 1e-3),
 ]
 
 # resolved-particle routine cases (oracle/ref/ibm_driver.c on the ibm2d build):

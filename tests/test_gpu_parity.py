@@ -219,6 +219,28 @@ def test_hundred_steps_128x512_against_reference():
     assert all(r <= 1e-10 for r in worst.values()), worst
 
 
+def test_hundred_steps_axisym_against_reference():
+    """The axisymmetric rising bubble with surface tension (32x64, density
+    ratio 0.1, We 200), 100 RK3 steps at dt 1e-3, solver tolerances near
+    machine precision (pressure 1e-12, above the axisymmetric rounding
+    floor): C_L, u, v and p on the physical cells within 1e-10 relative L2 of
+    the reference's own time step (fixture axi_st_100steps, written by the
+    axi2d_st reference build)."""
+    from pvof import cases
+    grid, params, _, d, meta = load_golden("axi_st_100steps")
+    build = {k: v for k, v in meta["builder"].items() if k != "_builder"}
+    _, _, planes = cases.rising_bubble(**build)
+    g = solver_for(grid, params, planes)
+    g.run_steps(meta["steps"], meta["dt"])
+    NX, NY, _ = cases.dims(grid)
+    worst = {}
+    for f in ("C_L", "U", "V", "P"):
+        a = g_range(grid, g.get(f))[:NY - 1, :NX - 1]
+        worst[f] = rel_l2(a, d["s%d/%s" % (meta["steps"], f)])
+    print(worst)
+    assert all(r <= 1e-10 for r in worst.values()), worst
+
+
 def test_liquid_mass_conserved():
     """Sum of C_L over the physical cells stays at its initial value to 1e-13
     (relative) when the solves are converged and no clamp event happens; the

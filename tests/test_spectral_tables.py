@@ -84,6 +84,7 @@ def matrix(N, M, w, idx2, idy2):
 
 
 @pytest.mark.parametrize("N,M,idx2,idy2", [(8, 5, 64.0, 64.0), (16, 16, 256.0, 64.0), (4, 33, 16.0, 100.0),
+                                          (12, 40, 1.0, 1.0), (80, 160, 1.0, 1.0),
                                           (32, 2, 1024.0, 1024.0), (8, 3, 1.0, 1.0), (16, 1000, 1.0, 4.0),
                                           (8, 1023, 1.0, 1.0), (1024, 1024, 1.0, 1.0)])
 def test_tables_solve_every_wave_number(N, M, idx2, idy2):
@@ -118,6 +119,7 @@ def test_invalid_sizes_are_refused():
     L = load()
     L.pvof_spectral_tables.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double), C.c_longlong]
     L.pvof_spectral_tables.restype = C.c_longlong
-    assert L.pvof_spectral_tables(12, 8, 1.0, 1.0, None, 0) == -1
+    assert L.pvof_spectral_tables(14, 8, 1.0, 1.0, None, 0) == -1   # 7 x 2: not 2^a, 3 2^a or 5 2^a
+    assert L.pvof_spectral_tables(15, 8, 1.0, 1.0, None, 0) == -1   # odd
     assert L.pvof_spectral_tables(8, 0, 1.0, 1.0, None, 0) == -1
     assert L.pvof_spectral_tables(8, 1, 1.0, 1.0, None, 0) == -1
