@@ -597,8 +597,9 @@ def droplet_batch(args, dist, device, ws, rank):
         s.initialize()
         return s
 
-    def run_batch(idx):
-        solvers = [start(allc[q]) for q in idx]
+    def run_batch(idx, cases_=None):
+        cases_ = allc if cases_ is None else cases_
+        solvers = [start(cases_[q]) for q in idx]
         # stencil tiles: each case tuned alone on the GPU (launch times taken
         # while other cases run would include their waits), a few steps each
         for s in solvers:
@@ -631,6 +632,12 @@ def droplet_batch(args, dist, device, ws, rank):
 
     merged, shard, secs = pdist.run_sharded_batch(dist, costs, run_batch, device="cuda")
     cells = int(sum(costs))
+    plain = None
+    if args.droplet_plain:   # the same cases in the plain FP64 path (no form), timed the same way
+        plain_cases = cases.droplet_batch(args.droplets, seed=args.droplet_seed, P_CG_MAXIT=20000)
+        _, _, psecs = pdist.run_sharded_batch(dist, costs, lambda idx: run_batch(idx, plain_cases), device="cuda")
+        plain = {"value": cells * nsteps / psecs, "seconds": psecs,
+                 "form": "plain FP64 (the reference's solvers), same tuning, warm-up and graph replay"}
     out = {"cases": len(allc), "cells": cells, "steps": nsteps, "warmup_steps": max(1, args.droplet_warmup),
            "dt": DROP_DT, "value": cells * nsteps / secs, "unit": UNIT, "seconds": secs,
            "clock": "host wall clock around pvof_run_steps_batched, max over ranks",
@@ -650,6 +657,9 @@ def droplet_batch(args, dist, device, ws, rank):
                                 "at the default 32x8]",
                         "smallest_case": merged[min(merged, key=lambda q: (costs[q], q))]["tiles"],
                         "largest_case": merged[max(merged, key=lambda q: (costs[q], q))]["tiles"]}}
+    if plain is not None:
+        out["plain"] = plain
+        out["vs_plain"] = out["value"] / plain["value"]
     if rank == 0:
         small = sorted(range(len(allc)), key=lambda q: (costs[q], q))[:2]
         errs = []
@@ -830,6 +840,11 @@ def run_ours(args):
     for _ in range(args.warmup):
         g.run_steps(1, DT)
     g.synchronize()
+    # the state at the start of the timed steps: the end-to-end pass below
+    # replays the same steps from it, through host buffers
+    start_blocks = {f: pinned_like(g.block_count(f)) for f in STATE_FIELDS}
+    for f in STATE_FIELDS:
+        g.download(f, out=start_blocks[f])
 
     # ---- device-resident timing (substeps replayed from CUDA graphs) --------
     clocks = Clocks(local)
@@ -858,10 +873,10 @@ def run_ours(args):
     mass_report = {"clamp_mass_timed_steps": g.clamp_mass_total() - clamp0, "liquid_mass_change": m64 - mass0,
                    "liquid_mass": mass0}
 
-    # ---- end to end through the C ABI with host buffers ---------------------
-    blocks = {f: pinned_like(g.block_count(f)) for f in STATE_FIELDS}
-    for f in STATE_FIELDS:
-        g.download(f, out=blocks[f])
+    # ---- end to end through the C ABI with host buffers: the timed steps
+    # again, from the state they started from (same iterations, same work),
+    # the state uploaded before and downloaded after every step ----------------
+    blocks = start_blocks
     h2d = d2h = 0
     NX, NY, NZ = cases.dims(grid)
     plane_flow = (NX + 6) * (NY + 6) * 8
@@ -870,7 +885,7 @@ def run_ours(args):
         ng = abi.FIELD[f] in abi.NG_FIELDS
         h2d += plane_ng if ng else plane_flow
         d2h += (plane_ng if ng else plane_flow) * NZ
-    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    e2e_steps = max(1, min(args.steps, args.e2e_steps or args.steps))
     barrier(dist)
     e2e_ms = 0.0
     g.synchronize()
@@ -1016,7 +1031,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end pass (0: --steps, the same steps)")
     ap.add_argument("--cpu-steps", type=int, default=5)
     ap.add_argument("--ref-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1034,6 +1049,8 @@ def main():
                          "from the third time its launches recur (stage x surface-tension buffer parity x warm "
                          "start: about six steps)")
     ap.add_argument("--droplet-seed", type=int, default=0)
+    ap.add_argument("--no-droplet-plain", dest="droplet_plain", action="store_false",
+                    help="skip timing the droplet cases in the plain FP64 path")
     ap.add_argument("--droplet-ref-steps", type=int, default=1,
                     help="steps of the reference build on the smallest droplet case (0: off)")
     ap.add_argument("--batch-mixed", action="store_true",

@@ -1909,6 +1909,7 @@ int pvof_destroy(pvof_ctx *c)
     if (c->scal) cudaFree(c->scal);
     if (c->scal_host) cudaFreeHost(c->scal_host);
     if (c->flush_buf) cudaFree(c->flush_buf);
+    if (c->host_stage) cudaFree(c->host_stage);
     for (int q = 0; q < 2; q++) if (c->timer_ev[q]) cudaEventDestroy(c->timer_ev[q]);
     for (int q = 0; q < Ctx::NPEND; q++)
         for (int e = 0; e < 2; e++) if (c->pend_ev[q][e]) cudaEventDestroy(c->pend_ev[q][e]);
@@ -1932,22 +1933,38 @@ size_t pvof_field_block_count(const pvof_ctx *c, int field)
     return (NX + 2 * NG) * (NY + 2 * NG) * (NZ + 2 * NG);
 }
 
+// the device staging block of the host copies (one field's plane, grown on demand)
+static int host_stage(pvof_ctx *c, size_t elems)
+{
+    if (c->host_stage_elems >= elems) return PVOF_OK;
+    CK(cudaStreamSynchronize(c->stream));   // the old block may be in use
+    cudaFree(c->host_stage);
+    c->host_stage = nullptr;
+    c->host_stage_elems = 0;
+    if (cudaMalloc(&c->host_stage, elems * sizeof(double)) != cudaSuccess)
+        return set_err(PVOF_ENOMEM, "cudaMalloc host staging block");
+    c->host_stage_elems = elems;
+    return PVOF_OK;
+}
+
+// One field between its host block (the reference's layout) and the device
+// plane: one contiguous copy of the k = 0 plane (the 2D modes keep the k
+// planes identical) through a staging block, the row pitch done by a kernel
+// (a pitched 2D copy moves each short row as its own transfer).
 int pvof_upload_field(pvof_ctx *c, int field, const double *host, size_t count)
 {
     if (!c || !host) return set_err(PVOF_EINVAL, "null argument");
     if (count != pvof_field_block_count(c, field)) return set_err(PVOF_EINVAL, "block size does not match the field");
     CK(cudaSetDevice(c->device));
     const size_t NX = (size_t)c->dom.NX, NY = (size_t)c->dom.NY;
-    if (is_ng(field)) {
-        // k = 0 plane of the G range -> device rows 0..NY-1, columns 0..NX-1
-        CK(cudaMemcpy2DAsync(c->f[field], (size_t)c->dom.P * sizeof(double), host, NX * sizeof(double),
-                             NX * sizeof(double), NY, cudaMemcpyHostToDevice, c->stream));
-    } else {
-        const size_t SX = NX + 2 * NG, SY = NY + 2 * NG;
-        const double *plane = host + (size_t)NG * SX * SY;  // k = 0
-        CK(cudaMemcpy2DAsync(c->f[field] - (ptrdiff_t)NG * c->dom.P - NG, (size_t)c->dom.P * sizeof(double), plane,
-                             SX * sizeof(double), SX * sizeof(double), SY, cudaMemcpyHostToDevice, c->stream));
-    }
+    const bool ng = is_ng(field);
+    const size_t W = ng ? NX : NX + 2 * NG, H = ng ? NY : NY + 2 * NG;
+    const double *plane = ng ? host : host + (size_t)NG * W * H;   // k = 0
+    double *dst = ng ? c->f[field] : c->f[field] - (ptrdiff_t)NG * c->dom.P - NG;
+    TRY(host_stage(c, W * H));
+    CK(cudaMemcpyAsync(c->host_stage, plane, W * H * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    k_unpack_rows<<<(unsigned)((W * H + 255) / 256), 256, 0, c->stream>>>(dst, c->dom.P, c->host_stage, (int)W, (int)H);
+    CKL(c);
     return PVOF_OK;
 }
 
@@ -1957,17 +1974,15 @@ int pvof_download_field(pvof_ctx *c, int field, double *host, size_t count)
     if (count != pvof_field_block_count(c, field)) return set_err(PVOF_EINVAL, "block size does not match the field");
     CK(cudaSetDevice(c->device));
     const size_t NX = (size_t)c->dom.NX, NY = (size_t)c->dom.NY, NZ = (size_t)c->g.NZM + 1;
-    if (is_ng(field)) {
-        for (size_t k = 0; k < NZ; k++)
-            CK(cudaMemcpy2DAsync(host + k * NX * NY, NX * sizeof(double), c->f[field], (size_t)c->dom.P * sizeof(double),
-                                 NX * sizeof(double), NY, cudaMemcpyDeviceToHost, c->stream));
-    } else {
-        const size_t SX = NX + 2 * NG, SY = NY + 2 * NG;
-        for (size_t k = 0; k < NZ; k++)
-            CK(cudaMemcpy2DAsync(host + (NG + k) * SX * SY, SX * sizeof(double), c->f[field] - (ptrdiff_t)NG * c->dom.P - NG,
-                                 (size_t)c->dom.P * sizeof(double), SX * sizeof(double), SY, cudaMemcpyDeviceToHost,
-                                 c->stream));
-    }
+    const bool ng = is_ng(field);
+    const size_t W = ng ? NX : NX + 2 * NG, H = ng ? NY : NY + 2 * NG;
+    const double *src = ng ? c->f[field] : c->f[field] - (ptrdiff_t)NG * c->dom.P - NG;
+    TRY(host_stage(c, W * H));
+    k_pack_rows<<<(unsigned)((W * H + 255) / 256), 256, 0, c->stream>>>(c->host_stage, src, c->dom.P, (int)W, (int)H);
+    CKL(c);
+    for (size_t k = 0; k < NZ; k++)
+        CK(cudaMemcpyAsync(host + (ng ? k : NG + k) * W * H, c->host_stage, W * H * sizeof(double),
+                           cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return PVOF_OK;
 }

@@ -173,6 +173,8 @@ struct Ctx {
     // measurement
     cudaEvent_t timer_ev[2];
     double *flush_buf;
+    double *host_stage;      // contiguous staging of one field block for the host copies
+    size_t host_stage_elems;
     size_t flush_bytes;
     int solver_timing;
     static constexpr int NPEND = 16;

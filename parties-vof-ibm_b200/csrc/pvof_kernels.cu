@@ -239,6 +239,25 @@ __global__ void k_phase_cache(size_t n, const double *__restrict__ CL, const dou
     F[q] = CL[q];
 }
 
+// a W x H block between a contiguous buffer (row stride W) and a pitched
+// plane (row stride P): the host copies move one contiguous block, these
+// kernels do the strides on the device
+__global__ void k_unpack_rows(double *__restrict__ dst, int P, const double *__restrict__ src, int W, int H)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (size_t)W * H) return;
+    const int j = (int)(q / W), i = (int)(q - (size_t)j * W);
+    dst[(size_t)j * P + i] = src[q];
+}
+
+__global__ void k_pack_rows(double *__restrict__ dst, const double *__restrict__ src, int P, int W, int H)
+{
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (size_t)W * H) return;
+    const int j = (int)(q / W), i = (int)(q - (size_t)j * W);
+    dst[q] = src[(size_t)j * P + i];
+}
+
 // C_L = clamp01(F) over the L ranges (VOF_DIFFUSE.c:532-538)
 __global__ void k_clamp_from(size_t n, const double *__restrict__ F, double *__restrict__ CL)
 {

@@ -74,6 +74,9 @@ struct SpecArgs {
     DevScalars *scal;
 };
 
+__global__ void k_unpack_rows(double *dst, int P, const double *src, int W, int H);
+__global__ void k_pack_rows(double *dst, const double *src, int P, int W, int H);
+
 // raise a kernel's dynamic shared memory limit to at least bytes (never lower it)
 bool raise_dynamic_smem(const void *fn, size_t bytes);
 
