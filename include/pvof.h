@@ -266,11 +266,16 @@ int pvof_run_steps_batched(pvof_ctx *const *ctxs, int n, int nsteps, double dt, 
  * VOF_DIFFUSE.c:1071-1091), computed on the device in FP64. */
 int pvof_liquid_mass(pvof_ctx *ctx, double *mass);
 
-/* --- resolved solid particles (planar mode) ------------------------------
+/* --- resolved solid particles (planar cylinders, axisymmetric spheres) ----
  * The reference keeps particles in two linked lists (p_mobile, p_fixed,
  * PARTIES/src/Include/DataTypes.h:1327-1527) read from p_mobile.inp /
  * p_fixed.inp.  Here the caller passes the owned particles once; the library
- * derives markers, masses and the periodic copies itself. */
+ * derives markers, masses and the periodic copies itself and keeps the lists
+ * in device memory: the list updates, markers, flags and the rigid-body
+ * motion run on the device, so the calls below enqueue work without waiting
+ * for it, except those that return particle data (pvof_particle_entries,
+ * _forces, _markers, pvof_get_particles), which read the device state back,
+ * and pvof_Lagrangian_advect_particles, which reads its error state. */
 typedef struct pvof_particle {
     int mobile;         /* 1: mobile list, 0: fixed list */
     double X[2];        /* centre (x, y) */
@@ -281,7 +286,9 @@ typedef struct pvof_particle {
 } pvof_particle;
 
 /* Replaces the particle lists; IDs as Particle_initialize assigns them (fixed
- * first, then mobile; Lagrangian/Particle.c:213-221). */
+ * first, then mobile; Lagrangian/Particle.c:213-221).  Sizes the device lists
+ * (at most nine entries per particle: two periodic copies per periodic axis)
+ * and drops the context's captured substep graphs. */
 int pvof_set_particles(pvof_ctx *ctx, const pvof_particle *particles, int n);
 /* Particle_MPI_update of both lists on one rank (periodic copies) and
  * Lagrangian_flag_points (Lagrangian/Lagrangian.c:2515-2627): markers of
