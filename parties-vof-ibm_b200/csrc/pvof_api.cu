@@ -273,7 +273,6 @@ const TuneRec *tunable(const void *fn)
             t.push_back(r);
         };
 #define PVOF_TUNABLE(k) add((const void *)k, #k)
-        PVOF_TUNABLE(k_weno_flux); PVOF_TUNABLE(k_weno_flux_f); PVOF_TUNABLE(k_flux_div);
         PVOF_TUNABLE(k_laplacian); PVOF_TUNABLE(k_laplacian_f); PVOF_TUNABLE(k_bulk_S); PVOF_TUNABLE(k_bulk_S_f);
         PVOF_TUNABLE(k_psi_LG); PVOF_TUNABLE(k_psi_LG_f); PVOF_TUNABLE(k_f_sigma); PVOF_TUNABLE(k_f_sigma_f);
         PVOF_TUNABLE(k_u_impexp); PVOF_TUNABLE(k_v_impexp); PVOF_TUNABLE(k_set_rhs); PVOF_TUNABLE(k_rhs_vec);
@@ -471,20 +470,19 @@ int compute_laplacian(pvof_ctx *c, double *in, double *out, bool fp32 = false)
     return fill(c, BK_SCALAR, out);
 }
 
+// VOF_DIFFUSE_advect_WENO5 (VOF_DIFFUSE.c:931-996): the face fluxes, their
+// ghost update and the divergence in one TMA-tiled kernel (pvof_advect.cu)
 int advect(pvof_ctx *c, double *out)
 {
-    const int NX = c->dom.NX, NY = c->dom.NY;
     double *CL = F(c, PVOF_F_C_L);
     TRY(fill(c, BK_SCALAR, CL));
-    if (fp32_stencils(c))
-        TRY(launch2d(c, k_weno_flux_f, 0, NX, 0, NY, (const double *)CL, (const double *)F(c, PVOF_F_U),
-                     (const double *)F(c, PVOF_F_V), S(c, SC_FLUX_X), S(c, SC_FLUX_Y), c->p.weno_order == 5 ? 1 : 0));
-    else
-        TRY(launch2d(c, k_weno_flux, 0, NX, 0, NY, (const double *)CL, (const double *)F(c, PVOF_F_U),
-                     (const double *)F(c, PVOF_F_V), S(c, SC_FLUX_X), S(c, SC_FLUX_Y), c->p.weno_order == 5 ? 1 : 0));
-    TRY(fill(c, BK_WRAP_U, S(c, SC_FLUX_X)));
-    TRY(fill(c, BK_WRAP_V, S(c, SC_FLUX_Y)));
-    TRY(launch2d(c, k_flux_div, 0, NX, 0, NY, (const double *)S(c, SC_FLUX_X), (const double *)S(c, SC_FLUX_Y), out));
+    if (!c->adv_maps) {
+        c->adv_maps = advect_maps_create(c->base[PVOF_F_C_L], c->base[PVOF_F_U], c->base[PVOF_F_V], c->dom.P, c->dom.NY);
+        if (!c->adv_maps) return set_err(PVOF_ECUDA, "cuTensorMapEncodeTiled is not available for the advection tiles");
+    }
+    CK(advect_tma_launch(c->adv_maps, c->dom, c->maps[BK_WRAP_U], c->maps[BK_WRAP_V], CL, F(c, PVOF_F_U),
+                         F(c, PVOF_F_V), c->p.weno_order == 5 ? 1 : 0, fp32_stencils(c) != 0, out, c->scal, c->stream));
+    c->launches++;
     return fill(c, BK_SCALAR, out);
 }
 
@@ -993,7 +991,8 @@ int read_scalars(pvof_ctx *c)
         CK(cudaMemsetAsync(c->scal, 0, sizeof(DevScalars), c->stream));
         if (c->spec_s) CK(cudaMemsetAsync(c->spec_s, 0, sizeof(SpecScal), c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        return set_err(PVOF_ECUDA, code == 3 ? "cluster solver: a slab edge outside the owner's boundary rows"
+        return set_err(PVOF_ECUDA, code == 4 ? "advection tile load timed out"
+                                   : code == 3 ? "cluster solver: a slab edge outside the owner's boundary rows"
                                               : code == 2 ? "solver grid barrier timed out (spectral pressure solve)"
                                                           : "solver grid barrier timed out (grid-wide solver)");
     }
@@ -1915,6 +1914,7 @@ int pvof_destroy(pvof_ctx *c)
         for (int e = 0; e < 2; e++) if (c->pend_ev[q][e]) cudaEventDestroy(c->pend_ev[q][e]);
     delete c->ibm;
     delete c->tune;
+    advect_maps_destroy(c->adv_maps);
     for (GraphEntry &g : c->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     if (c->fft_coef) cudaFree(c->fft_coef);
@@ -2252,6 +2252,7 @@ int pvof_set_autotune(pvof_ctx *c, int enabled)
             ok = cudaEventCreate(&c->tune->ev[q][0]) == cudaSuccess && cudaEventCreate(&c->tune->ev[q][1]) == cudaSuccess;
         if (!ok) {
             delete c->tune;
+    advect_maps_destroy(c->adv_maps);
             c->tune = nullptr;
             return set_err(PVOF_ECUDA, "cudaEventCreate for the autotuner");
         }

@@ -83,7 +83,7 @@ __host__ __device__ inline size_t at(const Dom &d, int i, int j) { return (size_
 // scratch arrays beyond the public fields
 enum Scratch {
     SC_PSI = 0, SC_BULK_S, SC_CH_AUX1, SC_CH_RHS_NM1, SC_CH_RES, SC_CH_DIR, SC_CH_DIR2,
-    SC_FLUX_X, SC_FLUX_Y, SC_P_RES, SC_P_D, SC_P_AD, SC_P_MINV,
+    SC_P_RES, SC_P_D, SC_P_AD, SC_P_MINV,
     SC_U_R, SC_U_D, SC_U_AD, SC_U_DIAG, SC_V_R, SC_V_D, SC_V_AD, SC_V_DIAG,
     SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_SNAP, SC_PHI_PREV, SC_PHI_PREV1, SC_PHI_PREV2, SC_PHI_OLD, SC_PHI_OLD1, SC_PHI_OLD2, SC_P_HAT,
     SC_COUNT
@@ -196,6 +196,7 @@ struct Ctx {
     int graph_next;
     long long graph_replays; // substeps whose launches came from a graph
     struct TuneState *tune;  // stencil tile autotuner (null until pvof_set_autotune)
+    struct AdvectMaps *adv_maps;   // tensor maps of the C_L, u, v planes for the advection tiles
 };
 
 }  // namespace pvof

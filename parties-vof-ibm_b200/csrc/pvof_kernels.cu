@@ -48,58 +48,6 @@ __global__ void k_fill(Dom d, BcMap m, double *__restrict__ f)
 // Cahn-Hilliard substep (Eulerian/VOF_DIFFUSE.c)
 // ---------------------------------------------------------------------------
 
-// VOF_DIFFUSE_advect_WENO5 face fluxes (VOF_DIFFUSE.c:958-973, :453-498)
-__global__ void k_weno_flux(Dom d, int i0, int i1, int j0, int j1, const double *__restrict__ C,
-                            const double *__restrict__ u, const double *__restrict__ v,
-                            double *__restrict__ fx, double *__restrict__ fy, int weno5)
-{
-    KERNEL_2D_INDEX
-    double vel = AT_(u, i, j), st;
-    if (weno5) st = (vel >= 0.0) ? weno5_left(AT_(C, i - 3, j), AT_(C, i - 2, j), AT_(C, i - 1, j), AT_(C, i, j), AT_(C, i + 1, j))
-                                 : weno5_left(AT_(C, i + 2, j), AT_(C, i + 1, j), AT_(C, i, j), AT_(C, i - 1, j), AT_(C, i - 2, j));
-    else st = (vel >= 0.0) ? AT_(C, i - 1, j) : AT_(C, i, j);
-    AT_(fx, i, j) = vel * st;
-    vel = AT_(v, i, j);
-    if (weno5) st = (vel >= 0.0) ? weno5_left(AT_(C, i, j - 3), AT_(C, i, j - 2), AT_(C, i, j - 1), AT_(C, i, j), AT_(C, i, j + 1))
-                                 : weno5_left(AT_(C, i, j + 2), AT_(C, i, j + 1), AT_(C, i, j), AT_(C, i, j - 1), AT_(C, i, j - 2));
-    else st = (vel >= 0.0) ? AT_(C, i, j - 1) : AT_(C, i, j);
-    AT_(fy, i, j) = vel * st;
-}
-
-// the same face fluxes with the WENO5 states and the products in single
-// precision (the FP32 stencil form); each face flux is one stored value that
-// the two cells beside it share, so the divergence still telescopes
-__global__ void k_weno_flux_f(Dom d, int i0, int i1, int j0, int j1, const double *__restrict__ C,
-                              const double *__restrict__ u, const double *__restrict__ v,
-                              double *__restrict__ fx, double *__restrict__ fy, int weno5)
-{
-    KERNEL_2D_INDEX
-    auto c = [&](int a, int b) { return (float)AT_(C, a, b); };
-    float vel = (float)AT_(u, i, j), st;
-    if (weno5) st = (vel >= 0.0f) ? weno5_left_f(c(i - 3, j), c(i - 2, j), c(i - 1, j), c(i, j), c(i + 1, j))
-                                  : weno5_left_f(c(i + 2, j), c(i + 1, j), c(i, j), c(i - 1, j), c(i - 2, j));
-    else st = (vel >= 0.0f) ? c(i - 1, j) : c(i, j);
-    AT_(fx, i, j) = (double)(vel * st);
-    vel = (float)AT_(v, i, j);
-    if (weno5) st = (vel >= 0.0f) ? weno5_left_f(c(i, j - 3), c(i, j - 2), c(i, j - 1), c(i, j), c(i, j + 1))
-                                  : weno5_left_f(c(i, j + 2), c(i, j + 1), c(i, j), c(i, j - 1), c(i, j - 2));
-    else st = (vel >= 0.0f) ? c(i, j - 1) : c(i, j);
-    AT_(fy, i, j) = (double)(vel * st);
-}
-
-// rhs = -div(flux), TwodOps_scalar_flux_divergence (TwodOps.c:201-229)
-__global__ void k_flux_div(Dom d, int i0, int i1, int j0, int j1, const double *__restrict__ fx,
-                           const double *__restrict__ fy, double *__restrict__ out)
-{
-    KERNEL_2D_INDEX
-    double div_x = (AT_(fx, i + 1, j) - AT_(fx, i, j)) / d.m.dx_c[i];
-    double div_y = (AT_(fy, i, j + 1) - AT_(fy, i, j)) / d.m.dy_c[j];
-    double div;
-    if (d.planar) div = div_x + div_y;
-    else div = (d.m.r_u[i + 1] * AT_(fx, i + 1, j) - d.m.r_u[i] * AT_(fx, i, j)) * d.m.inv_r_c[i] / d.m.dx_c[i] + div_y;
-    AT_(out, i, j) = -div;
-}
-
 // VOF_DIFFUSE_compute_bulk_S (VOF_DIFFUSE.c:865-885)
 __global__ void k_bulk_S(Dom d, int i0, int i1, int j0, int j1, const double *__restrict__ CL,
                          const double *__restrict__ CS, double *__restrict__ bS)

@@ -74,6 +74,14 @@ struct SpecArgs {
     DevScalars *scal;
 };
 
+// VOF_DIFFUSE_advect_WENO5 as one TMA-tiled kernel (pvof_advect.cu)
+struct AdvectMaps;
+AdvectMaps *advect_maps_create(const double *C_base, const double *u_base, const double *v_base, int P, int NY);
+void advect_maps_destroy(AdvectMaps *a);
+cudaError_t advect_tma_launch(const AdvectMaps *a, const Dom &d, const BcMap &mu, const BcMap &mv, const double *C,
+                              const double *u, const double *v, int weno5, bool fp32, double *out, DevScalars *scal,
+                              cudaStream_t st);
+
 __global__ void k_unpack_rows(double *dst, int P, const double *src, int W, int H);
 __global__ void k_pack_rows(double *dst, const double *src, int P, int W, int H);
 
@@ -87,10 +95,6 @@ cudaError_t spec_launch_pcg(const SpecArgs &A, int blocks, double *d0, double *d
 const void *spec_pcg_kernel();   // k_spec_pcg, for marking graph nodes cooperative
 
 __global__ void k_fill(Dom d, BcMap m, double *f);
-__global__ void k_weno_flux(Dom d, int i0, int i1, int j0, int j1, const double *C, const double *u, const double *v,
-                            double *fx, double *fy, int weno5);
-__global__ void k_weno_flux_f(Dom d, int i0, int i1, int j0, int j1, const double *C, const double *u,
-                              const double *v, double *fx, double *fy, int weno5);
 __global__ void k_bulk_S_f(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *CS, double *bS);
 __global__ void k_laplacian_f(Dom d, int i0, int i1, int j0, int j1, const double *in, double *out);
 __global__ void k_psi_LG_f(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *lap, double *psi,
@@ -98,7 +102,6 @@ __global__ void k_psi_LG_f(Dom d, int i0, int i1, int j0, int j1, const double *
 __global__ void k_f_sigma_f(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *CG,
                             const double *CS, const double *psi, double *fx, double *fy, double scale, int ui0,
                             int ui1, int uj1, int vj0, int vi1, int vj1);
-__global__ void k_flux_div(Dom d, int i0, int i1, int j0, int j1, const double *fx, const double *fy, double *out);
 __global__ void k_bulk_S(Dom d, int i0, int i1, int j0, int j1, const double *CL, const double *CS, double *bS);
 __global__ void k_laplacian(Dom d, int i0, int i1, int j0, int j1, const double *in, double *out);
 __global__ void k_div_by(Dom d, int i0, int i1, int j0, int j1, double *a, double s);
