@@ -84,6 +84,13 @@ LONG_CASES = [
                                          zc=0.7, Cn=0.04, surface_tension=True, We=200.0, **AXI_TIGHT), 100, 1e-3),
 ]
 
+# long resolved-particle cases (final state only): the axisymmetric bubble below
+# the fixed sphere on the axis, surface tension, contact angle 90 degrees
+LONG_IBM_CASES = [
+    ("ibm_axi_st_100steps", "ibm_axi_st", dict(_builder="rising_bubble", **AXI_GRID_IBM, surface_tension=True,
+                                               We=200.0, **AXI_TIGHT), AXI_SPHERE, 90.0, 100, 1e-3),
+]
+
 # resolved-particle routine cases (oracle/ref/ibm_driver.c on the ibm2d build):
 # name, builder kwargs, particles (mobile, x, y, R, u, v, omega_z, rho_s), dt, stage
 IBM_CASES = [
@@ -248,6 +255,35 @@ def make_long(name, refcase, kw, steps, dt, outdir, refsrc=None):
     return path
 
 
+def make_long_ibm(name, refcase, kw, particles, theta, steps, dt, outdir, refsrc=None):
+    """steps whole steps of the immersed-boundary driver (oracle/ref/ibm_driver.c
+    "steps" mode); only the final state's physical cells are kept."""
+    grid, params, planes, _ = build_case(kw)
+    params.contact_angle_deg = theta
+    if not os.path.exists(po.ref_binary(refcase)):
+        po.build_reference(refcase, refsrc)
+    NX, NY, _ = cases.dims(grid)
+    fixed = [p[1:7] for p in particles if not p[0]]
+    mobile = [p[1:7] for p in particles if p[0]]
+    data = {}
+    with tempfile.TemporaryDirectory() as wd:
+        cp = po.run_reference_ibm(wd, grid, params, planes, fixed, mobile, dt, 0, case=refcase, mode="steps",
+                                  nsteps=steps, timeout=7200)
+        tag = "s%d" % steps
+        for fname, pname in (("C_L", "C_L"), ("u", "U"), ("v", "V"), ("p", "P")):
+            a = g_range(grid, po.read_reference_field(wd, tag, fname, grid), False)
+            data["%s/%s" % (tag, pname)] = a[:NY - 1, :NX - 1]
+        pid, X, U, Om = po.read_reference_particle_state(wd, tag)
+        data[tag + "/pid"], data[tag + "/pX"], data[tag + "/pU"] = pid, X, U
+        data["iterations"] = parse_iterations(cp.stdout)
+    meta = {"grid": struct_to_dict(grid), "params": struct_to_dict(params), "particles": [list(p) for p in particles],
+            "steps": steps, "dt": dt, "builder": kw, "refcase": refcase, "physical_only": True}
+    data["meta"] = np.array(repr(meta))
+    path = os.path.join(outdir, name + ".npz")
+    np.savez_compressed(path, **data)
+    return path
+
+
 def make_ibm(name, kw, particles, dt, stage, outdir, refsrc=None):
     grid, params, planes, refcase = build_case(kw)
     refcase = refcase or "ibm2d"
@@ -393,6 +429,9 @@ def main():
     for name, refcase, kw, steps, dt in LONG_CASES:
         if ap_only is not None and name in ap_only:   # minutes of CPU: only on request
             print(make_long(name, refcase, kw, steps, dt, a.out, a.refsrc))
+    for name, refcase, kw, parts, theta, steps, dt in LONG_IBM_CASES:
+        if ap_only is not None and name in ap_only:
+            print(make_long_ibm(name, refcase, kw, parts, theta, steps, dt, a.out, a.refsrc))
     for name, kw, parts, dt, stage in IBM_CASES:
         if ap_only is None or name in ap_only:
             print(make_ibm(name, kw, parts, dt, stage, a.out, a.refsrc))

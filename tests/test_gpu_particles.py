@@ -137,3 +137,27 @@ def test_droplet_on_cylinder_fp32_form_and_graphs():
     print("volume rel %.2e, graph replays %d" % (abs(mb - ma) / ma, replays))
     assert abs(mb - ma) <= 1e-6 * ma
     assert replays > 0
+
+
+def test_hundred_steps_axisym_sphere_against_reference():
+    """The axisymmetric bubble below the fixed sphere on the axis (32x64,
+    surface tension We 200, contact angle 90 degrees, density ratio 0.1),
+    100 RK3 steps at dt 1e-3 with tight solver tolerances: C_L, u, v and p on
+    the physical cells within 1e-10 relative L2 of the reference's own time
+    step (fixture ibm_axi_st_100steps, written by the ibm_axi_st reference
+    build), every substep replayed from CUDA graphs after the first few."""
+    from pvof import cases, runtime
+    grid, params, _, d, meta = load_golden("ibm_axi_st_100steps")
+    build = {k: v for k, v in meta["builder"].items() if k != "_builder"}
+    _, _, planes = cases.rising_bubble(**build)
+    s = runtime.Solver(grid, params, device=0)
+    s.set_particles([tuple(p) for p in meta["particles"]])
+    s.set_planes(dict(planes, C_L=planes["F"]))
+    s.initialize()
+    s.run_steps(meta["steps"], meta["dt"])
+    NX, NY, _ = cases.dims(grid)
+    tag = "s%d" % meta["steps"]
+    worst = {f: rel_l2(g_range(grid, s.get(f))[:NY - 1, :NX - 1], d["%s/%s" % (tag, f)]) for f in ("C_L", "U", "V", "P")}
+    print(worst, "graph replays", s.graph_replays())
+    assert all(r <= 1e-10 for r in worst.values()), worst
+    assert s.graph_replays() > 250
