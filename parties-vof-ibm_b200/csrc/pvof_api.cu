@@ -405,6 +405,8 @@ template <class A>
 int coop_launch(pvof_ctx *c, const void *fn, A &args, int n, int kind, int comp)
 {
     int nb = coop_blocks(c, n, kind);
+    // the solvers' counting grid barriers start from zero arrivals
+    CK(cudaMemsetAsync(&c->scal->bar_arrivals, 0, sizeof(unsigned long long), c->stream));
     return timed_launch(c, kind, comp, n, [&]() {
         void *params[] = {&args};
         return cudaLaunchCooperativeKernel(fn, dim3((unsigned)nb), dim3(COOP_THREADS), params, 0, c->stream);
@@ -951,11 +953,13 @@ int p_solve(pvof_ctx *c)
     A.maxit = c->p.P_CG_MAXIT;
     A.partials = c->partials;
     A.scal = c->scal;
+    A.bx = S(c, SC_P_BX);
+    A.by = S(c, SC_P_BY);
     const int n = (c->dom.NX - 1) * (c->dom.NY - 1);
     if (c->cgs_p_smem)
         TRY(timed_launch(c, PVOF_SOLVER_PRESSURE, 0, n, [&]() { return cgs_pressure_launch(A, StripPlan{c->cgs_p_smem, c->cgs_p_threads}, c->stream); }));
     else
-        TRY(coop_launch(c, (const void *)k_cg_pressure, A, n, PVOF_SOLVER_PRESSURE, 0));
+        TRY(coop_launch(c, (const void *)k_cg_pressure_fw, A, n, PVOF_SOLVER_PRESSURE, 0));
     return fill(c, BK_WRAP_C, F(c, PVOF_F_DELTAP));
 }
 
@@ -1125,7 +1129,7 @@ bool keep_cooperative(cudaGraph_t g)
     if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return false;
     std::vector<cudaGraphNode_t> nodes(n);
     if (n && cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return false;
-    const void *coop[] = {(const void *)k_cg_biharmonic, (const void *)k_cg_velocity, (const void *)k_cg_pressure,
+    const void *coop[] = {(const void *)k_cg_biharmonic, (const void *)k_cg_velocity, (const void *)k_cg_pressure_fw,
                           spec_pcg_kernel()};
     for (cudaGraphNode_t nd : nodes) {
         cudaGraphNodeType t;
@@ -1850,7 +1854,7 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     if (!coop) return fail(PVOF_ENODEV, "device without cooperative launch");
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_cg_biharmonic, COOP_THREADS, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_cg_velocity, COOP_THREADS, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, k_cg_pressure, COOP_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, k_cg_pressure_fw, COOP_THREADS, 0);
     ob = std::min(o1, std::min(o2, o3));
     if (ob < 1) return fail(PVOF_ECUDA, "persistent solver kernels do not fit on an SM");
     c->coop_blocks_of[PVOF_SOLVER_BIHARMONIC] = o1 * nsm;   // each as many as it keeps co-resident
@@ -2300,7 +2304,7 @@ const char *pvof_solver_kernel(const pvof_ctx *c, int solver)
     switch (solver) {
     case PVOF_SOLVER_BIHARMONIC: return "k_cg_biharmonic";
     case PVOF_SOLVER_VELOCITY: return c->cgs_v_smem ? "k_cgs_velocity" : "k_cg_velocity";
-    case PVOF_SOLVER_PRESSURE: return c->cgs_p_smem ? "k_cgs_pressure" : "k_cg_pressure";
+    case PVOF_SOLVER_PRESSURE: return c->cgs_p_smem ? "k_cgs_pressure" : "k_cg_pressure_fw";
     default: return "";
     }
 }

@@ -16,9 +16,13 @@
 // arithmetic per value is the reference's, so the iterates are those of the
 // reference's loop.
 //
-// The grid barrier is this file's own (not cooperative_groups::grid_group::
-// sync) so that its wait is bounded: if the other blocks never arrive it
-// records an error in DevScalars::error and every block leaves the solver.
+// The grid barriers are this file's own (not cooperative_groups::grid_group::
+// sync) so that their waits are bounded: if the other blocks never arrive
+// they record an error in DevScalars::error and every block leaves the
+// solver.  The context's solvers count arrivals on a counter that the host
+// zeroes before each launch (grid_barrier_counted: a fence, one atomic and
+// the poll that sees the total); the no-allocation entry point's pressure
+// solve keeps the generation barrier (grid_barrier), which needs no reset.
 #include "pvof_device.cuh"
 #include "pvof_kernels.cuh"
 
@@ -65,6 +69,53 @@ __device__ __noinline__ bool grid_barrier(const GridSync &gs)
     __syncthreads();
     return ok != 0;
 }
+
+// Grid barrier on a counter of arrivals that the host zeroes before the
+// launch: the g-th barrier of a launch is passed once the counter reaches
+// g * gridDim.x.  Each block's thread 0 publishes the block's writes
+// (block barrier, then a device-scope fence), adds its arrival without
+// waiting for the result and polls the counter; nothing is reset or bumped
+// after the last arrival, so the barrier costs a fence, one atomic and the
+// poll that sees the total.  Bounded like grid_barrier: false (in every
+// thread of the block) when it gave up, with the error recorded.
+__device__ __noinline__ bool grid_barrier_counted(unsigned long long *arrivals, int *error, unsigned long long target)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned long long *va = arrivals;
+        volatile int *verr = error;
+        int good = 1;
+        __threadfence();
+        atomicAdd(arrivals, 1ull);
+        unsigned long long spins = 0;
+        while (*va < target) {
+            ++spins;
+            if ((spins & 1023ull) == 0 && (*verr != 0 || spins > BARRIER_SPIN_LIMIT)) {
+                atomicCAS(error, 0, 1);   // 1: a grid-wide solver's barrier
+                good = 0;
+                break;
+            }
+            if (spins > 4096) __nanosleep(64);
+        }
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// The counting barrier of one launch: the launch's g-th call waits for
+// g * gridDim.x arrivals.
+struct CountedSync {
+    DevScalars *s;
+    unsigned long long target;
+    __device__ bool sync()
+    {
+        target += gridDim.x;
+        return grid_barrier_counted(&s->bar_arrivals, &s->error, target);
+    }
+};
 
 // sum of v over the block (1D blocks, multiple of 32 threads)
 __device__ double block_sum(double v)
@@ -139,7 +190,7 @@ __global__ void __launch_bounds__(512) k_cg_biharmonic(BihArgs A)
 {
     const Dom &d = A.d;
     const int P = d.P, NX = d.NX, NY = d.NY;
-    const GridSync gs{A.scal, gridDim.x};
+    CountedSync gs{A.scal, 0};
     const Range R{0, 0, NX - 1, (NX - 1) * (NY - 1)};
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
     const double nk = (double)d.nk;
@@ -180,7 +231,7 @@ __global__ void __launch_bounds__(512) k_cg_biharmonic(BihArgs A)
     }
     put_partial(part0, sbb);
     put_partial(part1, srr);
-    if (!grid_barrier(gs)) return;
+    if (!gs.sync()) return;
     double rhs_norm = sqrt(nk * grid_total(part0));
     if (rhs_norm < 1e-30) rhs_norm = 1.0;
     double rz = nk * grid_total(part1);
@@ -217,7 +268,7 @@ __global__ void __launch_bounds__(512) k_cg_biharmonic(BihArgs A)
         if (!first) { double *t = pcur; pcur = pnxt; pnxt = t; }
         first = false;
         put_partial(part2, spap);
-        if (!grid_barrier(gs)) return;
+        if (!gs.sync()) return;
         double pAp = nk * grid_total(part2);
         if (fabs(pAp) < 1e-30) break;
         double alpha = rz / pAp;
@@ -231,7 +282,7 @@ __global__ void __launch_bounds__(512) k_cg_biharmonic(BihArgs A)
             srr2 += d.m.wx[i] * d.m.wy[j] * d.wz * rv * rv;
         }
         put_partial(part3, srr2);
-        if (!grid_barrier(gs)) return;
+        if (!gs.sync()) return;
         ++iter;
         double rr = nk * grid_total(part3);
         rel = sqrt(rr) / rhs_norm;
@@ -251,7 +302,7 @@ __global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
 {
     const Dom &d = A.d;
     const int P = d.P, NX = d.NX, NY = d.NY;
-    const GridSync gs{A.scal, gridDim.x};
+    CountedSync gs{A.scal, 0};
     const Range R{A.i0, A.j0, A.i1 - A.i0, (A.i1 - A.i0) * (A.j1 - A.j0)};
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
     const double EPS = 1e-14;
@@ -274,7 +325,7 @@ __global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
         srz += rv * dv;
     }
     put_partial(part0, srz);
-    if (!grid_barrier(gs)) return;
+    if (!gs.sync()) return;
     double rz = grid_total(part0);
     double RMS = 0.0, beta = 0.0;
     int iters = 0;
@@ -316,7 +367,7 @@ __global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
         if (!first) { double *t = dcur; dcur = dnxt; dnxt = t; }
         first = false;
         put_partial(part1, sdad);
-        if (!grid_barrier(gs)) return;
+        if (!gs.sync()) return;
         double dAd = grid_total(part1);
         double alpha = rz / (dAd + A.step_eps);
         double s0 = 0.0, s1 = 0.0;
@@ -333,7 +384,7 @@ __global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
         }
         put_partial(part2, s0);
         put_partial(part3, s1);
-        if (!grid_barrier(gs)) return;
+        if (!gs.sync()) return;
         double rz_new = grid_total(part2), rr = grid_total(part3);
         RMS = sqrt(A.in_tot * rr);
         if (RMS < A.tol) break;
@@ -347,8 +398,32 @@ __global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
 // Pressure_solve_cg (Eulerian/lsolver/psolve_cg.c:130-293): Jacobi PCG on the
 // variable-density Poisson operator, absolute stop on sqrt(r.M^-1 r), mean
 // removed at the end.
+//
+// FW (the context's solve): the operator's face weights 2 / (rho_P + rho_N)
+// are computed once, in the set-up phase, into the planes A.bx / A.by, so an
+// iteration multiplies instead of dividing four times per cell; without FW
+// (the no-allocation entry point, which has no room for the planes) they are
+// computed from rho at every application.  The pressure ghost rules copy
+// with weight 1 (psolve_cg.c:374-460: Neumann copies, periodic wrap) and
+// leave the solve range [0, NX-2] x [0, NY-2] unmapped, so a neighbour's
+// source differs from it only at the four ends of the axes: those sources
+// are read once from the maps and the stencil is gathered without branches.
+// The FW form also uses counting grid barriers (grid_barrier_counted; the
+// host zeroes the counter before the launch).  DEFER: the update
+// phi += alpha d of an iteration is applied in the next iteration's direction
+// pass, which reads d at the cell anyway (the same operands and operation,
+// one pass later; before the mean removal after the last iteration), so the
+// update pass reads three planes instead of five.  U1: cells per loop trip
+// of the direction pass (the update pass takes two), their loads issued
+// before either cell's stores.  Measured per iteration on B200 (the same
+// results bit for bit in every form): 1024x1024 31.7 us for the plain form
+// (without FW), 20.8 us for FW with DEFER and U1 = 1, which the context
+// uses; 2048x2048 154 and 96.6 us; 256x512 10.7 and 8.2 us.  At 64
+// registers (two 512-thread blocks per SM) U1 = 2 with DEFER loses loads in
+// flight and ran 16% slower at 2048x2048.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_cg_pressure(PresArgs A)
+template <bool FW, bool DEFER, int U1>
+__device__ __forceinline__ void cg_pressure(const PresArgs &A)
 {
     const Dom &d = A.d;
     const int P = d.P, NX = d.NX, NY = d.NY;
@@ -356,12 +431,21 @@ __global__ void __launch_bounds__(512) k_cg_pressure(PresArgs A)
     const Range R{0, 0, NX - 1, (NX - 1) * (NY - 1)};
     const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
     double *part0 = A.partials, *part1 = A.partials + gridDim.x, *part2 = A.partials + 2 * gridDim.x;
+    // sources of the neighbours beyond the ends of the solve range
+    const int xw = A.mp.x.src[NG - 1], xe = A.mp.x.src[NX - 1 + NG];
+    const int ys = A.mp.y.src[NG - 1], yn = A.mp.y.src[NY - 1 + NG];
+    const double *__restrict__ rho = A.rho;
+    const double *__restrict__ bx = A.bx;
+    const double *__restrict__ by = A.by;
+    CountedSync cs{A.scal, 0};
+    auto barrier = [&]() { return FW ? cs.sync() : grid_barrier(gs); };
 
     double sg = 0.0;
     for (int q = tid; q < R.n; q += nth) {
         int i, j;
         R.ij(q, i, j);
-        double ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, A.phi, P, NX, NY, a, b); });
+        if (FW) pressure_face_weights(d, rho, A.bx, A.by, i, j);
+        double ad = pressure_op(d, rho, i, j, [&](int a, int b) { return remap(A.mp, A.phi, P, NX, NY, a, b); });
         // the axisymmetric right-hand side carries the row weight r_c of the
         // operator (psolve_hypre.c:184-200)
         double rv = (d.axisym ? AT_(A.rhs, i, j) * d.m.r_c[i] : AT_(A.rhs, i, j)) - ad;
@@ -372,72 +456,144 @@ __global__ void __launch_bounds__(512) k_cg_pressure(PresArgs A)
         sg += rv * z;
     }
     put_partial(part0, sg);
-    if (!grid_barrier(gs)) return;
+    if (!barrier()) return;
     double gamma = grid_total(part0), gamma_new = 0.0, beta = 0.0;
     if (sqrt(gamma) < A.tol) {
         if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->p_iters = 0; A.scal->p_res = sqrt(gamma); }
         return;
     }
+
+    // d = z + beta d_old at the five points of cell q (d_old alone on the
+    // first iteration) and A d at the cell
+    auto direction = [&](int q, bool first, const double *__restrict__ zp, const double *__restrict__ dold, double bt,
+                         double &dv, double &ad) {
+        int i, j;
+        R.ij(q, i, j);
+        const int iw = i > 0 ? i - 1 : xw, ie = i < NX - 2 ? i + 1 : xe;
+        const int js = j > 0 ? j - 1 : ys, jn = j < NY - 2 ? j + 1 : yn;
+        const ptrdiff_t row = (ptrdiff_t)j * P;
+        const ptrdiff_t cC = row + i, cE = row + ie, cW = row + iw;
+        const ptrdiff_t cN = (ptrdiff_t)jn * P + i, cS = (ptrdiff_t)js * P + i;
+        double vc, ve, vw, vn, vs;
+        if (first) {
+            vc = dold[cC]; ve = dold[cE]; vw = dold[cW]; vn = dold[cN]; vs = dold[cS];
+        } else {
+            vc = zp[cC] + bt * dold[cC];
+            ve = zp[cE] + bt * dold[cE];
+            vw = zp[cW] + bt * dold[cW];
+            vn = zp[cN] + bt * dold[cN];
+            vs = zp[cS] + bt * dold[cS];
+        }
+        double bxm, bxp, bym, byp;
+        if (FW) {
+            bxm = bx[cC - 1]; bxp = bx[cC]; bym = by[cC - P]; byp = by[cC];
+        } else {
+            const double r0 = rho[cC];
+            bxp = 2.0 / (r0 + rho[cC + 1]);
+            bxm = 2.0 / (r0 + rho[cC - 1]);
+            byp = 2.0 / (r0 + rho[cC + P]);
+            bym = 2.0 / (r0 + rho[cC - P]);
+        }
+        double cxm, cxp, cym, cyp;
+        face_coeffs(d, i, bxm, bxp, bym, byp, cxm, cxp, cym, cyp);
+        const double val = cxp * (ve - vc) - cxm * (vc - vw) + cyp * (vn - vc) - cym * (vc - vs);
+        dv = vc;
+        ad = row_weight(d, i) * val;
+    };
+
     double *dcur = A.dir, *dnxt = A.dir2;
     bool first = true;
+    double alpha = 0.0;   // FW: the step of the update phi += alpha d_cur still to be applied
     int iters;
     for (iters = 1; iters <= A.maxit; iters++) {
-        // d = z + beta d (z = M r), Ad with the pressure ghost update of d
+        // d = z + beta d (z = M r), Ad with the pressure ghost update of d;
+        // FW: phi += alpha d_old from the previous iteration at the cell
         double sdad = 0.0;
-        const double bt = beta;
+        const double bt = beta, al = alpha;
         const double *dold = dcur;
-        for (int q = tid; q < R.n; q += nth) {
+        for (int q = tid; q < R.n; q += U1 * nth) {
+            const int q1 = q + nth;
+            const bool two = U1 == 2 && q1 < R.n;
+            double dv0, ad0, dv1 = 0.0, ad1 = 0.0;
+            direction(q, first, A.z, dold, bt, dv0, ad0);
+            if (two) direction(q1, first, A.z, dold, bt, dv1, ad1);
             int i, j;
             R.ij(q, i, j);
-            double dv, ad;
-            if (first) {
-                dv = AT_(dold, i, j);
-                ad = pressure_op(d, A.rho, i, j, [&](int a, int b) { return remap(A.mp, dold, P, NX, NY, a, b); });
-            } else {
-                dv = AT_(A.z, i, j) + bt * AT_(dold, i, j);
-                AT_(dnxt, i, j) = dv;
-                ad = pressure_op(d, A.rho, i, j, [&](int a, int b) {
-                    int si, sj;
-                    double mul;
-                    src_of(A.mp, NX, NY, a, b, si, sj, mul);
-                    return AT_(A.z, si, sj) + bt * AT_(dold, si, sj);
-                });
+            double ph0 = 0.0, do0 = 0.0, ph1 = 0.0, do1 = 0.0;
+            if (DEFER && !first) {
+                ph0 = AT_(A.phi, i, j); do0 = AT_(dold, i, j);
+                if (two) {
+                    int i1, j1;
+                    R.ij(q1, i1, j1);
+                    ph1 = AT_(A.phi, i1, j1); do1 = AT_(dold, i1, j1);
+                }
             }
-            AT_(A.Ad, i, j) = ad;
-            sdad += dv * ad;
+            if (!first) AT_(dnxt, i, j) = dv0;
+            AT_(A.Ad, i, j) = ad0;
+            if (DEFER && !first) AT_(A.phi, i, j) = ph0 + al * do0;
+            sdad += dv0 * ad0;
+            if (two) {
+                R.ij(q1, i, j);
+                if (!first) AT_(dnxt, i, j) = dv1;
+                AT_(A.Ad, i, j) = ad1;
+                if (DEFER && !first) AT_(A.phi, i, j) = ph1 + al * do1;
+                sdad += dv1 * ad1;
+            }
         }
         if (!first) { double *t = dcur; dcur = dnxt; dnxt = t; }
         first = false;
         put_partial(part1, sdad);
-        if (!grid_barrier(gs)) return;
-        double alpha = gamma / (grid_total(part1) + 1e-30);
+        if (!barrier()) return;
+        alpha = gamma / (grid_total(part1) + 1e-30);
         double sgn = 0.0;
-        for (int q = tid; q < R.n; q += nth) {
-            int i, j;
-            R.ij(q, i, j);
-            AT_(A.phi, i, j) += alpha * AT_(dcur, i, j);
-            double rv = AT_(A.res, i, j) - alpha * AT_(A.Ad, i, j);
-            AT_(A.res, i, j) = rv;
-            double z = rv * AT_(A.M, i, j);
-            AT_(A.z, i, j) = z;
-            sgn += rv * z;
+        for (int q = tid; q < R.n; q += 2 * nth) {
+            const int q1 = q + nth;
+            const bool two = q1 < R.n;
+            int i0, j0, i1 = 0, j1 = 0;
+            R.ij(q, i0, j0);
+            double ph0 = 0.0, dc0 = 0.0, ph1 = 0.0, dc1 = 0.0;
+            if (!DEFER) { ph0 = AT_(A.phi, i0, j0); dc0 = AT_(dcur, i0, j0); }
+            double r0 = AT_(A.res, i0, j0), a0 = AT_(A.Ad, i0, j0), m0 = AT_(A.M, i0, j0);
+            double r1 = 0.0, a1 = 0.0, m1 = 0.0;
+            if (two) {
+                R.ij(q1, i1, j1);
+                if (!DEFER) { ph1 = AT_(A.phi, i1, j1); dc1 = AT_(dcur, i1, j1); }
+                r1 = AT_(A.res, i1, j1); a1 = AT_(A.Ad, i1, j1); m1 = AT_(A.M, i1, j1);
+            }
+            {
+                const double rv = r0 - alpha * a0, z = rv * m0;
+                if (!DEFER) AT_(A.phi, i0, j0) = ph0 + alpha * dc0;
+                AT_(A.res, i0, j0) = rv;
+                AT_(A.z, i0, j0) = z;
+                sgn += rv * z;
+            }
+            if (two) {
+                const double rv = r1 - alpha * a1, z = rv * m1;
+                if (!DEFER) AT_(A.phi, i1, j1) = ph1 + alpha * dc1;
+                AT_(A.res, i1, j1) = rv;
+                AT_(A.z, i1, j1) = z;
+                sgn += rv * z;
+            }
         }
         put_partial(part2, sgn);
-        if (!grid_barrier(gs)) return;
+        if (!barrier()) return;
         gamma_new = grid_total(part2);
         if (sqrt(gamma_new) < A.tol) break;
         beta = gamma_new / (gamma + 1e-30);
         gamma = gamma_new;
     }
-    // remove the mean (every face Neumann or periodic), psolve_cg.c:255-279
+    // remove the mean (every face Neumann or periodic), psolve_cg.c:255-279;
+    // FW: after the last iteration's pending update
     double ssum = 0.0;
+    const bool pending = DEFER && !first;
     for (int q = tid; q < R.n; q += nth) {
         int i, j;
         R.ij(q, i, j);
+        if (pending) AT_(A.phi, i, j) += alpha * AT_(dcur, i, j);
         ssum += AT_(A.phi, i, j);
     }
     put_partial(part0, ssum);
-    if (!grid_barrier(gs)) return;
+    if (!barrier()) return;
     double avg = grid_total(part0) / (double)R.n;
     for (int q = tid; q < R.n; q += nth) {
         int i, j;
@@ -447,5 +603,8 @@ __global__ void __launch_bounds__(512) k_cg_pressure(PresArgs A)
     if (iters > A.maxit) iters = A.maxit;
     if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->p_iters = iters; A.scal->p_res = sqrt(gamma_new); }
 }
+
+__global__ void __launch_bounds__(512) k_cg_pressure(PresArgs A) { cg_pressure<false, false, 2>(A); }
+__global__ void __launch_bounds__(512, 2) k_cg_pressure_fw(PresArgs A) { cg_pressure<true, true, 1>(A); }
 
 }  // namespace pvof

@@ -184,6 +184,35 @@ __device__ __forceinline__ double pressure_op(const Dom &d, const double *__rest
     return row_weight(d, i) * val;
 }
 
+// The face weights 2 / (rho_P + rho_N) of pressure_op, one per east face
+// (bx(i,j), between cells i and i+1) and one per north face (by(i,j)).  The
+// west weight of cell i is the east weight of cell i-1: the same two
+// densities added in the other order, the same sum exactly.
+__device__ __forceinline__ void pressure_face_weights(const Dom &d, const double *__restrict__ rho, double *bx,
+                                                      double *by, int i, int j)
+{
+    const int P = d.P;
+    const double r0 = AT_(rho, i, j);
+    AT_(bx, i, j) = 2.0 / (r0 + AT_(rho, i + 1, j));
+    AT_(by, i, j) = 2.0 / (r0 + AT_(rho, i, j + 1));
+    if (i == 0) AT_(bx, i - 1, j) = 2.0 / (r0 + AT_(rho, i - 1, j));
+    if (j == 0) AT_(by, i, j - 1) = 2.0 / (r0 + AT_(rho, i, j - 1));
+}
+
+// pressure_op with the face weights read from pressure_face_weights' planes:
+// bit for bit the same value, without the four divisions
+template <class Get>
+__device__ __forceinline__ double pressure_op_w(const Dom &d, const double *__restrict__ bx,
+                                                const double *__restrict__ by, int i, int j, Get get)
+{
+    const int P = d.P;
+    double cxm, cxp, cym, cyp;
+    face_coeffs(d, i, AT_(bx, i - 1, j), AT_(bx, i, j), AT_(by, i, j - 1), AT_(by, i, j), cxm, cxp, cym, cyp);
+    double c = get(i, j);
+    double val = cxp * (get(i + 1, j) - c) - cxm * (c - get(i - 1, j)) + cyp * (get(i, j + 1) - c) - cym * (c - get(i, j - 1));
+    return row_weight(d, i) * val;
+}
+
 // vel_jacobi_diag (Eulerian/lsolver/msolve_cg.c:98-249), diffuse VOF
 __device__ __forceinline__ double vel_diag(const Dom &d, int comp, const double *__restrict__ rho,
                                            const double *__restrict__ mu, int i, int j, double iRe, double alpha_dt)

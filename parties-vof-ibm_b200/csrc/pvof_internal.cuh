@@ -86,6 +86,7 @@ enum Scratch {
     SC_P_RES, SC_P_D, SC_P_AD, SC_P_MINV,
     SC_U_R, SC_U_D, SC_U_AD, SC_U_DIAG, SC_V_R, SC_V_D, SC_V_AD, SC_V_DIAG,
     SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_SNAP, SC_PHI_PREV, SC_PHI_PREV1, SC_PHI_PREV2, SC_PHI_OLD, SC_PHI_OLD1, SC_PHI_OLD2, SC_P_HAT,
+    SC_P_BX, SC_P_BY,
     SC_COUNT
 };
 
@@ -104,6 +105,7 @@ struct DevScalars {
     int error;          // non-zero: a grid barrier gave up (see pvof_cg.cu)
     unsigned bar_count; // grid barrier state
     unsigned bar_gen;
+    unsigned long long bar_arrivals;   // arrivals at the counting grid barrier, zeroed before each launch
 };
 
 // launch shape of a strip solver: threads per CTA (0: the range does not fit)

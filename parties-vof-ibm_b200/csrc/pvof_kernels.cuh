@@ -46,11 +46,12 @@ struct PresArgs {
     int maxit;
     double *partials;
     DevScalars *scal;
+    double *bx = nullptr, *by = nullptr;   // face-weight planes (k_cg_pressure_fw)
 };
 
 // spectral-preconditioned pressure PCG (pvof_spec.cu)
 struct SpecScal {
-    unsigned bar_count, bar_gen;   // grid barrier of the cooperative solve (arrivals, generation)
+    unsigned arrivals;   // arrivals at the solve's grid barriers, zeroed before each launch
 };
 
 constexpr int SPEC_PT = 1024;        // threads per block of the cooperative solve
@@ -265,5 +266,6 @@ __global__ void k_fft_inverse(Dom d, int N, int logN, const double *hc, double *
 __global__ void k_cg_biharmonic(BihArgs A);
 __global__ void k_cg_velocity(VelArgs A);
 __global__ void k_cg_pressure(PresArgs A);
+__global__ void k_cg_pressure_fw(PresArgs A);
 
 }  // namespace pvof

@@ -105,36 +105,38 @@ __device__ double block_sum(double v, double *sh)
     return t;
 }
 
-// Grid barrier: the last block to arrive resets the arrival count and
-// advances the generation that the others wait on, so the barrier needs no
-// reset between launches.  The wait is bounded; returns false (in every
-// thread of the block) when it gave up or another block did.
+// Grid barrier on a counter of arrivals that the host zeroes before the
+// launch: the launch's g-th barrier is passed once the counter reaches
+// g * gridDim.x (spec_bar_target, kept by the block's thread 0 in shared
+// memory so that it takes no register of the solve; at most four barriers
+// per iteration, so 32 bits hold the count of any iteration cap below
+// about 7 million).  Each block's thread 0 publishes
+// the block's writes (block barrier, device-scope fence), adds its arrival
+// without waiting for the result and polls the counter.  The wait is
+// bounded; returns false (in every thread of the block) when it gave up or
+// another block did.
+__shared__ unsigned spec_bar_target;
+
 __device__ __noinline__ bool spec_barrier(SpecScal *s, int *err)
 {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned *vgen = &s->bar_gen;
+        const unsigned target = spec_bar_target += gridDim.x;
+        volatile unsigned *va = &s->arrivals;
         volatile int *verr = err;
-        int good = (*verr == 0);
-        const unsigned g = *vgen;
+        int good = 1;
         __threadfence();
-        const unsigned arrived = atomicAdd(&s->bar_count, 1u);
-        if (arrived == gridDim.x - 1) {
-            s->bar_count = 0u;
-            __threadfence();
-            atomicAdd(&s->bar_gen, 1u);
-        } else {
-            unsigned long long spins = 0;
-            while (*vgen == g) {
-                ++spins;
-                if ((spins & 1023ull) == 0 && (*verr != 0 || spins > SPEC_SPIN_LIMIT)) {
-                    atomicCAS(err, 0, 2);   // 2: the spectral solve's barrier
-                    good = 0;
-                    break;
-                }
-                if (spins > 4096) __nanosleep(64);
+        atomicAdd(&s->arrivals, 1u);
+        unsigned long long spins = 0;
+        while (*va < target) {
+            ++spins;
+            if ((spins & 1023ull) == 0 && (*verr != 0 || spins > SPEC_SPIN_LIMIT)) {
+                atomicCAS(err, 0, 2);   // 2: the spectral solve's barrier
+                good = 0;
+                break;
             }
+            if (spins > 4096) __nanosleep(64);
         }
         __threadfence();
         ok = good;
@@ -503,6 +505,7 @@ __global__ void __launch_bounds__(SPEC_PT) k_spec_pcg(SpecArgs A, double *d0, do
     double *slotA = A.part, *slotB = A.part + gridDim.x, *slotC = A.part + 2 * gridDim.x;
     SpecScal *S = A.s;
     int *err = &A.scal->error;
+    if (threadIdx.x == 0) spec_bar_target = 0;
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
     for (int k = threadIdx.x; k < N / 2; k += blockDim.x) tw[k] = A.tw[k];
     __syncthreads();
@@ -777,6 +780,9 @@ cudaError_t spec_launch_pcg(const SpecArgs &A, int blocks, double *d0, double *d
 {
     SpecArgs a = A;
     void *args[] = {&a, &d0, &d1};
+    // the grid barriers count arrivals from zero
+    const cudaError_t e = cudaMemsetAsync(&A.s->arrivals, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
     return cudaLaunchCooperativeKernel((const void *)k_spec_pcg, dim3((unsigned)blocks), dim3(SPEC_PT), args,
                                        spec_pcg_smem(A.N, A.M), st);
 }
