@@ -337,6 +337,54 @@ def large_case(args, device):
     return out
 
 
+def poisson_case(args, device):
+    """The reference's variable-density Jacobi-PCG alone
+    (pvof_Pressure_solve_cg, psolve_cg.c:130-293) on a grid whose solver
+    planes do not fit in L2: the planar instability at --poisson-grid with a
+    density ratio of 1e-3 and a seeded random velocity, so that the
+    right-hand side of Pressure_set_RHS (the divergence of that velocity over
+    the stage's dt) is not small.  Each of --poisson-reps solves starts from
+    zero (Pressure_set_RHS resets the correction) after an L2 flush and runs
+    --poisson-maxit iterations or to the reference's tolerance, timed by CUDA
+    events around the solve; achieved bandwidth counts 56 algorithmic bytes per
+    cell and iteration (x, r and the direction read and written, the density
+    the coefficients come from)."""
+    from pvof import cases, runtime
+    nxm, nym = (int(v) for v in args.poisson_grid.lower().split("x"))
+    ratio = 1e-3
+    grid, params, planes = cases.rayleigh_taylor(nxm, nym, Lx=1.0, Ly=nym / nxm, Cn=0.005,
+                                                 atwood=(1 - ratio) / (1 + ratio), velocity_seed=7,
+                                                 velocity_amp=0.01, P_CG_MAXIT=args.poisson_maxit)
+    s = runtime.Solver(grid, params, device=device)
+    s.set_planes(planes)
+    s.initialize()
+    s.set_stage(0, 1e-4)
+    s.set_solver_timing(True)
+    ms, iters = 0.0, 0
+    for r in range(args.poisson_reps + 1):
+        s.call("Pressure_set_RHS")
+        s.call("Pressure_compute_preconditioner")
+        s.flush_l2()
+        s.timer_start()
+        it = s.call("Pressure_solve_cg", None)
+        t = s.timer_stop()
+        if r > 0:   # the first solve warms up
+            ms += t
+            iters += it
+    name = s.solver_kernel(2)
+    s.set_solver_timing(False)
+    s.close()
+    cells = nxm * nym
+    peak, peak_kind = measured_peak()
+    gbs = ALG_BYTES[2] * cells * iters / (ms * 1e-3) / 1e9
+    return {"case": "planar instability %dx%d, density ratio 1e-3, random velocity (seed 7, amplitude 0.01); "
+                    "pressure Jacobi-PCG alone from zero, at most %d iterations" % (nxm, nym, args.poisson_maxit),
+            "kernel": name, "cells": cells, "solves": args.poisson_reps, "iterations": iters,
+            "us_per_iteration": 1e3 * ms / max(iters, 1),
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": gbs / peak, "alg_bytes_per_cell_iter": ALG_BYTES[2]}}
+
+
 # the axisymmetric benchmark case: a bubble (R 0.5 at z = 1) rising towards a
 # fixed sphere (R 0.25 at z = 2.5) on the axis, 256 x 512 cells over
 # r in [0, 2], z in [0, 4]
@@ -960,6 +1008,12 @@ def run_ours(args):
             droplets = droplet_batch(args, dist, local, ws, rank)
         except Exception as e:   # noqa: BLE001
             droplets = {"error": "%s: %s" % (type(e).__name__, e)}
+    poisson = None
+    if args.poisson:
+        try:
+            poisson = poisson_case(args, local)
+        except Exception as e:   # noqa: BLE001
+            poisson = {"error": "%s: %s" % (type(e).__name__, e)}
     large = None
     if args.large:
         try:
@@ -1012,6 +1066,8 @@ def run_ours(args):
             line["large"] = large
         if axisym is not None:
             line["axisym"] = axisym
+        if poisson is not None:
+            line["poisson"] = poisson
         if learned is not None:
             line["learned"] = learned
         if mixed is not None:
@@ -1061,6 +1117,12 @@ def main():
     ap.add_argument("--large-steps", type=int, default=3)
     ap.add_argument("--large-forms", default="plain,spectral,spectral-unreg",
                     help="comma-separated forms of --large: plain, spectral, spectral-unreg")
+    ap.add_argument("--poisson", action="store_true",
+                    help="also time the reference's pressure Jacobi-PCG alone on --poisson-grid (default 2048x2048, "
+                         "solver planes larger than L2) against the HBM roofline")
+    ap.add_argument("--poisson-grid", default="2048x2048")
+    ap.add_argument("--poisson-maxit", type=int, default=3000)
+    ap.add_argument("--poisson-reps", type=int, default=3)
     ap.add_argument("--axisym", action="store_true",
                     help="also time the axisymmetric bubble-and-sphere case (256x512) and the reference on it")
     ap.add_argument("--axisym-steps", type=int, default=10)
