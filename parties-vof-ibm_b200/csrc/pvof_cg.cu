@@ -420,9 +420,12 @@ __global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
 // (without FW), 20.8 us for FW with DEFER and U1 = 1, which the context
 // uses; 2048x2048 154 and 96.6 us; 256x512 10.7 and 8.2 us.  At 64
 // registers (two 512-thread blocks per SM) U1 = 2 with DEFER loses loads in
-// flight and ran 16% slower at 2048x2048.
+// flight and ran 16% slower at 2048x2048.  PAIR (k_cg_pressure_fwp): both
+// passes over pairs of neighbouring cells with 16-byte accesses, for ranges
+// of at least two cells per resident thread (the context picks it by size):
+// 2048x2048 94.0 -> 86.9 us, 1024x1024 20.7 -> 19.9 us.
 // ---------------------------------------------------------------------------
-template <bool FW, bool DEFER, int U1>
+template <bool FW, bool DEFER, int U1, bool PAIR>
 __device__ __forceinline__ void cg_pressure(const PresArgs &A)
 {
     const Dom &d = A.d;
@@ -501,6 +504,80 @@ __device__ __forceinline__ void cg_pressure(const PresArgs &A)
         ad = row_weight(d, i) * val;
     };
 
+    // PAIR: the two passes over pairs of cells (2k, 2k+1) of a row with
+    // 16-byte loads and stores (the planes' rows start on 16-byte boundaries
+    // and i = 0 sits at an even column); a row of odd length ends in a single
+    // cell, whose stores are 8 bytes wide.  The values are those of the
+    // single-cell passes: the same operands in the same operations.
+    const int W = NX - 1, Wp = (W + 1) / 2, Np = Wp * (NY - 1);
+    auto ld2 = [](const double *p) { return *reinterpret_cast<const double2 *>(p); };
+    auto st2 = [](double *p, double a, double b) { *reinterpret_cast<double2 *>(p) = make_double2(a, b); };
+    auto direction_pair = [&](int p, bool first, const double *__restrict__ zp, const double *__restrict__ dold,
+                              double *__restrict__ dn, double bt, double al, double &sdad) {
+        const int j = p / Wp, i0 = 2 * (p - j * Wp), i1 = i0 + 1;
+        const bool has1 = i1 < W;
+        const int iw = i0 > 0 ? i0 - 1 : xw, ie = i0 + 2 <= NX - 2 ? i0 + 2 : xe;
+        const int js = j > 0 ? j - 1 : ys, jn = j < NY - 2 ? j + 1 : yn;
+        const ptrdiff_t r = (ptrdiff_t)j * P + i0, rn = (ptrdiff_t)jn * P + i0, rs = (ptrdiff_t)js * P + i0;
+        const ptrdiff_t rw = (ptrdiff_t)j * P + iw, re = (ptrdiff_t)j * P + ie;
+        const double2 oc = ld2(dold + r), on = ld2(dold + rn), os = ld2(dold + rs);
+        const double ow = dold[rw], oe = dold[re];
+        double2 vc = oc, vn = on, vs = os;
+        double vw = ow, ve = oe;
+        if (!first) {
+            const double2 zc = ld2(zp + r), zn = ld2(zp + rn), zs = ld2(zp + rs);
+            const double zw = zp[rw], ze = zp[re];
+            vc = make_double2(zc.x + bt * oc.x, zc.y + bt * oc.y);
+            vn = make_double2(zn.x + bt * on.x, zn.y + bt * on.y);
+            vs = make_double2(zs.x + bt * os.x, zs.y + bt * os.y);
+            vw = zw + bt * ow;
+            ve = ze + bt * oe;
+        }
+        const double2 bxc = ld2(bx + r), byc = ld2(by + r), bys = ld2(by + r - P);
+        const double bxw = bx[r - 1];
+        double cxm, cxp, cym, cyp;
+        face_coeffs(d, i0, bxw, bxc.x, bys.x, byc.x, cxm, cxp, cym, cyp);
+        const double e0 = has1 ? vc.y : ve;
+        const double ad0 = row_weight(d, i0) *
+                           (cxp * (e0 - vc.x) - cxm * (vc.x - vw) + cyp * (vn.x - vc.x) - cym * (vc.x - vs.x));
+        face_coeffs(d, i1, bxc.x, bxc.y, bys.y, byc.y, cxm, cxp, cym, cyp);
+        const double ad1 = row_weight(d, i1) *
+                           (cxp * (ve - vc.y) - cxm * (vc.y - vc.x) + cyp * (vn.y - vc.y) - cym * (vc.y - vs.y));
+        if (has1) {
+            if (DEFER && !first) {
+                const double2 ph = ld2(A.phi + r);
+                st2(A.phi + r, ph.x + al * oc.x, ph.y + al * oc.y);
+            }
+            if (!first) st2(dn + r, vc.x, vc.y);
+            st2(A.Ad + r, ad0, ad1);
+            sdad += vc.x * ad0;
+            sdad += vc.y * ad1;
+        } else {
+            if (DEFER && !first) A.phi[r] = A.phi[r] + al * oc.x;
+            if (!first) dn[r] = vc.x;
+            A.Ad[r] = ad0;
+            sdad += vc.x * ad0;
+        }
+    };
+    auto update_pair = [&](int p, double alpha, double &sgn) {
+        const int j = p / Wp, i0 = 2 * (p - j * Wp);
+        const bool has1 = i0 + 1 < W;
+        const ptrdiff_t r = (ptrdiff_t)j * P + i0;
+        const double2 rr = ld2(A.res + r), aa = ld2(A.Ad + r), mm = ld2(A.M + r);
+        const double rv0 = rr.x - alpha * aa.x, z0 = rv0 * mm.x;
+        const double rv1 = rr.y - alpha * aa.y, z1 = rv1 * mm.y;
+        if (has1) {
+            st2(A.res + r, rv0, rv1);
+            st2(A.z + r, z0, z1);
+            sgn += rv0 * z0;
+            sgn += rv1 * z1;
+        } else {
+            A.res[r] = rv0;
+            A.z[r] = z0;
+            sgn += rv0 * z0;
+        }
+    };
+
     double *dcur = A.dir, *dnxt = A.dir2;
     bool first = true;
     double alpha = 0.0;   // FW: the step of the update phi += alpha d_cur still to be applied
@@ -511,6 +588,9 @@ __device__ __forceinline__ void cg_pressure(const PresArgs &A)
         double sdad = 0.0;
         const double bt = beta, al = alpha;
         const double *dold = dcur;
+        if (PAIR)
+            for (int p = tid; p < Np; p += nth) direction_pair(p, first, A.z, dold, dnxt, bt, al, sdad);
+        else
         for (int q = tid; q < R.n; q += U1 * nth) {
             const int q1 = q + nth;
             const bool two = U1 == 2 && q1 < R.n;
@@ -546,6 +626,9 @@ __device__ __forceinline__ void cg_pressure(const PresArgs &A)
         if (!barrier()) return;
         alpha = gamma / (grid_total(part1) + 1e-30);
         double sgn = 0.0;
+        if (PAIR)
+            for (int p = tid; p < Np; p += nth) update_pair(p, alpha, sgn);
+        else
         for (int q = tid; q < R.n; q += 2 * nth) {
             const int q1 = q + nth;
             const bool two = q1 < R.n;
@@ -604,7 +687,8 @@ __device__ __forceinline__ void cg_pressure(const PresArgs &A)
     if (blockIdx.x == 0 && threadIdx.x == 0) { A.scal->p_iters = iters; A.scal->p_res = sqrt(gamma_new); }
 }
 
-__global__ void __launch_bounds__(512) k_cg_pressure(PresArgs A) { cg_pressure<false, false, 2>(A); }
-__global__ void __launch_bounds__(512, 2) k_cg_pressure_fw(PresArgs A) { cg_pressure<true, true, 1>(A); }
+__global__ void __launch_bounds__(512) k_cg_pressure(PresArgs A) { cg_pressure<false, false, 2, false>(A); }
+__global__ void __launch_bounds__(512, 2) k_cg_pressure_fw(PresArgs A) { cg_pressure<true, true, 1, false>(A); }
+__global__ void __launch_bounds__(512, 2) k_cg_pressure_fwp(PresArgs A) { cg_pressure<true, true, 1, true>(A); }
 
 }  // namespace pvof

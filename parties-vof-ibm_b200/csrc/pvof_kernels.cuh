@@ -267,5 +267,6 @@ __global__ void k_cg_biharmonic(BihArgs A);
 __global__ void k_cg_velocity(VelArgs A);
 __global__ void k_cg_pressure(PresArgs A);
 __global__ void k_cg_pressure_fw(PresArgs A);
+__global__ void k_cg_pressure_fwp(PresArgs A);
 
 }  // namespace pvof
