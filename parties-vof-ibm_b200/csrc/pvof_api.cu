@@ -746,6 +746,8 @@ VelArgs vel_args(pvof_ctx *c, int comp)
     A.maxit = c->p.CG_MAXIT;
     A.partials = c->partials;
     A.scal = c->scal;
+    A.ft = S(c, comp == 0 ? SC_U_FT : SC_V_FT);
+    A.mc = S(c, comp == 0 ? SC_U_MC : SC_V_MC);
     return A;
 }
 

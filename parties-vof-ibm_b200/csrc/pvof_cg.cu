@@ -316,6 +316,7 @@ __global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
         R.ij(q, i, j);
         double dg = vel_diag(d, A.comp, A.rho, A.mu, i, j, A.iRe, A.alpha_dt) + EPS;
         AT_(A.diag, i, j) = dg;
+        vel_weights(d, A.comp, A.rho, A.mu, A.ft, A.mc, i, j, A.i0, A.j0, A.alpha_dt);
         double ad = vel_op(d, A.comp, A.rho, A.mu, i, j, A.iRe, A.alpha_dt, [&](int a, int b) { return AT_(A.x, a, b); });
         double rv = AT_(A.rhs, i, j) - ad;
         AT_(A.r, i, j) = rv;
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
             double dv, ad;
             if (first) {
                 dv = AT_(dold, i, j);
-                ad = vel_op(d, A.comp, A.rho, A.mu, i, j, A.iRe, A.alpha_dt, [&](int a, int b) {
+                ad = vel_op_w(d, A.comp, A.ft, A.mc, A.mu, i, j, A.iRe, [&](int a, int b) {
                     int si, sj;
                     double mul;
                     src_of(A.mcg, NX, NY, a, b, si, sj, mul);
@@ -353,7 +354,7 @@ __global__ void __launch_bounds__(512) k_cg_velocity(VelArgs A)
             } else {
                 dv = AT_(A.z, i, j) + bt * AT_(dold, i, j);
                 AT_(dnxt, i, j) = dv;
-                ad = vel_op(d, A.comp, A.rho, A.mu, i, j, A.iRe, A.alpha_dt, [&](int a, int b) {
+                ad = vel_op_w(d, A.comp, A.ft, A.mc, A.mu, i, j, A.iRe, [&](int a, int b) {
                     int si, sj;
                     double mul;
                     src_of(A.mcg, NX, NY, a, b, si, sj, mul);

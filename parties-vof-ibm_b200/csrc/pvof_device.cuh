@@ -240,6 +240,68 @@ __device__ __forceinline__ double vel_diag(const Dom &d, int comp, const double 
     }
 }
 
+// The quotients of vel_op, stored once per solve: the time term
+// ft = 0.5 (rho_P + rho_W|S) / (alpha dt) per cell and the harmonic mean of
+// the viscosity at the cell's upper corner (u: north, v: east), mc.  The
+// lower corner of a cell is the upper corner of the neighbour below (u) or
+// to the west (v): the same expression with the same operands, so
+// mc(i, j-1) (u) and mc(i-1, j) (v) are vel_op's mu_ym and mu_xm bit for bit.
+// The cell at the start of the range also stores its lower corner.
+__device__ __forceinline__ void vel_weights(const Dom &d, int comp, const double *__restrict__ rho,
+                                            const double *__restrict__ mu, double *ft, double *mc, int i, int j,
+                                            int i0, int j0, double alpha_dt)
+{
+    const int P = d.P;
+    if (comp == 0) {
+        AT_(ft, i, j) = 0.5 * (AT_(rho, i, j) + AT_(rho, i - 1, j)) / alpha_dt;
+        AT_(mc, i, j) = harm(avg2(AT_(mu, i - 1, j + 1), AT_(mu, i, j + 1)), avg2(AT_(mu, i - 1, j), AT_(mu, i, j)));
+        if (j == j0)
+            AT_(mc, i, j - 1) =
+                harm(avg2(AT_(mu, i - 1, j), AT_(mu, i, j)), avg2(AT_(mu, i - 1, j - 1), AT_(mu, i, j - 1)));
+    } else {
+        AT_(ft, i, j) = 0.5 * (AT_(rho, i, j) + AT_(rho, i, j - 1)) / alpha_dt;
+        AT_(mc, i, j) = harm(avg2(AT_(mu, i + 1, j - 1), AT_(mu, i + 1, j)), avg2(AT_(mu, i, j - 1), AT_(mu, i, j)));
+        if (i == i0)
+            AT_(mc, i - 1, j) =
+                harm(avg2(AT_(mu, i, j - 1), AT_(mu, i, j)), avg2(AT_(mu, i - 1, j - 1), AT_(mu, i - 1, j)));
+    }
+}
+
+// vel_op with its quotients read from vel_weights' planes: the same value
+// without the three divisions
+template <class Get>
+__device__ __forceinline__ double vel_op_w(const Dom &d, int comp, const double *__restrict__ ft,
+                                           const double *__restrict__ mc, const double *__restrict__ mu, int i,
+                                           int j, double iRe, Get x)
+{
+    const int P = d.P;
+    double op = 0.0;
+    double c = x(i, j);
+    double Ax = AT_(ft, i, j) * c;
+    if (comp == 0) {
+        double mu_xp = AT_(mu, i, j), mu_xm = AT_(mu, i - 1, j);
+        double mu_yp = AT_(mc, i, j), mu_ym = AT_(mc, i, j - 1);
+        double fxp = mu_xp * (x(i + 1, j) - c) * d.m.idx_u[i];
+        double fxm = mu_xm * (c - x(i - 1, j)) * d.m.idx_u[i - 1];
+        double fyp = mu_yp * (x(i, j + 1) - c) * d.m.idy_c[j];
+        double fym = mu_ym * (c - x(i, j - 1)) * d.m.idy_c[j - 1];
+        op += iRe * u_cv_x_div(d, i, fxp, fxm);
+        op += iRe * (fyp - fym) * d.m.idy_v[j];
+        op += axisym_ur_term(d, i, iRe * 0.5 * (mu_xp + mu_xm), c);
+        return Ax - op;
+    } else {
+        double mu_yp = AT_(mu, i, j), mu_ym = AT_(mu, i, j - 1);
+        double mu_xp = AT_(mc, i, j), mu_xm = AT_(mc, i - 1, j);
+        double fxp = mu_xp * (x(i + 1, j) - c) * d.m.idx_c[i];
+        double fxm = mu_xm * (c - x(i - 1, j)) * d.m.idx_c[i - 1];
+        double fyp = mu_yp * (x(i, j + 1) - c) * d.m.idy_v[j];
+        double fym = mu_ym * (c - x(i, j - 1)) * d.m.idy_v[j - 1];
+        op += iRe * v_cv_x_div(d, i, fxp, fxm);
+        op += iRe * (fyp - fym) * d.m.idy_c[j - 1];
+        return Ax - op;
+    }
+}
+
 // matVec (Eulerian/lsolver/msolve_cg.c:255-493), diffuse VOF, at (i,j)
 template <class Get>
 __device__ __forceinline__ double vel_op(const Dom &d, int comp, const double *__restrict__ rho,

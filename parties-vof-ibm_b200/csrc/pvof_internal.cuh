@@ -86,7 +86,7 @@ enum Scratch {
     SC_P_RES, SC_P_D, SC_P_AD, SC_P_MINV,
     SC_U_R, SC_U_D, SC_U_AD, SC_U_DIAG, SC_V_R, SC_V_D, SC_V_AD, SC_V_DIAG,
     SC_OLD, SC_U_D2, SC_V_D2, SC_P_D2, SC_U_Z, SC_V_Z, SC_P_Z, SC_SNAP, SC_PHI_PREV, SC_PHI_PREV1, SC_PHI_PREV2, SC_PHI_OLD, SC_PHI_OLD1, SC_PHI_OLD2, SC_P_HAT,
-    SC_P_BX, SC_P_BY,
+    SC_P_BX, SC_P_BY, SC_U_FT, SC_U_MC, SC_V_FT, SC_V_MC,
     SC_COUNT
 };
 

@@ -34,6 +34,7 @@ struct VelArgs {
     int maxit;
     double *partials;
     DevScalars *scal;
+    double *ft = nullptr, *mc = nullptr;   // time-term and corner-viscosity planes (k_cg_velocity)
 };
 
 struct PresArgs {
