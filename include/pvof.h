@@ -448,6 +448,15 @@ int pvof_clamp_mass_total(const pvof_ctx *ctx, double *total);
  * to rounding (their inner products are summed in different orders).  Waits
  * for the context's stream and drops its captured substep graphs. */
 int pvof_set_cluster_solvers(pvof_ctx *ctx, int enabled);
+/* No counterpart in the reference: how the grid-wide pressure solve
+ * (Pressure_solve_cg, psolve_cg.c:130-293, on ranges larger than one
+ * cluster) assigns cells to threads.  -1 (the default): pairs of
+ * neighbouring cells with 16-byte accesses once every resident thread has at
+ * least two cells, single cells below that; 1: pairs at every size; 0:
+ * single cells at every size.  The same iteration either way; results agree
+ * to rounding (the inner products are summed in different orders).  Waits
+ * for the context's stream and drops its captured substep graphs. */
+int pvof_set_pressure_pairs(pvof_ctx *ctx, int mode);
 
 /* No counterpart in the reference: the host-computed table of the spectral
  * pressure preconditioner's tridiagonal solves for an N x M grid (x spacing

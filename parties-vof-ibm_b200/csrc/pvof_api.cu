@@ -944,6 +944,7 @@ int p_solve_spectral(pvof_ctx *c)
 // 8.7 with pairs).
 bool grid_pressure_pairs(const pvof_ctx *c)
 {
+    if (c->pressure_pairs >= 0) return c->pressure_pairs != 0;
     const long long n = (long long)(c->dom.NX - 1) * (c->dom.NY - 1);
     return n >= 2LL * c->coop_blocks_of[PVOF_SOLVER_PRESSURE] * COOP_THREADS;
 }
@@ -1783,6 +1784,7 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     pvof_ctx *c = new pvof_ctx();
     std::memset(static_cast<Ctx *>(c), 0, sizeof(Ctx));
     c->use_graphs = 1;
+    c->pressure_pairs = -1;
     c->g = *grid;
     c->p = *params;
     c->device = device;
@@ -2236,6 +2238,17 @@ int pvof_clamp_mass_total(const pvof_ctx *c, double *total)
 {
     if (!c || !total) return set_err(PVOF_EINVAL, "null context or output");
     *total = c->clamp_total;
+    return PVOF_OK;
+}
+
+int pvof_set_pressure_pairs(pvof_ctx *c, int mode)
+{
+    ENTER(c);
+    if (mode < -1 || mode > 1) return set_err(PVOF_EINVAL, "pvof_set_pressure_pairs: mode -1, 0 or 1");
+    // the captured substeps hold the old solver launches: wait for them and drop them
+    CK(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
+    c->pressure_pairs = mode;
     return PVOF_OK;
 }
 

@@ -161,6 +161,7 @@ struct Ctx {
     int cgs_p_threads, cgs_v_threads;   // their threads per CTA
     StripPlan cgs_p_fit, cgs_v_fit;     // the cluster plans that fit this grid (kept for pvof_set_cluster_solvers)
     int vel_one_cluster;     // momentum solve as u then v on one cluster (batched runs)
+    int pressure_pairs;      // grid-wide pressure solve over pairs of cells: -1 by size, 0 never, 1 always
     int phi_prev_mask;       // stages whose last correction is kept in SC_PHI_PREV + stage
     int phi_old_mask;        // stages whose correction one step before that is in SC_PHI_OLD + stage
     // learned warm start (pvof_cnn.cu): FP32 and BF16 parameters, the input

@@ -128,7 +128,7 @@ EXPORTS = [
     "pvof_launch_count", "pvof_timer_start", "pvof_timer_stop", "pvof_flush_l2",
     "pvof_set_solver_timing", "pvof_solver_timing", "pvof_set_autotune", "pvof_autotune_active",
     "pvof_autotune_entries", "pvof_autotune_entry", "pvof_solver_kernel", "pvof_set_graphs", "pvof_graph_replays", "pvof_spectral_tables",
-    "pvof_set_cluster_solvers", "pvof_clamp_mass_total",
+    "pvof_set_cluster_solvers", "pvof_set_pressure_pairs", "pvof_clamp_mass_total",
     "pvof_Pressure_solve_cg_noalloc", "pvof_noalloc_last_error",
     "pvof_set_particles", "pvof_Lagrangian_flag_points", "pvof_particle_entries", "pvof_particle_forces",
     "pvof_particle_markers", "pvof_VOF_DIFFUSE_compute_C_S", "pvof_Velocity_solve_explicit",

@@ -73,6 +73,7 @@ def load():
     L.pvof_graph_replays.argtypes = [V]
     L.pvof_graph_replays.restype = C.c_longlong
     L.pvof_set_cluster_solvers.argtypes = [V, C.c_int]
+    L.pvof_set_pressure_pairs.argtypes = [V, C.c_int]
     L.pvof_clamp_mass_total.argtypes = [V, P(C.c_double)]
     L.pvof_solver_timing.argtypes = [V, C.c_int, P(C.c_double), P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]
     L.pvof_solver_kernel.argtypes = [V, C.c_int]
@@ -300,6 +301,10 @@ class Solver:
     def set_cluster_solvers(self, on):
         """Cluster-resident solvers where they fit (default), or the grid-wide ones."""
         check(load().pvof_set_cluster_solvers(self.h, 1 if on else 0), "pvof_set_cluster_solvers")
+
+    def set_pressure_pairs(self, mode):
+        """Grid-wide pressure solve over pairs of cells: -1 by size (default), 0 never, 1 always."""
+        check(load().pvof_set_pressure_pairs(self.h, int(mode)), "pvof_set_pressure_pairs")
 
     def solver_kernel(self, solver):
         """Name of the kernel that runs solver abi.SOLVER_* in this context."""

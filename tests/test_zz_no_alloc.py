@@ -39,6 +39,7 @@ def test_noalloc_pressure_solve_matches_context_solve(kind):
     grid, params, planes = _case(kind)
     g = runtime.Solver(grid, params, device=0)
     g.set_cluster_solvers(False)   # the grid-wide kernel, as the entry point uses
+    g.set_pressure_pairs(0)        # one cell per thread and trip, the entry point's summation order
     g.set_planes(planes)
     g.initialize()
     g.set_stage(1, 1e-4)
