@@ -385,6 +385,108 @@ def poisson_case(args, device):
                          "frac": gbs / peak, "alg_bytes_per_cell_iter": ALG_BYTES[2]}}
 
 
+def box_reference(grid_str, steps, timeout=3600):
+    """The reference's 3D build (oracle/_ref/ref_rt3d_st) on a smaller box of
+    the same case for ``steps`` steps on one host core; (cell-updates/s,
+    seconds, cells) or None."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle as po  # checker / CPU baseline only
+    from pvof import cases
+    if not os.path.exists(po.ref_binary("rt3d_st")):
+        return None
+    n = [int(v) for v in grid_str.lower().split("x")]
+    grid, params, fields = box_setup(n, 20000)
+    with tempfile.TemporaryDirectory() as wd:
+        cp = po.run_reference("rt3d_st", wd, grid, params, fields, steps, BOX_DT, 0, timeout=timeout)
+    for line in cp.stdout.splitlines():
+        if line.startswith("REF_TIMING"):
+            kv = dict(x.split("=") for x in line.split()[1:])
+            secs = float(kv["seconds"])
+            return int(kv["cells"]) * int(kv["steps"]) / secs, secs, int(kv["cells"])
+    return None
+
+
+BOX_DT = 1e-4
+
+
+def box_setup(n, maxit):
+    """The 3D box of the precision form's configuration: x, z periodic, no-slip
+    walls in y, side 2 along x with cubic cells, a liquid layer under gas with
+    a seeded 16-mode interface (cases.interface_box, seed 3), density ratio
+    1e-3, viscosity ratio 1e-2, Re 1000, We 100, Cn 0.005."""
+    from pvof import cases
+    return cases.interface_box(n[0], n[1], n[2], L=2.0, seed=3, Cn=0.005, rho_ratio=1e-3, mu_ratio=1e-2,
+                               Re=1000.0, We=100.0, P_CG_MAXIT=maxit)
+
+
+def box_case(args, device):
+    """The plain FP64 path in the 3D mode on --box-grid (default 256^3, the
+    only configuration whose fields do not fit in L2): --box-warmup untimed
+    steps, --box-steps timed steps (device time, L2 flushed before each), one
+    more step with per-solver events; the pressure Jacobi-PCG's achieved
+    bandwidth counts 56 algorithmic bytes per cell and iteration; the
+    reference's 3D build on a --box-ref-grid box for --box-ref-steps steps."""
+    from pvof import runtime
+    n = [int(v) for v in args.box_grid.lower().split("x")]
+    grid, params, fields = box_setup(n, args.box_maxit)
+    cells = n[0] * n[1] * n[2]
+    s = runtime.Solver(grid, params, device=device)
+    s.set_fields({k: fields[k] for k in ("F", "U", "V", "W", "P")})
+    del fields
+    s.initialize()
+    m0 = s.liquid_mass()
+    s.run_steps(max(0, args.box_warmup), BOX_DT)
+    nsteps = max(1, args.box_steps)
+    l0, ms = s.launch_count(), 0.0
+    for _ in range(nsteps):
+        s.flush_l2()
+        s.timer_start()
+        s.run_steps(1, BOX_DT)
+        ms += s.timer_stop()
+    launches = s.launch_count() - l0
+    s.set_solver_timing(True)
+    s.flush_l2()
+    s.timer_start()
+    st = s.run_steps(1, BOX_DT)
+    step_ms = s.timer_stop()
+    t = [s.solver_timing(k) for k in range(3)]
+    s.set_solver_timing(False)
+    m1 = s.liquid_mass()
+    clamp = s.clamp_mass_total()
+    peak, peak_kind = measured_peak()
+    names = ["biharmonic CG", "velocity PCG (u, v, w)", "pressure Jacobi-PCG"]
+    out = {"case": "3D box %s, x and z periodic, no-slip walls in y, liquid layer under gas with a seeded 16-mode "
+                   "interface (seed 3), density ratio 1e-3, viscosity ratio 1e-2, Re 1000, We 100, Cn 0.005, "
+                   "dt %g, plain FP64" % (args.box_grid, BOX_DT),
+           "value": cells * nsteps / (ms * 1e-3), "unit": UNIT, "steps": nsteps, "warmup": args.box_warmup,
+           "ms_per_step": ms / nsteps, "launches_per_step": launches / nsteps, "cells": cells,
+           "l2": "flushed before every timed step", "timing_step_ms": step_ms,
+           "solvers": {names[k]: {"ms": t[k]["ms"], "iterations": t[k]["iterations"],
+                                  "us_per_iteration": 1e3 * t[k]["ms"] / max(1, t[k]["iterations"]),
+                                  "share": t[k]["ms"] / step_ms} for k in range(3)},
+           "last_substep": {"ch_iters": st.ch_iters, "u_iters": st.u_iters, "v_iters": st.v_iters,
+                            "w_iters": st.w_iters, "p_iters": st.p_iters, "poisson_passes": st.poisson_passes,
+                            "div_max": st.div_max},
+           "mass": {"initial": m0, "final": m1, "clamp_total": clamp,
+                    "rel_change_net_of_clamp": (m1 - m0 - clamp) / m0}}
+    for k, bpc in ((0, ALG_BYTES[0]), (2, ALG_BYTES[2])):
+        if t[k]["ms"] > 0:
+            gbs = bpc * t[k]["cell_iters"] / (t[k]["ms"] * 1e-3) / 1e9
+            out["solvers"][names[k]]["roofline"] = {"bound": "hbm", "achieved": gbs, "peak": peak,
+                                                    "peak_kind": peak_kind, "unit": "GB/s", "frac": gbs / peak,
+                                                    "alg_bytes_per_cell_iter": bpc}
+    s.close()
+    if args.box_ref_steps > 0:
+        r = box_reference(args.box_ref_grid, args.box_ref_steps)
+        if r is not None:
+            out["cpu_reference"] = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
+                                    "sample": "%d time step(s) of the same case on a %s box (%d cells) by the "
+                                              "single-rank 3D reference build, %.1f s" % (args.box_ref_steps,
+                                                                                       args.box_ref_grid, r[2], r[1])}
+            out["vs_cpu_reference"] = out["value"] / r[0]
+    return out
+
+
 # the axisymmetric benchmark case: a bubble (R 0.5 at z = 1) rising towards a
 # fixed sphere (R 0.25 at z = 2.5) on the axis, 256 x 512 cells over
 # r in [0, 2], z in [0, 4]
@@ -1014,6 +1116,12 @@ def run_ours(args):
             poisson = poisson_case(args, local)
         except Exception as e:   # noqa: BLE001
             poisson = {"error": "%s: %s" % (type(e).__name__, e)}
+    box = None
+    if args.box:
+        try:
+            box = box_case(args, local)
+        except Exception as e:   # noqa: BLE001
+            box = {"error": "%s: %s" % (type(e).__name__, e)}
     large = None
     if args.large:
         try:
@@ -1066,6 +1174,8 @@ def run_ours(args):
             line["large"] = large
         if axisym is not None:
             line["axisym"] = axisym
+        if box is not None:
+            line["box"] = box
         if poisson is not None:
             line["poisson"] = poisson
         if learned is not None:
@@ -1123,6 +1233,14 @@ def main():
     ap.add_argument("--poisson-grid", default="2048x2048")
     ap.add_argument("--poisson-maxit", type=int, default=3000)
     ap.add_argument("--poisson-reps", type=int, default=3)
+    ap.add_argument("--box", action="store_true",
+                    help="also time the 3D mode on --box-grid (the precision form's 256^3 box, plain FP64)")
+    ap.add_argument("--box-grid", default="256x256x256")
+    ap.add_argument("--box-steps", type=int, default=2)
+    ap.add_argument("--box-warmup", type=int, default=1)
+    ap.add_argument("--box-maxit", type=int, default=20000)
+    ap.add_argument("--box-ref-grid", default="32x32x32")
+    ap.add_argument("--box-ref-steps", type=int, default=1)
     ap.add_argument("--axisym", action="store_true",
                     help="also time the axisymmetric bubble-and-sphere case (256x512) and the reference on it")
     ap.add_argument("--axisym-steps", type=int, default=10)

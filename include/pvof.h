@@ -17,6 +17,16 @@
  * reads the k = 0 plane of the block and download writes it to every plane
  * of the G range (the reference keeps those planes identical).
  *
+ * The 3D mode (PVOF_GEOM_3D, the reference built without TWOD_* flags) keeps
+ * every plane.  It supports x and z periodic with walls in y and no solids,
+ * and the whole-substep entry points: pvof_create/destroy, the field copies,
+ * pvof_set_stage, pvof_initialize, pvof_substep, pvof_run_steps,
+ * pvof_liquid_mass and the measurement calls (launch count, timers, L2
+ * flush, clamp total).  Other entry points return PVOF_EINVAL on a 3D
+ * context.  In 3D the fields C_G, rho and mu are download-only (they are
+ * functions of C_L), *_EXPLICIT and *_VISC_EXPLICIT equal their _OLD copies
+ * after a substep, and CH_RHS_CUR equals CH_RHS_N.
+ *
  * Routine entry points keep the reference's names with a pvof_ prefix.  The
  * reference passes the RK stage and dt through Parameters (which_stage, dt);
  * here they are set once per substep with pvof_set_stage().
@@ -37,7 +47,7 @@
 extern "C" {
 #endif
 
-#define PVOF_ABI_VERSION 3
+#define PVOF_ABI_VERSION 4
 
 /* error codes */
 #define PVOF_OK 0
@@ -148,6 +158,10 @@ enum pvof_field {
     PVOF_F_FSIG_OLD_X, PVOF_F_FSIG_OLD_Y, PVOF_F_FSIG_NEW_X, PVOF_F_FSIG_NEW_Y,
     /* solid normals of the contact-line projection (VolumeFraction nx_IBM, ny_IBM) */
     PVOF_F_NX_IBM, PVOF_F_NY_IBM,
+    /* the 3D mode's w momentum arrays and z surface-tension force (no-ghost) */
+    PVOF_F_W_EXPLICIT, PVOF_F_W_EXPLICIT_OLD, PVOF_F_W_IMPLICIT,
+    PVOF_F_W_VISC_EXPLICIT, PVOF_F_W_VISC_EXPLICIT_OLD, PVOF_F_W_RHS,
+    PVOF_F_FSIG_OLD_Z, PVOF_F_FSIG_NEW_Z,
     PVOF_F_COUNT
 };
 
@@ -165,6 +179,8 @@ typedef struct pvof_stats {
     double div_max;        /* Pressure_compute_velocity_divergence */
     double clamp_mass;     /* liquid mass changed by the C_L clamp over the physical cells
                               (VOF_DIFFUSE.c:1093-1127) */
+    int w_iters;           /* w-velocity PCG iterations (3D mode; 0 in 2D) */
+    double w_rms;
 } pvof_stats;
 
 typedef struct pvof_ctx pvof_ctx;

@@ -1193,7 +1193,8 @@ static double pressure_divergence(orc_t *o)
 
 static int is_ng(int field)
 {
-    return field >= PVOF_F_U_EXPLICIT && field <= PVOF_F_FSIG_NEW_Y;
+    return (field >= PVOF_F_U_EXPLICIT && field <= PVOF_F_FSIG_NEW_Y) ||
+           (field >= PVOF_F_W_EXPLICIT && field <= PVOF_F_FSIG_NEW_Z);
 }
 
 int orc_create(const pvof_grid_desc *grid, const pvof_params *params, orc_t **out)

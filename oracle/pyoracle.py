@@ -190,7 +190,7 @@ def run_reference(case, workdir, grid, params, planes, nsteps, dt, dump_every=1,
     which leaves out the first ``warmup`` of the ``nsteps`` steps)."""
     os.makedirs(workdir, exist_ok=True)
     write_parties_inp(os.path.join(workdir, "parties.inp"), grid, params)
-    names = {"F": "init_C.bin", "U": "init_u.bin", "V": "init_v.bin", "P": "init_p.bin"}
+    names = {"F": "init_C.bin", "U": "init_u.bin", "V": "init_v.bin", "W": "init_w.bin", "P": "init_p.bin"}
     for k, fn in names.items():
         if k in planes:
             np.ascontiguousarray(planes[k], dtype="<f8").tofile(os.path.join(workdir, fn))

@@ -14,10 +14,12 @@
  *
  * Usage: ref_driver <case_dir> <nsteps> <dt> <dump_every> [substeps] [warmup]
  *   <case_dir>/parties.inp            INI parameters (reference format)
- *   <case_dir>/init_{C,u,v,p}.bin     doubles on the G range of one plane,
+ *   <case_dir>/init_{C,u,v,w,p}.bin   doubles on the G range of one plane,
  *                                     [j][i] order, i fastest, NX*NY values
- *                                     (NX = NXM+1, NY = NYM+1); replicated
- *                                     over every k plane (2D cases)
+ *                                     (NX = NXM+1, NY = NYM+1), replicated
+ *                                     over every k plane (2D cases); or on the
+ *                                     whole G range, [k][j][i], NX*NY*NZ
+ *                                     values (3D cases)
  *   outputs in <case_dir>/out/: s<step>_<field>.bin, each the full ghosted
  *   block of the field (L ranges, [k][j][i], i fastest); "substeps" > 0 also
  *   dumps after every RK substep as s<step>_<rk>_<field>.bin.
@@ -97,6 +99,31 @@ static void inject(double ***a, const double *plane, MAC_grid *g)
                 a[k][j][i] = plane[(size_t)j * NX + i];
 }
 
+/* An init file of NX*NY values (one plane, copied to every k plane) or of
+ * NX*NY*NZ values ([k][j][i] over the whole G range); returns 0 if absent. */
+static int inject_file(double ***a, const char *name, MAC_grid *g)
+{
+    FILE *f = fopen(name, "rb");
+    if (!f) return 0;
+    fseek(f, 0, SEEK_END);
+    long bytes = ftell(f);
+    fclose(f);
+    size_t n2 = (size_t)g->NX * (size_t)g->NY, n3 = n2 * (size_t)g->NZ;
+    if ((size_t)bytes != n3 * sizeof(double) || n3 == n2) {
+        double *plane = read_plane(name, (int)n2);
+        inject(a, plane, g);
+        free(plane);
+        return 1;
+    }
+    double *buf = read_plane(name, (int)n3);
+    for (int k = g->G_Ks; k < g->G_Ke; k++)
+        for (int j = 0; j < g->NY; j++)
+            for (int i = 0; i < g->NX; i++)
+                a[k][j][i] = buf[((size_t)(k - g->G_Ks) * g->NY + j) * g->NX + i];
+    free(buf);
+    return 1;
+}
+
 static void dump(double ***a, MAC_grid *g, const char *path)
 {
     size_t n = (size_t)(g->L_Ie - g->L_Is) * (size_t)(g->L_Je - g->L_Js) * (size_t)(g->L_Ke - g->L_Ks);
@@ -135,10 +162,18 @@ static void dump_state(Cart3d_bag *db, const char *tag)
     DUMPNG(db->v->ng_explicit_old, "v_explicit_old");
     DUMPNG(db->u->ng_visc_explicit_old, "u_visc_explicit_old");
     DUMPNG(db->v->ng_visc_explicit_old, "v_visc_explicit_old");
+#ifndef TWOD_MODE
+    DUMP(db->w->data, "w");
+    DUMPNG(db->w->ng_explicit_old, "w_explicit_old");
+    DUMPNG(db->w->ng_visc_explicit_old, "w_visc_explicit_old");
+#endif
 #ifdef SURFACE_TENSION
     DUMP(vof->psi_LG, "psi_LG");
     DUMPNG(vof->f_sigma_old_x, "f_sigma_old_x");
     DUMPNG(vof->f_sigma_old_y, "f_sigma_old_y");
+#ifndef TWOD_MODE
+    DUMPNG(vof->f_sigma_old_z, "f_sigma_old_z");
+#endif
 #endif
 #undef DUMP
 #undef DUMPNG
@@ -179,14 +214,11 @@ int main(int argc, char **argv)
     db->vof = VoF_create(grid, params);
     db->lag = NULL;
 
-    int NX = grid->NX, NY = grid->NY;
-    double *plane;
-    if (!(plane = read_plane("init_C.bin", NX * NY))) die("missing init_C.bin");
-    inject(db->vof->F, plane, grid);
-    free(plane);
-    if ((plane = read_plane("init_u.bin", NX * NY))) { inject(db->u->data, plane, grid); free(plane); }
-    if ((plane = read_plane("init_v.bin", NX * NY))) { inject(db->v->data, plane, grid); free(plane); }
-    if ((plane = read_plane("init_p.bin", NX * NY))) { inject(db->p->p_data, plane, grid); free(plane); }
+    if (!inject_file(db->vof->F, "init_C.bin", grid)) die("missing init_C.bin");
+    inject_file(db->u->data, "init_u.bin", grid);
+    inject_file(db->v->data, "init_v.bin", grid);
+    inject_file(db->w->data, "init_w.bin", grid);
+    inject_file(db->p->p_data, "init_p.bin", grid);
 #if defined(PVOF_BRIDGE_DRIVER) && PVOF_BRIDGE_DRIVER == 2
     /* the bridged routines below work on the device copy from here on */
     params->dt = dt;

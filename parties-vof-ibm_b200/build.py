@@ -13,13 +13,13 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "pvof", "libpvof.so")
-SOURCES = ["pvof_api.cu", "pvof_kernels.cu", "pvof_cg.cu", "pvof_cgs.cu", "pvof_ibm.cu", "pvof_fft.cu", "pvof_mcl.cu", "pvof_cnn.cu", "pvof_noalloc.cu", "pvof_spec.cu", "pvof_advect.cu"]
-HEADERS = ["pvof_internal.cuh", "pvof_device.cuh", "pvof_kernels.cuh", "pvof_particles.cuh",
+SOURCES = ["pvof_api.cu", "pvof_kernels.cu", "pvof_cg.cu", "pvof_cgs.cu", "pvof_ibm.cu", "pvof_fft.cu", "pvof_mcl.cu", "pvof_cnn.cu", "pvof_noalloc.cu", "pvof_spec.cu", "pvof_advect.cu", "pvof_3d.cu"]
+HEADERS = ["pvof_internal.cuh", "pvof_device.cuh", "pvof_kernels.cuh", "pvof_particles.cuh", "pvof_3d.cuh", "pvof_3d_api.h",
            os.path.join("..", "..", "include", "pvof.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-lineinfo", "-O3", "--fmad=false", "-std=c++17",
+    "-lineinfo", "-O3", "--fmad=false", "-std=c++17", "--extended-lambda",
     "-Xcompiler", "-fPIC", "-shared",
 ]
 

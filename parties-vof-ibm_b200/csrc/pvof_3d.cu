@@ -1,0 +1,604 @@
+// CUDA executor of the 3D mode and its entry points (called from the C ABI
+// in pvof_api.cu when a context is created with PVOF_GEOM_3D).
+//
+// Launch shapes: a box of cells is walked row by row, one warp per (j,k)
+// row and 32 consecutive i per step, so every field access of a warp is one
+// coalesced run along i; grids are capped at a multiple of the SM count and
+// stride over the remaining rows.  Reductions write one partial per block
+// (a fixed grid of at most NBR blocks) and a one-block scalar kernel adds
+// the partials in a fixed order, so every sum is the same from run to run.
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "pvof_3d.cuh"
+#include "pvof_3d_api.h"
+
+namespace pvof3 {
+
+constexpr int TPB = 256;
+constexpr int WPB = TPB / 32;
+constexpr int NBR = 148 * 8;        // most blocks of a reduction
+constexpr int NBC = 148 * 16;       // most blocks of a cell-wise pass
+
+thread_local std::string g_err3;
+const char *last_error() { return g_err3.c_str(); }
+static int fail(int code, const std::string &m)
+{
+    g_err3 = m;
+    return code;
+}
+
+template <class F>
+__global__ void __launch_bounds__(TPB) k3_cells(Range r, const int *gate, F f)
+{
+    if (gate && *gate == 0) return;
+    const int nj = r.j1 - r.j0;
+    const long long nrows = (long long)nj * (r.k1 - r.k0);
+    const int lane = threadIdx.x & 31;
+    for (long long row = (long long)blockIdx.x * WPB + (threadIdx.x >> 5); row < nrows; row += (long long)gridDim.x * WPB) {
+        const int j = r.j0 + (int)(row % nj), k = r.k0 + (int)(row / nj);
+        for (int i = r.i0 + lane; i < r.i1; i += 32) f(i, j, k);
+    }
+}
+
+template <int N, bool MAX, class F>
+__global__ void __launch_bounds__(TPB) k3_reduce(Range r, const int *gate, double *part, F f)
+{
+    __shared__ double sh[WPB][N];
+    if (gate && *gate == 0) return;
+    double acc[N];
+#pragma unroll
+    for (int q = 0; q < N; q++) acc[q] = 0.0;
+    const int nj = r.j1 - r.j0;
+    const long long nrows = (long long)nj * (r.k1 - r.k0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (long long row = (long long)blockIdx.x * WPB + warp; row < nrows; row += (long long)gridDim.x * WPB) {
+        const int j = r.j0 + (int)(row % nj), k = r.k0 + (int)(row / nj);
+        for (int i = r.i0 + lane; i < r.i1; i += 32) {
+            const Vec<N> t = f(i, j, k);
+#pragma unroll
+            for (int q = 0; q < N; q++) acc[q] = MAX ? fmax(acc[q], t.v[q]) : acc[q] + t.v[q];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < N; q++) {
+        double a = acc[q];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double b = __shfl_down_sync(0xffffffffu, a, o);
+            a = MAX ? fmax(a, b) : a + b;
+        }
+        if (lane == 0) sh[warp][q] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < N) {
+        double a = sh[0][threadIdx.x];
+        for (int w = 1; w < WPB; w++) a = MAX ? fmax(a, sh[w][threadIdx.x]) : a + sh[w][threadIdx.x];
+        part[(size_t)blockIdx.x * 4 + threadIdx.x] = a;
+    }
+}
+
+struct Pend {
+    int nb[NSLOT], nq[NSLOT], mx[NSLOT];
+    unsigned mask;
+};
+
+template <class F>
+__global__ void __launch_bounds__(TPB) k3_scalar(const double *part, Pend pd, const int *gate, Sc3 *sc, F f)
+{
+    __shared__ double sh[TPB];
+    if (gate && *gate == 0) return;
+    for (int s = 0; s < NSLOT; s++) {
+        if (!(pd.mask & (1u << s))) continue;
+        for (int q = 0; q < pd.nq[s]; q++) {
+            double a = 0.0;
+            for (int b = threadIdx.x; b < pd.nb[s]; b += TPB) {
+                const double v = part[((size_t)s * NBR + b) * 4 + q];
+                a = pd.mx[s] ? fmax(a, v) : a + v;
+            }
+            sh[threadIdx.x] = a;
+            __syncthreads();
+            for (int w = TPB / 2; w > 0; w >>= 1) {
+                if (threadIdx.x < w) sh[threadIdx.x] = pd.mx[s] ? fmax(sh[threadIdx.x], sh[threadIdx.x + w]) : sh[threadIdx.x] + sh[threadIdx.x + w];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) sc->sum[s][q] = sh[0];
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) f(sc);
+}
+
+// host block (reference layout) <-> padded field
+__global__ void k3_unpack(Dom3 d, double *fld, const double *blk, int ng)
+{
+    const int nx = ng ? d.NX : d.NX + 2 * NG, ny = ng ? d.NY : d.NY + 2 * NG, nz = ng ? d.NZ : d.NZ + 2 * NG;
+    const int o = ng ? 0 : NG;
+    const long long n = (long long)nx * ny * nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % nx), j = (int)((t / nx) % ny), k = (int)(t / ((long long)nx * ny));
+        fld[at(d, i - o, j - o, k - o)] = blk[t];
+    }
+}
+
+// the reference's array after its ghost update, into the host block layout;
+// xf: 0 the field, 1 C_G, 2 rho, 3 mu of C_L
+template <int K>
+__global__ void k3_pack(Dom3 d, Phase ph, const double *fld, double *blk, int ng, int xf)
+{
+    const int nx = ng ? d.NX : d.NX + 2 * NG, ny = ng ? d.NY : d.NY + 2 * NG, nz = ng ? d.NZ : d.NZ + 2 * NG;
+    const int o = ng ? 0 : NG;
+    const long long n = (long long)nx * ny * nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % nx) - o, j = (int)((t / nx) % ny) - o, k = (int)(t / ((long long)nx * ny)) - o;
+        double v = ng ? fld[at(d, i, j, k)] : rd<K>(d, fld, i, j, k);
+        if (xf == 1) v = ph.cg(v);
+        else if (xf == 2) v = ph.rho(v);
+        else if (xf == 3) v = ph.mu(v);
+        // rho and mu are computed on the G range only: the positions their
+        // ghost update leaves alone keep the zeros of the allocation
+        if (xf >= 2 && !written<K>(d, i, j, k)) v = 0.0;
+        blk[t] = v;
+    }
+}
+
+__global__ void k3_flush(double *buf, size_t n, double v)
+{
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) buf[t] = v;
+}
+
+struct GpuExec {
+    cudaStream_t stream = nullptr;
+    Sc3 *sc = nullptr;         // device scalars
+    Sc3 *sc_host = nullptr;    // pinned mirror
+    int *int_host = nullptr;   // pinned word
+    double *part = nullptr;    // NSLOT x NBR x 4 partial sums
+    Pend pend{};
+    long long launches = 0;
+    cudaError_t err = cudaSuccess;
+    size_t field_elems = 0;    // doubles per padded field
+    long long origin = 0;      // offset of element (0,0,0) in a field
+    // per-solver device time (pvof_set_solver_timing): events around each solve
+    int timing = 0;
+    cudaEvent_t tev[2] = {nullptr, nullptr};
+    double sol_ms[3] = {0.0, 0.0, 0.0};
+
+    void tic()
+    {
+        if (timing) cudaEventRecord(tev[0], stream);
+    }
+    void toc(int solver)
+    {
+        if (!timing) return;
+        float t = 0.f;
+        if (cudaEventRecord(tev[1], stream) == cudaSuccess && cudaEventSynchronize(tev[1]) == cudaSuccess &&
+            cudaEventElapsedTime(&t, tev[0], tev[1]) == cudaSuccess)
+            sol_ms[solver] += t;
+    }
+
+    void note()
+    {
+        launches++;
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess && err == cudaSuccess) err = e;
+    }
+    static int blocks(const Range &r, int cap)
+    {
+        const long long nrows = (long long)(r.j1 - r.j0) * (r.k1 - r.k0);
+        long long b = (nrows + WPB - 1) / WPB;
+        if (b < 1) b = 1;
+        if (b > cap) b = cap;
+        return (int)b;
+    }
+    static bool empty(const Range &r) { return r.i1 <= r.i0 || r.j1 <= r.j0 || r.k1 <= r.k0; }
+
+    template <class F>
+    void cells(const Range &r, const int *gate, F f)
+    {
+        if (empty(r)) return;
+        k3_cells<<<blocks(r, NBC), TPB, 0, stream>>>(r, gate, f);
+        note();
+    }
+    template <int N, bool MAX = false, class F>
+    void reduce(const Range &r, const int *gate, int slot, F f)
+    {
+        const int nb = blocks(r, NBR);
+        k3_reduce<N, MAX><<<nb, TPB, 0, stream>>>(r, gate, part + (size_t)slot * NBR * 4, f);
+        note();
+        pend.nb[slot] = empty(r) ? 0 : nb;
+        pend.nq[slot] = N;
+        pend.mx[slot] = MAX ? 1 : 0;
+        pend.mask |= 1u << slot;
+    }
+    template <class F>
+    void scalar(const int *gate, F f)
+    {
+        k3_scalar<<<1, TPB, 0, stream>>>(part, pend, gate, sc, f);
+        note();
+        pend.mask = 0;
+    }
+    int read_int(const int *p)
+    {
+        if (cudaMemcpyAsync(int_host, p, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+            if (err == cudaSuccess) err = cudaGetLastError();
+            return 0;
+        }
+        return *int_host;
+    }
+    double read_double(const double *p)
+    {
+        Sc3 s = read_scalars();
+        const char *base = reinterpret_cast<const char *>(sc);
+        return *reinterpret_cast<const double *>(reinterpret_cast<const char *>(&s) + (reinterpret_cast<const char *>(p) - base));
+    }
+    Sc3 read_scalars()
+    {
+        if (cudaMemcpyAsync(sc_host, sc, sizeof(Sc3), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+            if (err == cudaSuccess) err = cudaGetLastError();
+        }
+        return *sc_host;
+    }
+    void zero(double *fld)
+    {
+        const cudaError_t e = cudaMemsetAsync(fld - origin, 0, field_elems * sizeof(double), stream);
+        if (e != cudaSuccess && err == cudaSuccess) err = e;
+    }
+    int status()
+    {
+        if (err != cudaSuccess) return fail(PVOF_ECUDA, std::string("CUDA: ") + cudaGetErrorString(err));
+        return PVOF_OK;
+    }
+};
+
+struct Handle {
+    Box3<GpuExec> b;
+    int device = 0;
+    double *mem = nullptr;      // all fields
+    double *tables = nullptr;   // metrics, weights, maps (doubles)
+    int *itables = nullptr;     // map sources
+    double *stage = nullptr;    // staging block for host copies
+    size_t stage_elems = 0;
+    double *flush = nullptr;
+    size_t flush_elems = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+static size_t block_elems(const Dom3 &d, bool ng)
+{
+    return ng ? (size_t)d.NX * d.NY * d.NZ : (size_t)(d.NX + 2 * NG) * (d.NY + 2 * NG) * (d.NZ + 2 * NG);
+}
+
+#define CK3(call)                                                                              \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) return fail(PVOF_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int destroy(Handle *h)
+{
+    if (!h) return PVOF_OK;
+    cudaSetDevice(h->device);
+    GpuExec &x = h->b.x;
+    if (x.stream) cudaStreamSynchronize(x.stream);
+    cudaFree(h->mem);
+    cudaFree(h->tables);
+    cudaFree(h->itables);
+    cudaFree(h->stage);
+    cudaFree(h->flush);
+    cudaFree(x.sc);
+    cudaFree(x.part);
+    cudaFreeHost(x.sc_host);
+    cudaFreeHost(x.int_host);
+    for (int q = 0; q < 2; q++) {
+        if (h->ev[q]) cudaEventDestroy(h->ev[q]);
+        if (x.tev[q]) cudaEventDestroy(x.tev[q]);
+    }
+    if (x.stream) cudaStreamDestroy(x.stream);
+    delete h;
+    return PVOF_OK;
+}
+
+int create(const pvof_grid_desc *g, const pvof_params *p, int device, Handle **out)
+{
+    *out = nullptr;
+    if (!g->periodic[0] || g->periodic[1] || !g->periodic[2])
+        return fail(PVOF_EINVAL, "the 3D mode needs x and z periodic and walls in y");
+    if (g->NXM < 8 || g->NYM < 8 || g->NZM < 8) return fail(PVOF_EINVAL, "the 3D mode needs at least 8 cells per direction");
+    if (p->stencil_fp32 || p->pressure_warm_start || p->pressure_preconditioner)
+        return fail(PVOF_EINVAL, "the FP32 stencil form, the pressure warm starts and the spectral preconditioner are 2D only");
+    const double hx = (g->xmax - g->xmin) / g->NXM, hy = (g->ymax - g->ymin) / g->NYM, hz = (g->zmax - g->zmin) / g->NZM;
+    if (!(hx > 0 && hy > 0 && hz > 0)) return fail(PVOF_EINVAL, "empty box");
+    CK3(cudaSetDevice(device));
+    Handle *h = new Handle();
+    h->device = device;
+    Box3<GpuExec> &b = h->b;
+    b.g = *g;
+    b.p = *p;
+    b.ph.rho_g = p->rho2 / p->rho1;
+    b.ph.mu_g = p->mu2 / p->mu1;
+    Dom3 &d = b.d;
+    d.NX = g->NXM + 1;
+    d.NY = g->NYM + 1;
+    d.NZ = g->NZM + 1;
+    d.P = ((OX + d.NX + NG) + 7) / 8 * 8;
+    d.S = (long long)d.P * (d.NY + 2 * NG);
+    GpuExec &x = b.x;
+    x.field_elems = (size_t)d.S * (size_t)(d.NZ + 2 * NG);
+    x.origin = (long long)NG * d.S + (long long)NG * d.P + OX;
+    auto bail = [&](int rc) { destroy(h); return rc; };
+    if (cudaStreamCreateWithFlags(&x.stream, cudaStreamNonBlocking) != cudaSuccess) return bail(fail(PVOF_ECUDA, "stream"));
+    // fields (zeroed once: never-written positions read as the reference's zero-initialised arrays)
+    const int nfields = F3_COUNT + 2;
+    if (cudaMalloc(&h->mem, x.field_elems * sizeof(double) * nfields) != cudaSuccess)
+        return bail(fail(PVOF_ENOMEM, "device memory for the 3D fields"));
+    if (cudaMemsetAsync(h->mem, 0, x.field_elems * sizeof(double) * nfields, x.stream) != cudaSuccess)
+        return bail(fail(PVOF_ECUDA, "memset"));
+    for (int q = 0; q < F3_COUNT; q++) b.f[q] = h->mem + (size_t)q * x.field_elems + x.origin;
+    b.vd[0] = b.f[F3_VD];
+    b.vd[1] = h->mem + (size_t)F3_COUNT * x.field_elems + x.origin;
+    b.vd[2] = h->mem + (size_t)(F3_COUNT + 1) * x.field_elems + x.origin;
+    // tables: metrics per axis (8 arrays), weights, map multipliers; map sources
+    HostAxis ax[3];
+    const bool per[3] = {true, false, true};
+    const double lo[3] = {g->xmin, g->ymin, g->zmin}, hi[3] = {g->xmax, g->ymax, g->zmax};
+    const int N[3] = {d.NX, d.NY, d.NZ};
+    for (int a = 0; a < 3; a++) {
+        host_axis_metrics(ax[a], N[a], lo[a], hi[a], per[a]);
+        host_axis_maps(ax[a], N[a], per[a], false, false, false, a, g->wall[PVOF_BOTTOM], g->wall[PVOF_TOP]);
+    }
+    std::vector<double> dt_;
+    std::vector<int> it_;
+    std::vector<size_t> doff, ioff;
+    auto addd = [&](const std::vector<double> &v) { doff.push_back(dt_.size()); dt_.insert(dt_.end(), v.begin(), v.end()); };
+    auto addi = [&](const std::vector<int> &v) { ioff.push_back(it_.size()); it_.insert(it_.end(), v.begin(), v.end()); };
+    for (int a = 0; a < 3; a++) {
+        addd(ax[a].idf); addd(ax[a].idc); addd(ax[a].df); addd(ax[a].dc); addd(ax[a].w);
+        for (int kind = 0; kind < K_COUNT; kind++) {
+            addd(ax[a].mul[kind]);
+            addi(ax[a].src[kind]);
+        }
+    }
+    if (cudaMalloc(&h->tables, dt_.size() * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&h->itables, it_.size() * sizeof(int)) != cudaSuccess)
+        return bail(fail(PVOF_ENOMEM, "device memory for the tables"));
+    if (cudaMemcpy(h->tables, dt_.data(), dt_.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->itables, it_.data(), it_.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(PVOF_ECUDA, "table upload"));
+    size_t qd = 0, qi = 0;
+    for (int a = 0; a < 3; a++) {
+        const double *idf = h->tables + doff[qd++] + NG, *idc = h->tables + doff[qd++] + NG;
+        const double *df = h->tables + doff[qd++] + NG, *dc = h->tables + doff[qd++] + NG;
+        const double *w = h->tables + doff[qd++] + NG;
+        if (a == 0) { d.idx_u = idf; d.idx_c = idc; d.dx_u = df; d.dx_c = dc; d.wx = w; }
+        if (a == 1) { d.idy_v = idf; d.idy_c = idc; d.dy_v = df; d.dy_c = dc; d.wy = w; }
+        if (a == 2) { d.idz_w = idf; d.idz_c = idc; d.dz_w = df; d.dz_c = dc; d.wz = w; }
+        for (int kind = 0; kind < K_COUNT; kind++) {
+            Axis A{h->itables + ioff[qi++], h->tables + doff[qd++]};
+            if (a == 0) d.map[kind].x = A;
+            if (a == 1) d.map[kind].y = A;
+            if (a == 2) d.map[kind].z = A;
+        }
+    }
+    d.idx2 = ax[0].idc[1 + NG] * ax[0].idc[1 + NG];
+    d.idy2 = ax[1].idc[1 + NG] * ax[1].idc[1 + NG];
+    d.idz2 = ax[2].idc[1 + NG] * ax[2].idc[1 + NG];
+    if (cudaMalloc(&x.sc, sizeof(Sc3)) != cudaSuccess || cudaMalloc(&x.part, sizeof(double) * NSLOT * NBR * 4) != cudaSuccess)
+        return bail(fail(PVOF_ENOMEM, "device scalars"));
+    cudaMemsetAsync(x.sc, 0, sizeof(Sc3), x.stream);
+    cudaMemsetAsync(x.part, 0, sizeof(double) * NSLOT * NBR * 4, x.stream);
+    if (cudaMallocHost(&x.sc_host, sizeof(Sc3)) != cudaSuccess || cudaMallocHost(&x.int_host, sizeof(int)) != cudaSuccess)
+        return bail(fail(PVOF_ENOMEM, "pinned scalars"));
+    h->stage_elems = block_elems(d, false);
+    if (cudaMalloc(&h->stage, h->stage_elems * sizeof(double)) != cudaSuccess)
+        return bail(fail(PVOF_ENOMEM, "staging block"));
+    for (int q = 0; q < 2; q++)
+        if (cudaEventCreate(&h->ev[q]) != cudaSuccess || cudaEventCreate(&x.tev[q]) != cudaSuccess)
+            return bail(fail(PVOF_ECUDA, "event"));
+    if (cudaStreamSynchronize(x.stream) != cudaSuccess) return bail(fail(PVOF_ECUDA, "set-up"));
+    *out = h;
+    return PVOF_OK;
+}
+
+// field of the ABI -> (slot, ghost kind, no-ghost, derived quantity)
+struct FieldRef {
+    int slot, kind, ng, xf;
+};
+static bool field_ref(const Handle *h, int field, bool upload, FieldRef &r)
+{
+    r = FieldRef{-1, K_SCALAR, 0, 0};
+    switch (field) {
+    case PVOF_F_C_L: r.slot = F3_CL; break;
+    case PVOF_F_F: r.slot = (upload || !h->b.initialized) ? F3_F : F3_CL; break;
+    case PVOF_F_C_G: if (upload) return false; r.slot = F3_CL; r.xf = 1; break;
+    case PVOF_F_RHO: if (upload) return false; r.slot = F3_CL; r.xf = 2; break;
+    case PVOF_F_MU: if (upload) return false; r.slot = F3_CL; r.xf = 3; break;
+    case PVOF_F_PSI_LG: r.slot = F3_PSI; break;
+    case PVOF_F_CH_RHS_N:
+    case PVOF_F_CH_RHS_CUR: r.slot = F3_RN; break;
+    case PVOF_F_U: r.slot = F3_U; r.kind = K_U; break;
+    case PVOF_F_V: r.slot = F3_V; r.kind = K_V; break;
+    case PVOF_F_W: r.slot = F3_W; r.kind = K_W; break;
+    case PVOF_F_P: r.slot = F3_P; r.kind = K_PRESSURE; break;
+    case PVOF_F_DELTAP: r.slot = F3_DP; r.kind = K_PRESSURE; break;
+    case PVOF_F_P_RHS: r.slot = F3_PRHS; r.kind = K_WRAP_C; break;
+    case PVOF_F_U_EXPLICIT: case PVOF_F_U_EXPLICIT_OLD: r.slot = F3_U_EXO; r.ng = 1; break;
+    case PVOF_F_V_EXPLICIT: case PVOF_F_V_EXPLICIT_OLD: r.slot = F3_V_EXO; r.ng = 1; break;
+    case PVOF_F_W_EXPLICIT: case PVOF_F_W_EXPLICIT_OLD: r.slot = F3_W_EXO; r.ng = 1; break;
+    case PVOF_F_U_VISC_EXPLICIT: case PVOF_F_U_VISC_EXPLICIT_OLD: r.slot = F3_U_VXO; r.ng = 1; break;
+    case PVOF_F_V_VISC_EXPLICIT: case PVOF_F_V_VISC_EXPLICIT_OLD: r.slot = F3_V_VXO; r.ng = 1; break;
+    case PVOF_F_W_VISC_EXPLICIT: case PVOF_F_W_VISC_EXPLICIT_OLD: r.slot = F3_W_VXO; r.ng = 1; break;
+    case PVOF_F_U_RHS: r.slot = F3_U_RHS; r.ng = 1; break;
+    case PVOF_F_V_RHS: r.slot = F3_V_RHS; r.ng = 1; break;
+    case PVOF_F_W_RHS: r.slot = F3_W_RHS; r.ng = 1; break;
+    case PVOF_F_FSIG_OLD_X: r.slot = F3_FSO_X; r.ng = 1; break;
+    case PVOF_F_FSIG_OLD_Y: r.slot = F3_FSO_Y; r.ng = 1; break;
+    case PVOF_F_FSIG_OLD_Z: r.slot = F3_FSO_Z; r.ng = 1; break;
+    case PVOF_F_FSIG_NEW_X: r.slot = F3_FSN_X; r.ng = 1; break;
+    case PVOF_F_FSIG_NEW_Y: r.slot = F3_FSN_Y; r.ng = 1; break;
+    case PVOF_F_FSIG_NEW_Z: r.slot = F3_FSN_Z; r.ng = 1; break;
+    default: return false;
+    }
+    return true;
+}
+
+static bool is_ng_field(int field)
+{
+    return (field >= PVOF_F_U_EXPLICIT && field <= PVOF_F_FSIG_NEW_Y) || (field >= PVOF_F_W_EXPLICIT && field <= PVOF_F_FSIG_NEW_Z);
+}
+
+size_t block_count(const Handle *h, int field)
+{
+    if (field < 0 || field >= PVOF_F_COUNT) return 0;
+    return block_elems(h->b.d, is_ng_field(field));
+}
+
+int upload(Handle *h, int field, const double *host, size_t count)
+{
+    FieldRef r;
+    if (!field_ref(h, field, true, r)) return fail(PVOF_EINVAL, "this field cannot be uploaded in the 3D mode");
+    const size_t n = block_elems(h->b.d, r.ng);
+    if (count != n) return fail(PVOF_EINVAL, "block size mismatch");
+    CK3(cudaSetDevice(h->device));
+    GpuExec &x = h->b.x;
+    CK3(cudaMemcpyAsync(h->stage, host, n * sizeof(double), cudaMemcpyHostToDevice, x.stream));
+    k3_unpack<<<592, 256, 0, x.stream>>>(h->b.d, h->b.f[r.slot], h->stage, r.ng);
+    x.note();
+    CK3(cudaStreamSynchronize(x.stream));
+    return x.status();
+}
+
+int download(Handle *h, int field, double *host, size_t count)
+{
+    FieldRef r;
+    if (!field_ref(h, field, false, r)) return fail(PVOF_EINVAL, "this field is not kept in the 3D mode");
+    const size_t n = block_elems(h->b.d, r.ng);
+    if (count != n) return fail(PVOF_EINVAL, "block size mismatch");
+    CK3(cudaSetDevice(h->device));
+    GpuExec &x = h->b.x;
+    const Dom3 &d = h->b.d;
+    const double *fld = h->b.f[r.slot];
+    switch (r.kind) {
+    case K_U: k3_pack<K_U><<<592, 256, 0, x.stream>>>(d, h->b.ph, fld, h->stage, r.ng, r.xf); break;
+    case K_V: k3_pack<K_V><<<592, 256, 0, x.stream>>>(d, h->b.ph, fld, h->stage, r.ng, r.xf); break;
+    case K_W: k3_pack<K_W><<<592, 256, 0, x.stream>>>(d, h->b.ph, fld, h->stage, r.ng, r.xf); break;
+    case K_PRESSURE: k3_pack<K_PRESSURE><<<592, 256, 0, x.stream>>>(d, h->b.ph, fld, h->stage, r.ng, r.xf); break;
+    case K_WRAP_C: k3_pack<K_WRAP_C><<<592, 256, 0, x.stream>>>(d, h->b.ph, fld, h->stage, r.ng, r.xf); break;
+    default: k3_pack<K_SCALAR><<<592, 256, 0, x.stream>>>(d, h->b.ph, fld, h->stage, r.ng, r.xf); break;
+    }
+    x.note();
+    CK3(cudaMemcpyAsync(host, h->stage, n * sizeof(double), cudaMemcpyDeviceToHost, x.stream));
+    CK3(cudaStreamSynchronize(x.stream));
+    return x.status();
+}
+
+int synchronize(Handle *h)
+{
+    CK3(cudaSetDevice(h->device));
+    CK3(cudaStreamSynchronize(h->b.x.stream));
+    return h->b.x.status();
+}
+
+int set_stage(Handle *h, int stage, double dt)
+{
+    if (stage < 0 || stage > 2 || !(dt > 0.0)) return fail(PVOF_EINVAL, "stage must be 0..2 and dt positive");
+    h->b.stage = stage;
+    h->b.dt = dt;
+    return PVOF_OK;
+}
+
+int initialize(Handle *h)
+{
+    CK3(cudaSetDevice(h->device));
+    const int rc = h->b.initialize();
+    if (rc < 0) return rc;
+    CK3(cudaStreamSynchronize(h->b.x.stream));
+    return h->b.x.status();
+}
+
+int substep(Handle *h, pvof_stats *st)
+{
+    CK3(cudaSetDevice(h->device));
+    if (!h->b.initialized) return fail(PVOF_EINVAL, "pvof_initialize() first");
+    if (!(h->b.dt > 0.0)) return fail(PVOF_EINVAL, "pvof_set_stage() first");
+    const int rc = h->b.substep(st);
+    if (rc == PVOF_EDIVERGED) return fail(rc, "the outer Poisson loop did not reach div < 1e-6 in 10 passes");
+    return rc;
+}
+
+int run_steps(Handle *h, int nsteps, double dt, pvof_stats *st)
+{
+    CK3(cudaSetDevice(h->device));
+    if (!h->b.initialized) return fail(PVOF_EINVAL, "pvof_initialize() first");
+    if (nsteps < 0 || !(dt > 0.0)) return fail(PVOF_EINVAL, "nsteps >= 0 and dt > 0");
+    const int rc = h->b.run_steps(nsteps, dt, st);
+    if (rc == PVOF_EDIVERGED) return fail(rc, "the outer Poisson loop did not reach div < 1e-6 in 10 passes");
+    return rc;
+}
+
+int liquid_mass(Handle *h, double *m)
+{
+    CK3(cudaSetDevice(h->device));
+    return h->b.liquid_mass(m);
+}
+
+long long launch_count(const Handle *h) { return h->b.x.launches; }
+
+int set_solver_timing(Handle *h, int on)
+{
+    h->b.x.timing = on ? 1 : 0;
+    for (int k = 0; k < 3; k++) {
+        h->b.x.sol_ms[k] = 0.0;
+        h->b.sol_launches[k] = h->b.sol_iters[k] = h->b.sol_cell_iters[k] = 0;
+    }
+    return PVOF_OK;
+}
+
+int solver_timing(const Handle *h, int solver, double *ms, long long *launches, long long *iters, long long *cell_iters)
+{
+    if (solver < 0 || solver > 2) return fail(PVOF_EINVAL, "bad solver index");
+    if (ms) *ms = h->b.x.sol_ms[solver];
+    if (launches) *launches = h->b.sol_launches[solver];
+    if (iters) *iters = h->b.sol_iters[solver];
+    if (cell_iters) *cell_iters = h->b.sol_cell_iters[solver];
+    return PVOF_OK;
+}
+double clamp_total(const Handle *h) { return h->b.clamp_total; }
+
+int timer_start(Handle *h)
+{
+    CK3(cudaSetDevice(h->device));
+    CK3(cudaEventRecord(h->ev[0], h->b.x.stream));
+    return PVOF_OK;
+}
+
+int timer_stop(Handle *h, double *ms)
+{
+    CK3(cudaSetDevice(h->device));
+    CK3(cudaEventRecord(h->ev[1], h->b.x.stream));
+    CK3(cudaEventSynchronize(h->ev[1]));
+    float t = 0.f;
+    CK3(cudaEventElapsedTime(&t, h->ev[0], h->ev[1]));
+    *ms = t;
+    return h->b.x.status();
+}
+
+// writes a buffer twice the size of the L2 so the next launch starts cold
+int flush_l2(Handle *h)
+{
+    CK3(cudaSetDevice(h->device));
+    if (!h->flush) {
+        int l2 = 0;
+        CK3(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, h->device));
+        h->flush_elems = (size_t)2 * (size_t)l2 / sizeof(double);
+        CK3(cudaMalloc(&h->flush, h->flush_elems * sizeof(double)));
+    }
+    k3_flush<<<592, 256, 0, h->b.x.stream>>>(h->flush, h->flush_elems, 0.0);
+    CK3(cudaGetLastError());
+    return PVOF_OK;
+}
+
+}  // namespace pvof3

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "pvof_particles.cuh"
+#include "pvof_3d_api.h"
 
 using namespace pvof;
 
@@ -53,7 +54,17 @@ int set_err(int code, const std::string &msg)
 constexpr int TBX = 32, TBY = 8;
 constexpr int COOP_THREADS = 512;
 
-bool is_ng(int field) { return field >= PVOF_F_U_EXPLICIT && field <= PVOF_F_FSIG_NEW_Y; }
+bool is_ng(int field)
+{
+    return (field >= PVOF_F_U_EXPLICIT && field <= PVOF_F_FSIG_NEW_Y) || (field >= PVOF_F_W_EXPLICIT && field <= PVOF_F_FSIG_NEW_Z);
+}
+
+// a 3D-mode result: the message of a failure comes from pvof_3d.cu
+int from3(int rc)
+{
+    if (rc < 0) g_err = pvof3::last_error();
+    return rc;
+}
 
 // ---------------------------------------------------------------------------
 // metrics and ghost maps, built on the host exactly as the reference does
@@ -1755,8 +1766,25 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
     if (!grid || !params || !out) return set_err(PVOF_EINVAL, "null argument");
     *out = nullptr;
     if (grid->ghost_nodes != NG) return set_err(PVOF_EINVAL, "ghost_nodes must be 3");
+    if (grid->geometry == PVOF_GEOM_3D) {
+        if (params->Re <= 0 || params->Pe_CH <= 0 || params->Cn <= 0) return set_err(PVOF_EINVAL, "Re, Pe_CH and Cn must be positive");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(PVOF_ENODEV, "no CUDA device");
+        if (device < 0 || device >= ndev) return set_err(PVOF_EINVAL, "bad device index");
+        pvof3::Handle *h = nullptr;
+        int rc = from3(pvof3::create(grid, params, device, &h));
+        if (rc < 0) return rc;
+        pvof_ctx *c = new pvof_ctx();
+        std::memset(static_cast<Ctx *>(c), 0, sizeof(Ctx));
+        c->g = *grid;
+        c->p = *params;
+        c->device = device;
+        c->h3 = h;
+        *out = c;
+        return PVOF_OK;
+    }
     if (grid->geometry != PVOF_GEOM_PLANAR && grid->geometry != PVOF_GEOM_AXISYM)
-        return set_err(PVOF_EINVAL, "only the 2D modes (planar, axisymmetric) are supported");
+        return set_err(PVOF_EINVAL, "geometry must be PVOF_GEOM_3D, PVOF_GEOM_PLANAR or PVOF_GEOM_AXISYM");
     if (grid->NZM != 1) return set_err(PVOF_EINVAL, "2D modes need NZM == 1");
     if (grid->NXM < 8 || grid->NYM < 8) return set_err(PVOF_EINVAL, "at least 8 cells per direction");
     if (grid->geometry == PVOF_GEOM_AXISYM && grid->periodic[0]) return set_err(PVOF_EINVAL, "the axis cannot be periodic");
@@ -1923,6 +1951,11 @@ int pvof_create(const pvof_grid_desc *grid, const pvof_params *params, int devic
 int pvof_destroy(pvof_ctx *c)
 {
     if (!c) return PVOF_OK;
+    if (c->h3) {
+        pvof3::destroy(c->h3);
+        delete c;
+        return PVOF_OK;
+    }
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (int q = 0; q < PVOF_F_COUNT; q++) if (c->base[q]) cudaFree(c->base[q]);
@@ -1959,6 +1992,7 @@ int pvof_destroy(pvof_ctx *c)
 size_t pvof_field_block_count(const pvof_ctx *c, int field)
 {
     if (!c || field < 0 || field >= PVOF_F_COUNT) return 0;
+    if (c->h3) return pvof3::block_count(c->h3, field);
     size_t NX = (size_t)c->dom.NX, NY = (size_t)c->dom.NY, NZ = (size_t)c->g.NZM + 1;
     if (is_ng(field)) return NX * NY * NZ;
     return (NX + 2 * NG) * (NY + 2 * NG) * (NZ + 2 * NG);
@@ -1985,6 +2019,7 @@ static int host_stage(pvof_ctx *c, size_t elems)
 int pvof_upload_field(pvof_ctx *c, int field, const double *host, size_t count)
 {
     if (!c || !host) return set_err(PVOF_EINVAL, "null argument");
+    if (c->h3) return from3(pvof3::upload(c->h3, field, host, count));
     if (count != pvof_field_block_count(c, field)) return set_err(PVOF_EINVAL, "block size does not match the field");
     CK(cudaSetDevice(c->device));
     const size_t NX = (size_t)c->dom.NX, NY = (size_t)c->dom.NY;
@@ -2002,6 +2037,7 @@ int pvof_upload_field(pvof_ctx *c, int field, const double *host, size_t count)
 int pvof_download_field(pvof_ctx *c, int field, double *host, size_t count)
 {
     if (!c || !host) return set_err(PVOF_EINVAL, "null argument");
+    if (c->h3) return from3(pvof3::download(c->h3, field, host, count));
     if (count != pvof_field_block_count(c, field)) return set_err(PVOF_EINVAL, "block size does not match the field");
     CK(cudaSetDevice(c->device));
     const size_t NX = (size_t)c->dom.NX, NY = (size_t)c->dom.NY, NZ = (size_t)c->g.NZM + 1;
@@ -2021,6 +2057,7 @@ int pvof_download_field(pvof_ctx *c, int field, double *host, size_t count)
 int pvof_synchronize(pvof_ctx *c)
 {
     if (!c) return set_err(PVOF_EINVAL, "null context");
+    if (c->h3) return from3(pvof3::synchronize(c->h3));
     CK(cudaStreamSynchronize(c->stream));
     return PVOF_OK;
 }
@@ -2029,6 +2066,7 @@ int pvof_set_stage(pvof_ctx *c, int which_stage, double dt)
 {
     if (!c) return set_err(PVOF_EINVAL, "null context");
     if (which_stage < 0 || which_stage > 2 || !(dt > 0.0)) return set_err(PVOF_EINVAL, "stage must be 0..2 and dt > 0");
+    if (c->h3) return from3(pvof3::set_stage(c->h3, which_stage, dt));
     c->stage = which_stage;
     c->dt = dt;
     return PVOF_OK;
@@ -2037,14 +2075,26 @@ int pvof_set_stage(pvof_ctx *c, int which_stage, double dt)
 #define ENTER(c)                                                        \
     do {                                                                \
         if (!(c)) return set_err(PVOF_EINVAL, "null context");          \
+        if ((c)->h3) return set_err(PVOF_EINVAL, "not available in the 3D mode"); \
         CK(cudaSetDevice((c)->device));                                 \
+    } while (0)
+// entry points that the 3D mode supports: null check only
+#define ENTER_ANY(c)                                                    \
+    do {                                                                \
+        if (!(c)) return set_err(PVOF_EINVAL, "null context");          \
     } while (0)
 #define NEED_DT(c)                                                      \
     do {                                                                \
         if (!((c)->dt > 0.0)) return set_err(PVOF_EINVAL, "pvof_set_stage() first"); \
     } while (0)
 
-int pvof_initialize(pvof_ctx *c) { ENTER(c); return initialize(c); }
+int pvof_initialize(pvof_ctx *c)
+{
+    ENTER_ANY(c);
+    if (c->h3) return from3(pvof3::initialize(c->h3));
+    ENTER(c);
+    return initialize(c);
+}
 int pvof_VOF_DIFFUSE_init(pvof_ctx *c) { ENTER(c); return vof_diffuse_init(c); }
 int pvof_VOF_DIFFUSE_step(pvof_ctx *c, pvof_stats *st)
 {
@@ -2121,6 +2171,8 @@ int pvof_Pressure_compute_velocity_divergence(pvof_ctx *c, double *div_max)
 
 int pvof_substep(pvof_ctx *c, pvof_stats *st)
 {
+    ENTER_ANY(c);
+    if (c->h3) return from3(pvof3::substep(c->h3, st));
     ENTER(c);
     NEED_DT(c);
     return substep(c, st);
@@ -2128,6 +2180,8 @@ int pvof_substep(pvof_ctx *c, pvof_stats *st)
 
 int pvof_run_steps(pvof_ctx *c, int nsteps, double dt, pvof_stats *st)
 {
+    ENTER_ANY(c);
+    if (c->h3) return from3(pvof3::run_steps(c->h3, nsteps, dt, st));
     ENTER(c);
     if (nsteps < 0 || !(dt > 0.0)) return set_err(PVOF_EINVAL, "nsteps >= 0 and dt > 0");
     for (int n = 0; n < nsteps; n++) {
@@ -2147,6 +2201,7 @@ int pvof_run_steps_batched(pvof_ctx *const *ctxs, int n, int nsteps, double dt, 
     if (n < 0 || (n > 0 && !ctxs)) return set_err(PVOF_EINVAL, "bad context array");
     for (int q = 0; q < n; q++) {
         if (!ctxs[q]) return set_err(PVOF_EINVAL, "null context in the batch");
+        if (ctxs[q]->h3) return set_err(PVOF_EINVAL, "the batched form takes 2D contexts");
         for (int r = 0; r < q; r++)
             if (ctxs[r] == ctxs[q]) return set_err(PVOF_EINVAL, "a context appears twice in the batch");
     }
@@ -2176,6 +2231,13 @@ int pvof_run_steps_batched(pvof_ctx *const *ctxs, int n, int nsteps, double dt, 
 
 int pvof_liquid_mass(pvof_ctx *c, double *mass)
 {
+    ENTER_ANY(c);
+    if (c->h3) {
+        double m = 0.0;
+        const int rc = from3(pvof3::liquid_mass(c->h3, &m));
+        if (mass) *mass = m;
+        return rc;
+    }
     ENTER(c);
     const int NX = c->dom.NX, NY = c->dom.NY;
     dim3 blk(TBX, TBY);
@@ -2189,10 +2251,12 @@ int pvof_liquid_mass(pvof_ctx *c, double *mass)
     return PVOF_OK;
 }
 
-long long pvof_launch_count(const pvof_ctx *c) { return c ? c->launches : 0; }
+long long pvof_launch_count(const pvof_ctx *c) { return c ? (c->h3 ? pvof3::launch_count(c->h3) : c->launches) : 0; }
 
 int pvof_timer_start(pvof_ctx *c)
 {
+    ENTER_ANY(c);
+    if (c->h3) return from3(pvof3::timer_start(c->h3));
     ENTER(c);
     CK(cudaEventRecord(c->timer_ev[0], c->stream));
     return PVOF_OK;
@@ -2200,6 +2264,13 @@ int pvof_timer_start(pvof_ctx *c)
 
 int pvof_timer_stop(pvof_ctx *c, double *ms)
 {
+    ENTER_ANY(c);
+    if (c->h3) {
+        double t = 0.0;
+        const int rc = from3(pvof3::timer_stop(c->h3, &t));
+        if (ms) *ms = t;
+        return rc;
+    }
     ENTER(c);
     CK(cudaEventRecord(c->timer_ev[1], c->stream));
     CK(cudaEventSynchronize(c->timer_ev[1]));
@@ -2211,6 +2282,8 @@ int pvof_timer_stop(pvof_ctx *c, double *ms)
 
 int pvof_flush_l2(pvof_ctx *c)
 {
+    ENTER_ANY(c);
+    if (c->h3) return from3(pvof3::flush_l2(c->h3));
     ENTER(c);
     if (!c->flush_buf) {
         int l2 = 0;
@@ -2232,12 +2305,12 @@ int pvof_set_graphs(pvof_ctx *c, int enabled)
     return PVOF_OK;
 }
 
-long long pvof_graph_replays(const pvof_ctx *c) { return c ? c->graph_replays : -1; }
+long long pvof_graph_replays(const pvof_ctx *c) { return (c && !c->h3) ? c->graph_replays : -1; }
 
 int pvof_clamp_mass_total(const pvof_ctx *c, double *total)
 {
     if (!c || !total) return set_err(PVOF_EINVAL, "null context or output");
-    *total = c->clamp_total;
+    *total = c->h3 ? pvof3::clamp_total(c->h3) : c->clamp_total;
     return PVOF_OK;
 }
 
@@ -2326,6 +2399,8 @@ int pvof_autotune_entry(const pvof_ctx *c, int q, const char **name, int *bx, in
 
 int pvof_set_solver_timing(pvof_ctx *c, int enabled)
 {
+    ENTER_ANY(c);
+    if (c->h3) return from3(pvof3::set_solver_timing(c->h3, enabled));
     ENTER(c);
     c->solver_timing = enabled ? 1 : 0;
     for (int k = 0; k < 3; k++) {
@@ -2339,6 +2414,10 @@ int pvof_set_solver_timing(pvof_ctx *c, int enabled)
 const char *pvof_solver_kernel(const pvof_ctx *c, int solver)
 {
     if (!c) return "";
+    if (c->h3) {
+        static const char *k3[] = {"k3_reduce (biharmonic CG)", "k3_reduce (velocity PCG)", "k3_reduce (pressure PCG)"};
+        return (solver >= 0 && solver <= 2) ? k3[solver] : "";
+    }
     switch (solver) {
     case PVOF_SOLVER_BIHARMONIC: return "k_cg_biharmonic";
     case PVOF_SOLVER_VELOCITY: return c->cgs_v_smem ? "k_cgs_velocity" : "k_cg_velocity";
@@ -2352,6 +2431,7 @@ int pvof_solver_timing(const pvof_ctx *c, int solver, double *ms, long long *lau
                        long long *cell_iters)
 {
     if (!c || solver < 0 || solver > 2) return set_err(PVOF_EINVAL, "bad solver index");
+    if (c->h3) return from3(pvof3::solver_timing(c->h3, solver, ms, launches, iterations, cell_iters));
     if (ms) *ms = c->sol_ms[solver];
     if (launches) *launches = c->sol_launches[solver];
     if (iterations) *iterations = c->sol_iters[solver];

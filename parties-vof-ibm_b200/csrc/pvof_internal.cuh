@@ -15,6 +15,10 @@
 
 #include "../../include/pvof.h"
 
+namespace pvof3 {
+struct Handle;
+}
+
 namespace pvof {
 
 constexpr int NG = 3;        // ghost layers
@@ -186,6 +190,7 @@ struct Ctx {
     long long pend_cells[NPEND], pend_cells2[NPEND];
     int npend;
     IbmState *ibm;           // resolved particles (null until pvof_set_particles)
+    pvof3::Handle *h3;       // the 3D mode's state (PVOF_GEOM_3D); null for the 2D modes
     double *fft_coef;        // as, ap, an (NY-1 each) and the modified wavenumbers (NX-1)
     double *spec_mem;        // spectral pressure preconditioner: twiddles, block sums, reduction tables
     struct SpecScal *spec_s; // its grid barrier state

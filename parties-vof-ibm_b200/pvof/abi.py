@@ -5,7 +5,7 @@ field; tests/test_abi.py checks the exported symbols and the sizes.
 """
 import ctypes as C
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 OK = 0
 EINVAL = -1
@@ -35,11 +35,14 @@ FIELD_NAMES = [
     "V_VISC_EXPLICIT", "V_VISC_EXPLICIT_OLD", "V_RHS",
     "FSIG_OLD_X", "FSIG_OLD_Y", "FSIG_NEW_X", "FSIG_NEW_Y",
     "NX_IBM", "NY_IBM",
+    "W_EXPLICIT", "W_EXPLICIT_OLD", "W_IMPLICIT",
+    "W_VISC_EXPLICIT", "W_VISC_EXPLICIT_OLD", "W_RHS",
+    "FSIG_OLD_Z", "FSIG_NEW_Z",
 ]
 FIELD = {name: idx for idx, name in enumerate(FIELD_NAMES)}
 FIELD_COUNT = len(FIELD_NAMES)
 # no-ghost ("ng_") fields: G-range blocks
-NG_FIELDS = set(range(FIELD["U_EXPLICIT"], FIELD["FSIG_NEW_Y"] + 1))
+NG_FIELDS = set(range(FIELD["U_EXPLICIT"], FIELD["FSIG_NEW_Y"] + 1)) | set(range(FIELD["W_EXPLICIT"], FIELD["FSIG_NEW_Z"] + 1))
 
 
 class GridDesc(C.Structure):
@@ -94,6 +97,7 @@ class Stats(C.Structure):
         ("poisson_passes", C.c_int),
         ("div_max", C.c_double),
         ("clamp_mass", C.c_double),
+        ("w_iters", C.c_int), ("w_rms", C.c_double),
     ]
 
     def as_dict(self):

@@ -303,3 +303,85 @@ def droplet_batch(n=64, seed=0, nxm_min=64, nxm_max=512, **kw):
         Rd, Rs, th = rng.uniform(0.3, 0.6), rng.uniform(0.2, 0.4), rng.uniform(30.0, 150.0)
         out.append(droplet_on_cylinder(nxm, Rd=Rd, Rs=Rs, theta=th, **kw))
     return out
+
+
+def box_grid(NXM, NYM, NZM, Lx=2.0, Ly=2.0, Lz=2.0, wall_y=abi.WALL_NOSLIP):
+    """3D box: x and z periodic, walls of type ``wall_y`` at y = 0 and Ly."""
+    g = abi.GridDesc()
+    g.NXM, g.NYM, g.NZM = NXM, NYM, NZM
+    g.ghost_nodes = G
+    g.geometry = abi.GEOM_3D
+    g.periodic[0], g.periodic[1], g.periodic[2] = 1, 0, 1
+    for f in range(6):
+        g.wall[f] = abi.WALL_NOSLIP
+    g.wall[abi.BOTTOM] = wall_y
+    g.wall[abi.TOP] = wall_y
+    g.xmin, g.xmax = 0.0, float(Lx)
+    g.ymin, g.ymax = 0.0, float(Ly)
+    g.zmin, g.zmax = 0.0, float(Lz)
+    hx = (g.xmax - g.xmin) / float(NXM)
+    hy = (g.ymax - g.ymin) / float(NYM)
+    g.slab_thickness = min(hx, hy)
+    g.theta_span = 2.0 * math.pi
+    return g
+
+
+def field_to_block(grid, arr, ng=False):
+    """A host block of the field layout from a G-range plane (NY, NX), copied
+    to every k plane, or a G-range array (NZ, NY, NX)."""
+    arr = np.asarray(arr, dtype=np.float64)
+    if arr.ndim == 2:
+        return plane_to_block(grid, arr, ng)
+    NX, NY, NZ = dims(grid)
+    assert arr.shape == (NZ, NY, NX), (arr.shape, (NZ, NY, NX))
+    blk = np.zeros(block_shape(grid, ng), dtype=np.float64)
+    if ng:
+        blk[:] = arr
+    else:
+        blk[G:G + NZ, G:G + NY, G:G + NX] = arr
+    return blk
+
+
+def interface_box(NXM=256, NYM=256, NZM=256, L=2.0, seed=3, modes=16, amp_max=0.02, Cn=0.005, rho_ratio=1e-3,
+                  mu_ratio=1e-2, Re=1000.0, We=100.0, velocity_seed=None, velocity_amp=0.0, **param_kw):
+    """3D liquid layer under gas in an L^3 box (x, z periodic, no-slip walls in
+    y), the precision form's case: the interface height is
+    h(x, z) = L/2 + sum_k a_k cos(pi (n_x x + n_z z) + phi_k) over ``modes``
+    seeded (n_x, n_z) in {1..4}^2, a_k ~ U(0, amp_max), phi_k ~ U(0, 2 pi);
+    liquid (C = 1) below, C = 0.5 (1 + tanh((h - y) / (sqrt(2) Cn))); gas of
+    density ratio ``rho_ratio`` and viscosity ratio ``mu_ratio``; surface
+    tension at Weber number We and gravity -y.  The cells are cubes of side
+    L / NXM (the reference's uniform grid needs dx = dy = dz), so the box is
+    L x (NYM/NXM) L x (NZM/NXM) L and the modes are cos(2 pi (n_x x / Lx +
+    n_z z / Lz) + phi_k), the same as above for a cube.  ``velocity_seed`` adds
+    a seeded random velocity of size ``velocity_amp`` (parity cases).  Returns
+    (grid, params, fields) with G-range arrays (NZ, NY, NX)."""
+    h = L / float(NXM)
+    Lx, Ly, Lz = L, h * NYM, h * NZM
+    grid = box_grid(NXM, NYM, NZM, Lx, Ly, Lz)
+    params = default_params(Re=Re, rho1=1.0, rho2=rho_ratio, mu1=1.0, mu2=mu_ratio, Cn=Cn, Pe_CH=1.0 / Cn,
+                            surface_tension=1, We=We, **param_kw)
+    rng = np.random.default_rng(seed)
+    nx = rng.integers(1, 5, size=modes)
+    nz = rng.integers(1, 5, size=modes)
+    a = rng.uniform(0.0, amp_max, size=modes)
+    ph = rng.uniform(0.0, 2.0 * np.pi, size=modes)
+    NX, NY, NZ = dims(grid)
+    xc = (0.5 + np.arange(NX)) * h
+    yc = (0.5 + np.arange(NY)) * h
+    zc = (0.5 + np.arange(NZ)) * h
+    Z, X = np.meshgrid(zc, xc, indexing="ij")
+    H = 0.5 * Ly + sum(a[q] * np.cos(2.0 * np.pi * (nx[q] * X / Lx + nz[q] * Z / Lz) + ph[q]) for q in range(modes))
+    C = 0.5 * (1.0 + np.tanh((H[:, None, :] - yc[None, :, None]) / (math.sqrt(2.0) * Cn)))
+    fields = {"F": C}
+    shape = (NZ, NY, NX)
+    if velocity_seed is not None:
+        vr = np.random.default_rng(velocity_seed)
+        fields["U"] = velocity_amp * vr.standard_normal(shape)
+        fields["V"] = velocity_amp * vr.standard_normal(shape)
+        fields["W"] = velocity_amp * vr.standard_normal(shape)
+        fields["P"] = velocity_amp * vr.standard_normal(shape)
+    else:
+        for k in ("U", "V", "W", "P"):
+            fields[k] = np.zeros(shape)
+    return grid, params, fields

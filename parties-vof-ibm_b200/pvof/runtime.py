@@ -159,6 +159,28 @@ class Solver:
         f = abi.FIELD[name]
         return cases.block_plane(self.grid, self.download(name), ng=f in abi.NG_FIELDS)
 
+    def set_fields(self, fields):
+        """Upload G-range arrays: (NY, NX) planes copied to every k plane, or
+        (NZ, NY, NX) boxes (the 3D mode)."""
+        for name, arr in fields.items():
+            ng = abi.FIELD[name] in abi.NG_FIELDS
+            self.upload(name, cases.field_to_block(self.grid, arr, ng=ng))
+
+    def get_block(self, name):
+        """Whole host block of a field: (NZ+2G, NY+2G, NX+2G) for flow
+        fields, (NZ, NY, NX) for no-ghost fields."""
+        ng = abi.FIELD[name] in abi.NG_FIELDS
+        return self.download(name).reshape(cases.block_shape(self.grid, ng))
+
+    def get_g_range(self, name):
+        """G-range part (NZ, NY, NX) of a field."""
+        b = self.get_block(name)
+        if abi.FIELD[name] in abi.NG_FIELDS:
+            return b
+        NX, NY, NZ = cases.dims(self.grid)
+        G = cases.G
+        return b[G:G + NZ, G:G + NY, G:G + NX]
+
     def set_planes(self, planes):
         for name, plane in planes.items():
             ng = abi.FIELD[name] in abi.NG_FIELDS

@@ -174,6 +174,9 @@ def parse_iterations(log):
     u = [int(m) for m in re.findall(r"u-component of velocity converged to \S+ after (\d+) iterations", log)]
     v = [int(m) for m in re.findall(r"v-component of velocity converged to \S+ after (\d+) iterations", log)]
     p = [int(m) for m in re.findall(r"pressure converged to \S+ after (\d+) iterations", log)]
+    w = [int(m) for m in re.findall(r"w-component of velocity converged to \S+ after (\d+) iterations", log)]
+    if w:
+        return np.array([ch, u, v, p, w], dtype=np.int64)
     return np.array([ch, u, v, p], dtype=np.int64)
 
 
@@ -416,6 +419,62 @@ def make_fft(name, NXM, NYM, Lx, Ly, seed, outdir, refsrc=None):
     return path
 
 
+# 3D cases (the reference built without TWOD_* flags, oracle/ref/cfg/rt3d_st.h):
+# x and z periodic, no-slip walls in y, surface tension, gravity -y.  Fixtures
+# hold the G range (NZ, NY, NX) of the flow fields and the no-ghost arrays.
+BOX_FLOW = {"C_L": "C_L", "C_G": "C_G", "rho": "RHO", "mu": "MU", "ch_rhs_n": "CH_RHS_N", "u": "U", "v": "V",
+            "w": "W", "p": "P", "psi_LG": "PSI_LG"}
+BOX_NG = {"u_explicit_old": "U_EXPLICIT_OLD", "v_explicit_old": "V_EXPLICIT_OLD", "w_explicit_old": "W_EXPLICIT_OLD",
+          "u_visc_explicit_old": "U_VISC_EXPLICIT_OLD", "v_visc_explicit_old": "V_VISC_EXPLICIT_OLD",
+          "w_visc_explicit_old": "W_VISC_EXPLICIT_OLD", "f_sigma_old_x": "FSIG_OLD_X",
+          "f_sigma_old_y": "FSIG_OLD_Y", "f_sigma_old_z": "FSIG_OLD_Z"}
+BOX_TIGHT = dict(TIGHT, CG_ETOL=1e-13)
+BOX_GRID = dict(NXM=16, NYM=24, NZM=12, Cn=0.1, amp_max=0.1, We=10.0, Re=100.0)
+# name, reference case, builder kwargs, steps, dt, snapshots kept (None: the last only)
+BOX_CASES = [
+    ("box_st_tight", "rt3d_st", dict(BOX_GRID, rho_ratio=0.1, mu_ratio=0.1, velocity_seed=5, velocity_amp=0.05,
+                                     **BOX_TIGHT), 2, 1e-3, ["s1_0", "s2_2"]),
+    # the precision form's density and viscosity ratios on a small cube
+    ("box_rho1e-3", "rt3d_st", dict(NXM=16, NYM=16, NZM=16, Cn=0.1, amp_max=0.1, We=100.0, Re=1000.0,
+                                    rho_ratio=1e-3, mu_ratio=1e-2, velocity_seed=8, velocity_amp=0.02, **BOX_TIGHT),
+     2, 1e-3, ["s2_2"]),
+]
+BOX_LONG = [("box_st_100steps", "rt3d_st", dict(BOX_GRID, rho_ratio=0.1, mu_ratio=0.1, **BOX_TIGHT), 100, 1e-3)]
+
+
+def make_3d(name, refcase, kw, steps, dt, keep, outdir, refsrc=None):
+    """A 3D fixture: the reference's fields after the kept substeps (or the
+    last step), the initial fields and the solver iteration counts."""
+    build = dict(kw)
+    grid, params, fields = cases.interface_box(**build)
+    if not os.path.exists(po.ref_binary(refcase)):
+        po.build_reference(refcase, refsrc)
+    NX, NY, NZ = cases.dims(grid)
+    G = cases.G
+    with tempfile.TemporaryDirectory() as wd:
+        cp = po.run_reference(refcase, wd, grid, params, fields, steps, dt, 1 if keep else steps,
+                              substeps=bool(keep), timeout=7200)
+        data = {}
+        tags = keep if keep else ["s%d" % steps]
+        for tag in tags:
+            for fname, pname in BOX_FLOW.items():
+                a = np.fromfile(os.path.join(wd, "out", "%s_%s.bin" % (tag, fname)), dtype="<f8")
+                a = a.reshape(cases.block_shape(grid))[G:G + NZ, G:G + NY, G:G + NX]
+                data["%s/%s" % (tag, pname)] = a
+            for fname, pname in BOX_NG.items():
+                a = np.fromfile(os.path.join(wd, "out", "%s_%s.bin" % (tag, fname)), dtype="<f8")
+                data["%s/%s" % (tag, pname)] = a.reshape(cases.block_shape(grid, ng=True))
+        data["iterations"] = parse_iterations(cp.stdout)
+    for k, v in fields.items():
+        data["init/" + k] = v
+    meta = {"grid": struct_to_dict(grid), "params": struct_to_dict(params), "steps": steps, "dt": dt,
+            "refcase": refcase, "builder": kw}
+    data["meta"] = np.array(repr(meta))
+    path = os.path.join(outdir, name + ".npz")
+    np.savez_compressed(path, **data)
+    return path
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--refsrc", default=None)
@@ -444,6 +503,12 @@ def main():
     for name, NXM, NYM, Lx, Ly, seed in FFT_CASES:
         if ap_only is None or name in ap_only:
             print(make_fft(name, NXM, NYM, Lx, Ly, seed, a.out, a.refsrc))
+    for name, refcase, kw, steps, dt, keep in BOX_CASES:
+        if ap_only is None or name in ap_only:
+            print(make_3d(name, refcase, kw, steps, dt, keep, a.out, a.refsrc))
+    for name, refcase, kw, steps, dt in BOX_LONG:
+        if ap_only is not None and name in ap_only:
+            print(make_3d(name, refcase, kw, steps, dt, None, a.out, a.refsrc))
 
 
 if __name__ == "__main__":
