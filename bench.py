@@ -426,6 +426,7 @@ def box_case(args, device):
     more step with per-solver events; the pressure Jacobi-PCG's achieved
     bandwidth counts 56 algorithmic bytes per cell and iteration; the
     reference's 3D build on a --box-ref-grid box for --box-ref-steps steps."""
+    import numpy as np
     from pvof import runtime
     n = [int(v) for v in args.box_grid.lower().split("x")]
     grid, params, fields = box_setup(n, args.box_maxit)
@@ -453,6 +454,7 @@ def box_case(args, device):
     s.set_solver_timing(False)
     m1 = s.liquid_mass()
     clamp = s.clamp_mass_total()
+    ref64 = {f: s.get_g_range(f) for f in ("U", "V", "W")} if args.box_fp32 else None
     peak, peak_kind = measured_peak()
     names = ["biharmonic CG", "velocity PCG (u, v, w)", "pressure Jacobi-PCG"]
     out = {"case": "3D box %s, x and z periodic, no-slip walls in y, liquid layer under gas with a seeded 16-mode "
@@ -476,6 +478,34 @@ def box_case(args, device):
                                                     "peak_kind": peak_kind, "unit": "GB/s", "frac": gbs / peak,
                                                     "alg_bytes_per_cell_iter": bpc}
     s.close()
+    if args.box_fp32:
+        # the precision form: FP32 stencils from the same start over the same
+        # steps, its throughput and its errors against the FP64 path above
+        grid, params, fields = box_setup(n, args.box_maxit)
+        params.stencil_fp32 = 1
+        s32 = runtime.Solver(grid, params, device=device)
+        s32.set_fields({k: fields[k] for k in ("F", "U", "V", "W", "P")})
+        del fields
+        s32.initialize()
+        s32.run_steps(max(0, args.box_warmup), BOX_DT)
+        ms32 = 0.0
+        for _ in range(nsteps):
+            s32.flush_l2()
+            s32.timer_start()
+            s32.run_steps(1, BOX_DT)
+            ms32 += s32.timer_stop()
+        s32.run_steps(1, BOX_DT)
+        num = den = 0.0
+        for f in ("U", "V", "W"):
+            a, b = s32.get_g_range(f), ref64[f]
+            num += float(np.sum((a - b) ** 2))
+            den += float(np.sum(b ** 2))
+        m32 = s32.liquid_mass()
+        out["fp32_form"] = {"value": cells * nsteps / (ms32 * 1e-3), "ms_per_step": ms32 / nsteps,
+                            "velocity_rel_l2_vs_fp64": (num / den) ** 0.5,
+                            "volume_rel_error_vs_fp64": abs(m32 - m1) / m1,
+                            "steps_compared": max(0, args.box_warmup) + nsteps + 1}
+        s32.close()
     if args.box_ref_steps > 0:
         r = box_reference(args.box_ref_grid, args.box_ref_steps)
         if r is not None:
@@ -1239,6 +1269,8 @@ def main():
     ap.add_argument("--box-steps", type=int, default=2)
     ap.add_argument("--box-warmup", type=int, default=1)
     ap.add_argument("--box-maxit", type=int, default=20000)
+    ap.add_argument("--box-fp32", action="store_true",
+                    help="with --box, also the FP32 stencil form from the same start and its errors against FP64")
     ap.add_argument("--box-ref-grid", default="32x32x32")
     ap.add_argument("--box-ref-steps", type=int, default=1)
     ap.add_argument("--axisym", action="store_true",

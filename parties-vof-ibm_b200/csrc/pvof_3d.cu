@@ -7,6 +7,7 @@
 // stride over the remaining rows.  Reductions write one partial per block
 // (a fixed grid of at most NBR blocks) and a one-block scalar kernel adds
 // the partials in a fixed order, so every sum is the same from run to run.
+#include <algorithm>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -83,6 +84,7 @@ __global__ void __launch_bounds__(TPB) k3_reduce(Range r, const int *gate, doubl
 struct Pend {
     int nb[NSLOT], nq[NSLOT], mx[NSLOT];
     unsigned mask;
+    int stride;   // partial sums per slot (blocks), times 4 values
 };
 
 template <class F>
@@ -95,7 +97,7 @@ __global__ void __launch_bounds__(TPB) k3_scalar(const double *part, Pend pd, co
         for (int q = 0; q < pd.nq[s]; q++) {
             double a = 0.0;
             for (int b = threadIdx.x; b < pd.nb[s]; b += TPB) {
-                const double v = part[((size_t)s * NBR + b) * 4 + q];
+                const double v = part[(size_t)s * pd.stride + (size_t)b * 4 + q];
                 a = pd.mx[s] ? fmax(a, v) : a + v;
             }
             sh[threadIdx.x] = a;
@@ -109,6 +111,177 @@ __global__ void __launch_bounds__(TPB) k3_scalar(const double *part, Pend pd, co
         }
     }
     if (threadIdx.x == 0) f(sc);
+}
+
+// ---------------------------------------------------------------------------
+// the pressure PCG iteration (psolve_cg.c:209-253) as three streaming kernels
+// over the physical cells: a thread takes two neighbouring cells of a row
+// (16-byte loads; i = 0 is 16-byte aligned and every row and plane pitch is
+// even) in PKB consecutive planes, a block a 64 x 8 tile of (i, j).  Reads at
+// ghost and half cells go through the pressure ghost map; the arithmetic is
+// that of p_apply_st and of the reference's loops, operand for operand.
+// ---------------------------------------------------------------------------
+constexpr int PKB = 1;
+
+__device__ __forceinline__ double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
+__device__ __forceinline__ void st2(double *p, double a, double b) { *reinterpret_cast<double2 *>(p) = make_double2(a, b); }
+
+// the cells (i, i+1) of a pressure field at (j, k), after the ghost update
+__device__ __forceinline__ void p_pair(const Dom3 &d, const double *__restrict__ X, int i, int j, int k, double &a,
+                                       double &b)
+{
+    if (j >= 0 && j <= d.NY - 2 && k >= 0 && k <= d.NZ - 2) {
+        const double2 v = ld2(X + at(d, i, j, k));
+        a = v.x;
+        b = v.y;
+    } else {
+        a = rd<K_PRESSURE>(d, X, i, j, k);
+        b = rd<K_PRESSURE>(d, X, i + 1, j, k);
+    }
+}
+
+// The block's sum into part[block]; the last block to finish adds all the
+// partials in block order (the same order whichever block is last) and runs
+// the scalar step then(sc, sum) on one thread, so no separate launch is
+// needed between the passes.
+template <class F>
+__device__ __forceinline__ void block_sum_then(double acc, double *part, Sc3 *sc, F then)
+{
+    __shared__ double sh[256];
+    __shared__ bool last;
+    const int t = threadIdx.x + 32 * threadIdx.y;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (threadIdx.x == 0) sh[threadIdx.y] = acc;
+    __syncthreads();
+    const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
+    if (t == 0) {
+        double a = sh[0];
+        for (int q = 1; q < 8; q++) a += sh[q];
+        part[(size_t)(blockIdx.x + gridDim.x * (blockIdx.y + (size_t)gridDim.y * blockIdx.z)) * 4] = a;
+        __threadfence();
+        last = (atomicAdd(&sc->p_count, 1u) == nb - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double a = 0.0;
+    for (unsigned b = t; b < nb; b += 256) a += __ldcg(part + (size_t)b * 4);
+    sh[t] = a;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (t < w) sh[t] += sh[t + w];
+        __syncthreads();
+    }
+    if (t == 0) {
+        sc->p_count = 0;
+        then(sc, sh[0]);
+    }
+}
+
+template <class F>
+__global__ void __launch_bounds__(256, 4) k3p_apply(Dom3 d, const double *__restrict__ CX, const double *__restrict__ CY,
+                                                    const double *__restrict__ CZ, const double *__restrict__ X,
+                                                    double *__restrict__ AD, const int *gate, double *part, Sc3 *sc,
+                                                    F then)
+{
+    if (gate && *gate == 0) return;
+    const int ni = d.NX - 1, nj = d.NY - 1, nk = d.NZ - 1;
+    const int i = 2 * (blockIdx.x * 32 + threadIdx.x), j = blockIdx.y * 8 + threadIdx.y;
+    double acc = 0.0;
+    if (i < ni && j < nj) {
+        const bool two = i + 1 < ni;
+#pragma unroll
+        for (int kk = 0; kk < PKB; kk++) {
+            const int k = blockIdx.z * PKB + kk;
+            if (k >= nk) break;
+            const long long q = at(d, i, j, k);
+            if (!two) {
+                const double ad = p_apply_st(d, CX, CY, CZ, X, i, j, k);
+                AD[q] = ad;
+                acc += X[q] * ad;
+                continue;
+            }
+            const double2 c = ld2(X + q);
+            const double w0 = (i >= 1) ? X[q - 1] : rd<K_PRESSURE>(d, X, i - 1, j, k);
+            const double e1 = (i + 2 <= ni - 1) ? X[q + 2] : rd<K_PRESSURE>(d, X, i + 2, j, k);
+            double s0, s1, n0, n1, b0, b1, f0, f1;
+            p_pair(d, X, i, j - 1, k, s0, s1);
+            p_pair(d, X, i, j + 1, k, n0, n1);
+            p_pair(d, X, i, j, k - 1, b0, b1);
+            p_pair(d, X, i, j, k + 1, f0, f1);
+            const double2 cx = ld2(CX + q), cy = ld2(CY + q), cz = ld2(CZ + q);
+            const double2 cym = ld2(CY + q - d.P), czm = ld2(CZ + q - d.S);
+            const double cxm = CX[q - 1];
+            const double v0 = cx.x * (c.y - c.x) - cxm * (c.x - w0) + cy.x * (n0 - c.x) - cym.x * (c.x - s0) +
+                              cz.x * (f0 - c.x) - czm.x * (c.x - b0);
+            const double v1 = cx.y * (e1 - c.y) - cx.x * (c.y - c.x) + cy.y * (n1 - c.y) - cym.y * (c.y - s1) +
+                              cz.y * (f1 - c.y) - czm.y * (c.y - b1);
+            const double ad0 = 1.0 * v0, ad1 = 1.0 * v1;
+            st2(AD + q, ad0, ad1);
+            acc += c.x * ad0;
+            acc += c.y * ad1;
+        }
+    }
+    block_sum_then(acc, part, sc, then);
+}
+
+template <class F>
+__global__ void __launch_bounds__(256) k3p_update(Dom3 d, double *__restrict__ PHI, double *__restrict__ R,
+                                                  const double *__restrict__ DD, const double *__restrict__ AD,
+                                                  const double *__restrict__ M, const int *gate, Sc3 *sc,
+                                                  double *part, F then)
+{
+    if (gate && *gate == 0) return;
+    const int ni = d.NX - 1, nj = d.NY - 1, nk = d.NZ - 1;
+    const int i = 2 * (blockIdx.x * 32 + threadIdx.x), j = blockIdx.y * 8 + threadIdx.y;
+    const double alpha = sc->p_alpha;
+    double acc = 0.0;
+    if (i < ni && j < nj) {
+        const bool two = i + 1 < ni;
+#pragma unroll
+        for (int kk = 0; kk < PKB; kk++) {
+            const int k = blockIdx.z * PKB + kk;
+            if (k >= nk) break;
+            const long long q = at(d, i, j, k);
+            if (!two) {
+                PHI[q] += alpha * DD[q];
+                const double r = R[q] - alpha * AD[q];
+                R[q] = r;
+                acc += r * (r * M[q]);
+                continue;
+            }
+            const double2 x = ld2(PHI + q), dd = ld2(DD + q), r = ld2(R + q), ad = ld2(AD + q), m = ld2(M + q);
+            st2(PHI + q, x.x + alpha * dd.x, x.y + alpha * dd.y);
+            const double r0 = r.x - alpha * ad.x, r1 = r.y - alpha * ad.y;
+            st2(R + q, r0, r1);
+            acc += r0 * (r0 * m.x);
+            acc += r1 * (r1 * m.y);
+        }
+    }
+    block_sum_then(acc, part, sc, then);
+}
+
+__global__ void __launch_bounds__(256) k3p_dir(Dom3 d, const double *__restrict__ R, const double *__restrict__ M,
+                                               double *__restrict__ DD, const int *gate, const Sc3 *sc)
+{
+    if (gate && *gate == 0) return;
+    const int ni = d.NX - 1, nj = d.NY - 1, nk = d.NZ - 1;
+    const int i = 2 * (blockIdx.x * 32 + threadIdx.x), j = blockIdx.y * 8 + threadIdx.y;
+    if (i >= ni || j >= nj) return;
+    const double beta = sc->p_beta;
+    const bool two = i + 1 < ni;
+#pragma unroll
+    for (int kk = 0; kk < PKB; kk++) {
+        const int k = blockIdx.z * PKB + kk;
+        if (k >= nk) break;
+        const long long q = at(d, i, j, k);
+        if (!two) {
+            DD[q] = R[q] * M[q] + beta * DD[q];
+            continue;
+        }
+        const double2 r = ld2(R + q), m = ld2(M + q), dd = ld2(DD + q);
+        st2(DD + q, r.x * m.x + beta * dd.x, r.y * m.y + beta * dd.y);
+    }
 }
 
 // host block (reference layout) <-> padded field
@@ -154,7 +327,8 @@ struct GpuExec {
     Sc3 *sc = nullptr;         // device scalars
     Sc3 *sc_host = nullptr;    // pinned mirror
     int *int_host = nullptr;   // pinned word
-    double *part = nullptr;    // NSLOT x NBR x 4 partial sums
+    double *part = nullptr;    // NSLOT x pstride partial sums
+    size_t pstride = 0;        // doubles per slot: 4 per block of the largest reduction grid
     Pend pend{};
     long long launches = 0;
     cudaError_t err = cudaSuccess;
@@ -205,7 +379,7 @@ struct GpuExec {
     void reduce(const Range &r, const int *gate, int slot, F f)
     {
         const int nb = blocks(r, NBR);
-        k3_reduce<N, MAX><<<nb, TPB, 0, stream>>>(r, gate, part + (size_t)slot * NBR * 4, f);
+        k3_reduce<N, MAX><<<nb, TPB, 0, stream>>>(r, gate, part + (size_t)slot * pstride, f);
         note();
         pend.nb[slot] = empty(r) ? 0 : nb;
         pend.nq[slot] = N;
@@ -215,9 +389,38 @@ struct GpuExec {
     template <class F>
     void scalar(const int *gate, F f)
     {
+        pend.stride = pstride;
         k3_scalar<<<1, TPB, 0, stream>>>(part, pend, gate, sc, f);
         note();
         pend.mask = 0;
+    }
+    // the pressure PCG iteration's three passes (k3p_*)
+    static dim3 pgrid(const Dom3 &d)
+    {
+        return dim3((unsigned)((d.NX - 1 + 63) / 64), (unsigned)((d.NY - 1 + 7) / 8), (unsigned)((d.NZ - 1 + PKB - 1) / PKB));
+    }
+    // the partials of these passes use the last slot, which the generic
+    // reductions of the pressure loop do not touch
+    template <class F>
+    void p_apply(const Dom3 &d, const double *CX, const double *CY, const double *CZ, const double *X, double *AD,
+                 const int *gate, F then)
+    {
+        k3p_apply<<<pgrid(d), dim3(32, 8), 0, stream>>>(d, CX, CY, CZ, X, AD, gate, part + (size_t)(NSLOT - 1) * pstride,
+                                                        sc, then);
+        note();
+    }
+    template <class F>
+    void p_update(const Dom3 &d, double *PHI, double *R, const double *DD, const double *AD, const double *M,
+                  const int *gate, F then)
+    {
+        k3p_update<<<pgrid(d), dim3(32, 8), 0, stream>>>(d, PHI, R, DD, AD, M, gate, sc,
+                                                         part + (size_t)(NSLOT - 1) * pstride, then);
+        note();
+    }
+    void p_dir(const Dom3 &d, const double *R, const double *M, double *DD, const int *gate)
+    {
+        k3p_dir<<<pgrid(d), dim3(32, 8), 0, stream>>>(d, R, M, DD, gate, sc);
+        note();
     }
     int read_int(const int *p)
     {
@@ -308,8 +511,9 @@ int create(const pvof_grid_desc *g, const pvof_params *p, int device, Handle **o
     if (!g->periodic[0] || g->periodic[1] || !g->periodic[2])
         return fail(PVOF_EINVAL, "the 3D mode needs x and z periodic and walls in y");
     if (g->NXM < 8 || g->NYM < 8 || g->NZM < 8) return fail(PVOF_EINVAL, "the 3D mode needs at least 8 cells per direction");
-    if (p->stencil_fp32 || p->pressure_warm_start || p->pressure_preconditioner)
-        return fail(PVOF_EINVAL, "the FP32 stencil form, the pressure warm starts and the spectral preconditioner are 2D only");
+    if (p->pressure_warm_start || p->pressure_preconditioner)
+        return fail(PVOF_EINVAL, "the pressure warm starts and the spectral preconditioner are 2D only");
+    if (p->stencil_fp32 < 0 || p->stencil_fp32 > 1) return fail(PVOF_EINVAL, "stencil_fp32 must be 0 or 1");
     const double hx = (g->xmax - g->xmin) / g->NXM, hy = (g->ymax - g->ymin) / g->NYM, hz = (g->zmax - g->zmin) / g->NZM;
     if (!(hx > 0 && hy > 0 && hz > 0)) return fail(PVOF_EINVAL, "empty box");
     CK3(cudaSetDevice(device));
@@ -386,10 +590,16 @@ int create(const pvof_grid_desc *g, const pvof_params *p, int device, Handle **o
     d.idx2 = ax[0].idc[1 + NG] * ax[0].idc[1 + NG];
     d.idy2 = ax[1].idc[1 + NG] * ax[1].idc[1 + NG];
     d.idz2 = ax[2].idc[1 + NG] * ax[2].idc[1 + NG];
-    if (cudaMalloc(&x.sc, sizeof(Sc3)) != cudaSuccess || cudaMalloc(&x.part, sizeof(double) * NSLOT * NBR * 4) != cudaSuccess)
+    d.idx_u1 = ax[0].idf[1 + NG];
+    {
+        const dim3 pg = GpuExec::pgrid(d);
+        const size_t nb = std::max((size_t)NBR, (size_t)pg.x * pg.y * pg.z);
+        x.pstride = 4 * nb;
+    }
+    if (cudaMalloc(&x.sc, sizeof(Sc3)) != cudaSuccess || cudaMalloc(&x.part, sizeof(double) * NSLOT * x.pstride) != cudaSuccess)
         return bail(fail(PVOF_ENOMEM, "device scalars"));
     cudaMemsetAsync(x.sc, 0, sizeof(Sc3), x.stream);
-    cudaMemsetAsync(x.part, 0, sizeof(double) * NSLOT * NBR * 4, x.stream);
+    cudaMemsetAsync(x.part, 0, sizeof(double) * NSLOT * x.pstride, x.stream);
     if (cudaMallocHost(&x.sc_host, sizeof(Sc3)) != cudaSuccess || cudaMallocHost(&x.int_host, sizeof(int)) != cudaSuccess)
         return bail(fail(PVOF_ENOMEM, "pinned scalars"));
     h->stage_elems = block_elems(d, false);

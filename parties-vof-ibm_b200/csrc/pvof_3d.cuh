@@ -73,6 +73,7 @@ struct Dom3 {
     // of the half cells that copy it; weight = wx[i] * wy[j] * wz[k]
     const double *wx, *wy, *wz;
     double idx2, idy2, idz2;   // idx_c[1]^2, ... (TwodOps.c:45-93)
+    double idx_u1;             // idx_u[1] (Pressure_set_RHS on a uniform grid), for host code
     Map3 map[K_COUNT];
 };
 
@@ -183,6 +184,51 @@ __host__ __device__ __forceinline__ double face_state(int weno_order, double vel
                      c(i - di, j - dj, k - dk), c(i - 2 * di, j - 2 * dj, k - 2 * dk));
     }
     return (vel >= 0.0) ? c(i - di, j - dj, k - dk) : c(i, j, k);
+}
+
+// single-precision forms of the stencils above (the FP32 stencil form):
+// operands and metrics rounded to float on load, arithmetic in float
+__host__ __device__ __forceinline__ float weno5f(float v0, float v1, float v2, float v3, float v4)
+{
+    const float eps = 1e-6f;
+    const float q0 = (2.0f * v0 - 7.0f * v1 + 11.0f * v2) * (1.0f / 6.0f);
+    const float q1 = (-v1 + 5.0f * v2 + 2.0f * v3) * (1.0f / 6.0f);
+    const float q2 = (2.0f * v2 + 5.0f * v3 - v4) * (1.0f / 6.0f);
+    const float t0 = v0 - 2.0f * v1 + v2, t1 = v0 - 4.0f * v1 + 3.0f * v2;
+    const float b0 = (13.0f / 12.0f) * (t0 * t0) + 0.25f * (t1 * t1);
+    const float t2 = v1 - 2.0f * v2 + v3, t3 = v1 - v3;
+    const float b1 = (13.0f / 12.0f) * (t2 * t2) + 0.25f * (t3 * t3);
+    const float t4 = v2 - 2.0f * v3 + v4, t5 = 3.0f * v2 - 4.0f * v3 + v4;
+    const float b2 = (13.0f / 12.0f) * (t4 * t4) + 0.25f * (t5 * t5);
+    const float a0 = 0.1f / ((eps + b0) * (eps + b0));
+    const float a1 = 0.6f / ((eps + b1) * (eps + b1));
+    const float a2 = 0.3f / ((eps + b2) * (eps + b2));
+    return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+}
+template <class Get>
+__host__ __device__ __forceinline__ float face_state_f(int weno_order, float vel, int i, int j, int k, int di, int dj,
+                                                       int dk, Get c)
+{
+    if (weno_order == 5) {
+        if (vel >= 0.0f)
+            return weno5f(c(i - 3 * di, j - 3 * dj, k - 3 * dk), c(i - 2 * di, j - 2 * dj, k - 2 * dk),
+                          c(i - di, j - dj, k - dk), c(i, j, k), c(i + di, j + dj, k + dk));
+        return weno5f(c(i + 2 * di, j + 2 * dj, k + 2 * dk), c(i + di, j + dj, k + dk), c(i, j, k),
+                      c(i - di, j - dj, k - dk), c(i - 2 * di, j - 2 * dj, k - 2 * dk));
+    }
+    return (vel >= 0.0f) ? c(i - di, j - dj, k - dk) : c(i, j, k);
+}
+template <class Get>
+__host__ __device__ __forceinline__ float lap3f(const Dom3 &d, int i, int j, int k, Get get)
+{
+    const float c = get(i, j, k);
+    const float dfdxE = (get(i + 1, j, k) - c) * (float)d.idx_c[i];
+    const float dfdxW = (c - get(i - 1, j, k)) * (float)((i != 0) ? d.idx_c[i - 1] : d.idx_c[i]);
+    const float dfdyN = (get(i, j + 1, k) - c) * (float)d.idy_c[j];
+    const float dfdyS = (c - get(i, j - 1, k)) * (float)((j != 0) ? d.idy_c[j - 1] : d.idy_c[j]);
+    const float dfdzF = (get(i, j, k + 1) - c) * (float)d.idz_c[k];
+    const float dfdzB = (c - get(i, j, k - 1)) * (float)((k != 0) ? d.idz_c[k - 1] : d.idz_c[k]);
+    return (dfdxE - dfdxW) * (float)d.idx_u[i] + (dfdyN - dfdyS) * (float)d.idy_v[j] + (dfdzF - dfdzB) * (float)d.idz_w[k];
 }
 
 // HARMONIC(AVG2, AVG2) of msolve_cg.c:78-79; the same expression as the
@@ -311,6 +357,7 @@ struct Sc3 {
     // pressure PCG (Pressure_solve_cg, psolve_cg.c:130-293)
     double p_gamma, p_gamma_new, p_alpha, p_beta, p_tol, p_avg;
     int p_iter, p_maxit, p_active, p_ran;
+    unsigned p_count;   // blocks of the current reduction that have written their partial sum
     // results kept for the statistics
     int ch_iters_out, v_iters_out[3], p_iters_out;
     double ch_rel_out, v_rms_out[3], p_res_out;
@@ -324,6 +371,7 @@ enum F3 {
     F3_U_EXO, F3_U_VXO, F3_U_RHS, F3_V_EXO, F3_V_VXO, F3_V_RHS, F3_W_EXO, F3_W_VXO, F3_W_RHS,
     F3_VR, F3_VD, F3_VAD, F3_VDIAG,
     F3_FSO_X, F3_FSO_Y, F3_FSO_Z, F3_FSN_X, F3_FSN_Y, F3_FSN_Z,
+    F3_PCX, F3_PCY, F3_PCZ,
     F3_COUNT
 };
 
@@ -633,6 +681,21 @@ __host__ __device__ __forceinline__ double p_apply(const Dom3 &d, const PFaces &
     return 1.0 * val;
 }
 
+// the same operator with the face coefficients of one solve stored: CX at
+// (i,j,k) is cxp of that cell and cxm of cell i+1 (2/(rho_i + rho_i+1) is the
+// same number seen from either side); CX, CY, CZ hold one layer below the
+// physical cells too
+__host__ __device__ __forceinline__ double p_apply_st(const Dom3 &d, const double *CX, const double *CY,
+                                                      const double *CZ, const double *X, int i, int j, int k)
+{
+    auto x = [&](int a, int b, int e) { return rd<K_PRESSURE>(d, X, a, b, e); };
+    const long long q = at(d, i, j, k);
+    const double xc = x(i, j, k);
+    const double val = CX[q] * (x(i + 1, j, k) - xc) - CX[q - 1] * (xc - x(i - 1, j, k)) + CY[q] * (x(i, j + 1, k) - xc) -
+                       CY[q - d.P] * (xc - x(i, j - 1, k)) + CZ[q] * (x(i, j, k + 1) - xc) - CZ[q - d.S] * (xc - x(i, j, k - 1));
+    return 1.0 * val;
+}
+
 // TwodOps_cell_center_divergence, 3D branch (TwodOps.c:12-43)
 __host__ __device__ __forceinline__ double cc_div(const Dom3 &d, const double *U, const double *V, const double *W, int i,
                                                   int j, int k, double ix, double iy, double iz)
@@ -658,6 +721,21 @@ __host__ __device__ __forceinline__ double f_sigma(const Dom3 &d, const Phase &p
     const double id = C == 0 ? d.idx_c[i - 1] : (C == 1 ? d.idy_c[j - 1] : d.idz_c[k - 1]);
     const double gradC = (c0 - c1) * id;
     return scale * psi_f * gradC;
+}
+
+// the same face force in single precision (the FP32 stencil form)
+template <int C>
+__host__ __device__ __forceinline__ double f_sigma_f(const Dom3 &d, const Phase &ph, float scale, const double *CL,
+                                                     const double *PSI, int i, int j, int k)
+{
+    const int a = C == 0 ? i - 1 : i, b = C == 1 ? j - 1 : j, e = C == 2 ? k - 1 : k;
+    const float c0 = (float)rd<K_SCALAR>(d, CL, i, j, k), c1 = (float)rd<K_SCALAR>(d, CL, a, b, e);
+    const float cl = 0.5f * (c0 + c1);
+    const float cg = 0.5f * ((float)ph.cg(c0) + (float)ph.cg(c1));
+    if (cl < 0.005f || cl > 0.995f || cg < 0.005f || cg > 0.995f) return 0.0;
+    const float psi_f = 0.5f * ((float)rd<K_SCALAR>(d, PSI, i, j, k) + (float)rd<K_SCALAR>(d, PSI, a, b, e));
+    const float id = (float)(C == 0 ? d.idx_c[i - 1] : (C == 1 ? d.idy_c[j - 1] : d.idz_c[k - 1]));
+    return (double)(scale * psi_f * ((c0 - c1) * id));
 }
 
 __host__ __device__ __forceinline__ double weight(const Dom3 &d, int i, int j, int k) { return d.wx[i] * d.wy[j] * d.wz[k]; }
@@ -691,6 +769,42 @@ struct Box3 {
         double *CUR = f[F3_CUR], *VEC = f[F3_VEC], *AUX = f[F3_AUX];
         const int wo = p.weno_order, s = stage;
         const double pe = p.Pe_CH, gs = gamb(s), zs = zetb(s);
+        if (p.stencil_fp32) {
+            // the FP32 stencil form: fluxes, their divergence and L S in float;
+            // each face flux is the same float number seen from both cells, so
+            // the advection still telescopes
+            x.cells(cells_range(d), nullptr, [=] __host__ __device__(int i, int j, int k) {
+                auto c = [&](int a, int b, int e) { return (float)rd<K_SCALAR>(d, CL, a, b, e); };
+                auto fx = [&](int a, int b, int e) {
+                    src<K_WRAP_U>(d, a, b, e);
+                    const float vel = (float)rd<K_U>(d, U, a, b, e);
+                    return vel * face_state_f(wo, vel, a, b, e, 1, 0, 0, c);
+                };
+                auto fy = [&](int a, int b, int e) {
+                    src<K_WRAP_V>(d, a, b, e);
+                    const float vel = (float)rd<K_V>(d, V, a, b, e);
+                    return vel * face_state_f(wo, vel, a, b, e, 0, 1, 0, c);
+                };
+                auto fz = [&](int a, int b, int e) {
+                    src<K_WRAP_W>(d, a, b, e);
+                    const float vel = (float)rd<K_W>(d, W, a, b, e);
+                    return vel * face_state_f(wo, vel, a, b, e, 0, 0, 1, c);
+                };
+                const float div = (fx(i + 1, j, k) - fx(i, j, k)) / (float)d.dx_c[i] +
+                                  (fy(i, j + 1, k) - fy(i, j, k)) / (float)d.dy_c[j] +
+                                  (fz(i, j, k + 1) - fz(i, j, k)) / (float)d.dz_c[k];
+                auto bulk = [&](int a, int b, int e) {
+                    const float cc = c(a, b, e);
+                    return 0.5f * cc - 1.5f * cc * cc + cc * cc * cc;
+                };
+                const double tmp = (double)lap3f(d, i, j, k, bulk) / pe;
+                const double cu = -(double)div + tmp;
+                const long long q = at(d, i, j, k);
+                CUR[q] = cu;
+                const double cl = CL[q];
+                VEC[q] = (s == 0) ? a_dt * cl + gs * cu : a_dt * cl + gs * cu + zs * RN[q];
+            });
+        } else
         // VOF_DIFFUSE_advect_WENO5 (:931-996) + compute_bulk_S / explicit_diffusion
         // (:865-885, :998-1016) + the rhs assembly (:1290-1310): the face fluxes
         // after their exchange are evaluated at the face the exchange copies
@@ -818,7 +932,10 @@ struct Box3 {
         });
     }
 
-    // diffuse_bound_liquid_fraction (VOF_DIFFUSE.c:1093-1127) without solids
+    // diffuse_bound_liquid_fraction (VOF_DIFFUSE.c:1093-1127) without solids;
+    // the mass change is summed over the physical cells (the reference's sum
+    // also counts the half cells, which copy physical ones), the cells that
+    // pvof_liquid_mass sums
     void clamp()
     {
         const Dom3 d = this->d;
@@ -833,7 +950,7 @@ struct Box3 {
             if (new_cl < 0.0) new_cl = 0.0;
             if (new_cl > max_cl) new_cl = max_cl;
             CL[q] = new_cl;
-            return Vec<1>{{(new_cl - old_cl) * weight(d, i, j, k)}};
+            return Vec<1>{{(new_cl - old_cl) * (d.dx_u[i] * d.dy_v[j] * d.dz_w[k])}};
         });
         x.scalar(nullptr, [=] __host__ __device__(Sc3 * s) { s->clamp_delta = s->sum[0][0]; });
     }
@@ -845,6 +962,16 @@ struct Box3 {
         const double *CL = f[F3_CL];
         double *PSI = f[F3_PSI];
         const double cn2 = p.Cn * p.Cn;
+        if (p.stencil_fp32) {
+            const float cn2f = (float)cn2;
+            x.cells(cells_range(d), nullptr, [=] __host__ __device__(int i, int j, int k) {
+                const float L = lap3f(d, i, j, k, [&](int a, int b, int e) { return (float)rd<K_SCALAR>(d, CL, a, b, e); });
+                const long long q = at(d, i, j, k);
+                const float c = (float)CL[q];
+                PSI[q] = (double)(c * c * c - 1.5f * c * c + 0.5f * c - cn2f * L);
+            });
+            return;
+        }
         x.cells(cells_range(d), nullptr, [=] __host__ __device__(int i, int j, int k) {
             const double L = lap3(d, i, j, k, [&](int a, int b, int e) { return rd<K_SCALAR>(d, CL, a, b, e); });
             const long long q = at(d, i, j, k);
@@ -864,8 +991,9 @@ struct Box3 {
         const double *CL = f[F3_CL], *PSI = f[F3_PSI];
         double *FN = f[F3_FSN_X + C], *FO = f[F3_FSO_X + C];
         const double scale = fsig_scale();
+        const int f32 = p.stencil_fp32;
         x.cells(face_range(d, C), nullptr, [=] __host__ __device__(int i, int j, int k) {
-            const double v = f_sigma<C>(d, ph, scale, CL, PSI, i, j, k);
+            const double v = f32 ? f_sigma_f<C>(d, ph, (float)scale, CL, PSI, i, j, k) : f_sigma<C>(d, ph, scale, CL, PSI, i, j, k);
             FN[at(d, i, j, k)] = v;
             FO[at(d, i, j, k)] = v;
         });
@@ -887,6 +1015,7 @@ struct Box3 {
         const double dpdx_src = (C == 0) ? 2.0 * (-p.dp_dx) : 0.0;
         const int st = p.surface_tension, grav = p.gravity;
         const double scale = fsig_scale(), Ri = p.richardson;
+        const int f32 = p.stencil_fp32;
         x.cells(face_range(d, C), nullptr, [=] __host__ __device__(int i, int j, int k) {
             const MomTerms t = mom_terms<C>(d, ph, iRe, CL, U, V, W, i, j, k);
             const int a = C == 0 ? i - 1 : i, b = C == 1 ? j - 1 : j, e = C == 2 ? k - 1 : k;
@@ -901,7 +1030,7 @@ struct Box3 {
             EXO[q] = t.ex;
             VXO[q] = t.vx;
             if (st) {
-                FN[q] = f_sigma<C>(d, ph, scale, CL, PSI, i, j, k);
+                FN[q] = f32 ? f_sigma_f<C>(d, ph, (float)scale, CL, PSI, i, j, k) : f_sigma<C>(d, ph, scale, CL, PSI, i, j, k);
                 r += FO[q];
             }
             if (grav) r += 2.0 * rf * Ri * gdir;
@@ -1000,14 +1129,22 @@ struct Box3 {
         const Dom3 d = this->d;
         const Phase ph = this->ph;
         const double *U = f[F3_U], *V = f[F3_V], *W = f[F3_W], *CL = f[F3_CL];
-        double *RHS = f[F3_PRHS], *M = f[F3_PM];
+        double *RHS = f[F3_PRHS], *M = f[F3_PM], *CX = f[F3_PCX], *CY = f[F3_PCY], *CZ = f[F3_PCZ];
         const double a_dt = 1.0 / (dt * 2.0 * bet(stage));
-        const double ihdt = d.idx_u[1] * a_dt;
+        const double ihdt = d.idx_u1 * a_dt;
+        // the +x, +y, +z face coefficients of the cells and of one layer below
+        x.cells(Range{-1, d.NX - 1, -1, d.NY - 1, -1, d.NZ - 1}, nullptr, [=] __host__ __device__(int i, int j, int k) {
+            auto rho = [&](int a, int b, int e) { return ph.rho(rd<K_SCALAR>(d, CL, a, b, e)); };
+            const long long q = at(d, i, j, k);
+            const double r0 = rho(i, j, k);
+            CX[q] = 2.0 / (r0 + rho(i + 1, j, k)) * d.idx2;
+            CY[q] = 2.0 / (r0 + rho(i, j + 1, k)) * d.idy2;
+            CZ[q] = 2.0 / (r0 + rho(i, j, k + 1)) * d.idz2;
+        });
         x.cells(cells_range(d), nullptr, [=] __host__ __device__(int i, int j, int k) {
             const long long q = at(d, i, j, k);
             RHS[q] = cc_div(d, U, V, W, i, j, k, ihdt, ihdt, ihdt);
-            const PFaces c = p_faces(d, ph, CL, i, j, k);
-            const double aii = c.cxm + c.cxp + c.cym + c.cyp + c.czm + c.czp;
+            const double aii = CX[q - 1] + CX[q] + CY[q - d.P] + CY[q] + CZ[q - d.S] + CZ[q];
             M[q] = 1.0 / (1.0 * aii + 1e-12);
         });
     }
@@ -1016,17 +1153,15 @@ struct Box3 {
     void pressure_solve()
     {
         const Dom3 d = this->d;
-        const Phase ph = this->ph;
         Sc3 *sc = x.sc;
-        const double *CL = f[F3_CL], *B = f[F3_PRHS], *M = f[F3_PM];
+        const double *B = f[F3_PRHS], *M = f[F3_PM], *CX = f[F3_PCX], *CY = f[F3_PCY], *CZ = f[F3_PCZ];
         double *PHI = f[F3_DP], *R = f[F3_PR], *DD = f[F3_PD], *AD = f[F3_PAD];
         const double tol = p.P_CG_ETOL;
         const int maxit = p.P_CG_MAXIT;
         const Range cr = cells_range(d);
         x.template reduce<1>(cr, nullptr, 0, [=] __host__ __device__(int i, int j, int k) {
-            const PFaces c = p_faces(d, ph, CL, i, j, k);
             const long long q = at(d, i, j, k);
-            const double r = B[q] - p_apply(d, c, PHI, i, j, k);
+            const double r = B[q] - p_apply_st(d, CX, CY, CZ, PHI, i, j, k);
             R[q] = r;
             const double z = r * M[q];
             DD[q] = z;
@@ -1045,23 +1180,15 @@ struct Box3 {
         const int *gate = &sc->p_active;
         for (int it = 0; it < maxit; it += CHUNK) {
             for (int q = 0; q < CHUNK && it + q < maxit; q++) {
-                x.template reduce<1>(cr, gate, 0, [=] __host__ __device__(int i, int j, int k) {
-                    const PFaces c = p_faces(d, ph, CL, i, j, k);
-                    const double ad = p_apply(d, c, DD, i, j, k);
-                    const long long q = at(d, i, j, k);
-                    AD[q] = ad;
-                    return Vec<1>{{DD[q] * ad}};
+                // AD = A d and d.AD (the executor's streaming form of p_apply_st),
+                // then the step length from the finished sum
+                x.p_apply(d, CX, CY, CZ, DD, AD, gate, [=] __host__ __device__(Sc3 * s, double dAd) {
+                    s->p_alpha = s->p_gamma / (dAd + 1e-30);
                 });
-                x.scalar(gate, [=] __host__ __device__(Sc3 * s) { s->p_alpha = s->p_gamma / (s->sum[0][0] + 1e-30); });
-                x.template reduce<1>(cr, gate, 0, [=] __host__ __device__(int i, int j, int k) {
-                    const double alpha = sc->p_alpha;
-                    const long long q = at(d, i, j, k);
-                    PHI[q] += alpha * DD[q];
-                    const double r = R[q] - alpha * AD[q];
-                    R[q] = r;
-                    return Vec<1>{{r * (r * M[q])}};
-                });
-                x.scalar(gate, [=] __host__ __device__(Sc3 * s) {
+                // phi += alpha d, r -= alpha AD and r.(M r), then the stopping test
+                // and the direction's coefficient
+                x.p_update(d, PHI, R, DD, AD, M, gate, [=] __host__ __device__(Sc3 * s, double rz) {
+                    s->sum[0][0] = rz;
                     s->p_iter++;
                     s->p_gamma_new = s->sum[0][0];
                     if (sqrt(s->p_gamma_new) < s->p_tol) {
@@ -1072,10 +1199,8 @@ struct Box3 {
                         if (s->p_iter >= s->p_maxit) s->p_active = 0;
                     }
                 });
-                x.cells(cr, gate, [=] __host__ __device__(int i, int j, int k) {
-                    const long long q = at(d, i, j, k);
-                    DD[q] = R[q] * M[q] + sc->p_beta * DD[q];
-                });
+                // d = M r + beta d
+                x.p_dir(d, R, M, DD, gate);
             }
             if (!x.read_int(gate)) break;
         }

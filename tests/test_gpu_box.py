@@ -112,3 +112,30 @@ def test_box_rejects_2d_only_calls_and_other_boundaries():
     grid.periodic[2] = 0
     with pytest.raises(runtime.PvofError):
         runtime.Solver(grid, params, device=0)
+
+
+def test_box_fp32_form_within_targets():
+    """The FP32 stencil form in 3D (WENO5 fluxes, chemical potential and
+    surface-tension force in float; the solvers, sums and fields in FP64)
+    against the plain FP64 path from the same start, 10 steps at density
+    ratio 1e-3: velocity relative L2 <= 1e-5, liquid volume <= 1e-6."""
+    from pvof import abi
+    grid, params, fields, d, meta = load_golden("box_rho1e-3")
+    p32 = abi.Params.from_buffer_copy(params)
+    p32.stencil_fp32 = 1
+    g64 = box_solver(grid, params, fields)
+    g32 = box_solver(grid, p32, fields)
+    for g in (g64, g32):
+        g.run_steps(10, meta["dt"])
+    num = den = 0.0
+    for f in ("U", "V", "W"):
+        a, b = owned(g32.get_g_range(f), f), owned(g64.get_g_range(f), f)
+        num += float(np.sum((a - b) ** 2))
+        den += float(np.sum(b ** 2))
+    vel = (num / den) ** 0.5
+    m64, m32 = g64.liquid_mass(), g32.liquid_mass()
+    vol = abs(m32 - m64) / m64
+    cl = rel_l2(owned(g32.get_g_range("C_L"), "C_L"), owned(g64.get_g_range("C_L"), "C_L"))
+    assert 0.0 < vel <= 1e-5 and vol <= 1e-6 and cl <= 1e-5, (vel, vol, cl)
+    g64.close()
+    g32.close()
