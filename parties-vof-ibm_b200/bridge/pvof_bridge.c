@@ -19,7 +19,10 @@
 #error "pvof_bridge.c bridges the diffuse-interface two-phase build (VOF, VOF_DIFFUSE)"
 #endif
 #if !defined(TWOD_CARTESIAN) && !defined(AXISYM_RZ)
-#error "pvof_bridge.c bridges the 2D modes (TWOD_CARTESIAN or AXISYM_RZ)"
+#define PVOF_BRIDGE_3D 1   /* the 3D mode: x and z periodic, walls in y, no solids */
+#if !defined(XPERIODIC) || !defined(ZPERIODIC) || defined(YPERIODIC) || defined(VOF_IBM)
+#error "pvof_bridge.c bridges 3D builds with XPERIODIC, ZPERIODIC, walls in y and no solids"
+#endif
 #endif
 
 static pvof_ctx *g_ctx;
@@ -56,7 +59,7 @@ static int bridge_fail(int rc, const char *what)
 static double ***field_array(Cart3d_bag *b, int f, int *ng)
 {
     VolumeFraction *vof = b->vof;
-    *ng = (f >= PVOF_F_U_EXPLICIT && f <= PVOF_F_FSIG_NEW_Y);
+    *ng = (f >= PVOF_F_U_EXPLICIT && f <= PVOF_F_FSIG_NEW_Y) || (f >= PVOF_F_W_EXPLICIT && f <= PVOF_F_FSIG_NEW_Z);
     switch (f) {
     case PVOF_F_C_L: return vof->C_L;
     case PVOF_F_C_G: return vof->C_G;
@@ -92,6 +95,15 @@ static double ***field_array(Cart3d_bag *b, int f, int *ng)
     case PVOF_F_FSIG_OLD_Y: return vof->f_sigma_old_y;
     case PVOF_F_FSIG_NEW_X: return vof->f_sigma_new_x;
     case PVOF_F_FSIG_NEW_Y: return vof->f_sigma_new_y;
+#ifdef PVOF_BRIDGE_3D
+    case PVOF_F_W_EXPLICIT: return b->w->ng_explicit;
+    case PVOF_F_W_EXPLICIT_OLD: return b->w->ng_explicit_old;
+    case PVOF_F_W_VISC_EXPLICIT: return b->w->ng_visc_explicit;
+    case PVOF_F_W_VISC_EXPLICIT_OLD: return b->w->ng_visc_explicit_old;
+    case PVOF_F_W_RHS: return b->w->ng_rhs;
+    case PVOF_F_FSIG_OLD_Z: return vof->f_sigma_old_z;
+    case PVOF_F_FSIG_NEW_Z: return vof->f_sigma_new_z;
+#endif
 #ifdef VOF_IBM
     case PVOF_F_NX_IBM: return vof->nx_IBM;
     case PVOF_F_NY_IBM: return vof->ny_IBM;
@@ -108,8 +120,31 @@ static double *field_block(Cart3d_bag *b, int f)
     return ng ? NG_BLOCK(a, b->grid) : FLOW_BLOCK(a, b->grid);
 }
 
+#ifdef PVOF_BRIDGE_3D
+/* the fields the 3D mode keeps: the rest are scratch or derived there */
+static int kept_3d(int f, int to_device)
+{
+    switch (f) {
+    case PVOF_F_C_G: case PVOF_F_RHO: case PVOF_F_MU:
+        return !to_device;
+    case PVOF_F_C_L: case PVOF_F_F: case PVOF_F_PSI_LG: case PVOF_F_CH_RHS_N: case PVOF_F_U: case PVOF_F_V:
+    case PVOF_F_W: case PVOF_F_P: case PVOF_F_DELTAP:
+    case PVOF_F_U_EXPLICIT_OLD: case PVOF_F_V_EXPLICIT_OLD: case PVOF_F_W_EXPLICIT_OLD:
+    case PVOF_F_U_VISC_EXPLICIT_OLD: case PVOF_F_V_VISC_EXPLICIT_OLD: case PVOF_F_W_VISC_EXPLICIT_OLD:
+    case PVOF_F_FSIG_OLD_X: case PVOF_F_FSIG_OLD_Y: case PVOF_F_FSIG_OLD_Z:
+    case PVOF_F_FSIG_NEW_X: case PVOF_F_FSIG_NEW_Y: case PVOF_F_FSIG_NEW_Z:
+        return 1;
+    default:
+        return 0;
+    }
+}
+#endif
+
 static int copy_field(Cart3d_bag *b, int f, int to_device)
 {
+#ifdef PVOF_BRIDGE_3D
+    if (!kept_3d(f, to_device)) return PVOF_OK;
+#endif
     double *blk = field_block(b, f);
     if (!blk) return PVOF_OK;
     size_t n = pvof_field_block_count(g_ctx, f);
@@ -126,10 +161,12 @@ static void grid_desc(Cart3d_bag *b, pvof_grid_desc *gd)
     gd->NYM = p->NYM;
     gd->NZM = p->NZM;
     gd->ghost_nodes = p->ghost_nodes;
-#ifdef AXISYM_RZ
+#if defined(AXISYM_RZ)
     gd->geometry = PVOF_GEOM_AXISYM;
-#else
+#elif defined(TWOD_CARTESIAN)
     gd->geometry = PVOF_GEOM_PLANAR;
+#else
+    gd->geometry = PVOF_GEOM_3D;
 #endif
 #ifdef XPERIODIC
     gd->periodic[0] = 1;
@@ -137,7 +174,7 @@ static void grid_desc(Cart3d_bag *b, pvof_grid_desc *gd)
 #ifdef YPERIODIC
     gd->periodic[1] = 1;
 #endif
-    gd->periodic[2] = 1;   /* the collapsed storage direction */
+    gd->periodic[2] = 1;   /* ZPERIODIC, or the collapsed storage direction of the 2D modes */
     for (int f = 0; f < 6; f++) gd->wall[f] = PVOF_WALL_NOSLIP;
 #ifdef LEFT_WALL_VELOCITY_FREESLIP
     gd->wall[PVOF_LEFT] = PVOF_WALL_FREESLIP;
@@ -272,6 +309,9 @@ int pvof_bridge_start(Cart3d_bag *b, int device)
     }
     TRYB(copy_field(b, PVOF_F_U, 1), "upload u");
     TRYB(copy_field(b, PVOF_F_V, 1), "upload v");
+#ifdef PVOF_BRIDGE_3D
+    TRYB(copy_field(b, PVOF_F_W, 1), "upload w");
+#endif
     TRYB(copy_field(b, PVOF_F_P, 1), "upload p");
 #if defined(VOF_IBM) && defined(LAG_PARTICLE_RESOLVED)
     TRYB(set_particles(b), "pvof_set_particles");
@@ -287,7 +327,10 @@ int pvof_bridge_substep(Cart3d_bag *b)
     TRYB(pvof_set_stage(g_ctx, p->which_stage, p->dt), "pvof_set_stage");
     /* Temporal_int_rk3 refreshes the cell-centred velocity before the first
      * stage of every step after the first (Temporal_int.c:420-424) */
+#ifndef PVOF_BRIDGE_3D
+    /* (the 3D mode evaluates the cell-centred velocity where it reads it) */
     if (p->which_stage == 0 && p->time != 0.0) TRYB(pvof_Velocity_cell_center(g_ctx), "Velocity_cell_center");
+#endif
     TRYB(pvof_substep(g_ctx, &g_stats), "pvof_substep");
     return PVOF_OK;
 }

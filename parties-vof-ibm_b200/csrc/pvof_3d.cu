@@ -117,11 +117,13 @@ __global__ void __launch_bounds__(TPB) k3_scalar(const double *part, Pend pd, co
 // the pressure PCG iteration (psolve_cg.c:209-253) as three streaming kernels
 // over the physical cells: a thread takes two neighbouring cells of a row
 // (16-byte loads; i = 0 is 16-byte aligned and every row and plane pitch is
-// even) in PKB consecutive planes, a block a 64 x 8 tile of (i, j).  Reads at
+// even) in PKB consecutive planes, a block a 64 x 8 tile of (i, j); PKB
+// planes per block keep the end-of-block reduction barrier and the number of
+// partial sums small.  Reads at
 // ghost and half cells go through the pressure ghost map; the arithmetic is
 // that of p_apply_st and of the reference's loops, operand for operand.
 // ---------------------------------------------------------------------------
-constexpr int PKB = 1;
+constexpr int PKB = 4;
 
 __device__ __forceinline__ double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
 __device__ __forceinline__ void st2(double *p, double a, double b) { *reinterpret_cast<double2 *>(p) = make_double2(a, b); }
@@ -164,8 +166,17 @@ __device__ __forceinline__ void block_sum_then(double acc, double *part, Sc3 *sc
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // eight loads in flight per thread; the order of the additions is fixed
     double a = 0.0;
-    for (unsigned b = t; b < nb; b += 256) a += __ldcg(part + (size_t)b * 4);
+    unsigned b = t;
+    for (; b + 7 * 256 < nb; b += 8 * 256) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) v[u] = __ldcg(part + (size_t)(b + u * 256) * 4);
+#pragma unroll
+        for (int u = 0; u < 8; u++) a += v[u];
+    }
+    for (; b < nb; b += 256) a += __ldcg(part + (size_t)b * 4);
     sh[t] = a;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
@@ -190,7 +201,7 @@ __global__ void __launch_bounds__(256, 4) k3p_apply(Dom3 d, const double *__rest
     double acc = 0.0;
     if (i < ni && j < nj) {
         const bool two = i + 1 < ni;
-#pragma unroll
+#pragma unroll 1
         for (int kk = 0; kk < PKB; kk++) {
             const int k = blockIdx.z * PKB + kk;
             if (k >= nk) break;

@@ -127,3 +127,31 @@ def test_reference_time_loop_with_a_sphere_drives_the_device():
         assert np.array_equal(pid_c, pid_g)
         assert np.abs(X_g - X_c).max() <= 1e-10
         assert np.abs(U_g - U_c).max() <= 1e-10
+
+
+def test_reference_3d_time_loop_drives_the_device():
+    """The 3D build (x and z periodic, no-slip walls in y, surface tension):
+    5 RK3 steps of the reference's loop on the CPU against the same program
+    whose substep runs on the B200 through the bridge; every dumped field
+    (the whole ghosted block, w included) within 1e-12."""
+    import pyoracle as po
+    from pvof import cases
+    need("rt3d_st")
+    need("rt3d_st_bridge")
+    grid, params, fields = cases.interface_box(16, 24, 12, Cn=0.1, amp_max=0.1, We=10.0, Re=100.0, rho_ratio=0.1,
+                                               mu_ratio=0.1, velocity_seed=6, velocity_amp=0.05,
+                                               **dict(TIGHT, CG_ETOL=1e-13))
+    steps = 5
+    flow = FLOW + ["w", "psi_LG"]
+    ng = NG + ["w_explicit_old", "w_visc_explicit_old", "f_sigma_old_x", "f_sigma_old_y", "f_sigma_old_z"]
+    with tempfile.TemporaryDirectory() as cpu, tempfile.TemporaryDirectory() as gpu:
+        po.run_reference("rt3d_st", cpu, grid, params, fields, steps, 1e-3, steps)
+        cp = po.run_reference("rt3d_st_bridge", gpu, grid, params, fields, steps, 1e-3, steps)
+        assert "REF_TIMING" in cp.stdout
+        worst = {}
+        for name in flow + ng:
+            a = np.fromfile(os.path.join(gpu, "out", "s%d_%s.bin" % (steps, name)), dtype="<f8")
+            b = np.fromfile(os.path.join(cpu, "out", "s%d_%s.bin" % (steps, name)), dtype="<f8")
+            worst[name] = rel_l2(a, b)
+        bad = {k: v for k, v in worst.items() if not v <= 1e-12}
+        assert not bad, bad
