@@ -61,6 +61,14 @@ case (1024x1024, three mobile cylinders on a flat interface, density ratio
 solver's own samples, then pressure iterations and time per step with a cold
 start, the same-stage warm start and the learned one.
 
+The line also carries a "box" object (unless --no-box): the 3D mode on the
+precision form's configuration, 256^3 (--box-grid), x and z periodic, walls
+in y, density ratio 1e-3: --box-warmup untimed steps and --box-steps timed
+steps of the plain FP64 path (device time, L2 flushed), the per-solver times
+of one more step with the pressure PCG's roofline, the FP32 stencil form
+from the same start with its errors against FP64 (unless --no-box-fp32), and
+the reference's 3D build on a --box-ref-grid box on one host core.
+
 --impl reference runs the reference's own time step (compiled from its
 sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host:
 --warmup untimed steps, then min(--steps, --ref-steps) timed ones.
@@ -1263,14 +1271,15 @@ def main():
     ap.add_argument("--poisson-grid", default="2048x2048")
     ap.add_argument("--poisson-maxit", type=int, default=3000)
     ap.add_argument("--poisson-reps", type=int, default=3)
-    ap.add_argument("--box", action="store_true",
-                    help="also time the 3D mode on --box-grid (the precision form's 256^3 box, plain FP64)")
+    ap.add_argument("--no-box", dest="box", action="store_false",
+                    help="leave out the 3D mode on --box-grid (the precision form's 256^3 box; timed by default)")
     ap.add_argument("--box-grid", default="256x256x256")
     ap.add_argument("--box-steps", type=int, default=2)
     ap.add_argument("--box-warmup", type=int, default=1)
     ap.add_argument("--box-maxit", type=int, default=20000)
-    ap.add_argument("--box-fp32", action="store_true",
-                    help="with --box, also the FP32 stencil form from the same start and its errors against FP64")
+    ap.add_argument("--no-box-fp32", dest="box_fp32", action="store_false",
+                    help="leave out the FP32 stencil form of the 3D box (from the same start, with its errors "
+                         "against FP64)")
     ap.add_argument("--box-ref-grid", default="32x32x32")
     ap.add_argument("--box-ref-steps", type=int, default=1)
     ap.add_argument("--axisym", action="store_true",
