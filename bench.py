@@ -462,7 +462,7 @@ def box_case(args, device):
     s.set_solver_timing(False)
     m1 = s.liquid_mass()
     clamp = s.clamp_mass_total()
-    ref64 = {f: s.get_g_range(f) for f in ("U", "V", "W")} if args.box_fp32 else None
+    ref64 = {f: s.get_g_range(f) for f in ("U", "V", "W")} if (args.box_fp32 or args.box_spectral) else None
     peak, peak_kind = measured_peak()
     names = ["biharmonic CG", "velocity PCG (u, v, w)", "pressure Jacobi-PCG"]
     out = {"case": "3D box %s, x and z periodic, no-slip walls in y, liquid layer under gas with a seeded 16-mode "
@@ -514,6 +514,41 @@ def box_case(args, device):
                             "volume_rel_error_vs_fp64": abs(m32 - m1) / m1,
                             "steps_compared": max(0, args.box_warmup) + nsteps + 1}
         s32.close()
+    if args.box_spectral:
+        # the spectral preconditioner form from the same start over the same
+        # steps (FP64 throughout), its throughput and its errors against the
+        # Jacobi path above
+        grid, params, fields = box_setup(n, args.box_maxit)
+        params.pressure_preconditioner = 1
+        ss = runtime.Solver(grid, params, device=device)
+        ss.set_fields({k: fields[k] for k in ("F", "U", "V", "W", "P")})
+        del fields
+        ss.initialize()
+        ss.run_steps(max(0, args.box_warmup), BOX_DT)
+        mss = 0.0
+        for _ in range(nsteps):
+            ss.flush_l2()
+            ss.timer_start()
+            ss.run_steps(1, BOX_DT)
+            mss += ss.timer_stop()
+        ss.set_solver_timing(True)
+        st_s = ss.run_steps(1, BOX_DT)
+        ts = ss.solver_timing(2)
+        ss.set_solver_timing(False)
+        num = den = 0.0
+        for f in ("U", "V", "W"):
+            a, b = ss.get_g_range(f), ref64[f]
+            num += float(np.sum((a - b) ** 2))
+            den += float(np.sum(b ** 2))
+        ms_ = ss.liquid_mass()
+        out["spectral_form"] = {"value": cells * nsteps / (mss * 1e-3), "ms_per_step": mss / nsteps,
+                                "vs_plain": (cells * nsteps / (mss * 1e-3)) / out["value"],
+                                "pressure_iterations_per_step": ts["iterations"],
+                                "pressure_us_per_iteration": 1e3 * ts["ms"] / max(1, ts["iterations"]),
+                                "last_substep_p_iters": st_s.p_iters,
+                                "velocity_rel_l2_vs_jacobi": (num / den) ** 0.5,
+                                "volume_rel_error_vs_jacobi": abs(ms_ - m1) / m1}
+        ss.close()
     if args.box_ref_steps > 0:
         r = box_reference(args.box_ref_grid, args.box_ref_steps)
         if r is not None:
@@ -1280,7 +1315,9 @@ def main():
     ap.add_argument("--no-box-fp32", dest="box_fp32", action="store_false",
                     help="leave out the FP32 stencil form of the 3D box (from the same start, with its errors "
                          "against FP64)")
-    ap.add_argument("--box-ref-grid", default="32x32x32")
+    ap.add_argument("--no-box-spectral", dest="box_spectral", action="store_false",
+                    help="leave out the 3D box with the spectral pressure preconditioner")
+    ap.add_argument("--box-ref-grid", default="64x64x64")
     ap.add_argument("--box-ref-steps", type=int, default=1)
     ap.add_argument("--axisym", action="store_true",
                     help="also time the axisymmetric bubble-and-sphere case (256x512) and the reference on it")

@@ -8,6 +8,7 @@
 // (a fixed grid of at most NBR blocks) and a one-block scalar kernel adds
 // the partials in a fixed order, so every sum is the same from run to run.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -295,6 +296,203 @@ __global__ void __launch_bounds__(256) k3p_dir(Dom3 d, const double *__restrict_
     }
 }
 
+// ---------------------------------------------------------------------------
+// spectral preconditioner of the 3D pressure PCG (pressure_preconditioner = 1):
+// z = s (-L)^-1 (s r), s = sqrt of the Jacobi weights, L the 7-point operator at
+// density one with the reference's ghost rules (x, z periodic, mirror walls in
+// y).  A real transform along x (N cells) and a complex one along z (K cells)
+// diagonalise L into one tridiagonal system in y per (kx, kz), solved by the
+// Thomas algorithm from host tables; the constant mode (the operator's null
+// space) gets eigenvalue 1 in units of 1/dy^2.  Spectrum layout: element
+// (kx, j, kz) at ((kz * ny + j) * H + kx), H = N/2 + 1.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+
+// twiddles w[q] = exp(sign 2 pi i q / n), q < n/2, into shared memory
+__device__ __forceinline__ void fft_twiddles(double2 *w, int n, double sign)
+{
+    for (int q = threadIdx.x; q < n / 2; q += blockDim.x) {
+        double sn, cs;
+        sincospi(sign * 2.0 * (double)q / (double)n, &sn, &cs);
+        w[q] = make_double2(cs, sn);
+    }
+}
+
+// in-place radix-2 transform of a[0..n) (n = 2^logn) by the nt threads of
+// one group (t = the thread's index in it); every thread of the block runs
+// the same stages, so the block barriers line up
+__device__ __forceinline__ void fft_group(double2 *a, const double2 *w, int n, int logn, int t, int nt)
+{
+    for (int q = t; q < n; q += nt) {
+        const int r = (int)(__brev((unsigned)q) >> (32 - logn));
+        if (r > q) {
+            const double2 x = a[q];
+            a[q] = a[r];
+            a[r] = x;
+        }
+    }
+    __syncthreads();
+    for (int s = 1; s <= logn; s++) {
+        const int half = 1 << (s - 1), stride = n >> s;
+        for (int b = t; b < n / 2; b += nt) {
+            const int pos = b & (half - 1), i0 = ((b >> (s - 1)) << s) + pos, i1 = i0 + half;
+            const double2 u = a[i0], v = cmul(w[pos * stride], a[i1]);
+            a[i0] = make_double2(u.x + v.x, u.y + v.y);
+            a[i1] = make_double2(u.x - v.x, u.y - v.y);
+        }
+        __syncthreads();
+    }
+}
+
+struct SpecDims {
+    int N, logN, K, logK, ny, H;
+    int nt_x, g_x;   // x transforms: threads per row, rows per block
+    int ch_z, nt_z;  // z transforms: columns per block, threads per column
+};
+
+// t = s r along each x row, forward transform, half spectrum out
+__global__ void __launch_bounds__(256) k3s_fwd_x(Dom3 d, SpecDims sd, const double *__restrict__ R,
+                                                 const double *__restrict__ M, double2 *__restrict__ SP, const int *gate)
+{
+    extern __shared__ double2 sm[];
+    if (gate && *gate == 0) return;
+    double2 *w = sm, *a = sm + sd.N / 2 + (threadIdx.x / sd.nt_x) * sd.N;
+    fft_twiddles(w, sd.N, -1.0);
+    const int g = threadIdx.x / sd.nt_x, t = threadIdx.x % sd.nt_x;
+    const long long row = (long long)blockIdx.x * sd.g_x + g;   // row = k * ny + j
+    const bool live = row < (long long)sd.K * sd.ny;
+    const int j = live ? (int)(row % sd.ny) : 0, k = live ? (int)(row / sd.ny) : 0;
+    for (int i = t; i < sd.N; i += sd.nt_x) {
+        double v = 0.0;
+        if (live) {
+            const long long q = at(d, i, j, k);
+            v = sqrt(M[q]) * R[q];
+        }
+        a[i] = make_double2(v, 0.0);
+    }
+    __syncthreads();
+    fft_group(a, w, sd.N, sd.logN, t, sd.nt_x);
+    if (live)
+        for (int kx = t; kx < sd.H; kx += sd.nt_x) SP[((long long)k * sd.ny + j) * sd.H + kx] = a[kx];
+}
+
+// complex transform along z of ch_z neighbouring kx columns at one j
+__global__ void __launch_bounds__(256) k3s_z(SpecDims sd, double2 *__restrict__ SP, double sign, const int *gate)
+{
+    extern __shared__ double2 sm[];
+    if (gate && *gate == 0) return;
+    double2 *w = sm, *a = sm + sd.K / 2;
+    fft_twiddles(w, sd.K, sign);
+    const int nchunk = (sd.H + sd.ch_z - 1) / sd.ch_z;
+    const int j = blockIdx.x / nchunk, kx0 = (blockIdx.x % nchunk) * sd.ch_z;
+    const int c = threadIdx.x / sd.nt_z, t = threadIdx.x % sd.nt_z;
+    // load: element (kz, col) of the tile at a[col * K + kz]
+    for (int e = threadIdx.x; e < sd.K * sd.ch_z; e += blockDim.x) {
+        const int kz = e / sd.ch_z, col = e % sd.ch_z, kx = kx0 + col;
+        a[col * sd.K + kz] = (kx < sd.H) ? SP[((long long)kz * sd.ny + j) * sd.H + kx] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    fft_group(a + c * sd.K, w, sd.K, sd.logK, t, sd.nt_z);
+    for (int e = threadIdx.x; e < sd.K * sd.ch_z; e += blockDim.x) {
+        const int kz = e / sd.ch_z, col = e % sd.ch_z, kx = kx0 + col;
+        if (kx < sd.H) SP[((long long)kz * sd.ny + j) * sd.H + kx] = a[col * sd.K + kz];
+    }
+}
+
+// one tridiagonal system in y per (kx, kz): (m_j)^-1 and c'_j from the host
+// tables; the right-hand side scaled by dy^2 / (N K) (the transforms' norm)
+__global__ void __launch_bounds__(256) k3s_tri(SpecDims sd, double2 *__restrict__ SP, const double *__restrict__ CP,
+                                               const double *__restrict__ IM, double scale, const int *gate)
+{
+    if (gate && *gate == 0) return;
+    const long long sys = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (sys >= (long long)sd.K * sd.H) return;
+    const int kz = (int)(sys / sd.H), kx = (int)(sys % sd.H);
+    const int ny = sd.ny;
+    auto idx = [&](int j) { return ((long long)kz * ny + j) * sd.H + kx; };
+    if (kx == 0 && kz == 0) {
+        // the constant mode: the mean-free part by the recurrence of rows
+        // 0..ny-2 from u_0 = 0, its mean removed, plus the mean itself
+        double2 mean = make_double2(0.0, 0.0);
+        for (int j = 0; j < ny; j++) {
+            const double2 v = SP[idx(j)];
+            mean.x += v.x;
+            mean.y += v.y;
+        }
+        mean.x *= scale / ny;
+        mean.y *= scale / ny;
+        double2 um = make_double2(0.0, 0.0), uc = make_double2(0.0, 0.0), su = make_double2(0.0, 0.0);
+        for (int j = 0; j < ny; j++) {
+            double2 un;
+            const double2 dj = SP[idx(j)];
+            const double2 dd = make_double2(dj.x * scale - mean.x, dj.y * scale - mean.y);
+            SP[idx(j)] = uc;
+            su.x += uc.x;
+            su.y += uc.y;
+            if (j == 0) un = make_double2(uc.x - dd.x, uc.y - dd.y);
+            else un = make_double2(2.0 * uc.x - um.x - dd.x, 2.0 * uc.y - um.y - dd.y);
+            um = uc;
+            uc = un;
+        }
+        su.x /= ny;
+        su.y /= ny;
+        for (int j = 0; j < ny; j++) {
+            const double2 v = SP[idx(j)];
+            SP[idx(j)] = make_double2(v.x - su.x + mean.x, v.y - su.y + mean.y);
+        }
+        return;
+    }
+    double2 dp = make_double2(0.0, 0.0);
+    for (int j = 0; j < ny; j++) {
+        const long long q = idx(j);
+        const double2 dj = SP[q];
+        const double im = IM[q];
+        dp = make_double2((dj.x * scale + dp.x) * im, (dj.y * scale + dp.y) * im);
+        SP[q] = dp;
+    }
+    double2 u = dp;
+    for (int j = ny - 2; j >= 0; j--) {
+        const long long q = idx(j);
+        const double2 v = SP[q];
+        const double cp = CP[q];
+        u = make_double2(v.x - cp * u.x, v.y - cp * u.y);
+        SP[q] = u;
+    }
+}
+
+// inverse transform along x from the half spectrum, z = s u
+__global__ void __launch_bounds__(256) k3s_inv_x(Dom3 d, SpecDims sd, const double2 *__restrict__ SP,
+                                                 const double *__restrict__ M, double *__restrict__ Z, const int *gate)
+{
+    extern __shared__ double2 sm[];
+    if (gate && *gate == 0) return;
+    double2 *w = sm, *a = sm + sd.N / 2 + (threadIdx.x / sd.nt_x) * sd.N;
+    fft_twiddles(w, sd.N, 1.0);
+    const int g = threadIdx.x / sd.nt_x, t = threadIdx.x % sd.nt_x;
+    const long long row = (long long)blockIdx.x * sd.g_x + g;
+    const bool live = row < (long long)sd.K * sd.ny;
+    const int j = live ? (int)(row % sd.ny) : 0, k = live ? (int)(row / sd.ny) : 0;
+    for (int kx = t; kx < sd.N; kx += sd.nt_x) {
+        double2 v = make_double2(0.0, 0.0);
+        if (live) {
+            if (kx < sd.H) {
+                v = SP[((long long)k * sd.ny + j) * sd.H + kx];
+            } else {
+                const double2 c = SP[((long long)k * sd.ny + j) * sd.H + (sd.N - kx)];
+                v = make_double2(c.x, -c.y);
+            }
+        }
+        a[kx] = v;
+    }
+    __syncthreads();
+    fft_group(a, w, sd.N, sd.logN, t, sd.nt_x);
+    if (live)
+        for (int i = t; i < sd.N; i += sd.nt_x) {
+            const long long q = at(d, i, j, k);
+            Z[q] = sqrt(M[q]) * a[i].x;
+        }
+}
+
 // host block (reference layout) <-> padded field
 __global__ void k3_unpack(Dom3 d, double *fld, const double *blk, int ng)
 {
@@ -433,6 +631,30 @@ struct GpuExec {
         k3p_dir<<<pgrid(d), dim3(32, 8), 0, stream>>>(d, R, M, DD, gate, sc);
         note();
     }
+    // spectral preconditioner: spectrum, tridiagonal tables, launch shapes
+    double2 *spec = nullptr;
+    double *tri_cp = nullptr, *tri_im = nullptr;
+    SpecDims sd{};
+    double spec_scale = 0.0;
+    // z = s (-L)^-1 (s r) over the physical cells (the k3s_* kernels)
+    void spec_apply(const Dom3 &d, const double *R, const double *M, double *Z, const int *gate)
+    {
+        const size_t smx = (size_t)(sd.N / 2 + sd.g_x * sd.N) * sizeof(double2);
+        const size_t smz = (size_t)(sd.K / 2 + sd.ch_z * sd.K) * sizeof(double2);
+        const unsigned gx = (unsigned)(((long long)sd.K * sd.ny + sd.g_x - 1) / sd.g_x);
+        const unsigned gz = (unsigned)(sd.ny * ((sd.H + sd.ch_z - 1) / sd.ch_z));
+        const unsigned gt = (unsigned)(((long long)sd.K * sd.H + 255) / 256);
+        k3s_fwd_x<<<gx, 256, smx, stream>>>(d, sd, R, M, spec, gate);
+        note();
+        k3s_z<<<gz, 256, smz, stream>>>(sd, spec, -1.0, gate);
+        note();
+        k3s_tri<<<gt, 256, 0, stream>>>(sd, spec, tri_cp, tri_im, spec_scale, gate);
+        note();
+        k3s_z<<<gz, 256, smz, stream>>>(sd, spec, 1.0, gate);
+        note();
+        k3s_inv_x<<<gx, 256, smx, stream>>>(d, sd, spec, M, Z, gate);
+        note();
+    }
     int read_int(const int *p)
     {
         if (cudaMemcpyAsync(int_host, p, sizeof(int), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
@@ -505,6 +727,9 @@ int destroy(Handle *h)
     cudaFree(h->flush);
     cudaFree(x.sc);
     cudaFree(x.part);
+    cudaFree(x.spec);
+    cudaFree(x.tri_cp);
+    cudaFree(x.tri_im);
     cudaFreeHost(x.sc_host);
     cudaFreeHost(x.int_host);
     for (int q = 0; q < 2; q++) {
@@ -516,14 +741,68 @@ int destroy(Handle *h)
     return PVOF_OK;
 }
 
+// the spectral preconditioner's launch shapes, tables and spectrum (host
+// tables in FP64 from the same modified wave numbers as the operator)
+static int spec_setup(GpuExec &x, const Dom3 &d, const pvof_grid_desc *g)
+{
+    SpecDims &sd = x.sd;
+    sd.N = d.NX - 1;
+    sd.K = d.NZ - 1;
+    sd.ny = d.NY - 1;
+    sd.H = sd.N / 2 + 1;
+    sd.logN = 0;
+    while ((1 << sd.logN) < sd.N) sd.logN++;
+    sd.logK = 0;
+    while ((1 << sd.logK) < sd.K) sd.logK++;
+    sd.nt_x = std::min(256, sd.N / 2);
+    sd.g_x = 256 / sd.nt_x;
+    int ch = (int)((48 * 1024 / sizeof(double2) - sd.K / 2) / sd.K);
+    sd.ch_z = 1;
+    while (sd.ch_z * 2 <= std::min(ch, 16)) sd.ch_z *= 2;
+    sd.nt_z = 256 / sd.ch_z;
+    const double idy2 = d.idy2;
+    x.spec_scale = (1.0 / idy2) / ((double)sd.N * (double)sd.K);
+    const size_t n = (size_t)sd.K * sd.ny * sd.H;
+    std::vector<double> cp(n), im(n);
+    const double pi = 3.14159265358979323846;
+    for (int kz = 0; kz < sd.K; kz++)
+        for (int kx = 0; kx < sd.H; kx++) {
+            const double lam = (d.idx2 * (2.0 - 2.0 * std::cos(2.0 * pi * kx / sd.N)) +
+                                d.idz2 * (2.0 - 2.0 * std::cos(2.0 * pi * kz / sd.K))) / idy2;
+            double cprev = 0.0;
+            for (int j = 0; j < sd.ny; j++) {
+                const double b = ((j == 0 || j == sd.ny - 1) ? 1.0 : 2.0) + lam;
+                const double m = b + cprev;
+                const size_t q = ((size_t)kz * sd.ny + j) * sd.H + kx;
+                im[q] = 1.0 / m;
+                cp[q] = -1.0 / m;
+                cprev = cp[q];
+            }
+        }
+    (void)g;
+    if (cudaMalloc(&x.spec, n * sizeof(double2)) != cudaSuccess || cudaMalloc(&x.tri_cp, n * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&x.tri_im, n * sizeof(double)) != cudaSuccess)
+        return fail(PVOF_ENOMEM, "device memory for the spectral preconditioner");
+    if (cudaMemcpy(x.tri_cp, cp.data(), n * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(x.tri_im, im.data(), n * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(PVOF_ECUDA, "spectral tables upload");
+    return PVOF_OK;
+}
+
 int create(const pvof_grid_desc *g, const pvof_params *p, int device, Handle **out)
 {
     *out = nullptr;
     if (!g->periodic[0] || g->periodic[1] || !g->periodic[2])
         return fail(PVOF_EINVAL, "the 3D mode needs x and z periodic and walls in y");
     if (g->NXM < 8 || g->NYM < 8 || g->NZM < 8) return fail(PVOF_EINVAL, "the 3D mode needs at least 8 cells per direction");
-    if (p->pressure_warm_start || p->pressure_preconditioner)
-        return fail(PVOF_EINVAL, "the pressure warm starts and the spectral preconditioner are 2D only");
+    if (p->pressure_warm_start) return fail(PVOF_EINVAL, "the pressure warm starts are 2D only");
+    if (p->pressure_preconditioner < 0 || p->pressure_preconditioner > 1)
+        return fail(PVOF_EINVAL, "pressure_preconditioner must be 0 (Jacobi) or 1 (spectral)");
+    if (p->pressure_preconditioner) {
+        auto pow2 = [](int n) { return n >= 2 && n <= 1024 && (n & (n - 1)) == 0; };
+        if (!pow2(g->NXM) || !pow2(g->NZM) || g->NYM > 4096)
+            return fail(PVOF_EINVAL, "the 3D spectral preconditioner needs power-of-two x and z cell counts up to 1024");
+    }
     if (p->stencil_fp32 < 0 || p->stencil_fp32 > 1) return fail(PVOF_EINVAL, "stencil_fp32 must be 0 or 1");
     const double hx = (g->xmax - g->xmin) / g->NXM, hy = (g->ymax - g->ymin) / g->NYM, hz = (g->zmax - g->zmin) / g->NZM;
     if (!(hx > 0 && hy > 0 && hz > 0)) return fail(PVOF_EINVAL, "empty box");
@@ -613,6 +892,7 @@ int create(const pvof_grid_desc *g, const pvof_params *p, int device, Handle **o
     cudaMemsetAsync(x.part, 0, sizeof(double) * NSLOT * x.pstride, x.stream);
     if (cudaMallocHost(&x.sc_host, sizeof(Sc3)) != cudaSuccess || cudaMallocHost(&x.int_host, sizeof(int)) != cudaSuccess)
         return bail(fail(PVOF_ENOMEM, "pinned scalars"));
+    if (p->pressure_preconditioner && spec_setup(x, d, g) < 0) return bail(PVOF_ENOMEM);
     h->stage_elems = block_elems(d, false);
     if (cudaMalloc(&h->stage, h->stage_elems * sizeof(double)) != cudaSuccess)
         return bail(fail(PVOF_ENOMEM, "staging block"));

@@ -371,7 +371,7 @@ enum F3 {
     F3_U_EXO, F3_U_VXO, F3_U_RHS, F3_V_EXO, F3_V_VXO, F3_V_RHS, F3_W_EXO, F3_W_VXO, F3_W_RHS,
     F3_VR, F3_VD, F3_VAD, F3_VDIAG,
     F3_FSO_X, F3_FSO_Y, F3_FSO_Z, F3_FSN_X, F3_FSN_Y, F3_FSN_Z,
-    F3_PCX, F3_PCY, F3_PCZ,
+    F3_PCX, F3_PCY, F3_PCZ, F3_PZ,
     F3_COUNT
 };
 
@@ -1149,9 +1149,91 @@ struct Box3 {
         });
     }
 
+    // the same solve preconditioned by z = s (-L)^-1 (s r), L the operator at
+    // density one and s the square root of the Jacobi weights
+    // (pressure_preconditioner = 1, no counterpart in the reference); the
+    // stopping test stays the reference's sqrt(r.Mr) < P_CG_ETOL, M the
+    // Jacobi weights, so the result moves within that tolerance
+    void pressure_solve_spectral()
+    {
+        const Dom3 d = this->d;
+        Sc3 *sc = x.sc;
+        const double *B = f[F3_PRHS], *M = f[F3_PM], *CX = f[F3_PCX], *CY = f[F3_PCY], *CZ = f[F3_PCZ];
+        double *PHI = f[F3_DP], *R = f[F3_PR], *DD = f[F3_PD], *AD = f[F3_PAD], *Z = f[F3_PZ];
+        const double tol = p.P_CG_ETOL;
+        const int maxit = p.P_CG_MAXIT;
+        const Range cr = cells_range(d);
+        x.template reduce<1>(cr, nullptr, 0, [=] __host__ __device__(int i, int j, int k) {
+            const long long q = at(d, i, j, k);
+            const double r = B[q] - p_apply_st(d, CX, CY, CZ, PHI, i, j, k);
+            R[q] = r;
+            return Vec<1>{{r * (r * M[q])}};
+        });
+        x.spec_apply(d, R, M, Z, nullptr);
+        x.template reduce<1>(cr, nullptr, 1, [=] __host__ __device__(int i, int j, int k) {
+            const long long q = at(d, i, j, k);
+            DD[q] = Z[q];
+            return Vec<1>{{R[q] * Z[q]}};
+        });
+        x.scalar(nullptr, [=] __host__ __device__(Sc3 * s) {
+            s->p_gamma = s->sum[1][0];
+            s->p_gamma_new = s->sum[0][0];   // r.Mr: the stopping quantity
+            s->p_iter = 0;
+            s->p_maxit = maxit;
+            s->p_tol = tol;
+            const int conv = sqrt(s->p_gamma_new) < tol;
+            s->p_ran = conv ? 0 : 1;
+            s->p_active = (conv || maxit <= 0) ? 0 : 1;
+        });
+        const int *gate = &sc->p_active;
+        for (int it = 0; it < maxit; it += CHUNK) {
+            for (int q = 0; q < CHUNK && it + q < maxit; q++) {
+                x.p_apply(d, CX, CY, CZ, DD, AD, gate, [=] __host__ __device__(Sc3 * s, double dAd) {
+                    s->p_alpha = s->p_gamma / (dAd + 1e-300);
+                });
+                x.p_update(d, PHI, R, DD, AD, M, gate, [=] __host__ __device__(Sc3 * s, double rMr) {
+                    s->p_iter++;
+                    s->p_gamma_new = rMr;
+                    if (sqrt(rMr) < s->p_tol) s->p_active = 0;
+                });
+                x.spec_apply(d, R, M, Z, gate);
+                x.template reduce<1>(cr, gate, 1, [=] __host__ __device__(int i, int j, int k) {
+                    const long long q = at(d, i, j, k);
+                    return Vec<1>{{R[q] * Z[q]}};
+                });
+                x.scalar(gate, [=] __host__ __device__(Sc3 * s) {
+                    const double g = s->sum[1][0];
+                    s->p_beta = g / (s->p_gamma + 1e-300);
+                    s->p_gamma = g;
+                    if (s->p_iter >= s->p_maxit) s->p_active = 0;
+                });
+                x.cells(cr, gate, [=] __host__ __device__(int i, int j, int k) {
+                    const long long q = at(d, i, j, k);
+                    DD[q] = Z[q] + sc->p_beta * DD[q];
+                });
+            }
+            if (!x.read_int(gate)) break;
+        }
+        const int *ran = &sc->p_ran;
+        const double count = (double)((long long)(d.NX - 1) * (d.NY - 1) * (d.NZ - 1));
+        x.template reduce<1>(cr, ran, 0, [=] __host__ __device__(int i, int j, int k) {
+            return Vec<1>{{PHI[at(d, i, j, k)]}};
+        });
+        x.scalar(ran, [=] __host__ __device__(Sc3 * s) { s->p_avg = s->sum[0][0] / count; });
+        x.cells(cr, ran, [=] __host__ __device__(int i, int j, int k) { PHI[at(d, i, j, k)] -= sc->p_avg; });
+        x.scalar(nullptr, [=] __host__ __device__(Sc3 * s) {
+            s->p_iters_out = s->p_iter;
+            s->p_res_out = sqrt(s->p_gamma_new);
+        });
+    }
+
     // Pressure_solve_cg (psolve_cg.c:130-293) for deltap from zero
     void pressure_solve()
     {
+        if (p.pressure_preconditioner) {
+            pressure_solve_spectral();
+            return;
+        }
         const Dom3 d = this->d;
         Sc3 *sc = x.sc;
         const double *B = f[F3_PRHS], *M = f[F3_PM], *CX = f[F3_PCX], *CY = f[F3_PCY], *CZ = f[F3_PCZ];
