@@ -130,8 +130,9 @@ typedef struct pvof_params {
      * diagonal; the solve still stops when sqrt(r^T D^-1 r), D the
      * Jacobi diagonal, is below P_CG_ETOL, so the result moves within that
      * tolerance.  Planar grids with x periodic, walls in y, a power-of-two x
-     * cell count up to 1024 and at most 1024 y cells; 0 is the reference's
-     * Jacobi-PCG */
+     * cell count up to 1024 and at most 1024 y cells; in the 3D mode the
+     * transforms run along x and z (power-of-two cell counts up to 1024) and
+     * the tridiagonal solves along y; 0 is the reference's Jacobi-PCG */
     int pressure_preconditioner;
     /* no counterpart in the reference: 1 drops the 1e-14 that the momentum
      * CG adds to its step-length and direction-update denominators

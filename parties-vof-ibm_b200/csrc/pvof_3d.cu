@@ -308,13 +308,13 @@ __global__ void __launch_bounds__(256) k3p_dir(Dom3 d, const double *__restrict_
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 
-// twiddles w[q] = exp(sign 2 pi i q / n), q < n/2, into shared memory
-__device__ __forceinline__ void fft_twiddles(double2 *w, int n, double sign)
+// twiddles w[q] = exp(sign 2 pi i q / n), q < n/2, into shared memory from
+// the table of exp(-2 pi i q / n) made once on the host
+__device__ __forceinline__ void fft_twiddles(double2 *w, const double2 *__restrict__ tab, int n, double sign)
 {
     for (int q = threadIdx.x; q < n / 2; q += blockDim.x) {
-        double sn, cs;
-        sincospi(sign * 2.0 * (double)q / (double)n, &sn, &cs);
-        w[q] = make_double2(cs, sn);
+        const double2 v = tab[q];
+        w[q] = make_double2(v.x, sign < 0.0 ? v.y : -v.y);
     }
 }
 
@@ -352,12 +352,13 @@ struct SpecDims {
 
 // t = s r along each x row, forward transform, half spectrum out
 __global__ void __launch_bounds__(256) k3s_fwd_x(Dom3 d, SpecDims sd, const double *__restrict__ R,
-                                                 const double *__restrict__ M, double2 *__restrict__ SP, const int *gate)
+                                                 const double *__restrict__ M, double2 *__restrict__ SP,
+                                                 const double2 *__restrict__ TW, const int *gate)
 {
     extern __shared__ double2 sm[];
     if (gate && *gate == 0) return;
     double2 *w = sm, *a = sm + sd.N / 2 + (threadIdx.x / sd.nt_x) * sd.N;
-    fft_twiddles(w, sd.N, -1.0);
+    fft_twiddles(w, TW, sd.N, -1.0);
     const int g = threadIdx.x / sd.nt_x, t = threadIdx.x % sd.nt_x;
     const long long row = (long long)blockIdx.x * sd.g_x + g;   // row = k * ny + j
     const bool live = row < (long long)sd.K * sd.ny;
@@ -377,12 +378,13 @@ __global__ void __launch_bounds__(256) k3s_fwd_x(Dom3 d, SpecDims sd, const doub
 }
 
 // complex transform along z of ch_z neighbouring kx columns at one j
-__global__ void __launch_bounds__(256) k3s_z(SpecDims sd, double2 *__restrict__ SP, double sign, const int *gate)
+__global__ void __launch_bounds__(256) k3s_z(SpecDims sd, double2 *__restrict__ SP, const double2 *__restrict__ TW,
+                                             double sign, const int *gate)
 {
     extern __shared__ double2 sm[];
     if (gate && *gate == 0) return;
     double2 *w = sm, *a = sm + sd.K / 2;
-    fft_twiddles(w, sd.K, sign);
+    fft_twiddles(w, TW, sd.K, sign);
     const int nchunk = (sd.H + sd.ch_z - 1) / sd.ch_z;
     const int j = blockIdx.x / nchunk, kx0 = (blockIdx.x % nchunk) * sd.ch_z;
     const int c = threadIdx.x / sd.nt_z, t = threadIdx.x % sd.nt_z;
@@ -442,32 +444,107 @@ __global__ void __launch_bounds__(256) k3s_tri(SpecDims sd, double2 *__restrict_
         }
         return;
     }
+    // both sweeps in runs of TU rows: a run's loads are all issued before its
+    // dependent chain of updates (a thread's loads would otherwise wait one
+    // memory latency per row)
+    constexpr int TU = 8;
     double2 dp = make_double2(0.0, 0.0);
-    for (int j = 0; j < ny; j++) {
-        const long long q = idx(j);
-        const double2 dj = SP[q];
-        const double im = IM[q];
-        dp = make_double2((dj.x * scale + dp.x) * im, (dj.y * scale + dp.y) * im);
-        SP[q] = dp;
+    for (int j0 = 0; j0 < ny; j0 += TU) {
+        double2 v[TU];
+        double m[TU];
+#pragma unroll
+        for (int u = 0; u < TU; u++)
+            if (j0 + u < ny) {
+                v[u] = SP[idx(j0 + u)];
+                m[u] = IM[idx(j0 + u)];
+            }
+#pragma unroll
+        for (int u = 0; u < TU; u++)
+            if (j0 + u < ny) {
+                dp = make_double2((v[u].x * scale + dp.x) * m[u], (v[u].y * scale + dp.y) * m[u]);
+                v[u] = dp;
+            }
+#pragma unroll
+        for (int u = 0; u < TU; u++)
+            if (j0 + u < ny) SP[idx(j0 + u)] = v[u];
     }
-    double2 u = dp;
-    for (int j = ny - 2; j >= 0; j--) {
-        const long long q = idx(j);
-        const double2 v = SP[q];
-        const double cp = CP[q];
-        u = make_double2(v.x - cp * u.x, v.y - cp * u.y);
-        SP[q] = u;
+    double2 x = dp;   // u_{ny-1}
+    for (int j1 = ny - 2; j1 >= 0; j1 -= TU) {
+        double2 v[TU];
+        double c[TU];
+#pragma unroll
+        for (int u = 0; u < TU; u++)
+            if (j1 - u >= 0) {
+                v[u] = SP[idx(j1 - u)];
+                c[u] = CP[idx(j1 - u)];
+            }
+#pragma unroll
+        for (int u = 0; u < TU; u++)
+            if (j1 - u >= 0) {
+                x = make_double2(v[u].x - c[u] * x.x, v[u].y - c[u] * x.y);
+                v[u] = x;
+            }
+#pragma unroll
+        for (int u = 0; u < TU; u++)
+            if (j1 - u >= 0) SP[idx(j1 - u)] = v[u];
     }
 }
 
-// inverse transform along x from the half spectrum, z = s u
+// the block's sum of a 1D block into part[block]; the last block adds them
+// all in block order and runs then(sc, sum) (block_sum_then for 1D blocks)
+template <class F>
+__device__ __forceinline__ void block_sum_then_1d(double acc, double *part, Sc3 *sc, F then)
+{
+    __shared__ double sh[256];
+    __shared__ bool last;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) sh[warp] = acc;
+    __syncthreads();
+    const unsigned nb = gridDim.x;
+    if (t == 0) {
+        double a = sh[0];
+        for (int q = 1; q < (int)(blockDim.x >> 5); q++) a += sh[q];
+        part[(size_t)blockIdx.x * 4] = a;
+        __threadfence();
+        last = (atomicAdd(&sc->p_count, 1u) == nb - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double a = 0.0;
+    unsigned b = t;
+    for (; b + 7 * 256 < nb; b += 8 * 256) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) v[u] = __ldcg(part + (size_t)(b + u * 256) * 4);
+#pragma unroll
+        for (int u = 0; u < 8; u++) a += v[u];
+    }
+    for (; b < nb; b += 256) a += __ldcg(part + (size_t)b * 4);
+    sh[t] = a;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (t < w) sh[t] += sh[t + w];
+        __syncthreads();
+    }
+    if (t == 0) {
+        sc->p_count = 0;
+        then(sc, sh[0]);
+    }
+}
+
+// inverse transform along x from the half spectrum, z = s u, and r.z
+template <class F>
 __global__ void __launch_bounds__(256) k3s_inv_x(Dom3 d, SpecDims sd, const double2 *__restrict__ SP,
-                                                 const double *__restrict__ M, double *__restrict__ Z, const int *gate)
+                                                 const double *__restrict__ M, const double *__restrict__ R,
+                                                 double *__restrict__ Z, const double2 *__restrict__ TW,
+                                                 const int *gate, double *part, Sc3 *sc, F then)
 {
     extern __shared__ double2 sm[];
     if (gate && *gate == 0) return;
     double2 *w = sm, *a = sm + sd.N / 2 + (threadIdx.x / sd.nt_x) * sd.N;
-    fft_twiddles(w, sd.N, 1.0);
+    fft_twiddles(w, TW, sd.N, 1.0);
     const int g = threadIdx.x / sd.nt_x, t = threadIdx.x % sd.nt_x;
     const long long row = (long long)blockIdx.x * sd.g_x + g;
     const bool live = row < (long long)sd.K * sd.ny;
@@ -486,11 +563,38 @@ __global__ void __launch_bounds__(256) k3s_inv_x(Dom3 d, SpecDims sd, const doub
     }
     __syncthreads();
     fft_group(a, w, sd.N, sd.logN, t, sd.nt_x);
+    double acc = 0.0;
     if (live)
         for (int i = t; i < sd.N; i += sd.nt_x) {
             const long long q = at(d, i, j, k);
-            Z[q] = sqrt(M[q]) * a[i].x;
+            const double z = sqrt(M[q]) * a[i].x;
+            Z[q] = z;
+            acc += R[q] * z;
         }
+    block_sum_then_1d(acc, part, sc, then);
+}
+
+// d = z + beta d (the spectral form's direction)
+__global__ void __launch_bounds__(256) k3p_dir_z(Dom3 d, const double *__restrict__ Z, double *__restrict__ DD,
+                                                 const int *gate, const Sc3 *sc)
+{
+    if (gate && *gate == 0) return;
+    const int ni = d.NX - 1, nj = d.NY - 1, nk = d.NZ - 1;
+    const int i = 2 * (blockIdx.x * 32 + threadIdx.x), j = blockIdx.y * 8 + threadIdx.y;
+    if (i >= ni || j >= nj) return;
+    const double beta = sc->p_beta;
+    const bool two = i + 1 < ni;
+    for (int kk = 0; kk < PKB; kk++) {
+        const int k = blockIdx.z * PKB + kk;
+        if (k >= nk) break;
+        const long long q = at(d, i, j, k);
+        if (!two) {
+            DD[q] = Z[q] + beta * DD[q];
+            continue;
+        }
+        const double2 z = ld2(Z + q), dd = ld2(DD + q);
+        st2(DD + q, z.x + beta * dd.x, z.y + beta * dd.y);
+    }
 }
 
 // host block (reference layout) <-> padded field
@@ -636,23 +740,33 @@ struct GpuExec {
     double *tri_cp = nullptr, *tri_im = nullptr;
     SpecDims sd{};
     double spec_scale = 0.0;
-    // z = s (-L)^-1 (s r) over the physical cells (the k3s_* kernels)
-    void spec_apply(const Dom3 &d, const double *R, const double *M, double *Z, const int *gate)
+    double2 *tw_x = nullptr, *tw_z = nullptr;   // exp(-2 pi i q / n), q < n/2
+    // z = s (-L)^-1 (s r) over the physical cells (the k3s_* kernels), then
+    // r.z and the scalar step then(sc, r.z) in the last block
+    static long long spec_xblocks(const SpecDims &sd) { return ((long long)sd.K * sd.ny + sd.g_x - 1) / sd.g_x; }
+    template <class F>
+    void spec_apply(const Dom3 &d, const double *R, const double *M, double *Z, const int *gate, F then)
     {
         const size_t smx = (size_t)(sd.N / 2 + sd.g_x * sd.N) * sizeof(double2);
         const size_t smz = (size_t)(sd.K / 2 + sd.ch_z * sd.K) * sizeof(double2);
         const unsigned gx = (unsigned)(((long long)sd.K * sd.ny + sd.g_x - 1) / sd.g_x);
         const unsigned gz = (unsigned)(sd.ny * ((sd.H + sd.ch_z - 1) / sd.ch_z));
         const unsigned gt = (unsigned)(((long long)sd.K * sd.H + 255) / 256);
-        k3s_fwd_x<<<gx, 256, smx, stream>>>(d, sd, R, M, spec, gate);
+        k3s_fwd_x<<<gx, 256, smx, stream>>>(d, sd, R, M, spec, tw_x, gate);
         note();
-        k3s_z<<<gz, 256, smz, stream>>>(sd, spec, -1.0, gate);
+        k3s_z<<<gz, 256, smz, stream>>>(sd, spec, tw_z, -1.0, gate);
         note();
         k3s_tri<<<gt, 256, 0, stream>>>(sd, spec, tri_cp, tri_im, spec_scale, gate);
         note();
-        k3s_z<<<gz, 256, smz, stream>>>(sd, spec, 1.0, gate);
+        k3s_z<<<gz, 256, smz, stream>>>(sd, spec, tw_z, 1.0, gate);
         note();
-        k3s_inv_x<<<gx, 256, smx, stream>>>(d, sd, spec, M, Z, gate);
+        k3s_inv_x<<<gx, 256, smx, stream>>>(d, sd, spec, M, R, Z, tw_x, gate, part + (size_t)(NSLOT - 1) * pstride, sc,
+                                             then);
+        note();
+    }
+    void p_dir_z(const Dom3 &d, const double *Z, double *DD, const int *gate)
+    {
+        k3p_dir_z<<<pgrid(d), dim3(32, 8), 0, stream>>>(d, Z, DD, gate, sc);
         note();
     }
     int read_int(const int *p)
@@ -730,6 +844,8 @@ int destroy(Handle *h)
     cudaFree(x.spec);
     cudaFree(x.tri_cp);
     cudaFree(x.tri_im);
+    cudaFree(x.tw_x);
+    cudaFree(x.tw_z);
     cudaFreeHost(x.sc_host);
     cudaFreeHost(x.int_host);
     for (int q = 0; q < 2; q++) {
@@ -780,6 +896,14 @@ static int spec_setup(GpuExec &x, const Dom3 &d, const pvof_grid_desc *g)
             }
         }
     (void)g;
+    std::vector<double2> twx((size_t)sd.N / 2), twz((size_t)sd.K / 2);
+    for (int q = 0; q < sd.N / 2; q++) twx[q] = make_double2(std::cos(2.0 * pi * q / sd.N), -std::sin(2.0 * pi * q / sd.N));
+    for (int q = 0; q < sd.K / 2; q++) twz[q] = make_double2(std::cos(2.0 * pi * q / sd.K), -std::sin(2.0 * pi * q / sd.K));
+    if (cudaMalloc(&x.tw_x, twx.size() * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&x.tw_z, twz.size() * sizeof(double2)) != cudaSuccess ||
+        cudaMemcpy(x.tw_x, twx.data(), twx.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(x.tw_z, twz.data(), twz.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(PVOF_ENOMEM, "twiddle tables");
     if (cudaMalloc(&x.spec, n * sizeof(double2)) != cudaSuccess || cudaMalloc(&x.tri_cp, n * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&x.tri_im, n * sizeof(double)) != cudaSuccess)
         return fail(PVOF_ENOMEM, "device memory for the spectral preconditioner");
@@ -881,9 +1005,13 @@ int create(const pvof_grid_desc *g, const pvof_params *p, int device, Handle **o
     d.idy2 = ax[1].idc[1 + NG] * ax[1].idc[1 + NG];
     d.idz2 = ax[2].idc[1 + NG] * ax[2].idc[1 + NG];
     d.idx_u1 = ax[0].idf[1 + NG];
+    if (p->pressure_preconditioner && spec_setup(x, d, g) < 0) return bail(PVOF_ENOMEM);
     {
+        // one partial sum per block of the largest reduction grid: the
+        // generic sums, the pressure passes and the spectral inverse-x pass
         const dim3 pg = GpuExec::pgrid(d);
-        const size_t nb = std::max((size_t)NBR, (size_t)pg.x * pg.y * pg.z);
+        size_t nb = std::max((size_t)NBR, (size_t)pg.x * pg.y * pg.z);
+        if (p->pressure_preconditioner) nb = std::max(nb, (size_t)GpuExec::spec_xblocks(x.sd));
         x.pstride = 4 * nb;
     }
     if (cudaMalloc(&x.sc, sizeof(Sc3)) != cudaSuccess || cudaMalloc(&x.part, sizeof(double) * NSLOT * x.pstride) != cudaSuccess)
@@ -892,7 +1020,6 @@ int create(const pvof_grid_desc *g, const pvof_params *p, int device, Handle **o
     cudaMemsetAsync(x.part, 0, sizeof(double) * NSLOT * x.pstride, x.stream);
     if (cudaMallocHost(&x.sc_host, sizeof(Sc3)) != cudaSuccess || cudaMallocHost(&x.int_host, sizeof(int)) != cudaSuccess)
         return bail(fail(PVOF_ENOMEM, "pinned scalars"));
-    if (p->pressure_preconditioner && spec_setup(x, d, g) < 0) return bail(PVOF_ENOMEM);
     h->stage_elems = block_elems(d, false);
     if (cudaMalloc(&h->stage, h->stage_elems * sizeof(double)) != cudaSuccess)
         return bail(fail(PVOF_ENOMEM, "staging block"));

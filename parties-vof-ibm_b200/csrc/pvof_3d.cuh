@@ -1169,14 +1169,13 @@ struct Box3 {
             R[q] = r;
             return Vec<1>{{r * (r * M[q])}};
         });
-        x.spec_apply(d, R, M, Z, nullptr);
-        x.template reduce<1>(cr, nullptr, 1, [=] __host__ __device__(int i, int j, int k) {
-            const long long q = at(d, i, j, k);
-            DD[q] = Z[q];
-            return Vec<1>{{R[q] * Z[q]}};
+        // z = P r and gamma = r.z, then d = z
+        x.spec_apply(d, R, M, Z, nullptr, [=] __host__ __device__(Sc3 * s, double rz) {
+            s->p_gamma = rz;
+            s->p_beta = 0.0;
         });
+        x.p_dir_z(d, Z, DD, nullptr);
         x.scalar(nullptr, [=] __host__ __device__(Sc3 * s) {
-            s->p_gamma = s->sum[1][0];
             s->p_gamma_new = s->sum[0][0];   // r.Mr: the stopping quantity
             s->p_iter = 0;
             s->p_maxit = maxit;
@@ -1196,21 +1195,13 @@ struct Box3 {
                     s->p_gamma_new = rMr;
                     if (sqrt(rMr) < s->p_tol) s->p_active = 0;
                 });
-                x.spec_apply(d, R, M, Z, gate);
-                x.template reduce<1>(cr, gate, 1, [=] __host__ __device__(int i, int j, int k) {
-                    const long long q = at(d, i, j, k);
-                    return Vec<1>{{R[q] * Z[q]}};
-                });
-                x.scalar(gate, [=] __host__ __device__(Sc3 * s) {
-                    const double g = s->sum[1][0];
+                // z = P r, r.z and the direction's coefficient, then d = z + beta d
+                x.spec_apply(d, R, M, Z, gate, [=] __host__ __device__(Sc3 * s, double g) {
                     s->p_beta = g / (s->p_gamma + 1e-300);
                     s->p_gamma = g;
                     if (s->p_iter >= s->p_maxit) s->p_active = 0;
                 });
-                x.cells(cr, gate, [=] __host__ __device__(int i, int j, int k) {
-                    const long long q = at(d, i, j, k);
-                    DD[q] = Z[q] + sc->p_beta * DD[q];
-                });
+                x.p_dir_z(d, Z, DD, gate);
             }
             if (!x.read_int(gate)) break;
         }
