@@ -66,8 +66,10 @@ precision form's configuration, 256^3 (--box-grid), x and z periodic, walls
 in y, density ratio 1e-3: --box-warmup untimed steps and --box-steps timed
 steps of the plain FP64 path (device time, L2 flushed), the per-solver times
 of one more step with the pressure PCG's roofline, the FP32 stencil form
-from the same start with its errors against FP64 (unless --no-box-fp32), and
-the reference's 3D build on a --box-ref-grid box on one host core.
+from the same start with its errors against FP64 (unless --no-box-fp32), the
+spectral pressure preconditioner from the same start (unless
+--no-box-spectral), and the reference's 3D build on a --box-ref-grid box on
+one host core.
 
 --impl reference runs the reference's own time step (compiled from its
 sources, single rank: oracle/_ref/ref_rt2d) on the same case on the host:
