@@ -332,7 +332,29 @@ __device__ __forceinline__ void fft_group(double2 *a, const double2 *w, int n, i
         }
     }
     __syncthreads();
-    for (int s = 1; s <= logn; s++) {
+    // two radix-2 stages per pass over shared memory: a thread takes the four
+    // elements the two stages combine (the same butterflies and twiddles as
+    // one stage at a time, so the same numbers), half the shared-memory round
+    // trips and barriers
+    int s = 1;
+    for (; s + 1 <= logn; s += 2) {
+        const int h = 1 << (s - 1), st0 = n >> s, st1 = n >> (s + 1);
+        for (int b = t; b < n / 4; b += nt) {
+            const int pos = b & (h - 1), p = ((b >> (s - 1)) << (s + 1)) + pos;
+            const double2 x0 = a[p], x1 = a[p + h], x2 = a[p + 2 * h], x3 = a[p + 3 * h];
+            const double2 w0 = w[pos * st0];
+            const double2 v1 = cmul(w0, x1), v3 = cmul(w0, x3);
+            const double2 y0 = make_double2(x0.x + v1.x, x0.y + v1.y), y1 = make_double2(x0.x - v1.x, x0.y - v1.y);
+            const double2 y2 = make_double2(x2.x + v3.x, x2.y + v3.y), y3 = make_double2(x2.x - v3.x, x2.y - v3.y);
+            const double2 u2 = cmul(w[pos * st1], y2), u3 = cmul(w[(pos + h) * st1], y3);
+            a[p] = make_double2(y0.x + u2.x, y0.y + u2.y);
+            a[p + 2 * h] = make_double2(y0.x - u2.x, y0.y - u2.y);
+            a[p + h] = make_double2(y1.x + u3.x, y1.y + u3.y);
+            a[p + 3 * h] = make_double2(y1.x - u3.x, y1.y - u3.y);
+        }
+        __syncthreads();
+    }
+    if (s == logn) {   // an odd number of stages: the last one alone
         const int half = 1 << (s - 1), stride = n >> s;
         for (int b = t; b < n / 2; b += nt) {
             const int pos = b & (half - 1), i0 = ((b >> (s - 1)) << s) + pos, i1 = i0 + half;
@@ -403,7 +425,7 @@ __global__ void __launch_bounds__(256) k3s_z(SpecDims sd, double2 *__restrict__ 
 
 // one tridiagonal system in y per (kx, kz): (m_j)^-1 and c'_j from the host
 // tables; the right-hand side scaled by dy^2 / (N K) (the transforms' norm)
-__global__ void __launch_bounds__(256) k3s_tri(SpecDims sd, double2 *__restrict__ SP, const double *__restrict__ CP,
+__global__ void __launch_bounds__(32) k3s_tri(SpecDims sd, double2 *__restrict__ SP, const double *__restrict__ CP,
                                                const double *__restrict__ IM, double scale, const int *gate)
 {
     if (gate && *gate == 0) return;
@@ -751,12 +773,13 @@ struct GpuExec {
         const size_t smz = (size_t)(sd.K / 2 + sd.ch_z * sd.K) * sizeof(double2);
         const unsigned gx = (unsigned)(((long long)sd.K * sd.ny + sd.g_x - 1) / sd.g_x);
         const unsigned gz = (unsigned)(sd.ny * ((sd.H + sd.ch_z - 1) / sd.ch_z));
-        const unsigned gt = (unsigned)(((long long)sd.K * sd.H + 255) / 256);
+        // one thread per system, a few thousand systems: blocks of 32 spread them over every SM
+        const unsigned gt = (unsigned)(((long long)sd.K * sd.H + 31) / 32);
         k3s_fwd_x<<<gx, 256, smx, stream>>>(d, sd, R, M, spec, tw_x, gate);
         note();
         k3s_z<<<gz, 256, smz, stream>>>(sd, spec, tw_z, -1.0, gate);
         note();
-        k3s_tri<<<gt, 256, 0, stream>>>(sd, spec, tri_cp, tri_im, spec_scale, gate);
+        k3s_tri<<<gt, 32, 0, stream>>>(sd, spec, tri_cp, tri_im, spec_scale, gate);
         note();
         k3s_z<<<gz, 256, smz, stream>>>(sd, spec, tw_z, 1.0, gate);
         note();
