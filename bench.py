@@ -429,7 +429,7 @@ def box_setup(n, maxit):
                                Re=1000.0, We=100.0, P_CG_MAXIT=maxit)
 
 
-def box_case(args, device):
+def box_case(args, device, with_ref=True):
     """The plain FP64 path in the 3D mode on --box-grid (default 256^3, the
     only configuration whose fields do not fit in L2): --box-warmup untimed
     steps, --box-steps timed steps (device time, L2 flushed before each), one
@@ -551,7 +551,7 @@ def box_case(args, device):
                                 "velocity_rel_l2_vs_jacobi": (num / den) ** 0.5,
                                 "volume_rel_error_vs_jacobi": abs(ms_ - m1) / m1}
         ss.close()
-    if args.box_ref_steps > 0:
+    if args.box_ref_steps > 0 and with_ref:
         r = box_reference(args.box_ref_grid, args.box_ref_steps)
         if r is not None:
             out["cpu_reference"] = {"value": r[0], "unit": UNIT, "cores": 1, "kind": "reference",
@@ -1194,7 +1194,7 @@ def run_ours(args):
     box = None
     if args.box:
         try:
-            box = box_case(args, local)
+            box = box_case(args, local, with_ref=(rank == 0 and ws == 1))
         except Exception as e:   # noqa: BLE001
             box = {"error": "%s: %s" % (type(e).__name__, e)}
     large = None
