@@ -22,7 +22,7 @@
  * and the whole-substep entry points: pvof_create/destroy, the field copies,
  * pvof_set_stage, pvof_initialize, pvof_substep, pvof_run_steps,
  * pvof_liquid_mass and the measurement calls (launch count, timers, L2
- * flush, clamp total).  Other entry points return PVOF_EINVAL on a 3D
+ * flush, clamp total, solver timing).  Other entry points return PVOF_EINVAL on a 3D
  * context.  In 3D the fields C_G, rho and mu are download-only (they are
  * functions of C_L), *_EXPLICIT and *_VISC_EXPLICIT equal their _OLD copies
  * after a substep, and CH_RHS_CUR equals CH_RHS_N.
