@@ -368,11 +368,14 @@ __device__ __forceinline__ void fft_group(double2 *a, const double2 *w, int n, i
 
 struct SpecDims {
     int N, logN, K, logK, ny, H;
-    int nt_x, g_x;   // x transforms: threads per row, rows per block
+    int nt_x, g_x;   // x transforms: threads per pair of rows, pairs per block
     int ch_z, nt_z;  // z transforms: columns per block, threads per column
 };
 
-// t = s r along each x row, forward transform, half spectrum out
+// t = s r along two x rows at once (one as the real part, the other as the
+// imaginary part of a complex row), forward transform, then the two half
+// spectra separated, X_a = (Z_k + conj Z_(N-k)) / 2 and
+// X_b = (Z_k - conj Z_(N-k)) / 2i, and stored
 __global__ void __launch_bounds__(256) k3s_fwd_x(Dom3 d, SpecDims sd, const double *__restrict__ R,
                                                  const double *__restrict__ M, double2 *__restrict__ SP,
                                                  const double2 *__restrict__ TW, const int *gate)
@@ -382,21 +385,30 @@ __global__ void __launch_bounds__(256) k3s_fwd_x(Dom3 d, SpecDims sd, const doub
     double2 *w = sm, *a = sm + sd.N / 2 + (threadIdx.x / sd.nt_x) * sd.N;
     fft_twiddles(w, TW, sd.N, -1.0);
     const int g = threadIdx.x / sd.nt_x, t = threadIdx.x % sd.nt_x;
-    const long long row = (long long)blockIdx.x * sd.g_x + g;   // row = k * ny + j
-    const bool live = row < (long long)sd.K * sd.ny;
-    const int j = live ? (int)(row % sd.ny) : 0, k = live ? (int)(row / sd.ny) : 0;
+    const long long rows = (long long)sd.K * sd.ny;
+    const long long ra = 2 * ((long long)blockIdx.x * sd.g_x + g), rb = ra + 1;   // row = k * ny + j
+    const bool la = ra < rows, lb = rb < rows;
+    const int ja = la ? (int)(ra % sd.ny) : 0, ka = la ? (int)(ra / sd.ny) : 0;
+    const int jb = lb ? (int)(rb % sd.ny) : 0, kb = lb ? (int)(rb / sd.ny) : 0;
     for (int i = t; i < sd.N; i += sd.nt_x) {
-        double v = 0.0;
-        if (live) {
-            const long long q = at(d, i, j, k);
-            v = sqrt(M[q]) * R[q];
+        double va = 0.0, vb = 0.0;
+        if (la) {
+            const long long q = at(d, i, ja, ka);
+            va = sqrt(M[q]) * R[q];
         }
-        a[i] = make_double2(v, 0.0);
+        if (lb) {
+            const long long q = at(d, i, jb, kb);
+            vb = sqrt(M[q]) * R[q];
+        }
+        a[i] = make_double2(va, vb);
     }
     __syncthreads();
     fft_group(a, w, sd.N, sd.logN, t, sd.nt_x);
-    if (live)
-        for (int kx = t; kx < sd.H; kx += sd.nt_x) SP[((long long)k * sd.ny + j) * sd.H + kx] = a[kx];
+    for (int kx = t; kx < sd.H; kx += sd.nt_x) {
+        const double2 zk = a[kx], zn = a[(sd.N - kx) & (sd.N - 1)];
+        if (la) SP[ra * sd.H + kx] = make_double2(0.5 * (zk.x + zn.x), 0.5 * (zk.y - zn.y));
+        if (lb) SP[rb * sd.H + kx] = make_double2(0.5 * (zk.y + zn.y), -0.5 * (zk.x - zn.x));
+    }
 }
 
 // complex transform along z of ch_z neighbouring kx columns at one j
@@ -556,7 +568,9 @@ __device__ __forceinline__ void block_sum_then_1d(double acc, double *part, Sc3 
     }
 }
 
-// inverse transform along x from the half spectrum, z = s u, and r.z
+// inverse transform along x of two rows at once (the complex row X_a + i X_b,
+// each spectrum extended by its Hermitian symmetry; row a comes back as the
+// real part, row b as the imaginary part), z = s u, and r.z
 template <class F>
 __global__ void __launch_bounds__(256) k3s_inv_x(Dom3 d, SpecDims sd, const double2 *__restrict__ SP,
                                                  const double *__restrict__ M, const double *__restrict__ R,
@@ -568,31 +582,43 @@ __global__ void __launch_bounds__(256) k3s_inv_x(Dom3 d, SpecDims sd, const doub
     double2 *w = sm, *a = sm + sd.N / 2 + (threadIdx.x / sd.nt_x) * sd.N;
     fft_twiddles(w, TW, sd.N, 1.0);
     const int g = threadIdx.x / sd.nt_x, t = threadIdx.x % sd.nt_x;
-    const long long row = (long long)blockIdx.x * sd.g_x + g;
-    const bool live = row < (long long)sd.K * sd.ny;
-    const int j = live ? (int)(row % sd.ny) : 0, k = live ? (int)(row / sd.ny) : 0;
+    const long long rows = (long long)sd.K * sd.ny;
+    const long long ra = 2 * ((long long)blockIdx.x * sd.g_x + g), rb = ra + 1;
+    const bool la = ra < rows, lb = rb < rows;
+    const int ja = la ? (int)(ra % sd.ny) : 0, ka = la ? (int)(ra / sd.ny) : 0;
+    const int jb = lb ? (int)(rb % sd.ny) : 0, kb = lb ? (int)(rb / sd.ny) : 0;
     for (int kx = t; kx < sd.N; kx += sd.nt_x) {
-        double2 v = make_double2(0.0, 0.0);
-        if (live) {
-            if (kx < sd.H) {
-                v = SP[((long long)k * sd.ny + j) * sd.H + kx];
-            } else {
-                const double2 c = SP[((long long)k * sd.ny + j) * sd.H + (sd.N - kx)];
-                v = make_double2(c.x, -c.y);
-            }
+        const bool lo = kx < sd.H;
+        const int c = lo ? kx : sd.N - kx;
+        const double sg = lo ? 1.0 : -1.0;
+        double2 xa = make_double2(0.0, 0.0), xb = make_double2(0.0, 0.0);
+        if (la) {
+            const double2 v = SP[ra * sd.H + c];
+            xa = make_double2(v.x, sg * v.y);
         }
-        a[kx] = v;
+        if (lb) {
+            const double2 v = SP[rb * sd.H + c];
+            xb = make_double2(v.x, sg * v.y);
+        }
+        a[kx] = make_double2(xa.x - xb.y, xa.y + xb.x);
     }
     __syncthreads();
     fft_group(a, w, sd.N, sd.logN, t, sd.nt_x);
     double acc = 0.0;
-    if (live)
-        for (int i = t; i < sd.N; i += sd.nt_x) {
-            const long long q = at(d, i, j, k);
+    for (int i = t; i < sd.N; i += sd.nt_x) {
+        if (la) {
+            const long long q = at(d, i, ja, ka);
             const double z = sqrt(M[q]) * a[i].x;
             Z[q] = z;
             acc += R[q] * z;
         }
+        if (lb) {
+            const long long q = at(d, i, jb, kb);
+            const double z = sqrt(M[q]) * a[i].y;
+            Z[q] = z;
+            acc += R[q] * z;
+        }
+    }
     block_sum_then_1d(acc, part, sc, then);
 }
 
@@ -765,13 +791,17 @@ struct GpuExec {
     double2 *tw_x = nullptr, *tw_z = nullptr;   // exp(-2 pi i q / n), q < n/2
     // z = s (-L)^-1 (s r) over the physical cells (the k3s_* kernels), then
     // r.z and the scalar step then(sc, r.z) in the last block
-    static long long spec_xblocks(const SpecDims &sd) { return ((long long)sd.K * sd.ny + sd.g_x - 1) / sd.g_x; }
+    // x transforms: one pair of rows per nt_x threads, g_x pairs per block
+    static long long spec_xblocks(const SpecDims &sd)
+    {
+        return (((long long)sd.K * sd.ny + 1) / 2 + sd.g_x - 1) / sd.g_x;
+    }
     template <class F>
     void spec_apply(const Dom3 &d, const double *R, const double *M, double *Z, const int *gate, F then)
     {
         const size_t smx = (size_t)(sd.N / 2 + sd.g_x * sd.N) * sizeof(double2);
         const size_t smz = (size_t)(sd.K / 2 + sd.ch_z * sd.K) * sizeof(double2);
-        const unsigned gx = (unsigned)(((long long)sd.K * sd.ny + sd.g_x - 1) / sd.g_x);
+        const unsigned gx = (unsigned)spec_xblocks(sd);
         const unsigned gz = (unsigned)(sd.ny * ((sd.H + sd.ch_z - 1) / sd.ch_z));
         // one thread per system, a few thousand systems: blocks of 32 spread them over every SM
         const unsigned gt = (unsigned)(((long long)sd.K * sd.H + 31) / 32);
